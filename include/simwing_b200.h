@@ -1,0 +1,543 @@
+/*
+ * simwing_b200.h -- C-ABI of the B200 XPBD structural solver.
+ *
+ * The entry points replace SimWing's structural adapter
+ * `simwing::fsi::Structure` (src/fsi/structure.h:273-309) and the XPBD core
+ * step it drives (`softwing::SoftBody::step` / `stepCoupled`,
+ * src/softwing/soft_body.cpp:981-1070). Only plain C types cross this
+ * boundary: fixed-width integers, doubles, floats and pointers with explicit
+ * sizes. Every function returns an `swb_status`; on a non-OK status a
+ * human-readable message is available from `swb_last_error()` (thread-local).
+ *
+ * Index fields are 64-bit like the reference's std::size_t indices.
+ * Doubles are used on the boundary (the reference is FP64); the device state
+ * is FP32.
+ */
+#ifndef SIMWING_B200_H
+#define SIMWING_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWB_ABI_VERSION 1u
+
+/* ------------------------------------------------------------------------ */
+/* Status codes.  The reference throws typed exceptions; each maps to one    */
+/* status (std::invalid_argument, std::out_of_range, SuspensionError,         */
+/* ContactStepError).  A failed step restores the pre-step state before it   */
+/* returns, as Structure::step does (src/fsi/structure.cpp:807-831).         */
+/* ------------------------------------------------------------------------ */
+typedef enum swb_status {
+    SWB_OK = 0,
+    SWB_INVALID_ARGUMENT = 1,   /* std::invalid_argument                    */
+    SWB_OUT_OF_RANGE = 2,       /* std::out_of_range                        */
+    SWB_SUSPENSION_ERROR = 3,   /* softwing::SuspensionError                */
+    SWB_CONTACT_ERROR = 4,      /* softwing::ContactStepError               */
+    SWB_NON_FINITE = 5,         /* device detected NaN/Inf in the trial step */
+    SWB_SYNC_TIMEOUT = 6,       /* a bounded device-wide barrier gave up     */
+    SWB_CUDA_ERROR = 7,         /* CUDA runtime failure                      */
+    SWB_UNSUPPORTED = 8,        /* feature not available in this build       */
+    SWB_OUT_OF_MEMORY = 9
+} swb_status;
+
+/* Thread-local message of the last failing call on this thread. */
+const char* swb_last_error(void);
+uint32_t swb_abi_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Definition: mirrors simwing::fsi::StructureDefinition                     */
+/* (src/fsi/structure.h:16-172).                                             */
+/* ------------------------------------------------------------------------ */
+typedef struct swb_vec3 {
+    double x, y, z;
+} swb_vec3;
+
+typedef struct swb_quat {
+    double w, x, y, z;
+} swb_quat;
+
+/* StructureNodeDefinition (structure.h:32-36) */
+typedef struct swb_node_def {
+    swb_vec3 position;
+    double mass;
+    uint32_t fixed;
+    uint32_t reserved;
+} swb_node_def;
+
+/* StructureTriangleDefinition (structure.h:38-40) plus the per-face pressure
+ * jump of softwing::Triangle::pressureDifference (soft_body.h:60-65).  A
+ * positive value pushes along the right-hand normal of (a, b, c). */
+typedef struct swb_triangle_def {
+    uint64_t nodes[3];
+    double pressure_difference;
+} swb_triangle_def;
+
+/* StructureConstraintKind (structure.h:42-47) */
+enum {
+    SWB_CONSTRAINT_DISTANCE = 1,
+    SWB_CONSTRAINT_CABLE = 2,
+    SWB_CONSTRAINT_SUSPENSION_TIE = 3,
+    SWB_CONSTRAINT_SEAM_STITCH = 4
+};
+
+/* StructureConstraintDefinition (structure.h:49-55) */
+typedef struct swb_constraint_def {
+    uint32_t kind;
+    uint32_t reserved;
+    uint64_t first_node;
+    uint64_t second_node;
+    double rest_length;
+    double compliance;
+} swb_constraint_def;
+
+/* StructureMembraneMaterial (structure.h:63-72) */
+typedef struct swb_membrane_material {
+    double warp_stiffness;
+    double weft_stiffness;
+    double coupling_stiffness;
+    double shear_stiffness;
+    double warp_pretension;
+    double weft_pretension;
+    double damping_seconds;
+    double compression_stiffness_ratio;
+} swb_membrane_material;
+
+enum {
+    SWB_ROLE_BULK = 1,
+    SWB_ROLE_SEAM = 2,
+    SWB_ROLE_REINFORCEMENT = 3
+};
+
+/* StructureMembraneDefinition (structure.h:74-79) */
+typedef struct swb_membrane_def {
+    uint64_t triangle;
+    double chart[3][2];
+    swb_membrane_material material;
+    uint32_t role;
+    uint32_t reserved;
+} swb_membrane_def;
+
+/* StructureDihedralDefinition (structure.h:81-85).  nodes = {a, b, c, d}:
+ * a-b is the hinge, c belongs to face (a, b, c), d to face (b, a, d). */
+typedef struct swb_dihedral_def {
+    uint64_t nodes[4];
+    double rest_angle;
+    double compliance;
+} swb_dihedral_def;
+
+/* StructureFabricContactDefinition (structure.h:90-97) */
+typedef struct swb_fabric_contact_def {
+    double half_thickness;
+    double normal_compliance;
+    double static_friction;
+    double dynamic_friction;
+} swb_fabric_contact_def;
+
+/* StructureSuspensionEndpointKind (structure.h:108-112) */
+enum {
+    SWB_ENDPOINT_SURFACE_ATTACHMENT = 1,
+    SWB_ENDPOINT_JUNCTION = 2,
+    SWB_ENDPOINT_PILOT_HARNESS = 3
+};
+
+typedef struct swb_suspension_endpoint {
+    uint32_t kind;
+    uint32_t reserved;
+    uint64_t stable_id;
+} swb_suspension_endpoint;
+
+typedef struct swb_suspension_attachment {
+    uint64_t stable_id;
+    uint64_t node;
+} swb_suspension_attachment;
+
+typedef struct swb_suspension_junction {
+    uint64_t stable_id;
+    uint64_t node;
+} swb_suspension_junction;
+
+typedef struct swb_pilot_harness {
+    uint64_t stable_id;
+    swb_vec3 local_position;
+} swb_pilot_harness;
+
+/* StructureSuspensionSegmentDefinition (structure.h:133-141) */
+typedef struct swb_suspension_segment {
+    uint64_t stable_id;
+    swb_suspension_endpoint from;
+    swb_suspension_endpoint to;
+    double rest_length;
+    double axial_stiffness;
+    double axial_damping;
+    uint32_t role;
+    uint32_t reserved;
+} swb_suspension_segment;
+
+/* StructureSuspensionDefinition (structure.h:143-162) */
+typedef struct swb_suspension_def {
+    uint64_t pilot_stable_id;
+    double pilot_mass;
+    swb_vec3 pilot_com_local;
+    swb_vec3 pilot_initial_com_world;
+    swb_vec3 pilot_initial_linear_velocity;
+    swb_vec3 pilot_initial_angular_velocity;
+    swb_quat pilot_initial_body_to_world;
+    swb_vec3 pilot_principal_inertia;
+    uint64_t attachment_count;
+    const swb_suspension_attachment* attachments;
+    uint64_t junction_count;
+    const swb_suspension_junction* junctions;
+    uint64_t harness_count;
+    const swb_pilot_harness* harness_points;
+    uint64_t segment_count;
+    const swb_suspension_segment* segments;
+    int32_t solver_iterations;
+    int32_t reserved;
+    double attachment_tolerance;
+    double minimum_line_length;
+    double maximum_line_residual;
+    double maximum_control_work;
+} swb_suspension_def;
+
+/* StructureDefinition (structure.h:164-172) */
+typedef struct swb_structure_definition {
+    uint64_t node_count;
+    const swb_node_def* nodes;
+    uint64_t triangle_count;
+    const swb_triangle_def* triangles;
+    uint64_t constraint_count;
+    const swb_constraint_def* constraints;
+    uint64_t membrane_count;
+    const swb_membrane_def* membranes;
+    uint64_t dihedral_count;
+    const swb_dihedral_def* dihedrals;
+    const swb_fabric_contact_def* fabric_self_contact; /* nullable */
+    const swb_suspension_def* suspension;              /* nullable */
+} swb_structure_definition;
+
+/* StructureStepSettings (structure.h:208-219) */
+typedef struct swb_step_settings {
+    double time_step;
+    int32_t substeps;
+    int32_t constraint_iterations;
+    int32_t cable_sweep_pairs;
+    uint32_t worker_threads; /* accepted for source compatibility; ignored */
+    swb_vec3 gravity;
+    double velocity_damping;
+    swb_vec3 damping_reference_velocity;
+} swb_step_settings;
+
+/* StructureStepSettings defaults: dt 1/120, 2 substeps, 12 iterations,
+ * gravity -9.80665 z, damping 0.25 (structure.h:208-219). */
+void swb_default_step_settings(swb_step_settings* out);
+
+/* StructureDiagnostics (structure.h:221-246) */
+typedef struct swb_diagnostics {
+    uint64_t node_count;
+    uint64_t dynamic_node_count;
+    uint64_t triangle_count;
+    uint64_t constraint_count;
+    uint64_t membrane_count;
+    uint64_t dihedral_count;
+    uint64_t contact_pair_count;
+    uint64_t active_contact_count;
+    uint64_t suspension_segment_count;
+    double total_dynamic_mass;
+    swb_vec3 center_of_mass;
+    swb_vec3 linear_momentum;
+    double kinetic_energy;
+    double maximum_distance_error;
+    double maximum_cable_extension;
+    double maximum_absolute_membrane_strain;
+    double maximum_membrane_residual;
+    double maximum_contact_penetration;
+    double maximum_suspension_residual;
+    swb_vec3 pending_external_force;
+    swb_vec3 last_applied_external_force;
+    uint32_t finite;
+    uint32_t reserved;
+} swb_diagnostics;
+
+/* StructureNodeState (structure.h:174-180) */
+typedef struct swb_node_state {
+    swb_vec3 position;
+    swb_vec3 previous_position;
+    swb_vec3 velocity;
+} swb_node_state;
+
+/* StructureRigidPayloadState (structure.h:182-189) */
+typedef struct swb_payload_state {
+    swb_vec3 center_of_mass;
+    swb_quat body_to_world;
+    swb_vec3 linear_velocity;
+    swb_vec3 angular_velocity;
+} swb_payload_state;
+
+/* StructureSuspensionSegmentState (structure.h:191-198) plus the segment's
+ * line wrench contribution on the payload (suspension.cpp:2582-2589). */
+typedef struct swb_segment_state {
+    uint64_t stable_id;
+    double current_length;
+    double commanded_rest_length;
+    double tension;
+} swb_segment_state;
+
+/* Payload line wrench of the last accepted substep: the force and moment the
+ * risers exert on the rigid pilot (SuspensionPayloadDiagnostics::lineWrench,
+ * suspension.cpp:2582-2589). */
+typedef struct swb_wrench {
+    swb_vec3 force;
+    swb_vec3 moment;
+} swb_wrench;
+
+/* ------------------------------------------------------------------------ */
+/* Solver options (no reference counterpart: launch shape of the persistent  */
+/* kernel; zero fields mean "choose automatically").                         */
+/* ------------------------------------------------------------------------ */
+typedef struct swb_solver_options {
+    int32_t device;          /* CUDA device ordinal                          */
+    int32_t blocks;          /* persistent CTAs; 0 = SM count                */
+    int32_t block_threads;   /* threads per CTA; 0 = autotuned               */
+    int32_t partition_levels;/* patch-partition levels; 0 = autotuned        */
+    int32_t colours_per_sync;/* reserved                                     */
+    uint32_t flags;          /* SWB_OPT_* bits                               */
+    int64_t sync_budget_cycles; /* bounded barrier spin; 0 = default (~2 s)  */
+} swb_solver_options;
+
+enum {
+    SWB_OPT_GLOBAL_ONLY = 1u << 0, /* no shared-memory patches: every colour
+                                      is a device-wide phase (debug/compare) */
+    SWB_OPT_NO_GRAPH = 1u << 1     /* batched: launch without CUDA graphs    */
+};
+
+void swb_default_solver_options(swb_solver_options* out);
+
+/* ------------------------------------------------------------------------ */
+/* Single structure (replaces simwing::fsi::Structure).                      */
+/* ------------------------------------------------------------------------ */
+typedef struct swb_structure swb_structure;
+
+/* Structure::Structure(StructureDefinition) (structure.h:275,
+ * structure.cpp:687-690): validates, builds the device image.  The
+ * definition is copied; the caller's arrays may be freed afterwards. */
+swb_status swb_structure_create(const swb_structure_definition* definition,
+                                const swb_solver_options* options,
+                                swb_structure** out);
+void swb_structure_destroy(swb_structure* structure);
+
+/* Structure::definitionFingerprint / acceptedStepCount /
+ * simulationTimeSeconds (structure.h:283-287). */
+uint64_t swb_structure_fingerprint(const swb_structure* structure);
+uint64_t swb_structure_accepted_steps(const swb_structure* structure);
+double swb_structure_simulation_time(const swb_structure* structure);
+uint64_t swb_structure_node_count(const swb_structure* structure);
+
+/* Structure::clearExternalForces / addExternalForce / setExternalForces
+ * (structure.h:291-295, structure.cpp:778-805). */
+swb_status swb_structure_clear_external_forces(swb_structure* structure);
+swb_status swb_structure_add_external_force(swb_structure* structure,
+                                            uint64_t node,
+                                            const swb_vec3* force);
+swb_status swb_structure_set_external_forces(swb_structure* structure,
+                                             const swb_vec3* forces,
+                                             uint64_t count);
+
+/* SoftBody::setFacePressureDifference / setUniformPressureDifference
+ * (soft_body.h:425-433): per-face pressure jump used by the device pressure
+ * gather (soft_body.cpp:1492-1534). */
+swb_status swb_structure_set_face_pressure(swb_structure* structure,
+                                           uint64_t triangle,
+                                           double pressure_difference);
+swb_status swb_structure_set_uniform_pressure(swb_structure* structure,
+                                              double pressure_difference);
+
+/* Structure::step (structure.h:297-300, structure.cpp:807-831).  Consumes the
+ * pending external forces only when the step is accepted; on failure the
+ * pre-step state is restored and the status says why.  `out` is nullable. */
+swb_status swb_structure_step(swb_structure* structure,
+                              const swb_step_settings* settings,
+                              swb_diagnostics* out);
+
+/* Runs `steps` accepted steps back to back with the same settings and the
+ * same pending loads re-applied each step (the loads are consumed after the
+ * last).  Diagnostics are those of the final step.  No reference
+ * counterpart: a caller loop over Structure::step with constant loads. */
+swb_status swb_structure_step_many(swb_structure* structure,
+                                   const swb_step_settings* settings,
+                                   int32_t steps,
+                                   swb_diagnostics* out);
+
+/* Structure::diagnostics (structure.h:301, structure.cpp:833-959), reduced
+ * on the device. */
+swb_status swb_structure_diagnostics(const swb_structure* structure,
+                                     swb_diagnostics* out);
+
+/* Structure::nodeStates (structure.h:288, structure.cpp:725-734). */
+swb_status swb_structure_read_nodes(const swb_structure* structure,
+                                    swb_node_state* out,
+                                    uint64_t count);
+/* Positions only, FP32 xyz triples (3*count floats). */
+swb_status swb_structure_read_positions_f32(const swb_structure* structure,
+                                            float* out_xyz,
+                                            uint64_t count);
+/* Overwrites node positions and velocities (previous positions are set to
+ * the positions).  No reference counterpart; used to start the device solver
+ * from a state produced elsewhere, e.g. another solver's checkpoint. */
+swb_status swb_structure_write_nodes(swb_structure* structure,
+                                     const swb_node_state* nodes,
+                                     uint64_t count);
+
+/* Structure::suspensionState (structure.h:289-290, structure.cpp:736-776).
+ * segments may be NULL when segment_capacity is 0. */
+swb_status swb_structure_read_suspension(const swb_structure* structure,
+                                         swb_payload_state* payload,
+                                         swb_segment_state* segments,
+                                         uint64_t segment_capacity,
+                                         swb_wrench* line_wrench);
+swb_status swb_structure_write_payload(swb_structure* structure,
+                                       const swb_payload_state* payload);
+
+/* Structure::checkpoint / restore (structure.h:303-304,
+ * structure.cpp:961-1027).  The checkpoint is an opaque, checksummed byte
+ * image bound to the definition fingerprint; restore rejects a foreign or
+ * tampered image with SWB_INVALID_ARGUMENT. */
+swb_status swb_structure_checkpoint_size(const swb_structure* structure,
+                                         uint64_t* bytes);
+swb_status swb_structure_checkpoint(const swb_structure* structure,
+                                    void* buffer,
+                                    uint64_t bytes);
+swb_status swb_structure_restore(swb_structure* structure,
+                                 const void* buffer,
+                                 uint64_t bytes);
+
+/* Schedule introspection (no reference counterpart).  The device sweeps
+ * distance-like constraints and dihedrals in a fixed order; running the
+ * reference's serial solver with its constraint lists permuted into this
+ * order reproduces the device sweep exactly.  `order` receives a
+ * permutation of [0, count): order[k] is the definition index of the k-th
+ * constraint swept. */
+swb_status swb_structure_sweep_order(const swb_structure* structure,
+                                     uint32_t which, /* SWB_SWEEP_* */
+                                     uint64_t* order,
+                                     uint64_t count);
+enum {
+    SWB_SWEEP_DISTANCE = 0,
+    SWB_SWEEP_DIHEDRAL = 1
+};
+
+/* Shape of the device schedule for reporting. */
+typedef struct swb_schedule_report {
+    int32_t blocks;
+    int32_t block_threads;
+    int32_t partition_levels;
+    int32_t device_phases_per_iteration; /* device-wide barriers / iteration */
+    int32_t local_stages_per_iteration;  /* CTA-local colour stages          */
+    int32_t global_colours_per_iteration;
+    int32_t max_patch_nodes;
+    int32_t shared_bytes;
+    uint64_t level_constraints[4];       /* distance+dihedral per level      */
+    uint64_t global_constraints;
+} swb_schedule_report;
+swb_status swb_structure_schedule_report(const swb_structure* structure,
+                                         swb_schedule_report* out);
+
+/* Device time of the most recent step's kernels in milliseconds, measured
+ * with CUDA events on the solver's stream. */
+double swb_structure_last_step_ms(const swb_structure* structure);
+
+/* ------------------------------------------------------------------------ */
+/* Reference colouring (bit-exact restatement of                             */
+/* SoftBody::constraintColouring, soft_body.cpp:1978-2075): greedy first-fit */
+/* over the line graph in insertion order, colours ranked by descending      */
+/* size.  order has constraint_count entries, offsets colour_count + 1.      */
+/* ------------------------------------------------------------------------ */
+swb_status swb_reference_colouring(const swb_structure_definition* definition,
+                                   uint64_t* order,
+                                   uint64_t* offsets,
+                                   uint64_t offsets_capacity,
+                                   uint64_t* colour_count,
+                                   uint64_t* parallel_colours);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic definitions.  Deterministic generators of the cloth patch and   */
+/* the ram-air wing; they emit a definition the way the reference's scene    */
+/* assembly would (area/3 mass lumping, one dihedral per interior sheet edge */
+/* with the series-strip compliance, seam stitches + rails, cable lines, a   */
+/* rigid pilot on two risers) -- src/fsi/scene_structure.cpp:278-892.        */
+/* ------------------------------------------------------------------------ */
+typedef struct swb_definition swb_definition;
+
+typedef struct swb_patch_params {
+    uint32_t nx, ny;          /* particles per side (33 x 33)             */
+    double width, height;     /* metres (1 x 1)                           */
+    double areal_density;     /* kg/m^2 (0.040)                           */
+    double distance_compliance; /* m/N (1e-7)                             */
+    double bend_compliance;   /* rad/(N m) (1e-3)                         */
+    double jitter;            /* std-dev metres of N(0, jitter) (1e-3)    */
+    uint64_t seed;
+    uint32_t pin_top_corners; /* 1 = two top corners fixed                */
+    uint32_t reserved;
+} swb_patch_params;
+
+typedef struct swb_wing_params {
+    uint32_t cells;           /* 40                                        */
+    uint32_t chordwise;       /* quads chordwise per surface (60)          */
+    uint32_t spanwise_per_cell; /* quads spanwise per cell (4)             */
+    uint32_t rib_layers;      /* quads through the rib thickness (6)       */
+    double span;              /* metres (11)                               */
+    double root_chord;        /* metres (2.6)                              */
+    double thickness;         /* fraction of chord (0.15)                  */
+    double areal_density;     /* kg/m^2 (0.045)                            */
+    double skin_compliance;   /* m/N for skin/rib edges                    */
+    double bend_rigidity;     /* N m bending rigidity of the fabric        */
+    double line_compliance_scale; /* multiplies L/EA of every line         */
+    double pressure;          /* Pa, outward (30)                          */
+    uint32_t line_levels;     /* cascade levels (4)                        */
+    uint32_t line_particles;  /* particles per line segment (8)            */
+    uint32_t line_rows;       /* A/B/C/brake = 4                           */
+    uint32_t pilot;           /* 1 = rigid pilot on two risers             */
+    double pilot_mass;        /* kg (90)                                   */
+    double aspect_ratio;      /* 0 = derive from span and chord            */
+    double compliance_jitter; /* sigma of lognormal compliance multiplier  */
+    uint64_t seed;
+} swb_wing_params;
+
+void swb_default_patch_params(swb_patch_params* out);
+void swb_default_wing_params(swb_wing_params* out);
+swb_status swb_generate_patch(const swb_patch_params* params,
+                              swb_definition** out);
+swb_status swb_generate_wing(const swb_wing_params* params,
+                             swb_definition** out);
+/* Copies an arbitrary definition into an owned one (for permutation). */
+swb_status swb_definition_copy(const swb_structure_definition* source,
+                               swb_definition** out);
+/* Reorders the constraint and dihedral lists (order arrays as returned by
+ * swb_structure_sweep_order; NULL keeps a list as is). */
+swb_status swb_definition_permute(swb_definition* definition,
+                                  const uint64_t* constraint_order,
+                                  const uint64_t* dihedral_order);
+/* Multiplies the rest length of constraint `index` (any kind) or, when
+ * index >= constraint_count, of suspension segment index - constraint_count. */
+swb_status swb_definition_scale_rest(swb_definition* definition,
+                                     uint64_t index,
+                                     double factor);
+const swb_structure_definition* swb_definition_view(
+    const swb_definition* definition);
+void swb_definition_destroy(swb_definition* definition);
+
+/* Definition fingerprint of Structure (structure.cpp:463-553 restated:
+ * FNV-1a over the definition's fields in declaration order). */
+uint64_t swb_definition_fingerprint(const swb_structure_definition* definition);
+
+/* Validation only (structure.cpp:102-455). */
+swb_status swb_validate_definition(const swb_structure_definition* definition);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* SIMWING_B200_H */

@@ -1,0 +1,203 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY.
+
+ctypes loaders for the two CPU checkers:
+  * PortStructure -- oracle/liboracle.so, the plain-C FP64 restatement of
+    the reference step (oracle/xpbd_oracle.c);
+  * RefStructure  -- oracle/_ref/libswref.so, the reference's own
+    softwing core + Structure adapter compiled from source
+    (oracle/ref_shim.cpp, oracle/Makefile).
+Both take the product's swb_structure_definition, so the device solver and
+the checkers run on identical inputs.  Only tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from simwing_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libswref.so")
+
+P = C.POINTER
+_PORT = {
+    "swo_last_error": (C.c_char_p, []),
+    "swo_create": (C.c_int, [P(abi.StructureDefinition), P(C.c_void_p)]),
+    "swo_destroy": (None, [C.c_void_p]),
+    "swo_set_external_forces": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "swo_add_external_force": (C.c_int, [C.c_void_p, C.c_uint64, P(abi.Vec3)]),
+    "swo_step": (C.c_int, [C.c_void_p, P(abi.StepSettings)]),
+    "swo_diagnostics": (C.c_int, [C.c_void_p, P(abi.Diagnostics)]),
+    "swo_read_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "swo_write_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "swo_read_payload": (C.c_int, [C.c_void_p, P(abi.PayloadState), P(abi.Wrench), P(C.c_double)]),
+    "swo_write_payload": (C.c_int, [C.c_void_p, P(abi.PayloadState)]),
+    "swo_read_segment_lambdas": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "swo_evaluate_dihedral": (None, [C.c_void_p, C.c_void_p]),
+}
+_REF = {
+    "swref_last_error": (C.c_char_p, []),
+    "swref_physical_cores": (C.c_uint, []),
+    "swref_create": (C.c_int, [P(abi.StructureDefinition), P(C.c_void_p)]),
+    "swref_destroy": (None, [C.c_void_p]),
+    "swref_set_external_forces": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "swref_add_external_force": (C.c_int, [C.c_void_p, C.c_uint64, P(abi.Vec3)]),
+    "swref_step": (C.c_int, [C.c_void_p, P(abi.StepSettings), P(abi.Diagnostics)]),
+    "swref_last_step_seconds": (C.c_double, [C.c_void_p]),
+    "swref_diagnostics": (C.c_int, [C.c_void_p, P(abi.Diagnostics)]),
+    "swref_read_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "swref_read_suspension": (C.c_int, [C.c_void_p, P(abi.PayloadState), C.c_void_p, C.c_uint64]),
+    "swref_colouring": (C.c_int, [P(abi.StructureDefinition), C.c_void_p, C.c_void_p, C.c_uint64,
+                                  P(C.c_uint64), P(C.c_uint64)]),
+}
+
+_libs = {}
+
+
+def port_available() -> bool:
+    return os.path.exists(PORT_PATH)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_PATH)
+
+
+def port_library() -> C.CDLL:
+    if "port" not in _libs:
+        _libs["port"] = abi.bind(C.CDLL(PORT_PATH), _PORT)
+    return _libs["port"]
+
+
+def ref_library() -> C.CDLL:
+    if "ref" not in _libs:
+        _libs["ref"] = abi.bind(C.CDLL(REF_PATH), _REF)
+    return _libs["ref"]
+
+
+class OracleError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"status {status}: {message}")
+        self.status = status
+
+
+class _Base:
+    _prefix = ""
+
+    def _lib(self):
+        raise NotImplementedError
+
+    def _check(self, status):
+        if status != 0:
+            raise OracleError(status, getattr(self._lib(), self._prefix + "last_error")().decode())
+
+    def __init__(self, definition):
+        self._definition = definition  # keep alive
+        h = C.c_void_p()
+        self._check(getattr(self._lib(), self._prefix + "create")(definition.pointer, C.byref(h)))
+        self._h = h
+        self.node_count = int(definition.view.node_count)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            getattr(self._lib(), self._prefix + "destroy")(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def set_external_forces(self, forces):
+        f = np.ascontiguousarray(forces, dtype=np.float64)
+        self._check(getattr(self._lib(), self._prefix + "set_external_forces")(self._h, f.ctypes.data, f.shape[0]))
+
+    def add_external_force(self, node, force):
+        self._check(getattr(self._lib(), self._prefix + "add_external_force")(self._h, node, C.byref(abi.Vec3(*force))))
+
+    def node_states(self):
+        out = np.zeros((self.node_count, 3, 3), dtype=np.float64)
+        self._check(getattr(self._lib(), self._prefix + "read_nodes")(self._h, out.ctypes.data, self.node_count))
+        return out
+
+    def positions(self):
+        return self.node_states()[:, 0, :]
+
+    def diagnostics(self):
+        d = abi.Diagnostics()
+        self._check(getattr(self._lib(), self._prefix + "diagnostics")(self._h, C.byref(d)))
+        return d
+
+
+class PortStructure(_Base):
+    """The C restatement (FP64)."""
+    _prefix = "swo_"
+
+    def _lib(self):
+        return port_library()
+
+    def step(self, settings):
+        self._check(port_library().swo_step(self._h, C.byref(settings)))
+
+    def write_node_states(self, states):
+        s = np.ascontiguousarray(states, dtype=np.float64)
+        self._check(port_library().swo_write_nodes(self._h, s.ctypes.data, self.node_count))
+
+    def payload(self):
+        p = abi.PayloadState()
+        w = abi.Wrench()
+        r = C.c_double()
+        self._check(port_library().swo_read_payload(self._h, C.byref(p), C.byref(w), C.byref(r)))
+        return p, w, r.value
+
+    def write_payload(self, p):
+        self._check(port_library().swo_write_payload(self._h, C.byref(p)))
+
+    def segment_lambdas(self, n):
+        out = np.zeros(n)
+        self._check(port_library().swo_read_segment_lambdas(self._h, out.ctypes.data, n))
+        return out
+
+
+class RefStructure(_Base):
+    """The reference's own Structure adapter (FP64, compiled from source)."""
+    _prefix = "swref_"
+
+    def _lib(self):
+        return ref_library()
+
+    def step(self, settings):
+        d = abi.Diagnostics()
+        self._check(ref_library().swref_step(self._h, C.byref(settings), C.byref(d)))
+        return d
+
+    def last_step_seconds(self):
+        return float(ref_library().swref_last_step_seconds(self._h))
+
+    def payload(self, segments=0):
+        p = abi.PayloadState()
+        segs = (abi.SegmentState * max(segments, 1))()
+        self._check(ref_library().swref_read_suspension(self._h, C.byref(p), segs, segments))
+        return p, list(segs)[:segments]
+
+
+def evaluate_dihedral(points12):
+    out = np.zeros(14)
+    p = np.ascontiguousarray(points12, dtype=np.float64)
+    port_library().swo_evaluate_dihedral(p.ctypes.data, out.ctypes.data)
+    return out[0], out[1:13].reshape(4, 3), bool(out[13])
+
+
+def ref_colouring(definition):
+    lib = ref_library()
+    m = definition.view.constraint_count
+    order = np.zeros(max(m, 1), dtype=np.uint64)
+    offsets = np.zeros(4096, dtype=np.uint64)
+    colours = C.c_uint64()
+    parallel = C.c_uint64()
+    status = lib.swref_colouring(definition.pointer, order.ctypes.data, offsets.ctypes.data, offsets.size,
+                                 C.byref(colours), C.byref(parallel))
+    if status != 0:
+        raise OracleError(status, lib.swref_last_error().decode())
+    return order[:m], offsets[: colours.value + 1 if m else 0], int(parallel.value)

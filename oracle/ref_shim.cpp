@@ -1,0 +1,458 @@
+// ORACLE / TEST INFRASTRUCTURE ONLY.  Never linked into the product library.
+//
+// C shim over the reference's own, unmodified structural adapter
+// `simwing::fsi::Structure` (src/fsi/structure.h:273-309) and XPBD core
+// (src/softwing).  oracle/Makefile compiles the reference sources where they
+// lie and links them with this file into oracle/_ref/libswref.so, which the
+// tests and bench.py's CPU-baseline leg load through ctypes.
+//
+// The shim takes the same `swb_structure_definition` as the device solver.
+// Per-face pressure: the adapter's StructureDefinition carries no face
+// pressure (structure.h:38-40), so the shim computes the softwing nodal
+// pressure load Δp·½(b−a)×(c−a)/3 (soft_body.cpp:1497-1508) from the state at
+// step start and adds it to the pending external forces.  With one substep
+// this is the force SoftBody::integrateSubstepTrial accumulates
+// (soft_body.cpp:1185), up to FP64 summation order.
+#include "simwing_b200.h"
+
+#include "structure.h"
+#include <softwing/parallel.h>
+#include <softwing/soft_body.h>
+#include <softwing/suspension.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_error;
+
+using namespace simwing::fsi;
+
+StructureDefinition convert(const swb_structure_definition& d) {
+    StructureDefinition out;
+    out.nodes.reserve(d.node_count);
+    for (uint64_t i = 0; i < d.node_count; ++i) {
+        const swb_node_def& n = d.nodes[i];
+        out.nodes.push_back({{n.position.x, n.position.y, n.position.z},
+                             n.mass,
+                             n.fixed != 0});
+    }
+    for (uint64_t i = 0; i < d.triangle_count; ++i) {
+        const swb_triangle_def& t = d.triangles[i];
+        out.triangles.push_back({{t.nodes[0], t.nodes[1], t.nodes[2]}});
+    }
+    for (uint64_t i = 0; i < d.constraint_count; ++i) {
+        const swb_constraint_def& c = d.constraints[i];
+        out.constraints.push_back(
+            {static_cast<StructureConstraintKind>(c.kind), c.first_node,
+             c.second_node, c.rest_length, c.compliance});
+    }
+    for (uint64_t i = 0; i < d.membrane_count; ++i) {
+        const swb_membrane_def& m = d.membranes[i];
+        StructureMembraneDefinition md;
+        md.triangle = m.triangle;
+        for (int k = 0; k < 3; ++k)
+            md.materialCoordinates[k] = {m.chart[k][0], m.chart[k][1]};
+        md.material.warpStiffnessNewtonsPerMeter = m.material.warp_stiffness;
+        md.material.weftStiffnessNewtonsPerMeter = m.material.weft_stiffness;
+        md.material.couplingStiffnessNewtonsPerMeter =
+            m.material.coupling_stiffness;
+        md.material.shearStiffnessNewtonsPerMeter = m.material.shear_stiffness;
+        md.material.warpPreTensionNewtonsPerMeter = m.material.warp_pretension;
+        md.material.weftPreTensionNewtonsPerMeter = m.material.weft_pretension;
+        md.material.dampingSeconds = m.material.damping_seconds;
+        md.material.compressionStiffnessRatio =
+            m.material.compression_stiffness_ratio;
+        md.role = static_cast<StructureMaterialRole>(m.role);
+        out.membranes.push_back(md);
+    }
+    for (uint64_t i = 0; i < d.dihedral_count; ++i) {
+        const swb_dihedral_def& h = d.dihedrals[i];
+        out.dihedrals.push_back(
+            {{h.nodes[0], h.nodes[1], h.nodes[2], h.nodes[3]},
+             h.rest_angle,
+             h.compliance});
+    }
+    if (d.fabric_self_contact) {
+        const swb_fabric_contact_def& c = *d.fabric_self_contact;
+        out.fabricSelfContact = StructureFabricContactDefinition{
+            c.half_thickness, c.normal_compliance, c.static_friction,
+            c.dynamic_friction};
+    }
+    if (d.suspension) {
+        const swb_suspension_def& s = *d.suspension;
+        StructureSuspensionDefinition sd;
+        sd.pilotStableId = s.pilot_stable_id;
+        sd.pilotMassKg = s.pilot_mass;
+        sd.pilotCenterOfMassLocalMeters = {s.pilot_com_local.x,
+                                           s.pilot_com_local.y,
+                                           s.pilot_com_local.z};
+        sd.pilotInitialCenterOfMassWorldMeters = {
+            s.pilot_initial_com_world.x, s.pilot_initial_com_world.y,
+            s.pilot_initial_com_world.z};
+        sd.pilotInitialLinearVelocityMetersPerSecond = {
+            s.pilot_initial_linear_velocity.x,
+            s.pilot_initial_linear_velocity.y,
+            s.pilot_initial_linear_velocity.z};
+        sd.pilotInitialAngularVelocityRadiansPerSecond = {
+            s.pilot_initial_angular_velocity.x,
+            s.pilot_initial_angular_velocity.y,
+            s.pilot_initial_angular_velocity.z};
+        sd.pilotInitialBodyToWorld = {
+            s.pilot_initial_body_to_world.w, s.pilot_initial_body_to_world.x,
+            s.pilot_initial_body_to_world.y, s.pilot_initial_body_to_world.z};
+        sd.pilotPrincipalInertiaKgSquareMeters = {
+            s.pilot_principal_inertia.x, s.pilot_principal_inertia.y,
+            s.pilot_principal_inertia.z};
+        for (uint64_t i = 0; i < s.attachment_count; ++i)
+            sd.attachments.push_back(
+                {s.attachments[i].stable_id, s.attachments[i].node});
+        for (uint64_t i = 0; i < s.junction_count; ++i)
+            sd.junctions.push_back(
+                {s.junctions[i].stable_id, s.junctions[i].node});
+        for (uint64_t i = 0; i < s.harness_count; ++i) {
+            const swb_pilot_harness& h = s.harness_points[i];
+            sd.harnessPoints.push_back(
+                {h.stable_id,
+                 {h.local_position.x, h.local_position.y,
+                  h.local_position.z}});
+        }
+        for (uint64_t i = 0; i < s.segment_count; ++i) {
+            const swb_suspension_segment& g = s.segments[i];
+            StructureSuspensionSegmentDefinition gd;
+            gd.stableId = g.stable_id;
+            gd.from = {static_cast<StructureSuspensionEndpointKind>(
+                           g.from.kind),
+                       g.from.stable_id};
+            gd.to = {static_cast<StructureSuspensionEndpointKind>(g.to.kind),
+                     g.to.stable_id};
+            gd.restLengthMeters = g.rest_length;
+            gd.axialStiffnessNewtons = g.axial_stiffness;
+            gd.axialDampingNewtonSecondsPerMeter = g.axial_damping;
+            gd.role = g.role;
+            sd.segments.push_back(gd);
+        }
+        sd.solverIterations = s.solver_iterations;
+        sd.attachmentTolerance = s.attachment_tolerance;
+        sd.minimumLineLengthMeters = s.minimum_line_length;
+        sd.maximumLineResidualMeters = s.maximum_line_residual;
+        sd.maximumControlWorkJoules = s.maximum_control_work;
+        out.suspension = std::move(sd);
+    }
+    return out;
+}
+
+struct RefHandle {
+    std::unique_ptr<Structure> structure;
+    std::vector<std::array<uint64_t, 3>> triangles;
+    std::vector<double> pressure;
+    bool anyPressure = false;
+    double lastStepSeconds = 0.0;
+};
+
+swb_status fail(swb_status status, const std::exception& error) {
+    g_error = error.what();
+    return status;
+}
+
+swb_status translate() {
+    try {
+        throw;
+    } catch (const softwing::SuspensionError& e) {
+        return fail(SWB_SUSPENSION_ERROR, e);
+    } catch (const softwing::ContactStepError& e) {
+        return fail(SWB_CONTACT_ERROR, e);
+    } catch (const std::out_of_range& e) {
+        return fail(SWB_OUT_OF_RANGE, e);
+    } catch (const std::invalid_argument& e) {
+        return fail(SWB_INVALID_ARGUMENT, e);
+    } catch (const std::exception& e) {
+        return fail(SWB_INVALID_ARGUMENT, e);
+    } catch (...) {
+        g_error = "unknown exception";
+        return SWB_INVALID_ARGUMENT;
+    }
+}
+
+void toDiagnostics(const StructureDiagnostics& d, swb_diagnostics* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->node_count = d.nodeCount;
+    o->dynamic_node_count = d.dynamicNodeCount;
+    o->triangle_count = d.triangleCount;
+    o->constraint_count = d.constraintCount;
+    o->membrane_count = d.membraneCount;
+    o->dihedral_count = d.dihedralCount;
+    o->contact_pair_count = d.contactPairCount;
+    o->active_contact_count = d.activeContactCount;
+    o->suspension_segment_count = d.suspensionSegmentCount;
+    o->total_dynamic_mass = d.totalDynamicMassKg;
+    o->center_of_mass = {d.centerOfMassMeters.x, d.centerOfMassMeters.y,
+                         d.centerOfMassMeters.z};
+    o->linear_momentum = {d.linearMomentumKgMetersPerSecond.x,
+                          d.linearMomentumKgMetersPerSecond.y,
+                          d.linearMomentumKgMetersPerSecond.z};
+    o->kinetic_energy = d.kineticEnergyJoules;
+    o->maximum_distance_error = d.maximumDistanceErrorMeters;
+    o->maximum_cable_extension = d.maximumCableExtensionMeters;
+    o->maximum_absolute_membrane_strain = d.maximumAbsoluteMembraneStrain;
+    o->maximum_membrane_residual = d.maximumMembraneResidual;
+    o->maximum_contact_penetration = d.maximumContactPenetrationMeters;
+    o->maximum_suspension_residual = d.maximumSuspensionResidualMeters;
+    o->pending_external_force = {d.pendingExternalForceNewtons.x,
+                                 d.pendingExternalForceNewtons.y,
+                                 d.pendingExternalForceNewtons.z};
+    o->last_applied_external_force = {d.lastAppliedExternalForceNewtons.x,
+                                      d.lastAppliedExternalForceNewtons.y,
+                                      d.lastAppliedExternalForceNewtons.z};
+    o->finite = d.finite ? 1u : 0u;
+}
+
+StructureStepSettings convert(const swb_step_settings& s) {
+    StructureStepSettings out;
+    out.timeStepSeconds = s.time_step;
+    out.substeps = s.substeps;
+    out.constraintIterations = s.constraint_iterations;
+    out.cableConstraintSweepPairs = s.cable_sweep_pairs;
+    out.gravityMetersPerSecondSquared = {s.gravity.x, s.gravity.y,
+                                         s.gravity.z};
+    out.velocityDampingPerSecond = s.velocity_damping;
+    out.dampingReferenceVelocityMetersPerSecond = {
+        s.damping_reference_velocity.x, s.damping_reference_velocity.y,
+        s.damping_reference_velocity.z};
+    out.workerThreads = s.worker_threads;
+    return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* swref_last_error(void) { return g_error.c_str(); }
+
+unsigned swref_physical_cores(void) {
+    return softwing::hardwarePhysicalCoreCount();
+}
+
+swb_status swref_create(const swb_structure_definition* definition,
+                        void** out) {
+    try {
+        auto handle = std::make_unique<RefHandle>();
+        handle->structure =
+            std::make_unique<Structure>(convert(*definition));
+        handle->triangles.reserve(definition->triangle_count);
+        handle->pressure.reserve(definition->triangle_count);
+        for (uint64_t i = 0; i < definition->triangle_count; ++i) {
+            const swb_triangle_def& t = definition->triangles[i];
+            handle->triangles.push_back({t.nodes[0], t.nodes[1], t.nodes[2]});
+            handle->pressure.push_back(t.pressure_difference);
+            handle->anyPressure =
+                handle->anyPressure || t.pressure_difference != 0.0;
+        }
+        *out = handle.release();
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+void swref_destroy(void* handle) { delete static_cast<RefHandle*>(handle); }
+
+swb_status swref_set_external_forces(void* handle,
+                                     const swb_vec3* forces,
+                                     uint64_t count) {
+    try {
+        auto* h = static_cast<RefHandle*>(handle);
+        std::vector<StructureVector3> values(count);
+        for (uint64_t i = 0; i < count; ++i)
+            values[i] = {forces[i].x, forces[i].y, forces[i].z};
+        h->structure->setExternalForces(values);
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+swb_status swref_add_external_force(void* handle,
+                                    uint64_t node,
+                                    const swb_vec3* force) {
+    try {
+        static_cast<RefHandle*>(handle)->structure->addExternalForce(
+            node, {force->x, force->y, force->z});
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+swb_status swref_step(void* handle,
+                      const swb_step_settings* settings,
+                      swb_diagnostics* out) {
+    try {
+        auto* h = static_cast<RefHandle*>(handle);
+        const auto start = std::chrono::steady_clock::now();
+        if (h->anyPressure) {
+            const std::vector<StructureNodeState> nodes =
+                h->structure->nodeStates();
+            for (std::size_t t = 0; t < h->triangles.size(); ++t) {
+                if (h->pressure[t] == 0.0) continue;
+                const auto& tri = h->triangles[t];
+                const StructureVector3& a = nodes[tri[0]].positionMeters;
+                const StructureVector3& b = nodes[tri[1]].positionMeters;
+                const StructureVector3& c = nodes[tri[2]].positionMeters;
+                const double ux = b.x - a.x, uy = b.y - a.y, uz = b.z - a.z;
+                const double vx = c.x - a.x, vy = c.y - a.y, vz = c.z - a.z;
+                const double ax = 0.5 * (uy * vz - uz * vy);
+                const double ay = 0.5 * (uz * vx - ux * vz);
+                const double az = 0.5 * (ux * vy - uy * vx);
+                const StructureVector3 f{h->pressure[t] * ax / 3.0,
+                                         h->pressure[t] * ay / 3.0,
+                                         h->pressure[t] * az / 3.0};
+                for (int k = 0; k < 3; ++k)
+                    h->structure->addExternalForce(tri[k], f);
+            }
+        }
+        const StructureDiagnostics d =
+            h->structure->step(convert(*settings));
+        h->lastStepSeconds = std::chrono::duration<double>(
+                                 std::chrono::steady_clock::now() - start)
+                                 .count();
+        if (out) toDiagnostics(d, out);
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+double swref_last_step_seconds(void* handle) {
+    return static_cast<RefHandle*>(handle)->lastStepSeconds;
+}
+
+swb_status swref_diagnostics(void* handle, swb_diagnostics* out) {
+    try {
+        toDiagnostics(static_cast<RefHandle*>(handle)->structure->diagnostics(),
+                      out);
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+swb_status swref_read_nodes(void* handle, swb_node_state* out, uint64_t count) {
+    try {
+        const auto nodes =
+            static_cast<RefHandle*>(handle)->structure->nodeStates();
+        if (count != nodes.size())
+            throw std::invalid_argument("node count mismatch");
+        for (uint64_t i = 0; i < count; ++i) {
+            out[i].position = {nodes[i].positionMeters.x,
+                               nodes[i].positionMeters.y,
+                               nodes[i].positionMeters.z};
+            out[i].previous_position = {nodes[i].previousPositionMeters.x,
+                                        nodes[i].previousPositionMeters.y,
+                                        nodes[i].previousPositionMeters.z};
+            out[i].velocity = {nodes[i].velocityMetersPerSecond.x,
+                               nodes[i].velocityMetersPerSecond.y,
+                               nodes[i].velocityMetersPerSecond.z};
+        }
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+// Reads the payload state and the per-segment tension, in definition order.
+swb_status swref_read_suspension(void* handle,
+                                 swb_payload_state* payload,
+                                 swb_segment_state* segments,
+                                 uint64_t capacity) {
+    try {
+        const auto state =
+            static_cast<RefHandle*>(handle)->structure->suspensionState();
+        if (!state) throw std::invalid_argument("no suspension");
+        const auto& p = state->payload;
+        payload->center_of_mass = {p.centerOfMassWorldMeters.x,
+                                   p.centerOfMassWorldMeters.y,
+                                   p.centerOfMassWorldMeters.z};
+        payload->body_to_world = {p.bodyToWorld.w, p.bodyToWorld.x,
+                                  p.bodyToWorld.y, p.bodyToWorld.z};
+        payload->linear_velocity = {p.linearVelocityMetersPerSecond.x,
+                                    p.linearVelocityMetersPerSecond.y,
+                                    p.linearVelocityMetersPerSecond.z};
+        payload->angular_velocity = {p.angularVelocityRadiansPerSecond.x,
+                                     p.angularVelocityRadiansPerSecond.y,
+                                     p.angularVelocityRadiansPerSecond.z};
+        for (uint64_t i = 0; i < capacity && i < state->segments.size(); ++i) {
+            segments[i].stable_id = state->segments[i].stableId;
+            segments[i].current_length = state->segments[i].currentLengthMeters;
+            segments[i].commanded_rest_length =
+                state->segments[i].commandedRestLengthMeters;
+            segments[i].tension = state->segments[i].tensionNewtons;
+        }
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+// softwing::SoftBody::constraintColouringView (soft_body.h:463-467) on a body
+// holding the definition's nodes and distance-like constraints.
+swb_status swref_colouring(const swb_structure_definition* d,
+                           uint64_t* order,
+                           uint64_t* offsets,
+                           uint64_t offsets_capacity,
+                           uint64_t* colour_count,
+                           uint64_t* parallel_colours) {
+    try {
+        softwing::SoftBody body;
+        for (uint64_t i = 0; i < d->node_count; ++i) {
+            const swb_node_def& n = d->nodes[i];
+            const softwing::Vec3 p{n.position.x, n.position.y, n.position.z};
+            if (n.fixed)
+                body.addFixedNode(p);
+            else
+                body.addNode(p, n.mass);
+        }
+        for (uint64_t i = 0; i < d->constraint_count; ++i) {
+            const swb_constraint_def& c = d->constraints[i];
+            switch (c.kind) {
+            case SWB_CONSTRAINT_CABLE:
+                body.addCableConstraint(c.first_node, c.second_node,
+                                        c.rest_length, c.compliance);
+                break;
+            case SWB_CONSTRAINT_SUSPENSION_TIE:
+                body.addSuspensionTieConstraint(c.first_node, c.second_node,
+                                                c.rest_length, c.compliance);
+                break;
+            case SWB_CONSTRAINT_SEAM_STITCH:
+                body.addSeamStitchConstraint(c.first_node, c.second_node);
+                break;
+            default:
+                body.addDistanceConstraint(c.first_node, c.second_node,
+                                           c.rest_length, c.compliance);
+            }
+        }
+        const auto view = body.constraintColouringView();
+        const auto report = body.constraintColouringReport();
+        for (std::size_t i = 0; i < view.order.size(); ++i)
+            order[i] = view.order[i];
+        if (view.colourOffsets.size() > offsets_capacity)
+            throw std::invalid_argument("offsets capacity too small");
+        for (std::size_t i = 0; i < view.colourOffsets.size(); ++i)
+            offsets[i] = view.colourOffsets[i];
+        *colour_count =
+            view.colourOffsets.empty() ? 0 : view.colourOffsets.size() - 1;
+        *parallel_colours = report.parallelColours;
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,386 @@
+"""B200 XPBD structural solver: Python mirror of SimWing's structural adapter.
+
+`Structure` follows `simwing::fsi::Structure` (src/fsi/structure.h:273-309):
+the same calls, argument meaning and error behaviour, over the library's
+C-ABI (include/simwing_b200.h).  Reference exception types map to Python
+ones: std::invalid_argument -> InvalidArgument (ValueError),
+std::out_of_range -> OutOfRange (IndexError), softwing::SuspensionError ->
+SuspensionError, softwing::ContactStepError -> ContactStepError.  A failed
+step restores the pre-step state before raising, as the reference does.
+
+There is no CPU fallback: importing the solver requires the built CUDA
+library (simwing_b200/libsimwing_b200.so) and a CUDA device to run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from .abi import Vec3
+
+__all__ = [
+    "Structure", "Definition", "StepSettings", "SolverOptions", "generate_patch", "generate_wing",
+    "SimwingError", "InvalidArgument", "OutOfRange", "SuspensionError", "ContactStepError",
+    "NonFiniteState", "SyncTimeout", "CudaError", "Unsupported", "reference_colouring",
+]
+
+
+class SimwingError(RuntimeError):
+    status = -1
+
+
+class InvalidArgument(SimwingError, ValueError):
+    status = abi.INVALID_ARGUMENT
+
+
+class OutOfRange(SimwingError, IndexError):
+    status = abi.OUT_OF_RANGE
+
+
+class SuspensionError(SimwingError):
+    status = abi.SUSPENSION_ERROR
+
+
+class ContactStepError(SimwingError):
+    status = abi.CONTACT_ERROR
+
+
+class NonFiniteState(SimwingError):
+    status = abi.NON_FINITE
+
+
+class SyncTimeout(SimwingError):
+    status = abi.SYNC_TIMEOUT
+
+
+class CudaError(SimwingError):
+    status = abi.CUDA_ERROR
+
+
+class Unsupported(SimwingError):
+    status = abi.UNSUPPORTED
+
+
+class OutOfMemory(SimwingError, MemoryError):
+    status = abi.OUT_OF_MEMORY
+
+
+_ERRORS = {cls.status: cls for cls in (InvalidArgument, OutOfRange, SuspensionError, ContactStepError,
+                                        NonFiniteState, SyncTimeout, CudaError, Unsupported, OutOfMemory)}
+
+
+def _check(status: int) -> None:
+    if status != abi.OK:
+        message = abi.library().swb_last_error().decode(errors="replace")
+        raise _ERRORS.get(status, SimwingError)(message)
+
+
+def StepSettings(**overrides) -> abi.StepSettings:
+    """StructureStepSettings with the reference defaults (structure.h:208-219)."""
+    s = abi.StepSettings()
+    abi.library().swb_default_step_settings(C.byref(s))
+    for key, value in overrides.items():
+        if key in ("gravity", "damping_reference_velocity"):
+            value = Vec3(*value)
+        setattr(s, key, value)
+    return s
+
+
+def SolverOptions(**overrides) -> abi.SolverOptions:
+    o = abi.SolverOptions()
+    abi.library().swb_default_solver_options(C.byref(o))
+    for key, value in overrides.items():
+        setattr(o, key, value)
+    return o
+
+
+def _array(ptr, count, ctype):
+    if count == 0:
+        return np.zeros(0, dtype=np.dtype(ctype))
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(count,))
+
+
+class Definition:
+    """An owned StructureDefinition (swb_definition handle)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+        self._lib = abi.library()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and h.value:
+            self._lib.swb_definition_destroy(h)
+            self._h = C.c_void_p()
+
+    @property
+    def view(self) -> abi.StructureDefinition:
+        return self._lib.swb_definition_view(self._h).contents
+
+    @property
+    def pointer(self):
+        return self._lib.swb_definition_view(self._h)
+
+    def copy(self) -> "Definition":
+        out = C.c_void_p()
+        _check(self._lib.swb_definition_copy(self.pointer, C.byref(out)))
+        return Definition(out.value)
+
+    def permuted(self, constraint_order=None, dihedral_order=None) -> "Definition":
+        d = self.copy()
+        co = None if constraint_order is None else np.ascontiguousarray(constraint_order, dtype=np.uint64)
+        ho = None if dihedral_order is None else np.ascontiguousarray(dihedral_order, dtype=np.uint64)
+        _check(self._lib.swb_definition_permute(
+            d._h, None if co is None else co.ctypes.data, None if ho is None else ho.ctypes.data))
+        return d
+
+    def scale_rest(self, index: int, factor: float) -> None:
+        _check(self._lib.swb_definition_scale_rest(self._h, index, factor))
+
+    @property
+    def fingerprint(self) -> int:
+        return int(self._lib.swb_definition_fingerprint(self.pointer))
+
+    def validate(self) -> None:
+        _check(self._lib.swb_validate_definition(self.pointer))
+
+    # numpy views (valid while the definition lives)
+    @property
+    def node_count(self) -> int:
+        return int(self.view.node_count)
+
+    def positions(self) -> np.ndarray:
+        v = self.view
+        raw = _array(v.nodes, v.node_count, abi.NodeDef)
+        return np.stack([raw["position"]["x"], raw["position"]["y"], raw["position"]["z"]], axis=1)
+
+    def nodes(self):
+        v = self.view
+        return _array(v.nodes, v.node_count, abi.NodeDef)
+
+    def triangles(self):
+        v = self.view
+        return _array(v.triangles, v.triangle_count, abi.TriangleDef)
+
+    def constraints(self):
+        v = self.view
+        return _array(v.constraints, v.constraint_count, abi.ConstraintDef)
+
+    def dihedrals(self):
+        v = self.view
+        return _array(v.dihedrals, v.dihedral_count, abi.DihedralDef)
+
+    @property
+    def has_suspension(self) -> bool:
+        return bool(self.view.suspension)
+
+    def counts(self) -> dict:
+        v = self.view
+        out = {"nodes": int(v.node_count), "triangles": int(v.triangle_count),
+               "constraints": int(v.constraint_count), "dihedrals": int(v.dihedral_count),
+               "membranes": int(v.membrane_count)}
+        if v.suspension:
+            out["suspension_segments"] = int(v.suspension.contents.segment_count)
+        c = self.constraints()
+        for name, kind in (("distance", abi.DISTANCE), ("cable", abi.CABLE), ("seam_stitch", abi.SEAM_STITCH),
+                           ("suspension_tie", abi.SUSPENSION_TIE)):
+            out[name] = int(np.count_nonzero(c["kind"] == kind))
+        return out
+
+
+def generate_patch(**overrides) -> Definition:
+    """The hanging cloth patch (33 x 33 on 1 m x 1 m by default)."""
+    lib = abi.library()
+    p = abi.PatchParams()
+    lib.swb_default_patch_params(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    out = C.c_void_p()
+    _check(lib.swb_generate_patch(C.byref(p), C.byref(out)))
+    return Definition(out.value)
+
+
+def generate_wing(**overrides) -> Definition:
+    """The ram-air wing with cascaded lines and rigid pilot (40 cells by default)."""
+    lib = abi.library()
+    p = abi.WingParams()
+    lib.swb_default_wing_params(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    out = C.c_void_p()
+    _check(lib.swb_generate_wing(C.byref(p), C.byref(out)))
+    return Definition(out.value)
+
+
+def reference_colouring(definition: Definition):
+    """Bit-exact restatement of SoftBody::constraintColouringView."""
+    lib = abi.library()
+    m = definition.view.constraint_count
+    order = np.zeros(max(m, 1), dtype=np.uint64)
+    offsets = np.zeros(4096, dtype=np.uint64)
+    colours = C.c_uint64()
+    parallel = C.c_uint64()
+    _check(lib.swb_reference_colouring(definition.pointer, order.ctypes.data, offsets.ctypes.data,
+                                       offsets.size, C.byref(colours), C.byref(parallel)))
+    return order[:m], offsets[: colours.value + 1 if m else 0], int(parallel.value)
+
+
+@dataclass
+class SuspensionState:
+    center_of_mass: np.ndarray
+    body_to_world: np.ndarray  # w, x, y, z
+    linear_velocity: np.ndarray
+    angular_velocity: np.ndarray
+    segments: list
+    line_force: np.ndarray
+    line_moment: np.ndarray
+
+
+def _vec(v) -> np.ndarray:
+    return np.array([v.x, v.y, v.z])
+
+
+class Structure:
+    """simwing::fsi::Structure on the device (src/fsi/structure.h:273-309)."""
+
+    def __init__(self, definition: Definition, options: abi.SolverOptions | None = None):
+        self._lib = abi.library()
+        self._definition = definition
+        h = C.c_void_p()
+        _check(self._lib.swb_structure_create(definition.pointer, None if options is None else C.byref(options),
+                                              C.byref(h)))
+        self._h = h
+        self.node_count = int(self._lib.swb_structure_node_count(h))
+        self._segments = int(definition.view.suspension.contents.segment_count) if definition.has_suspension else 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.swb_structure_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def definition_fingerprint(self) -> int:
+        return int(self._lib.swb_structure_fingerprint(self._h))
+
+    def accepted_step_count(self) -> int:
+        return int(self._lib.swb_structure_accepted_steps(self._h))
+
+    def simulation_time_seconds(self) -> float:
+        return float(self._lib.swb_structure_simulation_time(self._h))
+
+    def clear_external_forces(self) -> None:
+        _check(self._lib.swb_structure_clear_external_forces(self._h))
+
+    def add_external_force(self, node: int, force) -> None:
+        if node < 0:
+            raise OutOfRange("Structure force node is out of range")
+        _check(self._lib.swb_structure_add_external_force(self._h, int(node), C.byref(Vec3(*force))))
+
+    def set_external_forces(self, forces) -> None:
+        f = np.ascontiguousarray(forces, dtype=np.float64)
+        if f.ndim != 2 or f.shape[1] != 3:
+            raise InvalidArgument("Structure forces must be an (n, 3) array")
+        _check(self._lib.swb_structure_set_external_forces(self._h, f.ctypes.data, f.shape[0]))
+
+    def set_face_pressure(self, triangle: int, pressure: float) -> None:
+        _check(self._lib.swb_structure_set_face_pressure(self._h, int(triangle), float(pressure)))
+
+    def set_uniform_pressure(self, pressure: float) -> None:
+        _check(self._lib.swb_structure_set_uniform_pressure(self._h, float(pressure)))
+
+    def step(self, settings: abi.StepSettings | None = None, diagnostics: bool = True):
+        s = settings if settings is not None else StepSettings()
+        d = abi.Diagnostics()
+        _check(self._lib.swb_structure_step(self._h, C.byref(s), C.byref(d) if diagnostics else None))
+        return d if diagnostics else None
+
+    def step_many(self, settings: abi.StepSettings, steps: int, diagnostics: bool = False):
+        d = abi.Diagnostics()
+        _check(self._lib.swb_structure_step_many(self._h, C.byref(settings), int(steps),
+                                                 C.byref(d) if diagnostics else None))
+        return d if diagnostics else None
+
+    def diagnostics(self) -> abi.Diagnostics:
+        d = abi.Diagnostics()
+        _check(self._lib.swb_structure_diagnostics(self._h, C.byref(d)))
+        return d
+
+    def node_states(self) -> np.ndarray:
+        """(n, 3, 3) array: position, previous position, velocity."""
+        out = np.zeros((self.node_count, 3, 3), dtype=np.float64)
+        _check(self._lib.swb_structure_read_nodes(self._h, out.ctypes.data, self.node_count))
+        return out
+
+    def positions(self) -> np.ndarray:
+        return self.node_states()[:, 0, :]
+
+    def write_node_states(self, states: np.ndarray) -> None:
+        s = np.ascontiguousarray(states, dtype=np.float64)
+        if s.shape != (self.node_count, 3, 3):
+            raise InvalidArgument("node states must be (n, 3, 3)")
+        _check(self._lib.swb_structure_write_nodes(self._h, s.ctypes.data, self.node_count))
+
+    def suspension_state(self) -> SuspensionState | None:
+        if not self._segments:
+            return None
+        p = abi.PayloadState()
+        segs = (abi.SegmentState * self._segments)()
+        w = abi.Wrench()
+        _check(self._lib.swb_structure_read_suspension(self._h, C.byref(p), segs, self._segments, C.byref(w)))
+        q = p.body_to_world
+        return SuspensionState(_vec(p.center_of_mass), np.array([q.w, q.x, q.y, q.z]), _vec(p.linear_velocity),
+                               _vec(p.angular_velocity),
+                               [(s.stable_id, s.current_length, s.commanded_rest_length, s.tension) for s in segs],
+                               _vec(w.force), _vec(w.moment))
+
+    def write_payload_state(self, com, q_wxyz, v, w) -> None:
+        p = abi.PayloadState(Vec3(*com), abi.Quat(*q_wxyz), Vec3(*v), Vec3(*w))
+        _check(self._lib.swb_structure_write_payload(self._h, C.byref(p)))
+
+    def checkpoint(self) -> bytes:
+        n = C.c_uint64()
+        _check(self._lib.swb_structure_checkpoint_size(self._h, C.byref(n)))
+        buf = (C.c_uint8 * n.value)()
+        _check(self._lib.swb_structure_checkpoint(self._h, buf, n.value))
+        return bytes(buf)
+
+    def restore(self, image: bytes) -> None:
+        buf = (C.c_uint8 * len(image)).from_buffer_copy(image)
+        _check(self._lib.swb_structure_restore(self._h, buf, len(image)))
+
+    def sweep_order(self, which: int) -> np.ndarray:
+        v = self._definition.view
+        n = v.constraint_count if which == abi.SWEEP_DISTANCE else v.dihedral_count
+        out = np.zeros(max(n, 1), dtype=np.uint64)
+        _check(self._lib.swb_structure_sweep_order(self._h, which, out.ctypes.data, n))
+        return out[:n]
+
+    def oracle_definition(self) -> Definition:
+        """The definition with its constraint lists permuted into the device
+        sweep order: the reference serial solver run on it performs exactly
+        the device's Gauss-Seidel sweep."""
+        return self._definition.permuted(self.sweep_order(abi.SWEEP_DISTANCE),
+                                         self.sweep_order(abi.SWEEP_DIHEDRAL))
+
+    def schedule_report(self) -> abi.ScheduleReport:
+        r = abi.ScheduleReport()
+        _check(self._lib.swb_structure_schedule_report(self._h, C.byref(r)))
+        return r
+
+    def last_step_ms(self) -> float:
+        return float(self._lib.swb_structure_last_step_ms(self._h))

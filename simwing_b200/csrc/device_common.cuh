@@ -1,0 +1,146 @@
+// Device helpers: vector math, the bounded device-wide barrier and the
+// bulk-copy staging primitives used by the persistent XPBD kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace swb {
+namespace dev {
+
+// Status bits written by kernels (atomicOr into status[0]); status[1] holds
+// a detail code of the first suspension failure.
+enum : int {
+    kStatusSyncTimeout = 1,
+    kStatusNonFinite = 2,
+    kStatusSuspension = 4,
+    kStatusCopyTimeout = 8,
+};
+
+enum : int {
+    kSuspLineGeometry = 1,
+    kSuspLineInput = 2,
+    kSuspEffectiveMass = 3,
+    kSuspPayload = 4,
+    kSuspResidual = 5,
+    kSuspOrientation = 6,
+};
+
+__device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator/(float3 a, float s) { return make_float3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float length(float3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ bool finite3(float3 a) {
+    return isfinite(a.x) && isfinite(a.y) && isfinite(a.z);
+}
+
+// ---- bounded device-wide barrier -------------------------------------------
+// Sense-reversing barrier over all CTAs of a cooperative launch.  Thread 0
+// of each CTA arrives with a release fence and spins with acquire loads on
+// the generation word.  The spin is bounded by `budget` clock64 cycles;
+// when it runs out the CTA records kStatusSyncTimeout and every later
+// barrier returns immediately, so the kernel always terminates.
+struct GridBarrier {
+    unsigned int* count;
+    unsigned int* generation;
+    int* status;
+    long long budget;
+    unsigned int blocks;
+};
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_relaxed_status(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Returns false when the barrier (or an earlier one) timed out.
+__device__ __forceinline__ bool grid_sync(const GridBarrier& g) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = (ld_relaxed_status(g.status) & kStatusSyncTimeout) == 0;
+        if (ok) {
+            const unsigned int gen = ld_acquire(g.generation);
+            __threadfence();
+            const unsigned int arrived = atomicAdd(g.count, 1u) + 1u;
+            if (arrived == g.blocks) {
+                atomicExch(g.count, 0u);
+                __threadfence();
+                atomicAdd(g.generation, 1u);
+            } else {
+                const long long start = clock64();
+                while (ld_acquire(g.generation) == gen) {
+                    if (clock64() - start > g.budget) {
+                        atomicOr(g.status, kStatusSyncTimeout);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+            __threadfence();
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// ---- bulk global->shared staging (cp.async.bulk + mbarrier) ------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// One bulk copy; dst/src 16-byte aligned, bytes a non-zero multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait for phase `parity` of the barrier; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long budget) {
+    const long long start = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - start > budget) return false;
+    }
+    return true;
+}
+
+}  // namespace dev
+}  // namespace swb

@@ -1,0 +1,540 @@
+// Host construction of the device sweep schedule (see schedule.h).
+#include "schedule.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <queue>
+#include <tuple>
+
+namespace swb {
+namespace {
+
+struct Constraint {
+    uint32_t n[4];
+    int count;          // 2 or 4
+    uint32_t def_index;
+};
+
+// Recursive coordinate bisection into `parts` balanced parts, choosing on
+// every split the axis and the cut position (within the balance tolerance)
+// that cut the fewest constraints.  Items are groups of nodes that must
+// stay together; constraints are given over items.
+class Bisector {
+public:
+    Bisector(const std::vector<std::array<double, 3>>& item_pos,
+             const std::vector<double>& item_weight,
+             const std::vector<std::vector<uint32_t>>& cons_items,
+             double tolerance)
+        : pos_(item_pos), weight_(item_weight), cons_(cons_items),
+          tol_(tolerance), part_(item_pos.size(), 0), rank_(item_pos.size(), 0) {}
+
+    std::vector<int> run(int parts) {
+        std::vector<uint32_t> items(pos_.size());
+        std::iota(items.begin(), items.end(), 0u);
+        std::vector<uint32_t> cons;
+        for (uint32_t c = 0; c < cons_.size(); ++c) cons.push_back(c);
+        split(items, cons, parts, 0);
+        return part_;
+    }
+
+private:
+    void split(std::vector<uint32_t>& items, std::vector<uint32_t>& cons,
+               int parts, int base) {
+        if (parts <= 1 || items.size() <= 1) {
+            for (uint32_t i : items) part_[i] = base;
+            return;
+        }
+        const int left_parts = parts / 2;
+        double total = 0.0;
+        for (uint32_t i : items) total += weight_[i];
+        const double target = total * left_parts / parts;
+        const size_t n = items.size();
+        double best_score = 1e300;
+        int best_axis = 0;
+        size_t best_index = n / 2;
+        std::vector<uint32_t> sorted(items);
+        std::vector<int64_t> diff(n + 2);
+        std::vector<double> prefix(n + 1);
+        for (int axis = 0; axis < 3; ++axis) {
+            std::stable_sort(sorted.begin(), sorted.end(), [&](uint32_t l, uint32_t r) {
+                if (pos_[l][axis] != pos_[r][axis]) return pos_[l][axis] < pos_[r][axis];
+                return l < r;
+            });
+            for (size_t k = 0; k < n; ++k) rank_[sorted[k]] = static_cast<uint32_t>(k);
+            prefix[0] = 0.0;
+            for (size_t k = 0; k < n; ++k) prefix[k + 1] = prefix[k] + weight_[sorted[k]];
+            std::fill(diff.begin(), diff.end(), 0);
+            for (uint32_t c : cons) {
+                uint32_t lo = UINT32_MAX, hi = 0;
+                for (uint32_t it : cons_[c]) {
+                    lo = std::min(lo, rank_[it]);
+                    hi = std::max(hi, rank_[it]);
+                }
+                if (lo == hi) continue;
+                diff[lo + 1] += 1;
+                diff[hi + 1] -= 1;
+            }
+            int64_t cut = 0;
+            size_t closest = 1;
+            for (size_t i = 1; i < n; ++i)
+                if (std::fabs(prefix[i] - target) < std::fabs(prefix[closest] - target))
+                    closest = i;
+            for (size_t i = 1; i < n; ++i) {
+                cut += diff[i];
+                const double imbalance = std::fabs(prefix[i] - target) / total;
+                if (imbalance > tol_ && i != closest) continue;
+                const double score = static_cast<double>(cut) + 4.0 * imbalance * cons.size();
+                if (score < best_score) {
+                    best_score = score;
+                    best_axis = axis;
+                    best_index = i;
+                }
+            }
+        }
+        std::vector<uint32_t> best_sorted(items);
+        std::stable_sort(best_sorted.begin(), best_sorted.end(), [&](uint32_t l, uint32_t r) {
+            if (pos_[l][best_axis] != pos_[r][best_axis])
+                return pos_[l][best_axis] < pos_[r][best_axis];
+            return l < r;
+        });
+        for (size_t k = 0; k < n; ++k) rank_[best_sorted[k]] = static_cast<uint32_t>(k);
+        std::vector<uint32_t> left(best_sorted.begin(), best_sorted.begin() + best_index);
+        std::vector<uint32_t> right(best_sorted.begin() + best_index, best_sorted.end());
+        std::vector<uint32_t> lc, rc;
+        for (uint32_t c : cons) {
+            bool all_left = true, all_right = true;
+            for (uint32_t it : cons_[c]) {
+                if (rank_[it] < best_index) all_right = false;
+                else all_left = false;
+            }
+            if (all_left) lc.push_back(c);
+            else if (all_right) rc.push_back(c);
+        }
+        items.clear();
+        items.shrink_to_fit();
+        cons.clear();
+        cons.shrink_to_fit();
+        split(left, lc, left_parts, base);
+        split(right, rc, parts - left_parts, base + left_parts);
+    }
+
+    const std::vector<std::array<double, 3>>& pos_;
+    const std::vector<double>& weight_;
+    const std::vector<std::vector<uint32_t>>& cons_;
+    double tol_;
+    std::vector<int> part_;
+    std::vector<uint32_t> rank_;
+};
+
+// DSatur colouring of constraints that conflict when they share a node.
+// Returns colour per constraint and the colour count.
+int dsatur(const std::vector<const Constraint*>& cons, std::vector<int>& colour) {
+    const size_t m = cons.size();
+    colour.assign(m, -1);
+    if (m == 0) return 0;
+    // node -> constraints
+    std::vector<uint32_t> nodes;
+    for (const Constraint* c : cons)
+        for (int k = 0; k < c->count; ++k) nodes.push_back(c->n[k]);
+    std::sort(nodes.begin(), nodes.end());
+    nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+    auto node_id = [&](uint32_t n) {
+        return static_cast<size_t>(std::lower_bound(nodes.begin(), nodes.end(), n) - nodes.begin());
+    };
+    std::vector<uint32_t> off(nodes.size() + 1, 0);
+    std::vector<std::array<uint32_t, 4>> cn(m);
+    for (size_t i = 0; i < m; ++i)
+        for (int k = 0; k < cons[i]->count; ++k) {
+            cn[i][k] = static_cast<uint32_t>(node_id(cons[i]->n[k]));
+            ++off[cn[i][k] + 1];
+        }
+    for (size_t v = 0; v < nodes.size(); ++v) off[v + 1] += off[v];
+    std::vector<uint32_t> inc(off.back());
+    std::vector<uint32_t> cur(off.begin(), off.end() - 1);
+    for (size_t i = 0; i < m; ++i)
+        for (int k = 0; k < cons[i]->count; ++k) inc[cur[cn[i][k]]++] = static_cast<uint32_t>(i);
+    std::vector<uint32_t> degree(m, 0);
+    for (size_t i = 0; i < m; ++i)
+        for (int k = 0; k < cons[i]->count; ++k) degree[i] += off[cn[i][k] + 1] - off[cn[i][k]] - 1;
+    std::vector<std::vector<uint64_t>> used(m);
+    std::vector<uint32_t> sat(m, 0);
+    using Key = std::tuple<uint32_t, uint32_t, int64_t>;  // sat, degree, -index
+    std::priority_queue<Key> heap;
+    for (size_t i = 0; i < m; ++i) heap.emplace(0u, degree[i], -static_cast<int64_t>(i));
+    int colours = 0;
+    auto has = [&](size_t i, int c) {
+        const auto& u = used[i];
+        return static_cast<size_t>(c / 64) < u.size() && ((u[c / 64] >> (c % 64)) & 1u);
+    };
+    while (!heap.empty()) {
+        auto [s, dg, ni] = heap.top();
+        heap.pop();
+        const size_t i = static_cast<size_t>(-ni);
+        if (colour[i] >= 0 || s != sat[i]) continue;
+        int c = 0;
+        while (has(i, c)) ++c;
+        colour[i] = c;
+        colours = std::max(colours, c + 1);
+        for (int k = 0; k < cons[i]->count; ++k) {
+            const uint32_t v = cn[i][k];
+            for (uint32_t q = off[v]; q < off[v + 1]; ++q) {
+                const uint32_t j = inc[q];
+                if (colour[j] >= 0 || has(j, c)) continue;
+                auto& u = used[j];
+                if (u.size() <= static_cast<size_t>(c / 64)) u.resize(c / 64 + 1, 0);
+                u[c / 64] |= uint64_t{1} << (c % 64);
+                ++sat[j];
+                heap.emplace(sat[j], degree[j], -static_cast<int64_t>(j));
+            }
+        }
+    }
+    return colours;
+}
+
+}  // namespace
+
+Schedule build_schedule(const OwnedDefinition& d,
+                        const std::vector<uint32_t>& suspension_nodes,
+                        const ScheduleOptions& opt) {
+    Schedule S;
+    const uint32_t N = static_cast<uint32_t>(d.nodes.size());
+    const int G = std::max(1, opt.blocks);
+    S.blocks = G;
+    S.node_count = N;
+    const int L = opt.global_only ? 0 : std::clamp(opt.levels, 1, kMaxLevels);
+
+    // Constraints of both kinds.
+    std::array<std::vector<Constraint>, kKinds> all;
+    for (uint32_t i = 0; i < d.constraints.size(); ++i) {
+        const auto& c = d.constraints[i];
+        all[0].push_back({{static_cast<uint32_t>(c.first_node),
+                           static_cast<uint32_t>(c.second_node), 0, 0}, 2, i});
+    }
+    for (uint32_t i = 0; i < d.dihedrals.size(); ++i) {
+        const auto& h = d.dihedrals[i];
+        all[1].push_back({{static_cast<uint32_t>(h.nodes[0]), static_cast<uint32_t>(h.nodes[1]),
+                           static_cast<uint32_t>(h.nodes[2]), static_cast<uint32_t>(h.nodes[3])},
+                          4, i});
+    }
+
+    // ---- level 1: node partition over items (suspension nodes grouped) ----
+    std::vector<uint32_t> item_of(N);
+    std::vector<std::array<double, 3>> ipos;
+    std::vector<double> iweight;
+    std::vector<uint32_t> incidence(N, 0);
+    for (int k = 0; k < kKinds; ++k)
+        for (const Constraint& c : all[k])
+            for (int q = 0; q < c.count; ++q) ++incidence[c.n[q]];
+    {
+        std::vector<uint8_t> is_susp(N, 0);
+        for (uint32_t n : suspension_nodes) is_susp[n] = 1;
+        int32_t group = -1;
+        std::array<double, 3> gsum{0, 0, 0};
+        double gw = 0.0;
+        uint32_t gcount = 0;
+        for (uint32_t n = 0; n < N; ++n) {
+            const auto& p = d.nodes[n].position;
+            const double w = 1.0 + 0.5 * incidence[n];
+            if (is_susp[n]) {
+                if (group < 0) {
+                    group = static_cast<int32_t>(ipos.size());
+                    ipos.push_back({0, 0, 0});
+                    iweight.push_back(0);
+                }
+                item_of[n] = static_cast<uint32_t>(group);
+                gsum[0] += p.x; gsum[1] += p.y; gsum[2] += p.z;
+                gw += w;
+                ++gcount;
+            } else {
+                item_of[n] = static_cast<uint32_t>(ipos.size());
+                ipos.push_back({p.x, p.y, p.z});
+                iweight.push_back(w);
+            }
+        }
+        if (group >= 0) {
+            ipos[group] = {gsum[0] / gcount, gsum[1] / gcount, gsum[2] / gcount};
+            iweight[group] = gw;
+        }
+    }
+    std::vector<std::vector<uint32_t>> cons_items;
+    for (int k = 0; k < kKinds; ++k)
+        for (const Constraint& c : all[k]) {
+            std::vector<uint32_t> it;
+            for (int q = 0; q < c.count; ++q) it.push_back(item_of[c.n[q]]);
+            cons_items.push_back(std::move(it));
+        }
+    std::vector<int> item_part = Bisector(ipos, iweight, cons_items, opt.balance_tolerance).run(G);
+    std::vector<int> part1(N);
+    for (uint32_t n = 0; n < N; ++n) part1[n] = item_part[item_of[n]];
+
+    // Slots: level-1 part-major, node index within.
+    S.l1_begin.assign(G + 1, 0);
+    for (uint32_t n = 0; n < N; ++n) ++S.l1_begin[part1[n] + 1];
+    for (int b = 0; b < G; ++b) S.l1_begin[b + 1] += S.l1_begin[b];
+    S.node_of_slot.assign(N, 0);
+    S.slot_of_node.assign(N, 0);
+    {
+        std::vector<uint32_t> cur(S.l1_begin.begin(), S.l1_begin.end() - 1);
+        for (uint32_t n = 0; n < N; ++n) {
+            const uint32_t s = cur[part1[n]]++;
+            S.node_of_slot[s] = n;
+            S.slot_of_node[n] = s;
+        }
+    }
+    for (int b = 0; b < G; ++b)
+        S.max_patch_nodes = std::max<int>(S.max_patch_nodes, S.l1_begin[b + 1] - S.l1_begin[b]);
+    if (S.max_patch_nodes > 65535)
+        raise(SWB_UNSUPPORTED, "a level-1 patch exceeds 65535 nodes; use more blocks");
+    if (!suspension_nodes.empty()) S.suspension_block = part1[suspension_nodes[0]];
+
+    // ---- levels: assign interior constraints, repartition the rest --------
+    std::array<std::vector<const Constraint*>, kKinds> remaining;
+    for (int k = 0; k < kKinds; ++k)
+        for (const Constraint& c : all[k]) remaining[k].push_back(&c);
+
+    // per-level per-kind per-block constraint lists
+    std::vector<std::array<std::vector<std::vector<const Constraint*>>, kKinds>> lists(kMaxLevels);
+    std::vector<std::vector<int>> level_part(kMaxLevels);  // node -> part (or -1)
+    int used_levels = 0;
+    for (int level = 0; level < L; ++level) {
+        std::vector<int> part(N, -1);
+        if (level == 0) {
+            part = part1;
+        } else {
+            // items = nodes touched by remaining constraints
+            std::vector<int32_t> item(N, -1);
+            std::vector<std::array<double, 3>> p2;
+            std::vector<double> w2;
+            std::vector<uint32_t> node_of_item;
+            for (int k = 0; k < kKinds; ++k)
+                for (const Constraint* c : remaining[k])
+                    for (int q = 0; q < c->count; ++q) {
+                        const uint32_t n = c->n[q];
+                        if (item[n] < 0) {
+                            item[n] = static_cast<int32_t>(p2.size());
+                            const auto& pp = d.nodes[n].position;
+                            p2.push_back({pp.x, pp.y, pp.z});
+                            w2.push_back(0.0);
+                            node_of_item.push_back(n);
+                        }
+                        w2[item[n]] += 1.0;
+                    }
+            if (p2.empty()) break;
+            std::vector<std::vector<uint32_t>> ci;
+            for (int k = 0; k < kKinds; ++k)
+                for (const Constraint* c : remaining[k]) {
+                    std::vector<uint32_t> it;
+                    for (int q = 0; q < c->count; ++q) it.push_back(static_cast<uint32_t>(item[c->n[q]]));
+                    ci.push_back(std::move(it));
+                }
+            std::vector<int> ip = Bisector(p2, w2, ci, opt.balance_tolerance).run(G);
+            for (size_t i = 0; i < ip.size(); ++i) part[node_of_item[i]] = ip[i];
+        }
+        level_part[level] = part;
+        bool any = false;
+        for (int k = 0; k < kKinds; ++k) {
+            lists[level][k].assign(G, {});
+            std::vector<const Constraint*> rest;
+            for (const Constraint* c : remaining[k]) {
+                const int p0 = part[c->n[0]];
+                bool inside = p0 >= 0;
+                for (int q = 1; q < c->count && inside; ++q) inside = part[c->n[q]] == p0;
+                if (inside) {
+                    lists[level][k][p0].push_back(c);
+                    any = true;
+                } else {
+                    rest.push_back(c);
+                }
+            }
+            remaining[k].swap(rest);
+        }
+        if (!any && level > 0) break;
+        used_levels = level + 1;
+    }
+    S.levels = used_levels;
+
+    // ---- per level tables ---------------------------------------------------
+    std::vector<uint8_t> touched_outside_l1(N, 0);
+    for (int level = 0; level < used_levels; ++level) {
+        // Patch node lists for levels >= 2: nodes referenced by that level.
+        std::vector<int32_t> local(N, -1);
+        if (level > 0) {
+            S.patch_begin[level].assign(G + 1, 0);
+            for (int b = 0; b < G; ++b) {
+                std::vector<uint32_t> nodes;
+                for (int k = 0; k < kKinds; ++k)
+                    for (const Constraint* c : lists[level][k][b])
+                        for (int q = 0; q < c->count; ++q) nodes.push_back(c->n[q]);
+                std::sort(nodes.begin(), nodes.end(), [&](uint32_t x, uint32_t y) {
+                    return S.slot_of_node[x] < S.slot_of_node[y];
+                });
+                nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+                if (nodes.size() > 65535)
+                    raise(SWB_UNSUPPORTED, "a gathered patch exceeds 65535 nodes");
+                for (size_t i = 0; i < nodes.size(); ++i) {
+                    local[nodes[i]] = static_cast<int32_t>(i);
+                    S.patch_slots[level].push_back(S.slot_of_node[nodes[i]]);
+                    touched_outside_l1[nodes[i]] = 1;
+                }
+                S.patch_begin[level][b + 1] = S.patch_begin[level][b] + static_cast<uint32_t>(nodes.size());
+                S.max_gather_nodes = std::max<int>(S.max_gather_nodes, static_cast<int>(nodes.size()));
+            }
+        }
+        for (int k = 0; k < kKinds; ++k) {
+            Table& T = S.tables[level][k];
+            T.block_begin.assign(G + 1, 0);
+            std::vector<std::vector<const Constraint*>> staged(G);
+            std::vector<std::vector<uint32_t>> stage_sizes(G);
+            int max_stages = 0;
+            for (int b = 0; b < G; ++b) {
+                const auto& cl = lists[level][k][b];
+                std::vector<int> colour;
+                const int colours = dsatur(cl, colour);
+                max_stages = std::max(max_stages, colours);
+                std::vector<uint32_t> count(colours, 0);
+                for (int c : colour) ++count[c];
+                // stable colour-major order
+                std::vector<uint32_t> idx(cl.size());
+                std::iota(idx.begin(), idx.end(), 0u);
+                std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+                    return colour[x] < colour[y];
+                });
+                for (uint32_t i : idx) staged[b].push_back(cl[i]);
+                stage_sizes[b] = count;
+            }
+            T.stages = max_stages;
+            T.stage_offsets.assign(static_cast<size_t>(G) * (max_stages + 1), 0);
+            for (int b = 0; b < G; ++b) {
+                const uint32_t count = static_cast<uint32_t>(staged[b].size());
+                const uint32_t padded = (count + 3u) & ~3u;
+                T.block_begin[b + 1] = T.block_begin[b] + padded;
+                T.max_block_count = std::max(T.max_block_count, padded);
+                uint32_t off = 0;
+                for (int s = 0; s < max_stages; ++s) {
+                    T.stage_offsets[static_cast<size_t>(b) * (max_stages + 1) + s] = off;
+                    if (s < static_cast<int>(stage_sizes[b].size())) off += stage_sizes[b][s];
+                }
+                T.stage_offsets[static_cast<size_t>(b) * (max_stages + 1) + max_stages] = off;
+                const uint32_t base = (level == 0) ? S.l1_begin[b] : 0;
+                for (uint32_t i = 0; i < padded; ++i) {
+                    if (i < count) {
+                        const Constraint* c = staged[b][i];
+                        uint32_t li[4] = {0, 0, 0, 0};
+                        for (int q = 0; q < c->count; ++q)
+                            li[q] = level == 0 ? S.slot_of_node[c->n[q]] - base
+                                               : static_cast<uint32_t>(local[c->n[q]]);
+                        T.ab.push_back(li[0] | (li[1] << 16));
+                        if (k == 1) T.cd.push_back(li[2] | (li[3] << 16));
+                        if (k == 0) {
+                            const auto& dc = d.constraints[c->def_index];
+                            const bool stitch = dc.kind == SWB_CONSTRAINT_SEAM_STITCH;
+                            T.rest.push_back(stitch ? 0.0f : static_cast<float>(dc.rest_length));
+                            float cp = stitch ? 0.0f : static_cast<float>(dc.compliance);
+                            if (dc.kind == SWB_CONSTRAINT_CABLE) cp = std::copysign(std::fabs(cp), -1.0f);
+                            T.comp.push_back(cp);
+                        } else {
+                            const auto& dh = d.dihedrals[c->def_index];
+                            T.rest.push_back(static_cast<float>(dh.rest_angle));
+                            T.comp.push_back(static_cast<float>(dh.compliance));
+                        }
+                        T.def_index.push_back(c->def_index);
+                        T.valid.push_back(1);
+                    } else {
+                        T.ab.push_back(0);
+                        if (k == 1) T.cd.push_back(0);
+                        T.rest.push_back(0.0f);
+                        T.comp.push_back(0.0f);
+                        T.def_index.push_back(0);
+                        T.valid.push_back(0);
+                    }
+                }
+                S.level_constraints[level] += count;
+            }
+        }
+    }
+
+    // ---- global leftovers -------------------------------------------------
+    for (int k = 0; k < kKinds; ++k) {
+        GlobalTable& T = S.global[k];
+        std::vector<int> colour;
+        const int colours = dsatur(remaining[k], colour);
+        std::vector<uint32_t> idx(remaining[k].size());
+        std::iota(idx.begin(), idx.end(), 0u);
+        std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+            return colour[x] < colour[y];
+        });
+        T.colour_offsets.assign(colours + 1, 0);
+        for (int c : colour) ++T.colour_offsets[c + 1];
+        for (int c = 0; c < colours; ++c) T.colour_offsets[c + 1] += T.colour_offsets[c];
+        for (uint32_t i : idx) {
+            const Constraint* c = remaining[k][i];
+            T.a.push_back(S.slot_of_node[c->n[0]]);
+            T.b.push_back(S.slot_of_node[c->n[1]]);
+            for (int q = 0; q < c->count; ++q) touched_outside_l1[c->n[q]] = 1;
+            if (k == 1) {
+                T.c.push_back(S.slot_of_node[c->n[2]]);
+                T.d.push_back(S.slot_of_node[c->n[3]]);
+                const auto& dh = d.dihedrals[c->def_index];
+                T.rest.push_back(static_cast<float>(dh.rest_angle));
+                T.comp.push_back(static_cast<float>(dh.compliance));
+            } else {
+                const auto& dc = d.constraints[c->def_index];
+                const bool stitch = dc.kind == SWB_CONSTRAINT_SEAM_STITCH;
+                T.rest.push_back(stitch ? 0.0f : static_cast<float>(dc.rest_length));
+                float cp = stitch ? 0.0f : static_cast<float>(dc.compliance);
+                if (dc.kind == SWB_CONSTRAINT_CABLE) cp = std::copysign(std::fabs(cp), -1.0f);
+                T.comp.push_back(cp);
+            }
+            T.def_index.push_back(c->def_index);
+        }
+        S.global_constraints += remaining[k].size();
+    }
+
+    // ---- sweep orders --------------------------------------------------------
+    for (int k = 0; k < kKinds; ++k) {
+        auto& order = k == 0 ? S.distance_order : S.dihedral_order;
+        for (int level = 0; level < used_levels; ++level) {
+            const Table& T = S.tables[level][k];
+            for (size_t i = 0; i < T.def_index.size(); ++i)
+                if (T.valid[i]) order.push_back(T.def_index[i]);
+        }
+        for (uint32_t i : S.global[k].def_index) order.push_back(i);
+    }
+
+    // ---- seam closing pass: level scheduling in sweep order -------------------
+    {
+        std::vector<int32_t> node_stage(N, -1);
+        std::vector<std::pair<int, uint64_t>> st;
+        for (uint64_t i : S.distance_order) {
+            const auto& c = d.constraints[i];
+            if (c.kind != SWB_CONSTRAINT_SEAM_STITCH) continue;
+            const int s = std::max(node_stage[c.first_node], node_stage[c.second_node]) + 1;
+            node_stage[c.first_node] = node_stage[c.second_node] = s;
+            st.emplace_back(s, i);
+            touched_outside_l1[c.first_node] = touched_outside_l1[c.second_node] = 1;
+        }
+        std::stable_sort(st.begin(), st.end(),
+                         [](const auto& x, const auto& y) { return x.first < y.first; });
+        int stages = st.empty() ? 0 : st.back().first + 1;
+        S.seam_stage_offsets.assign(stages + 1, 0);
+        for (const auto& [s, i] : st) {
+            ++S.seam_stage_offsets[s + 1];
+            S.seam_a.push_back(S.slot_of_node[d.constraints[i].first_node]);
+            S.seam_b.push_back(S.slot_of_node[d.constraints[i].second_node]);
+        }
+        for (int s = 0; s < stages; ++s) S.seam_stage_offsets[s + 1] += S.seam_stage_offsets[s];
+    }
+
+    // ---- level-1 interface -----------------------------------------------------
+    S.iface_begin.assign(G + 1, 0);
+    for (int b = 0; b < G; ++b) {
+        for (uint32_t s = S.l1_begin[b]; s < S.l1_begin[b + 1]; ++s)
+            if (touched_outside_l1[S.node_of_slot[s]])
+                S.iface_local.push_back(static_cast<uint16_t>(s - S.l1_begin[b]));
+        S.iface_begin[b + 1] = static_cast<uint32_t>(S.iface_local.size());
+    }
+    return S;
+}
+
+}  // namespace swb

@@ -1,0 +1,931 @@
+// Single-structure device solver: the swb_structure_* entry points.
+// Replaces simwing::fsi::Structure (src/fsi/structure.h:273-309).
+#include "common.h"
+#include "schedule.h"
+#include "step_kernel.cuh"
+#include "structure_impl.h"
+
+#include <algorithm>
+#include <bit>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+
+namespace swb {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        raise(e == cudaErrorMemoryAllocation ? SWB_OUT_OF_MEMORY : SWB_CUDA_ERROR,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+template <class T>
+T* dalloc(std::vector<void*>& owned, size_t count) {
+    void* p = nullptr;
+    cuda_check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMalloc");
+    owned.push_back(p);
+    return static_cast<T*>(p);
+}
+
+template <class T>
+T* dupload(std::vector<void*>& owned, const std::vector<T>& host, cudaStream_t s) {
+    T* p = dalloc<T>(owned, host.size());
+    if (!host.empty())
+        cuda_check(cudaMemcpyAsync(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, s),
+                   "cudaMemcpyAsync");
+    return p;
+}
+
+uint32_t align16(uint32_t v) { return (v + 15u) & ~15u; }
+
+// Sort key of the reference's suspension normalisation: records are sorted
+// by their string ids "segment:<id>" / "harness:<id>"
+// (suspension.cpp:1000-1006), i.e. by the decimal spelling of the id.
+bool id_string_less(uint64_t a, uint64_t b) { return std::to_string(a) < std::to_string(b); }
+
+// Diagnostics partial sums per CTA (double).
+constexpr int kDiagFields = 16;
+
+__global__ void diagnostics_kernel(const float4* pos, const float4* prev, const float4* vel, uint32_t n,
+                                   const uint32_t* ca, const uint32_t* cb, const float* rest, const uint8_t* kind,
+                                   uint32_t m, double* partials) {
+    // fields: 0 dyn count, 1 mass, 2-4 sum m x, 5-7 sum m v, 8 KE, 9 finite(min),
+    //         10 max |distance error|, 11 max cable extension
+    double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0};
+    const uint32_t stride = blockDim.x * gridDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float4 X = pos[i], P = prev[i], V = vel[i];
+        const bool fin = isfinite(X.x) && isfinite(X.y) && isfinite(X.z) && isfinite(P.x) && isfinite(P.y) &&
+                         isfinite(P.z) && isfinite(V.x) && isfinite(V.y) && isfinite(V.z) && isfinite(X.w) &&
+                         X.w >= 0.0f;
+        if (!fin) acc[9] = 0.0;
+        if (X.w > 0.0f) {
+            const double mass = 1.0 / static_cast<double>(X.w);
+            acc[0] += 1.0;
+            acc[1] += mass;
+            acc[2] += mass * X.x; acc[3] += mass * X.y; acc[4] += mass * X.z;
+            acc[5] += mass * V.x; acc[6] += mass * V.y; acc[7] += mass * V.z;
+            acc[8] += 0.5 * mass * (double(V.x) * V.x + double(V.y) * V.y + double(V.z) * V.z);
+        }
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const float4 A = pos[ca[i]], B = pos[cb[i]];
+        const double dx = double(B.x) - A.x, dy = double(B.y) - A.y, dz = double(B.z) - A.z;
+        const double e = sqrt(dx * dx + dy * dy + dz * dz) - rest[i];
+        if (kind[i] == SWB_CONSTRAINT_CABLE) acc[11] = fmax(acc[11], fmax(0.0, e));
+        else acc[10] = fmax(acc[10], fabs(e));
+    }
+    __shared__ double red[32][12];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int f = 0; f < 12; ++f) {
+        double v = acc[f];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double u = __shfl_down_sync(0xffffffffu, v, o);
+            v = f == 9 ? fmin(v, u) : (f >= 10 ? fmax(v, u) : v + u);
+        }
+        if (lane == 0) red[warp][f] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int warps = (blockDim.x + 31) / 32;
+        for (int f = 0; f < 12; ++f) {
+            double v = red[0][f];
+            for (int w = 1; w < warps; ++w)
+                v = f == 9 ? fmin(v, red[w][f]) : (f >= 10 ? fmax(v, red[w][f]) : v + red[w][f]);
+            partials[blockIdx.x * kDiagFields + f] = v;
+        }
+    }
+}
+
+}  // namespace
+
+// ---- Structure construction --------------------------------------------------
+
+StructureImpl::~StructureImpl() {
+    if (device >= 0) cudaSetDevice(device);
+    for (void* p : owned) cudaFree(p);
+    if (h_force) cudaFreeHost(h_force);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void StructureImpl::build(const swb_structure_definition& definition, const swb_solver_options* options) {
+    def.assign(definition);
+    validate_definition(def.view);
+    fingerprint = definition_fingerprint(def.view);
+    if (def.has_contact) raise(SWB_UNSUPPORTED, "fabric self-contact is not available in this build");
+    if (!def.membranes.empty()) raise(SWB_UNSUPPORTED, "membrane elements are not available in this build");
+    swb_solver_options opt;
+    swb_default_solver_options(&opt);
+    if (options) opt = *options;
+    device = opt.device;
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cudaDeviceProp prop{};
+    cuda_check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (!prop.cooperativeLaunch) raise(SWB_UNSUPPORTED, "device lacks cooperative launch");
+    sm_count = prop.multiProcessorCount;
+    cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaEventCreate(&ev0), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&ev1), "cudaEventCreate");
+
+    const uint64_t N = def.nodes.size();
+    if (N >= (1ull << 31)) raise(SWB_UNSUPPORTED, "too many nodes");
+    pending.assign(N, swb_vec3{0, 0, 0});
+    pressure.resize(def.triangles.size());
+    for (size_t t = 0; t < def.triangles.size(); ++t) pressure[t] = def.triangles[t].pressure_difference;
+
+    // Suspension: endpoint nodes must share one level-1 patch.
+    std::vector<uint32_t> susp_nodes;
+    if (def.has_suspension) {
+        if (def.segments.size() > 8 || def.harness.size() > 8)
+            raise(SWB_UNSUPPORTED, "more than 8 suspension segments or harness points");
+        for (const auto& g : def.segments)
+            for (const swb_suspension_endpoint* e : {&g.from, &g.to}) {
+                if (e->kind == SWB_ENDPOINT_SURFACE_ATTACHMENT) {
+                    for (const auto& a : def.attachments)
+                        if (a.stable_id == e->stable_id) susp_nodes.push_back(static_cast<uint32_t>(a.node));
+                } else if (e->kind == SWB_ENDPOINT_JUNCTION) {
+                    for (const auto& j : def.junctions)
+                        if (j.stable_id == e->stable_id) susp_nodes.push_back(static_cast<uint32_t>(j.node));
+                }
+            }
+        std::sort(susp_nodes.begin(), susp_nodes.end());
+        susp_nodes.erase(std::unique(susp_nodes.begin(), susp_nodes.end()), susp_nodes.end());
+    }
+    ScheduleOptions so;
+    so.blocks = opt.blocks > 0 ? opt.blocks : sm_count;
+    so.blocks = static_cast<int>(std::min<uint64_t>(so.blocks, std::max<uint64_t>(1, N)));
+    so.levels = opt.partition_levels > 0 ? opt.partition_levels : 3;
+    so.global_only = (opt.flags & SWB_OPT_GLOBAL_ONLY) != 0;
+    sched = build_schedule(def, susp_nodes, so);
+    G = sched.blocks;
+
+    // Threads per CTA: enough for the widest local stage, in warps.
+    uint32_t widest = 32;
+    for (int l = 0; l < sched.levels; ++l)
+        for (int k = 0; k < kKinds; ++k) {
+            const Table& t = sched.tables[l][k];
+            for (int b = 0; b < G; ++b)
+                for (int s = 0; s < t.stages; ++s) {
+                    const size_t o = static_cast<size_t>(b) * (t.stages + 1) + s;
+                    widest = std::max(widest, t.stage_offsets[o + 1] - t.stage_offsets[o]);
+                }
+        }
+    threads = opt.block_threads > 0 ? opt.block_threads
+                                    : static_cast<int>(std::clamp<uint32_t>((widest + 31) / 32 * 32, 64, 512));
+    if (threads % 32 != 0 || threads < 32 || threads > 1024) raise(SWB_INVALID_ARGUMENT, "block_threads");
+
+    // ---- device images -------------------------------------------------------
+    // nodes (slot order)
+    std::vector<float4> pos(N), vel(N, make_float4(0, 0, 0, 0));
+    for (uint64_t s = 0; s < N; ++s) {
+        const swb_node_def& n = def.nodes[sched.node_of_slot[s]];
+        const float w = n.fixed ? 0.0f : static_cast<float>(1.0 / n.mass);
+        pos[s] = make_float4(static_cast<float>(n.position.x), static_cast<float>(n.position.y),
+                             static_cast<float>(n.position.z), w);
+    }
+    inv_mass.resize(N);
+    for (uint64_t s = 0; s < N; ++s) inv_mass[s] = pos[s].w;
+    for (int i = 0; i < 3; ++i) {
+        d_pos[i] = dupload(owned, pos, stream);
+        d_vel[i] = dupload(owned, vel, stream);
+        d_prev[i] = dupload(owned, pos, stream);
+    }
+    d_force = dalloc<float4>(owned, N);
+    cuda_check(cudaMemsetAsync(d_force, 0, N * sizeof(float4), stream), "memset");
+    cuda_check(cudaMallocHost(&h_force, std::max<uint64_t>(N, 1) * sizeof(float4)), "cudaMallocHost");
+    upload_pressure();
+
+    // schedule tables
+    StepParams& p = params;
+    std::memset(&p, 0, sizeof(p));
+    p.blocks = G;
+    p.levels = sched.levels;
+    p.l1_begin = dupload(owned, sched.l1_begin, stream);
+    uint32_t off = 0;
+    sched_n1_max = static_cast<uint32_t>(sched.max_patch_nodes);
+    sched_n2_max = static_cast<uint32_t>(sched.max_gather_nodes);
+    p.n1_max = sched_n1_max;
+    p.n2_max = sched_n2_max;
+    p.smem_x1 = off; off = align16(off + sched_n1_max * 16u);
+    p.smem_prev1 = off; off = align16(off + sched_n1_max * 16u);
+    p.smem_f1 = off; off = align16(off + sched_n1_max * 16u);
+    p.smem_x2 = off; off = align16(off + sched_n2_max * 16u);
+    for (int l = 0; l < kDevLevels; ++l)
+        for (int k = 0; k < kKinds; ++k) {
+            DevTable& t = p.tab[l][k];
+            std::memset(&t, 0, sizeof(t));
+            if (l >= sched.levels) {
+                static const uint32_t zero[2] = {0, 0};
+                (void)zero;
+                continue;
+            }
+            const Table& h = sched.tables[l][k];
+            t.block_begin = dupload(owned, h.block_begin, stream);
+            t.stage_offsets = dupload(owned, h.stage_offsets, stream);
+            t.ab = dupload(owned, h.ab, stream);
+            t.cd = k == 1 ? dupload(owned, h.cd, stream) : nullptr;
+            t.rest = dupload(owned, h.rest, stream);
+            t.comp = dupload(owned, h.comp, stream);
+            t.stages = h.stages;
+            t.max_count = h.max_block_count;
+            const uint32_t bytes = h.max_block_count * 4u;
+            t.smem_ab = off; off = align16(off + bytes);
+            if (k == 1) { t.smem_cd = off; off = align16(off + bytes); }
+            t.smem_rest = off; off = align16(off + bytes);
+            t.smem_comp = off; off = align16(off + bytes);
+            t.smem_lambda = off; off = align16(off + bytes);
+        }
+    p.smem_total = off;
+    for (int l = 1; l < sched.levels; ++l) {
+        p.patch_begin[l] = dupload(owned, sched.patch_begin[l], stream);
+        p.patch_slots[l] = dupload(owned, sched.patch_slots[l], stream);
+    }
+    for (int k = 0; k < kKinds; ++k) {
+        const GlobalTable& h = sched.global[k];
+        DevGlobal& g = p.glob[k];
+        g.colour_offsets = dupload(owned, h.colour_offsets, stream);
+        g.a = dupload(owned, h.a, stream);
+        g.b = dupload(owned, h.b, stream);
+        g.c = k == 1 ? dupload(owned, h.c, stream) : nullptr;
+        g.d = k == 1 ? dupload(owned, h.d, stream) : nullptr;
+        g.rest = dupload(owned, h.rest, stream);
+        g.comp = dupload(owned, h.comp, stream);
+        g.count = static_cast<uint32_t>(h.a.size());
+        g.lambda = dalloc<float>(owned, g.count);
+        g.colours = h.colour_offsets.empty() ? 0 : static_cast<int>(h.colour_offsets.size()) - 1;
+    }
+    p.iface_begin = dupload(owned, sched.iface_begin, stream);
+    p.iface_local = dupload(owned, sched.iface_local, stream);
+    p.seam_offsets = dupload(owned, sched.seam_stage_offsets, stream);
+    p.seam_stages = sched.seam_stage_offsets.empty() ? 0 : static_cast<int>(sched.seam_stage_offsets.size()) - 1;
+    p.seam_a = dupload(owned, sched.seam_a, stream);
+    p.seam_b = dupload(owned, sched.seam_b, stream);
+
+    // diagnostics arrays (definition order of distance-like constraints)
+    {
+        std::vector<uint32_t> a(def.constraints.size()), b(def.constraints.size());
+        std::vector<float> rest(def.constraints.size());
+        std::vector<uint8_t> kind(def.constraints.size());
+        for (size_t i = 0; i < def.constraints.size(); ++i) {
+            a[i] = sched.slot_of_node[def.constraints[i].first_node];
+            b[i] = sched.slot_of_node[def.constraints[i].second_node];
+            rest[i] = static_cast<float>(def.constraints[i].rest_length);
+            kind[i] = static_cast<uint8_t>(def.constraints[i].kind);
+        }
+        d_diag_a = dupload(owned, a, stream);
+        d_diag_b = dupload(owned, b, stream);
+        d_diag_rest = dupload(owned, rest, stream);
+        d_diag_kind = dupload(owned, kind, stream);
+        d_diag_partials = dalloc<double>(owned, static_cast<size_t>(kDiagBlocks) * kDiagFields);
+    }
+
+    // suspension
+    p.susp_block = -1;
+    DevPayloadDef pdef{};
+    DevPayloadState pstate{};
+    if (def.has_suspension) {
+        const swb_suspension_def& s = def.suspension;
+        p.susp_block = sched.suspension_block;
+        const uint32_t sbase = sched.l1_begin[sched.suspension_block];
+        pdef.mass = static_cast<float>(s.pilot_mass);
+        pdef.com_local = make_float3(s.pilot_com_local.x, s.pilot_com_local.y, s.pilot_com_local.z);
+        pdef.inertia = make_float3(s.pilot_principal_inertia.x, s.pilot_principal_inertia.y,
+                                   s.pilot_principal_inertia.z);
+        std::vector<size_t> horder(def.harness.size()), sorder(def.segments.size());
+        std::iota(horder.begin(), horder.end(), 0);
+        std::iota(sorder.begin(), sorder.end(), 0);
+        std::stable_sort(horder.begin(), horder.end(), [&](size_t x, size_t y) {
+            return id_string_less(def.harness[x].stable_id, def.harness[y].stable_id);
+        });
+        std::stable_sort(sorder.begin(), sorder.end(), [&](size_t x, size_t y) {
+            return id_string_less(def.segments[x].stable_id, def.segments[y].stable_id);
+        });
+        segment_order = sorder;
+        pdef.hang_points = static_cast<int>(horder.size());
+        for (size_t i = 0; i < horder.size(); ++i) {
+            const auto& h = def.harness[horder[i]].local_position;
+            pdef.hang_local[i] = make_float3(h.x, h.y, h.z);
+        }
+        pdef.segments = static_cast<int>(sorder.size());
+        for (size_t k = 0; k < sorder.size(); ++k) {
+            const swb_suspension_segment& g = def.segments[sorder[k]];
+            int node[2] = {-1, -1}, point[2] = {-1, -1};
+            const swb_suspension_endpoint* ends[2] = {&g.from, &g.to};
+            for (int e = 0; e < 2; ++e) {
+                if (ends[e]->kind == SWB_ENDPOINT_SURFACE_ATTACHMENT) {
+                    for (const auto& a : def.attachments)
+                        if (a.stable_id == ends[e]->stable_id)
+                            node[e] = static_cast<int>(sched.slot_of_node[a.node] - sbase);
+                } else if (ends[e]->kind == SWB_ENDPOINT_JUNCTION) {
+                    for (const auto& j : def.junctions)
+                        if (j.stable_id == ends[e]->stable_id)
+                            node[e] = static_cast<int>(sched.slot_of_node[j.node] - sbase);
+                } else if (ends[e]->kind == SWB_ENDPOINT_PILOT_HARNESS) {
+                    for (size_t i = 0; i < horder.size(); ++i)
+                        if (def.harness[horder[i]].stable_id == ends[e]->stable_id) point[e] = static_cast<int>(i);
+                } else {
+                    raise(SWB_INVALID_ARGUMENT, "Unknown structure suspension endpoint kind");
+                }
+                if (node[e] < 0 && point[e] < 0)
+                    raise(SWB_SUSPENSION_ERROR, "suspension segment endpoint does not resolve");
+            }
+            if (ends[0]->kind == SWB_ENDPOINT_PILOT_HARNESS || ends[1]->kind == SWB_ENDPOINT_SURFACE_ATTACHMENT)
+                raise(SWB_SUSPENSION_ERROR, "invalid directed endpoint kinds");
+            pdef.from_node[k] = node[0]; pdef.to_node[k] = node[1];
+            pdef.from_point[k] = point[0]; pdef.to_point[k] = point[1];
+            pdef.rest[k] = static_cast<float>(g.rest_length);
+            pdef.stiffness[k] = static_cast<float>(g.axial_stiffness);
+            pdef.damping[k] = static_cast<float>(g.axial_damping);
+        }
+        pdef.max_residual = static_cast<float>(s.maximum_line_residual);
+        pdef.min_length = static_cast<float>(s.minimum_line_length);
+        // canonical initial orientation (suspension.cpp:771)
+        const swb_quat& q0 = s.pilot_initial_body_to_world;
+        double n = std::sqrt(q0.w * q0.w + q0.x * q0.x + q0.y * q0.y + q0.z * q0.z);
+        double qw = q0.w / n, qx = q0.x / n, qy = q0.y / n, qz = q0.z / n;
+        if (qw < 0 || (qw == 0 && (qx < 0 || (qx == 0 && (qy < 0 || (qy == 0 && qz < 0)))))) {
+            qw = -qw; qx = -qx; qy = -qy; qz = -qz;
+        }
+        pstate.com = make_float3(s.pilot_initial_com_world.x, s.pilot_initial_com_world.y, s.pilot_initial_com_world.z);
+        pstate.q = make_float4(qw, qx, qy, qz);
+        pstate.v = make_float3(s.pilot_initial_linear_velocity.x, s.pilot_initial_linear_velocity.y,
+                               s.pilot_initial_linear_velocity.z);
+        pstate.w = make_float3(s.pilot_initial_angular_velocity.x, s.pilot_initial_angular_velocity.y,
+                               s.pilot_initial_angular_velocity.z);
+    }
+    payload_def_host = pdef;
+    d_payload_def = dupload(owned, std::vector<DevPayloadDef>{pdef}, stream);
+    for (int i = 0; i < 3; ++i) {
+        d_payload[i] = dupload(owned, std::vector<DevPayloadState>{pstate}, stream);
+        d_origin[i] = dupload(owned, std::vector<double>{0.0, 0.0, 0.0}, stream);
+    }
+    d_control = dalloc<Control>(owned, 1);
+    cuda_check(cudaMemsetAsync(d_control, 0, sizeof(Control), stream), "memset");
+    p.payload_def = d_payload_def;
+    p.recentre = def.has_suspension ? 1 : 0;
+    p.barrier.count = &d_control->count;
+    p.barrier.generation = &d_control->generation;
+    p.barrier.status = d_control->status;
+    p.barrier.blocks = static_cast<unsigned>(G);
+    p.status = d_control->status;
+    p.shift_out = &d_control->shift;
+    const long long budget = opt.sync_budget_cycles > 0 ? opt.sync_budget_cycles : 4000000000LL;
+    p.barrier.budget = budget;
+    p.copy_budget = budget;
+
+    // launch feasibility
+    cuda_check(cudaFuncSetAttribute(dev::xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(p.smem_total)),
+               "shared memory request (mesh patch too large for the block count)");
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::xpbd_step_kernel, threads, p.smem_total),
+               "occupancy");
+    if (per_sm * sm_count < G)
+        raise(SWB_UNSUPPORTED, "persistent grid of " + std::to_string(G) + " CTAs is not co-resident (" +
+                                   std::to_string(per_sm) + " per SM)");
+    cuda_check(cudaStreamSynchronize(stream), "upload");
+}
+
+void StructureImpl::upload_pressure() {
+    const uint64_t N = def.nodes.size();
+    std::vector<uint4> tri(def.triangles.size());
+    std::vector<uint32_t> off(N + 1, 0), list;
+    for (size_t t = 0; t < def.triangles.size(); ++t) {
+        const auto& tr = def.triangles[t];
+        const float pr = static_cast<float>(pressure[t]);
+        tri[t] = make_uint4(sched.slot_of_node[tr.nodes[0]], sched.slot_of_node[tr.nodes[1]],
+                            sched.slot_of_node[tr.nodes[2]], std::bit_cast<uint32_t>(pr));
+        if (pressure[t] == 0.0) continue;
+        for (int k = 0; k < 3; ++k) ++off[sched.slot_of_node[tr.nodes[k]] + 1];
+    }
+    for (uint64_t s = 0; s < N; ++s) off[s + 1] += off[s];
+    list.resize(off[N]);
+    std::vector<uint32_t> cur(off.begin(), off.end() - 1);
+    for (size_t t = 0; t < def.triangles.size(); ++t) {
+        if (pressure[t] == 0.0) continue;
+        for (int k = 0; k < 3; ++k) list[cur[sched.slot_of_node[def.triangles[t].nodes[k]]]++] = static_cast<uint32_t>(t);
+    }
+    if (d_tri) { cudaFree(d_tri); cudaFree(d_tri_off); cudaFree(d_tri_list); owned.erase(std::remove_if(owned.begin(), owned.end(), [&](void* q) { return q == d_tri || q == d_tri_off || q == d_tri_list; }), owned.end()); }
+    d_tri = dupload(owned, tri, stream);
+    d_tri_off = dupload(owned, off, stream);
+    d_tri_list = dupload(owned, list, stream);
+    params.tri = d_tri;
+    params.tri_offsets = d_tri_off;
+    params.tri_list = d_tri_list;
+    pressure_dirty = false;
+}
+
+void StructureImpl::upload_forces() {
+    const uint64_t N = def.nodes.size();
+    for (uint64_t n = 0; n < N; ++n) {
+        const swb_vec3& f = pending[n];
+        h_force[sched.slot_of_node[n]] =
+            make_float4(static_cast<float>(f.x), static_cast<float>(f.y), static_cast<float>(f.z), 0.0f);
+    }
+    cuda_check(cudaMemcpyAsync(d_force, h_force, N * sizeof(float4), cudaMemcpyHostToDevice, stream), "force upload");
+    forces_dirty = false;
+}
+
+void StructureImpl::validate_settings(const swb_step_settings& st) const {
+    auto fin = [](const swb_vec3& v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
+    // SoftBody::step / stepCoupled (soft_body.cpp:982-1003, 1024-1050)
+    if (!(st.time_step > 0.0) || !std::isfinite(st.time_step) || st.substeps <= 0 || st.constraint_iterations < 0 ||
+        st.cable_sweep_pairs < 0 || st.velocity_damping < 0.0 || !std::isfinite(st.velocity_damping) ||
+        !fin(st.gravity) || !fin(st.damping_reference_velocity) ||
+        (def.has_suspension && st.constraint_iterations == 0))
+        raise(SWB_INVALID_ARGUMENT, def.has_suspension ? "Invalid coupled SoftBody step settings"
+                                                        : "Invalid SoftBody step settings");
+    if (def.has_suspension && st.constraint_iterations != def.suspension.solver_iterations)
+        raise(SWB_INVALID_ARGUMENT,
+              "Coupled structural iterations must equal the registered suspension lineIterations contract");
+    if (st.cable_sweep_pairs != 0)
+        raise(SWB_UNSUPPORTED, "load-path cable sweep pairs are not available in this build");
+}
+
+void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out) {
+    StepParams p = params;
+    const double dt = st.time_step / st.substeps;
+    p.pos_in = d_pos[in]; p.vel_in = d_vel[in];
+    p.pos_out = d_pos[out]; p.vel_out = d_vel[out]; p.prev_out = d_prev[out];
+    p.force = d_force;
+    p.payload_in = d_payload[in]; p.payload_out = d_payload[out];
+    p.origin_in = d_origin[in]; p.origin_out = d_origin[out];
+    p.dt = static_cast<float>(dt);
+    p.inv_dt = static_cast<float>(1.0 / dt);
+    p.inv_dt2 = static_cast<float>(1.0 / (dt * dt));
+    p.damping = static_cast<float>(std::exp(-st.velocity_damping * dt));
+    p.gravity = make_float3(st.gravity.x, st.gravity.y, st.gravity.z);
+    p.ref_velocity = make_float3(st.damping_reference_velocity.x, st.damping_reference_velocity.y,
+                                 st.damping_reference_velocity.z);
+    p.iterations = st.constraint_iterations;
+    cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
+    void* args[] = {&p};
+    cuda_check(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dev::xpbd_step_kernel), dim3(G), dim3(threads),
+                                           args, p.smem_total, stream),
+               "cudaLaunchCooperativeKernel");
+}
+
+swb_status StructureImpl::read_status(std::string& message) {
+    Control c{};
+    cuda_check(cudaMemcpyAsync(&c, d_control, sizeof(Control), cudaMemcpyDeviceToHost, stream), "status");
+    cuda_check(cudaStreamSynchronize(stream), "step");
+    if (c.status[0] == 0) return SWB_OK;
+    if (c.status[0] & dev::kStatusSyncTimeout) {
+        message = "device-wide barrier timed out";
+        return SWB_SYNC_TIMEOUT;
+    }
+    if (c.status[0] & dev::kStatusCopyTimeout) {
+        message = "shared-memory staging timed out";
+        return SWB_SYNC_TIMEOUT;
+    }
+    if (c.status[0] & dev::kStatusSuspension) {
+        static const char* what[] = {"suspension failure", "line geometry is non-finite or scale-degenerate",
+                                     "invalid unilateral line projection input", "zero generalized effective mass",
+                                     "payload trial state is non-finite or unnormalized",
+                                     "maximum line residual exceeds configured bound", "invalid payload orientation"};
+        message = std::string("SuspensionError: ") + what[std::clamp(c.status[1], 0, 6)];
+        return SWB_SUSPENSION_ERROR;
+    }
+    message = "trial step produced a non-finite state";
+    return SWB_NON_FINITE;
+}
+
+swb_status StructureImpl::step(const swb_step_settings& st, int steps, swb_diagnostics* out) {
+    validate_settings(st);
+    if (steps < 1) raise(SWB_INVALID_ARGUMENT, "steps must be positive");
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    if (pressure_dirty) upload_pressure();
+    if (forces_dirty) upload_forces();
+    const int start = cur;
+    const int total = steps * st.substeps;
+    // Transaction: substeps ping-pong between buffers `start` and `other`;
+    // with more than one substep the committed state is first copied to the
+    // third buffer so a failure can restore it.
+    int backup = -1;
+    int a = start, b = (start + 1) % 3;
+    if (b == start) b = (start + 2) % 3;
+    if (total > 1) {
+        backup = 3 - a - b;
+        copy_state(a, backup);
+    }
+    cuda_check(cudaEventRecord(ev0, stream), "event");
+    for (int k = 0; k < total; ++k) {
+        launch_substep(st, a, b);
+        std::swap(a, b);
+    }
+    cuda_check(cudaEventRecord(ev1, stream), "event");
+    std::string message;
+    const swb_status status = read_status(message);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    last_ms = ms;
+    if (status != SWB_OK) {
+        if (backup >= 0) {
+            copy_state(backup, start);
+            cuda_check(cudaStreamSynchronize(stream), "restore");
+        }
+        cur = start;
+        raise(status, message);
+    }
+    cur = a;
+    swb_vec3 applied{0, 0, 0};
+    for (auto& f : pending) {
+        applied.x += f.x; applied.y += f.y; applied.z += f.z;
+        if (f.x != 0.0 || f.y != 0.0 || f.z != 0.0) forces_dirty = true;
+        f = swb_vec3{0, 0, 0};
+    }
+    last_applied = applied;
+    accepted += static_cast<uint64_t>(steps);
+    time += st.time_step * steps;
+    last_dt = st.time_step / st.substeps;
+    if (out) diagnostics(out);
+    return SWB_OK;
+}
+
+void StructureImpl::copy_state(int from, int to) {
+    const size_t N = def.nodes.size();
+    cuda_check(cudaMemcpyAsync(d_pos[to], d_pos[from], N * sizeof(float4), cudaMemcpyDeviceToDevice, stream), "copy");
+    cuda_check(cudaMemcpyAsync(d_vel[to], d_vel[from], N * sizeof(float4), cudaMemcpyDeviceToDevice, stream), "copy");
+    cuda_check(cudaMemcpyAsync(d_prev[to], d_prev[from], N * sizeof(float4), cudaMemcpyDeviceToDevice, stream), "copy");
+    cuda_check(cudaMemcpyAsync(d_payload[to], d_payload[from], sizeof(DevPayloadState), cudaMemcpyDeviceToDevice,
+                               stream), "copy");
+    cuda_check(cudaMemcpyAsync(d_origin[to], d_origin[from], 3 * sizeof(double), cudaMemcpyDeviceToDevice, stream),
+               "copy");
+}
+
+void StructureImpl::fetch(std::vector<float4>& pos, std::vector<float4>& prev, std::vector<float4>& vel,
+                          DevPayloadState& pay, double origin[3]) const {
+    const size_t N = def.nodes.size();
+    pos.resize(N); prev.resize(N); vel.resize(N);
+    cuda_check(cudaMemcpyAsync(pos.data(), d_pos[cur], N * sizeof(float4), cudaMemcpyDeviceToHost, stream), "read");
+    cuda_check(cudaMemcpyAsync(prev.data(), d_prev[cur], N * sizeof(float4), cudaMemcpyDeviceToHost, stream), "read");
+    cuda_check(cudaMemcpyAsync(vel.data(), d_vel[cur], N * sizeof(float4), cudaMemcpyDeviceToHost, stream), "read");
+    cuda_check(cudaMemcpyAsync(&pay, d_payload[cur], sizeof(pay), cudaMemcpyDeviceToHost, stream), "read");
+    cuda_check(cudaMemcpyAsync(origin, d_origin[cur], 3 * sizeof(double), cudaMemcpyDeviceToHost, stream), "read");
+    cuda_check(cudaStreamSynchronize(stream), "read");
+}
+
+void StructureImpl::diagnostics(swb_diagnostics* o) const {
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    const uint32_t N = static_cast<uint32_t>(def.nodes.size());
+    const uint32_t M = static_cast<uint32_t>(def.constraints.size());
+    diagnostics_kernel<<<kDiagBlocks, 256, 0, stream>>>(d_pos[cur], d_prev[cur], d_vel[cur], N, d_diag_a, d_diag_b,
+                                                         d_diag_rest, d_diag_kind, M, d_diag_partials);
+    cuda_check(cudaGetLastError(), "diagnostics");
+    std::vector<double> part(static_cast<size_t>(kDiagBlocks) * kDiagFields);
+    DevPayloadState pay{};
+    double origin[3];
+    cuda_check(cudaMemcpyAsync(part.data(), d_diag_partials, part.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                               stream), "read");
+    cuda_check(cudaMemcpyAsync(&pay, d_payload[cur], sizeof(pay), cudaMemcpyDeviceToHost, stream), "read");
+    cuda_check(cudaMemcpyAsync(origin, d_origin[cur], sizeof(origin), cudaMemcpyDeviceToHost, stream), "read");
+    cuda_check(cudaStreamSynchronize(stream), "diagnostics");
+    double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0};
+    for (int b = 0; b < kDiagBlocks; ++b) {
+        const double* q = &part[static_cast<size_t>(b) * kDiagFields];
+        for (int f = 0; f < 9; ++f) acc[f] += q[f];
+        acc[9] = std::min(acc[9], q[9]);
+        acc[10] = std::max(acc[10], q[10]);
+        acc[11] = std::max(acc[11], q[11]);
+    }
+    std::memset(o, 0, sizeof(*o));
+    o->node_count = N;
+    o->dynamic_node_count = static_cast<uint64_t>(acc[0]);
+    o->triangle_count = def.triangles.size();
+    o->constraint_count = def.constraints.size();
+    o->membrane_count = def.membranes.size();
+    o->dihedral_count = def.dihedrals.size();
+    double mass = acc[1];
+    double wx = acc[2] + acc[1] * origin[0], wy = acc[3] + acc[1] * origin[1], wz = acc[4] + acc[1] * origin[2];
+    double px = acc[5], py = acc[6], pz = acc[7], ke = acc[8];
+    bool finite = acc[9] > 0.5;
+    if (mass > 0.0) o->center_of_mass = {wx / mass, wy / mass, wz / mass};
+    if (def.has_suspension) {
+        const double m = def.suspension.pilot_mass;
+        const double cx = pay.com.x + origin[0], cy = pay.com.y + origin[1], cz = pay.com.z + origin[2];
+        wx += cx * m; wy += cy * m; wz += cz * m;
+        mass += m;
+        o->center_of_mass = {wx / mass, wy / mass, wz / mass};
+        px += m * pay.v.x; py += m * pay.v.y; pz += m * pay.v.z;
+        // 0.5 m |v|^2 + 0.5 w . (I_world w)
+        const double qw = pay.q.x, qx = pay.q.y, qy = pay.q.z, qz = pay.q.w;
+        const double R[9] = {1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy),
+                             2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx),
+                             2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)};
+        const double I[3] = {def.suspension.pilot_principal_inertia.x, def.suspension.pilot_principal_inertia.y,
+                             def.suspension.pilot_principal_inertia.z};
+        const double w[3] = {pay.w.x, pay.w.y, pay.w.z};
+        double Rtw[3] = {0, 0, 0};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) Rtw[i] += R[j * 3 + i] * w[j];
+        double rot = 0.0;
+        for (int i = 0; i < 3; ++i) rot += I[i] * Rtw[i] * Rtw[i];
+        ke += 0.5 * m * (double(pay.v.x) * pay.v.x + double(pay.v.y) * pay.v.y + double(pay.v.z) * pay.v.z) +
+              0.5 * rot;
+        o->suspension_segment_count = def.segments.size();
+        o->maximum_suspension_residual = pay.max_residual;
+        finite = finite && std::isfinite(cx) && std::isfinite(cy) && std::isfinite(cz) && std::isfinite(ke);
+    }
+    o->total_dynamic_mass = mass;
+    o->linear_momentum = {px, py, pz};
+    o->kinetic_energy = ke;
+    o->maximum_distance_error = acc[10];
+    o->maximum_cable_extension = acc[11];
+    swb_vec3 pend{0, 0, 0};
+    for (const auto& f : pending) {
+        pend.x += f.x; pend.y += f.y; pend.z += f.z;
+        finite = finite && std::isfinite(f.x) && std::isfinite(f.y) && std::isfinite(f.z);
+    }
+    o->pending_external_force = pend;
+    o->last_applied_external_force = last_applied;
+    o->finite = finite && std::isfinite(acc[10]) && std::isfinite(acc[11]) ? 1u : 0u;
+}
+
+}  // namespace swb
+
+using namespace swb;
+
+extern "C" {
+
+void swb_default_solver_options(swb_solver_options* out) {
+    std::memset(out, 0, sizeof(*out));
+}
+
+swb_status swb_structure_create(const swb_structure_definition* definition, const swb_solver_options* options,
+                                swb_structure** out) {
+    return guarded([&] {
+        if (!definition || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
+        auto impl = std::make_unique<swb_structure>();
+        impl->s.build(*definition, options);
+        *out = impl.release();
+    });
+}
+
+void swb_structure_destroy(swb_structure* s) { delete s; }
+
+uint64_t swb_structure_fingerprint(const swb_structure* s) { return s ? s->s.fingerprint : 0; }
+uint64_t swb_structure_accepted_steps(const swb_structure* s) { return s ? s->s.accepted : 0; }
+double swb_structure_simulation_time(const swb_structure* s) { return s ? s->s.time : 0.0; }
+uint64_t swb_structure_node_count(const swb_structure* s) { return s ? s->s.def.nodes.size() : 0; }
+double swb_structure_last_step_ms(const swb_structure* s) { return s ? s->s.last_ms : 0.0; }
+
+swb_status swb_structure_clear_external_forces(swb_structure* s) {
+    return guarded([&] {
+        if (!s) raise(SWB_INVALID_ARGUMENT, "null structure");
+        for (auto& f : s->s.pending) f = swb_vec3{0, 0, 0};
+        s->s.forces_dirty = true;
+    });
+}
+
+swb_status swb_structure_add_external_force(swb_structure* s, uint64_t node, const swb_vec3* force) {
+    return guarded([&] {
+        if (!s || !force) raise(SWB_INVALID_ARGUMENT, "null argument");
+        if (node >= s->s.pending.size()) raise(SWB_OUT_OF_RANGE, "Structure force node is out of range");
+        if (!std::isfinite(force->x) || !std::isfinite(force->y) || !std::isfinite(force->z))
+            raise(SWB_INVALID_ARGUMENT, "Structure force must be finite");
+        s->s.pending[node].x += force->x;
+        s->s.pending[node].y += force->y;
+        s->s.pending[node].z += force->z;
+        s->s.forces_dirty = true;
+    });
+}
+
+swb_status swb_structure_set_external_forces(swb_structure* s, const swb_vec3* forces, uint64_t count) {
+    return guarded([&] {
+        if (!s) raise(SWB_INVALID_ARGUMENT, "null structure");
+        if (count != s->s.pending.size()) raise(SWB_INVALID_ARGUMENT, "Structure force count must equal the node count");
+        if (count && !forces) raise(SWB_INVALID_ARGUMENT, "null forces");
+        for (uint64_t i = 0; i < count; ++i)
+            if (!std::isfinite(forces[i].x) || !std::isfinite(forces[i].y) || !std::isfinite(forces[i].z))
+                raise(SWB_INVALID_ARGUMENT, "Structure forces must be finite");
+        std::copy(forces, forces + count, s->s.pending.begin());
+        s->s.forces_dirty = true;
+    });
+}
+
+swb_status swb_structure_set_face_pressure(swb_structure* s, uint64_t triangle, double dp) {
+    return guarded([&] {
+        if (!s) raise(SWB_INVALID_ARGUMENT, "null structure");
+        if (triangle >= s->s.pressure.size()) raise(SWB_OUT_OF_RANGE, "Triangle index is out of range");
+        if (!std::isfinite(dp)) raise(SWB_INVALID_ARGUMENT, "Pressure difference must be finite");
+        s->s.pressure[triangle] = dp;
+        s->s.pressure_dirty = true;
+    });
+}
+
+swb_status swb_structure_set_uniform_pressure(swb_structure* s, double dp) {
+    return guarded([&] {
+        if (!s) raise(SWB_INVALID_ARGUMENT, "null structure");
+        if (!std::isfinite(dp)) raise(SWB_INVALID_ARGUMENT, "Pressure difference must be finite");
+        for (auto& p : s->s.pressure) p = dp;
+        s->s.pressure_dirty = true;
+    });
+}
+
+swb_status swb_structure_step(swb_structure* s, const swb_step_settings* settings, swb_diagnostics* out) {
+    return guarded([&] {
+        if (!s || !settings) raise(SWB_INVALID_ARGUMENT, "null argument");
+        s->s.step(*settings, 1, out);
+    });
+}
+
+swb_status swb_structure_step_many(swb_structure* s, const swb_step_settings* settings, int32_t steps,
+                                   swb_diagnostics* out) {
+    return guarded([&] {
+        if (!s || !settings) raise(SWB_INVALID_ARGUMENT, "null argument");
+        s->s.step(*settings, steps, out);
+    });
+}
+
+swb_status swb_structure_diagnostics(const swb_structure* s, swb_diagnostics* out) {
+    return guarded([&] {
+        if (!s || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
+        s->s.diagnostics(out);
+    });
+}
+
+swb_status swb_structure_read_nodes(const swb_structure* s, swb_node_state* out, uint64_t count) {
+    return guarded([&] {
+        if (!s || (!out && count)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        if (count != s->s.def.nodes.size()) raise(SWB_INVALID_ARGUMENT, "node count mismatch");
+        std::vector<float4> pos, prev, vel;
+        DevPayloadState pay;
+        double o[3];
+        s->s.fetch(pos, prev, vel, pay, o);
+        for (uint64_t n = 0; n < count; ++n) {
+            const uint32_t sl = s->s.sched.slot_of_node[n];
+            out[n].position = {pos[sl].x + o[0], pos[sl].y + o[1], pos[sl].z + o[2]};
+            out[n].previous_position = {prev[sl].x + o[0], prev[sl].y + o[1], prev[sl].z + o[2]};
+            out[n].velocity = {vel[sl].x, vel[sl].y, vel[sl].z};
+        }
+    });
+}
+
+swb_status swb_structure_read_positions_f32(const swb_structure* s, float* out, uint64_t count) {
+    return guarded([&] {
+        if (!s || (!out && count)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        if (count != s->s.def.nodes.size()) raise(SWB_INVALID_ARGUMENT, "node count mismatch");
+        std::vector<float4> pos, prev, vel;
+        DevPayloadState pay;
+        double o[3];
+        s->s.fetch(pos, prev, vel, pay, o);
+        for (uint64_t n = 0; n < count; ++n) {
+            const uint32_t sl = s->s.sched.slot_of_node[n];
+            out[3 * n + 0] = static_cast<float>(pos[sl].x + o[0]);
+            out[3 * n + 1] = static_cast<float>(pos[sl].y + o[1]);
+            out[3 * n + 2] = static_cast<float>(pos[sl].z + o[2]);
+        }
+    });
+}
+
+swb_status swb_structure_write_nodes(swb_structure* s, const swb_node_state* in, uint64_t count) {
+    return guarded([&] {
+        if (!s || (!in && count)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        StructureImpl& m = s->s;
+        if (count != m.def.nodes.size()) raise(SWB_INVALID_ARGUMENT, "node count mismatch");
+        std::vector<float4> pos, prev, vel;
+        DevPayloadState pay;
+        double o[3];
+        m.fetch(pos, prev, vel, pay, o);
+        for (uint64_t n = 0; n < count; ++n) {
+            const auto& st = in[n];
+            if (!std::isfinite(st.position.x) || !std::isfinite(st.position.y) || !std::isfinite(st.position.z) ||
+                !std::isfinite(st.velocity.x) || !std::isfinite(st.velocity.y) || !std::isfinite(st.velocity.z) ||
+                !std::isfinite(st.previous_position.x) || !std::isfinite(st.previous_position.y) ||
+                !std::isfinite(st.previous_position.z))
+                raise(SWB_INVALID_ARGUMENT, "node state must be finite");
+            const uint32_t sl = m.sched.slot_of_node[n];
+            const float w = m.inv_mass[sl];
+            pos[sl] = make_float4(st.position.x - o[0], st.position.y - o[1], st.position.z - o[2], w);
+            prev[sl] = make_float4(st.previous_position.x - o[0], st.previous_position.y - o[1],
+                                   st.previous_position.z - o[2], w);
+            vel[sl] = make_float4(st.velocity.x, st.velocity.y, st.velocity.z, 0.0f);
+        }
+        const size_t N = m.def.nodes.size();
+        cuda_check(cudaMemcpyAsync(m.d_pos[m.cur], pos.data(), N * sizeof(float4), cudaMemcpyHostToDevice, m.stream), "write");
+        cuda_check(cudaMemcpyAsync(m.d_prev[m.cur], prev.data(), N * sizeof(float4), cudaMemcpyHostToDevice, m.stream), "write");
+        cuda_check(cudaMemcpyAsync(m.d_vel[m.cur], vel.data(), N * sizeof(float4), cudaMemcpyHostToDevice, m.stream), "write");
+        cuda_check(cudaStreamSynchronize(m.stream), "write");
+    });
+}
+
+swb_status swb_structure_read_suspension(const swb_structure* s, swb_payload_state* payload,
+                                         swb_segment_state* segments, uint64_t capacity, swb_wrench* wrench) {
+    return guarded([&] {
+        if (!s) raise(SWB_INVALID_ARGUMENT, "null structure");
+        const StructureImpl& m = s->s;
+        if (!m.def.has_suspension) raise(SWB_INVALID_ARGUMENT, "structure has no suspension");
+        std::vector<float4> pos, prev, vel;
+        DevPayloadState pay;
+        double o[3];
+        m.fetch(pos, prev, vel, pay, o);
+        if (payload) {
+            payload->center_of_mass = {pay.com.x + o[0], pay.com.y + o[1], pay.com.z + o[2]};
+            payload->body_to_world = {pay.q.x, pay.q.y, pay.q.z, pay.q.w};
+            payload->linear_velocity = {pay.v.x, pay.v.y, pay.v.z};
+            payload->angular_velocity = {pay.w.x, pay.w.y, pay.w.z};
+        }
+        if (wrench) {
+            wrench->force = {pay.line_force.x, pay.line_force.y, pay.line_force.z};
+            wrench->moment = {pay.line_moment.x, pay.line_moment.y, pay.line_moment.z};
+        }
+        // segment states in definition order (Structure::suspensionState)
+        const uint64_t nseg = m.def.segments.size();
+        for (uint64_t k = 0; segments && k < nseg && k < capacity; ++k) {
+            // device index of definition segment k
+            size_t dk = 0;
+            for (size_t q = 0; q < m.segment_order.size(); ++q)
+                if (m.segment_order[q] == k) dk = q;
+            const DevPayloadDef& d = m.payload_def_host;
+            auto endpoint = [&](int node, int point) {
+                double r[3];
+                if (node >= 0) {
+                    const float4 X = pos[m.sched.l1_begin[m.sched.suspension_block] + node];
+                    r[0] = X.x; r[1] = X.y; r[2] = X.z;
+                } else {
+                    const double qw = pay.q.x, qx = pay.q.y, qy = pay.q.z, qz = pay.q.w;
+                    const double R[9] = {1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy),
+                                         2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx),
+                                         2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)};
+                    const double l[3] = {d.hang_local[point].x - d.com_local.x, d.hang_local[point].y - d.com_local.y,
+                                         d.hang_local[point].z - d.com_local.z};
+                    const double c[3] = {pay.com.x, pay.com.y, pay.com.z};
+                    for (int i = 0; i < 3; ++i) r[i] = c[i] + R[i * 3] * l[0] + R[i * 3 + 1] * l[1] + R[i * 3 + 2] * l[2];
+                }
+                return std::array<double, 3>{r[0], r[1], r[2]};
+            };
+            const auto a = endpoint(d.from_node[dk], d.from_point[dk]);
+            const auto b = endpoint(d.to_node[dk], d.to_point[dk]);
+            const double len = std::sqrt((b[0] - a[0]) * (b[0] - a[0]) + (b[1] - a[1]) * (b[1] - a[1]) +
+                                         (b[2] - a[2]) * (b[2] - a[2]));
+            segments[k].stable_id = m.def.segments[k].stable_id;
+            segments[k].current_length = m.accepted ? len : m.def.segments[k].rest_length;
+            segments[k].commanded_rest_length = m.def.segments[k].rest_length;
+            segments[k].tension = m.accepted ? pay.lambda[dk] / (m.last_dt * m.last_dt) : 0.0;
+        }
+    });
+}
+
+swb_status swb_structure_write_payload(swb_structure* s, const swb_payload_state* in) {
+    return guarded([&] {
+        if (!s || !in) raise(SWB_INVALID_ARGUMENT, "null argument");
+        StructureImpl& m = s->s;
+        if (!m.def.has_suspension) raise(SWB_INVALID_ARGUMENT, "structure has no suspension");
+        std::vector<float4> pos, prev, vel;
+        DevPayloadState pay;
+        double o[3];
+        m.fetch(pos, prev, vel, pay, o);
+        pay.com = make_float3(in->center_of_mass.x - o[0], in->center_of_mass.y - o[1], in->center_of_mass.z - o[2]);
+        pay.q = make_float4(in->body_to_world.w, in->body_to_world.x, in->body_to_world.y, in->body_to_world.z);
+        pay.v = make_float3(in->linear_velocity.x, in->linear_velocity.y, in->linear_velocity.z);
+        pay.w = make_float3(in->angular_velocity.x, in->angular_velocity.y, in->angular_velocity.z);
+        cuda_check(cudaMemcpyAsync(m.d_payload[m.cur], &pay, sizeof(pay), cudaMemcpyHostToDevice, m.stream), "write");
+        cuda_check(cudaStreamSynchronize(m.stream), "write");
+    });
+}
+
+swb_status swb_structure_sweep_order(const swb_structure* s, uint32_t which, uint64_t* order, uint64_t count) {
+    return guarded([&] {
+        if (!s || (!order && count)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        const auto& v = which == SWB_SWEEP_DISTANCE ? s->s.sched.distance_order : s->s.sched.dihedral_order;
+        if (which > SWB_SWEEP_DIHEDRAL) raise(SWB_INVALID_ARGUMENT, "unknown sweep");
+        if (count != v.size()) raise(SWB_INVALID_ARGUMENT, "order count mismatch");
+        std::copy(v.begin(), v.end(), order);
+    });
+}
+
+swb_status swb_structure_schedule_report(const swb_structure* s, swb_schedule_report* out) {
+    return guarded([&] {
+        if (!s || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
+        const StructureImpl& m = s->s;
+        const Schedule& S = m.sched;
+        std::memset(out, 0, sizeof(*out));
+        out->blocks = m.G;
+        out->block_threads = m.threads;
+        out->partition_levels = S.levels;
+        int phases = 0, stages = 0;
+        for (int k = 0; k < kKinds; ++k) {
+            bool outer = S.global[k].colour_offsets.size() > 1;
+            for (int l = 0; l < S.levels; ++l) {
+                stages += S.tables[l][k].stages;
+                if (l > 0 && S.tables[l][k].stages > 0) { outer = true; ++phases; }
+            }
+            const int gc = S.global[k].colour_offsets.empty() ? 0 : static_cast<int>(S.global[k].colour_offsets.size()) - 1;
+            out->global_colours_per_iteration += gc;
+            phases += gc + (outer ? 1 : 0);
+        }
+        out->device_phases_per_iteration = phases;
+        out->local_stages_per_iteration = stages;
+        out->max_patch_nodes = S.max_patch_nodes;
+        out->shared_bytes = static_cast<int32_t>(m.params.smem_total);
+        for (int l = 0; l < 4; ++l) out->level_constraints[l] = S.level_constraints[l];
+        out->global_constraints = S.global_constraints;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// Host-side state of one device structure (the swb_structure handle).
+#pragma once
+
+#include "common.h"
+#include "schedule.h"
+#include "step_params.h"
+
+#include <string>
+#include <vector>
+
+namespace swb {
+
+void cuda_check(cudaError_t e, const char* what);
+
+// Device control word block: status[0] = kStatus* bits, status[1] = detail,
+// barrier counters and the re-centring shift of the last substep.
+struct Control {
+    int status[2];
+    unsigned int count;
+    unsigned int generation;
+    float3 shift;
+    float pad;
+};
+
+constexpr int kDiagBlocks = 148;
+
+struct StructureImpl {
+    OwnedDefinition def;
+    Schedule sched;
+    uint64_t fingerprint = 0;
+    int device = -1;
+    int sm_count = 0;
+    int G = 0;
+    int threads = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<void*> owned;
+    // state buffers (three so that a multi-substep step can be rolled back)
+    float4* d_pos[3] = {};
+    float4* d_vel[3] = {};
+    float4* d_prev[3] = {};
+    DevPayloadState* d_payload[3] = {};
+    double* d_origin[3] = {};
+    int cur = 0;
+    std::vector<float> inv_mass;  // by slot
+    float4* d_force = nullptr;
+    float4* h_force = nullptr;    // pinned staging
+    uint4* d_tri = nullptr;
+    uint32_t* d_tri_off = nullptr;
+    uint32_t* d_tri_list = nullptr;
+    uint32_t* d_diag_a = nullptr;
+    uint32_t* d_diag_b = nullptr;
+    float* d_diag_rest = nullptr;
+    uint8_t* d_diag_kind = nullptr;
+    double* d_diag_partials = nullptr;
+    DevPayloadDef* d_payload_def = nullptr;
+    DevPayloadDef payload_def_host{};
+    std::vector<size_t> segment_order;  // device segment k -> definition index
+    Control* d_control = nullptr;
+    StepParams params{};
+    uint32_t sched_n1_max = 0, sched_n2_max = 0;
+    // host mirror of the adapter state
+    std::vector<swb_vec3> pending;
+    std::vector<double> pressure;
+    bool forces_dirty = false;
+    bool pressure_dirty = false;
+    swb_vec3 last_applied{0, 0, 0};
+    uint64_t accepted = 0;
+    double time = 0.0;
+    double last_dt = 1.0 / 120.0;
+    double last_ms = 0.0;
+
+    ~StructureImpl();
+    void build(const swb_structure_definition& definition, const swb_solver_options* options);
+    void upload_pressure();
+    void upload_forces();
+    void validate_settings(const swb_step_settings& st) const;
+    void launch_substep(const swb_step_settings& st, int in, int out);
+    swb_status read_status(std::string& message);
+    swb_status step(const swb_step_settings& st, int steps, swb_diagnostics* out);
+    void copy_state(int from, int to);
+    void fetch(std::vector<float4>& pos, std::vector<float4>& prev, std::vector<float4>& vel, DevPayloadState& pay,
+               double origin[3]) const;
+    void diagnostics(swb_diagnostics* out) const;
+};
+
+}  // namespace swb
+
+struct swb_structure {
+    swb::StructureImpl s;
+};
