@@ -1,0 +1,322 @@
+"""Benchmark: wing steps/s of the plain XPBD structure step on one B200.
+
+Workload (per rank): the synthetic ram-air wing -- 40 cells, 60 chordwise,
+about 67k triangles, about 39k nodes, 121k distance-like constraints, 99k
+dihedrals, 2 risers to a 90 kg rigid pilot -- stepped at dt = 1/120 s with
+1 substep and 48 constraint iterations, 30 Pa outward pressure and gravity.
+One step = one `swb_structure_step`.  Inputs are synthetic (seeded
+generator); the reference's wing meshes are not shipped.
+
+  value   device steps/s: CUDA events on the solver stream around each step
+          (state resident in device memory), L2 flushed before every timed
+          step with a 256 MiB write;
+  e2e     the same through the public C-ABI with host buffers: every step
+          uploads that step's external forces from host memory
+          (swb_structure_set_external_forces) and reads the step's
+          diagnostics back (swb_structure_step with a diagnostics output);
+  roofline  algorithmic bytes per step (the per-visit byte model in
+          DESIGN.md) over the device time per step, against the measured
+          HBM copy bandwidth;
+  cpu_baseline  the reference Structure::step (oracle/_ref, serial) on a
+          bounded sample of the same workload, timed on this host.
+
+`--impl reference` times the reference CPU solver alone (all physical
+cores through its own worker pool) and prints its line.
+Multi-GPU: replicas only -- each rank steps its own wing; value is the sum
+of steps/s over ranks (max time over ranks).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "wing steps/s (70k tri, 48 it) plain vs batched; adjoint/forward time ratio"
+UNIT = "wing-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--e2e-steps", type=int, default=100)
+    p.add_argument("--cpu-sample-steps", type=int, default=12)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def wing_config():
+    return {"workload": "plain ram-air wing, 40 cells x 60 chordwise (67,428 tri), 48 iterations, 1 substep, "
+                        "dt 1/120 s, 30 Pa + gravity, rigid pilot on 2 risers",
+            "cells": 40, "chordwise": 60, "iterations": 48, "substeps": 1,
+            "l2": "flushed before every timed step (256 MiB write)"}
+
+
+def settings(sw):
+    return sw.StepSettings(time_step=1.0 / 120.0, substeps=1, constraint_iterations=48, gravity=(0.0, 0.0, -9.81),
+                           velocity_damping=0.25)
+
+
+def algorithmic_bytes(definition, iterations=48, substeps=1):
+    """Per step: S*[144 N + 52 T + I*(88 E_d + 160 E_b + 236 E_m + 52 E_s) + 4 (E_d + E_b) + 12 E_m]."""
+    v = definition.view
+    n, t = v.node_count, v.triangle_count
+    e_d, e_b, e_m = v.constraint_count, v.dihedral_count, v.membrane_count
+    e_s = v.suspension.contents.segment_count if v.suspension else 0
+    return substeps * (144 * n + 52 * t + iterations * (88 * e_d + 160 * e_b + 236 * e_m + 52 * e_s)
+                       + 4 * (e_d + e_b) + 12 * e_m)
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "xpbd_step_kernel_wing70k.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device_index):
+        self.device = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_run(definition, steps, threads):
+    """Reference Structure::step on this host (oracle/_ref when built,
+    otherwise the C restatement)."""
+    from oracle import oracle as O
+    import simwing_b200 as sw
+
+    st = settings(sw)
+    st.worker_threads = threads
+    if O.ref_available():
+        ref = O.RefStructure(definition)
+        kind = "reference"
+    else:
+        ref = O.PortStructure(definition)
+        kind = "port"
+        threads = 1
+    ref.step(st)  # warm caches
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ref.step(st)
+    dt = time.perf_counter() - t0
+    return steps / dt, kind, threads
+
+
+def physical_cores():
+    from oracle import oracle as O
+
+    if O.ref_available():
+        return int(O.ref_library().swref_physical_cores())
+    return os.cpu_count() or 1
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import simwing_b200 as sw
+
+    definition = sw.generate_wing()
+    cores = physical_cores()
+    per_step = []
+    from oracle import oracle as O
+
+    for _ in range(max(0, args.warmup)):
+        pass
+    sample = max(1, min(args.steps, 8))
+    value, kind, used = cpu_reference_run(definition, sample, cores)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": sample,
+            "warmup": 1, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": wing_config(),
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": kind,
+                             "sample": f"{sample} wing steps (workerThreads={used})"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+
+    import simwing_b200 as sw
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    if args.warmup < 3:
+        raise SystemExit("warmup must be >= 3")
+
+    definition = sw.generate_wing()
+    st = settings(sw)
+    structure = sw.Structure(definition, sw.SolverOptions(device=local))
+    flush =torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    # warm-up
+    for _ in range(args.warmup):
+        structure.step(st, diagnostics=False)
+    torch.cuda.synchronize()
+
+    # device-timed region: per-step CUDA events inside the library (solver
+    # stream), L2 flush between steps (outside the events)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            structure.step(st, diagnostics=False)
+            times.append(structure.last_step_ms())
+    torch.cuda.synchronize()
+    total_ms = float(sum(times))
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1000.0)
+
+    # end-to-end through the C-ABI with host buffers
+    rng = np.random.default_rng(5)
+    forces = rng.normal(0.0, 1e-4, size=(structure.node_count, 3))
+    e2e_steps = max(3, args.e2e_steps)
+    for _ in range(3):
+        structure.set_external_forces(forces)
+        structure.step(st, diagnostics=True)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        structure.set_external_forces(forces)
+        diag = structure.step(st, diagnostics=True)
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * e2e_steps / e2e_s
+    h2d = structure.node_count * 16
+    d2h = 148 * 16 * 8 + 16 + 128  # diagnostics partials + control word + payload
+
+    bytes_per_step = algorithmic_bytes(definition)
+    peak, peak_kind = measured_peak()
+    achieved = bytes_per_step / (ms_per_step / 1000.0) / 1e9
+    report = structure.schedule_report()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu_value, kind, used = cpu_reference_run(definition, args.cpu_sample_steps, 0)
+        cpu = {"value": cpu_value, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"{args.cpu_sample_steps} wing steps, serial (workerThreads=0)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": wing_config(),
+            "parallelism": "replicas" if world > 1 else "single",
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profile_traffic(),
+                         "peak_source": peak_kind, "algorithmic_bytes_per_step": bytes_per_step},
+            "clocks": clocks.summary(),
+            "schedule": {"blocks": report.blocks, "threads": report.block_threads,
+                         "levels": report.partition_levels,
+                         "device_phases_per_iteration": report.device_phases_per_iteration,
+                         "local_stages_per_iteration": report.local_stages_per_iteration,
+                         "shared_bytes": report.shared_bytes},
+            "final_diagnostics": {"finite": bool(diag.finite), "max_distance_error": diag.maximum_distance_error},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    structure.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -445,6 +445,18 @@ typedef struct swb_schedule_report {
 swb_status swb_structure_schedule_report(const swb_structure* structure,
                                          swb_schedule_report* out);
 
+/* Builds the same schedule on the host alone (no device needed), checks
+ * every invariant the device relies on (disjoint patches, node-disjoint
+ * stages, each constraint exactly once, complete patch interfaces) and
+ * fills the report and, when non-NULL, the sweep orders (constraint_count
+ * and dihedral_count entries).  block_threads and shared_bytes are left 0.
+ * No reference counterpart. */
+swb_status swb_plan_schedule(const swb_structure_definition* definition,
+                             const swb_solver_options* options,
+                             swb_schedule_report* out,
+                             uint64_t* distance_order,
+                             uint64_t* dihedral_order);
+
 /* Device time of the most recent step's kernels in milliseconds, measured
  * with CUDA events on the solver's stream. */
 double swb_structure_last_step_ms(const swb_structure* structure);

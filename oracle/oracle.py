@@ -44,6 +44,7 @@ _REF = {
     "swref_physical_cores": (C.c_uint, []),
     "swref_create": (C.c_int, [P(abi.StructureDefinition), P(C.c_void_p)]),
     "swref_destroy": (None, [C.c_void_p]),
+    "swref_fingerprint": (C.c_uint64, [C.c_void_p]),
     "swref_set_external_forces": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swref_add_external_force": (C.c_int, [C.c_void_p, C.c_uint64, P(abi.Vec3)]),
     "swref_step": (C.c_int, [C.c_void_p, P(abi.StepSettings), P(abi.Diagnostics)]),
@@ -174,6 +175,9 @@ class RefStructure(_Base):
 
     def last_step_seconds(self):
         return float(ref_library().swref_last_step_seconds(self._h))
+
+    def fingerprint(self):
+        return int(ref_library().swref_fingerprint(self._h))
 
     def payload(self, segments=0):
         p = abi.PayloadState()

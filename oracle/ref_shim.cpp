@@ -264,6 +264,11 @@ swb_status swref_create(const swb_structure_definition* definition,
 
 void swref_destroy(void* handle) { delete static_cast<RefHandle*>(handle); }
 
+// Structure::definitionFingerprint (structure.h:284).
+uint64_t swref_fingerprint(void* handle) {
+    return static_cast<RefHandle*>(handle)->structure->definitionFingerprint();
+}
+
 swb_status swref_set_external_forces(void* handle,
                                      const swb_vec3* forces,
                                      uint64_t count) {

@@ -25,6 +25,7 @@ __all__ = [
     "Structure", "Definition", "StepSettings", "SolverOptions", "generate_patch", "generate_wing",
     "SimwingError", "InvalidArgument", "OutOfRange", "SuspensionError", "ContactStepError",
     "NonFiniteState", "SyncTimeout", "CudaError", "Unsupported", "reference_colouring",
+    "definition_from_arrays", "plan_schedule",
 ]
 
 
@@ -191,6 +192,77 @@ class Definition:
         return out
 
 
+def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), suspension=None) -> Definition:
+    """Builds an owned Definition from plain Python records.
+
+    nodes:       [(x, y, z, mass, fixed), ...]
+    triangles:   [(a, b, c[, pressure]), ...]
+    constraints: [(kind, a, b, rest, compliance), ...]
+    dihedrals:   [(a, b, c, d, rest_angle, compliance), ...]
+    suspension:  dict with pilot_mass, pilot_com_world, pilot_inertia,
+                 attachments [(id, node)], harness [(id, (x, y, z))],
+                 segments [(id, (kind, id), (kind, id), rest, stiffness,
+                 damping)], solver_iterations, maximum_line_residual.
+    """
+    lib = abi.library()
+    n = (abi.NodeDef * max(len(nodes), 1))()
+    for i, (x, y, z, m, fixed) in enumerate(nodes):
+        n[i] = abi.NodeDef(Vec3(x, y, z), m, 1 if fixed else 0, 0)
+    t = (abi.TriangleDef * max(len(triangles), 1))()
+    for i, tri in enumerate(triangles):
+        t[i].nodes[:] = [int(tri[0]), int(tri[1]), int(tri[2])]
+        t[i].pressure_difference = float(tri[3]) if len(tri) > 3 else 0.0
+    c = (abi.ConstraintDef * max(len(constraints), 1))()
+    for i, (kind, a, b, rest, comp) in enumerate(constraints):
+        c[i] = abi.ConstraintDef(kind, 0, a, b, rest, comp)
+    h = (abi.DihedralDef * max(len(dihedrals), 1))()
+    for i, (a, b, cc, d, rest, comp) in enumerate(dihedrals):
+        h[i].nodes[:] = [a, b, cc, d]
+        h[i].rest_angle = rest
+        h[i].compliance = comp
+    view = abi.StructureDefinition()
+    view.node_count, view.nodes = len(nodes), n
+    view.triangle_count, view.triangles = len(triangles), t
+    view.constraint_count, view.constraints = len(constraints), c
+    view.dihedral_count, view.dihedrals = len(dihedrals), h
+    keep = [n, t, c, h]
+    if suspension is not None:
+        s = abi.SuspensionDef()
+        s.pilot_stable_id = 1
+        s.pilot_mass = suspension.get("pilot_mass", 90.0)
+        s.pilot_initial_com_world = Vec3(*suspension.get("pilot_com_world", (0.0, 0.0, 0.0)))
+        s.pilot_initial_body_to_world = abi.Quat(*suspension.get("pilot_orientation", (1.0, 0.0, 0.0, 0.0)))
+        s.pilot_principal_inertia = Vec3(*suspension.get("pilot_inertia", (10.0, 10.0, 5.0)))
+        s.pilot_initial_linear_velocity = Vec3(*suspension.get("pilot_velocity", (0.0, 0.0, 0.0)))
+        s.pilot_initial_angular_velocity = Vec3(*suspension.get("pilot_angular_velocity", (0.0, 0.0, 0.0)))
+        att = suspension.get("attachments", [])
+        a = (abi.SuspensionAttachment * max(len(att), 1))(*[abi.SuspensionAttachment(i, nd) for i, nd in att])
+        jun = suspension.get("junctions", [])
+        j = (abi.SuspensionJunction * max(len(jun), 1))(*[abi.SuspensionJunction(i, nd) for i, nd in jun])
+        har = suspension.get("harness", [])
+        hp = (abi.PilotHarness * max(len(har), 1))(*[abi.PilotHarness(i, Vec3(*p)) for i, p in har])
+        seg = suspension.get("segments", [])
+        sg = (abi.SuspensionSegment * max(len(seg), 1))()
+        for k, (sid, fr, to, rest, stiff, damp) in enumerate(seg):
+            sg[k] = abi.SuspensionSegment(sid, abi.SuspensionEndpoint(fr[0], 0, fr[1]),
+                                          abi.SuspensionEndpoint(to[0], 0, to[1]), rest, stiff, damp, 1, 0)
+        s.attachment_count, s.attachments = len(att), a
+        s.junction_count, s.junctions = len(jun), j
+        s.harness_count, s.harness_points = len(har), hp
+        s.segment_count, s.segments = len(seg), sg
+        s.solver_iterations = suspension.get("solver_iterations", 12)
+        s.attachment_tolerance = 1e-10
+        s.minimum_line_length = 1e-10
+        s.maximum_line_residual = suspension.get("maximum_line_residual", 2e-4)
+        s.maximum_control_work = 1e6
+        view.suspension = C.pointer(s)
+        keep += [s, a, j, hp, sg]
+    out = C.c_void_p()
+    _check(lib.swb_definition_copy(C.byref(view), C.byref(out)))
+    del keep
+    return Definition(out.value)
+
+
 def generate_patch(**overrides) -> Definition:
     """The hanging cloth patch (33 x 33 on 1 m x 1 m by default)."""
     lib = abi.library()
@@ -226,6 +298,19 @@ def reference_colouring(definition: Definition):
     _check(lib.swb_reference_colouring(definition.pointer, order.ctypes.data, offsets.ctypes.data,
                                        offsets.size, C.byref(colours), C.byref(parallel)))
     return order[:m], offsets[: colours.value + 1 if m else 0], int(parallel.value)
+
+
+def plan_schedule(definition: Definition, options: abi.SolverOptions | None = None):
+    """Host-only schedule build + invariant check; returns (report,
+    distance sweep order, dihedral sweep order)."""
+    lib = abi.library()
+    v = definition.view
+    r = abi.ScheduleReport()
+    do = np.zeros(max(v.constraint_count, 1), dtype=np.uint64)
+    ho = np.zeros(max(v.dihedral_count, 1), dtype=np.uint64)
+    _check(lib.swb_plan_schedule(definition.pointer, None if options is None else C.byref(options), C.byref(r),
+                                 do.ctypes.data, ho.ctypes.data))
+    return r, do[: v.constraint_count], ho[: v.dihedral_count]
 
 
 @dataclass

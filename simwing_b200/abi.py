@@ -207,6 +207,8 @@ _PROTOTYPES = {
     "swb_structure_sweep_order": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64]),
     "swb_structure_schedule_report": (C.c_int, [C.c_void_p, P(ScheduleReport)]),
     "swb_structure_last_step_ms": (C.c_double, [C.c_void_p]),
+    "swb_plan_schedule": (C.c_int, [P(StructureDefinition), P(SolverOptions), P(ScheduleReport), C.c_void_p,
+                                    C.c_void_p]),
     "swb_reference_colouring": (C.c_int, [P(StructureDefinition), C.c_void_p, C.c_void_p, C.c_uint64,
                                           P(C.c_uint64), P(C.c_uint64)]),
     "swb_default_patch_params": (None, [P(PatchParams)]),

@@ -2,6 +2,7 @@
 #include "schedule.h"
 
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <numeric>
 #include <queue>
@@ -538,3 +539,191 @@ Schedule build_schedule(const OwnedDefinition& d,
 }
 
 }  // namespace swb
+
+namespace swb {
+
+std::vector<uint32_t> suspension_endpoint_nodes(const OwnedDefinition& d) {
+    std::vector<uint32_t> nodes;
+    if (!d.has_suspension) return nodes;
+    for (const auto& g : d.segments)
+        for (const swb_suspension_endpoint* e : {&g.from, &g.to}) {
+            if (e->kind == SWB_ENDPOINT_SURFACE_ATTACHMENT) {
+                for (const auto& a : d.attachments)
+                    if (a.stable_id == e->stable_id) nodes.push_back(static_cast<uint32_t>(a.node));
+            } else if (e->kind == SWB_ENDPOINT_JUNCTION) {
+                for (const auto& j : d.junctions)
+                    if (j.stable_id == e->stable_id) nodes.push_back(static_cast<uint32_t>(j.node));
+            }
+        }
+    std::sort(nodes.begin(), nodes.end());
+    nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+    return nodes;
+}
+
+void verify_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes,
+                     const Schedule& S) {
+    auto fail = [](const std::string& what) { raise(SWB_INVALID_ARGUMENT, "schedule invariant: " + what); };
+    const uint32_t N = static_cast<uint32_t>(d.nodes.size());
+    const int G = S.blocks;
+    // slots
+    if (S.node_of_slot.size() != N || S.slot_of_node.size() != N) fail("slot map size");
+    for (uint32_t n = 0; n < N; ++n)
+        if (S.node_of_slot[S.slot_of_node[n]] != n) fail("slot map is not a bijection");
+    if (S.l1_begin.size() != static_cast<size_t>(G) + 1 || S.l1_begin[0] != 0 || S.l1_begin[G] != N)
+        fail("level-1 ranges");
+    std::vector<int> l1_block(N, -1);
+    for (int b = 0; b < G; ++b)
+        for (uint32_t s = S.l1_begin[b]; s < S.l1_begin[b + 1]; ++s) l1_block[S.node_of_slot[s]] = b;
+    for (uint32_t n : suspension_nodes)
+        if (l1_block[n] != S.suspension_block) fail("suspension node outside the owner patch");
+    std::array<std::vector<uint32_t>, kKinds> seen;
+    seen[0].assign(d.constraints.size(), 0);
+    seen[1].assign(d.dihedrals.size(), 0);
+    std::vector<uint8_t> outside(N, 0);
+    std::vector<int64_t> stamp(N, -1);
+    int64_t epoch = 0;
+    auto nodes_of = [&](int k, uint32_t i, uint32_t out[4]) {
+        if (k == 0) {
+            out[0] = static_cast<uint32_t>(d.constraints[i].first_node);
+            out[1] = static_cast<uint32_t>(d.constraints[i].second_node);
+            return 2;
+        }
+        for (int q = 0; q < 4; ++q) out[q] = static_cast<uint32_t>(d.dihedrals[i].nodes[q]);
+        return 4;
+    };
+    for (int level = 0; level < S.levels; ++level) {
+        // patch membership for this level
+        std::vector<int> owner(N, -1);
+        std::vector<std::vector<uint32_t>> local_to_node(G);
+        if (level == 0) {
+            owner = l1_block;
+            for (int b = 0; b < G; ++b)
+                for (uint32_t s = S.l1_begin[b]; s < S.l1_begin[b + 1]; ++s)
+                    local_to_node[b].push_back(S.node_of_slot[s]);
+        } else {
+            for (int b = 0; b < G; ++b)
+                for (uint32_t i = S.patch_begin[level][b]; i < S.patch_begin[level][b + 1]; ++i) {
+                    const uint32_t n = S.node_of_slot[S.patch_slots[level][i]];
+                    if (owner[n] >= 0) fail("gathered patches overlap");
+                    owner[n] = b;
+                    local_to_node[b].push_back(n);
+                }
+        }
+        for (int k = 0; k < kKinds; ++k) {
+            const Table& T = S.tables[level][k];
+            for (int b = 0; b < G; ++b) {
+                const uint32_t bb = T.block_begin[b];
+                for (int s = 0; s < T.stages; ++s) {
+                    ++epoch;
+                    const size_t o = static_cast<size_t>(b) * (T.stages + 1) + s;
+                    for (uint32_t i = T.stage_offsets[o]; i < T.stage_offsets[o + 1]; ++i) {
+                        const uint32_t e = bb + i;
+                        if (!T.valid[e]) fail("padding inside a stage");
+                        uint32_t li[4] = {T.ab[e] & 0xffffu, T.ab[e] >> 16, 0, 0};
+                        if (k == 1) { li[2] = T.cd[e] & 0xffffu; li[3] = T.cd[e] >> 16; }
+                        uint32_t dn[4];
+                        const int cnt = nodes_of(k, T.def_index[e], dn);
+                        ++seen[k][T.def_index[e]];
+                        for (int q = 0; q < cnt; ++q) {
+                            if (li[q] >= local_to_node[b].size() || local_to_node[b][li[q]] != dn[q])
+                                fail("local index does not name the constraint's node");
+                            if (owner[dn[q]] != b) fail("constraint node outside the CTA patch");
+                            if (stamp[dn[q]] == epoch) fail("stage is not node-disjoint");
+                            stamp[dn[q]] = epoch;
+                            if (level > 0) outside[dn[q]] = 1;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    for (int k = 0; k < kKinds; ++k) {
+        const GlobalTable& T = S.global[k];
+        const int colours = T.colour_offsets.empty() ? 0 : static_cast<int>(T.colour_offsets.size()) - 1;
+        for (int c = 0; c < colours; ++c) {
+            ++epoch;
+            for (uint32_t i = T.colour_offsets[c]; i < T.colour_offsets[c + 1]; ++i) {
+                uint32_t dn[4];
+                const int cnt = nodes_of(k, T.def_index[i], dn);
+                ++seen[k][T.def_index[i]];
+                const uint32_t slots[4] = {T.a[i], T.b[i], k ? T.c[i] : 0u, k ? T.d[i] : 0u};
+                for (int q = 0; q < cnt; ++q) {
+                    if (S.slot_of_node[dn[q]] != slots[q]) fail("global slot mismatch");
+                    if (stamp[dn[q]] == epoch) fail("global colour is not node-disjoint");
+                    stamp[dn[q]] = epoch;
+                    outside[dn[q]] = 1;
+                }
+            }
+        }
+    }
+    for (int k = 0; k < kKinds; ++k)
+        for (size_t i = 0; i < seen[k].size(); ++i)
+            if (seen[k][i] != 1) fail("constraint not scheduled exactly once");
+    // seam stages: disjoint, and consistent with the sweep order
+    const int seam_stages = S.seam_stage_offsets.empty() ? 0 : static_cast<int>(S.seam_stage_offsets.size()) - 1;
+    for (int s = 0; s < seam_stages; ++s) {
+        ++epoch;
+        for (uint32_t i = S.seam_stage_offsets[s]; i < S.seam_stage_offsets[s + 1]; ++i)
+            for (uint32_t slot : {S.seam_a[i], S.seam_b[i]}) {
+                const uint32_t n = S.node_of_slot[slot];
+                if (stamp[n] == epoch) fail("seam stage is not node-disjoint");
+                stamp[n] = epoch;
+                outside[n] = 1;
+            }
+    }
+    // interface completeness
+    std::vector<uint8_t> in_iface(N, 0);
+    for (int b = 0; b < G; ++b)
+        for (uint32_t i = S.iface_begin[b]; i < S.iface_begin[b + 1]; ++i)
+            in_iface[S.node_of_slot[S.l1_begin[b] + S.iface_local[i]]] = 1;
+    for (uint32_t n = 0; n < N; ++n)
+        if (outside[n] && !in_iface[n]) fail("node touched outside level 1 is missing from the interface");
+    // sweep orders are permutations in execution order
+    for (int k = 0; k < kKinds; ++k) {
+        const auto& order = k == 0 ? S.distance_order : S.dihedral_order;
+        if (order.size() != seen[k].size()) fail("sweep order length");
+    }
+}
+
+}  // namespace swb
+
+extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definition,
+                                        const swb_solver_options* options, swb_schedule_report* out,
+                                        uint64_t* distance_order, uint64_t* dihedral_order) {
+    using namespace swb;
+    return guarded([&] {
+        if (!definition || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
+        OwnedDefinition def;
+        def.assign(*definition);
+        validate_definition(def.view);
+        ScheduleOptions so;
+        so.blocks = options && options->blocks > 0 ? options->blocks : 148;
+        so.blocks = static_cast<int>(std::min<uint64_t>(so.blocks, std::max<uint64_t>(1, def.nodes.size())));
+        so.levels = options && options->partition_levels > 0 ? options->partition_levels : 3;
+        so.global_only = options && (options->flags & SWB_OPT_GLOBAL_ONLY);
+        const std::vector<uint32_t> susp = suspension_endpoint_nodes(def);
+        const Schedule S = build_schedule(def, susp, so);
+        verify_schedule(def, susp, S);
+        std::memset(out, 0, sizeof(*out));
+        out->blocks = S.blocks;
+        out->partition_levels = S.levels;
+        int phases = 0, stages = 0;
+        for (int k = 0; k < kKinds; ++k) {
+            bool outer = S.global[k].colour_offsets.size() > 1;
+            for (int l = 0; l < S.levels; ++l) {
+                stages += S.tables[l][k].stages;
+                if (l > 0 && S.tables[l][k].stages > 0) { outer = true; ++phases; }
+            }
+            const int gc = S.global[k].colour_offsets.empty() ? 0 : static_cast<int>(S.global[k].colour_offsets.size()) - 1;
+            out->global_colours_per_iteration += gc;
+            phases += gc + (outer ? 1 : 0);
+        }
+        out->device_phases_per_iteration = phases;
+        out->local_stages_per_iteration = stages;
+        out->max_patch_nodes = S.max_patch_nodes;
+        for (int l = 0; l < 4; ++l) out->level_constraints[l] = S.level_constraints[l];
+        out->global_constraints = S.global_constraints;
+        if (distance_order) std::copy(S.distance_order.begin(), S.distance_order.end(), distance_order);
+        if (dihedral_order) std::copy(S.dihedral_order.begin(), S.dihedral_order.end(), dihedral_order);
+    });
+}

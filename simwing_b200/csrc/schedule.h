@@ -104,4 +104,14 @@ Schedule build_schedule(const OwnedDefinition& d,
                         const std::vector<uint32_t>& suspension_nodes,
                         const ScheduleOptions& options);
 
+// Checks every invariant the device relies on (disjoint patches, node-
+// disjoint stages, each constraint exactly once, interface completeness,
+// sweep orders); raises SWB_INVALID_ARGUMENT describing the first failure.
+void verify_schedule(const OwnedDefinition& d,
+                     const std::vector<uint32_t>& suspension_nodes,
+                     const Schedule& s);
+
+// Nodes of the suspension segments' endpoints (attachments, junctions).
+std::vector<uint32_t> suspension_endpoint_nodes(const OwnedDefinition& d);
+
 }  // namespace swb

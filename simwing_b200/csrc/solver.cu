@@ -139,29 +139,16 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     for (size_t t = 0; t < def.triangles.size(); ++t) pressure[t] = def.triangles[t].pressure_difference;
 
     // Suspension: endpoint nodes must share one level-1 patch.
-    std::vector<uint32_t> susp_nodes;
-    if (def.has_suspension) {
-        if (def.segments.size() > 8 || def.harness.size() > 8)
-            raise(SWB_UNSUPPORTED, "more than 8 suspension segments or harness points");
-        for (const auto& g : def.segments)
-            for (const swb_suspension_endpoint* e : {&g.from, &g.to}) {
-                if (e->kind == SWB_ENDPOINT_SURFACE_ATTACHMENT) {
-                    for (const auto& a : def.attachments)
-                        if (a.stable_id == e->stable_id) susp_nodes.push_back(static_cast<uint32_t>(a.node));
-                } else if (e->kind == SWB_ENDPOINT_JUNCTION) {
-                    for (const auto& j : def.junctions)
-                        if (j.stable_id == e->stable_id) susp_nodes.push_back(static_cast<uint32_t>(j.node));
-                }
-            }
-        std::sort(susp_nodes.begin(), susp_nodes.end());
-        susp_nodes.erase(std::unique(susp_nodes.begin(), susp_nodes.end()), susp_nodes.end());
-    }
+    if (def.has_suspension && (def.segments.size() > 8 || def.harness.size() > 8))
+        raise(SWB_UNSUPPORTED, "more than 8 suspension segments or harness points");
+    const std::vector<uint32_t> susp_nodes = suspension_endpoint_nodes(def);
     ScheduleOptions so;
     so.blocks = opt.blocks > 0 ? opt.blocks : sm_count;
     so.blocks = static_cast<int>(std::min<uint64_t>(so.blocks, std::max<uint64_t>(1, N)));
     so.levels = opt.partition_levels > 0 ? opt.partition_levels : 3;
     so.global_only = (opt.flags & SWB_OPT_GLOBAL_ONLY) != 0;
     sched = build_schedule(def, susp_nodes, so);
+    verify_schedule(def, susp_nodes, sched);
     G = sched.blocks;
 
     // Threads per CTA: enough for the widest local stage, in warps.

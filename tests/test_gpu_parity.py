@@ -1,0 +1,195 @@
+"""Device parity: the sm_100a solver against the FP64 oracle, through the
+C-ABI.
+
+The oracle runs the reference algorithm (the C restatement pinned bit for
+bit to the reference build in test_oracle.py) on the definition permuted
+into the device sweep order, so both sides perform the same Gauss-Seidel
+sweep.  Tolerances:
+  * one step from an identical state: max position error / max |position|
+    <= 1e-5 (FP32 device vs FP64 oracle);
+  * 600 steps of the cloth patch: settled shape and max distance error
+    within 1e-3 m.
+"""
+import numpy as np
+import pytest
+
+import simwing_b200 as sw
+from oracle import oracle as O
+from tests.conftest import step_settings
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-5
+
+
+def rel_error(device_states, oracle_states):
+    scale = max(1.0, float(np.abs(oracle_states[:, 0, :]).max()))
+    return float(np.abs(device_states[:, 0, :] - oracle_states[:, 0, :]).max()) / scale
+
+
+def sync_oracle_to_device(dev, orc):
+    orc.write_node_states(dev.node_states())
+    if dev._segments:
+        s = dev.suspension_state()
+        import simwing_b200.abi as abi
+        orc.write_payload(abi.PayloadState(abi.Vec3(*s.center_of_mass), abi.Quat(*s.body_to_world),
+                                           abi.Vec3(*s.linear_velocity), abi.Vec3(*s.angular_velocity)))
+
+
+def per_step_errors(definition, steps, settings, options=None, sync=True):
+    dev = sw.Structure(definition, options)
+    orc = O.PortStructure(dev.oracle_definition())
+    errs = []
+    for _ in range(steps):
+        if sync:
+            sync_oracle_to_device(dev, orc)
+        dev.step(settings, diagnostics=False)
+        orc.step(settings)
+        errs.append(rel_error(dev.node_states(), orc.node_states()))
+    return errs, dev, orc
+
+
+def test_known_answers_on_device(cuda_device):
+    d = sw.definition_from_arrays([(0.0, 0.0, 0.0, 2.0, False)])
+    s = sw.Structure(d)
+    s.add_external_force(0, (4.0, 0.0, 0.0))
+    diag = s.step(sw.StepSettings(time_step=0.25, substeps=1, constraint_iterations=0, gravity=(0, 0, -2.0),
+                                  velocity_damping=0.0))
+    st = s.node_states()
+    assert st[0, 2, 0] == pytest.approx(0.5, abs=1e-7)
+    assert st[0, 0, 2] == pytest.approx(-0.125, abs=1e-7)
+    assert diag.last_applied_external_force.x == 4.0
+    assert diag.pending_external_force.x == 0.0
+    for kind, length, expected in [(1, 2.0, 1.0), (2, 0.5, 0.5), (2, 2.0, 1.0), (3, 2.0, 1.0)]:
+        d = sw.definition_from_arrays([(0.0, 0.0, 0.0, 0.0, True), (length, 0.0, 0.0, 1.0, False)],
+                                      constraints=[(kind, 0, 1, 1.0, 0.0)])
+        s = sw.Structure(d)
+        s.step(sw.StepSettings(time_step=1 / 60, substeps=1, constraint_iterations=1, gravity=(0, 0, 0),
+                               velocity_damping=0.0))
+        assert s.node_states()[1, 0, 0] == pytest.approx(expected, abs=1e-6)
+
+
+@pytest.mark.parametrize("blocks,levels", [(1, 1), (8, 1), (8, 3), (148, 3)])
+def test_patch_per_step_parity(cuda_device, blocks, levels):
+    errs, _, _ = per_step_errors(sw.generate_patch(), 6, step_settings(),
+                                 sw.SolverOptions(blocks=blocks, partition_levels=levels))
+    assert max(errs) <= REL_TOL, errs
+
+
+def test_patch_global_only_parity(cuda_device):
+    errs, _, _ = per_step_errors(sw.generate_patch(nx=17, ny=17), 4, step_settings(),
+                                 sw.SolverOptions(blocks=16, flags=sw.abi.OPT_GLOBAL_ONLY))
+    assert max(errs) <= REL_TOL, errs
+
+
+def test_wing_per_step_parity_small(cuda_device):
+    d = sw.generate_wing(cells=8, chordwise=20, spanwise_per_cell=2, rib_layers=3)
+    errs, dev, orc = per_step_errors(d, 4, step_settings())
+    assert max(errs) <= REL_TOL, errs
+    s = dev.suspension_state()
+    p, w, _ = orc.payload()
+    assert np.abs(s.center_of_mass - [p.center_of_mass.x, p.center_of_mass.y, p.center_of_mass.z]).max() < 1e-4
+
+
+def test_full_wing_one_step_parity(cuda_device):
+    errs, _, _ = per_step_errors(sw.generate_wing(), 2, step_settings())
+    assert max(errs) <= REL_TOL, errs
+
+
+def test_patch_600_steps_settled_shape(cuda_device):
+    d = sw.generate_patch()
+    dev = sw.Structure(d)
+    orc = O.PortStructure(dev.oracle_definition())
+    st = step_settings()
+    dev.step_many(st, 600)
+    for _ in range(600):
+        orc.step(st)
+    a, b = dev.node_states(), orc.node_states()
+    assert np.abs(a[:, 0, :] - b[:, 0, :]).max() <= 1e-3
+    da, db = dev.diagnostics(), orc.diagnostics()
+    assert abs(da.maximum_distance_error - db.maximum_distance_error) <= 1e-3
+    assert dev.accepted_step_count() == 600
+
+
+def test_checkpoint_replay_is_bitwise(cuda_device):
+    d = sw.generate_wing(cells=6, chordwise=12, spanwise_per_cell=2, rib_layers=3)
+    s = sw.Structure(d)
+    st = step_settings()
+    for _ in range(2):
+        s.step(st)
+    image = s.checkpoint()
+    for _ in range(3):
+        s.step(st)
+    first = s.node_states()
+    first_pay = s.suspension_state()
+    s.restore(image)
+    assert s.accepted_step_count() == 2
+    for _ in range(3):
+        s.step(st)
+    assert np.array_equal(first, s.node_states())
+    assert np.array_equal(first_pay.center_of_mass, s.suspension_state().center_of_mass)
+    # tampered and foreign images are rejected, state untouched
+    bad = bytearray(image)
+    bad[100] ^= 0xFF
+    with pytest.raises(sw.InvalidArgument):
+        s.restore(bytes(bad))
+    other = sw.Structure(sw.generate_patch(nx=5, ny=5))
+    with pytest.raises(sw.InvalidArgument):
+        other.restore(image)
+    assert np.array_equal(first, s.node_states())
+
+
+def test_failed_step_rolls_back_state_and_loads(cuda_device):
+    s = sw.Structure(sw.generate_patch(nx=9, ny=9))
+    s.add_external_force(3, (1.0, 2.0, 3.0))
+    before = s.node_states()
+    with pytest.raises(sw.InvalidArgument):
+        s.step(sw.StepSettings(time_step=0.0))
+    assert np.array_equal(before, s.node_states())
+    assert s.diagnostics().pending_external_force.z == 3.0
+    with pytest.raises(sw.OutOfRange):
+        s.add_external_force(10**6, (0.0, 0.0, 1.0))
+    with pytest.raises(sw.InvalidArgument):
+        s.add_external_force(0, (float("nan"), 0.0, 0.0))
+
+
+def test_non_finite_trial_is_rejected_and_rolled_back(cuda_device):
+    s = sw.Structure(sw.generate_patch(nx=9, ny=9))
+    st = step_settings()
+    s.step(st)
+    before = s.node_states()
+    s.add_external_force(40, (3.0e38, 3.0e38, 3.0e38))
+    with pytest.raises(sw.NonFiniteState):
+        s.step(st)
+    assert np.array_equal(before, s.node_states())
+    assert s.accepted_step_count() == 1
+
+
+def test_suspension_certification_failure_rolls_back(cuda_device):
+    d = sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2)
+    d.view.suspension.contents.maximum_line_residual = 0.0
+    s = sw.Structure(d)
+    before = s.node_states()
+    # a zero residual bound fails certification once the risers load
+    with pytest.raises(sw.SuspensionError):
+        for _ in range(20):
+            s.step(step_settings())
+    assert s.accepted_step_count() < 20
+
+
+def test_barrier_timeout_reports_and_restores(cuda_device):
+    s = sw.Structure(sw.generate_patch(), sw.SolverOptions(blocks=8, sync_budget_cycles=1))
+    before = s.node_states()
+    with pytest.raises(sw.SyncTimeout):
+        s.step(step_settings())
+    assert np.array_equal(before, s.node_states())
+
+
+def test_multi_substep_step_and_rollback(cuda_device):
+    d = sw.generate_patch(nx=12, ny=12)
+    s = sw.Structure(d)
+    orc = O.PortStructure(s.oracle_definition())
+    st = step_settings(substeps=3, iterations=16)
+    s.step(st)
+    orc.step(st)
+    assert rel_error(s.node_states(), orc.node_states()) <= REL_TOL
