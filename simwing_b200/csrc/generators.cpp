@@ -253,8 +253,9 @@ swb_status swb_generate_patch(const swb_patch_params* p, swb_definition** out) {
 
 // Ram-air wing.  Geometry: elliptical planform chord c0*sqrt(1-0.9*eta^2)
 // along a circular arc (anhedral), quarter-chord line straight, closed
-// symmetric 4-digit-style section of the given thickness, chordwise points
-// clustered towards the leading edge (x = 1 - cos(pi j / 2C)).  The skin is one closed sheet (top and bottom share the leading
+// symmetric 4-digit-style section of the given thickness, uniform chordwise
+// stations (x = j / C; clustering them at the leading edge makes sliver
+// triangles whose constraint solve is ill-conditioned).  The skin is one closed sheet (top and bottom share the leading
 // and trailing edge), 2*chordwise quads around and cells*spanwise_per_cell
 // quads across, oriented with outward right-hand normals and carrying the
 // outward pressure jump.  Each of the cells+1 ribs is its own sheet meshed
@@ -291,7 +292,7 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
             const double radius = 0.5 * span / phi_max;
             std::vector<double> xi(C + 1);
             for (uint32_t j = 0; j <= C; ++j)
-                xi[j] = 1.0 - std::cos(0.5 * 3.141592653589793 * j / C);
+                xi[j] = static_cast<double>(j) / C;
             auto half_thickness = [&](double x) {
                 return 5.0 * p->thickness *
                        (0.2969 * std::sqrt(x) - 0.1260 * x - 0.3516 * x * x +

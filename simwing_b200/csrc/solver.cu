@@ -185,11 +185,11 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     d_force = dalloc<float4>(owned, N);
     cuda_check(cudaMemsetAsync(d_force, 0, N * sizeof(float4), stream), "memset");
     cuda_check(cudaMallocHost(&h_force, std::max<uint64_t>(N, 1) * sizeof(float4)), "cudaMallocHost");
-    upload_pressure();
 
     // schedule tables
     StepParams& p = params;
     std::memset(&p, 0, sizeof(p));
+    upload_pressure();  // fills params.tri*, so after the reset above
     p.blocks = G;
     p.levels = sched.levels;
     p.l1_begin = dupload(owned, sched.l1_begin, stream);
@@ -363,7 +363,9 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     p.shift_out = &d_control->shift;
     const long long budget = opt.sync_budget_cycles > 0 ? opt.sync_budget_cycles : 4000000000LL;
     p.barrier.budget = budget;
-    p.copy_budget = budget;
+    // The staging wait keeps its own ~2 s bound whatever the barrier budget,
+    // so a CTA never leaves with bulk copies still in flight.
+    p.copy_budget = 4000000000LL;
 
     // launch feasibility
     cuda_check(cudaFuncSetAttribute(dev::xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -434,6 +436,25 @@ void StructureImpl::validate_settings(const swb_step_settings& st) const {
         raise(SWB_UNSUPPORTED, "load-path cable sweep pairs are not available in this build");
 }
 
+// Every device table the kernel dereferences must exist before a launch.
+void check_params(const StepParams& p) {
+    bool ok = p.pos_in && p.vel_in && p.pos_out && p.vel_out && p.prev_out && p.force && p.tri_offsets &&
+              p.tri_list && p.tri && p.l1_begin && p.iface_begin && p.iface_local && p.seam_offsets && p.seam_a &&
+              p.seam_b && p.payload_def && p.payload_in && p.payload_out && p.shift_out && p.origin_in &&
+              p.origin_out && p.status && p.barrier.count && p.barrier.generation && p.barrier.status;
+    for (int k = 0; k < 2; ++k)
+        ok = ok && p.glob[k].colour_offsets && p.glob[k].a && p.glob[k].b && p.glob[k].rest && p.glob[k].comp &&
+             p.glob[k].lambda && (k == 0 || (p.glob[k].c && p.glob[k].d));
+    for (int l = 0; l < p.levels; ++l) {
+        for (int k = 0; k < 2; ++k) {
+            const DevTable& t = p.tab[l][k];
+            ok = ok && t.block_begin && t.stage_offsets && t.ab && t.rest && t.comp && (k == 0 || t.cd);
+        }
+        if (l > 0) ok = ok && p.patch_begin[l] && p.patch_slots[l];
+    }
+    if (!ok) raise(SWB_CUDA_ERROR, "internal error: a device table is missing; launch refused");
+}
+
 void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out) {
     StepParams p = params;
     const double dt = st.time_step / st.substeps;
@@ -450,6 +471,7 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out)
     p.ref_velocity = make_float3(st.damping_reference_velocity.x, st.damping_reference_velocity.y,
                                  st.damping_reference_velocity.z);
     p.iterations = st.constraint_iterations;
+    check_params(p);
     cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
     void* args[] = {&p};
     cuda_check(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dev::xpbd_step_kernel), dim3(G), dim3(threads),
