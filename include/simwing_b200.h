@@ -298,20 +298,29 @@ typedef struct swb_wrench {
 /* Solver options (no reference counterpart: launch shape of the persistent  */
 /* kernel; zero fields mean "choose automatically").                         */
 /* ------------------------------------------------------------------------ */
+/* Two device schedules exist.  The cluster schedule (default when the mesh
+ * fits: at most 16 x 4096 nodes and the shared-memory budget) keeps every
+ * node in the distributed shared memory of one thread-block cluster and
+ * separates colour stages with cluster barriers.  The grid schedule spreads
+ * patches over a persistent cooperative grid with device-wide barriers and
+ * serves meshes that do not fit one cluster. */
 typedef struct swb_solver_options {
     int32_t device;          /* CUDA device ordinal                          */
-    int32_t blocks;          /* persistent CTAs; 0 = SM count                */
-    int32_t block_threads;   /* threads per CTA; 0 = autotuned               */
-    int32_t partition_levels;/* patch-partition levels; 0 = autotuned        */
-    int32_t colours_per_sync;/* reserved                                     */
+    int32_t blocks;          /* grid schedule: persistent CTAs; 0 = SMs      */
+    int32_t block_threads;   /* threads per CTA; 0 = chosen from the mesh    */
+    int32_t partition_levels;/* grid schedule: patch levels; 0 = 3           */
+    int32_t cluster_ctas;    /* cluster schedule: CTAs per cluster (1..16);
+                                0 = smallest power of two that fits          */
     uint32_t flags;          /* SWB_OPT_* bits                               */
     int64_t sync_budget_cycles; /* bounded barrier spin; 0 = default (~2 s)  */
 } swb_solver_options;
 
 enum {
-    SWB_OPT_GLOBAL_ONLY = 1u << 0, /* no shared-memory patches: every colour
-                                      is a device-wide phase (debug/compare) */
-    SWB_OPT_NO_GRAPH = 1u << 1     /* batched: launch without CUDA graphs    */
+    SWB_OPT_GLOBAL_ONLY = 1u << 0, /* grid schedule without shared-memory
+                                      patches: every colour is a device-wide
+                                      phase (comparison/debug)               */
+    SWB_OPT_NO_GRAPH = 1u << 1,    /* batched: launch without CUDA graphs    */
+    SWB_OPT_GRID = 1u << 2         /* force the grid schedule                */
 };
 
 void swb_default_solver_options(swb_solver_options* out);
@@ -441,6 +450,8 @@ typedef struct swb_schedule_report {
     int32_t shared_bytes;
     uint64_t level_constraints[4];       /* distance+dihedral per level      */
     uint64_t global_constraints;
+    int32_t cluster_ctas;                /* 0 = grid schedule                */
+    int32_t cluster_barriers_per_iteration;
 } swb_schedule_report;
 swb_status swb_structure_schedule_report(const swb_structure* structure,
                                          swb_schedule_report* out);

@@ -138,7 +138,7 @@ class Wrench(C.Structure):
 
 class SolverOptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("blocks", C.c_int32), ("block_threads", C.c_int32),
-                ("partition_levels", C.c_int32), ("colours_per_sync", C.c_int32), ("flags", C.c_uint32),
+                ("partition_levels", C.c_int32), ("cluster_ctas", C.c_int32), ("flags", C.c_uint32),
                 ("sync_budget_cycles", C.c_int64)]
 
 
@@ -147,7 +147,8 @@ class ScheduleReport(C.Structure):
                 ("device_phases_per_iteration", C.c_int32), ("local_stages_per_iteration", C.c_int32),
                 ("global_colours_per_iteration", C.c_int32), ("max_patch_nodes", C.c_int32),
                 ("shared_bytes", C.c_int32), ("level_constraints", C.c_uint64 * 4),
-                ("global_constraints", C.c_uint64)]
+                ("global_constraints", C.c_uint64), ("cluster_ctas", C.c_int32),
+                ("cluster_barriers_per_iteration", C.c_int32)]
 
 
 class PatchParams(C.Structure):
@@ -172,7 +173,7 @@ OK, INVALID_ARGUMENT, OUT_OF_RANGE, SUSPENSION_ERROR, CONTACT_ERROR, NON_FINITE,
     CUDA_ERROR, UNSUPPORTED, OUT_OF_MEMORY = range(10)
 
 DISTANCE, CABLE, SUSPENSION_TIE, SEAM_STITCH = 1, 2, 3, 4
-OPT_GLOBAL_ONLY, OPT_NO_GRAPH = 1, 2
+OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID = 1, 2, 4
 SWEEP_DISTANCE, SWEEP_DIHEDRAL = 0, 1
 
 P = C.POINTER

@@ -64,7 +64,7 @@ std::vector<uint8_t> serialize(const StructureImpl& m) {
     const uint64_t N = m.def.nodes.size();
     w.u64(N);
     for (uint64_t n = 0; n < N; ++n) {
-        const uint32_t s = m.sched.slot_of_node[n];
+        const uint32_t s = m.slot_of_node[n];
         for (const float4* a : {&pos[s], &prev[s], &vel[s]}) {
             w.f64(a->x); w.f64(a->y); w.f64(a->z);
         }
@@ -134,7 +134,7 @@ swb_status swb_structure_restore(swb_structure* s, const void* buffer, uint64_t 
             raise(SWB_INVALID_ARGUMENT, "Invalid structure checkpoint");
         std::vector<float4> pos(N), prev(N), vel(N);
         for (uint64_t n = 0; n < N; ++n) {
-            const uint32_t sl = m.sched.slot_of_node[n];
+            const uint32_t sl = m.slot_of_node[n];
             double v[9];
             for (double& x : v) {
                 x = r.f64();

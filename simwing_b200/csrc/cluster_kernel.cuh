@@ -1,0 +1,256 @@
+// Cluster XPBD step kernel: one thread-block cluster (up to 16 CTAs)
+// steps one structure, with every node resident in the distributed shared
+// memory of the cluster for the whole substep.
+//
+// Same substep as xpbd_step_kernel (SoftBody::integrateSubstepTrial,
+// src/softwing/soft_body.cpp:1175-1460) with a different schedule: every
+// colour of the whole mesh is one stage, each CTA executes the stage's
+// constraints it owns, nodes of other CTAs are read and written through
+// distributed shared memory, and a cluster barrier (not a device-wide one)
+// separates stages.  A launch may carry several independent clusters; the
+// cluster index selects the instance (see ClusterInstance).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "cluster_params.h"
+#include "step_kernel.cuh"
+
+namespace swb {
+
+namespace dev {
+
+__device__ __forceinline__ float4* node_at(uint32_t ref, uint32_t me, float4* x, float4* const* peers) {
+    const uint32_t r = ref >> 12;
+    return (r == me ? x : peers[r]) + (ref & 0xfffu);
+}
+
+// One constraint record held in registers between its prefetch and its use.
+struct ClusterRecord {
+    uint32_t ab, cd;
+    float rest, comp;
+    uint32_t index;  // record index (global), or ~0u when the slot is empty
+};
+
+__device__ __forceinline__ ClusterRecord load_record(const ClusterKindDev& K, int kind, uint32_t i, uint32_t hi) {
+    ClusterRecord r;
+    r.index = ~0u;
+    if (i < hi) {
+        r.ab = __ldg(K.ab + i);
+        r.cd = kind ? __ldg(K.cd + i) : 0u;
+        r.rest = __ldg(K.rest + i);
+        r.comp = __ldg(K.comp + i);
+        r.index = i;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, uint32_t me, float4* x,
+                                             float4* const* peers, float* lam, uint32_t first, float inv_dt2) {
+    float4* pa = node_at(r.ab & 0xffffu, me, x, peers);
+    float4* pb = node_at(r.ab >> 16, me, x, peers);
+    float l = lam[r.index - first];
+    if (kind == 0) {
+        float4 A = *pa, B = *pb;
+        project_distance(A, B, r.rest, r.comp, l, inv_dt2);
+        *pa = A;
+        *pb = B;
+    } else {
+        float4* pc = node_at(r.cd & 0xffffu, me, x, peers);
+        float4* pd = node_at(r.cd >> 16, me, x, peers);
+        float4 A = *pa, B = *pb, C = *pc, D = *pd;
+        project_dihedral(A, B, C, D, r.rest, r.comp, l, inv_dt2);
+        *pa = A;
+        *pb = B;
+        *pc = C;
+        *pd = D;
+    }
+    lam[r.index - first] = l;
+}
+
+constexpr int kClusterMaxThreads = 768;
+
+__global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const __grid_constant__ ClusterParams p) {
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t bar;
+    __shared__ DevPayloadState pay;
+    __shared__ float4* peers[16];
+    __shared__ float3 shift_s;
+    cg::cluster_group cluster = cg::this_cluster();
+    const uint32_t me = cluster.block_rank();
+    const ClusterInstance& I = p.instances[blockIdx.x / p.ctas];
+    const int tid = threadIdx.x;
+    float4* x = reinterpret_cast<float4*>(smem + p.smem_x);
+    float4* v = reinterpret_cast<float4*>(smem + p.smem_v);
+    float* lam0 = reinterpret_cast<float*>(smem + I.kind[0].smem_lambda);
+    float* lam1 = reinterpret_cast<float*>(smem + I.kind[1].smem_lambda);
+    const uint32_t base = __ldg(I.patch_begin + me);
+    const uint32_t n = __ldg(I.patch_begin + me + 1) - base;
+    const bool owner = static_cast<int>(me) == I.susp_cta;
+
+    if (tid < p.ctas) peers[tid] = cluster.map_shared_rank(x, tid);
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_expect_tx(&bar, n * 16u);
+        if (n) bulk_load(x, I.pos_in + base, n * 16u, &bar);
+    }
+    // multipliers restart every substep (soft_body.cpp:1207-1218)
+    for (int k = 0; k < 2; ++k) {
+        const uint32_t* off = I.kind[k].offsets + static_cast<size_t>(me) * (I.kind[k].stages + 1);
+        const uint32_t cnt = __ldg(off + I.kind[k].stages) - __ldg(off);
+        float* lam = k == 0 ? lam0 : lam1;
+        for (uint32_t i = tid; i < cnt; i += blockDim.x) lam[i] = 0.0f;
+    }
+    // pressure gather (ascending triangle order) into v
+    for (uint32_t i = tid; i < n; i += blockDim.x) {
+        const uint32_t slot = base + i;
+        float3 f = f3(__ldg(I.force + slot));
+        const uint32_t lo = __ldg(I.tri_offsets + slot), hi = __ldg(I.tri_offsets + slot + 1);
+        for (uint32_t q = lo; q < hi; ++q) {
+            const uint4 t = __ldg(I.tri + __ldg(I.tri_list + q));
+            const float3 pa = f3(__ldg(I.pos_in + t.x));
+            const float3 pb = f3(__ldg(I.pos_in + t.y));
+            const float3 pc = f3(__ldg(I.pos_in + t.z));
+            const float3 area = 0.5f * cross(pb - pa, pc - pa);
+            f = f + (__uint_as_float(t.w) * area) / 3.0f;
+        }
+        v[i] = make_float4(f.x, f.y, f.z, 0.0f);
+    }
+    if (owner && tid == 0) pay = *I.payload_in;
+    __syncthreads();  // mbarrier initialised before any thread waits on it
+    if (!mbar_wait(&bar, 0, p.copy_budget)) {
+        atomicOr(I.status, kStatusCopyTimeout);
+        mbar_wait(&bar, 0, p.copy_budget);
+    }
+    // predict (soft_body.cpp:1536-1566)
+    for (uint32_t i = tid; i < n; i += blockDim.x) {
+        float4 X = x[i];
+        if (X.w == 0.0f) continue;
+        const float4 V0 = __ldg(I.vel_in + base + i);
+        const float4 F = v[i];
+        const float ax = p.gravity.x + F.x * X.w, ay = p.gravity.y + F.y * X.w, az = p.gravity.z + F.z * X.w;
+        const float vx = p.ref_velocity.x + ((V0.x + ax * p.dt) - p.ref_velocity.x) * p.damping;
+        const float vy = p.ref_velocity.y + ((V0.y + ay * p.dt) - p.ref_velocity.y) * p.damping;
+        const float vz = p.ref_velocity.z + ((V0.z + az * p.dt) - p.ref_velocity.z) * p.damping;
+        X.x += vx * p.dt;
+        X.y += vy * p.dt;
+        X.z += vz * p.dt;
+        x[i] = X;
+    }
+    if (owner && tid == 0) {
+        for (int k = 0; k < 8; ++k) pay.lambda[k] = 0.0f;
+        if (!payload_predict(*I.payload_def, pay, p.dt, p.gravity)) susp_fail(I.status, kSuspPayload);
+    }
+    cluster.sync();
+
+    // ---- constraint iterations ------------------------------------------------
+    // Stages of one iteration: distance colours then dihedral colours.  Each
+    // thread prefetches its first record of the next stage before it works
+    // on the current one, so the record fetch from L2 overlaps the current
+    // stage and its cluster barrier.
+    const int S0 = I.kind[0].stages, S1 = I.kind[1].stages, S = S0 + S1;
+    uint32_t* soff = reinterpret_cast<uint32_t*>(smem + p.smem_offsets);  // [S + 2]: stage starts, then ends
+    for (int i = tid; i <= S0; i += blockDim.x)
+        soff[i] = __ldg(I.kind[0].offsets + static_cast<size_t>(me) * (S0 + 1) + i);
+    for (int i = tid; i <= S1; i += blockDim.x)
+        soff[S0 + 1 + i] = __ldg(I.kind[1].offsets + static_cast<size_t>(me) * (S1 + 1) + i);
+    __syncthreads();
+    // global stage g -> (kind, [lo, hi)) with first = start of that kind's CTA list
+    auto stage_lo = [&](int g) { return g < S0 ? soff[g] : soff[S0 + 1 + (g - S0)]; };
+    auto stage_hi = [&](int g) { return g < S0 ? soff[g + 1] : soff[S0 + 2 + (g - S0)]; };
+    const uint32_t first0 = soff[0], first1 = soff[S0 + 1];
+    ClusterRecord next;
+    next.index = ~0u;
+    if (p.iterations > 0 && S > 0) next = load_record(I.kind[S0 > 0 ? 0 : 1], S0 > 0 ? 0 : 1, stage_lo(0) + tid,
+                                                      stage_hi(0));
+    for (int it = 0; it < p.iterations; ++it) {
+        for (int g = 0; g < S; ++g) {
+            const int kind = g < S0 ? 0 : 1;
+            const ClusterRecord cur = next;
+            // prefetch the next stage (wrapping to the next iteration)
+            const int gn = g + 1 < S ? g + 1 : 0;
+            const int kn = gn < S0 ? 0 : 1;
+            next = load_record(I.kind[kn], kn, stage_lo(gn) + tid, stage_hi(gn));
+            const uint32_t first = kind ? first1 : first0;
+            float* lam = kind ? lam1 : lam0;
+            if (cur.index != ~0u) apply_record(cur, kind, me, x, peers, lam, first, p.inv_dt2);
+            for (uint32_t i = stage_lo(g) + tid + blockDim.x; i < stage_hi(g); i += blockDim.x)
+                apply_record(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, x, peers, lam, first,
+                             p.inv_dt2);
+            cluster.sync();
+        }
+        if (I.susp_cta >= 0) {
+            if (owner && tid == 0) line_iteration(*I.payload_def, pay, x, p.dt, I.status);
+            cluster.sync();
+        }
+    }
+    // ---- final seam-stitch projections (soft_body.cpp:1389-1405) ----------
+    if (p.iterations > 0) {
+        for (int s = 0; s < I.seam_stages; ++s) {
+            const uint32_t* off = I.seam_offsets + static_cast<size_t>(me) * (I.seam_stages + 1);
+            for (uint32_t i = __ldg(off + s) + tid; i < __ldg(off + s + 1); i += blockDim.x) {
+                const uint32_t r = __ldg(I.seam_ab + i);
+                float4* pa = node_at(r & 0xffffu, me, x, peers);
+                float4* pb = node_at(r >> 16, me, x, peers);
+                float4 A = *pa, B = *pb;
+                float l = 0.0f;  // rigid stitch: alpha = 0
+                project_distance(A, B, 0.0f, 0.0f, l, p.inv_dt2);
+                *pa = A;
+                *pb = B;
+            }
+            cluster.sync();
+        }
+    }
+    // ---- finalize (soft_body.cpp:1568-1585) --------------------------------
+    for (uint32_t i = tid; i < n; i += blockDim.x) {
+        const float4 X = x[i];
+        float4 V = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (X.w != 0.0f) {
+            const float4 P = __ldg(I.pos_in + base + i);
+            V = make_float4((X.x - P.x) * p.inv_dt, (X.y - P.y) * p.inv_dt, (X.z - P.z) * p.inv_dt, 0.0f);
+        }
+        v[i] = V;
+    }
+    __syncthreads();
+    if (owner && tid == 0) {
+        payload_finish(*I.payload_def, pay, *I.payload_in, x, v, p.dt, I.status);
+        float3 s = make_float3(0.0f, 0.0f, 0.0f);
+        if (I.recentre && finite3(pay.com) &&
+            fmaxf(fabsf(pay.com.x), fmaxf(fabsf(pay.com.y), fabsf(pay.com.z))) > 0.25f)
+            s = make_float3(rintf(pay.com.x * 256.0f) / 256.0f, rintf(pay.com.y * 256.0f) / 256.0f,
+                            rintf(pay.com.z * 256.0f) / 256.0f);
+        shift_s = s;
+    }
+    if (I.susp_cta < 0 && tid == 0) shift_s = make_float3(0.0f, 0.0f, 0.0f);
+    cluster.sync();
+    float3 shift = shift_s;
+    if (I.susp_cta >= 0) shift = *cluster.map_shared_rank(&shift_s, I.susp_cta);
+    // ---- write the trial state --------------------------------------------
+    int bad = 0;
+    for (uint32_t i = tid; i < n; i += blockDim.x) {
+        float4 X = x[i];
+        float4 P = __ldg(I.pos_in + base + i);
+        const float4 V = v[i];
+        X.x -= shift.x; X.y -= shift.y; X.z -= shift.z;
+        P.x -= shift.x; P.y -= shift.y; P.z -= shift.z;
+        bad |= !(isfinite(X.x) && isfinite(X.y) && isfinite(X.z) && isfinite(V.x) && isfinite(V.y) && isfinite(V.z));
+        I.pos_out[base + i] = X;
+        I.prev_out[base + i] = P;
+        I.vel_out[base + i] = V;
+    }
+    if (__syncthreads_or(bad) && tid == 0) atomicOr(I.status, kStatusNonFinite);
+    if (owner && tid == 0) {
+        pay.com = pay.com - shift;
+        *I.payload_out = pay;
+    }
+    if (me == 0 && tid == 0) {
+        I.origin_out[0] = I.origin_in[0] + static_cast<double>(shift.x);
+        I.origin_out[1] = I.origin_in[1] + static_cast<double>(shift.y);
+        I.origin_out[2] = I.origin_in[2] + static_cast<double>(shift.z);
+    }
+    cluster.sync();  // no CTA leaves while a peer may still read its memory
+}
+
+}  // namespace dev
+}  // namespace swb

@@ -1,0 +1,232 @@
+// Host construction and checking of the cluster sweep schedule.
+#include "cluster_schedule.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+namespace swb {
+
+namespace {
+
+uint32_t make_ref(const ClusterSchedule& s, uint32_t node) {
+    const uint32_t slot = s.slot_of_node[node];
+    const uint32_t cta = static_cast<uint32_t>(
+        std::upper_bound(s.patch_begin.begin(), s.patch_begin.end(), slot) - s.patch_begin.begin() - 1);
+    return (cta << 12) | (slot - s.patch_begin[cta]);
+}
+
+}  // namespace
+
+bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes, int ctas,
+                            ClusterSchedule& S) {
+    S = ClusterSchedule{};
+    const uint32_t N = static_cast<uint32_t>(d.nodes.size());
+    ctas = std::clamp(ctas, 1, kClusterMaxCtas);
+    if (N == 0) ctas = 1;
+    S.ctas = ctas;
+    S.node_count = N;
+    const std::vector<int> part = bisect_nodes(d, suspension_nodes, ctas, 0.03);
+    S.patch_begin.assign(ctas + 1, 0);
+    for (uint32_t n = 0; n < N; ++n) ++S.patch_begin[part[n] + 1];
+    for (int c = 0; c < ctas; ++c) {
+        S.max_patch = std::max(S.max_patch, S.patch_begin[c + 1]);
+        S.patch_begin[c + 1] += S.patch_begin[c];
+    }
+    if (S.max_patch > kClusterPatchNodes) {
+        S = ClusterSchedule{};
+        return false;
+    }
+    S.node_of_slot.assign(N, 0);
+    S.slot_of_node.assign(N, 0);
+    {
+        std::vector<uint32_t> cur(S.patch_begin.begin(), S.patch_begin.end() - 1);
+        for (uint32_t n = 0; n < N; ++n) {
+            const uint32_t s = cur[part[n]]++;
+            S.node_of_slot[s] = n;
+            S.slot_of_node[n] = s;
+        }
+    }
+    if (!suspension_nodes.empty()) S.susp_cta = part[suspension_nodes[0]];
+
+    for (int k = 0; k < 2; ++k) {
+        ClusterKind& K = S.kinds[k];
+        const size_t m = k == 0 ? d.constraints.size() : d.dihedrals.size();
+        std::vector<std::array<uint32_t, 4>> nodes(m);
+        std::vector<int> counts(m, k == 0 ? 2 : 4);
+        for (size_t i = 0; i < m; ++i) {
+            if (k == 0)
+                nodes[i] = {static_cast<uint32_t>(d.constraints[i].first_node),
+                            static_cast<uint32_t>(d.constraints[i].second_node), 0, 0};
+            else
+                for (int q = 0; q < 4; ++q) nodes[i][q] = static_cast<uint32_t>(d.dihedrals[i].nodes[q]);
+        }
+        std::vector<int> colour;
+        const int stages = dsatur_colour(nodes, counts, colour);
+        K.stages = stages;
+        // executing CTA: owner of most of the constraint's nodes (ties: first)
+        std::vector<int> cta_of(m, 0);
+        for (size_t i = 0; i < m; ++i) {
+            int best = part[nodes[i][0]], best_count = 0;
+            for (int q = 0; q < counts[i]; ++q) {
+                int cnt = 0;
+                for (int r = 0; r < counts[i]; ++r) cnt += part[nodes[i][r]] == part[nodes[i][q]];
+                if (cnt > best_count) {
+                    best_count = cnt;
+                    best = part[nodes[i][q]];
+                }
+            }
+            cta_of[i] = best;
+        }
+        // records CTA-major, stage within, definition order within
+        std::vector<uint32_t> idx(m);
+        std::iota(idx.begin(), idx.end(), 0u);
+        std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+            if (cta_of[x] != cta_of[y]) return cta_of[x] < cta_of[y];
+            return colour[x] < colour[y];
+        });
+        K.offsets.assign(static_cast<size_t>(ctas) * (stages + 1), 0);
+        std::vector<uint32_t> count(static_cast<size_t>(ctas) * std::max(stages, 1), 0);
+        for (size_t i = 0; i < m; ++i) ++count[static_cast<size_t>(cta_of[i]) * stages + colour[i]];
+        uint32_t off = 0;
+        for (int c = 0; c < ctas; ++c) {
+            const uint32_t cta_start = off;
+            for (int s = 0; s < stages; ++s) {
+                K.offsets[static_cast<size_t>(c) * (stages + 1) + s] = off;
+                off += count[static_cast<size_t>(c) * stages + s];
+            }
+            K.offsets[static_cast<size_t>(c) * (stages + 1) + stages] = off;
+            K.max_cta_records = std::max(K.max_cta_records, off - cta_start);
+        }
+        for (uint32_t i : idx) {
+            K.ab.push_back(make_ref(S, nodes[i][0]) | (make_ref(S, nodes[i][1]) << 16));
+            if (k == 1) {
+                K.cd.push_back(make_ref(S, nodes[i][2]) | (make_ref(S, nodes[i][3]) << 16));
+                K.rest.push_back(static_cast<float>(d.dihedrals[i].rest_angle));
+                K.comp.push_back(static_cast<float>(d.dihedrals[i].compliance));
+            } else {
+                const auto& dc = d.constraints[i];
+                const bool stitch = dc.kind == SWB_CONSTRAINT_SEAM_STITCH;
+                K.rest.push_back(stitch ? 0.0f : static_cast<float>(dc.rest_length));
+                float cp = stitch ? 0.0f : static_cast<float>(dc.compliance);
+                if (dc.kind == SWB_CONSTRAINT_CABLE) cp = std::copysign(std::fabs(cp), -1.0f);
+                K.comp.push_back(cp);
+            }
+            K.def_index.push_back(i);
+        }
+        // sweep order: stage-major, CTA, record order
+        auto& order = k == 0 ? S.distance_order : S.dihedral_order;
+        for (int s = 0; s < stages; ++s)
+            for (int c = 0; c < ctas; ++c)
+                for (uint32_t r = K.offsets[static_cast<size_t>(c) * (stages + 1) + s];
+                     r < K.offsets[static_cast<size_t>(c) * (stages + 1) + s + 1]; ++r)
+                    order.push_back(K.def_index[r]);
+    }
+
+    // seam closing pass: level scheduling in sweep order, executing CTA =
+    // owner of the first node
+    {
+        std::vector<int32_t> node_stage(N, -1);
+        struct Rec { int stage, cta; uint64_t index; };
+        std::vector<Rec> recs;
+        for (uint64_t i : S.distance_order) {
+            const auto& c = d.constraints[i];
+            if (c.kind != SWB_CONSTRAINT_SEAM_STITCH) continue;
+            const int s = std::max(node_stage[c.first_node], node_stage[c.second_node]) + 1;
+            node_stage[c.first_node] = node_stage[c.second_node] = s;
+            recs.push_back({s, part[c.first_node], i});
+        }
+        S.seam_stages = 0;
+        for (const Rec& r : recs) S.seam_stages = std::max(S.seam_stages, r.stage + 1);
+        std::stable_sort(recs.begin(), recs.end(), [](const Rec& x, const Rec& y) {
+            if (x.cta != y.cta) return x.cta < y.cta;
+            return x.stage < y.stage;
+        });
+        S.seam_offsets.assign(static_cast<size_t>(ctas) * (S.seam_stages + 1), 0);
+        size_t at = 0;
+        for (int c = 0; c < ctas; ++c) {
+            for (int s = 0; s <= S.seam_stages; ++s) {
+                while (at < recs.size() && recs[at].cta == c && recs[at].stage < s) ++at;
+                S.seam_offsets[static_cast<size_t>(c) * (S.seam_stages + 1) + s] = static_cast<uint32_t>(at);
+            }
+            while (at < recs.size() && recs[at].cta == c) ++at;
+        }
+        for (const Rec& r : recs) {
+            const auto& c = d.constraints[r.index];
+            S.seam_ab.push_back(make_ref(S, static_cast<uint32_t>(c.first_node)) |
+                                (make_ref(S, static_cast<uint32_t>(c.second_node)) << 16));
+        }
+    }
+    return true;
+}
+
+void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes,
+                             const ClusterSchedule& S) {
+    auto fail = [](const std::string& what) { raise(SWB_INVALID_ARGUMENT, "cluster schedule invariant: " + what); };
+    const uint32_t N = static_cast<uint32_t>(d.nodes.size());
+    const int C = S.ctas;
+    if (C < 1 || C > kClusterMaxCtas) fail("cta count");
+    if (S.patch_begin.size() != static_cast<size_t>(C) + 1 || S.patch_begin[C] != N) fail("patch ranges");
+    for (uint32_t n = 0; n < N; ++n)
+        if (S.node_of_slot[S.slot_of_node[n]] != n) fail("slot map");
+    auto node_of_ref = [&](uint32_t ref) {
+        const uint32_t cta = ref >> 12, local = ref & 0xfffu;
+        if (static_cast<int>(cta) >= C || S.patch_begin[cta] + local >= S.patch_begin[cta + 1])
+            fail("reference outside its patch");
+        return S.node_of_slot[S.patch_begin[cta] + local];
+    };
+    for (uint32_t n : suspension_nodes) {
+        const uint32_t slot = S.slot_of_node[n];
+        if (slot < S.patch_begin[S.susp_cta] || slot >= S.patch_begin[S.susp_cta + 1])
+            fail("suspension node outside the owner patch");
+    }
+    std::vector<int64_t> stamp(N, -1);
+    int64_t epoch = 0;
+    for (int k = 0; k < 2; ++k) {
+        const ClusterKind& K = S.kinds[k];
+        const size_t m = k == 0 ? d.constraints.size() : d.dihedrals.size();
+        std::vector<uint8_t> seen(m, 0);
+        for (int s = 0; s < K.stages; ++s) {
+            ++epoch;
+            for (int c = 0; c < C; ++c)
+                for (uint32_t r = K.offsets[static_cast<size_t>(c) * (K.stages + 1) + s];
+                     r < K.offsets[static_cast<size_t>(c) * (K.stages + 1) + s + 1]; ++r) {
+                    const uint32_t i = K.def_index[r];
+                    if (seen[i]++) fail("constraint scheduled twice");
+                    uint32_t refs[4] = {K.ab[r] & 0xffffu, K.ab[r] >> 16, 0, 0};
+                    uint32_t want[4];
+                    int cnt = 2;
+                    if (k == 0) {
+                        want[0] = static_cast<uint32_t>(d.constraints[i].first_node);
+                        want[1] = static_cast<uint32_t>(d.constraints[i].second_node);
+                    } else {
+                        refs[2] = K.cd[r] & 0xffffu;
+                        refs[3] = K.cd[r] >> 16;
+                        cnt = 4;
+                        for (int q = 0; q < 4; ++q) want[q] = static_cast<uint32_t>(d.dihedrals[i].nodes[q]);
+                    }
+                    for (int q = 0; q < cnt; ++q) {
+                        const uint32_t n = node_of_ref(refs[q]);
+                        if (n != want[q]) fail("reference does not name the constraint's node");
+                        if (stamp[n] == epoch) fail("stage is not node-disjoint");
+                        stamp[n] = epoch;
+                    }
+                }
+        }
+        for (size_t i = 0; i < m; ++i)
+            if (!seen[i]) fail("constraint not scheduled");
+    }
+    for (int s = 0; s < S.seam_stages; ++s) {
+        ++epoch;
+        for (int c = 0; c < C; ++c)
+            for (uint32_t r = S.seam_offsets[static_cast<size_t>(c) * (S.seam_stages + 1) + s];
+                 r < S.seam_offsets[static_cast<size_t>(c) * (S.seam_stages + 1) + s + 1]; ++r)
+                for (uint32_t ref : {S.seam_ab[r] & 0xffffu, S.seam_ab[r] >> 16}) {
+                    const uint32_t n = node_of_ref(ref);
+                    if (stamp[n] == epoch) fail("seam stage is not node-disjoint");
+                    stamp[n] = epoch;
+                }
+    }
+}
+
+}  // namespace swb

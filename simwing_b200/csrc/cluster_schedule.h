@@ -1,0 +1,75 @@
+// Cluster sweep schedule: one thread-block cluster solves one structure.
+//
+// The nodes are split into one patch per CTA of the cluster (recursive
+// bisection, suspension endpoint nodes kept together) and live in that
+// CTA's shared memory for the whole step.  Each constraint kind is
+// coloured over the whole mesh (DSatur); a colour is one stage, and every
+// constraint of a stage is executed by the CTA that owns most of its nodes,
+// reaching nodes of other CTAs through distributed shared memory.  A
+// cluster barrier separates stages.  Node references are 16-bit: the owner
+// rank in the top 4 bits and the index in its patch in the low 12 bits.
+//
+// Sweep order per kind: stage-major, then CTA rank, then record order --
+// the reference serial solver run on the definition permuted into this
+// order performs exactly the device sweep (constraints of one stage share
+// no node).
+#pragma once
+
+#include "common.h"
+
+#include <array>
+#include <cstdint>
+#include <vector>
+
+namespace swb {
+
+constexpr int kClusterMaxCtas = 16;
+constexpr uint32_t kClusterPatchNodes = 4096;
+
+struct ClusterKind {
+    int stages = 0;
+    // [ctas * (stages + 1)]: record offsets of (cta, stage); records are
+    // stored CTA-major, stage within.
+    std::vector<uint32_t> offsets;
+    std::vector<uint32_t> ab;    // ref(a) | ref(b) << 16
+    std::vector<uint32_t> cd;    // dihedral: ref(c) | ref(d) << 16
+    std::vector<float> rest;
+    std::vector<float> comp;     // distance: sign bit = cable
+    std::vector<uint32_t> def_index;
+    uint32_t max_cta_records = 0;  // multipliers held in shared memory per CTA
+};
+
+struct ClusterSchedule {
+    int ctas = 0;
+    uint32_t node_count = 0;
+    std::vector<uint32_t> node_of_slot, slot_of_node;  // slots: patch-major
+    std::vector<uint32_t> patch_begin;                 // [ctas + 1]
+    uint32_t max_patch = 0;
+    std::array<ClusterKind, 2> kinds;
+    // seam closing pass: level-scheduled in sweep order, per (cta, stage)
+    int seam_stages = 0;
+    std::vector<uint32_t> seam_offsets;  // [ctas * (seam_stages + 1)]
+    std::vector<uint32_t> seam_ab;
+    int susp_cta = -1;
+    std::vector<uint64_t> distance_order, dihedral_order;
+};
+
+// Returns false (and leaves `out` empty) when the mesh does not fit one
+// cluster of `ctas` CTAs (a patch over kClusterPatchNodes nodes).
+bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes, int ctas,
+                            ClusterSchedule& out);
+
+// Checks the invariants the cluster kernel relies on; raises on failure.
+void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes,
+                             const ClusterSchedule& s);
+
+// Colouring helper shared with the grid schedule: DSatur over constraints
+// given as node lists (2 or 4 nodes), conflicts = shared nodes.
+int dsatur_colour(const std::vector<std::array<uint32_t, 4>>& nodes, const std::vector<int>& counts,
+                  std::vector<int>& colour);
+
+// Recursive coordinate bisection of nodes into `parts` (see schedule.cpp).
+std::vector<int> bisect_nodes(const OwnedDefinition& d, const std::vector<uint32_t>& grouped_nodes, int parts,
+                              double tolerance);
+
+}  // namespace swb

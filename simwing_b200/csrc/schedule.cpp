@@ -1,5 +1,6 @@
 // Host construction of the device sweep schedule (see schedule.h).
 #include "schedule.h"
+#include "cluster_schedule.h"
 
 #include <algorithm>
 #include <cstring>
@@ -195,6 +196,74 @@ int dsatur(const std::vector<const Constraint*>& cons, std::vector<int>& colour)
 
 }  // namespace
 
+// Node partition into `parts` by cut-minimising recursive coordinate
+// bisection; `grouped_nodes` form one item that is never split.  Item
+// weight = 1 + half the number of constraint incidences (work proxy).
+std::vector<int> bisect_nodes(const OwnedDefinition& d, const std::vector<uint32_t>& grouped_nodes, int parts,
+                              double tolerance) {
+    const uint32_t N = static_cast<uint32_t>(d.nodes.size());
+    std::vector<uint32_t> incidence(N, 0);
+    for (const auto& c : d.constraints) {
+        ++incidence[c.first_node];
+        ++incidence[c.second_node];
+    }
+    for (const auto& h : d.dihedrals)
+        for (uint64_t n : h.nodes) ++incidence[n];
+    std::vector<uint32_t> item_of(N);
+    std::vector<std::array<double, 3>> ipos;
+    std::vector<double> iweight;
+    std::vector<uint8_t> grouped(N, 0);
+    for (uint32_t n : grouped_nodes) grouped[n] = 1;
+    int32_t group = -1;
+    std::array<double, 3> gsum{0, 0, 0};
+    double gw = 0.0;
+    uint32_t gcount = 0;
+    for (uint32_t n = 0; n < N; ++n) {
+        const auto& p = d.nodes[n].position;
+        const double w = 1.0 + 0.5 * incidence[n];
+        if (grouped[n]) {
+            if (group < 0) {
+                group = static_cast<int32_t>(ipos.size());
+                ipos.push_back({0, 0, 0});
+                iweight.push_back(0);
+            }
+            item_of[n] = static_cast<uint32_t>(group);
+            gsum[0] += p.x; gsum[1] += p.y; gsum[2] += p.z;
+            gw += w;
+            ++gcount;
+        } else {
+            item_of[n] = static_cast<uint32_t>(ipos.size());
+            ipos.push_back({p.x, p.y, p.z});
+            iweight.push_back(w);
+        }
+    }
+    if (group >= 0) {
+        ipos[group] = {gsum[0] / gcount, gsum[1] / gcount, gsum[2] / gcount};
+        iweight[group] = gw;
+    }
+    std::vector<std::vector<uint32_t>> cons_items;
+    cons_items.reserve(d.constraints.size() + d.dihedrals.size());
+    for (const auto& c : d.constraints)
+        cons_items.push_back({item_of[c.first_node], item_of[c.second_node]});
+    for (const auto& h : d.dihedrals)
+        cons_items.push_back({item_of[h.nodes[0]], item_of[h.nodes[1]], item_of[h.nodes[2]], item_of[h.nodes[3]]});
+    const std::vector<int> item_part = Bisector(ipos, iweight, cons_items, tolerance).run(parts);
+    std::vector<int> part(N);
+    for (uint32_t n = 0; n < N; ++n) part[n] = item_part[item_of[n]];
+    return part;
+}
+
+int dsatur_colour(const std::vector<std::array<uint32_t, 4>>& nodes, const std::vector<int>& counts,
+                  std::vector<int>& colour) {
+    std::vector<Constraint> cons(nodes.size());
+    std::vector<const Constraint*> ptrs(nodes.size());
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        cons[i] = {{nodes[i][0], nodes[i][1], nodes[i][2], nodes[i][3]}, counts[i], static_cast<uint32_t>(i)};
+        ptrs[i] = &cons[i];
+    }
+    return dsatur(ptrs, colour);
+}
+
 Schedule build_schedule(const OwnedDefinition& d,
                         const std::vector<uint32_t>& suspension_nodes,
                         const ScheduleOptions& opt) {
@@ -219,55 +288,8 @@ Schedule build_schedule(const OwnedDefinition& d,
                           4, i});
     }
 
-    // ---- level 1: node partition over items (suspension nodes grouped) ----
-    std::vector<uint32_t> item_of(N);
-    std::vector<std::array<double, 3>> ipos;
-    std::vector<double> iweight;
-    std::vector<uint32_t> incidence(N, 0);
-    for (int k = 0; k < kKinds; ++k)
-        for (const Constraint& c : all[k])
-            for (int q = 0; q < c.count; ++q) ++incidence[c.n[q]];
-    {
-        std::vector<uint8_t> is_susp(N, 0);
-        for (uint32_t n : suspension_nodes) is_susp[n] = 1;
-        int32_t group = -1;
-        std::array<double, 3> gsum{0, 0, 0};
-        double gw = 0.0;
-        uint32_t gcount = 0;
-        for (uint32_t n = 0; n < N; ++n) {
-            const auto& p = d.nodes[n].position;
-            const double w = 1.0 + 0.5 * incidence[n];
-            if (is_susp[n]) {
-                if (group < 0) {
-                    group = static_cast<int32_t>(ipos.size());
-                    ipos.push_back({0, 0, 0});
-                    iweight.push_back(0);
-                }
-                item_of[n] = static_cast<uint32_t>(group);
-                gsum[0] += p.x; gsum[1] += p.y; gsum[2] += p.z;
-                gw += w;
-                ++gcount;
-            } else {
-                item_of[n] = static_cast<uint32_t>(ipos.size());
-                ipos.push_back({p.x, p.y, p.z});
-                iweight.push_back(w);
-            }
-        }
-        if (group >= 0) {
-            ipos[group] = {gsum[0] / gcount, gsum[1] / gcount, gsum[2] / gcount};
-            iweight[group] = gw;
-        }
-    }
-    std::vector<std::vector<uint32_t>> cons_items;
-    for (int k = 0; k < kKinds; ++k)
-        for (const Constraint& c : all[k]) {
-            std::vector<uint32_t> it;
-            for (int q = 0; q < c.count; ++q) it.push_back(item_of[c.n[q]]);
-            cons_items.push_back(std::move(it));
-        }
-    std::vector<int> item_part = Bisector(ipos, iweight, cons_items, opt.balance_tolerance).run(G);
-    std::vector<int> part1(N);
-    for (uint32_t n = 0; n < N; ++n) part1[n] = item_part[item_of[n]];
+    // ---- level 1: node partition (suspension nodes grouped) ---------------
+    const std::vector<int> part1 = bisect_nodes(d, suspension_nodes, G, opt.balance_tolerance);
 
     // Slots: level-1 part-major, node index within.
     S.l1_begin.assign(G + 1, 0);
@@ -696,6 +718,38 @@ extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definiti
         OwnedDefinition def;
         def.assign(*definition);
         validate_definition(def.view);
+        if (!(options && (options->flags & (SWB_OPT_GRID | SWB_OPT_GLOBAL_ONLY)))) {
+            // Same choice as swb_structure_create, with the B200 opt-in
+            // shared-memory budget (227 KB).
+            const std::vector<uint32_t> susp = suspension_endpoint_nodes(def);
+            const uint64_t N = def.nodes.size();
+            int c = options && options->cluster_ctas > 0 ? options->cluster_ctas : 1;
+            if (!(options && options->cluster_ctas > 0))
+                while (c < kClusterMaxCtas && static_cast<uint64_t>(c) * 2048 < N) c *= 2;
+            const int last = options && options->cluster_ctas > 0 ? c : kClusterMaxCtas;
+            for (; c <= last; c *= 2) {
+                ClusterSchedule C;
+                if (!build_cluster_schedule(def, susp, c, C)) continue;
+                const size_t bytes = C.max_patch * 32ull + C.kinds[0].max_cta_records * 4ull +
+                                     C.kinds[1].max_cta_records * 4ull +
+                                     (C.kinds[0].stages + C.kinds[1].stages + 2) * 4ull + 64;
+                if (bytes > 227 * 1024 - 2048) continue;
+                verify_cluster_schedule(def, susp, C);
+                std::memset(out, 0, sizeof(*out));
+                out->blocks = C.ctas;
+                out->cluster_ctas = C.ctas;
+                out->local_stages_per_iteration = C.kinds[0].stages + C.kinds[1].stages;
+                out->cluster_barriers_per_iteration = C.kinds[0].stages + C.kinds[1].stages + (C.susp_cta >= 0);
+                out->max_patch_nodes = static_cast<int32_t>(C.max_patch);
+                out->shared_bytes = static_cast<int32_t>(bytes);
+                out->level_constraints[0] = def.constraints.size() + def.dihedrals.size();
+                if (distance_order) std::copy(C.distance_order.begin(), C.distance_order.end(), distance_order);
+                if (dihedral_order) std::copy(C.dihedral_order.begin(), C.dihedral_order.end(), dihedral_order);
+                return;
+            }
+            if (options && options->cluster_ctas > 0)
+                raise(SWB_UNSUPPORTED, "the mesh does not fit the requested cluster");
+        }
         ScheduleOptions so;
         so.blocks = options && options->blocks > 0 ? options->blocks : 148;
         so.blocks = static_cast<int>(std::min<uint64_t>(so.blocks, std::max<uint64_t>(1, def.nodes.size())));

@@ -2,6 +2,7 @@
 // Replaces simwing::fsi::Structure (src/fsi/structure.h:273-309).
 #include "common.h"
 #include "schedule.h"
+#include "cluster_kernel.cuh"
 #include "step_kernel.cuh"
 #include "structure_impl.h"
 
@@ -142,35 +143,83 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     if (def.has_suspension && (def.segments.size() > 8 || def.harness.size() > 8))
         raise(SWB_UNSUPPORTED, "more than 8 suspension segments or harness points");
     const std::vector<uint32_t> susp_nodes = suspension_endpoint_nodes(def);
-    ScheduleOptions so;
-    so.blocks = opt.blocks > 0 ? opt.blocks : sm_count;
-    so.blocks = static_cast<int>(std::min<uint64_t>(so.blocks, std::max<uint64_t>(1, N)));
-    so.levels = opt.partition_levels > 0 ? opt.partition_levels : 3;
-    so.global_only = (opt.flags & SWB_OPT_GLOBAL_ONLY) != 0;
-    sched = build_schedule(def, susp_nodes, so);
-    verify_schedule(def, susp_nodes, sched);
-    G = sched.blocks;
-
-    // Threads per CTA: enough for the widest local stage, in warps.
+    const size_t smem_limit = prop.sharedMemPerBlockOptin > 2048 ? prop.sharedMemPerBlockOptin - 2048 : 0;
+    cluster_mode = false;
+    if (!(opt.flags & (SWB_OPT_GRID | SWB_OPT_GLOBAL_ONLY))) {
+        if (opt.cluster_ctas < 0 || opt.cluster_ctas > kClusterMaxCtas)
+            raise(SWB_INVALID_ARGUMENT, "cluster_ctas must be in 0..16");
+        std::vector<int> candidates;
+        if (opt.cluster_ctas > 0) {
+            candidates.push_back(opt.cluster_ctas);
+        } else {
+            int c = 1;
+            while (c < kClusterMaxCtas && static_cast<uint64_t>(c) * 2048 < N) c *= 2;
+            for (; c <= kClusterMaxCtas; c *= 2) candidates.push_back(c);
+        }
+        for (int c : candidates) {
+            if (!build_cluster_schedule(def, susp_nodes, c, csched)) continue;
+            const size_t bytes = csched.max_patch * 32ull + csched.kinds[0].max_cta_records * 4ull +
+                                 csched.kinds[1].max_cta_records * 4ull +
+                                 (csched.kinds[0].stages + csched.kinds[1].stages + 2) * 4ull + 64;
+            if (bytes > smem_limit) continue;
+            cluster_mode = true;
+            break;
+        }
+        if (!cluster_mode && opt.cluster_ctas > 0)
+            raise(SWB_UNSUPPORTED, "the mesh does not fit a cluster of " + std::to_string(opt.cluster_ctas) + " CTAs");
+    }
     uint32_t widest = 32;
-    for (int l = 0; l < sched.levels; ++l)
-        for (int k = 0; k < kKinds; ++k) {
-            const Table& t = sched.tables[l][k];
-            for (int b = 0; b < G; ++b)
-                for (int s = 0; s < t.stages; ++s) {
-                    const size_t o = static_cast<size_t>(b) * (t.stages + 1) + s;
-                    widest = std::max(widest, t.stage_offsets[o + 1] - t.stage_offsets[o]);
+    if (cluster_mode) {
+        verify_cluster_schedule(def, susp_nodes, csched);
+        G = csched.ctas;
+        slot_of_node = csched.slot_of_node;
+        node_of_slot = csched.node_of_slot;
+        susp_owner = csched.susp_cta;
+        susp_base = susp_owner >= 0 ? csched.patch_begin[susp_owner] : 0;
+        for (int k = 0; k < 2; ++k) {
+            const ClusterKind& K = csched.kinds[k];
+            for (int c = 0; c < G; ++c)
+                for (int s = 0; s < K.stages; ++s) {
+                    const size_t o = static_cast<size_t>(c) * (K.stages + 1) + s;
+                    widest = std::max(widest, K.offsets[o + 1] - K.offsets[o]);
                 }
         }
-    threads = opt.block_threads > 0 ? opt.block_threads
-                                    : static_cast<int>(std::clamp<uint32_t>((widest + 31) / 32 * 32, 64, 512));
-    if (threads % 32 != 0 || threads < 32 || threads > 1024) raise(SWB_INVALID_ARGUMENT, "block_threads");
+    } else {
+        ScheduleOptions so;
+        so.blocks = opt.blocks > 0 ? opt.blocks : sm_count;
+        so.blocks = static_cast<int>(std::min<uint64_t>(so.blocks, std::max<uint64_t>(1, N)));
+        so.levels = opt.partition_levels > 0 ? opt.partition_levels : 3;
+        so.global_only = (opt.flags & SWB_OPT_GLOBAL_ONLY) != 0;
+        sched = build_schedule(def, susp_nodes, so);
+        verify_schedule(def, susp_nodes, sched);
+        G = sched.blocks;
+        slot_of_node = sched.slot_of_node;
+        node_of_slot = sched.node_of_slot;
+        susp_owner = sched.suspension_block;
+        susp_base = susp_owner >= 0 ? sched.l1_begin[susp_owner] : 0;
+        // Threads per CTA: enough for the widest local stage, in warps.
+        for (int l = 0; l < sched.levels; ++l)
+            for (int k = 0; k < kKinds; ++k) {
+                const Table& t = sched.tables[l][k];
+                for (int b = 0; b < G; ++b)
+                    for (int s = 0; s < t.stages; ++s) {
+                        const size_t o = static_cast<size_t>(b) * (t.stages + 1) + s;
+                        widest = std::max(widest, t.stage_offsets[o + 1] - t.stage_offsets[o]);
+                    }
+            }
+    }
+    threads = opt.block_threads > 0
+                  ? opt.block_threads
+                  : static_cast<int>(std::clamp<uint32_t>((widest + 31) / 32 * 32, 64,
+                                                          cluster_mode ? dev::kClusterMaxThreads : 512));
+    if (threads % 32 != 0 || threads < 32 || threads > (cluster_mode ? dev::kClusterMaxThreads : 1024))
+        raise(SWB_INVALID_ARGUMENT, "block_threads out of range for the chosen schedule");
 
     // ---- device images -------------------------------------------------------
     // nodes (slot order)
     std::vector<float4> pos(N), vel(N, make_float4(0, 0, 0, 0));
     for (uint64_t s = 0; s < N; ++s) {
-        const swb_node_def& n = def.nodes[sched.node_of_slot[s]];
+        const swb_node_def& n = def.nodes[node_of_slot[s]];
         const float w = n.fixed ? 0.0f : static_cast<float>(1.0 / n.mass);
         pos[s] = make_float4(static_cast<float>(n.position.x), static_cast<float>(n.position.y),
                              static_cast<float>(n.position.z), w);
@@ -191,6 +240,46 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     std::memset(&p, 0, sizeof(p));
     upload_pressure();  // fills params.tri*, so after the reset above
     p.blocks = G;
+    if (cluster_mode) {
+        upload_cluster_tables();
+    } else {
+        upload_grid_tables();
+    }
+    finish_build(opt, prop);
+}
+
+void StructureImpl::upload_cluster_tables() {
+    ClusterParams& cp = cparams;
+    std::memset(&cp, 0, sizeof(cp));
+    cp.ctas = G;
+    uint32_t off = 0;
+    cp.smem_x = off; off = align16(off + csched.max_patch * 16u);
+    cp.smem_v = off; off = align16(off + csched.max_patch * 16u);
+    ClusterInstance base{};
+    base.patch_begin = dupload(owned, csched.patch_begin, stream);
+    for (int k = 0; k < 2; ++k) {
+        const ClusterKind& K = csched.kinds[k];
+        ClusterKindDev& dk = base.kind[k];
+        dk.offsets = dupload(owned, K.offsets, stream);
+        dk.ab = dupload(owned, K.ab, stream);
+        dk.cd = k == 1 ? dupload(owned, K.cd, stream) : dk.ab;
+        dk.rest = dupload(owned, K.rest, stream);
+        dk.comp = dupload(owned, K.comp, stream);
+        dk.stages = K.stages;
+        dk.smem_lambda = off;
+        off = align16(off + K.max_cta_records * 4u);
+    }
+    cp.smem_offsets = off;
+    off = align16(off + (csched.kinds[0].stages + csched.kinds[1].stages + 2) * 4u);
+    cluster_smem = off;
+    base.seam_offsets = dupload(owned, csched.seam_offsets, stream);
+    base.seam_ab = dupload(owned, csched.seam_ab, stream);
+    base.seam_stages = csched.seam_stages;
+    cluster_base = base;
+}
+
+void StructureImpl::upload_grid_tables() {
+    StepParams& p = params;
     p.levels = sched.levels;
     p.l1_begin = dupload(owned, sched.l1_begin, stream);
     uint32_t off = 0;
@@ -252,15 +341,19 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     p.seam_stages = sched.seam_stage_offsets.empty() ? 0 : static_cast<int>(sched.seam_stage_offsets.size()) - 1;
     p.seam_a = dupload(owned, sched.seam_a, stream);
     p.seam_b = dupload(owned, sched.seam_b, stream);
+}
 
+void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDeviceProp& prop) {
+    StepParams& p = params;
+    (void)prop;
     // diagnostics arrays (definition order of distance-like constraints)
     {
         std::vector<uint32_t> a(def.constraints.size()), b(def.constraints.size());
         std::vector<float> rest(def.constraints.size());
         std::vector<uint8_t> kind(def.constraints.size());
         for (size_t i = 0; i < def.constraints.size(); ++i) {
-            a[i] = sched.slot_of_node[def.constraints[i].first_node];
-            b[i] = sched.slot_of_node[def.constraints[i].second_node];
+            a[i] = slot_of_node[def.constraints[i].first_node];
+            b[i] = slot_of_node[def.constraints[i].second_node];
             rest[i] = static_cast<float>(def.constraints[i].rest_length);
             kind[i] = static_cast<uint8_t>(def.constraints[i].kind);
         }
@@ -277,8 +370,8 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     DevPayloadState pstate{};
     if (def.has_suspension) {
         const swb_suspension_def& s = def.suspension;
-        p.susp_block = sched.suspension_block;
-        const uint32_t sbase = sched.l1_begin[sched.suspension_block];
+        p.susp_block = susp_owner;
+        const uint32_t sbase = susp_base;
         pdef.mass = static_cast<float>(s.pilot_mass);
         pdef.com_local = make_float3(s.pilot_com_local.x, s.pilot_com_local.y, s.pilot_com_local.z);
         pdef.inertia = make_float3(s.pilot_principal_inertia.x, s.pilot_principal_inertia.y,
@@ -307,11 +400,11 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
                 if (ends[e]->kind == SWB_ENDPOINT_SURFACE_ATTACHMENT) {
                     for (const auto& a : def.attachments)
                         if (a.stable_id == ends[e]->stable_id)
-                            node[e] = static_cast<int>(sched.slot_of_node[a.node] - sbase);
+                            node[e] = static_cast<int>(slot_of_node[a.node] - sbase);
                 } else if (ends[e]->kind == SWB_ENDPOINT_JUNCTION) {
                     for (const auto& j : def.junctions)
                         if (j.stable_id == ends[e]->stable_id)
-                            node[e] = static_cast<int>(sched.slot_of_node[j.node] - sbase);
+                            node[e] = static_cast<int>(slot_of_node[j.node] - sbase);
                 } else if (ends[e]->kind == SWB_ENDPOINT_PILOT_HARNESS) {
                     for (size_t i = 0; i < horder.size(); ++i)
                         if (def.harness[horder[i]].stable_id == ends[e]->stable_id) point[e] = static_cast<int>(i);
@@ -367,16 +460,61 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     // so a CTA never leaves with bulk copies still in flight.
     p.copy_budget = 4000000000LL;
 
-    // launch feasibility
-    cuda_check(cudaFuncSetAttribute(dev::xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(p.smem_total)),
-               "shared memory request (mesh patch too large for the block count)");
-    int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::xpbd_step_kernel, threads, p.smem_total),
-               "occupancy");
-    if (per_sm * sm_count < G)
-        raise(SWB_UNSUPPORTED, "persistent grid of " + std::to_string(G) + " CTAs is not co-resident (" +
-                                   std::to_string(per_sm) + " per SM)");
+    if (cluster_mode) {
+        // One instance record per (input, output) buffer pair so a launch
+        // only selects a pointer.
+        std::vector<ClusterInstance> inst(9);
+        for (int in = 0; in < 3; ++in)
+            for (int out = 0; out < 3; ++out) {
+                ClusterInstance c = cluster_base;
+                c.pos_in = d_pos[in]; c.vel_in = d_vel[in];
+                c.pos_out = d_pos[out]; c.vel_out = d_vel[out]; c.prev_out = d_prev[out];
+                c.force = d_force;
+                c.tri_offsets = d_tri_off; c.tri_list = d_tri_list; c.tri = d_tri;
+                c.susp_cta = def.has_suspension ? susp_owner : -1;
+                c.payload_def = d_payload_def;
+                c.payload_in = d_payload[in]; c.payload_out = d_payload[out];
+                c.origin_in = d_origin[in]; c.origin_out = d_origin[out];
+                c.status = d_control->status;
+                c.recentre = def.has_suspension ? 1 : 0;
+                inst[in * 3 + out] = c;
+            }
+        d_instances = dupload(owned, inst, stream);
+        cparams.copy_budget = 4000000000LL;
+        cuda_check(cudaFuncSetAttribute(dev::xpbd_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(cluster_smem)),
+                   "shared memory request of the cluster schedule");
+        if (G > 8)
+            cuda_check(cudaFuncSetAttribute(dev::xpbd_cluster_kernel,
+                                            cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+                       "non-portable cluster size");
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = static_cast<unsigned>(G);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(G);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = cluster_smem;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        cuda_check(cudaOccupancyMaxActiveClusters(&clusters, dev::xpbd_cluster_kernel, &cfg), "cluster occupancy");
+        if (clusters < 1) raise(SWB_UNSUPPORTED, "a cluster of " + std::to_string(G) + " CTAs cannot be scheduled");
+    } else {
+        // launch feasibility of the cooperative grid
+        cuda_check(cudaFuncSetAttribute(dev::xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(p.smem_total)),
+                   "shared memory request (mesh patch too large for the block count)");
+        int per_sm = 0;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::xpbd_step_kernel, threads,
+                                                                 p.smem_total),
+                   "occupancy");
+        if (per_sm * sm_count < G)
+            raise(SWB_UNSUPPORTED, "persistent grid of " + std::to_string(G) + " CTAs is not co-resident (" +
+                                       std::to_string(per_sm) + " per SM)");
+    }
     cuda_check(cudaStreamSynchronize(stream), "upload");
 }
 
@@ -387,17 +525,17 @@ void StructureImpl::upload_pressure() {
     for (size_t t = 0; t < def.triangles.size(); ++t) {
         const auto& tr = def.triangles[t];
         const float pr = static_cast<float>(pressure[t]);
-        tri[t] = make_uint4(sched.slot_of_node[tr.nodes[0]], sched.slot_of_node[tr.nodes[1]],
-                            sched.slot_of_node[tr.nodes[2]], std::bit_cast<uint32_t>(pr));
+        tri[t] = make_uint4(slot_of_node[tr.nodes[0]], slot_of_node[tr.nodes[1]],
+                            slot_of_node[tr.nodes[2]], std::bit_cast<uint32_t>(pr));
         if (pressure[t] == 0.0) continue;
-        for (int k = 0; k < 3; ++k) ++off[sched.slot_of_node[tr.nodes[k]] + 1];
+        for (int k = 0; k < 3; ++k) ++off[slot_of_node[tr.nodes[k]] + 1];
     }
     for (uint64_t s = 0; s < N; ++s) off[s + 1] += off[s];
     list.resize(off[N]);
     std::vector<uint32_t> cur(off.begin(), off.end() - 1);
     for (size_t t = 0; t < def.triangles.size(); ++t) {
         if (pressure[t] == 0.0) continue;
-        for (int k = 0; k < 3; ++k) list[cur[sched.slot_of_node[def.triangles[t].nodes[k]]]++] = static_cast<uint32_t>(t);
+        for (int k = 0; k < 3; ++k) list[cur[slot_of_node[def.triangles[t].nodes[k]]]++] = static_cast<uint32_t>(t);
     }
     if (d_tri) { cudaFree(d_tri); cudaFree(d_tri_off); cudaFree(d_tri_list); owned.erase(std::remove_if(owned.begin(), owned.end(), [&](void* q) { return q == d_tri || q == d_tri_off || q == d_tri_list; }), owned.end()); }
     d_tri = dupload(owned, tri, stream);
@@ -413,7 +551,7 @@ void StructureImpl::upload_forces() {
     const uint64_t N = def.nodes.size();
     for (uint64_t n = 0; n < N; ++n) {
         const swb_vec3& f = pending[n];
-        h_force[sched.slot_of_node[n]] =
+        h_force[slot_of_node[n]] =
             make_float4(static_cast<float>(f.x), static_cast<float>(f.y), static_cast<float>(f.z), 0.0f);
     }
     cuda_check(cudaMemcpyAsync(d_force, h_force, N * sizeof(float4), cudaMemcpyHostToDevice, stream), "force upload");
@@ -456,8 +594,37 @@ void check_params(const StepParams& p) {
 }
 
 void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out) {
-    StepParams p = params;
     const double dt = st.time_step / st.substeps;
+    if (cluster_mode) {
+        ClusterParams cp = cparams;
+        cp.instances = d_instances + in * 3 + out;
+        cp.ctas = G;
+        cp.dt = static_cast<float>(dt);
+        cp.inv_dt = static_cast<float>(1.0 / dt);
+        cp.inv_dt2 = static_cast<float>(1.0 / (dt * dt));
+        cp.damping = static_cast<float>(std::exp(-st.velocity_damping * dt));
+        cp.gravity = make_float3(st.gravity.x, st.gravity.y, st.gravity.z);
+        cp.ref_velocity = make_float3(st.damping_reference_velocity.x, st.damping_reference_velocity.y,
+                                      st.damping_reference_velocity.z);
+        cp.iterations = st.constraint_iterations;
+        if (!cp.instances || in == out) raise(SWB_CUDA_ERROR, "internal error: cluster instance table");
+        cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = static_cast<unsigned>(G);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(G);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = cluster_smem;
+        cfg.stream = stream;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cuda_check(cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_kernel, cp), "cudaLaunchKernelEx (cluster)");
+        return;
+    }
+    StepParams p = params;
     p.pos_in = d_pos[in]; p.vel_in = d_vel[in];
     p.pos_out = d_pos[out]; p.vel_out = d_vel[out]; p.prev_out = d_prev[out];
     p.force = d_force;
@@ -767,7 +934,7 @@ swb_status swb_structure_read_nodes(const swb_structure* s, swb_node_state* out,
         double o[3];
         s->s.fetch(pos, prev, vel, pay, o);
         for (uint64_t n = 0; n < count; ++n) {
-            const uint32_t sl = s->s.sched.slot_of_node[n];
+            const uint32_t sl = s->s.slot_of_node[n];
             out[n].position = {pos[sl].x + o[0], pos[sl].y + o[1], pos[sl].z + o[2]};
             out[n].previous_position = {prev[sl].x + o[0], prev[sl].y + o[1], prev[sl].z + o[2]};
             out[n].velocity = {vel[sl].x, vel[sl].y, vel[sl].z};
@@ -784,7 +951,7 @@ swb_status swb_structure_read_positions_f32(const swb_structure* s, float* out, 
         double o[3];
         s->s.fetch(pos, prev, vel, pay, o);
         for (uint64_t n = 0; n < count; ++n) {
-            const uint32_t sl = s->s.sched.slot_of_node[n];
+            const uint32_t sl = s->s.slot_of_node[n];
             out[3 * n + 0] = static_cast<float>(pos[sl].x + o[0]);
             out[3 * n + 1] = static_cast<float>(pos[sl].y + o[1]);
             out[3 * n + 2] = static_cast<float>(pos[sl].z + o[2]);
@@ -808,7 +975,7 @@ swb_status swb_structure_write_nodes(swb_structure* s, const swb_node_state* in,
                 !std::isfinite(st.previous_position.x) || !std::isfinite(st.previous_position.y) ||
                 !std::isfinite(st.previous_position.z))
                 raise(SWB_INVALID_ARGUMENT, "node state must be finite");
-            const uint32_t sl = m.sched.slot_of_node[n];
+            const uint32_t sl = m.slot_of_node[n];
             const float w = m.inv_mass[sl];
             pos[sl] = make_float4(st.position.x - o[0], st.position.y - o[1], st.position.z - o[2], w);
             prev[sl] = make_float4(st.previous_position.x - o[0], st.previous_position.y - o[1],
@@ -854,7 +1021,7 @@ swb_status swb_structure_read_suspension(const swb_structure* s, swb_payload_sta
             auto endpoint = [&](int node, int point) {
                 double r[3];
                 if (node >= 0) {
-                    const float4 X = pos[m.sched.l1_begin[m.sched.suspension_block] + node];
+                    const float4 X = pos[m.susp_base + node];
                     r[0] = X.x; r[1] = X.y; r[2] = X.z;
                 } else {
                     const double qw = pay.q.x, qx = pay.q.y, qy = pay.q.z, qz = pay.q.w;
@@ -901,7 +1068,10 @@ swb_status swb_structure_write_payload(swb_structure* s, const swb_payload_state
 swb_status swb_structure_sweep_order(const swb_structure* s, uint32_t which, uint64_t* order, uint64_t count) {
     return guarded([&] {
         if (!s || (!order && count)) raise(SWB_INVALID_ARGUMENT, "null argument");
-        const auto& v = which == SWB_SWEEP_DISTANCE ? s->s.sched.distance_order : s->s.sched.dihedral_order;
+        const StructureImpl& m = s->s;
+        const auto& v = m.cluster_mode
+                            ? (which == SWB_SWEEP_DISTANCE ? m.csched.distance_order : m.csched.dihedral_order)
+                            : (which == SWB_SWEEP_DISTANCE ? m.sched.distance_order : m.sched.dihedral_order);
         if (which > SWB_SWEEP_DIHEDRAL) raise(SWB_INVALID_ARGUMENT, "unknown sweep");
         if (count != v.size()) raise(SWB_INVALID_ARGUMENT, "order count mismatch");
         std::copy(v.begin(), v.end(), order);
@@ -916,6 +1086,17 @@ swb_status swb_structure_schedule_report(const swb_structure* s, swb_schedule_re
         std::memset(out, 0, sizeof(*out));
         out->blocks = m.G;
         out->block_threads = m.threads;
+        if (m.cluster_mode) {
+            const ClusterSchedule& C = m.csched;
+            out->cluster_ctas = C.ctas;
+            out->local_stages_per_iteration = C.kinds[0].stages + C.kinds[1].stages;
+            out->cluster_barriers_per_iteration =
+                C.kinds[0].stages + C.kinds[1].stages + (C.susp_cta >= 0 ? 1 : 0);
+            out->max_patch_nodes = static_cast<int32_t>(C.max_patch);
+            out->shared_bytes = static_cast<int32_t>(m.cluster_smem);
+            out->level_constraints[0] = m.def.constraints.size() + m.def.dihedrals.size();
+            return;
+        }
         out->partition_levels = S.levels;
         int phases = 0, stages = 0;
         for (int k = 0; k < kKinds; ++k) {

@@ -26,12 +26,27 @@ namespace dev {
 constexpr float kMinimumLengthF = 1.0e-12f;
 constexpr float kTwoPiF = 6.28318530717958647692f;
 
+// remainder(x, 2*pi) as IEEE remainderf(x, kTwoPiF).  For |x| <= kTwoPiF the
+// quotient rounds to n in {-1, 0, 1} (a tie at |x| = pi rounds to the even
+// n = 0) and x - n*kTwoPiF is exact by Sterbenz' lemma, so the fast path
+// returns the same bits as remainderf; larger |x| takes remainderf.
+__device__ __forceinline__ float wrap_two_pi(float x) {
+    const float half = 0.5f * kTwoPiF;
+    if (fabsf(x) <= kTwoPiF) return x > half ? x - kTwoPiF : (x < -half ? x + kTwoPiF : x);
+    return remainderf(x, kTwoPiF);
+}
+
 // projectDistanceConstraint (soft_body.cpp:1598-1640) on float4 nodes
 // (xyz, w = inverse mass).  comp carries the cable flag in its sign bit.
+// The length and the two divisions use the reciprocal square root and a
+// reciprocal (about one ulp each) instead of IEEE sqrt and division.
 __device__ __forceinline__ void project_distance(float4& pa, float4& pb, float rest, float comp_raw,
                                                  float& lambda, float inv_dt2) {
     const float dx = pb.x - pa.x, dy = pb.y - pa.y, dz = pb.z - pa.z;
-    const float l = sqrtf(dx * dx + dy * dy + dz * dz);
+    const float l2 = dx * dx + dy * dy + dz * dz;
+    if (!(l2 > kMinimumLengthF * kMinimumLengthF)) return;
+    const float il = rsqrtf(l2);
+    const float l = l2 * il;
     if (l <= kMinimumLengthF) return;
     const float value = l - rest;
     const bool cable = signbit(comp_raw);
@@ -39,7 +54,7 @@ __device__ __forceinline__ void project_distance(float4& pa, float4& pb, float r
     const float wsum = pa.w + pb.w;
     const float alpha = fabsf(comp_raw) * inv_dt2;
     if (wsum + alpha <= 0.0f) return;
-    const float dl = (-value - alpha * lambda) / (wsum + alpha);
+    const float dl = (-value - alpha * lambda) * __frcp_rn(wsum + alpha);
     float applied = dl;
     if (cable) {
         const float sum = lambda + dl;
@@ -49,7 +64,7 @@ __device__ __forceinline__ void project_distance(float4& pa, float4& pb, float r
     } else {
         lambda += dl;
     }
-    const float scale = applied / l;
+    const float scale = applied * il;
     const float sa = pa.w * scale, sb = pb.w * scale;
     pa.x -= sa * dx; pa.y -= sa * dy; pa.z -= sa * dz;
     pb.x += sb * dx; pb.y += sb * dy; pb.z += sb * dz;
@@ -66,9 +81,11 @@ __device__ __forceinline__ void project_dihedral(float4& A, float4& B, float4& C
     const float3 toD = d - a;
     const float3 A1 = cross(edge, toC);
     const float3 A2 = cross(toD, edge);
-    const float el = length(edge), l1 = length(A1), l2 = length(A2);
+    const float e2 = dot(edge, edge), q1 = dot(A1, A1), q2 = dot(A2, A2);
+    if (!(e2 > kMinimumLengthF * kMinimumLengthF) || !(q1 > 0.0f) || !(q2 > 0.0f)) return;
+    const float iel = rsqrtf(e2), il1 = rsqrtf(q1), il2 = rsqrtf(q2);
+    const float el = e2 * iel, l1 = q1 * il1, l2 = q2 * il2;
     if (!(el > kMinimumLengthF) || !(l1 > kMinimumLengthF * el) || !(l2 > kMinimumLengthF * el)) return;
-    const float iel = 1.0f / el, il1 = 1.0f / l1, il2 = 1.0f / l2;
     const float3 e = edge * iel;
     const float3 n1 = A1 * il1;
     const float3 n2 = A2 * il2;
@@ -92,8 +109,8 @@ __device__ __forceinline__ void project_dihedral(float4& A, float4& B, float4& C
     const float alpha = comp * inv_dt2;
     const float den = wg + alpha;
     if (!(den > 0.0f) || !isfinite(den)) return;
-    const float value = remainderf(angle - rest, kTwoPiF);
-    const float dl = (-value - alpha * lambda) / den;
+    const float value = wrap_two_pi(angle - rest);
+    const float dl = (-value - alpha * lambda) * __frcp_rn(den);
     if (!isfinite(dl)) return;
     const float sa = A.w * dl, sb = B.w * dl, sc = C.w * dl, sd = D.w * dl;
     A.x += sa * ga.x; A.y += sa * ga.y; A.z += sa * ga.z;

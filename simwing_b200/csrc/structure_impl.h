@@ -1,6 +1,8 @@
 // Host-side state of one device structure (the swb_structure handle).
 #pragma once
 
+#include "cluster_params.h"
+#include "cluster_schedule.h"
 #include "common.h"
 #include "schedule.h"
 #include "step_params.h"
@@ -26,7 +28,16 @@ constexpr int kDiagBlocks = 148;
 
 struct StructureImpl {
     OwnedDefinition def;
-    Schedule sched;
+    bool cluster_mode = false;
+    Schedule sched;            // grid schedule (cluster_mode == false)
+    ClusterSchedule csched;    // cluster schedule (cluster_mode == true)
+    std::vector<uint32_t> slot_of_node, node_of_slot;
+    int susp_owner = -1;       // CTA owning the suspension endpoint nodes
+    uint32_t susp_base = 0;    // first slot of that CTA's patch
+    ClusterParams cparams{};
+    ClusterInstance cluster_base{};
+    ClusterInstance* d_instances = nullptr;
+    uint32_t cluster_smem = 0;
     uint64_t fingerprint = 0;
     int device = -1;
     int sm_count = 0;
@@ -72,6 +83,9 @@ struct StructureImpl {
 
     ~StructureImpl();
     void build(const swb_structure_definition& definition, const swb_solver_options* options);
+    void upload_cluster_tables();
+    void upload_grid_tables();
+    void finish_build(const swb_solver_options& opt, const cudaDeviceProp& prop);
     void upload_pressure();
     void upload_forces();
     void validate_settings(const swb_step_settings& st) const;

@@ -69,10 +69,19 @@ def test_known_answers_on_device(cuda_device):
         assert s.node_states()[1, 0, 0] == pytest.approx(expected, abs=1e-6)
 
 
+@pytest.mark.parametrize("ctas", [1, 4, 16])
+def test_patch_per_step_parity_cluster(cuda_device, ctas):
+    d = sw.generate_patch()
+    dev = sw.Structure(d, sw.SolverOptions(cluster_ctas=ctas))
+    assert dev.schedule_report().cluster_ctas == ctas
+    errs, _, _ = per_step_errors(d, 6, step_settings(), sw.SolverOptions(cluster_ctas=ctas))
+    assert max(errs) <= REL_TOL, errs
+
+
 @pytest.mark.parametrize("blocks,levels", [(1, 1), (8, 1), (8, 3), (148, 3)])
-def test_patch_per_step_parity(cuda_device, blocks, levels):
+def test_patch_per_step_parity_grid(cuda_device, blocks, levels):
     errs, _, _ = per_step_errors(sw.generate_patch(), 6, step_settings(),
-                                 sw.SolverOptions(blocks=blocks, partition_levels=levels))
+                                 sw.SolverOptions(blocks=blocks, partition_levels=levels, flags=sw.abi.OPT_GRID))
     assert max(errs) <= REL_TOL, errs
 
 
@@ -82,18 +91,22 @@ def test_patch_global_only_parity(cuda_device):
     assert max(errs) <= REL_TOL, errs
 
 
-def test_wing_per_step_parity_small(cuda_device):
+@pytest.mark.parametrize("options", [dict(), dict(cluster_ctas=4), dict(flags=4)])
+def test_wing_per_step_parity_small(cuda_device, options):
     d = sw.generate_wing(cells=8, chordwise=20, spanwise_per_cell=2, rib_layers=3)
-    errs, dev, orc = per_step_errors(d, 4, step_settings())
+    errs, dev, orc = per_step_errors(d, 4, step_settings(), sw.SolverOptions(**options))
     assert max(errs) <= REL_TOL, errs
     s = dev.suspension_state()
     p, w, _ = orc.payload()
     assert np.abs(s.center_of_mass - [p.center_of_mass.x, p.center_of_mass.y, p.center_of_mass.z]).max() < 1e-4
 
 
-def test_full_wing_one_step_parity(cuda_device):
-    errs, _, _ = per_step_errors(sw.generate_wing(), 2, step_settings())
+@pytest.mark.parametrize("options", [dict(), dict(flags=4)])
+def test_full_wing_one_step_parity(cuda_device, options):
+    errs, dev, _ = per_step_errors(sw.generate_wing(), 2, step_settings(), sw.SolverOptions(**options))
     assert max(errs) <= REL_TOL, errs
+    if not options:
+        assert dev.schedule_report().cluster_ctas == 16
 
 
 def test_patch_600_steps_settled_shape(cuda_device):
@@ -178,7 +191,7 @@ def test_suspension_certification_failure_rolls_back(cuda_device):
 
 
 def test_barrier_timeout_reports_and_restores(cuda_device):
-    s = sw.Structure(sw.generate_patch(), sw.SolverOptions(blocks=8, sync_budget_cycles=1))
+    s = sw.Structure(sw.generate_patch(), sw.SolverOptions(blocks=8, sync_budget_cycles=1, flags=sw.abi.OPT_GRID))
     before = s.node_states()
     with pytest.raises(sw.SyncTimeout):
         s.step(step_settings())

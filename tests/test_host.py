@@ -137,15 +137,31 @@ def test_wing_generator_shape():
 @pytest.mark.parametrize("blocks", [1, 7, 148])
 def test_schedule_invariants_patch(levels, blocks):
     d = sw.generate_patch(nx=20, ny=20)
-    r, do, ho = sw.plan_schedule(d, sw.SolverOptions(blocks=blocks, partition_levels=levels))
+    r, do, ho = sw.plan_schedule(d, sw.SolverOptions(blocks=blocks, partition_levels=levels, flags=abi.OPT_GRID))
     assert sorted(do.tolist()) == list(range(d.view.constraint_count))
     assert sorted(ho.tolist()) == list(range(d.view.dihedral_count))
     assert r.blocks == min(blocks, d.node_count)
 
 
+@pytest.mark.parametrize("ctas", [1, 2, 4, 8, 16])
+def test_cluster_schedule_invariants(ctas):
+    d = sw.generate_wing(cells=8, chordwise=16, spanwise_per_cell=2, rib_layers=3)
+    r, do, ho = sw.plan_schedule(d, sw.SolverOptions(cluster_ctas=ctas))
+    assert r.cluster_ctas == ctas
+    assert sorted(do.tolist()) == list(range(d.view.constraint_count))
+    assert sorted(ho.tolist()) == list(range(d.view.dihedral_count))
+    assert r.cluster_barriers_per_iteration == r.local_stages_per_iteration + 1  # + suspension stage
+
+
+def test_full_wing_fits_one_cluster():
+    r, _, _ = sw.plan_schedule(sw.generate_wing())
+    assert r.cluster_ctas == 16 and r.max_patch_nodes <= 4096
+    assert r.shared_bytes <= 227 * 1024
+
+
 def test_schedule_invariants_wing_and_global_only():
     d = sw.generate_wing(cells=8, chordwise=16, spanwise_per_cell=2, rib_layers=3)
-    r, _, _ = sw.plan_schedule(d, sw.SolverOptions(blocks=148))
+    r, _, _ = sw.plan_schedule(d, sw.SolverOptions(blocks=148, flags=abi.OPT_GRID))
     assert r.level_constraints[0] > 0
     r, _, _ = sw.plan_schedule(d, sw.SolverOptions(blocks=32, flags=abi.OPT_GLOBAL_ONLY))
     assert r.partition_levels == 0 and r.global_constraints == d.view.constraint_count + d.view.dihedral_count
@@ -153,7 +169,7 @@ def test_schedule_invariants_wing_and_global_only():
 
 def test_full_wing_schedule_invariants():
     d = sw.generate_wing()
-    r, do, ho = sw.plan_schedule(d, sw.SolverOptions(blocks=148))
+    r, do, ho = sw.plan_schedule(d, sw.SolverOptions(blocks=148, flags=abi.OPT_GRID))
     total = d.view.constraint_count + d.view.dihedral_count
     assert sum(r.level_constraints) + r.global_constraints == total
     assert r.max_patch_nodes < 65536
