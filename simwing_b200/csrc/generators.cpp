@@ -339,8 +339,12 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
             b.edge_constraints(skin_first, skin_last, skin_compliance);
             b.dihedrals(skin_first, skin_last, p->bend_rigidity, -1.0);
 
-            // Ribs with their own nodes, sewn to the skin.
+            // Ribs with their own nodes, sewn to the skin.  The last rib
+            // column is one station before the trailing edge (the section is
+            // thinnest there); the rib fans from it to the trailing-edge node,
+            // and the skin station between them is not sewn.
             const uint32_t L = p->rib_layers;
+            const uint32_t J = C - 1;  // rib columns 1 .. J-1, fan from J-1 to the trailing edge
             const double seam_ea = 1.0e5;
             for (uint32_t r = 0; r <= p->cells; ++r) {
                 const uint32_t s = r * p->spanwise_per_cell;
@@ -348,7 +352,7 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                 std::vector<uint64_t> col((C + 1) * (L + 1), 0);
                 const uint64_t le = b.node(surface_point(st, 0.0, 1.0));
                 const uint64_t te = b.node(surface_point(st, 1.0, 1.0));
-                for (uint32_t j = 1; j < C; ++j) {
+                for (uint32_t j = 1; j < J; ++j) {
                     const V lo = surface_point(st, xi[j], -1.0);
                     const V hi = surface_point(st, xi[j], 1.0);
                     for (uint32_t l = 0; l <= L; ++l)
@@ -360,7 +364,7 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                 for (uint32_t l = 0; l < L; ++l)
                     b.triangle(le, col[1 * (L + 1) + l], col[1 * (L + 1) + l + 1], rib_pressure,
                                p->areal_density);
-                for (uint32_t j = 1; j + 1 < C; ++j)
+                for (uint32_t j = 1; j + 1 < J; ++j)
                     for (uint32_t l = 0; l < L; ++l) {
                         const uint64_t a = col[j * (L + 1) + l];
                         const uint64_t bb = col[(j + 1) * (L + 1) + l];
@@ -370,26 +374,29 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                         b.triangle(a, c, dd, rib_pressure, p->areal_density);
                     }
                 for (uint32_t l = 0; l < L; ++l)
-                    b.triangle(col[(C - 1) * (L + 1) + l], te, col[(C - 1) * (L + 1) + l + 1],
+                    b.triangle(col[(J - 1) * (L + 1) + l], te, col[(J - 1) * (L + 1) + l + 1],
                                rib_pressure, p->areal_density);
                 const size_t last = def->def.triangles.size();
                 b.edge_constraints(first, last, skin_compliance);
                 b.dihedrals(first, last, p->bend_rigidity, -1.0);
-                // Seam: rib boundary loop (same loop order as the skin) to
-                // the skin loop of this station.
-                std::vector<uint64_t> rib_loop(loop), skin_loop(loop);
+                // Seam: the rib boundary loop (skin loop order, skipping the
+                // skin station next to the trailing edge on both surfaces)
+                // sewn to the matching skin nodes.
+                std::vector<uint64_t> rib_loop, skin_loop;
                 for (uint32_t k = 0; k < loop; ++k) {
-                    skin_loop[k] = skin[s * loop + k];
-                    if (k == 0) rib_loop[k] = te;
-                    else if (k == C) rib_loop[k] = le;
-                    else if (k < C) rib_loop[k] = col[(C - k) * (L + 1) + 0];
-                    else rib_loop[k] = col[(k - C) * (L + 1) + L];
+                    if (k == 1 || k == loop - 1) continue;
+                    skin_loop.push_back(skin[s * loop + k]);
+                    if (k == 0) rib_loop.push_back(te);
+                    else if (k == C) rib_loop.push_back(le);
+                    else if (k < C) rib_loop.push_back(col[(C - k) * (L + 1) + 0]);
+                    else rib_loop.push_back(col[(k - C) * (L + 1) + L]);
                 }
-                for (uint32_t k = 0; k < loop; ++k)
+                const size_t seam = rib_loop.size();
+                for (size_t k = 0; k < seam; ++k)
                     b.distance(SWB_CONSTRAINT_SEAM_STITCH, rib_loop[k], skin_loop[k], 0.0, 0.0);
                 for (const auto* chain : {&rib_loop, &skin_loop})
-                    for (uint32_t k = 0; k < loop; ++k) {
-                        const uint64_t a = (*chain)[k], bb = (*chain)[(k + 1) % loop];
+                    for (size_t k = 0; k < seam; ++k) {
+                        const uint64_t a = (*chain)[k], bb = (*chain)[(k + 1) % seam];
                         const double len = length(b.design[bb] - b.design[a]);
                         b.distance(SWB_CONSTRAINT_DISTANCE, a, bb, len, 2.0 * len / seam_ea);
                     }

@@ -127,7 +127,7 @@ def test_wing_generator_shape():
     assert 65000 <= c["triangles"] <= 72000
     assert 36000 <= c["nodes"] <= 40000
     assert c["suspension_segments"] == 2
-    assert c["seam_stitch"] == 41 * 120
+    assert c["seam_stitch"] == 41 * (120 - 2)  # every rib sewn except next to the trailing edge
     assert 2000 <= c["cable"] <= 3000
     assert 95000 <= c["dihedrals"] <= 105000
     assert sw.generate_wing().fingerprint == d.fingerprint
