@@ -45,25 +45,51 @@ __device__ __forceinline__ ClusterRecord load_record(const ClusterKindDev& K, in
     return r;
 }
 
-__device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, uint32_t me, float4* x,
-                                             float4* const* peers, float* lam, uint32_t first, float inv_dt2) {
-    float4* pa = node_at(r.ab & 0xffffu, me, x, peers);
-    float4* pb = node_at(r.ab >> 16, me, x, peers);
+// Cluster-window address of node `ref`: the node arrays sit at the same
+// shared-memory offset in every CTA, so a peer's node is this CTA's address
+// mapped to the peer's rank (mapa); a local node keeps its own address,
+// which is valid in the cluster window.
+__device__ __forceinline__ uint32_t node_addr(uint32_t ref, uint32_t me, uint32_t x_base) {
+    const uint32_t rank = ref >> 12;
+    const uint32_t local = x_base + (ref & 0xfffu) * 16u;
+    if (rank == me) return local;
+    uint32_t remote;
+    asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+    return remote;
+}
+__device__ __forceinline__ float4 ld_node(uint32_t addr) {
+    float4 v;
+    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(addr)
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_node(uint32_t addr, float4 v) {
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z),
+                 "f"(v.w)
+                 : "memory");
+}
+
+__device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, uint32_t me, uint32_t x_base,
+                                             float* lam, uint32_t first, float inv_dt2) {
+    const uint32_t pa = node_addr(r.ab & 0xffffu, me, x_base);
+    const uint32_t pb = node_addr(r.ab >> 16, me, x_base);
     float l = lam[r.index - first];
     if (kind == 0) {
-        float4 A = *pa, B = *pb;
+        float4 A = ld_node(pa), B = ld_node(pb);
         project_distance(A, B, r.rest, r.comp, l, inv_dt2);
-        *pa = A;
-        *pb = B;
+        st_node(pa, A);
+        st_node(pb, B);
     } else {
-        float4* pc = node_at(r.cd & 0xffffu, me, x, peers);
-        float4* pd = node_at(r.cd >> 16, me, x, peers);
-        float4 A = *pa, B = *pb, C = *pc, D = *pd;
+        const uint32_t pc = node_addr(r.cd & 0xffffu, me, x_base);
+        const uint32_t pd = node_addr(r.cd >> 16, me, x_base);
+        float4 A = ld_node(pa), B = ld_node(pb), C = ld_node(pc), D = ld_node(pd);
         project_dihedral(A, B, C, D, r.rest, r.comp, l, inv_dt2);
-        *pa = A;
-        *pb = B;
-        *pc = C;
-        *pd = D;
+        st_node(pa, A);
+        st_node(pb, B);
+        st_node(pc, C);
+        st_node(pd, D);
     }
     lam[r.index - first] = l;
 }
@@ -88,6 +114,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const 
     const uint32_t base = __ldg(I.patch_begin + me);
     const uint32_t n = __ldg(I.patch_begin + me + 1) - base;
     const bool owner = static_cast<int>(me) == I.susp_cta;
+    const uint32_t x_base = smem_addr(x);
 
     if (tid < p.ctas) peers[tid] = cluster.map_shared_rank(x, tid);
     if (tid == 0) {
@@ -174,9 +201,9 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const 
             next = load_record(I.kind[kn], kn, stage_lo(gn) + tid, stage_hi(gn));
             const uint32_t first = kind ? first1 : first0;
             float* lam = kind ? lam1 : lam0;
-            if (cur.index != ~0u) apply_record(cur, kind, me, x, peers, lam, first, p.inv_dt2);
+            if (cur.index != ~0u) apply_record(cur, kind, me, x_base, lam, first, p.inv_dt2);
             for (uint32_t i = stage_lo(g) + tid + blockDim.x; i < stage_hi(g); i += blockDim.x)
-                apply_record(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, x, peers, lam, first,
+                apply_record(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, x_base, lam, first,
                              p.inv_dt2);
             cluster.sync();
         }

@@ -71,8 +71,19 @@ __device__ __forceinline__ void project_distance(float4& pa, float4& pb, float r
 }
 
 // evaluateDihedral + solveDihedralConstraint (soft_body.cpp:1648-1711,
-// 1754-1792): signed hinge angle atan2(sin, cos) of the face normals and its
-// analytic reverse-mode gradient, then one XPBD angle projection.
+// 1754-1792): one XPBD projection of the signed hinge angle.
+//
+// The reference evaluates theta = atan2(e.(n1 x n2), n1.n2) from unit
+// vectors and its gradient by reverse mode through the normalisations.  The
+// same function and gradient are evaluated here in closed form (an identity,
+// checked against the reference evaluation in the tests): with the face
+// areas A1 = e x (c - a), A2 = (d - a) x e and the hinge e = b - a,
+//   theta = atan2(e.(A1 x A2) / |e|, A1.A2)      (atan2 is scale-invariant),
+//   grad_c = -|e| / |A1|^2 A1,   grad_d = -|e| / |A2|^2 A2,
+//   grad_b = -t1 grad_c - t2 grad_d,   grad_a = -(grad_b + grad_c + grad_d),
+// where t1, t2 are the projections of c and d on the hinge
+// ((c - a).e / |e|^2, (d - a).e / |e|^2).  The degeneracy gates are the
+// reference's (|e|, |A1|/|e|, |A2|/|e| above 1e-12).
 __device__ __forceinline__ void project_dihedral(float4& A, float4& B, float4& C, float4& D, float rest,
                                                  float comp, float& lambda, float inv_dt2) {
     const float3 a = f3(A), b = f3(B), c = f3(C), d = f3(D);
@@ -82,33 +93,28 @@ __device__ __forceinline__ void project_dihedral(float4& A, float4& B, float4& C
     const float3 A1 = cross(edge, toC);
     const float3 A2 = cross(toD, edge);
     const float e2 = dot(edge, edge), q1 = dot(A1, A1), q2 = dot(A2, A2);
-    if (!(e2 > kMinimumLengthF * kMinimumLengthF) || !(q1 > 0.0f) || !(q2 > 0.0f)) return;
-    const float iel = rsqrtf(e2), il1 = rsqrtf(q1), il2 = rsqrtf(q2);
-    const float el = e2 * iel, l1 = q1 * il1, l2 = q2 * il2;
-    if (!(el > kMinimumLengthF) || !(l1 > kMinimumLengthF * el) || !(l2 > kMinimumLengthF * el)) return;
-    const float3 e = edge * iel;
-    const float3 n1 = A1 * il1;
-    const float3 n2 = A2 * il2;
-    const float cosine = fminf(fmaxf(dot(n1, n2), -1.0f), 1.0f);
-    const float3 n1xn2 = cross(n1, n2);
-    const float sine = dot(e, n1xn2);
-    const float3 n1adj = cosine * cross(n2, e) - sine * n2;
-    const float3 n2adj = cosine * cross(e, n1) - sine * n1;
-    const float3 eadj = cosine * n1xn2;
-    const float3 a1adj = (n1adj - dot(n1adj, n1) * n1) * il1;
-    const float3 a2adj = (n2adj - dot(n2adj, n2) * n2) * il2;
-    float3 gb = (eadj - dot(eadj, e) * e) * iel;
-    gb = gb + cross(toC, a1adj);
-    const float3 gc = cross(a1adj, edge);
-    gb = gb + cross(a2adj, toD);
-    const float3 gd = cross(edge, a2adj);
+    const float k2 = kMinimumLengthF * kMinimumLengthF;
+    if (!(e2 > k2) || !(q1 > k2 * e2) || !(q2 > k2 * e2)) return;
+    const float iel = rsqrtf(e2);
+    const float el = e2 * iel;
+    const float sine = dot(edge, cross(A1, A2)) * iel;
+    const float cosine = dot(A1, A2);
+    const float s1 = -el * __frcp_rn(q1), s2 = -el * __frcp_rn(q2);
+    const float3 gc = A1 * s1;
+    const float3 gd = A2 * s2;
+    const float ie2 = iel * iel;
+    const float t1 = dot(toC, edge) * ie2, t2 = dot(toD, edge) * ie2;
+    const float3 gb = -(gc * t1 + gd * t2);
     const float3 ga = -((gb + gc) + gd);
     const float angle = atan2f(sine, cosine);
-    if (!isfinite(angle) || !finite3(ga) || !finite3(gb) || !finite3(gc) || !finite3(gd)) return;
+    // The reference skips a hinge whose angle or gradient is not finite.  A
+    // non-finite gradient component makes wg (and den) non-finite, and a
+    // non-finite angle makes dl non-finite, so the two checks below reject
+    // exactly those cases without testing each component.
     const float wg = A.w * dot(ga, ga) + B.w * dot(gb, gb) + C.w * dot(gc, gc) + D.w * dot(gd, gd);
     const float alpha = comp * inv_dt2;
     const float den = wg + alpha;
-    if (!(den > 0.0f) || !isfinite(den)) return;
+    if (!(den > 0.0f) || !isfinite(den) || !isfinite(wg)) return;
     const float value = wrap_two_pi(angle - rest);
     const float dl = (-value - alpha * lambda) * __frcp_rn(den);
     if (!isfinite(dl)) return;

@@ -130,6 +130,31 @@ def test_dihedral_gradient_matches_finite_difference():
     assert worst < 2e-6
 
 
+def test_closed_form_dihedral_equals_reference_evaluation():
+    """The device evaluates the hinge angle and gradient in closed form; it
+    must be the same function as the reference's reverse-mode evaluation
+    (soft_body.cpp:1648-1711), up to FP64 round-off."""
+    rng = np.random.default_rng(0)
+    worst_g = worst_a = 0.0
+    for _ in range(2000):
+        p = rng.normal(size=(4, 3))
+        angle, grad, valid = O.evaluate_dihedral(p.ravel())
+        if not valid:
+            continue
+        a, b, c, d = p
+        e = b - a
+        A1, A2 = np.cross(e, c - a), np.cross(d - a, e)
+        e2, q1, q2 = e @ e, A1 @ A1, A2 @ A2
+        el = np.sqrt(e2)
+        theta = np.arctan2(e @ np.cross(A1, A2) / el, A1 @ A2)
+        gc, gd = -(el / q1) * A1, -(el / q2) * A2
+        gb = -((c - a) @ e / e2) * gc - ((d - a) @ e / e2) * gd
+        ga = -(gb + gc + gd)
+        worst_g = max(worst_g, np.abs(np.array([ga, gb, gc, gd]) - grad).max() / np.abs(grad).max())
+        worst_a = max(worst_a, abs(np.remainder(theta - angle + np.pi, 2 * np.pi) - np.pi))
+    assert worst_g < 1e-12 and worst_a < 1e-12
+
+
 # ---- the restatement is the reference, bit for bit -------------------------
 @needs_ref
 def test_port_matches_reference_bitwise_on_patch():
