@@ -85,7 +85,7 @@ def measured_peak():
 
 def profile_traffic():
     """dram bytes per launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "xpbd_step_kernel_wing70k.md")
+    path = os.path.join(ROOT, "profiles", "xpbd_cluster_kernel_wing70k.md")
     try:
         for line in open(path):
             if line.strip().startswith("traffic_bytes_per_launch:"):
@@ -229,7 +229,7 @@ def main():
     definition = sw.generate_wing()
     st = settings(sw)
     structure = sw.Structure(definition, sw.SolverOptions(device=local))
-    flush =torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
     # warm-up
     for _ in range(args.warmup):
@@ -304,9 +304,9 @@ def main():
                          "peak_source": peak_kind, "algorithmic_bytes_per_step": bytes_per_step},
             "clocks": clocks.summary(),
             "schedule": {"blocks": report.blocks, "threads": report.block_threads,
-                         "levels": report.partition_levels,
-                         "device_phases_per_iteration": report.device_phases_per_iteration,
-                         "local_stages_per_iteration": report.local_stages_per_iteration,
+                         "cluster_ctas": report.cluster_ctas,
+                         "cluster_barriers_per_iteration": report.cluster_barriers_per_iteration,
+                         "stages_per_iteration": report.local_stages_per_iteration,
                          "shared_bytes": report.shared_bytes},
             "final_diagnostics": {"finite": bool(diag.finite), "max_distance_error": diag.maximum_distance_error},
             "cpu_baseline": cpu,
