@@ -385,6 +385,42 @@ swb_status swb_structure_step_many(swb_structure* structure,
 swb_status swb_structure_diagnostics(const swb_structure* structure,
                                      swb_diagnostics* out);
 
+/* Diagnostics of caller-owned device arrays that allocates no device memory.
+ * No counterpart in the reference: it is for callers that cannot call
+ * cudaMalloc (a coupled flow solver that reserves the GPU's memory in its own
+ * pool and keeps the structural state there; fixed-budget loops that must
+ * not let an allocation synchronize the device).  It computes the node and
+ * distance-constraint reductions of Structure::diagnostics
+ * (structure.cpp:833-959) over:
+ *   positions, previous_positions, velocities: device float4[node_count],
+ *       xyz in metres (w of positions = inverse mass, 0 = fixed);
+ *   first_nodes, second_nodes: device uint32[constraint_count];
+ *   rest_lengths: device float[constraint_count];
+ *   kinds: device uint8[constraint_count] (SWB_CONSTRAINT_*).
+ * Filled: node_count, dynamic_node_count, constraint_count,
+ * total_dynamic_mass, center_of_mass, linear_momentum, kinetic_energy,
+ * maximum_distance_error, maximum_cable_extension, finite; the rest is 0.
+ * Scratch is one fixed static device array shared by every call: at most
+ * SWB_NOALLOC_MAX_NODES nodes and SWB_NOALLOC_MAX_CONSTRAINTS constraints,
+ * larger inputs are rejected with SWB_INVALID_ARGUMENT.  Calls whose work
+ * overlaps on the GPU would race on that array; the function serialises its
+ * own calls per device and returns only when its result is on the host.  It
+ * runs on the legacy default stream, after the caller's work on blocking
+ * streams. */
+#define SWB_NOALLOC_MAX_NODES 524288u
+#define SWB_NOALLOC_MAX_CONSTRAINTS 524288u
+swb_status swb_diagnostics_noalloc(int32_t device,
+                                   const void* positions,
+                                   const void* previous_positions,
+                                   const void* velocities,
+                                   uint64_t node_count,
+                                   const uint32_t* first_nodes,
+                                   const uint32_t* second_nodes,
+                                   const float* rest_lengths,
+                                   const uint8_t* kinds,
+                                   uint64_t constraint_count,
+                                   swb_diagnostics* out);
+
 /* Structure::nodeStates (structure.h:288, structure.cpp:725-734). */
 swb_status swb_structure_read_nodes(const swb_structure* structure,
                                     swb_node_state* out,

@@ -196,6 +196,8 @@ _PROTOTYPES = {
     "swb_structure_step": (C.c_int, [C.c_void_p, P(StepSettings), P(Diagnostics)]),
     "swb_structure_step_many": (C.c_int, [C.c_void_p, P(StepSettings), C.c_int32, P(Diagnostics)]),
     "swb_structure_diagnostics": (C.c_int, [C.c_void_p, P(Diagnostics)]),
+    "swb_diagnostics_noalloc": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, P(Diagnostics)]),
     "swb_structure_read_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swb_structure_read_positions_f32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swb_structure_write_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
