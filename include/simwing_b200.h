@@ -509,6 +509,85 @@ swb_status swb_plan_schedule(const swb_structure_definition* definition,
 double swb_structure_last_step_ms(const swb_structure* structure);
 
 /* ------------------------------------------------------------------------ */
+/* Batched structures.  No reference counterpart: the reference steps one    */
+/* Structure per call, and a caller with many wings loops over them.  A      */
+/* batch holds many independent structures of uneven sizes and steps all of  */
+/* them with one kernel launch per substep: each structure occupies a        */
+/* contiguous range of ranks of a thread-block cluster (several small        */
+/* structures share one cluster), and the launches of a block of steps are   */
+/* captured in one CUDA graph.  Each structure steps exactly as a plain      */
+/* structure created with cluster_ctas = its rank count (bit-identical).     */
+/* ------------------------------------------------------------------------ */
+typedef struct swb_batch swb_batch;
+
+typedef struct swb_batch_options {
+    int32_t device;
+    int32_t cluster_ctas;        /* CTAs per cluster, 1..16; 0 = 16            */
+    int32_t target_patch_nodes;  /* nodes per CTA each structure is split for;
+                                    0 = autotune when SWB_BATCH_AUTOTUNE is
+                                    set, else 2048                           */
+    int32_t block_threads;       /* 0 = widest stage of any structure        */
+    int32_t graph_steps;         /* steps per captured graph; 0 = 120        */
+    uint32_t flags;              /* SWB_OPT_NO_GRAPH | SWB_BATCH_AUTOTUNE    */
+    int32_t autotune_iterations; /* iterations of the timed trial steps; 0 = 48 */
+    int32_t reserved;
+} swb_batch_options;
+
+enum {
+    SWB_BATCH_AUTOTUNE = 1u << 8  /* time candidate patch sizes at creation */
+};
+
+void swb_default_batch_options(swb_batch_options* out);
+
+/* Builds every structure (validation as swb_structure_create), splits each
+ * into ranks, packs the ranks into clusters and, with SWB_BATCH_AUTOTUNE,
+ * keeps the patch size whose trial launches were fastest. */
+swb_status swb_batch_create(const swb_structure_definition* const* definitions,
+                            uint64_t count,
+                            const swb_batch_options* options,
+                            swb_batch** out);
+void swb_batch_destroy(swb_batch* batch);
+uint64_t swb_batch_size(const swb_batch* batch);
+
+/* Borrowed handle of structure `index` (valid until swb_batch_destroy; do
+ * not destroy it).  Every swb_structure_* call works on it: loads, pressure,
+ * read_nodes, diagnostics, checkpoint/restore, even a single plain step. */
+swb_structure* swb_batch_structure(swb_batch* batch, uint64_t index);
+
+/* Steps every structure `steps` times with the same settings and its own
+ * pending loads re-applied each step.  Per structure the steps form
+ * transactions of up to graph_steps steps: a structure whose block failed
+ * keeps its state and loads from before that block and stops; the others
+ * commit.  `statuses` (nullable, `count` entries) receives each structure's
+ * status; the return value is SWB_OK or the first failure. */
+swb_status swb_batch_step(swb_batch* batch,
+                          const swb_step_settings* settings,
+                          int32_t steps,
+                          int32_t* statuses);
+
+typedef struct swb_batch_report {
+    int32_t structures;
+    int32_t clusters;
+    int32_t cluster_ctas;
+    int32_t idle_ctas;           /* ranks of clusters no structure uses      */
+    int32_t block_threads;
+    int32_t target_patch_nodes;
+    int32_t shared_bytes;
+    int32_t max_cluster_stages;  /* colour stages per iteration, worst cluster */
+    int32_t resident_clusters;   /* clusters the device holds at once        */
+    int32_t colours_per_sync;    /* colour stages between cluster barriers   */
+    int32_t autotune_candidates; /* patch sizes timed at creation            */
+    int32_t reserved;
+    int32_t candidate_patch_nodes[8];
+    double candidate_ms_per_step[8];
+} swb_batch_report;
+swb_status swb_batch_get_report(const swb_batch* batch, swb_batch_report* out);
+
+/* Device time of the most recent swb_batch_step, in milliseconds (CUDA
+ * events on the batch's stream around its graphs or launches). */
+double swb_batch_last_step_ms(const swb_batch* batch);
+
+/* ------------------------------------------------------------------------ */
 /* Reference colouring (bit-exact restatement of                             */
 /* SoftBody::constraintColouring, soft_body.cpp:1978-2075): greedy first-fit */
 /* over the line graph in insertion order, colours ranked by descending      */

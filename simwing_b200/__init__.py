@@ -287,6 +287,24 @@ def generate_wing(**overrides) -> Definition:
     return Definition(out.value)
 
 
+def wing_batch_parameters(count: int = 64, seed: int = 2024):
+    """Seeded uneven wing sizes of the batched workload: cells ~ U{20..60},
+    chordwise in {30, 45, 60}, aspect ratio ~ U(4.5, 7), per-wing compliance
+    multiplier lognormal(0, 0.2) (drawn by the generator from its seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        out.append(dict(cells=int(rng.integers(20, 61)), chordwise=int(rng.choice([30, 45, 60])),
+                        aspect_ratio=float(rng.uniform(4.5, 7.0)), compliance_jitter=0.2,
+                        seed=int(seed) * 1000 + i))
+    return out
+
+
+def generate_wing_batch(count: int = 64, seed: int = 2024, **overrides) -> list:
+    """Definitions of the batched workload (see wing_batch_parameters)."""
+    return [generate_wing(**dict(p, **overrides)) for p in wing_batch_parameters(count, seed)]
+
+
 def reference_colouring(definition: Definition):
     """Bit-exact restatement of SoftBody::constraintColouringView."""
     lib = abi.library()
@@ -331,19 +349,25 @@ def _vec(v) -> np.ndarray:
 class Structure:
     """simwing::fsi::Structure on the device (src/fsi/structure.h:273-309)."""
 
-    def __init__(self, definition: Definition, options: abi.SolverOptions | None = None):
+    def __init__(self, definition: Definition, options: abi.SolverOptions | None = None, *, _borrowed=None):
         self._lib = abi.library()
         self._definition = definition
-        h = C.c_void_p()
-        _check(self._lib.swb_structure_create(definition.pointer, None if options is None else C.byref(options),
-                                              C.byref(h)))
+        self._owner = None
+        if _borrowed is not None:
+            # a structure owned by a Batch: the batch keeps it alive
+            h, self._owner = _borrowed
+        else:
+            h = C.c_void_p()
+            _check(self._lib.swb_structure_create(definition.pointer, None if options is None else C.byref(options),
+                                                  C.byref(h)))
         self._h = h
         self.node_count = int(self._lib.swb_structure_node_count(h))
         self._segments = int(definition.view.suspension.contents.segment_count) if definition.has_suspension else 0
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
-            self._lib.swb_structure_destroy(self._h)
+            if getattr(self, "_owner", None) is None:
+                self._lib.swb_structure_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):
@@ -469,3 +493,71 @@ class Structure:
 
     def last_step_ms(self) -> float:
         return float(self._lib.swb_structure_last_step_ms(self._h))
+
+
+def BatchOptions(**overrides) -> abi.BatchOptions:
+    o = abi.BatchOptions()
+    abi.library().swb_default_batch_options(C.byref(o))
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    return o
+
+
+class Batch:
+    """Many independent structures stepped together by one packed cluster
+    launch per substep (swb_batch_*).  Each structure is reachable as a
+    `Structure` through `structure(i)`; it steps exactly as a plain structure
+    built with `cluster_ctas` equal to its rank count."""
+
+    def __init__(self, definitions, options: abi.BatchOptions | None = None):
+        self._lib = abi.library()
+        self._definitions = list(definitions)
+        ptrs = (C.c_void_p * len(self._definitions))(*[C.cast(d.pointer, C.c_void_p) for d in self._definitions])
+        h = C.c_void_p()
+        _check(self._lib.swb_batch_create(ptrs, len(self._definitions),
+                                          None if options is None else C.byref(options), C.byref(h)))
+        self._h = h
+        self._structures = [Structure(d, _borrowed=(C.c_void_p(self._lib.swb_batch_structure(h, i)), self))
+                            for i, d in enumerate(self._definitions)]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            for s in self._structures:
+                s.close()
+            self._lib.swb_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self) -> int:
+        return len(self._definitions)
+
+    def structure(self, index: int) -> Structure:
+        return self._structures[index]
+
+    def step(self, settings: abi.StepSettings, steps: int = 1) -> np.ndarray:
+        """Steps every structure; returns the per-structure status codes.
+        Raises the first failure after the others have committed."""
+        statuses = np.zeros(len(self), dtype=np.int32)
+        rc = self._lib.swb_batch_step(self._h, C.byref(settings), int(steps),
+                                      statuses.ctypes.data_as(C.c_void_p))
+        if rc != abi.OK:
+            err = _ERRORS.get(rc, SimwingError)(self._lib.swb_last_error().decode())
+            err.statuses = statuses
+            raise err
+        return statuses
+
+    def report(self) -> abi.BatchReport:
+        r = abi.BatchReport()
+        _check(self._lib.swb_batch_get_report(self._h, C.byref(r)))
+        return r
+
+    def last_step_ms(self) -> float:
+        return float(self._lib.swb_batch_last_step_ms(self._h))

@@ -151,6 +151,19 @@ class ScheduleReport(C.Structure):
                 ("cluster_barriers_per_iteration", C.c_int32)]
 
 
+class BatchOptions(C.Structure):
+    _fields_ = [("device", C.c_int32), ("cluster_ctas", C.c_int32), ("target_patch_nodes", C.c_int32),
+                ("block_threads", C.c_int32), ("graph_steps", C.c_int32), ("flags", C.c_uint32),
+                ("autotune_iterations", C.c_int32), ("reserved", C.c_int32)]
+
+
+class BatchReport(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "structures", "clusters", "cluster_ctas", "idle_ctas", "block_threads", "target_patch_nodes",
+        "shared_bytes", "max_cluster_stages", "resident_clusters", "colours_per_sync", "autotune_candidates",
+        "reserved")] + [("candidate_patch_nodes", C.c_int32 * 8), ("candidate_ms_per_step", C.c_double * 8)]
+
+
 class PatchParams(C.Structure):
     _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("width", C.c_double), ("height", C.c_double),
                 ("areal_density", C.c_double), ("distance_compliance", C.c_double),
@@ -174,6 +187,7 @@ OK, INVALID_ARGUMENT, OUT_OF_RANGE, SUSPENSION_ERROR, CONTACT_ERROR, NON_FINITE,
 
 DISTANCE, CABLE, SUSPENSION_TIE, SEAM_STITCH = 1, 2, 3, 4
 OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID = 1, 2, 4
+BATCH_AUTOTUNE = 1 << 8
 SWEEP_DISTANCE, SWEEP_DIHEDRAL = 0, 1
 
 P = C.POINTER
@@ -212,6 +226,14 @@ _PROTOTYPES = {
     "swb_structure_last_step_ms": (C.c_double, [C.c_void_p]),
     "swb_plan_schedule": (C.c_int, [P(StructureDefinition), P(SolverOptions), P(ScheduleReport), C.c_void_p,
                                     C.c_void_p]),
+    "swb_default_batch_options": (None, [P(BatchOptions)]),
+    "swb_batch_create": (C.c_int, [C.c_void_p, C.c_uint64, P(BatchOptions), P(C.c_void_p)]),
+    "swb_batch_destroy": (None, [C.c_void_p]),
+    "swb_batch_size": (C.c_uint64, [C.c_void_p]),
+    "swb_batch_structure": (C.c_void_p, [C.c_void_p, C.c_uint64]),
+    "swb_batch_step": (C.c_int, [C.c_void_p, P(StepSettings), C.c_int32, C.c_void_p]),
+    "swb_batch_get_report": (C.c_int, [C.c_void_p, P(BatchReport)]),
+    "swb_batch_last_step_ms": (C.c_double, [C.c_void_p]),
     "swb_reference_colouring": (C.c_int, [P(StructureDefinition), C.c_void_p, C.c_void_p, C.c_uint64,
                                           P(C.c_uint64), P(C.c_uint64)]),
     "swb_default_patch_params": (None, [P(PatchParams)]),

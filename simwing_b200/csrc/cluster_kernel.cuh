@@ -20,9 +20,13 @@ namespace swb {
 
 namespace dev {
 
-__device__ __forceinline__ float4* node_at(uint32_t ref, uint32_t me, float4* x, float4* const* peers) {
+// `ref` names a node by (instance rank << 12 | local index); `rank_base` is
+// the instance's first rank in the cluster (0 unless several structures
+// share the cluster).
+__device__ __forceinline__ float4* node_at(uint32_t ref, uint32_t me, uint32_t rank_base, float4* x,
+                                           float4* const* peers) {
     const uint32_t r = ref >> 12;
-    return (r == me ? x : peers[r]) + (ref & 0xfffu);
+    return (r == me ? x : peers[r + rank_base]) + (ref & 0xfffu);
 }
 
 // One constraint record held in registers between its prefetch and its use.
@@ -49,12 +53,12 @@ __device__ __forceinline__ ClusterRecord load_record(const ClusterKindDev& K, in
 // shared-memory offset in every CTA, so a peer's node is this CTA's address
 // mapped to the peer's rank (mapa); a local node keeps its own address,
 // which is valid in the cluster window.
-__device__ __forceinline__ uint32_t node_addr(uint32_t ref, uint32_t me, uint32_t x_base) {
+__device__ __forceinline__ uint32_t node_addr(uint32_t ref, uint32_t me, uint32_t rank_base, uint32_t x_base) {
     const uint32_t rank = ref >> 12;
     const uint32_t local = x_base + (ref & 0xfffu) * 16u;
     if (rank == me) return local;
     uint32_t remote;
-    asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+    asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank + rank_base));
     return remote;
 }
 __device__ __forceinline__ float4 ld_node(uint32_t addr) {
@@ -71,10 +75,10 @@ __device__ __forceinline__ void st_node(uint32_t addr, float4 v) {
                  : "memory");
 }
 
-__device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, uint32_t me, uint32_t x_base,
-                                             float* lam, uint32_t first, float inv_dt2) {
-    const uint32_t pa = node_addr(r.ab & 0xffffu, me, x_base);
-    const uint32_t pb = node_addr(r.ab >> 16, me, x_base);
+__device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, uint32_t me, uint32_t rank_base,
+                                             uint32_t x_base, float* lam, uint32_t first, float inv_dt2) {
+    const uint32_t pa = node_addr(r.ab & 0xffffu, me, rank_base, x_base);
+    const uint32_t pb = node_addr(r.ab >> 16, me, rank_base, x_base);
     float l = lam[r.index - first];
     if (kind == 0) {
         float4 A = ld_node(pa), B = ld_node(pb);
@@ -82,8 +86,8 @@ __device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, u
         st_node(pa, A);
         st_node(pb, B);
     } else {
-        const uint32_t pc = node_addr(r.cd & 0xffffu, me, x_base);
-        const uint32_t pd = node_addr(r.cd >> 16, me, x_base);
+        const uint32_t pc = node_addr(r.cd & 0xffffu, me, rank_base, x_base);
+        const uint32_t pd = node_addr(r.cd >> 16, me, rank_base, x_base);
         float4 A = ld_node(pa), B = ld_node(pb), C = ld_node(pc), D = ld_node(pd);
         project_dihedral(A, B, C, D, r.rest, r.comp, l, inv_dt2);
         st_node(pa, A);
@@ -94,9 +98,14 @@ __device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, u
     lam[r.index - first] = l;
 }
 
-constexpr int kClusterMaxThreads = 768;
 
-__global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const __grid_constant__ ClusterParams p) {
+// kPacked = false: one structure per cluster (cluster index = structure).
+// kPacked = true: a cluster carries several structures, each on its own
+// contiguous range of ranks, all in lockstep over the cluster's stage count;
+// the structure's buffers follow the launch role and its committed-buffer
+// rotation (see ClusterParams).
+template <bool kPacked>
+__global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(const __grid_constant__ ClusterParams p) {
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t bar;
@@ -104,8 +113,22 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const 
     __shared__ float4* peers[16];
     __shared__ float3 shift_s;
     cg::cluster_group cluster = cg::this_cluster();
-    const uint32_t me = cluster.block_rank();
-    const ClusterInstance& I = p.instances[blockIdx.x / p.ctas];
+    ClusterSlot slot{};
+    if constexpr (kPacked) {
+        slot = p.slots[blockIdx.x];
+        if (slot.instance < 0) {
+            // idle rank: take every cluster barrier the busy ranks take
+            const int barriers = 3 + p.iterations * (slot.stages + slot.suspension) +
+                                 (p.iterations > 0 ? slot.seam_stages : 0);
+            for (int b = 0; b < barriers; ++b) cluster.sync();
+            return;
+        }
+    }
+    const uint32_t rank_base = kPacked ? static_cast<uint32_t>(slot.rank_base) : 0u;
+    const uint32_t me = cluster.block_rank() - rank_base;
+    const ClusterInstance& I =
+        kPacked ? p.instances[(static_cast<size_t>(slot.instance) * 3 + p.rotation[slot.instance]) * 3 + p.role]
+                : p.instances[blockIdx.x / p.ctas];
     const int tid = threadIdx.x;
     float4* x = reinterpret_cast<float4*>(smem + p.smem_x);
     float4* v = reinterpret_cast<float4*>(smem + p.smem_v);
@@ -177,6 +200,9 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const 
     // on the current one, so the record fetch from L2 overlaps the current
     // stage and its cluster barrier.
     const int S0 = I.kind[0].stages, S1 = I.kind[1].stages, S = S0 + S1;
+    const int stages_c = kPacked ? slot.stages : S;                       // cluster-wide
+    const bool susp_c = kPacked ? slot.suspension != 0 : I.susp_cta >= 0;  // cluster-wide
+    const int seam_c = kPacked ? slot.seam_stages : I.seam_stages;         // cluster-wide
     uint32_t* soff = reinterpret_cast<uint32_t*>(smem + p.smem_offsets);  // [S + 2]: stage starts, then ends
     for (int i = tid; i <= S0; i += blockDim.x)
         soff[i] = __ldg(I.kind[0].offsets + static_cast<size_t>(me) * (S0 + 1) + i);
@@ -192,34 +218,38 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const 
     if (p.iterations > 0 && S > 0) next = load_record(I.kind[S0 > 0 ? 0 : 1], S0 > 0 ? 0 : 1, stage_lo(0) + tid,
                                                       stage_hi(0));
     for (int it = 0; it < p.iterations; ++it) {
-        for (int g = 0; g < S; ++g) {
-            const int kind = g < S0 ? 0 : 1;
-            const ClusterRecord cur = next;
-            // prefetch the next stage (wrapping to the next iteration)
-            const int gn = g + 1 < S ? g + 1 : 0;
-            const int kn = gn < S0 ? 0 : 1;
-            next = load_record(I.kind[kn], kn, stage_lo(gn) + tid, stage_hi(gn));
-            const uint32_t first = kind ? first1 : first0;
-            float* lam = kind ? lam1 : lam0;
-            if (cur.index != ~0u) apply_record(cur, kind, me, x_base, lam, first, p.inv_dt2);
-            for (uint32_t i = stage_lo(g) + tid + blockDim.x; i < stage_hi(g); i += blockDim.x)
-                apply_record(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, x_base, lam, first,
-                             p.inv_dt2);
+        for (int g = 0; g < stages_c; ++g) {
+            if (!kPacked || g < S) {
+                const int kind = g < S0 ? 0 : 1;
+                const ClusterRecord cur = next;
+                // prefetch the next stage (wrapping to the next iteration)
+                const int gn = g + 1 < S ? g + 1 : 0;
+                const int kn = gn < S0 ? 0 : 1;
+                next = load_record(I.kind[kn], kn, stage_lo(gn) + tid, stage_hi(gn));
+                const uint32_t first = kind ? first1 : first0;
+                float* lam = kind ? lam1 : lam0;
+                if (cur.index != ~0u) apply_record(cur, kind, me, rank_base, x_base, lam, first, p.inv_dt2);
+                for (uint32_t i = stage_lo(g) + tid + blockDim.x; i < stage_hi(g); i += blockDim.x)
+                    apply_record(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, rank_base, x_base, lam,
+                                 first, p.inv_dt2);
+            }
             cluster.sync();
         }
-        if (I.susp_cta >= 0) {
+        if (susp_c) {
             if (owner && tid == 0) line_iteration(*I.payload_def, pay, x, p.dt, I.status);
             cluster.sync();
         }
     }
     // ---- final seam-stitch projections (soft_body.cpp:1389-1405) ----------
     if (p.iterations > 0) {
-        for (int s = 0; s < I.seam_stages; ++s) {
+        for (int s = 0; s < seam_c; ++s) {
             const uint32_t* off = I.seam_offsets + static_cast<size_t>(me) * (I.seam_stages + 1);
-            for (uint32_t i = __ldg(off + s) + tid; i < __ldg(off + s + 1); i += blockDim.x) {
+            const uint32_t lo = s < I.seam_stages ? __ldg(off + s) : 0u;
+            const uint32_t hi = s < I.seam_stages ? __ldg(off + s + 1) : 0u;
+            for (uint32_t i = lo + tid; i < hi; i += blockDim.x) {
                 const uint32_t r = __ldg(I.seam_ab + i);
-                float4* pa = node_at(r & 0xffffu, me, x, peers);
-                float4* pb = node_at(r >> 16, me, x, peers);
+                float4* pa = node_at(r & 0xffffu, me, rank_base, x, peers);
+                float4* pb = node_at(r >> 16, me, rank_base, x, peers);
                 float4 A = *pa, B = *pb;
                 float l = 0.0f;  // rigid stitch: alpha = 0
                 project_distance(A, B, 0.0f, 0.0f, l, p.inv_dt2);
@@ -252,7 +282,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const 
     if (I.susp_cta < 0 && tid == 0) shift_s = make_float3(0.0f, 0.0f, 0.0f);
     cluster.sync();
     float3 shift = shift_s;
-    if (I.susp_cta >= 0) shift = *cluster.map_shared_rank(&shift_s, I.susp_cta);
+    if (I.susp_cta >= 0) shift = *cluster.map_shared_rank(&shift_s, I.susp_cta + static_cast<int>(rank_base));
     // ---- write the trial state --------------------------------------------
     int bad = 0;
     for (uint32_t i = tid; i < n; i += blockDim.x) {
@@ -278,6 +308,11 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel(const 
     }
     cluster.sync();  // no CTA leaves while a peer may still read its memory
 }
+
+// One structure per cluster (the plain step) and several structures per
+// cluster (the batched step).
+inline constexpr auto xpbd_cluster_kernel = &xpbd_cluster_kernel_t<false>;
+inline constexpr auto xpbd_cluster_packed_kernel = &xpbd_cluster_kernel_t<true>;
 
 }  // namespace dev
 }  // namespace swb

@@ -8,6 +8,10 @@
 
 namespace swb {
 
+namespace dev {
+constexpr int kClusterMaxThreads = 768;  // threads per CTA of the cluster step kernels
+}
+
 struct ClusterKindDev {
     const uint32_t* offsets;   // [ctas * (stages + 1)]
     const uint32_t* ab;
@@ -45,9 +49,24 @@ struct ClusterInstance {
     int pad;
 };
 
+// Packed launches (several structures per cluster): what one CTA runs.
+// The loop bounds are those of the whole cluster, so that every CTA of the
+// cluster takes the same cluster barriers.
+struct ClusterSlot {
+    int instance;      // index into the launch's structures; -1 = idle CTA
+    int rank_base;     // first cluster rank of that structure
+    int stages;        // colour stages per iteration: max over the cluster
+    int seam_stages;   // seam stages: max over the cluster
+    int suspension;    // 1 when a structure of the cluster has a pilot
+    int pad[3];
+};
+
 struct ClusterParams {
-    const ClusterInstance* instances;  // one per cluster of the launch
-    int ctas;
+    const ClusterInstance* instances;  // one per cluster of the launch; packed: [structure][rotation][role]
+    int ctas;                          // CTAs per cluster
+    const ClusterSlot* slots;          // packed launches: one per CTA
+    const int* rotation;               // packed launches: committed buffer per structure
+    int role;                          // packed launches: 0 = S->T1, 1 = T1->T2, 2 = T2->T1
     float dt, inv_dt, inv_dt2, damping;
     float3 gravity, ref_velocity;
     int iterations;

@@ -345,7 +345,7 @@ void StructureImpl::upload_grid_tables() {
 
 void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDeviceProp& prop) {
     StepParams& p = params;
-    (void)prop;
+    const size_t smem_limit_ = prop.sharedMemPerBlockOptin > 2048 ? prop.sharedMemPerBlockOptin - 2048 : 0;
     // diagnostics arrays (definition order of distance-like constraints)
     {
         std::vector<uint32_t> a(def.constraints.size()), b(def.constraints.size());
@@ -481,8 +481,12 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
             }
         d_instances = dupload(owned, inst, stream);
         cparams.copy_budget = 4000000000LL;
+        // The attribute is a per-kernel limit shared by every structure in
+        // the process: it is raised to the device limit, never set to this
+        // structure's need (a smaller structure built later would otherwise
+        // lower it below what an earlier one launches with).
         cuda_check(cudaFuncSetAttribute(dev::xpbd_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(cluster_smem)),
+                                        static_cast<int>(smem_limit_)),
                    "shared memory request of the cluster schedule");
         if (G > 8)
             cuda_check(cudaFuncSetAttribute(dev::xpbd_cluster_kernel,
@@ -504,9 +508,11 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
         if (clusters < 1) raise(SWB_UNSUPPORTED, "a cluster of " + std::to_string(G) + " CTAs cannot be scheduled");
     } else {
         // launch feasibility of the cooperative grid
+        if (p.smem_total > smem_limit_)
+            raise(SWB_UNSUPPORTED, "shared memory request (mesh patch too large for the block count)");
         cuda_check(cudaFuncSetAttribute(dev::xpbd_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(p.smem_total)),
-                   "shared memory request (mesh patch too large for the block count)");
+                                        static_cast<int>(smem_limit_)),
+                   "shared memory limit of the grid schedule");
         int per_sm = 0;
         cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::xpbd_step_kernel, threads,
                                                                  p.smem_total),
@@ -537,10 +543,24 @@ void StructureImpl::upload_pressure() {
         if (pressure[t] == 0.0) continue;
         for (int k = 0; k < 3; ++k) list[cur[slot_of_node[def.triangles[t].nodes[k]]]++] = static_cast<uint32_t>(t);
     }
-    if (d_tri) { cudaFree(d_tri); cudaFree(d_tri_off); cudaFree(d_tri_list); owned.erase(std::remove_if(owned.begin(), owned.end(), [&](void* q) { return q == d_tri || q == d_tri_off || q == d_tri_list; }), owned.end()); }
-    d_tri = dupload(owned, tri, stream);
-    d_tri_off = dupload(owned, off, stream);
-    d_tri_list = dupload(owned, list, stream);
+    // The tables keep their addresses for the structure's lifetime (the
+    // cluster instance records and batches hold them): allocated once, with
+    // room for every triangle under pressure, then overwritten in stream order.
+    if (!d_tri) {
+        d_tri = dalloc<uint4>(owned, tri.size());
+        d_tri_off = dalloc<uint32_t>(owned, N + 1);
+        d_tri_list = dalloc<uint32_t>(owned, 3 * def.triangles.size());
+    }
+    if (!tri.empty())
+        cuda_check(cudaMemcpyAsync(d_tri, tri.data(), tri.size() * sizeof(uint4), cudaMemcpyHostToDevice, stream),
+                   "pressure upload");
+    cuda_check(cudaMemcpyAsync(d_tri_off, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream),
+               "pressure upload");
+    if (!list.empty())
+        cuda_check(cudaMemcpyAsync(d_tri_list, list.data(), list.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                   stream),
+                   "pressure upload");
+    cuda_check(cudaStreamSynchronize(stream), "pressure upload");
     params.tri = d_tri;
     params.tri_offsets = d_tri_off;
     params.tri_list = d_tri_list;
@@ -646,29 +666,63 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out)
                "cudaLaunchCooperativeKernel");
 }
 
-swb_status StructureImpl::read_status(std::string& message) {
-    Control c{};
-    cuda_check(cudaMemcpyAsync(&c, d_control, sizeof(Control), cudaMemcpyDeviceToHost, stream), "status");
-    cuda_check(cudaStreamSynchronize(stream), "step");
-    if (c.status[0] == 0) return SWB_OK;
-    if (c.status[0] & dev::kStatusSyncTimeout) {
+cudaError_t packed_kernel_limits(int max_dynamic_smem, bool non_portable_cluster) {
+    cudaError_t rc = cudaFuncSetAttribute(dev::xpbd_cluster_packed_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem);
+    if (rc == cudaSuccess && non_portable_cluster)
+        rc = cudaFuncSetAttribute(dev::xpbd_cluster_packed_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return rc;
+}
+
+cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg) {
+    return cudaOccupancyMaxActiveClusters(clusters, dev::xpbd_cluster_packed_kernel, &cfg);
+}
+
+cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params) {
+    return cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_packed_kernel, params);
+}
+
+swb_status decode_status(const int status[2], std::string& message) {
+    if (status[0] == 0) return SWB_OK;
+    if (status[0] & dev::kStatusSyncTimeout) {
         message = "device-wide barrier timed out";
         return SWB_SYNC_TIMEOUT;
     }
-    if (c.status[0] & dev::kStatusCopyTimeout) {
+    if (status[0] & dev::kStatusCopyTimeout) {
         message = "shared-memory staging timed out";
         return SWB_SYNC_TIMEOUT;
     }
-    if (c.status[0] & dev::kStatusSuspension) {
+    if (status[0] & dev::kStatusSuspension) {
         static const char* what[] = {"suspension failure", "line geometry is non-finite or scale-degenerate",
                                      "invalid unilateral line projection input", "zero generalized effective mass",
                                      "payload trial state is non-finite or unnormalized",
                                      "maximum line residual exceeds configured bound", "invalid payload orientation"};
-        message = std::string("SuspensionError: ") + what[std::clamp(c.status[1], 0, 6)];
+        message = std::string("SuspensionError: ") + what[std::clamp(status[1], 0, 6)];
         return SWB_SUSPENSION_ERROR;
     }
     message = "trial step produced a non-finite state";
     return SWB_NON_FINITE;
+}
+
+swb_status StructureImpl::read_status(std::string& message) {
+    Control c{};
+    cuda_check(cudaMemcpyAsync(&c, d_control, sizeof(Control), cudaMemcpyDeviceToHost, stream), "status");
+    cuda_check(cudaStreamSynchronize(stream), "step");
+    return decode_status(c.status, message);
+}
+
+void StructureImpl::commit(int new_cur, int steps, const swb_step_settings& st) {
+    cur = new_cur;
+    swb_vec3 applied{0, 0, 0};
+    for (auto& f : pending) {
+        applied.x += f.x; applied.y += f.y; applied.z += f.z;
+        if (f.x != 0.0 || f.y != 0.0 || f.z != 0.0) forces_dirty = true;
+        f = swb_vec3{0, 0, 0};
+    }
+    last_applied = applied;
+    accepted += static_cast<uint64_t>(steps);
+    time += st.time_step * steps;
+    last_dt = st.time_step / st.substeps;
 }
 
 swb_status StructureImpl::step(const swb_step_settings& st, int steps, swb_diagnostics* out) {
@@ -708,17 +762,7 @@ swb_status StructureImpl::step(const swb_step_settings& st, int steps, swb_diagn
         cur = start;
         raise(status, message);
     }
-    cur = a;
-    swb_vec3 applied{0, 0, 0};
-    for (auto& f : pending) {
-        applied.x += f.x; applied.y += f.y; applied.z += f.z;
-        if (f.x != 0.0 || f.y != 0.0 || f.z != 0.0) forces_dirty = true;
-        f = swb_vec3{0, 0, 0};
-    }
-    last_applied = applied;
-    accepted += static_cast<uint64_t>(steps);
-    time += st.time_step * steps;
-    last_dt = st.time_step / st.substeps;
+    commit(a, steps, st);
     if (out) diagnostics(out);
     return SWB_OK;
 }
@@ -842,7 +886,9 @@ swb_status swb_structure_create(const swb_structure_definition* definition, cons
     });
 }
 
-void swb_structure_destroy(swb_structure* s) { delete s; }
+void swb_structure_destroy(swb_structure* s) {
+    if (s && !s->borrowed) delete s;
+}
 
 uint64_t swb_structure_fingerprint(const swb_structure* s) { return s ? s->s.fingerprint : 0; }
 uint64_t swb_structure_accepted_steps(const swb_structure* s) { return s ? s->s.accepted : 0; }

@@ -26,6 +26,15 @@ struct Control {
 
 constexpr int kDiagBlocks = 148;
 
+// Host entry points of the packed cluster kernel (several structures per
+// cluster), defined beside the kernels.
+cudaError_t packed_kernel_limits(int max_dynamic_smem, bool non_portable_cluster);
+cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg);
+cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params);
+
+// Status words written by the step kernels -> status and message.
+swb_status decode_status(const int status[2], std::string& message);
+
 struct StructureImpl {
     OwnedDefinition def;
     bool cluster_mode = false;
@@ -91,6 +100,9 @@ struct StructureImpl {
     void validate_settings(const swb_step_settings& st) const;
     void launch_substep(const swb_step_settings& st, int in, int out);
     swb_status read_status(std::string& message);
+    // Accepts `steps` steps that left the state in buffer `new_cur`: the
+    // pending loads are consumed, the counters advance.
+    void commit(int new_cur, int steps, const swb_step_settings& st);
     swb_status step(const swb_step_settings& st, int steps, swb_diagnostics* out);
     void copy_state(int from, int to);
     void fetch(std::vector<float4>& pos, std::vector<float4>& prev, std::vector<float4>& vel, DevPayloadState& pay,
@@ -102,4 +114,5 @@ struct StructureImpl {
 
 struct swb_structure {
     swb::StructureImpl s;
+    bool borrowed = false;  // owned by a batch; swb_structure_destroy leaves it alone
 };
