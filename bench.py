@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=100)
     p.add_argument("--cpu-sample-steps", type=int, default=12)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--batch-size", type=int, default=64)
     return p.parse_args()
 
 
@@ -72,6 +74,62 @@ def algorithmic_bytes(definition, iterations=48, substeps=1):
     e_s = v.suspension.contents.segment_count if v.suspension else 0
     return substeps * (144 * n + 52 * t + iterations * (88 * e_d + 160 * e_b + 236 * e_m + 52 * e_s)
                        + 4 * (e_d + e_b) + 12 * e_m)
+
+
+def batched_leg(sw, st, count, rank, world, dist, device):
+    """Batched wings: `count` structures of uneven sizes in one packed
+    launch per step, 120-step CUDA-graph blocks; against the same wings
+    solved one after another by the plain solver."""
+    import concurrent.futures as cf
+
+    import torch
+
+    defs = sw.generate_wing_batch(count, seed=2024)
+    tris = [d.counts()["triangles"] for d in defs]
+    batch = sw.Batch(defs, sw.BatchOptions(device=device, flags=sw.abi.BATCH_AUTOTUNE))
+    rep = batch.report()
+    block = 120
+    batch.step(st, block)  # warm-up block (captures the graph)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    batch.step(st, block)
+    ms = batch.last_step_ms()
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / block
+    out = {"workload": f"{count} wings, cells U{{20..60}}, chordwise {{30,45,60}}, aspect ratio U(4.5,7), "
+                       "compliance x lognormal(0,0.2), seed 2024; 48 iterations, 1 substep",
+           "structures": count, "triangles_min": min(tris), "triangles_max": max(tris),
+           "triangles_total": sum(tris), "graph_steps": block, "launches_per_step": 1,
+           "ms_per_step": ms_per_step, "wing_steps_per_s": world * count / (ms_per_step / 1000.0),
+           "target_patch_nodes": rep.target_patch_nodes, "clusters": rep.clusters,
+           "cluster_ctas": rep.cluster_ctas, "resident_clusters": rep.resident_clusters,
+           "block_threads": rep.block_threads,
+           "autotune_ms_per_step": {str(rep.candidate_patch_nodes[k]): rep.candidate_ms_per_step[k]
+                                    for k in range(rep.autotune_candidates)}}
+    batch.close()
+    if rank == 0:
+        # the same wings, one plain structure after another
+        opts = sw.SolverOptions(device=device)
+        with cf.ThreadPoolExecutor(8) as pool:
+            plains = list(pool.map(lambda d: sw.Structure(d, opts), defs))
+        total = 0.0
+        for s in plains:
+            for _ in range(2):
+                s.step(st, diagnostics=False)
+            times = []
+            for _ in range(3):
+                s.step(st, diagnostics=False)
+                times.append(s.last_step_ms())
+            total += min(times)
+            s.close()
+        out["sequential_plain_ms_per_step"] = total / count
+        out["sequential_plain_wing_steps_per_s"] = count / (total / 1000.0)
+        out["speedup_vs_sequential"] = out["wing_steps_per_s"] / world / out["sequential_plain_wing_steps_per_s"]
+    return out
 
 
 def measured_peak():
@@ -176,6 +234,10 @@ def physical_cores():
 
 
 def run_reference_arm(args):
+    """The reference's own CPU step (oracle/_ref: src/softwing + src/fsi
+    compiled from source) on this host's cores, through Structure::step with
+    workerThreads = physical cores; each timed step is one wing step of the
+    same workload.  Rank 0 alone runs under torchrun."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -183,11 +245,6 @@ def run_reference_arm(args):
 
     definition = sw.generate_wing()
     cores = physical_cores()
-    per_step = []
-    from oracle import oracle as O
-
-    for _ in range(max(0, args.warmup)):
-        pass
     sample = max(1, min(args.steps, 8))
     value, kind, used = cpu_reference_run(definition, sample, cores)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": sample,
@@ -285,6 +342,10 @@ def main():
     achieved = bytes_per_step / (ms_per_step / 1000.0) / 1e9
     report = structure.schedule_report()
 
+    batched = None
+    if not args.no_batched:
+        batched = batched_leg(sw, st, args.batch_size, rank, world, dist, local)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu_value, kind, used = cpu_reference_run(definition, args.cpu_sample_steps, 0)
@@ -309,6 +370,7 @@ def main():
                          "stages_per_iteration": report.local_stages_per_iteration,
                          "shared_bytes": report.shared_bytes},
             "final_diagnostics": {"finite": bool(diag.finite), "max_distance_error": diag.maximum_distance_error},
+            "batched": batched,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -1,12 +1,14 @@
 """ORACLE / TEST INFRASTRUCTURE ONLY.
 
-ctypes loaders for the two CPU checkers:
+ctypes loaders for the CPU checkers:
   * PortStructure -- oracle/liboracle.so, the plain-C FP64 restatement of
     the reference step (oracle/xpbd_oracle.c);
   * RefStructure  -- oracle/_ref/libswref.so, the reference's own
     softwing core + Structure adapter compiled from source
-    (oracle/ref_shim.cpp, oracle/Makefile).
-Both take the product's swb_structure_definition, so the device solver and
+    (oracle/ref_shim.cpp, oracle/Makefile);
+  * rollout_gradient -- oracle/libadjoint.so, the FP64 reference gradient
+    of a rollout loss (oracle/xpbd_adjoint.cpp).
+All take the product's swb_structure_definition, so the device solver and
 the checkers run on identical inputs.  Only tests/, __graft_entry__.smoke()
 and bench.py's CPU-baseline leg import this module.
 """
@@ -22,6 +24,7 @@ from simwing_b200 import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libswref.so")
+ADJOINT_PATH = os.path.join(HERE, "libadjoint.so")
 
 P = C.POINTER
 _PORT = {
@@ -54,6 +57,13 @@ _REF = {
     "swref_read_suspension": (C.c_int, [C.c_void_p, P(abi.PayloadState), C.c_void_p, C.c_uint64]),
     "swref_colouring": (C.c_int, [P(abi.StructureDefinition), C.c_void_p, C.c_void_p, C.c_uint64,
                                   P(C.c_uint64), P(C.c_uint64)]),
+}
+
+_ADJ = {
+    "swa_last_error": (C.c_char_p, []),
+    "swa_rollout_gradient": (C.c_int, [P(abi.StructureDefinition), P(abi.StepSettings), C.c_int, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(C.c_double), C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(C.c_double)]),
 }
 
 _libs = {}
@@ -205,3 +215,47 @@ def ref_colouring(definition):
     if status != 0:
         raise OracleError(status, lib.swref_last_error().decode())
     return order[:m], offsets[: colours.value + 1 if m else 0], int(parallel.value)
+
+
+def adjoint_library() -> C.CDLL:
+    if "adjoint" not in _libs:
+        _libs["adjoint"] = abi.bind(C.CDLL(ADJOINT_PATH), _ADJ)
+    return _libs["adjoint"]
+
+
+def rollout_gradient(definition, settings, steps, target, weights, forces=None, state=None, payload=None):
+    """FP64 loss and gradient of sum_i w_i |x_i(T) - target_i|^2 / sum w over
+    `steps` steps (the definition's insertion order is the sweep order) from
+    `state` (N x 3 x 3 node states as read_nodes returns: position, previous,
+    velocity; default: the definition at rest) and `payload` (13 values: com,
+    orientation wxyz, linear and angular velocity; default: the definition's
+    pilot).  Returns a dict: loss, final (N x 3), d_rest and d_comp
+    (per constraint), d_dihedral_comp (per dihedral), d_segment_rest (per
+    suspension segment, definition order), d_mass."""
+    lib = adjoint_library()
+    v = definition.view
+    n, m, h = v.node_count, v.constraint_count, v.dihedral_count
+    ns = v.suspension.contents.segment_count if v.suspension else 0
+    target = np.ascontiguousarray(target, dtype=np.float64).reshape(n, 3)
+    weights = np.ascontiguousarray(weights, dtype=np.float64).reshape(n)
+    f = None if forces is None else np.ascontiguousarray(forces, dtype=np.float64).reshape(n, 3)
+    x0 = None
+    if state is not None:
+        st = np.asarray(state, dtype=np.float64).reshape(n, 3, 3)
+        x0 = np.ascontiguousarray(np.concatenate([st[:, 0, :], st[:, 2, :]], axis=1))
+    p0 = None if payload is None else np.ascontiguousarray(payload, dtype=np.float64).reshape(13)
+    out = {"final": np.zeros((n, 3)), "d_rest": np.zeros(max(m, 1)), "d_comp": np.zeros(max(m, 1)),
+           "d_dihedral_comp": np.zeros(max(h, 1)), "d_segment_rest": np.zeros(max(ns, 1))}
+    loss, mass = C.c_double(), C.c_double()
+    rc = lib.swa_rollout_gradient(definition.pointer, C.byref(settings), int(steps),
+                                  None if x0 is None else x0.ctypes.data, None if p0 is None else p0.ctypes.data,
+                                  None if f is None else f.ctypes.data, target.ctypes.data, weights.ctypes.data,
+                                  C.byref(loss), out["final"].ctypes.data, out["d_rest"].ctypes.data,
+                                  out["d_comp"].ctypes.data, out["d_dihedral_comp"].ctypes.data,
+                                  out["d_segment_rest"].ctypes.data, C.byref(mass))
+    if rc != 0:
+        raise OracleError(abi.INVALID_ARGUMENT, lib.swa_last_error().decode())
+    out["d_rest"], out["d_comp"] = out["d_rest"][:m], out["d_comp"][:m]
+    out["d_dihedral_comp"], out["d_segment_rest"] = out["d_dihedral_comp"][:h], out["d_segment_rest"][:ns]
+    out["loss"], out["d_mass"] = loss.value, mass.value
+    return out

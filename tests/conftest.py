@@ -19,9 +19,9 @@ def _ensure_built():
     lib = os.path.join(ROOT, "simwing_b200", "libsimwing_b200.so")
     if not os.path.exists(lib):
         subprocess.run(["make", "-C", os.path.join(ROOT, "simwing_b200"), "-j8"], check=True)
-    port = os.path.join(ROOT, "oracle", "liboracle.so")
-    if not os.path.exists(port):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "port"], check=True)
+    for target, lib in (("port", "liboracle.so"), ("adjoint", "libadjoint.so")):
+        if not os.path.exists(os.path.join(ROOT, "oracle", lib)):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), target], check=True)
 
 
 _ensure_built()
