@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--batch-size", type=int, default=64)
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
 
 
@@ -129,6 +130,63 @@ def batched_leg(sw, st, count, rank, world, dist, device):
         out["sequential_plain_ms_per_step"] = total / count
         out["sequential_plain_wing_steps_per_s"] = count / (total / 1000.0)
         out["speedup_vs_sequential"] = out["wing_steps_per_s"] / world / out["sequential_plain_wing_steps_per_s"]
+    return out
+
+
+def adjoint_leg(sw, st, device):
+    """Adjoint calibration workload: the wing generator at 20 cells x 30
+    chordwise, settled for 60 steps; the target is the shape after 240
+    steps with every line's rest length scaled by lognormal(0, 0.02); the
+    loss is the mean squared distance of the fabric (triangle) nodes to it;
+    one gradient = a 240-step forward with a checkpoint every 16 steps plus
+    the backward (segment recompute with tape + reverse sweep)."""
+    import numpy as np
+
+    d = sw.generate_wing(cells=20, chordwise=30)
+    opts = sw.SolverOptions(device=device)
+    s = sw.Structure(d, opts)
+    for _ in range(60):
+        s.step(st, diagnostics=False)
+    state = s.node_states()
+    pilot = s.suspension_state()
+    # target: perturbed line rest lengths from the same state
+    rng = np.random.default_rng(2024)
+    perturbed = d.copy()
+    lines = sw.line_groups(d)
+    rest = perturbed.constraints()["rest_length"]
+    for g in lines:
+        rest[g] *= float(np.exp(rng.normal(0.0, 0.02)))
+    t = sw.Structure(perturbed, opts)
+    t.write_node_states(state)
+    t.write_payload_state(pilot.center_of_mass, pilot.body_to_world, pilot.linear_velocity, pilot.angular_velocity)
+    steps = 240
+    for _ in range(steps):
+        t.step(st, diagnostics=False)
+    target = t.positions()
+    t.close()
+    weights = np.zeros(s.node_count)
+    weights[d.triangles()["nodes"].astype(np.int64).ravel()] = 1.0
+    r = sw.Rollout(s, steps, 16)
+    r.forward(st, target, weights)
+    r.backward()  # warm-up (allocates the tapes)
+    loss = r.forward(st, target, weights)
+    g = r.backward()
+    fwd, bwd = r.forward_ms(), r.backward_ms()
+    cons = d.constraints()
+    line_grad = [float(np.sum(g["d_rest"][x] * cons["rest_length"][x]) / np.sum(cons["rest_length"][x])) for x in lines]
+    counts = d.counts()
+    out = {"workload": "wing 20 cells x 30 chordwise, settled 60 steps; 240-step rollout, checkpoint every 16 steps; "
+                       "target from line rest lengths x lognormal(0, 0.02); loss = mean squared distance of the "
+                       "fabric nodes",
+           "triangles": counts["triangles"], "nodes": counts["nodes"], "steps": steps, "checkpoint_interval": 16,
+           "parameters": {"line_rest_lengths": len(lines), "compliance_classes": 3,
+                          "riser_rest_lengths": int(counts["suspension_segments"]), "pilot_mass": 1},
+           "loss": loss, "forward_ms": fwd, "backward_ms": bwd,
+           "backward_over_forward": bwd / fwd, "gradient_over_forward": (fwd + bwd) / fwd,
+           "gradient_norm_lines": float(np.linalg.norm(line_grad)), "d_pilot_mass": g["d_mass"],
+           "d_riser_rest": [float(v) for v in g["d_segment_rest"]]}
+    r.close()
+    s.close()
     return out
 
 
@@ -346,6 +404,10 @@ def main():
     if not args.no_batched:
         batched = batched_leg(sw, st, args.batch_size, rank, world, dist, local)
 
+    adjoint = None
+    if not args.no_adjoint and rank == 0:
+        adjoint = adjoint_leg(sw, st, local)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu_value, kind, used = cpu_reference_run(definition, args.cpu_sample_steps, 0)
@@ -371,6 +433,7 @@ def main():
                          "shared_bytes": report.shared_bytes},
             "final_diagnostics": {"finite": bool(diag.finite), "max_distance_error": diag.maximum_distance_error},
             "batched": batched,
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -588,6 +588,56 @@ swb_status swb_batch_get_report(const swb_batch* batch, swb_batch_report* out);
 double swb_batch_last_step_ms(const swb_batch* batch);
 
 /* ------------------------------------------------------------------------ */
+/* Differentiable rollouts (adjoint).  No reference counterpart: the        */
+/* reference has no adjoint.  An autograd-style pair: forward runs `steps`  */
+/* steps of the structure from its committed state (left unchanged) with a */
+/* checkpoint every `checkpoint_interval` steps and returns the loss        */
+/*   L = sum_i w_i |x_i(T) - target_i|^2 / sum_i w_i   (world positions);   */
+/* backward returns dL/d(parameter) for every constraint's rest length and  */
+/* compliance, every dihedral's compliance, every suspension segment's rest */
+/* length and the pilot mass, by a reverse sweep of the discrete step       */
+/* (segments recomputed from their checkpoint with a tape).  One substep    */
+/* per step; the structure must run on the cluster schedule.  The external */
+/* loads and face pressures pending on the structure stay constant.         */
+/* ------------------------------------------------------------------------ */
+typedef struct swb_rollout swb_rollout;
+
+/* Output arrays of a backward pass; each is nullable.  Arrays are in
+ * definition order: d_rest / d_compliance have constraint_count entries
+ * (compliance adjoints are with respect to the magnitude of the
+ * compliance), d_dihedral_compliance dihedral_count, d_segment_rest
+ * segment_count; d_pilot_mass is a single value (0 without a pilot). */
+typedef struct swb_rollout_gradient {
+    double* d_rest;
+    double* d_compliance;
+    double* d_dihedral_compliance;
+    double* d_segment_rest;
+    double* d_pilot_mass;
+} swb_rollout_gradient;
+
+swb_status swb_rollout_create(swb_structure* structure,
+                              int32_t steps,
+                              int32_t checkpoint_interval, /* 0 = 16 */
+                              swb_rollout** out);
+void swb_rollout_destroy(swb_rollout* rollout);
+
+/* target_xyz: node_count x 3 world positions; weights: node_count, >= 0. */
+swb_status swb_rollout_forward(swb_rollout* rollout,
+                               const swb_step_settings* settings,
+                               const double* target_xyz,
+                               const double* weights,
+                               double* loss);
+swb_status swb_rollout_backward(swb_rollout* rollout,
+                                const swb_rollout_gradient* gradient);
+/* World positions at the end of the last forward (node_count x 3). */
+swb_status swb_rollout_final_positions(const swb_rollout* rollout,
+                                       double* xyz,
+                                       uint64_t count);
+/* Device time of the last forward / backward in milliseconds. */
+double swb_rollout_forward_ms(const swb_rollout* rollout);
+double swb_rollout_backward_ms(const swb_rollout* rollout);
+
+/* ------------------------------------------------------------------------ */
 /* Reference colouring (bit-exact restatement of                             */
 /* SoftBody::constraintColouring, soft_body.cpp:1978-2075): greedy first-fit */
 /* over the line graph in insertion order, colours ranked by descending      */

@@ -62,8 +62,9 @@ _REF = {
 _ADJ = {
     "swa_last_error": (C.c_char_p, []),
     "swa_rollout_gradient": (C.c_int, [P(abi.StructureDefinition), P(abi.StepSettings), C.c_int, C.c_void_p,
-                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(C.c_double), C.c_void_p,
-                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, P(C.c_double)]),
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       P(C.c_double), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       P(C.c_double)]),
 }
 
 _libs = {}
@@ -223,13 +224,17 @@ def adjoint_library() -> C.CDLL:
     return _libs["adjoint"]
 
 
-def rollout_gradient(definition, settings, steps, target, weights, forces=None, state=None, payload=None):
+def rollout_gradient(definition, settings, steps, target, weights, forces=None, state=None, payload=None,
+                     trajectory=None, trajectory_payloads=None):
     """FP64 loss and gradient of sum_i w_i |x_i(T) - target_i|^2 / sum w over
     `steps` steps (the definition's insertion order is the sweep order) from
     `state` (N x 3 x 3 node states as read_nodes returns: position, previous,
     velocity; default: the definition at rest) and `payload` (13 values: com,
     orientation wxyz, linear and angular velocity; default: the definition's
-    pilot).  Returns a dict: loss, final (N x 3), d_rest and d_comp
+    pilot).  `trajectory` (steps x N x 3 x 3) and `trajectory_payloads`
+    (steps x 13), when given, restart every step s > 0 from that state, so
+    the reverse sweep is evaluated along another solver's trajectory.
+    Returns a dict: loss, final (N x 3), d_rest and d_comp
     (per constraint), d_dihedral_comp (per dihedral), d_segment_rest (per
     suspension segment, definition order), d_mass."""
     lib = adjoint_library()
@@ -244,11 +249,19 @@ def rollout_gradient(definition, settings, steps, target, weights, forces=None, 
         st = np.asarray(state, dtype=np.float64).reshape(n, 3, 3)
         x0 = np.ascontiguousarray(np.concatenate([st[:, 0, :], st[:, 2, :]], axis=1))
     p0 = None if payload is None else np.ascontiguousarray(payload, dtype=np.float64).reshape(13)
+    traj = None
+    if trajectory is not None:
+        tr = np.asarray(trajectory, dtype=np.float64).reshape(steps, n, 3, 3)
+        traj = np.ascontiguousarray(np.concatenate([tr[:, :, 0, :], tr[:, :, 2, :]], axis=2))
+    tpay = None if trajectory_payloads is None else \
+        np.ascontiguousarray(trajectory_payloads, dtype=np.float64).reshape(steps, 13)
     out = {"final": np.zeros((n, 3)), "d_rest": np.zeros(max(m, 1)), "d_comp": np.zeros(max(m, 1)),
            "d_dihedral_comp": np.zeros(max(h, 1)), "d_segment_rest": np.zeros(max(ns, 1))}
     loss, mass = C.c_double(), C.c_double()
     rc = lib.swa_rollout_gradient(definition.pointer, C.byref(settings), int(steps),
                                   None if x0 is None else x0.ctypes.data, None if p0 is None else p0.ctypes.data,
+                                  None if traj is None else traj.ctypes.data,
+                                  None if tpay is None else tpay.ctypes.data,
                                   None if f is None else f.ctypes.data, target.ctypes.data, weights.ctypes.data,
                                   C.byref(loss), out["final"].ctypes.data, out["d_rest"].ctypes.data,
                                   out["d_comp"].ctypes.data, out["d_dihedral_comp"].ctypes.data,

@@ -1013,13 +1013,16 @@ const char* swa_last_error() { return g_err.c_str(); }
 // the definition's positions at rest) and `payload` (com xyz, orientation
 // wxyz, linear and angular velocity xyz; nullable: the definition's initial
 // pilot) with `forces` (node_count xyz, nullable) as the constant external
-// load, then evaluates the loss against `target`
-// (node_count xyz) with node weights `weights` and its gradient.  Outputs
+// load.  `step_states` / `step_payloads` (nullable; steps x node_count x 6
+// and steps x 13 in the same layouts) restart every step s > 0 from a given
+// trajectory, so that the reverse sweep runs along another solver's states.
+// Then evaluates the loss against `target` (node_count xyz) with node weights `weights` and its gradient.  Outputs
 // (nullable): final positions (node_count xyz), d rest / d compliance per
 // constraint, d compliance per dihedral, d rest per suspension segment
 // (definition order), d pilot mass.  Returns 0 on success.
 int swa_rollout_gradient(const swb_structure_definition* def, const swb_step_settings* st, int steps,
-                         const double* state, const double* payload, const double* forces, const double* target,
+                         const double* state, const double* payload, const double* step_states,
+                         const double* step_payloads, const double* forces, const double* target,
                          const double* weights, double* loss,
                          double* final_xyz, double* d_rest, double* d_comp, double* d_dihedral_comp,
                          double* d_segment_rest, double* d_mass) {
@@ -1055,11 +1058,28 @@ int swa_rollout_gradient(const swb_structure_definition* def, const swb_step_set
             R.P.v = {payload[7], payload[8], payload[9]};
             R.P.w = {payload[10], payload[11], payload[12]};
         }
-        for (int s = 0; s < steps; ++s)
+        for (int s = 0; s < steps; ++s) {
+            // optionally restart every step from a given trajectory (node
+            // position and velocity, pilot), so that the reverse sweep is
+            // evaluated along another solver's states
+            if (step_states && s > 0)
+                for (uint64_t i = 0; i < M.n; ++i) {
+                    const double* q = step_states + (static_cast<size_t>(s) * M.n + i) * 6;
+                    R.X[i] = {q[0], q[1], q[2]};
+                    R.V[i] = {q[3], q[4], q[5]};
+                }
+            if (step_payloads && s > 0 && M.susp) {
+                const double* q = step_payloads + static_cast<size_t>(s) * 13;
+                R.P.com = {q[0], q[1], q[2]};
+                R.P.q = {q[3], q[4], q[5], q[6]};
+                R.P.v = {q[7], q[8], q[9]};
+                R.P.w = {q[10], q[11], q[12]};
+            }
             if (!forward_step(R, true)) {
                 g_err = "forward step failed";
                 return 1;
             }
+        }
         double wsum = 0.0, L = 0.0;
         std::vector<V3<double>> Xb(M.n, {0, 0, 0}), Vb(M.n, {0, 0, 0});
         for (uint64_t i = 0; i < M.n; ++i) wsum += weights[i];

@@ -305,6 +305,39 @@ def generate_wing_batch(count: int = 64, seed: int = 2024, **overrides) -> list:
     return [generate_wing(**dict(p, **overrides)) for p in wing_batch_parameters(count, seed)]
 
 
+def line_groups(definition: Definition) -> list:
+    """The suspension lines of a definition as groups of cable constraints:
+    maximal chains of cables through nodes that exactly two cables share (a
+    line's particles, or a junction where one line continues into one
+    other).  Returns a list of constraint-index arrays."""
+    cons = definition.constraints()
+    cables = np.where(cons["kind"] == abi.CABLE)[0]
+    a = cons["first_node"][cables].astype(np.int64)
+    b = cons["second_node"][cables].astype(np.int64)
+    degree = np.bincount(np.concatenate([a, b]), minlength=definition.node_count)
+    parent = np.arange(len(cables))
+
+    def find(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+
+    first_at = {}
+    for j, (u, v) in enumerate(zip(a, b)):
+        for node in (int(u), int(v)):
+            if degree[node] != 2:
+                continue
+            if node in first_at:
+                parent[find(j)] = find(first_at[node])
+            else:
+                first_at[node] = j
+    groups = {}
+    for j in range(len(cables)):
+        groups.setdefault(find(j), []).append(int(cables[j]))
+    return [np.array(g, dtype=np.int64) for g in groups.values()]
+
+
 def reference_colouring(definition: Definition):
     """Bit-exact restatement of SoftBody::constraintColouringView."""
     lib = abi.library()
@@ -561,3 +594,71 @@ class Batch:
 
     def last_step_ms(self) -> float:
         return float(self._lib.swb_batch_last_step_ms(self._h))
+
+
+class Rollout:
+    """Differentiable rollout of a structure (swb_rollout_*): `forward`
+    steps it `steps` times from its committed state (left unchanged) and
+    returns the loss sum_i w_i |x_i(T) - target_i|^2 / sum w; `backward`
+    returns the loss gradient with respect to every constraint's rest length
+    and compliance, every dihedral's compliance, every suspension segment's
+    rest length and the pilot mass (definition order)."""
+
+    def __init__(self, structure: Structure, steps: int, checkpoint_interval: int = 16):
+        self._lib = abi.library()
+        self._structure = structure
+        h = C.c_void_p()
+        _check(self._lib.swb_rollout_create(structure.handle, int(steps), int(checkpoint_interval), C.byref(h)))
+        self._h = h
+        self.steps = int(steps)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.swb_rollout_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def forward(self, settings: abi.StepSettings, target, weights) -> float:
+        n = self._structure.node_count
+        t = np.ascontiguousarray(target, dtype=np.float64).reshape(n, 3)
+        w = np.ascontiguousarray(weights, dtype=np.float64).reshape(n)
+        loss = C.c_double()
+        _check(self._lib.swb_rollout_forward(self._h, C.byref(settings), t.ctypes.data, w.ctypes.data,
+                                             C.byref(loss)))
+        return loss.value
+
+    def backward(self) -> dict:
+        v = self._structure._definition.view
+        m, h = v.constraint_count, v.dihedral_count
+        ns = v.suspension.contents.segment_count if v.suspension else 0
+        out = {"d_rest": np.zeros(max(m, 1)), "d_comp": np.zeros(max(m, 1)),
+               "d_dihedral_comp": np.zeros(max(h, 1)), "d_segment_rest": np.zeros(max(ns, 1))}
+        mass = np.zeros(1)
+        g = abi.RolloutGradient(out["d_rest"].ctypes.data, out["d_comp"].ctypes.data,
+                                out["d_dihedral_comp"].ctypes.data, out["d_segment_rest"].ctypes.data,
+                                mass.ctypes.data)
+        _check(self._lib.swb_rollout_backward(self._h, C.byref(g)))
+        out["d_rest"], out["d_comp"] = out["d_rest"][:m], out["d_comp"][:m]
+        out["d_dihedral_comp"], out["d_segment_rest"] = out["d_dihedral_comp"][:h], out["d_segment_rest"][:ns]
+        out["d_mass"] = float(mass[0])
+        return out
+
+    def final_positions(self) -> np.ndarray:
+        n = self._structure.node_count
+        out = np.zeros((n, 3))
+        _check(self._lib.swb_rollout_final_positions(self._h, out.ctypes.data, n))
+        return out
+
+    def forward_ms(self) -> float:
+        return float(self._lib.swb_rollout_forward_ms(self._h))
+
+    def backward_ms(self) -> float:
+        return float(self._lib.swb_rollout_backward_ms(self._h))

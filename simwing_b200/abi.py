@@ -164,6 +164,11 @@ class BatchReport(C.Structure):
         "reserved")] + [("candidate_patch_nodes", C.c_int32 * 8), ("candidate_ms_per_step", C.c_double * 8)]
 
 
+class RolloutGradient(C.Structure):
+    _fields_ = [("d_rest", C.c_void_p), ("d_compliance", C.c_void_p), ("d_dihedral_compliance", C.c_void_p),
+                ("d_segment_rest", C.c_void_p), ("d_pilot_mass", C.c_void_p)]
+
+
 class PatchParams(C.Structure):
     _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("width", C.c_double), ("height", C.c_double),
                 ("areal_density", C.c_double), ("distance_compliance", C.c_double),
@@ -234,6 +239,13 @@ _PROTOTYPES = {
     "swb_batch_step": (C.c_int, [C.c_void_p, P(StepSettings), C.c_int32, C.c_void_p]),
     "swb_batch_get_report": (C.c_int, [C.c_void_p, P(BatchReport)]),
     "swb_batch_last_step_ms": (C.c_double, [C.c_void_p]),
+    "swb_rollout_create": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, P(C.c_void_p)]),
+    "swb_rollout_destroy": (None, [C.c_void_p]),
+    "swb_rollout_forward": (C.c_int, [C.c_void_p, P(StepSettings), C.c_void_p, C.c_void_p, P(C.c_double)]),
+    "swb_rollout_backward": (C.c_int, [C.c_void_p, P(RolloutGradient)]),
+    "swb_rollout_final_positions": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "swb_rollout_forward_ms": (C.c_double, [C.c_void_p]),
+    "swb_rollout_backward_ms": (C.c_double, [C.c_void_p]),
     "swb_reference_colouring": (C.c_int, [P(StructureDefinition), C.c_void_p, C.c_void_p, C.c_uint64,
                                           P(C.c_uint64), P(C.c_uint64)]),
     "swb_default_patch_params": (None, [P(PatchParams)]),

@@ -75,13 +75,22 @@ __device__ __forceinline__ void st_node(uint32_t addr, float4 v) {
                  : "memory");
 }
 
+// Projects one record.  Taping launches first store the record's inputs
+// (node positions and multiplier) at its index in this iteration's tape
+// blocks of `rtotal` entries.
+template <bool kTape = false>
 __device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, uint32_t me, uint32_t rank_base,
-                                             uint32_t x_base, float* lam, uint32_t first, float inv_dt2) {
+                                             uint32_t x_base, float* lam, uint32_t first, float inv_dt2,
+                                             float4* tape = nullptr, uint32_t rtotal = 0) {
     const uint32_t pa = node_addr(r.ab & 0xffffu, me, rank_base, x_base);
     const uint32_t pb = node_addr(r.ab >> 16, me, rank_base, x_base);
     float l = lam[r.index - first];
     if (kind == 0) {
         float4 A = ld_node(pa), B = ld_node(pb);
+        if constexpr (kTape) {
+            tape[r.index] = make_float4(A.x, A.y, A.z, l);
+            tape[rtotal + r.index] = B;
+        }
         project_distance(A, B, r.rest, r.comp, l, inv_dt2);
         st_node(pa, A);
         st_node(pb, B);
@@ -89,6 +98,12 @@ __device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, u
         const uint32_t pc = node_addr(r.cd & 0xffffu, me, rank_base, x_base);
         const uint32_t pd = node_addr(r.cd >> 16, me, rank_base, x_base);
         float4 A = ld_node(pa), B = ld_node(pb), C = ld_node(pc), D = ld_node(pd);
+        if constexpr (kTape) {
+            tape[r.index] = make_float4(A.x, A.y, A.z, l);
+            tape[rtotal + r.index] = B;
+            tape[2 * rtotal + r.index] = C;
+            tape[3 * rtotal + r.index] = D;
+        }
         project_dihedral(A, B, C, D, r.rest, r.comp, l, inv_dt2);
         st_node(pa, A);
         st_node(pb, B);
@@ -98,13 +113,27 @@ __device__ __forceinline__ void apply_record(const ClusterRecord& r, int kind, u
     lam[r.index - first] = l;
 }
 
+// Records the pilot's inputs of a line iteration (or of the finish).
+__device__ __forceinline__ void tape_pilot(PilotTape& t, const DevPayloadState& pay, const AdjointPilot& ap,
+                                           const float4* x, const float4* v) {
+    t.com[0] = pay.com.x; t.com[1] = pay.com.y; t.com[2] = pay.com.z;
+    t.q[0] = pay.q.x; t.q[1] = pay.q.y; t.q[2] = pay.q.z; t.q[3] = pay.q.w;
+    for (int k = 0; k < 8; ++k) t.lambda[k] = pay.lambda[k];
+    for (int s = 0; s < ap.slots; ++s) {
+        t.xs[s] = x[ap.slot_node[s]];
+        if (v) t.vs[s] = v[ap.slot_node[s]];
+    }
+}
 
 // kPacked = false: one structure per cluster (cluster index = structure).
 // kPacked = true: a cluster carries several structures, each on its own
 // contiguous range of ranks, all in lockstep over the cluster's stage count;
 // the structure's buffers follow the launch role and its committed-buffer
 // rotation (see ClusterParams).
-template <bool kPacked>
+// kTape = true: one structure per cluster; the step also records the inputs
+// of every projection, line iteration and the pilot finish into p.tape for
+// the reverse sweep of the adjoint.
+template <bool kPacked, bool kTape = false>
 __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(const __grid_constant__ ClusterParams p) {
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -228,15 +257,25 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                 next = load_record(I.kind[kn], kn, stage_lo(gn) + tid, stage_hi(gn));
                 const uint32_t first = kind ? first1 : first0;
                 float* lam = kind ? lam1 : lam0;
-                if (cur.index != ~0u) apply_record(cur, kind, me, rank_base, x_base, lam, first, p.inv_dt2);
+                float4* tape = nullptr;
+                uint32_t rtotal = 0;
+                if constexpr (kTape) {
+                    rtotal = kind ? p.tape.r1 : p.tape.r0;
+                    tape = (kind ? p.tape.dih : p.tape.dist) + static_cast<size_t>(it) * (kind ? 4 : 2) * rtotal;
+                }
+                if (cur.index != ~0u)
+                    apply_record<kTape>(cur, kind, me, rank_base, x_base, lam, first, p.inv_dt2, tape, rtotal);
                 for (uint32_t i = stage_lo(g) + tid + blockDim.x; i < stage_hi(g); i += blockDim.x)
-                    apply_record(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, rank_base, x_base, lam,
-                                 first, p.inv_dt2);
+                    apply_record<kTape>(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, rank_base, x_base,
+                                        lam, first, p.inv_dt2, tape, rtotal);
             }
             cluster.sync();
         }
         if (susp_c) {
-            if (owner && tid == 0) line_iteration(*I.payload_def, pay, x, p.dt, I.status);
+            if (owner && tid == 0) {
+                if constexpr (kTape) tape_pilot(p.tape.line[it], pay, *p.tape.pilot, x, nullptr);
+                line_iteration(*I.payload_def, pay, x, p.dt, I.status);
+            }
             cluster.sync();
         }
     }
@@ -251,6 +290,10 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                 float4* pa = node_at(r & 0xffffu, me, rank_base, x, peers);
                 float4* pb = node_at(r >> 16, me, rank_base, x, peers);
                 float4 A = *pa, B = *pb;
+                if constexpr (kTape) {
+                    p.tape.seam[i] = A;
+                    p.tape.seam[p.tape.rs + i] = B;
+                }
                 float l = 0.0f;  // rigid stitch: alpha = 0
                 project_distance(A, B, 0.0f, 0.0f, l, p.inv_dt2);
                 *pa = A;
@@ -271,6 +314,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     }
     __syncthreads();
     if (owner && tid == 0) {
+        if constexpr (kTape) tape_pilot(*p.tape.finish, pay, *p.tape.pilot, x, v);
         payload_finish(*I.payload_def, pay, *I.payload_in, x, v, p.dt, I.status);
         float3 s = make_float3(0.0f, 0.0f, 0.0f);
         if (I.recentre && finite3(pay.com) &&
@@ -313,6 +357,8 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
 // cluster (the batched step).
 inline constexpr auto xpbd_cluster_kernel = &xpbd_cluster_kernel_t<false>;
 inline constexpr auto xpbd_cluster_packed_kernel = &xpbd_cluster_kernel_t<true>;
+// One structure per cluster, recording the adjoint's tape.
+inline constexpr auto xpbd_cluster_tape_kernel = &xpbd_cluster_kernel_t<false, true>;
 
 }  // namespace dev
 }  // namespace swb

@@ -49,6 +49,47 @@ struct ClusterInstance {
     int pad;
 };
 
+// Rigid pilot as the adjoint sees it: the suspension endpoint nodes are
+// numbered as attachment slots (distinct nodes, at most 16), each holding a
+// local index into the owner CTA's patch.
+struct AdjointPilot {
+    int slots;
+    int slot_node[16];     // local node index in the owner patch
+    float slot_w[16];      // inverse mass of the slot's node
+    int segments;
+    int from_slot[8], to_slot[8], from_point[8], to_point[8];
+    float rest[8], stiffness[8], damping[8];
+    float3 hang_local[8];
+    float3 com_local;
+    float3 inertia;
+    float mass;
+    float min_length;
+};
+
+// Inputs of one line iteration, or of the payload finish, as recorded by the
+// taping forward step.
+struct PilotTape {
+    float com[3];
+    float q[4];            // w, x, y, z
+    float lambda[8];
+    float4 xs[16];         // slot positions (xyz)
+    float4 vs[16];         // finish only: slot velocities before line damping
+};
+
+// Device pointers of one step's tape.  Per iteration, distance-type records
+// store two float4 blocks of R0 entries (node a xyz + lambda, node b xyz) and
+// dihedral records four blocks of R1 entries (a xyz + lambda, b, c, d); the
+// seam pass stores two blocks of its record count.
+struct TapeStep {
+    float4* dist;
+    float4* dih;
+    float4* seam;
+    PilotTape* line;       // [iterations]
+    PilotTape* finish;     // [1]
+    uint32_t r0, r1, rs;   // records per kind and seam records
+    const AdjointPilot* pilot;
+};
+
 // Packed launches (several structures per cluster): what one CTA runs.
 // The loop bounds are those of the whole cluster, so that every CTA of the
 // cluster takes the same cluster barriers.
@@ -73,6 +114,30 @@ struct ClusterParams {
     long long copy_budget;
     uint32_t smem_x, smem_v;       // byte offsets of node and force/velocity arrays
     uint32_t smem_offsets;         // byte offset of the CTA's stage offsets
+    TapeStep tape;                 // taping launches: where this step's tape goes
+};
+
+// Parameters of the reverse step kernel (one structure, one cluster).
+struct AdjointParams {
+    const ClusterInstance* inst;   // the step's instance record (in = step start, out = step end)
+    TapeStep tape;
+    const float4* xb_out;          // adjoint of the step's final positions (slot order)
+    const float4* vb_out;          // adjoint of the step's final velocities
+    float4* xb_in;                 // adjoint of the step-start positions
+    float4* vb_in;                 // adjoint of the step-start velocities
+    const float* pb_out;           // pilot adjoint: com 3, q 4 (w x y z), v 3, w 3
+    float* pb_in;
+    float4* fbar;                  // per-slot scratch: adjoint of the nodal force
+    double* g_rest0;               // per distance-type record
+    double* g_comp0;
+    double* g_comp1;               // per dihedral record
+    double* g_seg_rest;            // per device suspension segment
+    double* g_mass;
+    int ctas;
+    float dt, inv_dt, inv_dt2, damping;
+    float3 gravity;
+    int iterations;
+    uint32_t smem_xb, smem_vb, smem_lam0, smem_lam1, smem_acc0r, smem_acc0c, smem_acc1c, smem_offsets;
 };
 
 }  // namespace swb

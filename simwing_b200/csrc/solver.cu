@@ -2,6 +2,7 @@
 // Replaces simwing::fsi::Structure (src/fsi/structure.h:273-309).
 #include "common.h"
 #include "schedule.h"
+#include "adjoint_kernel.cuh"
 #include "cluster_kernel.cuh"
 #include "step_kernel.cuh"
 #include "structure_impl.h"
@@ -680,6 +681,34 @@ cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg
 
 cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params) {
     return cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_packed_kernel, params);
+}
+
+cudaError_t plain_cluster_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params) {
+    return cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_kernel, params);
+}
+
+cudaError_t tape_kernel_limits(int max_dynamic_smem, bool non_portable_cluster) {
+    cudaError_t rc = cudaFuncSetAttribute(dev::xpbd_cluster_tape_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem);
+    if (rc == cudaSuccess && non_portable_cluster)
+        rc = cudaFuncSetAttribute(dev::xpbd_cluster_tape_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return rc;
+}
+
+cudaError_t tape_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params) {
+    return cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_tape_kernel, params);
+}
+
+cudaError_t adjoint_kernel_limits(int max_dynamic_smem, bool non_portable_cluster) {
+    cudaError_t rc = cudaFuncSetAttribute(dev::xpbd_cluster_adjoint_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem);
+    if (rc == cudaSuccess && non_portable_cluster)
+        rc = cudaFuncSetAttribute(dev::xpbd_cluster_adjoint_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return rc;
+}
+
+cudaError_t adjoint_kernel_launch(const cudaLaunchConfig_t& cfg, const AdjointParams& params) {
+    return cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_adjoint_kernel, params);
 }
 
 swb_status decode_status(const int status[2], std::string& message) {

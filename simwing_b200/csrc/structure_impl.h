@@ -31,6 +31,12 @@ constexpr int kDiagBlocks = 148;
 cudaError_t packed_kernel_limits(int max_dynamic_smem, bool non_portable_cluster);
 cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg);
 cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params);
+// ... and of the single-structure kernels the differentiable rollout drives.
+cudaError_t plain_cluster_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params);
+cudaError_t tape_kernel_limits(int max_dynamic_smem, bool non_portable_cluster);
+cudaError_t tape_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params);
+cudaError_t adjoint_kernel_limits(int max_dynamic_smem, bool non_portable_cluster);
+cudaError_t adjoint_kernel_launch(const cudaLaunchConfig_t& cfg, const AdjointParams& params);
 
 // Status words written by the step kernels -> status and message.
 swb_status decode_status(const int status[2], std::string& message);
