@@ -320,7 +320,12 @@ enum {
                                       patches: every colour is a device-wide
                                       phase (comparison/debug)               */
     SWB_OPT_NO_GRAPH = 1u << 1,    /* batched: launch without CUDA graphs    */
-    SWB_OPT_GRID = 1u << 2         /* force the grid schedule                */
+    SWB_OPT_GRID = 1u << 2,        /* force the grid schedule                */
+    SWB_OPT_SPLIT_STAGES = 1u << 3 /* cluster schedule with split stages:
+                                      interior constraints coloured per CTA
+                                      behind CTA barriers, cluster barriers
+                                      only where constraints span CTAs (fewer
+                                      cluster barriers, more stages)         */
 };
 
 void swb_default_solver_options(swb_solver_options* out);

@@ -191,7 +191,7 @@ OK, INVALID_ARGUMENT, OUT_OF_RANGE, SUSPENSION_ERROR, CONTACT_ERROR, NON_FINITE,
     CUDA_ERROR, UNSUPPORTED, OUT_OF_MEMORY = range(10)
 
 DISTANCE, CABLE, SUSPENSION_TIE, SEAM_STITCH = 1, 2, 3, 4
-OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID = 1, 2, 4
+OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID, OPT_SPLIT_STAGES = 1, 2, 4, 8
 BATCH_AUTOTUNE = 1 << 8
 SWEEP_DISTANCE, SWEEP_DIHEDRAL = 0, 1
 

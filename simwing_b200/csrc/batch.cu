@@ -70,7 +70,7 @@ std::unique_ptr<swb_structure> build_member(const swb_structure_definition& def,
         swb_solver_options opt;
         swb_default_solver_options(&opt);
         opt.device = device;
-        opt.cluster_ctas = r;
+        opt.cluster_ctas = r;  // classic stages: a packed cluster takes the same barriers on every rank
         auto m = std::make_unique<swb_structure>();
         try {
             m->s.build(def, &opt);

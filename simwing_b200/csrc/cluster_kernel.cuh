@@ -40,10 +40,11 @@ __device__ __forceinline__ ClusterRecord load_record(const ClusterKindDev& K, in
     ClusterRecord r;
     r.index = ~0u;
     if (i < hi) {
-        r.ab = __ldg(K.ab + i);
-        r.cd = kind ? __ldg(K.cd + i) : 0u;
-        r.rest = __ldg(K.rest + i);
-        r.comp = __ldg(K.comp + i);
+        const uint4 q = __ldg(K.rec + i);
+        r.ab = q.x;
+        r.cd = q.y;
+        r.rest = __uint_as_float(q.z);
+        r.comp = __uint_as_float(q.w);
         r.index = i;
     }
     return r;
@@ -246,6 +247,8 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     next.index = ~0u;
     if (p.iterations > 0 && S > 0) next = load_record(I.kind[S0 > 0 ? 0 : 1], S0 > 0 ? 0 : 1, stage_lo(0) + tid,
                                                       stage_hi(0));
+    const uint64_t sync0 = I.kind[0].sync_mask, sync1 = I.kind[1].sync_mask;
+    const int interior0 = I.kind[0].interior_stages, interior1 = I.kind[1].interior_stages;
     for (int it = 0; it < p.iterations; ++it) {
         for (int g = 0; g < stages_c; ++g) {
             if (!kPacked || g < S) {
@@ -269,7 +272,22 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                     apply_record<kTape>(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, rank_base, x_base,
                                         lam, first, p.inv_dt2, tape, rtotal);
             }
-            cluster.sync();
+            if constexpr (kPacked) {
+                cluster.sync();
+            } else {
+                // split stages: a cluster barrier where the next stage may read
+                // what another CTA wrote, else a CTA barrier (after the
+                // single-CTA tail's writes to peer nodes are made visible)
+                const int kind = g < S0 ? 0 : 1;
+                const int gl = kind ? g - S0 : g;
+                const uint64_t mask = kind ? sync1 : sync0;
+                if (gl >= 64 || ((mask >> gl) & 1ull)) {
+                    cluster.sync();
+                } else {
+                    if (gl >= (kind ? interior1 : interior0)) asm volatile("fence.acq_rel.cluster;" ::: "memory");
+                    __syncthreads();
+                }
+            }
         }
         if (susp_c) {
             if (owner && tid == 0) {

@@ -14,12 +14,12 @@ constexpr int kClusterMaxThreads = 768;  // threads per CTA of the cluster step 
 
 struct ClusterKindDev {
     const uint32_t* offsets;   // [ctas * (stages + 1)]
-    const uint32_t* ab;
-    const uint32_t* cd;
-    const float* rest;
-    const float* comp;
+    const uint4* rec;          // per record: ab, cd (dihedral), rest bits, compliance bits (sign = cable)
     int stages;
     uint32_t smem_lambda;      // byte offset of this kind's multipliers
+    uint64_t sync_mask;        // bit g: a cluster barrier follows stage g (stages >= 64: always)
+    int interior_stages;       // stages before this one touch only the CTA's own nodes
+    int pad[3];
 };
 
 // Per-instance tables and state (one cluster each).

@@ -19,7 +19,7 @@ uint32_t make_ref(const ClusterSchedule& s, uint32_t node) {
 }  // namespace
 
 bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes, int ctas,
-                            ClusterSchedule& S) {
+                            ClusterSchedule& S, bool split) {
     S = ClusterSchedule{};
     const uint32_t N = static_cast<uint32_t>(d.nodes.size());
     ctas = std::clamp(ctas, 1, kClusterMaxCtas);
@@ -61,11 +61,9 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
             else
                 for (int q = 0; q < 4; ++q) nodes[i][q] = static_cast<uint32_t>(d.dihedrals[i].nodes[q]);
         }
-        std::vector<int> colour;
-        const int stages = dsatur_colour(nodes, counts, colour);
-        K.stages = stages;
         // executing CTA: owner of most of the constraint's nodes (ties: first)
         std::vector<int> cta_of(m, 0);
+        std::vector<uint8_t> interior(m, 0);
         for (size_t i = 0; i < m; ++i) {
             int best = part[nodes[i][0]], best_count = 0;
             for (int q = 0; q < counts[i]; ++q) {
@@ -77,7 +75,67 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
                 }
             }
             cta_of[i] = best;
+            interior[i] = best_count == counts[i];
         }
+        std::vector<int> colour(m, 0);  // becomes the stage
+        if (!split || ctas == 1) {
+            K.stages = dsatur_colour(nodes, counts, colour);
+            K.cluster_sync.assign(K.stages, 1);
+            K.interior_stages = 0;
+            K.boundary_stages = K.stages;
+        } else {
+            // interior constraints: coloured per CTA
+            int I = 0;
+            for (int c = 0; c < ctas; ++c) {
+                std::vector<size_t> ids;
+                std::vector<std::array<uint32_t, 4>> sub;
+                std::vector<int> subc;
+                for (size_t i = 0; i < m; ++i)
+                    if (interior[i] && cta_of[i] == c) {
+                        ids.push_back(i);
+                        sub.push_back(nodes[i]);
+                        subc.push_back(counts[i]);
+                    }
+                std::vector<int> col;
+                I = std::max(I, dsatur_colour(sub, subc, col));
+                for (size_t j = 0; j < ids.size(); ++j) colour[ids[j]] = col[j];
+            }
+            // constraints spanning CTAs: one colouring; the suffix of small
+            // colours becomes the single-CTA tail
+            std::vector<size_t> ids;
+            std::vector<std::array<uint32_t, 4>> sub;
+            std::vector<int> subc;
+            for (size_t i = 0; i < m; ++i)
+                if (!interior[i]) {
+                    ids.push_back(i);
+                    sub.push_back(nodes[i]);
+                    subc.push_back(counts[i]);
+                }
+            std::vector<int> col;
+            const int B = dsatur_colour(sub, subc, col);
+            std::vector<size_t> size(B, 0);
+            for (int c : col) ++size[c];
+            int tail = B;
+            while (tail > 0 && size[tail - 1] <= kClusterTailColourMax) --tail;
+            // the tail runs on the CTA owning most of its nodes
+            std::vector<size_t> owned(ctas, 0);
+            for (size_t j = 0; j < ids.size(); ++j)
+                if (col[j] >= tail)
+                    for (int q = 0; q < subc[j]; ++q) ++owned[part[sub[j][q]]];
+            K.tail_cta = tail < B ? static_cast<int>(std::max_element(owned.begin(), owned.end()) - owned.begin()) : -1;
+            for (size_t j = 0; j < ids.size(); ++j) {
+                colour[ids[j]] = I + col[j];
+                if (col[j] >= tail) cta_of[ids[j]] = K.tail_cta;
+            }
+            K.stages = I + B;
+            K.interior_stages = I;
+            K.boundary_stages = tail;
+            K.tail_stages = B - tail;
+            K.cluster_sync.assign(K.stages, 1);
+            for (int g = 0; g + 1 < I; ++g) K.cluster_sync[g] = 0;
+            for (int g = I + tail; g + 1 < I + B; ++g) K.cluster_sync[g] = 0;
+        }
+        const int stages = K.stages;
         // records CTA-major, stage within, definition order within
         std::vector<uint32_t> idx(m);
         std::iota(idx.begin(), idx.end(), 0u);
@@ -182,10 +240,16 @@ void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_
     }
     std::vector<int64_t> stamp(N, -1);
     int64_t epoch = 0;
+    // runs of stages joined by CTA barriers: a node may be touched by one CTA only
+    std::vector<int64_t> run_of(N, -1);
+    std::vector<int> run_cta(N, -1);
+    int64_t run = 0;
     for (int k = 0; k < 2; ++k) {
         const ClusterKind& K = S.kinds[k];
         const size_t m = k == 0 ? d.constraints.size() : d.dihedrals.size();
         std::vector<uint8_t> seen(m, 0);
+        if (K.cluster_sync.size() != static_cast<size_t>(K.stages)) fail("barrier kinds per stage");
+        if (K.stages > 0 && !K.cluster_sync.back()) fail("a kind must end with a cluster barrier");
         for (int s = 0; s < K.stages; ++s) {
             ++epoch;
             for (int c = 0; c < C; ++c)
@@ -210,8 +274,13 @@ void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_
                         if (n != want[q]) fail("reference does not name the constraint's node");
                         if (stamp[n] == epoch) fail("stage is not node-disjoint");
                         stamp[n] = epoch;
+                        if (run_of[n] == run && run_cta[n] != c)
+                            fail("a node is touched by two CTAs between cluster barriers");
+                        run_of[n] = run;
+                        run_cta[n] = c;
                     }
                 }
+            if (K.cluster_sync[s]) ++run;
         }
         for (size_t i = 0; i < m; ++i)
             if (!seen[i]) fail("constraint not scheduled");

@@ -9,10 +9,25 @@
 // cluster barrier separates stages.  Node references are 16-bit: the owner
 // rank in the top 4 bits and the index in its patch in the low 12 bits.
 //
+// Split stages (optional, SWB_OPT_SPLIT_STAGES): a constraint whose
+// nodes all lie in one CTA's patch is interior.  Per kind, the interior
+// constraints run first, coloured per CTA, with only a CTA barrier between
+// their stages (interior constraints of different CTAs share no node); one
+// cluster barrier follows.  The constraints that span CTAs are coloured
+// together; their large colours run one stage each with a cluster barrier
+// after it, and the short tail of small colours runs on a single CTA with CTA
+// barriers, closed by one cluster barrier.  Each stage carries the kind of
+// barrier that follows it.  Classic stages (the default: one colouring of
+// the whole mesh, a cluster barrier after every stage) are also what packed
+// batches need, whose structures must take identical barriers.  On the
+// B200 the classic form is faster: a stage's cost is mostly its records'
+// issue and latency, not its barrier, and split stages double the stages.
+//
 // Sweep order per kind: stage-major, then CTA rank, then record order --
 // the reference serial solver run on the definition permuted into this
-// order performs exactly the device sweep (constraints of one stage share
-// no node).
+// order performs exactly the device sweep: constraints of one stage share
+// no node, and within a run of stages joined by CTA barriers every node is
+// touched by one CTA only.
 #pragma once
 
 #include "common.h"
@@ -37,6 +52,9 @@ struct ClusterKind {
     std::vector<float> comp;     // distance: sign bit = cable
     std::vector<uint32_t> def_index;
     uint32_t max_cta_records = 0;  // multipliers held in shared memory per CTA
+    std::vector<uint8_t> cluster_sync;  // [stages]: 1 = cluster barrier after the stage, 0 = CTA barrier
+    int interior_stages = 0, boundary_stages = 0, tail_stages = 0;
+    int tail_cta = -1;
 };
 
 struct ClusterSchedule {
@@ -54,10 +72,23 @@ struct ClusterSchedule {
     std::vector<uint64_t> distance_order, dihedral_order;
 };
 
+// Cluster barriers per constraint iteration (stages followed by one, plus
+// the suspension stage).
+inline int cluster_barriers_per_iteration(const ClusterSchedule& s) {
+    int n = s.susp_cta >= 0 ? 1 : 0;
+    for (const ClusterKind& k : s.kinds)
+        for (uint8_t b : k.cluster_sync) n += b;
+    return n;
+}
+
 // Returns false (and leaves `out` empty) when the mesh does not fit one
 // cluster of `ctas` CTAs (a patch over kClusterPatchNodes nodes).
 bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes, int ctas,
-                            ClusterSchedule& out);
+                            ClusterSchedule& out, bool split = false);
+
+// Boundary colours with at most this many records may form the single-CTA
+// tail of a kind's split stages.
+constexpr size_t kClusterTailColourMax = 256;
 
 // Checks the invariants the cluster kernel relies on; raises on failure.
 void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes,

@@ -729,7 +729,8 @@ extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definiti
             const int last = options && options->cluster_ctas > 0 ? c : kClusterMaxCtas;
             for (; c <= last; c *= 2) {
                 ClusterSchedule C;
-                if (!build_cluster_schedule(def, susp, c, C)) continue;
+                if (!build_cluster_schedule(def, susp, c, C, options && (options->flags & SWB_OPT_SPLIT_STAGES)))
+                    continue;
                 const size_t bytes = C.max_patch * 32ull + C.kinds[0].max_cta_records * 4ull +
                                      C.kinds[1].max_cta_records * 4ull +
                                      (C.kinds[0].stages + C.kinds[1].stages + 2) * 4ull + 64;
@@ -739,7 +740,7 @@ extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definiti
                 out->blocks = C.ctas;
                 out->cluster_ctas = C.ctas;
                 out->local_stages_per_iteration = C.kinds[0].stages + C.kinds[1].stages;
-                out->cluster_barriers_per_iteration = C.kinds[0].stages + C.kinds[1].stages + (C.susp_cta >= 0);
+                out->cluster_barriers_per_iteration = cluster_barriers_per_iteration(C);
                 out->max_patch_nodes = static_cast<int32_t>(C.max_patch);
                 out->shared_bytes = static_cast<int32_t>(bytes);
                 out->level_constraints[0] = def.constraints.size() + def.dihedrals.size();

@@ -158,7 +158,7 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
             for (; c <= kClusterMaxCtas; c *= 2) candidates.push_back(c);
         }
         for (int c : candidates) {
-            if (!build_cluster_schedule(def, susp_nodes, c, csched)) continue;
+            if (!build_cluster_schedule(def, susp_nodes, c, csched, (opt.flags & SWB_OPT_SPLIT_STAGES) != 0)) continue;
             const size_t bytes = csched.max_patch * 32ull + csched.kinds[0].max_cta_records * 4ull +
                                  csched.kinds[1].max_cta_records * 4ull +
                                  (csched.kinds[0].stages + csched.kinds[1].stages + 2) * 4ull + 64;
@@ -262,12 +262,18 @@ void StructureImpl::upload_cluster_tables() {
         const ClusterKind& K = csched.kinds[k];
         ClusterKindDev& dk = base.kind[k];
         dk.offsets = dupload(owned, K.offsets, stream);
-        dk.ab = dupload(owned, K.ab, stream);
-        dk.cd = k == 1 ? dupload(owned, K.cd, stream) : dk.ab;
-        dk.rest = dupload(owned, K.rest, stream);
-        dk.comp = dupload(owned, K.comp, stream);
+        std::vector<uint4> rec(K.ab.size());
+        for (size_t r = 0; r < rec.size(); ++r)
+            rec[r] = make_uint4(K.ab[r], k == 1 ? K.cd[r] : 0u, std::bit_cast<uint32_t>(K.rest[r]),
+                                std::bit_cast<uint32_t>(K.comp[r]));
+        dk.rec = dupload(owned, rec, stream);
         dk.stages = K.stages;
         dk.smem_lambda = off;
+        // stages from 64 on always take a cluster barrier (a superset of any CTA barrier)
+        dk.sync_mask = 0;
+        for (int g = 0; g < std::min(K.stages, 64); ++g)
+            if (K.cluster_sync[g]) dk.sync_mask |= 1ull << g;
+        dk.interior_stages = K.interior_stages;
         off = align16(off + K.max_cta_records * 4u);
     }
     cp.smem_offsets = off;
@@ -1165,8 +1171,7 @@ swb_status swb_structure_schedule_report(const swb_structure* s, swb_schedule_re
             const ClusterSchedule& C = m.csched;
             out->cluster_ctas = C.ctas;
             out->local_stages_per_iteration = C.kinds[0].stages + C.kinds[1].stages;
-            out->cluster_barriers_per_iteration =
-                C.kinds[0].stages + C.kinds[1].stages + (C.susp_cta >= 0 ? 1 : 0);
+            out->cluster_barriers_per_iteration = cluster_barriers_per_iteration(C);
             out->max_patch_nodes = static_cast<int32_t>(C.max_patch);
             out->shared_bytes = static_cast<int32_t>(m.cluster_smem);
             out->level_constraints[0] = m.def.constraints.size() + m.def.dihedrals.size();

@@ -18,6 +18,7 @@
 // reference's serial sweep with its constraint lists permuted into it.
 #pragma once
 
+#include "fast_math.h"
 #include "step_params.h"
 
 namespace swb {
@@ -38,8 +39,9 @@ __device__ __forceinline__ float wrap_two_pi(float x) {
 
 // projectDistanceConstraint (soft_body.cpp:1598-1640) on float4 nodes
 // (xyz, w = inverse mass).  comp carries the cable flag in its sign bit.
-// The length and the two divisions use the reciprocal square root and a
-// reciprocal (about one ulp each) instead of IEEE sqrt and division.
+// The length and the two divisions use the reciprocal square root and the
+// approximate reciprocal (an ulp or two each) instead of IEEE sqrt and
+// division.
 __device__ __forceinline__ void project_distance(float4& pa, float4& pb, float rest, float comp_raw,
                                                  float& lambda, float inv_dt2) {
     const float dx = pb.x - pa.x, dy = pb.y - pa.y, dz = pb.z - pa.z;
@@ -54,7 +56,7 @@ __device__ __forceinline__ void project_distance(float4& pa, float4& pb, float r
     const float wsum = pa.w + pb.w;
     const float alpha = fabsf(comp_raw) * inv_dt2;
     if (wsum + alpha <= 0.0f) return;
-    const float dl = (-value - alpha * lambda) * __frcp_rn(wsum + alpha);
+    const float dl = (-value - alpha * lambda) * fast_rcp(wsum + alpha);
     float applied = dl;
     if (cable) {
         const float sum = lambda + dl;
@@ -73,6 +75,8 @@ __device__ __forceinline__ void project_distance(float4& pa, float4& pb, float r
 // evaluateDihedral + solveDihedralConstraint (soft_body.cpp:1648-1711,
 // 1754-1792): one XPBD projection of the signed hinge angle.
 //
+// The angle uses fast_atan2 (fast_math.h, within 4e-7 rad of atan2) and the
+// divisions the approximate reciprocal.
 // The reference evaluates theta = atan2(e.(n1 x n2), n1.n2) from unit
 // vectors and its gradient by reverse mode through the normalisations.  The
 // same function and gradient are evaluated here in closed form (an identity,
@@ -99,14 +103,14 @@ __device__ __forceinline__ void project_dihedral(float4& A, float4& B, float4& C
     const float el = e2 * iel;
     const float sine = dot(edge, cross(A1, A2)) * iel;
     const float cosine = dot(A1, A2);
-    const float s1 = -el * __frcp_rn(q1), s2 = -el * __frcp_rn(q2);
+    const float s1 = -el * fast_rcp(q1), s2 = -el * fast_rcp(q2);
     const float3 gc = A1 * s1;
     const float3 gd = A2 * s2;
     const float ie2 = iel * iel;
     const float t1 = dot(toC, edge) * ie2, t2 = dot(toD, edge) * ie2;
     const float3 gb = -(gc * t1 + gd * t2);
     const float3 ga = -((gb + gc) + gd);
-    const float angle = atan2f(sine, cosine);
+    const float angle = fast_atan2(sine, cosine);
     // The reference skips a hinge whose angle or gradient is not finite.  A
     // non-finite gradient component makes wg (and den) non-finite, and a
     // non-finite angle makes dl non-finite, so the two checks below reject
@@ -116,7 +120,7 @@ __device__ __forceinline__ void project_dihedral(float4& A, float4& B, float4& C
     const float den = wg + alpha;
     if (!(den > 0.0f) || !isfinite(den) || !isfinite(wg)) return;
     const float value = wrap_two_pi(angle - rest);
-    const float dl = (-value - alpha * lambda) * __frcp_rn(den);
+    const float dl = (-value - alpha * lambda) * fast_rcp(den);
     if (!isfinite(dl)) return;
     const float sa = A.w * dl, sb = B.w * dl, sc = C.w * dl, sd = D.w * dl;
     A.x += sa * ga.x; A.y += sa * ga.y; A.z += sa * ga.z;

@@ -91,7 +91,8 @@ def test_patch_global_only_parity(cuda_device):
     assert max(errs) <= REL_TOL, errs
 
 
-@pytest.mark.parametrize("options", [dict(), dict(cluster_ctas=4), dict(flags=4)])
+@pytest.mark.parametrize("options", [dict(), dict(cluster_ctas=4), dict(flags=sw.abi.OPT_GRID),
+                                     dict(cluster_ctas=4, flags=sw.abi.OPT_SPLIT_STAGES)])
 def test_wing_per_step_parity_small(cuda_device, options):
     d = sw.generate_wing(cells=8, chordwise=20, spanwise_per_cell=2, rib_layers=3)
     errs, dev, orc = per_step_errors(d, 4, step_settings(), sw.SolverOptions(**options))
@@ -101,7 +102,7 @@ def test_wing_per_step_parity_small(cuda_device, options):
     assert np.abs(s.center_of_mass - [p.center_of_mass.x, p.center_of_mass.y, p.center_of_mass.z]).max() < 1e-4
 
 
-@pytest.mark.parametrize("options", [dict(), dict(flags=4)])
+@pytest.mark.parametrize("options", [dict(), dict(flags=sw.abi.OPT_GRID), dict(flags=sw.abi.OPT_SPLIT_STAGES)])
 def test_full_wing_one_step_parity(cuda_device, options):
     errs, dev, _ = per_step_errors(sw.generate_wing(), 2, step_settings(), sw.SolverOptions(**options))
     assert max(errs) <= REL_TOL, errs

@@ -143,14 +143,28 @@ def test_schedule_invariants_patch(levels, blocks):
     assert r.blocks == min(blocks, d.node_count)
 
 
+@pytest.mark.parametrize("split", [False, True])
 @pytest.mark.parametrize("ctas", [1, 2, 4, 8, 16])
-def test_cluster_schedule_invariants(ctas):
+def test_cluster_schedule_invariants(ctas, split):
+    # plan_schedule runs the host verifier: node-disjoint stages, and within
+    # every run of stages joined by CTA barriers each node touched by one CTA
     d = sw.generate_wing(cells=8, chordwise=16, spanwise_per_cell=2, rib_layers=3)
-    r, do, ho = sw.plan_schedule(d, sw.SolverOptions(cluster_ctas=ctas))
+    flags = abi.OPT_SPLIT_STAGES if split else 0
+    r, do, ho = sw.plan_schedule(d, sw.SolverOptions(cluster_ctas=ctas, flags=flags))
     assert r.cluster_ctas == ctas
     assert sorted(do.tolist()) == list(range(d.view.constraint_count))
     assert sorted(ho.tolist()) == list(range(d.view.dihedral_count))
-    assert r.cluster_barriers_per_iteration == r.local_stages_per_iteration + 1  # + suspension stage
+    if not split or ctas == 1:
+        assert r.cluster_barriers_per_iteration == r.local_stages_per_iteration + 1  # + suspension stage
+    else:
+        assert r.cluster_barriers_per_iteration < r.local_stages_per_iteration + 1
+
+
+def test_split_stages_cut_cluster_barriers_on_the_full_wing():
+    d = sw.generate_wing()
+    classic, _, _ = sw.plan_schedule(d)
+    split, _, _ = sw.plan_schedule(d, sw.SolverOptions(flags=abi.OPT_SPLIT_STAGES))
+    assert split.cluster_barriers_per_iteration <= 16 < classic.cluster_barriers_per_iteration
 
 
 def test_full_wing_fits_one_cluster():
