@@ -16,6 +16,57 @@ uint32_t make_ref(const ClusterSchedule& s, uint32_t node) {
     return (cta << 12) | (slot - s.patch_begin[cta]);
 }
 
+// Evens out, CTA by CTA, how many records each colour gives the CTA, without
+// adding colours: a constraint whose colour holds more than the CTA's mean
+// moves to the colour with the fewest of the CTA's records that none of its
+// conflicting constraints (shared nodes) has, as long as that colour holds
+// at least two fewer.  Stages then carry similar record counts on every CTA,
+// so the largest colours no longer need two rounds of the CTA's threads
+// while the small ones leave them idle.
+void balance_colours(const std::vector<std::array<uint32_t, 4>>& nodes, const std::vector<int>& counts,
+                     const std::vector<int>& cta_of, int ctas, uint32_t node_count, int colours,
+                     std::vector<int>& colour) {
+    const size_t m = nodes.size();
+    if (colours < 2 || colours > 64 || m == 0) return;
+    std::vector<uint32_t> off(node_count + 1, 0);
+    for (size_t i = 0; i < m; ++i)
+        for (int q = 0; q < counts[i]; ++q) ++off[nodes[i][q] + 1];
+    for (uint32_t v = 0; v < node_count; ++v) off[v + 1] += off[v];
+    std::vector<uint32_t> inc(off.back());
+    {
+        std::vector<uint32_t> cur(off.begin(), off.end() - 1);
+        for (size_t i = 0; i < m; ++i)
+            for (int q = 0; q < counts[i]; ++q) inc[cur[nodes[i][q]]++] = static_cast<uint32_t>(i);
+    }
+    std::vector<int64_t> size(static_cast<size_t>(ctas) * colours, 0), total(ctas, 0);
+    for (size_t i = 0; i < m; ++i) {
+        ++size[static_cast<size_t>(cta_of[i]) * colours + colour[i]];
+        ++total[cta_of[i]];
+    }
+    for (int pass = 0; pass < 8; ++pass) {
+        bool moved = false;
+        for (size_t i = 0; i < m; ++i) {
+            const int c = colour[i];
+            int64_t* sz = size.data() + static_cast<size_t>(cta_of[i]) * colours;
+            const int64_t mean = (total[cta_of[i]] + colours - 1) / colours;
+            if (sz[c] <= mean) continue;
+            uint64_t used = 0;
+            for (int q = 0; q < counts[i]; ++q)
+                for (uint32_t k = off[nodes[i][q]]; k < off[nodes[i][q] + 1]; ++k)
+                    if (inc[k] != i) used |= 1ull << colour[inc[k]];
+            int best = -1;
+            for (int t = 0; t < colours; ++t)
+                if (!((used >> t) & 1ull) && sz[t] + 1 < sz[c] && (best < 0 || sz[t] < sz[best])) best = t;
+            if (best < 0) continue;
+            --sz[c];
+            ++sz[best];
+            colour[i] = best;
+            moved = true;
+        }
+        if (!moved) break;
+    }
+}
+
 }  // namespace
 
 bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes, int ctas,
@@ -80,6 +131,7 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
         std::vector<int> colour(m, 0);  // becomes the stage
         if (!split || ctas == 1) {
             K.stages = dsatur_colour(nodes, counts, colour);
+            balance_colours(nodes, counts, cta_of, ctas, N, K.stages, colour);
             K.cluster_sync.assign(K.stages, 1);
             K.interior_stages = 0;
             K.boundary_stages = K.stages;
