@@ -36,11 +36,11 @@ struct ClusterRecord {
     uint32_t index;  // record index (global), or ~0u when the slot is empty
 };
 
-__device__ __forceinline__ ClusterRecord load_record(const ClusterKindDev& K, int kind, uint32_t i, uint32_t hi) {
+__device__ __forceinline__ ClusterRecord load_record(const uint4* rec, uint32_t i, uint32_t hi) {
     ClusterRecord r;
     r.index = ~0u;
     if (i < hi) {
-        const uint4 q = __ldg(K.rec + i);
+        const uint4 q = __ldg(rec + i);
         r.ab = q.x;
         r.cd = q.y;
         r.rest = __uint_as_float(q.z);
@@ -48,6 +48,9 @@ __device__ __forceinline__ ClusterRecord load_record(const ClusterKindDev& K, in
         r.index = i;
     }
     return r;
+}
+__device__ __forceinline__ ClusterRecord load_record(const ClusterKindDev& K, int, uint32_t i, uint32_t hi) {
+    return load_record(K.rec, i, hi);
 }
 
 // Cluster-window address of node `ref`: the node arrays sit at the same
@@ -75,6 +78,12 @@ __device__ __forceinline__ void st_node(uint32_t addr, float4 v) {
                  "f"(v.w)
                  : "memory");
 }
+
+// The two halves of a cluster barrier, for a warp that works between its
+// arrival and its wait (arrive releases, wait acquires; every lane of the
+// warp executes both).
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
 
 // Projects one record.  Taping launches first store the record's inputs
 // (node positions and multiplier) at its index in this iteration's tape
@@ -243,12 +252,25 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     auto stage_lo = [&](int g) { return g < S0 ? soff[g] : soff[S0 + 1 + (g - S0)]; };
     auto stage_hi = [&](int g) { return g < S0 ? soff[g + 1] : soff[S0 + 2 + (g - S0)]; };
     const uint32_t first0 = soff[0], first1 = soff[S0 + 1];
+    // record arrays held in registers (the instance record lives in global memory)
+    const uint4* rec0 = I.kind[0].rec;
+    const uint4* rec1 = I.kind[1].rec;
+    auto apply = [&](const ClusterRecord& r, int kind, float* lam, uint32_t first, float4* tape, uint32_t rtotal) {
+        apply_record<kTape>(r, kind, me, rank_base, x_base, lam, first, p.inv_dt2, tape, rtotal);
+    };
     ClusterRecord next;
     next.index = ~0u;
-    if (p.iterations > 0 && S > 0) next = load_record(I.kind[S0 > 0 ? 0 : 1], S0 > 0 ? 0 : 1, stage_lo(0) + tid,
-                                                      stage_hi(0));
+    if (p.iterations > 0 && S > 0) next = load_record(S0 > 0 ? rec0 : rec1, stage_lo(0) + tid, stage_hi(0));
     const uint64_t sync0 = I.kind[0].sync_mask, sync1 = I.kind[1].sync_mask;
     const int interior0 = I.kind[0].interior_stages, interior1 = I.kind[1].interior_stages;
+    // line iteration beside the last two stages: neither touches a
+    // suspension endpoint node, so running it there gives the same result as
+    // running it after them.  The last warp of the suspension CTA (no record
+    // in either stage) arrives at the first stage's barrier, runs the line
+    // iteration, then waits; its writes are released at its arrival on the
+    // second stage's barrier, before the next iteration reads them.
+    const int line_stage = !kPacked && susp_c ? I.line_stage : -1;
+    const bool line_warp = line_stage >= 0 && owner && (tid >> 5) == static_cast<int>(blockDim.x >> 5) - 1;
     for (int it = 0; it < p.iterations; ++it) {
         for (int g = 0; g < stages_c; ++g) {
             if (!kPacked || g < S) {
@@ -257,7 +279,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                 // prefetch the next stage (wrapping to the next iteration)
                 const int gn = g + 1 < S ? g + 1 : 0;
                 const int kn = gn < S0 ? 0 : 1;
-                next = load_record(I.kind[kn], kn, stage_lo(gn) + tid, stage_hi(gn));
+                next = load_record(kn ? rec1 : rec0, stage_lo(gn) + tid, stage_hi(gn));
                 const uint32_t first = kind ? first1 : first0;
                 float* lam = kind ? lam1 : lam0;
                 float4* tape = nullptr;
@@ -266,13 +288,23 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                     rtotal = kind ? p.tape.r1 : p.tape.r0;
                     tape = (kind ? p.tape.dih : p.tape.dist) + static_cast<size_t>(it) * (kind ? 4 : 2) * rtotal;
                 }
-                if (cur.index != ~0u)
-                    apply_record<kTape>(cur, kind, me, rank_base, x_base, lam, first, p.inv_dt2, tape, rtotal);
+                if (cur.index != ~0u) apply(cur, kind, lam, first, tape, rtotal);
                 for (uint32_t i = stage_lo(g) + tid + blockDim.x; i < stage_hi(g); i += blockDim.x)
-                    apply_record<kTape>(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, rank_base, x_base,
-                                        lam, first, p.inv_dt2, tape, rtotal);
+                    apply(load_record(kind ? rec1 : rec0, i, stage_hi(g)), kind, lam, first, tape, rtotal);
             }
-            if constexpr (kPacked) {
+            if (g == line_stage) {
+                if (line_warp) {
+                    cluster_arrive();
+                    if ((tid & 31) == 0) {
+                        if constexpr (kTape) tape_pilot(p.tape.line[it], pay, *p.tape.pilot, x, nullptr);
+                        line_iteration(*I.payload_def, pay, x, p.dt, I.status);
+                    }
+                    __syncwarp();
+                    cluster_wait();
+                } else {
+                    cluster.sync();
+                }
+            } else if constexpr (kPacked) {
                 cluster.sync();
             } else {
                 // split stages: a cluster barrier where the next stage may read
@@ -289,7 +321,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                 }
             }
         }
-        if (susp_c) {
+        if (susp_c && line_stage < 0) {
             if (owner && tid == 0) {
                 if constexpr (kTape) tape_pilot(p.tape.line[it], pay, *p.tape.pilot, x, nullptr);
                 line_iteration(*I.payload_def, pay, x, p.dt, I.status);

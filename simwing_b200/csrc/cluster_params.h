@@ -46,7 +46,11 @@ struct ClusterInstance {
     double* origin_out;
     int* status;
     int recentre;
-    int pad;
+    // First of the two stages beside which the line iteration runs (on the
+    // last warp of the suspension CTA, which has no record in either), or -1:
+    // the line iteration then follows the iteration's stages behind a
+    // cluster barrier.  Single-structure launches only.
+    int line_stage;
 };
 
 // Rigid pilot as the adjoint sees it: the suspension endpoint nodes are

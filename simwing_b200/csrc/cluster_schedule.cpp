@@ -16,6 +16,115 @@ uint32_t make_ref(const ClusterSchedule& s, uint32_t node) {
     return (cta << 12) | (slot - s.patch_begin[cta]);
 }
 
+// Tries to colour with one colour fewer, repeatedly: the constraints of the
+// last colour are spread over the others and the conflicts that causes are
+// repaired by min-conflicts local search with a tabu list (each move puts a
+// conflicting constraint into the colour with the fewest conflicts for it,
+// not undoing a recent move unless that reaches a new best).  Stops at the
+// first count it cannot reach within `budget` moves and keeps the last
+// proper colouring.  Deterministic (fixed seed).  Returns the colour count.
+int reduce_colours(const std::vector<std::array<uint32_t, 4>>& nodes, const std::vector<int>& counts,
+                   uint32_t node_count, int colours, std::vector<int>& colour, long budget) {
+    const size_t m = nodes.size();
+    if (m == 0 || colours <= 1) return colours;
+    // conflict graph (constraints sharing a node)
+    std::vector<uint32_t> off(node_count + 1, 0);
+    for (size_t i = 0; i < m; ++i)
+        for (int q = 0; q < counts[i]; ++q) ++off[nodes[i][q] + 1];
+    for (uint32_t v = 0; v < node_count; ++v) off[v + 1] += off[v];
+    std::vector<uint32_t> inc(off.back());
+    {
+        std::vector<uint32_t> cur(off.begin(), off.end() - 1);
+        for (size_t i = 0; i < m; ++i)
+            for (int q = 0; q < counts[i]; ++q) inc[cur[nodes[i][q]]++] = static_cast<uint32_t>(i);
+    }
+    std::vector<uint32_t> nb_off(m + 1, 0), nb;
+    {
+        std::vector<uint32_t> tmp;
+        for (size_t i = 0; i < m; ++i) {
+            tmp.clear();
+            for (int q = 0; q < counts[i]; ++q)
+                for (uint32_t k = off[nodes[i][q]]; k < off[nodes[i][q] + 1]; ++k)
+                    if (inc[k] != i) tmp.push_back(inc[k]);
+            std::sort(tmp.begin(), tmp.end());
+            tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+            nb.insert(nb.end(), tmp.begin(), tmp.end());
+            nb_off[i + 1] = static_cast<uint32_t>(nb.size());
+        }
+    }
+    uint64_t state = 0x9e3779b97f4a7c15ull;
+    auto rnd = [&]() {
+        state ^= state << 13;
+        state ^= state >> 7;
+        state ^= state << 17;
+        return state;
+    };
+    // the constraints at one node form a clique: no colouring has fewer
+    // colours than the largest incidence count
+    uint32_t clique = 0;
+    for (uint32_t v = 0; v < node_count; ++v) clique = std::max(clique, off[v + 1] - off[v]);
+    for (int k = colours - 1; k >= static_cast<int>(std::max<uint32_t>(clique, 1)); --k) {
+        std::vector<int> c2 = colour;
+        for (size_t i = 0; i < m; ++i)
+            if (c2[i] >= k) c2[i] = static_cast<int>(rnd() % k);
+        std::vector<uint16_t> cnt(m * static_cast<size_t>(k), 0);
+        for (size_t i = 0; i < m; ++i)
+            for (uint32_t e = nb_off[i]; e < nb_off[i + 1]; ++e) ++cnt[i * k + c2[nb[e]]];
+        long conflicts = 0;
+        for (size_t i = 0; i < m; ++i) conflicts += cnt[i * k + c2[i]];
+        conflicts /= 2;
+        long best = conflicts;
+        std::vector<long> tabu(m * static_cast<size_t>(k), 0);
+        std::vector<uint32_t> open;
+        std::vector<int64_t> pos(m, -1);
+        auto update = [&](uint32_t i) {
+            const bool bad = cnt[i * k + c2[i]] > 0;
+            if (bad && pos[i] < 0) {
+                pos[i] = static_cast<int64_t>(open.size());
+                open.push_back(i);
+            } else if (!bad && pos[i] >= 0) {
+                const uint32_t last = open.back();
+                open[pos[i]] = last;
+                pos[last] = pos[i];
+                open.pop_back();
+                pos[i] = -1;
+            }
+        };
+        for (size_t i = 0; i < m; ++i) update(static_cast<uint32_t>(i));
+        for (long it = 0; it < budget && !open.empty(); ++it) {
+            const uint32_t i = open[rnd() % open.size()];
+            const int cur = c2[i];
+            int bc = -1, bv = 1 << 30;
+            for (int c = 0; c < k; ++c) {
+                if (c == cur) continue;
+                const int v = cnt[i * k + c];
+                const bool aspiration = conflicts - cnt[i * k + cur] + v < best;
+                if (tabu[i * k + c] > it && !aspiration) continue;
+                if (v < bv || (v == bv && (rnd() & 1))) {
+                    bv = v;
+                    bc = c;
+                }
+            }
+            if (bc < 0) continue;
+            conflicts += bv - cnt[i * k + cur];
+            tabu[i * k + cur] = it + 7 + static_cast<long>(rnd() % 10) + static_cast<long>(open.size() / 10);
+            c2[i] = bc;
+            for (uint32_t e = nb_off[i]; e < nb_off[i + 1]; ++e) {
+                const uint32_t j = nb[e];
+                --cnt[j * k + cur];
+                ++cnt[j * k + bc];
+                update(j);
+            }
+            update(i);
+            best = std::min(best, conflicts);
+        }
+        if (!open.empty()) return k + 1;
+        colour = c2;
+        colours = k;
+    }
+    return colours;
+}
+
 // Evens out, CTA by CTA, how many records each colour gives the CTA, without
 // adding colours: a constraint whose colour holds more than the CTA's mean
 // moves to the colour with the fewest of the CTA's records that none of its
@@ -68,6 +177,27 @@ void balance_colours(const std::vector<std::array<uint32_t, 4>>& nodes, const st
 }
 
 }  // namespace
+
+// True when a record of global stage g (distance stages, then dihedral
+// stages) has a node flagged in `attached`.
+static bool stage_touches(const OwnedDefinition& d, const ClusterSchedule& S, const std::vector<uint8_t>& attached,
+                          int g) {
+    const int S0 = S.kinds[0].stages;
+    const int k = g < S0 ? 0 : 1, s = k ? g - S0 : g;
+    const ClusterKind& K = S.kinds[k];
+    for (int c = 0; c < S.ctas; ++c)
+        for (uint32_t r = K.offsets[static_cast<size_t>(c) * (K.stages + 1) + s];
+             r < K.offsets[static_cast<size_t>(c) * (K.stages + 1) + s + 1]; ++r) {
+            const uint32_t i = K.def_index[r];
+            if (k == 0) {
+                if (attached[d.constraints[i].first_node] || attached[d.constraints[i].second_node]) return true;
+            } else {
+                for (int q = 0; q < 4; ++q)
+                    if (attached[d.dihedrals[i].nodes[q]]) return true;
+            }
+        }
+    return false;
+}
 
 bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes, int ctas,
                             ClusterSchedule& S, bool split) {
@@ -131,6 +261,7 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
         std::vector<int> colour(m, 0);  // becomes the stage
         if (!split || ctas == 1) {
             K.stages = dsatur_colour(nodes, counts, colour);
+            K.stages = reduce_colours(nodes, counts, N, K.stages, colour, kColourSearchMoves);
             balance_colours(nodes, counts, cta_of, ctas, N, K.stages, colour);
             K.cluster_sync.assign(K.stages, 1);
             K.interior_stages = 0;
@@ -233,6 +364,24 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
                     order.push_back(K.def_index[r]);
     }
 
+    // line iteration window: the last two stages of the iteration, when
+    // neither touches a suspension endpoint node (classic stages: both end in
+    // a cluster barrier)
+    if (S.susp_cta >= 0 && !(split && ctas > 1)) {
+        std::vector<uint8_t> attached(N, 0);
+        for (uint32_t n : suspension_nodes) attached[n] = 1;
+        const int S0 = S.kinds[0].stages, Sg = S0 + S.kinds[1].stages;
+        if (Sg >= 2 && !stage_touches(d, S, attached, Sg - 2) && !stage_touches(d, S, attached, Sg - 1)) {
+            S.line_stage = Sg - 2;
+            for (int g = Sg - 2; g < Sg; ++g) {
+                const int k = g < S0 ? 0 : 1, s = k ? g - S0 : g;
+                const ClusterKind& K = S.kinds[k];
+                const size_t o = static_cast<size_t>(S.susp_cta) * (K.stages + 1) + s;
+                S.line_owner_records = std::max(S.line_owner_records, K.offsets[o + 1] - K.offsets[o]);
+            }
+        }
+    }
+
     // seam closing pass: level scheduling in sweep order, executing CTA =
     // owner of the first node
     {
@@ -289,6 +438,20 @@ void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_
         const uint32_t slot = S.slot_of_node[n];
         if (slot < S.patch_begin[S.susp_cta] || slot >= S.patch_begin[S.susp_cta + 1])
             fail("suspension node outside the owner patch");
+    }
+    if (S.line_stage >= 0) {
+        const int S0 = S.kinds[0].stages, Sg = S0 + S.kinds[1].stages;
+        if (S.susp_cta < 0 || S.line_stage != Sg - 2) fail("line iteration window position");
+        std::vector<uint8_t> attached(N, 0);
+        for (uint32_t n : suspension_nodes) attached[n] = 1;
+        for (int g = Sg - 2; g < Sg; ++g) {
+            const int k = g < S0 ? 0 : 1, s = k ? g - S0 : g;
+            if (stage_touches(d, S, attached, g)) fail("line iteration window touches a suspension node");
+            if (!S.kinds[k].cluster_sync[s]) fail("line iteration window without cluster barriers");
+            const size_t o = static_cast<size_t>(S.susp_cta) * (S.kinds[k].stages + 1) + s;
+            if (S.kinds[k].offsets[o + 1] - S.kinds[k].offsets[o] > S.line_owner_records)
+                fail("line iteration window record count");
+        }
     }
     std::vector<int64_t> stamp(N, -1);
     int64_t epoch = 0;

@@ -69,22 +69,43 @@ struct ClusterSchedule {
     std::vector<uint32_t> seam_offsets;  // [ctas * (seam_stages + 1)]
     std::vector<uint32_t> seam_ab;
     int susp_cta = -1;
+    // Line iteration window (classic stages only): when the last two stages
+    // of an iteration touch no suspension endpoint node, the iteration's line
+    // iteration runs beside them on a warp of the suspension CTA that has no
+    // record in either, instead of after them behind a barrier of its own.
+    // line_stage = the first of the two (global stage index: distance stages
+    // then dihedral stages), -1 without a window; line_owner_records = the
+    // suspension CTA's larger record count of the two.
+    int line_stage = -1;
+    uint32_t line_owner_records = 0;
     std::vector<uint64_t> distance_order, dihedral_order;
 };
 
 // Cluster barriers per constraint iteration (stages followed by one, plus
-// the suspension stage).
+// the suspension stage unless the line iteration runs beside two stages).
 inline int cluster_barriers_per_iteration(const ClusterSchedule& s) {
-    int n = s.susp_cta >= 0 ? 1 : 0;
+    int n = s.susp_cta >= 0 && s.line_stage < 0 ? 1 : 0;
     for (const ClusterKind& k : s.kinds)
         for (uint8_t b : k.cluster_sync) n += b;
     return n;
+}
+
+// Dynamic shared memory of the cluster step kernel for this schedule
+// (nodes, forces/velocities, multipliers, stage offsets; with slack for the
+// 16-byte alignment of each array).
+inline size_t cluster_shared_bytes(const ClusterSchedule& s) {
+    return s.max_patch * 32ull + s.kinds[0].max_cta_records * 4ull + s.kinds[1].max_cta_records * 4ull +
+           (s.kinds[0].stages + s.kinds[1].stages + 2) * 4ull + 64;
 }
 
 // Returns false (and leaves `out` empty) when the mesh does not fit one
 // cluster of `ctas` CTAs (a patch over kClusterPatchNodes nodes).
 bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes, int ctas,
                             ClusterSchedule& out, bool split = false);
+
+// Move budget of the search for a colouring with fewer colours (per colour
+// count tried).
+constexpr long kColourSearchMoves = 300000;
 
 // Boundary colours with at most this many records may form the single-CTA
 // tail of a kind's split stages.

@@ -731,9 +731,7 @@ extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definiti
                 ClusterSchedule C;
                 if (!build_cluster_schedule(def, susp, c, C, options && (options->flags & SWB_OPT_SPLIT_STAGES)))
                     continue;
-                const size_t bytes = C.max_patch * 32ull + C.kinds[0].max_cta_records * 4ull +
-                                     C.kinds[1].max_cta_records * 4ull +
-                                     (C.kinds[0].stages + C.kinds[1].stages + 2) * 4ull + 64;
+                const size_t bytes = cluster_shared_bytes(C);
                 if (bytes > 227 * 1024 - 2048) continue;
                 verify_cluster_schedule(def, susp, C);
                 std::memset(out, 0, sizeof(*out));

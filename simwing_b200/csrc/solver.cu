@@ -159,9 +159,7 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
         }
         for (int c : candidates) {
             if (!build_cluster_schedule(def, susp_nodes, c, csched, (opt.flags & SWB_OPT_SPLIT_STAGES) != 0)) continue;
-            const size_t bytes = csched.max_patch * 32ull + csched.kinds[0].max_cta_records * 4ull +
-                                 csched.kinds[1].max_cta_records * 4ull +
-                                 (csched.kinds[0].stages + csched.kinds[1].stages + 2) * 4ull + 64;
+            const size_t bytes = cluster_shared_bytes(csched);
             if (bytes > smem_limit) continue;
             cluster_mode = true;
             break;
@@ -215,6 +213,13 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
                                                           cluster_mode ? dev::kClusterMaxThreads : 512));
     if (threads % 32 != 0 || threads < 32 || threads > (cluster_mode ? dev::kClusterMaxThreads : 1024))
         raise(SWB_INVALID_ARGUMENT, "block_threads out of range for the chosen schedule");
+    if (cluster_mode && csched.line_stage >= 0) {
+        // the line iteration needs a warp of the suspension CTA that is idle
+        // in its two stages
+        const int need = static_cast<int>((csched.line_owner_records + 31) / 32 * 32 + 32);
+        if (opt.block_threads <= 0 && need > threads && need <= dev::kClusterMaxThreads) threads = need;
+        if (need > threads) csched.line_stage = -1;
+    }
 
     // ---- device images -------------------------------------------------------
     // nodes (slot order)
@@ -282,6 +287,7 @@ void StructureImpl::upload_cluster_tables() {
     base.seam_offsets = dupload(owned, csched.seam_offsets, stream);
     base.seam_ab = dupload(owned, csched.seam_ab, stream);
     base.seam_stages = csched.seam_stages;
+    base.line_stage = csched.line_stage;
     cluster_base = base;
 }
 

@@ -253,7 +253,7 @@ __device__ __forceinline__ bool payload_point(const DevPayloadDef& d, const DevP
 // solveLineIteration (suspension.cpp:2197-2274): serial unilateral
 // projection of every segment with the rigid-endpoint effective mass.
 // Nodes are level-1 local indices into x (the owner CTA's patch).
-__device__ void line_iteration(const DevPayloadDef& d, DevPayloadState& s, float4* x, float dt, int* status) {
+__device__ __noinline__ void line_iteration(const DevPayloadDef& d, DevPayloadState& s, float4* x, float dt, int* status) {
     M3 R, I, invI;
     if (!q_rotation(s.q, R)) { susp_fail(status, kSuspOrientation); return; }
     I = world_inertia(R, d.inertia);
