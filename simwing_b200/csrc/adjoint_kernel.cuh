@@ -238,14 +238,35 @@ __device__ void predict_reverse(PilotAdjoint& A, const AdjointPilot& ap, const D
 // ---- projections ----------------------------------------------------------------
 __device__ __forceinline__ adj::V3<float> v3a(float4 a) { return {a.x, a.y, a.z}; }
 
+// The tape entries of record i of this iteration: position and multiplier of
+// the first node, then the other nodes' positions (2 entries for a distance
+// record, 4 for a dihedral).
+struct RecordTape {
+    float4 t[4];
+};
+__device__ __forceinline__ RecordTape load_tape(int kind, const TapeStep& tp, int it, uint32_t i) {
+    const uint32_t rtotal = kind ? tp.r1 : tp.r0;
+    const float4* tape = (kind ? tp.dih : tp.dist) + static_cast<size_t>(it) * (kind ? 4 : 2) * rtotal;
+    RecordTape t;
+    t.t[0] = __ldcs(tape + i);
+    t.t[1] = __ldcs(tape + rtotal + i);
+    if (kind) {
+        t.t[2] = __ldcs(tape + 2 * rtotal + i);
+        t.t[3] = __ldcs(tape + 3 * rtotal + i);
+    } else {
+        t.t[2] = t.t[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    return t;
+}
+
 __device__ __forceinline__ void reverse_record(const ClusterRecord& r, int kind, uint32_t me, uint32_t x_base,
-                                               const float4* tape, uint32_t rtotal, float* lamb, float* acc_r,
-                                               float* acc_c, uint32_t first, float inv_dt2) {
+                                               const RecordTape& tp, float* lamb, float* acc_r, float* acc_c,
+                                               uint32_t first, float inv_dt2) {
     const uint32_t pa = node_addr(r.ab & 0xffffu, me, 0u, x_base);
     const uint32_t pb = node_addr(r.ab >> 16, me, 0u, x_base);
     const uint32_t slot = r.index - first;
     if (kind == 0) {
-        const float4 A4 = __ldcs(tape + r.index), B4 = __ldcs(tape + rtotal + r.index);
+        const float4 A4 = tp.t[0], B4 = tp.t[1];
         const float4 XA = ld_node(pa), XB = ld_node(pb);
         adj::DistanceGrad<float> g{v3a(XA), v3a(XB), lamb[slot], 0.0f, 0.0f};
         adj::dist_reverse(v3a(A4), v3a(B4), XA.w, XB.w, A4.w, r.rest, fabsf(r.comp), signbit(r.comp) != 0, inv_dt2,
@@ -258,8 +279,7 @@ __device__ __forceinline__ void reverse_record(const ClusterRecord& r, int kind,
     } else {
         const uint32_t pc = node_addr(r.cd & 0xffffu, me, 0u, x_base);
         const uint32_t pd = node_addr(r.cd >> 16, me, 0u, x_base);
-        const float4 A4 = __ldcs(tape + r.index), B4 = __ldcs(tape + rtotal + r.index);
-        const float4 C4 = __ldcs(tape + 2 * rtotal + r.index), D4 = __ldcs(tape + 3 * rtotal + r.index);
+        const float4 A4 = tp.t[0], B4 = tp.t[1], C4 = tp.t[2], D4 = tp.t[3];
         const float4 XA = ld_node(pa), XB = ld_node(pb), XC = ld_node(pc), XD = ld_node(pd);
         const adj::V3<float> p[4] = {v3a(A4), v3a(B4), v3a(C4), v3a(D4)};
         const float w[4] = {XA.w, XB.w, XC.w, XD.w};
@@ -276,8 +296,12 @@ __device__ __forceinline__ void reverse_record(const ClusterRecord& r, int kind,
     }
 }
 
-__global__ void __launch_bounds__(kClusterMaxThreads)
-xpbd_cluster_adjoint_kernel(const __grid_constant__ AdjointParams p) {
+// kMaxThreads: the launch bound.  Up to 512 threads a thread has the
+// registers (128) to prefetch the next stage's record and tape entries; the
+// 768-thread instantiation (80 registers) loads them when it reaches them.
+template <int kMaxThreads>
+__global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(const __grid_constant__ AdjointParams p) {
+    constexpr bool kPrefetch = kMaxThreads <= 512;
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ PilotAdjoint pa;
@@ -369,6 +393,20 @@ xpbd_cluster_adjoint_kernel(const __grid_constant__ AdjointParams p) {
         }
     }
     // ---- iterations, last first --------------------------------------------------------
+    // In the narrow instantiation each thread prefetches its first record of
+    // the next stage visited and that record's tape entries before it works on
+    // the current one, so the loads from L2 and DRAM overlap the stage and its
+    // barrier.  The record arrays' pointers are held in registers.
+    const uint4* rec[2] = {I.kind[0].rec, I.kind[1].rec};
+    ClusterRecord next;
+    next.index = ~0u;
+    RecordTape next_tape{};
+    auto prefetch = [&](int it, int g) {
+        const int kind = g < S0 ? 0 : 1;
+        next = load_record(rec[kind], stage_lo(g) + tid, stage_hi(g));
+        if (next.index != ~0u) next_tape = load_tape(kind, p.tape, it, next.index);
+    };
+    if (kPrefetch && p.iterations > 0 && S > 0) prefetch(p.iterations - 1, S - 1);
     for (int it = p.iterations - 1; it >= 0; --it) {
         if (I.susp_cta >= 0) {
             if (pilot_warp) line_reverse(pa, *ap, p.tape.line[it], xb, p.dt);
@@ -376,10 +414,21 @@ xpbd_cluster_adjoint_kernel(const __grid_constant__ AdjointParams p) {
         }
         for (int g = S - 1; g >= 0; --g) {
             const int kind = g < S0 ? 0 : 1;
-            const uint32_t rtotal = kind ? p.tape.r1 : p.tape.r0;
-            const float4* tape = (kind ? p.tape.dih : p.tape.dist) + static_cast<size_t>(it) * (kind ? 4 : 2) * rtotal;
-            for (uint32_t i = stage_lo(g) + tid; i < stage_hi(g); i += blockDim.x)
-                reverse_record(load_record(I.kind[kind], kind, i, stage_hi(g)), kind, me, x_base, tape, rtotal,
+            uint32_t i = stage_lo(g) + tid;
+            if constexpr (kPrefetch) {
+                const ClusterRecord cur = next;
+                const RecordTape cur_tape = next_tape;
+                if (g > 0)
+                    prefetch(it, g - 1);
+                else if (it > 0)
+                    prefetch(it - 1, S - 1);
+                if (cur.index != ~0u)
+                    reverse_record(cur, kind, me, x_base, cur_tape, lam[kind], kind ? acc_c[1] : acc0r, acc_c[kind],
+                                   first[kind], p.inv_dt2);
+                i += blockDim.x;
+            }
+            for (; i < stage_hi(g); i += blockDim.x)
+                reverse_record(load_record(rec[kind], i, stage_hi(g)), kind, me, x_base, load_tape(kind, p.tape, it, i),
                                lam[kind], kind ? acc_c[1] : acc0r, acc_c[kind], first[kind], p.inv_dt2);
             cluster.sync();
         }
@@ -440,6 +489,9 @@ xpbd_cluster_adjoint_kernel(const __grid_constant__ AdjointParams p) {
     if (I.susp_cta < 0 && me == 0 && tid < 13) p.pb_in[tid] = 0.0f;
     cluster.sync();  // no CTA leaves while a peer may still read its memory
 }
+
+inline constexpr auto xpbd_cluster_adjoint_kernel = &xpbd_cluster_adjoint_kernel_t<kClusterMaxThreads>;
+inline constexpr auto xpbd_cluster_adjoint_kernel_narrow = &xpbd_cluster_adjoint_kernel_t<512>;
 
 }  // namespace dev
 }  // namespace swb

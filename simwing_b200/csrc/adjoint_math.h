@@ -20,6 +20,8 @@
 #include <cmath>
 #include <cstdint>
 
+#include "fast_math.h"
+
 #if defined(__CUDACC__)
 #define SWB_HD __host__ __device__ __forceinline__
 #else
@@ -89,6 +91,22 @@ template <class S> inline S m_rint(S x) { return std::rint(x); }
 template <class S> inline bool m_isfinite(S x) { return std::isfinite(x); }
 #endif
 
+// The projections' scalar forms: in float the device step's own (approximate
+// reciprocal, reciprocal square root, fast atan2), so that the reverse sweep
+// recomputes exactly the forward values the step produced; in double exact.
+SWB_HD float p_rcp(float x) { return fast_rcp(x); }
+SWB_HD double p_rcp(double x) { return 1.0 / x; }
+SWB_HD float p_rsqrt(float x) {
+#if defined(__CUDA_ARCH__)
+    return rsqrtf(x);
+#else
+    return 1.0f / std::sqrt(x);
+#endif
+}
+SWB_HD double p_rsqrt(double x) { return 1.0 / m_sqrt(x); }
+SWB_HD float p_atan2(float y, float x) { return fast_atan2(y, x); }
+SWB_HD double p_atan2(double y, double x) { return m_atan2(y, x); }
+
 template <class S> SWB_HD Dual<S> m_sqrt(Dual<S> a) {
     const S s = m_sqrt(a.v);
     return {s, a.d * S(0.5) / s};
@@ -136,13 +154,14 @@ SWB_HD void dist_forward(V3<S>& a, V3<S>& b, S wa, S wb, S& lambda, S rest, S co
     const S l2 = dot(d, d);
     const S k = S(1.0e-12);
     if (!(l2 > k * k)) return;
-    const S l = m_sqrt(l2);
+    const S il = p_rsqrt(l2);
+    const S l = l2 * il;
     if (l <= k) return;
     const S value = l - rest;
     if (cable && value <= S(0) && lambda == S(0)) return;
     const S W = wa + wb, alpha = comp * inv_dt2;
     if (W + alpha <= S(0)) return;
-    const S dl = (-value - alpha * lambda) / (W + alpha);
+    const S dl = (-value - alpha * lambda) * p_rcp(W + alpha);
     S applied = dl;
     if (cable) {
         const S s = lambda + dl;
@@ -152,7 +171,7 @@ SWB_HD void dist_forward(V3<S>& a, V3<S>& b, S wa, S wb, S& lambda, S rest, S co
     } else {
         lambda = lambda + dl;
     }
-    const S scale = applied / l;
+    const S scale = applied * il;
     a = a - d * (wa * scale);
     b = b + d * (wb * scale);
 }
@@ -167,14 +186,14 @@ SWB_HD void dist_reverse(V3<S> a, V3<S> b, S wa, S wb, S lambda, S rest, S comp,
     const S l2 = dot(d, d);
     const S k = S(1.0e-12);
     if (!(l2 > k * k)) return;
-    const S l = m_sqrt(l2);
+    const S il = p_rsqrt(l2);
+    const S l = l2 * il;
     if (l <= k) return;
-    const S il = S(1) / l;
     const S value = l - rest;
     if (cable && value <= S(0) && lambda == S(0)) return;
     const S W = wa + wb, alpha = comp * inv_dt2;
     if (W + alpha <= S(0)) return;
-    const S inv = S(1) / (W + alpha);
+    const S inv = p_rcp(W + alpha);
     const S dl = (-value - alpha * lambda) * inv;
     bool active = true;  // lambda' = lambda + dl, applied = dl
     S applied = dl;
@@ -214,6 +233,12 @@ SWB_HD S wrap_2pi(S x) {
     const S n = m_rint(x / two_pi);
     return x - n * two_pi;
 }
+// float: the device step's form (a branch within one turn, else remainderf)
+SWB_HD float wrap_2pi(float x) {
+    const float two_pi = 6.28318530717958647692f, half = 0.5f * two_pi;
+    if (fabsf(x) <= two_pi) return x > half ? x - two_pi : (x < -half ? x + two_pi : x);
+    return remainderf(x, two_pi);
+}
 
 template <class S>
 struct DihedralGrad {
@@ -229,25 +254,26 @@ SWB_HD void dihedral_forward(V3<S> p[4], const S w[4], S& lambda, S rest, S comp
     const S e2 = dot(e, e), q1 = dot(A1, A1), q2 = dot(A2, A2);
     const S k2 = S(1.0e-24);
     if (!(e2 > k2) || !(q1 > k2 * e2) || !(q2 > k2 * e2)) return;
-    const S iel = S(1) / m_sqrt(e2);
+    const S iel = p_rsqrt(e2);
     const S el = e2 * iel;
     const S Sv = dot(e, cross(A1, A2)) * iel;
     const S Cv = dot(A1, A2);
-    const S s1 = -el / q1, s2 = -el / q2;
+    const S rq1 = p_rcp(q1), rq2 = p_rcp(q2);
+    const S s1 = -el * rq1, s2 = -el * rq2;
     const V3<S> gc = A1 * s1, gd = A2 * s2;
     const S ie2 = iel * iel;
     const S t1 = dot(u, e) * ie2, t2 = dot(v, e) * ie2;
     const V3<S> gb = -(gc * t1 + gd * t2);
     const V3<S> ga = -((gb + gc) + gd);
     const V3<S> g[4] = {ga, gb, gc, gd};
-    const S theta = m_atan2(Sv, Cv);
+    const S theta = p_atan2(Sv, Cv);
     S wg = S(0);
     for (int k = 0; k < 4; ++k) wg = wg + w[k] * dot(g[k], g[k]);
     const S alpha = comp * inv_dt2;
     const S den = wg + alpha;
     if (!(den > S(0)) || !m_isfinite(den)) return;
     const S value = wrap_2pi(theta - rest);
-    const S dl = (-value - alpha * lambda) / den;
+    const S dl = (-value - alpha * lambda) * p_rcp(den);
     if (!m_isfinite(dl)) return;
     for (int k = 0; k < 4; ++k) p[k] = p[k] + g[k] * (w[k] * dl);
     lambda = lambda + dl;
@@ -263,13 +289,14 @@ SWB_HD void dihedral_reverse(const V3<S> p[4], const S w[4], S lambda, S rest, S
     const S e2 = dot(e, e), q1 = dot(A1, A1), q2 = dot(A2, A2);
     const S k2 = S(1.0e-24);
     if (!(e2 > k2) || !(q1 > k2 * e2) || !(q2 > k2 * e2)) return;
-    const S iel = S(1) / m_sqrt(e2);
+    const S iel = p_rsqrt(e2);
     const S el = e2 * iel;
     const V3<S> P = cross(A1, A2);
     const S Tv = dot(e, P);
     const S Sv = Tv * iel;
     const S Cv = dot(A1, A2);
-    const S s1 = -el / q1, s2 = -el / q2;
+    const S rq1 = p_rcp(q1), rq2 = p_rcp(q2);
+    const S s1 = -el * rq1, s2 = -el * rq2;
     const V3<S> gc = A1 * s1, gd = A2 * s2;
     const S ie2 = iel * iel;
     const S ue = dot(u, e), ve = dot(v, e);
@@ -277,14 +304,15 @@ SWB_HD void dihedral_reverse(const V3<S> p[4], const S w[4], S lambda, S rest, S
     const V3<S> gb = -(gc * t1 + gd * t2);
     const V3<S> ga = -((gb + gc) + gd);
     const V3<S> g[4] = {ga, gb, gc, gd};
-    const S theta = m_atan2(Sv, Cv);
+    const S theta = p_atan2(Sv, Cv);
     S wg = S(0);
     for (int k = 0; k < 4; ++k) wg = wg + w[k] * dot(g[k], g[k]);
     const S alpha = comp * inv_dt2;
     const S den = wg + alpha;
     if (!(den > S(0)) || !m_isfinite(den)) return;
+    const S iden = p_rcp(den);
     const S value = wrap_2pi(theta - rest);
-    const S dl = (-value - alpha * lambda) / den;
+    const S dl = (-value - alpha * lambda) * iden;
     if (!m_isfinite(dl)) return;
     // outputs: p_k' = p_k + w_k dl g_k, lambda' = lambda + dl
     S dlbar = G.lambda;
@@ -294,7 +322,6 @@ SWB_HD void dihedral_reverse(const V3<S> p[4], const S w[4], S lambda, S rest, S
         gbar[k] = G.p[k] * (w[k] * dl);
     }
     S lambar = G.lambda;
-    const S iden = S(1) / den;
     const S valuebar = -dlbar * iden;
     lambar = lambar - alpha * dlbar * iden;
     const S denbar = -dl * dlbar * iden;
@@ -305,9 +332,9 @@ SWB_HD void dihedral_reverse(const V3<S> p[4], const S w[4], S lambda, S rest, S
     // wg
     for (int k = 0; k < 4; ++k) gbar[k] = gbar[k] + g[k] * (S(2) * w[k] * denbar);
     // theta = atan2(Sv, Cv)
-    const S r2 = Sv * Sv + Cv * Cv;
-    const S Svbar = thetabar * Cv / r2;
-    const S Cvbar = -thetabar * Sv / r2;
+    const S ir2 = p_rcp(Sv * Sv + Cv * Cv);
+    const S Svbar = thetabar * Cv * ir2;
+    const S Cvbar = -thetabar * Sv * ir2;
     // ga = -(gb + gc + gd)
     V3<S> gbb = gbar[1] - gbar[0], gcb = gbar[2] - gbar[0], gdb = gbar[3] - gbar[0];
     // gb = -(t1 gc + t2 gd)
@@ -325,9 +352,9 @@ SWB_HD void dihedral_reverse(const V3<S> p[4], const S w[4], S lambda, S rest, S
     V3<S> A1bar = gcb * s1;
     V3<S> A2bar = gdb * s2;
     // s1 = -el / q1, s2 = -el / q2
-    S elbar = -s1bar / q1 - s2bar / q2;
-    const S q1bar = s1bar * el / (q1 * q1);
-    const S q2bar = s2bar * el / (q2 * q2);
+    S elbar = -s1bar * rq1 - s2bar * rq2;
+    const S q1bar = s1bar * el * rq1 * rq1;
+    const S q2bar = s2bar * el * rq2 * rq2;
     // Cv = A1 . A2
     A1bar = A1bar + A2 * Cvbar;
     A2bar = A2bar + A1 * Cvbar;

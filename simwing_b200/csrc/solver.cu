@@ -712,15 +712,22 @@ cudaError_t tape_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParam
 }
 
 cudaError_t adjoint_kernel_limits(int max_dynamic_smem, bool non_portable_cluster) {
-    cudaError_t rc = cudaFuncSetAttribute(dev::xpbd_cluster_adjoint_kernel,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem);
-    if (rc == cudaSuccess && non_portable_cluster)
-        rc = cudaFuncSetAttribute(dev::xpbd_cluster_adjoint_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaError_t rc = cudaSuccess;
+    for (auto kernel : {dev::xpbd_cluster_adjoint_kernel, dev::xpbd_cluster_adjoint_kernel_narrow}) {
+        if (rc == cudaSuccess)
+            rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem);
+        if (rc == cudaSuccess && non_portable_cluster)
+            rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
     return rc;
 }
 
+// Blocks of up to 512 threads take the instantiation with that launch bound
+// (registers for the tape prefetch).
 cudaError_t adjoint_kernel_launch(const cudaLaunchConfig_t& cfg, const AdjointParams& params) {
-    return cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_adjoint_kernel, params);
+    return cudaLaunchKernelEx(&cfg, cfg.blockDim.x <= 512 ? dev::xpbd_cluster_adjoint_kernel_narrow
+                                                          : dev::xpbd_cluster_adjoint_kernel,
+                              params);
 }
 
 swb_status decode_status(const int status[2], std::string& message) {

@@ -52,7 +52,7 @@ void distance_case(const char* name, V3<double> a, V3<double> b, double lambda, 
     const double adj[9] = {g.a.x, g.a.y, g.a.z, g.b.x, g.b.y, g.b.z, g.lambda, g.rest, g.comp};
     for (int j = 0; j < 9; ++j) {
         if (kink_lambda && j == 6) continue;
-        const double h = j == 8 ? 1e-12 : 1e-7;
+        const double h = j == 8 ? 1e-4 * comp : 1e-7;  // relative step for the compliance
         std::vector<double> up = u0, um = u0;
         up[j] += h;
         um[j] -= h;
