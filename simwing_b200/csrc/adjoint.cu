@@ -53,8 +53,10 @@ struct RolloutImpl {
     std::vector<StateBuf> ck, sg;      // checkpoints (segments + 1), segment states (interval + 1)
     std::vector<TapeStep> tape;        // per step of a segment
     int tape_iterations = -1;
+    float* line_jac = nullptr;  // per-iteration line-iteration Jacobians of the reverse step
     ClusterInstance* d_records = nullptr;  // step k of a segment: sg[k] -> sg[k + 1]
     AdjointPilot* d_pilot = nullptr;
+    int pilot_segments = 0, pilot_slots = 0;
     float4* xb[2] = {};
     float4* vb[2] = {};
     float* pb[2] = {};
@@ -155,6 +157,8 @@ struct RolloutImpl {
             ap.mass = d.mass;
             ap.min_length = d.min_length;
         }
+        pilot_segments = ap.segments;
+        pilot_slots = ap.slots;
         d_pilot = ralloc<AdjointPilot>(owned, 1);
         cuda_check(cudaMemcpyAsync(d_pilot, &ap, sizeof(ap), cudaMemcpyHostToDevice, S->stream), "pilot upload");
         // records of a segment's steps
@@ -233,6 +237,16 @@ struct RolloutImpl {
             t.rs = rs;
             t.pilot = d_pilot;
             tape.push_back(t);
+        }
+        if (line_jac) {
+            cudaFree(line_jac);
+            owned.erase(std::remove(owned.begin(), owned.end(), static_cast<void*>(line_jac)), owned.end());
+            line_jac = nullptr;
+        }
+        if (S->def.has_suspension) {
+            const size_t nin = 8 + 2 * static_cast<size_t>(pilot_segments) + 3 * static_cast<size_t>(pilot_slots);
+            const size_t nout = 7 + static_cast<size_t>(pilot_segments) + 3 * static_cast<size_t>(pilot_slots);
+            line_jac = ralloc<float>(owned, it * nin * nout);
         }
         tape_iterations = iterations;
     }
@@ -364,6 +378,7 @@ struct RolloutImpl {
         const double dt = settings.time_step;
         AdjointParams ap = base;
         ap.fbar = fbar;
+        ap.line_jac = line_jac;
         ap.g_rest0 = g_rest0;
         ap.g_comp0 = g_comp0;
         ap.g_comp1 = g_comp1;

@@ -144,30 +144,33 @@ __device__ void finish_reverse(PilotAdjoint& A, const AdjointPilot& ap, const Pi
 }
 
 // Line iteration: inputs com 3, q 4, lambda ns, xs 3S, rest ns, mass;
-// outputs com 3, q 4, lambda ns, xs 3S.
-__device__ void line_reverse(PilotAdjoint& A, const AdjointPilot& ap, const PilotTape& t, float4* xb, float dt) {
+// outputs com 3, q 4, lambda ns, xs 3S.  Its Jacobian depends only on the
+// taped inputs, so the kernel's prologue computes every iteration's Jacobian
+// at once (one warp per iteration, one input direction per lane, dual
+// numbers) and the sweep itself only contracts it with the output adjoints.
+__device__ __forceinline__ int line_inputs(const AdjointPilot& ap) { return 8 + 2 * ap.segments + 3 * ap.slots; }
+__device__ __forceinline__ int line_outputs(const AdjointPilot& ap) { return 7 + ap.segments + 3 * ap.slots; }
+
+// J[k * nin + j] = d out_k / d in_j at the taped inputs, by the calling warp.
+__device__ void line_jacobian(const AdjointPilot& ap, const PilotTape& t, float dt, float* J) {
     const int lane = threadIdx.x & 31;
     const int S = ap.slots, ns = ap.segments;
-    const int nin = 8 + 2 * ns + 3 * S, nout = 7 + ns + 3 * S;
-    if (lane == 0) {
-        for (int k = 0; k < 3; ++k) A.u[k] = t.com[k];
-        for (int k = 0; k < 4; ++k) A.u[3 + k] = t.q[k];
-        for (int k = 0; k < ns; ++k) A.u[7 + k] = t.lambda[k];
-        for (int s = 0; s < S; ++s) {
-            A.u[7 + ns + 3 * s] = t.xs[s].x; A.u[8 + ns + 3 * s] = t.xs[s].y; A.u[9 + ns + 3 * s] = t.xs[s].z;
-        }
-        for (int k = 0; k < ns; ++k) A.u[7 + ns + 3 * S + k] = ap.rest[k];
-        A.u[7 + 2 * ns + 3 * S] = ap.mass;
-        for (int k = 0; k < 7; ++k) A.ybar[k] = A.pb[k];
-        for (int k = 0; k < ns; ++k) A.ybar[7 + k] = A.seg_lambda[k];
-        for (int s = 0; s < S; ++s) {
-            const float4 X = xb[ap.slot_node[s]];
-            A.ybar[7 + ns + 3 * s] = X.x; A.ybar[8 + ns + 3 * s] = X.y; A.ybar[9 + ns + 3 * s] = X.z;
-        }
+    const int nin = line_inputs(ap), nout = line_outputs(ap);
+    float u[kPilotMaxIn];
+    for (int k = 0; k < 3; ++k) u[k] = t.com[k];
+    for (int k = 0; k < 4; ++k) u[3 + k] = t.q[k];
+    for (int k = 0; k < ns; ++k) u[7 + k] = t.lambda[k];
+    for (int s = 0; s < S; ++s) {
+        u[7 + ns + 3 * s] = t.xs[s].x; u[8 + ns + 3 * s] = t.xs[s].y; u[9 + ns + 3 * s] = t.xs[s].z;
     }
-    __syncwarp();
+    for (int k = 0; k < ns; ++k) u[7 + ns + 3 * S + k] = ap.rest[k];
+    u[7 + 2 * ns + 3 * S] = ap.mass;
     const adj::PilotDef<float> d = pilot_def(ap);
-    warp_vjp(nin, nout, A.u, A.ybar, A.ubar, [&](DualF* in, DualF* out) {
+    for (int base = 0; base < nin; base += 32) {
+        const int j = base + lane;
+        DualF in[kPilotMaxIn];
+        DualF out[kPilotMaxOut];
+        for (int k = 0; k < nin; ++k) in[k] = DualF(u[k], k == j ? 1.0f : 0.0f);
         adj::PilotState<DualF> s;
         s.com = {in[0], in[1], in[2]};
         s.q = {in[3], in[4], in[5], in[6]};
@@ -187,7 +190,32 @@ __device__ void line_reverse(PilotAdjoint& A, const AdjointPilot& ap, const Pilo
         for (int k = 0; k < S; ++k) {
             out[7 + ns + 3 * k] = xs[k].x; out[8 + ns + 3 * k] = xs[k].y; out[9 + ns + 3 * k] = xs[k].z;
         }
-    });
+        if (j < nin)
+            for (int k = 0; k < nout; ++k) J[k * nin + j] = out[k].d;
+    }
+}
+
+// Reverse of one line iteration through its Jacobian J (from the prologue):
+// ubar_j = sum_k ybar_k J[k][j], summed in the order of warp_vjp.
+__device__ void line_reverse(PilotAdjoint& A, const AdjointPilot& ap, const float* J, float4* xb) {
+    const int lane = threadIdx.x & 31;
+    const int S = ap.slots, ns = ap.segments;
+    const int nin = line_inputs(ap), nout = line_outputs(ap);
+    if (lane == 0) {
+        for (int k = 0; k < 7; ++k) A.ybar[k] = A.pb[k];
+        for (int k = 0; k < ns; ++k) A.ybar[7 + k] = A.seg_lambda[k];
+        for (int s = 0; s < S; ++s) {
+            const float4 X = xb[ap.slot_node[s]];
+            A.ybar[7 + ns + 3 * s] = X.x; A.ybar[8 + ns + 3 * s] = X.y; A.ybar[9 + ns + 3 * s] = X.z;
+        }
+    }
+    __syncwarp();
+    for (int j = lane; j < nin; j += 32) {
+        float s = 0.0f;
+        for (int k = 0; k < nout; ++k) s += A.ybar[k] * __ldcg(J + k * nin + j);
+        A.ubar[j] = s;
+    }
+    __syncwarp();
     if (lane == 0) {
         for (int k = 0; k < 7; ++k) A.pb[k] = A.ubar[k];
         for (int k = 0; k < ns; ++k) A.seg_lambda[k] = A.ubar[7 + k];
@@ -356,6 +384,22 @@ __global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(con
     auto stage_lo = [&](int g) { return g < S0 ? soff[g] : soff[S0 + 1 + (g - S0)]; };
     auto stage_hi = [&](int g) { return g < S0 ? soff[g + 1] : soff[S0 + 2 + (g - S0)]; };
 
+    // ---- line-iteration Jacobians of every iteration (all warps but the
+    // pilot warp, one iteration each; the pilot warp too when it is the only
+    // warp); read after the cluster barriers below
+    const int line_block = I.susp_cta >= 0 ? line_inputs(*ap) * line_outputs(*ap) : 0;
+    if (I.susp_cta >= 0) {
+        const int warps = static_cast<int>(blockDim.x >> 5);
+        const int total = p.ctas * warps;
+        const int workers = total > 1 ? total - 1 : 1;
+        int w = static_cast<int>(me) * warps + (tid >> 5);
+        const int pilot_at = I.susp_cta * warps;  // the pilot warp's index
+        if (total == 1 || w != pilot_at) {
+            if (total > 1 && w > pilot_at) --w;
+            for (int it = w; it < p.iterations; it += workers)
+                line_jacobian(*ap, p.tape.line[it], p.dt, p.line_jac + static_cast<size_t>(it) * line_block);
+        }
+    }
     // ---- payload finish ------------------------------------------------------------
     if (I.susp_cta >= 0) {
         if (pilot_warp) finish_reverse(pa, *ap, *p.tape.finish, *I.payload_in, xb, vb, p.dt);
@@ -407,9 +451,17 @@ __global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(con
         if (next.index != ~0u) next_tape = load_tape(kind, p.tape, it, next.index);
     };
     if (kPrefetch && p.iterations > 0 && S > 0) prefetch(p.iterations - 1, S - 1);
+    // The forward ran the line iteration beside its last two stages (neither
+    // touches a riser attachment node); the reverse of the line iteration runs
+    // beside the reverse of those two stages, on the same idle last warp of
+    // the suspension CTA: it arrives at the first reverse stage's barrier,
+    // runs, then waits, and its writes are released by its arrival at the
+    // second one's barrier.
+    const int line_stage = I.susp_cta >= 0 ? I.line_stage : -1;
+    const bool line_warp = line_stage >= 0 && owner && (tid >> 5) == static_cast<int>(blockDim.x >> 5) - 1;
     for (int it = p.iterations - 1; it >= 0; --it) {
-        if (I.susp_cta >= 0) {
-            if (pilot_warp) line_reverse(pa, *ap, p.tape.line[it], xb, p.dt);
+        if (I.susp_cta >= 0 && line_stage < 0) {
+            if (pilot_warp) line_reverse(pa, *ap, p.line_jac + static_cast<size_t>(it) * line_block, xb);
             cluster.sync();
         }
         for (int g = S - 1; g >= 0; --g) {
@@ -430,7 +482,13 @@ __global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(con
             for (; i < stage_hi(g); i += blockDim.x)
                 reverse_record(load_record(rec[kind], i, stage_hi(g)), kind, me, x_base, load_tape(kind, p.tape, it, i),
                                lam[kind], kind ? acc_c[1] : acc0r, acc_c[kind], first[kind], p.inv_dt2);
-            cluster.sync();
+            if (g == line_stage + 1 && line_warp) {
+                cluster_arrive();
+                line_reverse(pa, *ap, p.line_jac + static_cast<size_t>(it) * line_block, xb);
+                cluster_wait();
+            } else {
+                cluster.sync();
+            }
         }
     }
     // ---- predict: x = X + dt (ref + (V + (g + f w) dt - ref) damping) --------------------

@@ -137,6 +137,10 @@ struct AdjointParams {
     double* g_comp1;               // per dihedral record
     double* g_seg_rest;            // per device suspension segment
     double* g_mass;
+    // scratch: Jacobian of each iteration's line iteration, [iterations]
+    // blocks of nout x nin floats (output-major), written in the kernel's
+    // prologue; nullptr without a pilot
+    float* line_jac;
     int ctas;
     float dt, inv_dt, inv_dt2, damping;
     float3 gravity;
