@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t bar;
     __shared__ DevPayloadState pay;
+    __shared__ DevPayloadDef pdef;  // suspension CTA: the payload definition, read on every line iteration
     __shared__ float4* peers[16];
     __shared__ float3 shift_s;
     cg::cluster_group cluster = cg::this_cluster();
@@ -207,6 +208,9 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         v[i] = make_float4(f.x, f.y, f.z, 0.0f);
     }
     if (owner && tid == 0) pay = *I.payload_in;
+    if (owner)
+        for (uint32_t i = tid; i < sizeof(DevPayloadDef) / 4; i += blockDim.x)
+            reinterpret_cast<uint32_t*>(&pdef)[i] = __ldg(reinterpret_cast<const uint32_t*>(I.payload_def) + i);
     __syncthreads();  // mbarrier initialised before any thread waits on it
     if (!mbar_wait(&bar, 0, p.copy_budget)) {
         atomicOr(I.status, kStatusCopyTimeout);
@@ -229,7 +233,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     }
     if (owner && tid == 0) {
         for (int k = 0; k < 8; ++k) pay.lambda[k] = 0.0f;
-        if (!payload_predict(*I.payload_def, pay, p.dt, p.gravity)) susp_fail(I.status, kSuspPayload);
+        if (!payload_predict(pdef, pay, p.dt, p.gravity)) susp_fail(I.status, kSuspPayload);
     }
     cluster.sync();
 
@@ -297,7 +301,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                     cluster_arrive();
                     if ((tid & 31) == 0) {
                         if constexpr (kTape) tape_pilot(p.tape.line[it], pay, *p.tape.pilot, x, nullptr);
-                        line_iteration(*I.payload_def, pay, x, p.dt, I.status);
+                        line_iteration(pdef, pay, x, p.dt, I.status);
                     }
                     __syncwarp();
                     cluster_wait();
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         if (susp_c && line_stage < 0) {
             if (owner && tid == 0) {
                 if constexpr (kTape) tape_pilot(p.tape.line[it], pay, *p.tape.pilot, x, nullptr);
-                line_iteration(*I.payload_def, pay, x, p.dt, I.status);
+                line_iteration(pdef, pay, x, p.dt, I.status);
             }
             cluster.sync();
         }
@@ -365,7 +369,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     __syncthreads();
     if (owner && tid == 0) {
         if constexpr (kTape) tape_pilot(*p.tape.finish, pay, *p.tape.pilot, x, v);
-        payload_finish(*I.payload_def, pay, *I.payload_in, x, v, p.dt, I.status);
+        payload_finish(pdef, pay, *I.payload_in, x, v, p.dt, I.status);
         float3 s = make_float3(0.0f, 0.0f, 0.0f);
         if (I.recentre && finite3(pay.com) &&
             fmaxf(fabsf(pay.com.x), fmaxf(fabsf(pay.com.y), fabsf(pay.com.z))) > 0.25f)
