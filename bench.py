@@ -55,6 +55,24 @@ def parse():
     return p.parse_args()
 
 
+def max_over_ranks(value, dist, device):
+    """Largest `value` over the ranks of the process group (`value` itself
+    without one).  Every rank calls it at the same point."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, world, seconds):
+    """Whole-job rate of `world` independent replicas that each processed
+    `units_per_rank` units, over the slowest rank's time."""
+    return world * units_per_rank / seconds
+
+
 def wing_config():
     return {"workload": "plain ram-air wing, 40 cells x 60 chordwise (67,428 tri), 48 iterations, 1 substep, "
                         "dt 1/120 s, 30 Pa + gravity, rigid pilot on 2 risers",
@@ -95,17 +113,13 @@ def batched_leg(sw, st, count, rank, world, dist, device):
         dist.barrier()
     torch.cuda.synchronize()
     batch.step(st, block)
-    ms = batch.last_step_ms()
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{device}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(batch.last_step_ms(), dist, f"cuda:{device}")
     ms_per_step = ms / block
     out = {"workload": f"{count} wings, cells U{{20..60}}, chordwise {{30,45,60}}, aspect ratio U(4.5,7), "
                        "compliance x lognormal(0,0.2), seed 2024; 48 iterations, 1 substep",
            "structures": count, "triangles_min": min(tris), "triangles_max": max(tris),
            "triangles_total": sum(tris), "graph_steps": block, "launches_per_step": 1,
-           "ms_per_step": ms_per_step, "wing_steps_per_s": world * count / (ms_per_step / 1000.0),
+           "ms_per_step": ms_per_step, "wing_steps_per_s": replica_rate(count, world, ms_per_step / 1000.0),
            "target_patch_nodes": rep.target_patch_nodes, "clusters": rep.clusters,
            "cluster_ctas": rep.cluster_ctas, "resident_clusters": rep.resident_clusters,
            "block_threads": rep.block_threads,
@@ -364,14 +378,11 @@ def main():
             structure.step(st, diagnostics=False)
             times.append(structure.last_step_ms())
     torch.cuda.synchronize()
-    total_ms = float(sum(times))
+    total_ms = max_over_ranks(sum(times), dist, f"cuda:{local}")
     if dist is not None:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms / 1000.0)
+    value = replica_rate(args.steps, world, total_ms / 1000.0)
 
     # end-to-end through the C-ABI with host buffers
     rng = np.random.default_rng(5)
@@ -386,12 +397,8 @@ def main():
     for _ in range(e2e_steps):
         structure.set_external_forces(forces)
         diag = structure.step(st, diagnostics=True)
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+    e2e_value = replica_rate(e2e_steps, world, e2e_s)
     h2d = structure.node_count * 16
     d2h = 148 * 16 * 8 + 16 + 128  # diagnostics partials + control word + payload
 
