@@ -108,6 +108,8 @@ struct RolloutImpl {
         S = &s;
         if (!S->cluster_mode)
             raise(SWB_UNSUPPORTED, "differentiable rollouts need the cluster schedule (the mesh does not fit one)");
+        if (S->momentum_guard)
+            raise(SWB_UNSUPPORTED, "differentiable rollouts of free structures (momentum guard) are not available");
         if (n_steps < 1) raise(SWB_INVALID_ARGUMENT, "a rollout needs at least one step");
         if (every < 1) raise(SWB_INVALID_ARGUMENT, "checkpoint interval must be positive");
         steps = n_steps;
@@ -206,7 +208,7 @@ struct RolloutImpl {
         smem = off;
         cudaDeviceProp prop{};
         cuda_check(cudaGetDeviceProperties(&prop, S->device), "cudaGetDeviceProperties");
-        const size_t limit = prop.sharedMemPerBlockOptin > 2048 ? prop.sharedMemPerBlockOptin - 2048 : 0;
+        const size_t limit = dynamic_smem_limit(prop);
         if (smem > limit)
             raise(SWB_UNSUPPORTED, "the reverse sweep needs " + std::to_string(smem) +
                                        " B of shared memory per CTA; build the structure with more cluster CTAs");

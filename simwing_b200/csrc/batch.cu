@@ -142,12 +142,13 @@ void pack(Packing& P, int cluster, int threads_opt, size_t smem_limit) {
     P.idle = 0;
     P.max_stages = 0;
     for (int c = 0; c < P.clusters; ++c) {
-        int stages = 0, seam = 0, susp = 0;
+        int stages = 0, seam = 0, susp = 0, guard = 0;
         for (size_t i : content[c]) {
             const StructureImpl& m = P.members[i]->s;
             stages = std::max(stages, m.csched.kinds[0].stages + m.csched.kinds[1].stages);
             seam = std::max(seam, m.csched.seam_stages);
             susp |= m.def.has_suspension ? 1 : 0;
+            guard |= m.momentum_guard ? 1 : 0;
         }
         P.max_stages = std::max(P.max_stages, stages);
         int rank = 0;
@@ -156,6 +157,7 @@ void pack(Packing& P, int cluster, int threads_opt, size_t smem_limit) {
                 ClusterSlot& s = P.slots[static_cast<size_t>(c) * cluster + rank];
                 s.instance = static_cast<int>(i);
                 s.rank_base = rank - r;
+                s.ctas = P.ranks[i];
             }
         for (; rank < cluster; ++rank) {
             P.slots[static_cast<size_t>(c) * cluster + rank].instance = -1;
@@ -166,6 +168,7 @@ void pack(Packing& P, int cluster, int threads_opt, size_t smem_limit) {
             s.stages = stages;
             s.seam_stages = seam;
             s.suspension = susp;
+            s.guard = guard;
         }
     }
     // shared memory: node arrays for the largest patch, then per-structure
@@ -514,7 +517,7 @@ swb_status swb_batch_create(const swb_structure_definition* const* definitions, 
         cuda_check(cudaSetDevice(B.device), "cudaSetDevice");
         cudaDeviceProp prop{};
         cuda_check(cudaGetDeviceProperties(&prop, B.device), "cudaGetDeviceProperties");
-        const size_t smem_limit = prop.sharedMemPerBlockOptin > 2048 ? prop.sharedMemPerBlockOptin - 2048 : 0;
+        const size_t smem_limit = dynamic_smem_limit(prop);
         B.smem_limit = smem_limit;
         cuda_check(cudaStreamCreateWithFlags(&B.stream, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaEventCreate(&B.ev0), "cudaEventCreate");

@@ -85,6 +85,107 @@ __device__ __forceinline__ void st_node(uint32_t addr, float4 v) {
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
 
+// ---- momentum guard of free structures (soft_body.cpp:119-190) -------------
+// Sums over a CTA's free nodes, in double: [0] mass, [1..3] sum m x,
+// [4..6] sum m v, [7..9] sum m x cross v, [10..15] sum m x x^T (xx yy zz xy
+// xz yz), m = 1 / inverse mass.
+constexpr int kMomentumFields = 16;
+constexpr int kMaxWarps = kClusterMaxThreads / 32;
+
+// This CTA's sums into out[16] (shared), by the whole block.
+__device__ __noinline__ void cta_momentum_sums(const float4* x, const float4* vel, uint32_t n, double* out,
+                                               double* scratch) {
+    double acc[kMomentumFields];
+    for (int f = 0; f < kMomentumFields; ++f) acc[f] = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 X = x[i], V = vel[i];
+        if (!(X.w > 0.0f)) continue;
+        const double m = 1.0 / static_cast<double>(X.w);
+        const double px = X.x, py = X.y, pz = X.z, vx = V.x, vy = V.y, vz = V.z;
+        acc[0] += m;
+        acc[1] += m * px; acc[2] += m * py; acc[3] += m * pz;
+        acc[4] += m * vx; acc[5] += m * vy; acc[6] += m * vz;
+        acc[7] += m * (py * vz - pz * vy); acc[8] += m * (pz * vx - px * vz); acc[9] += m * (px * vy - py * vx);
+        acc[10] += m * px * px; acc[11] += m * py * py; acc[12] += m * pz * pz;
+        acc[13] += m * px * py; acc[14] += m * px * pz; acc[15] += m * py * pz;
+    }
+    for (int f = 0; f < kMomentumFields; ++f)
+        for (int off = 16; off > 0; off >>= 1) acc[f] += __shfl_down_sync(0xffffffffu, acc[f], off);
+    const int warp = static_cast<int>(threadIdx.x >> 5);
+    if ((threadIdx.x & 31) == 0)
+        for (int f = 0; f < kMomentumFields; ++f) scratch[warp * kMomentumFields + f] = acc[f];
+    __syncthreads();
+    if (threadIdx.x < kMomentumFields) {
+        double s = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += scratch[w * kMomentumFields + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// Cluster totals of the sums in `sums` (the same shared offset in every CTA
+// of the structure), added in rank order so every CTA holds the same values;
+// after a cluster barrier.
+__device__ __forceinline__ void cluster_momentum_totals(cooperative_groups::cluster_group& cluster, double* sums,
+                                                        int ctas, uint32_t rank_base, double* total) {
+    if (threadIdx.x < kMomentumFields) {
+        double s = 0.0;
+        for (int r = 0; r < ctas; ++r)
+            s += cluster.map_shared_rank(sums, r + static_cast<int>(rank_base))[threadIdx.x];
+        total[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// Momentum about the centre of mass from the totals: com, linear momentum
+// and angular momentum about com.
+struct MomentumTotals {
+    double mass, com[3], p[3], L[3];
+};
+__device__ __forceinline__ MomentumTotals momentum_of(const double* t) {
+    MomentumTotals r;
+    r.mass = t[0];
+    for (int k = 0; k < 3; ++k) {
+        r.com[k] = t[0] > 0.0 ? t[1 + k] / t[0] : 0.0;
+        r.p[k] = t[4 + k];
+    }
+    // sum m (x - c) x v = sum m x x v - c x sum m v
+    r.L[0] = t[7] - (r.com[1] * t[6] - r.com[2] * t[5]);
+    r.L[1] = t[8] - (r.com[2] * t[4] - r.com[0] * t[6]);
+    r.L[2] = t[9] - (r.com[0] * t[5] - r.com[1] * t[4]);
+    return r;
+}
+
+// isPositiveDefinite and checkedSolve of a symmetric 3x3 (xx yy zz xy xz yz)
+// as the reference's membrane math states them (membrane.cpp:153-257);
+// false when the matrix is not positive definite or the inverse is rejected.
+__device__ bool guard_solve(const double* m, const double* rhs, double* out) {
+    if (!isfinite(m[0]) || !isfinite(m[1]) || !isfinite(m[2]) || !isfinite(m[3]) || !isfinite(m[4]) ||
+        !isfinite(m[5]) || !(m[0] > 0.0) || !(m[1] > 0.0) || !(m[2] > 0.0))
+        return false;
+    const double sx = sqrt(m[0]), sy = sqrt(m[1]), sz = sqrt(m[2]);
+    const double l10 = m[3] / sx / sy, l20 = m[4] / sx / sz;
+    const double p1 = 1.0 - l10 * l10;
+    if (!isfinite(p1) || !(p1 > 0.0)) return false;
+    const double l11 = sqrt(p1);
+    const double l21 = (m[5] / sy / sz - l20 * l10) / l11;
+    const double p2 = 1.0 - l20 * l20 - l21 * l21;
+    if (!isfinite(p2) || !(p2 > 0.0)) return false;
+    double scale = 0.0;
+    for (int k = 0; k < 6; ++k) scale = fmax(scale, fabs(m[k]));
+    const double det = m[0] * (m[1] * m[2] - m[5] * m[5]) - m[3] * (m[3] * m[2] - m[5] * m[4]) +
+                       m[4] * (m[3] * m[5] - m[1] * m[4]);
+    if (!isfinite(det) || fabs(det) <= 128.0 * 2.220446049250313e-16 * scale * scale * scale) return false;
+    const double id = 1.0 / det;
+    const double ixx = (m[1] * m[2] - m[5] * m[5]) * id, iyy = (m[0] * m[2] - m[4] * m[4]) * id,
+                 izz = (m[0] * m[1] - m[3] * m[3]) * id, ixy = (m[4] * m[5] - m[3] * m[2]) * id,
+                 ixz = (m[3] * m[5] - m[4] * m[1]) * id, iyz = (m[3] * m[4] - m[0] * m[5]) * id;
+    out[0] = ixx * rhs[0] + ixy * rhs[1] + ixz * rhs[2];
+    out[1] = ixy * rhs[0] + iyy * rhs[1] + iyz * rhs[2];
+    out[2] = ixz * rhs[0] + iyz * rhs[1] + izz * rhs[2];
+    return true;
+}
+
 // Projects one record.  Taping launches first store the record's inputs
 // (node positions and multiplier) at its index in this iteration's tape
 // blocks of `rtotal` entries.
@@ -152,6 +253,9 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     __shared__ DevPayloadDef pdef;  // suspension CTA: the payload definition, read on every line iteration
     __shared__ float4* peers[16];
     __shared__ float3 shift_s;
+    __shared__ double mom_scratch[kMaxWarps * kMomentumFields];
+    __shared__ double mom_pred[kMomentumFields], mom_cur[kMomentumFields];
+    __shared__ double mom_ptot[kMomentumFields], mom_tot[kMomentumFields];
     cg::cluster_group cluster = cg::this_cluster();
     ClusterSlot slot{};
     if constexpr (kPacked) {
@@ -159,7 +263,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         if (slot.instance < 0) {
             // idle rank: take every cluster barrier the busy ranks take
             const int barriers = 3 + p.iterations * (slot.stages + slot.suspension) +
-                                 (p.iterations > 0 ? slot.seam_stages : 0);
+                                 (p.iterations > 0 ? slot.seam_stages : 0) + (slot.guard ? 3 : 0);
             for (int b = 0; b < barriers; ++b) cluster.sync();
             return;
         }
@@ -178,6 +282,12 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     const uint32_t n = __ldg(I.patch_begin + me + 1) - base;
     const bool owner = static_cast<int>(me) == I.susp_cta;
     const uint32_t x_base = smem_addr(x);
+    // momentum guard: `guard` = this structure runs it; `guard_c` = the
+    // cluster takes its barriers (a packed cluster when any of its
+    // structures runs it); `sctas` = the structure's ranks
+    const bool guard = I.momentum_guard != 0;
+    const bool guard_c = kPacked ? slot.guard != 0 : guard;
+    const int sctas = kPacked ? slot.ctas : p.ctas;
 
     if (tid < p.ctas) peers[tid] = cluster.map_shared_rank(x, tid);
     if (tid == 0) {
@@ -230,10 +340,16 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         X.y += vy * p.dt;
         X.z += vz * p.dt;
         x[i] = X;
+        if (guard) v[i] = make_float4(vx, vy, vz, 0.0f);  // the predicted velocity, for the momentum guard
     }
     if (owner && tid == 0) {
         for (int k = 0; k < 8; ++k) pay.lambda[k] = 0.0f;
         if (!payload_predict(pdef, pay, p.dt, p.gravity)) susp_fail(I.status, kSuspPayload);
+    }
+    if (guard) {
+        // momentum of the predicted state (the guard's target)
+        __syncthreads();
+        cta_momentum_sums(x, v, n, mom_pred, mom_scratch);
     }
     cluster.sync();
 
@@ -367,6 +483,64 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         v[i] = V;
     }
     __syncthreads();
+    if (guard_c) {
+        // restoreMomentum (soft_body.cpp:152-190): the linear momentum of the
+        // predicted state by a uniform velocity change, then its angular
+        // momentum about the centre of mass by a rigid rotation rate.  Three
+        // cluster barriers whatever the structure (packed clusters take them
+        // on every rank).
+        if (guard) cta_momentum_sums(x, v, n, mom_cur, mom_scratch);
+        cluster.sync();
+        bool go = false;
+        MomentumTotals target{};
+        if (guard) {
+            cluster_momentum_totals(cluster, mom_pred, sctas, rank_base, mom_ptot);
+            cluster_momentum_totals(cluster, mom_cur, sctas, rank_base, mom_tot);
+            target = momentum_of(mom_ptot);
+            const MomentumTotals now = momentum_of(mom_tot);
+            go = target.mass > 0.0;
+            if (go) {
+                const float dvx = static_cast<float>((target.p[0] - now.p[0]) / target.mass);
+                const float dvy = static_cast<float>((target.p[1] - now.p[1]) / target.mass);
+                const float dvz = static_cast<float>((target.p[2] - now.p[2]) / target.mass);
+                for (uint32_t i = tid; i < n; i += blockDim.x)
+                    if (x[i].w > 0.0f) {
+                        float4 V = v[i];
+                        V.x += dvx; V.y += dvy; V.z += dvz;
+                        v[i] = V;
+                    }
+            }
+            __syncthreads();
+        }
+        cluster.sync();  // every CTA has read the sums before they are replaced
+        if (go) cta_momentum_sums(x, v, n, mom_cur, mom_scratch);
+        cluster.sync();
+        if (go) {
+            cluster_momentum_totals(cluster, mom_cur, sctas, rank_base, mom_tot);
+            const double* t = mom_tot;
+            const MomentumTotals c = momentum_of(t);
+            // inertia about the centre of mass from the second moments
+            const double M = t[0];
+            const double sxx = t[10] - M * c.com[0] * c.com[0], syy = t[11] - M * c.com[1] * c.com[1],
+                         szz = t[12] - M * c.com[2] * c.com[2], sxy = t[13] - M * c.com[0] * c.com[1],
+                         sxz = t[14] - M * c.com[0] * c.com[2], syz = t[15] - M * c.com[1] * c.com[2];
+            const double inertia[6] = {syy + szz, sxx + szz, sxx + syy, -sxy, -sxz, -syz};
+            const double dL[3] = {target.L[0] - c.L[0], target.L[1] - c.L[1], target.L[2] - c.L[2]};
+            double w[3];
+            if (guard_solve(inertia, dL, w))
+                for (uint32_t i = tid; i < n; i += blockDim.x) {
+                    const float4 X = x[i];
+                    if (!(X.w > 0.0f)) continue;
+                    const double rx = X.x - c.com[0], ry = X.y - c.com[1], rz = X.z - c.com[2];
+                    float4 V = v[i];
+                    V.x += static_cast<float>(w[1] * rz - w[2] * ry);
+                    V.y += static_cast<float>(w[2] * rx - w[0] * rz);
+                    V.z += static_cast<float>(w[0] * ry - w[1] * rx);
+                    v[i] = V;
+                }
+            __syncthreads();
+        }
+    }
     if (owner && tid == 0) {
         if constexpr (kTape) tape_pilot(*p.tape.finish, pay, *p.tape.pilot, x, v);
         payload_finish(pdef, pay, *I.payload_in, x, v, p.dt, I.status);

@@ -51,6 +51,11 @@ struct ClusterInstance {
     // the line iteration then follows the iteration's stages behind a
     // cluster barrier.  Single-structure launches only.
     int line_stage;
+    // 1: the momentum guard of free structures runs (no suspension, no
+    // contact, bending or membranes present, every node free:
+    // soft_body.cpp:1192-1202).  Single-structure launches only.
+    int momentum_guard;
+    int pad;
 };
 
 // Rigid pilot as the adjoint sees it: the suspension endpoint nodes are
@@ -103,7 +108,9 @@ struct ClusterSlot {
     int stages;        // colour stages per iteration: max over the cluster
     int seam_stages;   // seam stages: max over the cluster
     int suspension;    // 1 when a structure of the cluster has a pilot
-    int pad[3];
+    int guard;         // 1 when a structure of the cluster runs the momentum guard
+    int ctas;          // ranks of this CTA's structure (0 when idle)
+    int pad;
 };
 
 struct ClusterParams {

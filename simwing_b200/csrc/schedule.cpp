@@ -732,7 +732,9 @@ extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definiti
                 if (!build_cluster_schedule(def, susp, c, C, options && (options->flags & SWB_OPT_SPLIT_STAGES)))
                     continue;
                 const size_t bytes = cluster_shared_bytes(C);
-                if (bytes > 227 * 1024 - 2048) continue;
+                // opt-in shared memory less the kernels' static shared memory
+                // (under 6 KB; the device build reads the exact figure)
+                if (bytes > 227 * 1024 - 6144) continue;
                 verify_cluster_schedule(def, susp, C);
                 std::memset(out, 0, sizeof(*out));
                 out->blocks = C.ctas;

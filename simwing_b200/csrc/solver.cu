@@ -121,6 +121,10 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     fingerprint = definition_fingerprint(def.view);
     if (def.has_contact) raise(SWB_UNSUPPORTED, "fabric self-contact is not available in this build");
     if (!def.membranes.empty()) raise(SWB_UNSUPPORTED, "membrane elements are not available in this build");
+    // Solver-drift momentum restoration of isolated free structures: no
+    // suspension, no contact, bending or membranes present, no fixed node.
+    momentum_guard = !def.has_suspension && !def.has_contact && (!def.dihedrals.empty() || !def.membranes.empty()) &&
+                     std::none_of(def.nodes.begin(), def.nodes.end(), [](const swb_node_def& n) { return n.fixed != 0; });
     swb_solver_options opt;
     swb_default_solver_options(&opt);
     if (options) opt = *options;
@@ -144,7 +148,7 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     if (def.has_suspension && (def.segments.size() > 8 || def.harness.size() > 8))
         raise(SWB_UNSUPPORTED, "more than 8 suspension segments or harness points");
     const std::vector<uint32_t> susp_nodes = suspension_endpoint_nodes(def);
-    const size_t smem_limit = prop.sharedMemPerBlockOptin > 2048 ? prop.sharedMemPerBlockOptin - 2048 : 0;
+    const size_t smem_limit = dynamic_smem_limit(prop);
     cluster_mode = false;
     if (!(opt.flags & (SWB_OPT_GRID | SWB_OPT_GLOBAL_ONLY))) {
         if (opt.cluster_ctas < 0 || opt.cluster_ctas > kClusterMaxCtas)
@@ -167,6 +171,8 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
         if (!cluster_mode && opt.cluster_ctas > 0)
             raise(SWB_UNSUPPORTED, "the mesh does not fit a cluster of " + std::to_string(opt.cluster_ctas) + " CTAs");
     }
+    if (!cluster_mode && momentum_guard)
+        raise(SWB_UNSUPPORTED, "the momentum guard of a free structure needs the cluster schedule (the mesh does not fit one)");
     uint32_t widest = 32;
     if (cluster_mode) {
         verify_cluster_schedule(def, susp_nodes, csched);
@@ -288,6 +294,7 @@ void StructureImpl::upload_cluster_tables() {
     base.seam_ab = dupload(owned, csched.seam_ab, stream);
     base.seam_stages = csched.seam_stages;
     base.line_stage = csched.line_stage;
+    base.momentum_guard = momentum_guard ? 1 : 0;
     cluster_base = base;
 }
 
@@ -358,7 +365,7 @@ void StructureImpl::upload_grid_tables() {
 
 void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDeviceProp& prop) {
     StepParams& p = params;
-    const size_t smem_limit_ = prop.sharedMemPerBlockOptin > 2048 ? prop.sharedMemPerBlockOptin - 2048 : 0;
+    const size_t smem_limit_ = dynamic_smem_limit(prop);
     // diagnostics arrays (definition order of distance-like constraints)
     {
         std::vector<uint32_t> a(def.constraints.size()), b(def.constraints.size());
@@ -677,6 +684,20 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out)
     cuda_check(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dev::xpbd_step_kernel), dim3(G), dim3(threads),
                                            args, p.smem_total, stream),
                "cudaLaunchCooperativeKernel");
+}
+
+size_t dynamic_smem_limit(const cudaDeviceProp& prop) {
+    size_t reserve = 2048;
+    for (const void* k : {reinterpret_cast<const void*>(dev::xpbd_cluster_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_packed_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_tape_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_kernel_narrow),
+                          reinterpret_cast<const void*>(dev::xpbd_step_kernel)}) {
+        cudaFuncAttributes a{};
+        if (cudaFuncGetAttributes(&a, k) == cudaSuccess) reserve = std::max(reserve, a.sharedSizeBytes + 256);
+    }
+    return prop.sharedMemPerBlockOptin > reserve ? prop.sharedMemPerBlockOptin - reserve : 0;
 }
 
 cudaError_t packed_kernel_limits(int max_dynamic_smem, bool non_portable_cluster) {

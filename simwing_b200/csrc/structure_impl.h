@@ -29,6 +29,10 @@ constexpr int kDiagBlocks = 148;
 // Host entry points of the packed cluster kernel (several structures per
 // cluster), defined beside the kernels.
 cudaError_t packed_kernel_limits(int max_dynamic_smem, bool non_portable_cluster);
+// Dynamic shared memory a step, taping, packed or reverse kernel may request
+// on this device: the opt-in maximum less the largest static shared memory
+// among those kernels (at least 2 KB).
+size_t dynamic_smem_limit(const cudaDeviceProp& prop);
 cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg);
 cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params);
 // ... and of the single-structure kernels the differentiable rollout drives.
@@ -44,6 +48,8 @@ swb_status decode_status(const int status[2], std::string& message);
 struct StructureImpl {
     OwnedDefinition def;
     bool cluster_mode = false;
+    // the momentum guard of free structures applies (soft_body.cpp:1192-1202)
+    bool momentum_guard = false;
     Schedule sched;            // grid schedule (cluster_mode == false)
     ClusterSchedule csched;    // cluster schedule (cluster_mode == true)
     std::vector<uint32_t> slot_of_node, node_of_slot;

@@ -110,6 +110,54 @@ def test_full_wing_one_step_parity(cuda_device, options):
         assert dev.schedule_report().cluster_ctas == 16
 
 
+@pytest.mark.parametrize("case,ctas", [("patch", 1), ("patch", 4), ("patch", 16), ("wing without pilot", 4)])
+def test_free_structure_momentum_guard_parity(cuda_device, case, ctas):
+    """Structures with no fixed node and no suspension (a patch with no pin,
+    a wing without its pilot): the reference restores the predicted linear
+    and angular momentum after every substep (soft_body.cpp:152-190,
+    1192-1202).  The correction changes velocities only, so velocities and
+    the momentum are compared as well as positions.  Tolerances: a velocity
+    is a position difference over dt, so the per-step position bound (1e-5
+    of the largest coordinate) over dt; the linear and angular momentum of
+    the structure within 1e-5 relative (the guard sets both to the predicted
+    state's, which FP32 and FP64 compute alike)."""
+    d = sw.generate_patch(pin_top_corners=0) if case == "patch" else \
+        sw.generate_wing(cells=8, chordwise=16, spanwise_per_cell=2, rib_layers=3, pilot=0)
+    options = sw.SolverOptions(cluster_ctas=ctas)
+    dev = sw.Structure(d, options)
+    orc = O.PortStructure(dev.oracle_definition())
+    st = step_settings()
+    mass = d.nodes()["mass"].astype(np.float64)
+
+    def momenta(states):
+        x, v = states[:, 0, :], states[:, 2, :]
+        p = (mass[:, None] * v).sum(axis=0)
+        com = (mass[:, None] * x).sum(axis=0) / mass.sum()
+        L = (mass[:, None] * np.cross(x - com, v)).sum(axis=0)
+        return p, L
+
+    for _ in range(6):
+        sync_oracle_to_device(dev, orc)
+        dev.step(st, diagnostics=False)
+        orc.step(st)
+        a, b = dev.node_states(), orc.node_states()
+        assert rel_error(a, b) <= REL_TOL
+        scale = max(1.0, float(np.abs(b[:, 0, :]).max()))
+        assert np.abs(a[:, 2, :] - b[:, 2, :]).max() <= REL_TOL * scale / st.time_step
+        (pa, La), (pb, Lb) = momenta(a), momenta(b)
+        assert np.abs(pa - pb).max() <= 1e-5 * max(1.0, np.abs(pb).max())
+        assert np.abs(La - Lb).max() <= 1e-5 * max(1.0, np.abs(Lb).max())
+
+
+def test_free_structures_are_refused_where_the_guard_is_not_built(cuda_device):
+    d = sw.generate_patch(pin_top_corners=0)
+    s = sw.Structure(d)
+    with pytest.raises(sw.Unsupported):
+        sw.Rollout(s, 4)
+    with pytest.raises(sw.Unsupported):
+        sw.Structure(d, sw.SolverOptions(flags=sw.abi.OPT_GRID))
+
+
 def test_patch_600_steps_settled_shape(cuda_device):
     d = sw.generate_patch()
     dev = sw.Structure(d)
