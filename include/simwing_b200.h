@@ -673,7 +673,11 @@ typedef struct swb_patch_params {
     double jitter;            /* std-dev metres of N(0, jitter) (1e-3)    */
     uint64_t seed;
     uint32_t pin_top_corners; /* 1 = two top corners fixed                */
-    uint32_t reserved;
+    uint32_t membranes;       /* 0 = none; 1 = one membrane element per
+                                 triangle (chart = the unjittered sheet
+                                 coordinates), linear orthotropic
+                                 material; 2 = the same with pre-tension,
+                                 damping and compression softening        */
 } swb_patch_params;
 
 typedef struct swb_wing_params {

@@ -150,7 +150,10 @@ class PortStructure(_Base):
         return port_library()
 
     def step(self, settings):
+        """One structure step; returns the diagnostics after it (as the
+        reference adapter's step does)."""
         self._check(port_library().swo_step(self._h, C.byref(settings)))
+        return self.diagnostics()
 
     def write_node_states(self, states):
         s = np.ascontiguousarray(states, dtype=np.float64)

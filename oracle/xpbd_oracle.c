@@ -17,6 +17,13 @@
  *   evaluate_dihedral  evaluateDihedral                  soft_body.cpp:1648-1711
  *   solve_dihedral     solveDihedralConstraint           soft_body.cpp:1754-1792
  *   measure/restore_momentum                             soft_body.cpp:119-190
+ *   membrane_setup     addMembraneElements               soft_body.cpp:664-690
+ *   membrane_strain    evaluateMembraneElement (strain)  soft_body.cpp:204-270
+ *   solve_membrane     membraneElementCorrections +
+ *                      solveMembraneElement              soft_body.cpp:1822-1929
+ *   membrane_residual  updateMembraneSolverDiagnostics   soft_body.cpp:2366-2404
+ *   material forms     complianceMatrix, effectiveMembraneStiffness,
+ *                      checkedInverse (2x2, sym 3x3)     membrane.cpp:131-296
  *   payload_*          rigid payload                     suspension.cpp:1018-1102
  *   project_line       projectUnilateralLine             suspension.cpp:1104-1163
  *   begin_substep      SuspensionSystem::beginSubstep    suspension.cpp:2072-2182
@@ -24,9 +31,11 @@
  *   certify/velocity/damping/finish                      suspension.cpp:2324-2610
  *   swo_diagnostics    Structure::diagnostics            structure.cpp:833-959
  *
- * Not restated (the functions return SWB_UNSUPPORTED): membranes, contact,
- * load-path cable sweep pairs, suspension controls and ground modes other
- * than Free (the Structure adapter always builds Free, structure.cpp:550).
+ * Not restated (the functions return SWB_UNSUPPORTED): contact, load-path
+ * cable sweep pairs, suspension controls and ground modes other than Free
+ * (the Structure adapter always builds Free, structure.cpp:550), and the
+ * equilibrated Cholesky fallback of a symmetric solve whose explicit inverse
+ * is rejected (membrane.cpp:247-256).
  */
 #include "simwing_b200.h"
 
@@ -243,6 +252,16 @@ typedef struct {
     uint64_t a, b, c, d;
     double rest, compliance, lambda;
 } Dihedral;
+typedef struct { double xx, yy, zz, xy, xz, yz; } S3;
+typedef struct {
+    uint64_t a, b, c;                /* the element's triangle corners      */
+    double inv00, inv01, inv10, inv11; /* inverse reference (chart) matrix  */
+    double area;                     /* reference area                      */
+    S3 stiffness, compliance;        /* material stiffness and its inverse  */
+    double warp_pre, weft_pre, damping_time, compression_ratio;
+    V3 multiplier;
+    double residual;                 /* normalizedResidual of the last substep */
+} Membrane;
 typedef struct {
     int from_node, to_node;      /* node index or -1                     */
     int from_point, to_point;    /* hang-point index or -1               */
@@ -252,7 +271,8 @@ typedef struct {
 } Segment;
 
 typedef struct swo_structure {
-    uint64_t n, t, m, h;
+    uint64_t n, t, m, h, nm;
+    Membrane* mem;
     Node* nodes;
     uint64_t (*tri)[3];
     double* pressure;
@@ -275,6 +295,188 @@ typedef struct swo_structure {
     V3 line_force, line_moment;
 } swo_structure;
 
+/* ---------------- membranes (soft_body.cpp, membrane.cpp) ---------------- */
+static const double kEpsilon = 2.220446049250313080847e-16;
+
+/* checkedInverse(Matrix2) (membrane.cpp:131-151): m = {m00, m01, m10, m11} */
+static int inverse2(const double m[4], double out[4]) {
+    for (int i = 0; i < 4; ++i)
+        if (!isfinite(m[i])) return 0;
+    double scale = fabs(m[0]);
+    for (int i = 1; i < 4; ++i) scale = fabs(m[i]) > scale ? fabs(m[i]) : scale;
+    const double det = m[0] * m[3] - m[1] * m[2];
+    const double tol = 64.0 * kEpsilon * scale * scale;
+    if (!(scale > 0.0) || !isfinite(det) || fabs(det) <= tol) return 0;
+    const double id = 1.0 / det;
+    out[0] = m[3] * id; out[1] = -m[1] * id; out[2] = -m[2] * id; out[3] = m[0] * id;
+    return 1;
+}
+/* checkedInverse(SymmetricMatrix3) (membrane.cpp:208-235) */
+static int inverse_s3(const S3* m, S3* out) {
+    const double e[6] = {m->xx, m->yy, m->zz, m->xy, m->xz, m->yz};
+    double scale = 0.0;
+    for (int i = 0; i < 6; ++i) {
+        if (!isfinite(e[i])) return 0;
+        scale = fabs(e[i]) > scale ? fabs(e[i]) : scale;
+    }
+    const double det = m->xx * (m->yy * m->zz - m->yz * m->yz) -
+                       m->xy * (m->xy * m->zz - m->yz * m->xz) +
+                       m->xz * (m->xy * m->yz - m->yy * m->xz);
+    const double tol = 128.0 * kEpsilon * scale * scale * scale;
+    if (!(scale > 0.0) || !isfinite(det) || fabs(det) <= tol) return 0;
+    const double id = 1.0 / det;
+    out->xx = (m->yy * m->zz - m->yz * m->yz) * id;
+    out->yy = (m->xx * m->zz - m->xz * m->xz) * id;
+    out->zz = (m->xx * m->yy - m->xy * m->xy) * id;
+    out->xy = (m->xz * m->yz - m->xy * m->zz) * id;
+    out->xz = (m->xy * m->yz - m->xz * m->yy) * id;
+    out->yz = (m->xy * m->xz - m->xx * m->yz) * id;
+    return 1;
+}
+static V3 s3v(const S3* m, V3 v) {
+    return v3(m->xx * v.x + m->xy * v.y + m->xz * v.z,
+              m->xy * v.x + m->yy * v.y + m->yz * v.z,
+              m->xz * v.x + m->yz * v.y + m->zz * v.z);
+}
+static S3 s3scale(double s, const S3* m) {
+    S3 r = {s * m->xx, s * m->yy, s * m->zz, s * m->xy, s * m->xz, s * m->yz};
+    return r;
+}
+static S3 s3add(const S3* a, const S3* b) {
+    S3 r = {a->xx + b->xx, a->yy + b->yy, a->zz + b->zz, a->xy + b->xy, a->xz + b->xz, a->yz + b->yz};
+    return r;
+}
+
+/* addMembraneElements (soft_body.cpp:664-690) with the material's
+ * stiffnessMatrix / complianceMatrix (membrane.cpp:259-271) */
+static int membrane_setup(const swb_membrane_def* d, const swb_triangle_def* tris, Membrane* e) {
+    const swb_triangle_def* t = &tris[d->triangle];
+    e->a = t->nodes[0]; e->b = t->nodes[1]; e->c = t->nodes[2];
+    const double e1x = d->chart[1][0] - d->chart[0][0], e1y = d->chart[1][1] - d->chart[0][1];
+    const double e2x = d->chart[2][0] - d->chart[0][0], e2y = d->chart[2][1] - d->chart[0][1];
+    const double ref[4] = {e1x, e2x, e1y, e2y};
+    double inv[4];
+    e->area = 0.5 * (ref[0] * ref[3] - ref[1] * ref[2]);
+    if (!inverse2(ref, inv)) return 0;
+    e->inv00 = inv[0]; e->inv01 = inv[1]; e->inv10 = inv[2]; e->inv11 = inv[3];
+    const swb_membrane_material* m = &d->material;
+    S3 k = {m->warp_stiffness, m->weft_stiffness, m->shear_stiffness, m->coupling_stiffness, 0.0, 0.0};
+    e->stiffness = k;
+    if (!inverse_s3(&k, &e->compliance)) return 0;
+    e->warp_pre = m->warp_pretension;
+    e->weft_pre = m->weft_pretension;
+    e->damping_time = m->damping_seconds;
+    e->compression_ratio = m->compression_stiffness_ratio;
+    return 1;
+}
+
+/* effectiveMembraneStiffness (membrane.cpp:273-296) */
+static S3 effective_stiffness(const Membrane* e, V3 strain) {
+    if (e->compression_ratio == 1.0) return e->stiffness;
+    const double retained = sqrt(e->compression_ratio);
+    const double ws = strain.x < 0.0 ? retained : 1.0;
+    const double fs = strain.y < 0.0 ? retained : 1.0;
+    const double ss = sqrt(ws * fs);
+    const S3* k = &e->stiffness;
+    S3 r = {k->xx * ws * ws, k->yy * fs * fs, k->zz * ss * ss, k->xy * ws * fs, k->xz * ws * ss, k->yz * fs * ss};
+    return r;
+}
+
+/* evaluateMembraneElement, strain and its gradients (soft_body.cpp:204-270):
+ * g[component][corner] */
+static V3 membrane_strain(const Node* nodes, const Membrane* e, V3 g[3][3]) {
+    const V3 pa = nodes[e->a].x, pb = nodes[e->b].x, pc = nodes[e->c].x;
+    const V3 e1 = sub(pb, pa), e2 = sub(pc, pa);
+    const V3 warp = add(smul(e->inv00, e1), smul(e->inv10, e2));
+    const V3 weft = add(smul(e->inv01, e1), smul(e->inv11, e2));
+    const V3 strain = v3(0.5 * (dot(warp, warp) - 1.0) + e->warp_pre,
+                         0.5 * (dot(weft, weft) - 1.0) + e->weft_pre, dot(warp, weft));
+    const V3 zero = v3(0, 0, 0);
+    const V3 by_warp[3] = {warp, zero, weft};
+    const V3 by_weft[3] = {zero, weft, warp};
+    for (int c = 0; c < 3; ++c) {
+        const V3 first = add(smul(e->inv00, by_warp[c]), smul(e->inv01, by_weft[c]));
+        const V3 second = add(smul(e->inv10, by_warp[c]), smul(e->inv11, by_weft[c]));
+        g[c][0] = neg(add(first, second));
+        g[c][1] = first;
+        g[c][2] = second;
+    }
+    return strain;
+}
+
+static int checked_solve(const S3* m, V3 rhs, V3* out);
+
+/* membraneElementCorrections + solveMembraneElement (soft_body.cpp:1822-1929) */
+static int solve_membrane(swo_structure* s, Membrane* e, double dt) {
+    V3 g[3][3];
+    const V3 strain = membrane_strain(s->nodes, e, g);
+    const uint64_t idx[3] = {e->a, e->b, e->c};
+    const double area_scale = sqrt(e->area);
+    V3 J[3][3];
+    for (int c = 0; c < 3; ++c)
+        for (int k = 0; k < 3; ++k) J[c][k] = mul(g[c][k], area_scale);
+    S3 M = {0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 3; ++k) {
+        const double w = s->nodes[idx[k]].w;
+        M.xx += w * dot(J[0][k], J[0][k]);
+        M.yy += w * dot(J[1][k], J[1][k]);
+        M.zz += w * dot(J[2][k], J[2][k]);
+        M.xy += w * dot(J[0][k], J[1][k]);
+        M.xz += w * dot(J[0][k], J[2][k]);
+        M.yz += w * dot(J[1][k], J[2][k]);
+    }
+    V3 damping = v3(0, 0, 0);
+    for (int k = 0; k < 3; ++k) {
+        const V3 disp = sub(s->nodes[idx[k]].x, s->nodes[idx[k]].prev);
+        damping.x += dot(J[0][k], disp);
+        damping.y += dot(J[1][k], disp);
+        damping.z += dot(J[2][k], disp);
+    }
+    const double inv_dt2 = 1.0 / (dt * dt);
+    S3 compliance = e->compliance;
+    if (!(e->compression_ratio == 1.0)) {
+        const S3 k = effective_stiffness(e, strain);
+        if (!inverse_s3(&k, &compliance)) return 0;
+    }
+    const S3 alpha = s3scale(inv_dt2, &compliance);
+    const double gamma = e->damping_time / dt;
+    const S3 Ms = s3scale(1.0 + gamma, &M);
+    const S3 system = s3add(&Ms, &alpha);
+    const V3 value = smul(area_scale, strain);
+    const V3 rhs = sub(sub(neg(value), s3v(&alpha, e->multiplier)), smul(gamma, damping));
+    if (!finite3(rhs)) return 0;
+    V3 dl;
+    if (!checked_solve(&system, rhs, &dl)) return 0;
+    V3 corr[3];
+    for (int k = 0; k < 3; ++k) {
+        const V3 c = add(add(mul(J[0][k], dl.x), mul(J[1][k], dl.y)), mul(J[2][k], dl.z));
+        corr[k] = smul(s->nodes[idx[k]].w, c);
+    }
+    e->multiplier = add(e->multiplier, dl);
+    for (int k = 0; k < 3; ++k) s->nodes[idx[k]].x = add(s->nodes[idx[k]].x, corr[k]);
+    return 1;
+}
+
+/* updateMembraneSolverDiagnostics: the normalized residual (soft_body.cpp:2366-2404) */
+static void membrane_residual(swo_structure* s, Membrane* e, double dt) {
+    V3 g[3][3];
+    const V3 strain = membrane_strain(s->nodes, e, g);
+    const uint64_t idx[3] = {e->a, e->b, e->c};
+    const double area_scale = sqrt(e->area);
+    const double inv_dt2 = 1.0 / (dt * dt);
+    const S3 alpha = s3scale(inv_dt2, &e->compliance);
+    const double gamma = e->damping_time / dt;
+    V3 damping = v3(0, 0, 0);
+    for (int k = 0; k < 3; ++k) {
+        const V3 disp = sub(s->nodes[idx[k]].x, s->nodes[idx[k]].prev);
+        damping.x += area_scale * dot(g[0][k], disp);
+        damping.y += area_scale * dot(g[1][k], disp);
+        damping.z += area_scale * dot(g[2][k], disp);
+    }
+    const V3 r = add(add(smul(area_scale, strain), s3v(&alpha, e->multiplier)), smul(gamma, damping));
+    e->residual = len(r) / area_scale;
+}
+
 static int cmp_u64str(uint64_t a, uint64_t b) {
     char sa[32], sb[32];
     snprintf(sa, sizeof sa, "%llu", (unsigned long long)a);
@@ -285,13 +487,13 @@ static int cmp_u64str(uint64_t a, uint64_t b) {
 void swo_destroy(swo_structure* s) {
     if (!s) return;
     free(s->nodes); free(s->tri); free(s->pressure); free(s->dist);
-    free(s->dih); free(s->pending); free(s->seg); free(s->hang_local);
+    free(s->dih); free(s->pending); free(s->seg); free(s->hang_local); free(s->mem);
     free(s);
 }
 
 swb_status swo_create(const swb_structure_definition* d, swo_structure** out) {
-    if (d->membrane_count || d->fabric_self_contact)
-        return fail(SWB_UNSUPPORTED, "oracle port: membranes/contact not restated");
+    if (d->fabric_self_contact)
+        return fail(SWB_UNSUPPORTED, "oracle port: contact not restated");
     swo_structure* s = calloc(1, sizeof *s);
     s->n = d->node_count; s->t = d->triangle_count;
     s->m = d->constraint_count; s->h = d->dihedral_count;
@@ -321,6 +523,13 @@ swb_status swo_create(const swb_structure_definition* d, swo_structure** out) {
         s->dist[i].compliance =
             c->kind == SWB_CONSTRAINT_SEAM_STITCH ? 0.0 : c->compliance;
     }
+    s->nm = d->membrane_count;
+    s->mem = calloc(s->nm ? s->nm : 1, sizeof(Membrane));
+    for (uint64_t i = 0; i < s->nm; ++i)
+        if (!membrane_setup(&d->membranes[i], d->triangles, &s->mem[i])) {
+            swo_destroy(s);
+            return fail(SWB_INVALID_ARGUMENT, "membrane chart or material is singular");
+        }
     for (uint64_t i = 0; i < s->h; ++i) {
         const swb_dihedral_def* h = &d->dihedrals[i];
         s->dih[i].a = h->nodes[0]; s->dih[i].b = h->nodes[1];
@@ -575,7 +784,6 @@ static Momentum measure_momentum(const swo_structure* s) {
     }
     return r;
 }
-typedef struct { double xx, yy, zz, xy, xz, yz; } S3;
 static int spd(const S3* m) {
     if (!isfinite(m->xx) || !isfinite(m->yy) || !isfinite(m->zz) ||
         !isfinite(m->xy) || !isfinite(m->xz) || !isfinite(m->yz) ||
@@ -863,6 +1071,7 @@ typedef struct {
     Distance* dist;
     Dihedral* dih;
     Segment* seg;
+    Membrane* mem;
     Payload payload, previous_payload;
 } Saved;
 
@@ -882,16 +1091,23 @@ static swb_status substep(swo_structure* s, double dt, const swb_step_settings* 
     }
     const double damping = exp(-st->velocity_damping * dt);
     predict(s, dt, g, damping, fromabi(st->damping_reference_velocity));
-    int preserve = !s->has_suspension && s->h > 0;
+    int preserve = !s->has_suspension && (s->h > 0 || s->nm > 0);
     for (uint64_t i = 0; preserve && i < s->n; ++i)
         if (!(s->nodes[i].w > 0.0)) preserve = 0;
     Momentum predicted; memset(&predicted, 0, sizeof predicted);
     if (preserve) predicted = measure_momentum(s);
     for (uint64_t i = 0; i < s->m; ++i) s->dist[i].lambda = 0.0;
+    for (uint64_t i = 0; i < s->nm; ++i) {
+        s->mem[i].multiplier = v3(0, 0, 0);
+        s->mem[i].residual = 0.0;
+    }
     for (uint64_t i = 0; i < s->h; ++i) s->dih[i].lambda = 0.0;
     const double inv_dt2 = 1.0 / (dt * dt);
     for (int it = 0; it < st->constraint_iterations; ++it) {
         for (uint64_t i = 0; i < s->m; ++i) project_distance(s, &s->dist[i], inv_dt2);
+        for (uint64_t i = 0; i < s->nm; ++i)
+            if (!solve_membrane(s, &s->mem[i], dt))
+                return fail(SWB_INVALID_ARGUMENT, "membrane system is singular or its right-hand side not finite");
         for (uint64_t i = 0; i < s->h; ++i) solve_dihedral(s, &s->dih[i], inv_dt2);
         if (s->has_suspension) {
             swb_status r = line_iteration(s, dt);
@@ -902,6 +1118,7 @@ static swb_status substep(swo_structure* s, double dt, const swb_step_settings* 
         for (uint64_t i = 0; i < s->m; ++i)
             if (s->dist[i].kind == SWB_CONSTRAINT_SEAM_STITCH)
                 project_distance(s, &s->dist[i], inv_dt2);
+    for (uint64_t i = 0; i < s->nm; ++i) membrane_residual(s, &s->mem[i], dt);
     finalize(s, dt);
     if (preserve && !restore_momentum(s, &predicted))
         return fail(SWB_UNSUPPORTED, "ill-conditioned momentum solve not restated");
@@ -931,6 +1148,8 @@ swb_status swo_step(swo_structure* s, const swb_step_settings* st) {
     memcpy(sv.nodes, s->nodes, s->n * sizeof(Node));
     sv.seg = malloc((s->nseg ? s->nseg : 1) * sizeof(Segment));
     if (s->nseg) memcpy(sv.seg, s->seg, s->nseg * sizeof(Segment));
+    sv.mem = malloc((s->nm ? s->nm : 1) * sizeof(Membrane));
+    if (s->nm) memcpy(sv.mem, s->mem, s->nm * sizeof(Membrane));
     sv.payload = s->payload;
     sv.previous_payload = s->previous_payload;
     const double dt = st->time_step / st->substeps;
@@ -942,6 +1161,7 @@ swb_status swo_step(swo_structure* s, const swb_step_settings* st) {
     if (status != SWB_OK) {
         memcpy(s->nodes, sv.nodes, s->n * sizeof(Node));
         if (s->nseg) memcpy(s->seg, sv.seg, s->nseg * sizeof(Segment));
+        if (s->nm) memcpy(s->mem, sv.mem, s->nm * sizeof(Membrane));
         s->payload = sv.payload;
         s->previous_payload = sv.previous_payload;
     } else {
@@ -957,6 +1177,7 @@ swb_status swo_step(swo_structure* s, const swb_step_settings* st) {
     }
     free(sv.nodes);
     free(sv.seg);
+    free(sv.mem);
     return status;
 }
 
@@ -1020,6 +1241,26 @@ swb_status swo_diagnostics(const swo_structure* s, swb_diagnostics* o) {
     }
     o->maximum_distance_error = maxd;
     o->maximum_cable_extension = maxc;
+    /* membrane strain at the current positions and the last substep's
+     * residual (structure.cpp:924-939, membrane diagnostics soft_body.cpp:204-270) */
+    o->membrane_count = s->nm;
+    double max_strain = 0.0, max_residual = 0.0;
+    for (uint64_t i = 0; i < s->nm; ++i) {
+        const Membrane* e = &s->mem[i];
+        V3 g[3][3];
+        const V3 strain = membrane_strain(s->nodes, e, g);
+        const S3 k = effective_stiffness(e, strain);
+        const V3 resultant = s3v(&k, strain);
+        const double energy = 0.5 * e->area * dot(strain, resultant);
+        double a = fabs(strain.x);
+        a = fabs(strain.y) > a ? fabs(strain.y) : a;
+        a = fabs(strain.z) > a ? fabs(strain.z) : a;
+        max_strain = a > max_strain ? a : max_strain;
+        max_residual = fabs(e->residual) > max_residual ? fabs(e->residual) : max_residual;
+        fin = fin && isfinite(energy) && isfinite(e->residual);
+    }
+    o->maximum_absolute_membrane_strain = max_strain;
+    o->maximum_membrane_residual = max_residual;
     V3 pend = v3(0, 0, 0);
     for (uint64_t i = 0; i < s->n; ++i) pend = add(pend, s->pending[i]);
     o->pending_external_force = toabi(pend);

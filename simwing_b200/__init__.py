@@ -192,13 +192,19 @@ class Definition:
         return out
 
 
-def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), suspension=None) -> Definition:
+def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), suspension=None,
+                           membranes=()) -> Definition:
     """Builds an owned Definition from plain Python records.
 
     nodes:       [(x, y, z, mass, fixed), ...]
     triangles:   [(a, b, c[, pressure]), ...]
     constraints: [(kind, a, b, rest, compliance), ...]
     dihedrals:   [(a, b, c, d, rest_angle, compliance), ...]
+    membranes:   [(triangle, ((u0, v0), (u1, v1), (u2, v2)), material[, role]), ...]
+                 material = dict of MembraneMaterial fields (warp_stiffness,
+                 weft_stiffness, coupling_stiffness, shear_stiffness,
+                 warp_pretension, weft_pretension, damping_seconds,
+                 compression_stiffness_ratio; the last defaults to 1)
     suspension:  dict with pilot_mass, pilot_com_world, pilot_inertia,
                  attachments [(id, node)], harness [(id, (x, y, z))],
                  segments [(id, (kind, id), (kind, id), rest, stiffness,
@@ -225,7 +231,19 @@ def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), su
     view.triangle_count, view.triangles = len(triangles), t
     view.constraint_count, view.constraints = len(constraints), c
     view.dihedral_count, view.dihedrals = len(dihedrals), h
-    keep = [n, t, c, h]
+    mb = (abi.MembraneDef * max(len(membranes), 1))()
+    for i, rec in enumerate(membranes):
+        tri, chart, material = rec[0], rec[1], rec[2]
+        mb[i].triangle = int(tri)
+        for k in range(3):
+            mb[i].chart[k][0], mb[i].chart[k][1] = float(chart[k][0]), float(chart[k][1])
+        fields = {"compression_stiffness_ratio": 1.0}
+        fields.update(material)
+        for name, value in fields.items():
+            setattr(mb[i].material, name, float(value))
+        mb[i].role = int(rec[3]) if len(rec) > 3 else abi.ROLE_BULK
+    view.membrane_count, view.membranes = len(membranes), mb
+    keep = [n, t, c, h, mb]
     if suspension is not None:
         s = abi.SuspensionDef()
         s.pilot_stable_id = 1

@@ -40,6 +40,9 @@ class MembraneMaterial(C.Structure):
         "warp_pretension", "weft_pretension", "damping_seconds", "compression_stiffness_ratio")]
 
 
+ROLE_BULK, ROLE_SEAM, ROLE_REINFORCEMENT = 1, 2, 3
+
+
 class MembraneDef(C.Structure):
     _fields_ = [("triangle", C.c_uint64), ("chart", (C.c_double * 2) * 3), ("material", MembraneMaterial),
                 ("role", C.c_uint32), ("reserved", C.c_uint32)]
@@ -173,7 +176,7 @@ class PatchParams(C.Structure):
     _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("width", C.c_double), ("height", C.c_double),
                 ("areal_density", C.c_double), ("distance_compliance", C.c_double),
                 ("bend_compliance", C.c_double), ("jitter", C.c_double), ("seed", C.c_uint64),
-                ("pin_top_corners", C.c_uint32), ("reserved", C.c_uint32)]
+                ("pin_top_corners", C.c_uint32), ("membranes", C.c_uint32)]
 
 
 class WingParams(C.Structure):

@@ -206,7 +206,8 @@ void swb_default_wing_params(swb_wing_params* p) {
 // x-z plane, triangulated like SoftBody::addRectangularPatch
 // (soft_body.cpp:2622-2632), one distance constraint per unique triangle
 // edge, one dihedral per interior edge (flat rest angle), area/3 lumped
-// mass, the two top corners fixed, every coordinate jittered by N(0, jitter).
+// mass, the two top corners fixed, every coordinate jittered by N(0, jitter);
+// optionally one membrane element per triangle.
 swb_status swb_generate_patch(const swb_patch_params* p, swb_definition** out) {
     return guarded([&] {
         if (!p || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
@@ -235,6 +236,34 @@ swb_status swb_generate_patch(const swb_patch_params* p, swb_definition** out) {
                 }
             b.edge_constraints(0, def->def.triangles.size(), p->distance_compliance);
             b.dihedrals(0, def->def.triangles.size(), 0.0, p->bend_compliance);
+            if (p->membranes > 2) raise(SWB_INVALID_ARGUMENT, "invalid patch membrane option");
+            if (p->membranes) {
+                // orthotropic fabric: warp along x, weft along z (N/m)
+                swb_membrane_material m{};
+                m.warp_stiffness = 2.0e4;
+                m.weft_stiffness = 1.5e4;
+                m.coupling_stiffness = 3.0e3;
+                m.shear_stiffness = 2.0e3;
+                m.compression_stiffness_ratio = 1.0;
+                if (p->membranes == 2) {
+                    m.warp_pretension = 1.0e-3;
+                    m.weft_pretension = 5.0e-4;
+                    m.damping_seconds = 2.0e-3;
+                    m.compression_stiffness_ratio = 0.1;
+                }
+                for (uint64_t t = 0; t < def->def.triangles.size(); ++t) {
+                    swb_membrane_def md{};
+                    md.triangle = t;
+                    for (int k = 0; k < 3; ++k) {
+                        const uint64_t n = def->def.triangles[t].nodes[k];
+                        md.chart[k][0] = static_cast<double>(n % p->nx) * dx;
+                        md.chart[k][1] = static_cast<double>(n / p->nx) * dz;
+                    }
+                    md.material = m;
+                    md.role = SWB_ROLE_BULK;
+                    def->def.membranes.push_back(md);
+                }
+            }
             b.finish_masses(0.0);
             Rng rng(p->seed);
             for (auto& n : def->def.nodes) {

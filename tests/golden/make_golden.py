@@ -2,8 +2,9 @@
 
 Runs only where the reference build exists (oracle/_ref/libswref.so, made
 by `make -C oracle ref` from the reference sources).  The fixtures hold
-FP64 positions after a fixed number of steps of two small seeded
-definitions, the reference colouring of their constraint lists, and the
+FP64 positions after a fixed number of steps of three small seeded
+definitions (a cloth patch, a wing with pilot, a patch of membrane
+elements), the reference colouring of their constraint lists, and the
 reference definition fingerprints; tests compare the oracle port and the
 device solver against them without needing the reference at run time.
 
@@ -34,6 +35,7 @@ def main():
     cases = {
         "patch": (sw.generate_patch(nx=17, ny=17, seed=7), 20),
         "wing": (sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, seed=3), 5),
+        "membrane_patch": (sw.generate_patch(nx=12, ny=12, seed=9, membranes=2), 10),
     }
     out = {}
     for name, (d, steps) in cases.items():

@@ -77,10 +77,17 @@ def test_suspension_validation():
             sw.definition_from_arrays(nodes, suspension=bad).validate()
 
 
-@pytest.mark.parametrize("name", ["patch", "wing"])
+def golden_definition(name):
+    if name == "patch":
+        return sw.generate_patch(nx=17, ny=17, seed=7)
+    if name == "membrane_patch":
+        return sw.generate_patch(nx=12, ny=12, seed=9, membranes=2)
+    return sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, seed=3)
+
+
+@pytest.mark.parametrize("name", ["patch", "wing", "membrane_patch"])
 def test_fingerprint_matches_reference_golden(name):
-    d = sw.generate_patch(nx=17, ny=17, seed=7) if name == "patch" else \
-        sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, seed=3)
+    d = golden_definition(name)
     if name == "wing":
         # the reference definition has no face pressure; hash without it
         t = d.triangles()
@@ -88,10 +95,9 @@ def test_fingerprint_matches_reference_golden(name):
     assert d.fingerprint == int(GOLDEN[f"{name}_fingerprint"])
 
 
-@pytest.mark.parametrize("name", ["patch", "wing"])
+@pytest.mark.parametrize("name", ["patch", "wing", "membrane_patch"])
 def test_reference_colouring_is_bit_exact(name):
-    d = sw.generate_patch(nx=17, ny=17, seed=7) if name == "patch" else \
-        sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, seed=3)
+    d = golden_definition(name)
     order, offsets, parallel = sw.reference_colouring(d)
     np.testing.assert_array_equal(order, GOLDEN[f"{name}_colour_order"])
     np.testing.assert_array_equal(offsets, GOLDEN[f"{name}_colour_offsets"])

@@ -196,12 +196,74 @@ def test_port_matches_reference_on_permuted_definition():
     assert np.array_equal(ref.node_states(), port.node_states())
 
 
+# ---- membranes ---------------------------------------------------------------
+# material of the reference's membrane tests (softwing_material_test.cpp:30-39,
+# simwing_structure_test.cpp:271-274)
+MEMBRANE = {"warp_stiffness": 800.0, "weft_stiffness": 500.0, "coupling_stiffness": 100.0,
+            "shear_stiffness": 180.0}
+RIGHT_CHART = ((0.0, 0.0), (1.0, 0.0), (0.0, 1.0))
+
+
+@pytest.mark.parametrize("cls", checkers())
+def test_membrane_rest_chart_known_answer(cls):
+    """simwing_structure_test.cpp:256-283: one orthotropic element at its
+    rest chart, one fixed corner, 4 iterations without gravity: finite, one
+    membrane, zero strain (1e-15)."""
+    d = sw.definition_from_arrays([(0.0, 0.0, 0.0, 0.0, True), (1.0, 0.0, 0.0, 1.0, False),
+                                   (0.0, 1.0, 0.0, 1.0, False)], triangles=[(0, 1, 2)],
+                                  membranes=[(0, RIGHT_CHART, MEMBRANE)])
+    s = cls(d)
+    diag = s.step(sw.StepSettings(time_step=1 / 60, substeps=1, constraint_iterations=4, gravity=(0, 0, 0),
+                                  velocity_damping=0.0))
+    assert diag.membrane_count == 1 and diag.finite
+    assert abs(diag.maximum_absolute_membrane_strain) <= 1e-15
+
+
+@pytest.mark.parametrize("cls", checkers())
+def test_compressed_membrane_solve_known_answer(cls):
+    """softwing_material_test.cpp:74-103: an element compressed to 0.9 of its
+    chart along the warp, compression softening 0.05, damping 0.02 s;
+    dt 1/60 in 2 substeps of 4 iterations without gravity: finite positions
+    and velocities, and the strain moves towards the chart."""
+    material = dict(MEMBRANE, damping_seconds=0.02, compression_stiffness_ratio=0.05)
+    d = sw.definition_from_arrays([(0.0, 0.0, 0.0, 0.0, True), (0.9, 0.0, 0.0, 1.0, False),
+                                   (0.0, 1.0, 0.0, 1.0, False)], triangles=[(0, 1, 2)],
+                                  membranes=[(0, RIGHT_CHART, material)])
+    s = cls(d)
+    diag = s.step(sw.StepSettings(time_step=1 / 60, substeps=2, constraint_iterations=4, gravity=(0, 0, 0),
+                                  velocity_damping=0.0))
+    st = s.node_states()
+    assert diag.finite and np.isfinite(st).all()
+    # initial warp strain 0.5 (0.81 - 1) = -0.095
+    assert 0.0 < diag.maximum_absolute_membrane_strain < 0.095
+
+
+@needs_ref
+@pytest.mark.parametrize("option,pinned", [(1, 1), (2, 1), (2, 0)])
+def test_port_matches_reference_bitwise_on_membrane_patch(option, pinned):
+    """Membrane elements on every triangle (linear material; pre-tension,
+    damping and compression softening), with the patch pinned and free (the
+    free patch also runs the momentum guard): node states and membrane
+    diagnostics bit for bit."""
+    d = sw.generate_patch(nx=12, ny=12, membranes=option, pin_top_corners=pinned)
+    ref, port = O.RefStructure(d), O.PortStructure(d)
+    st = step_settings(iterations=12)
+    for _ in range(4):
+        dr = ref.step(st)
+        dp = port.step(st)
+    assert np.array_equal(ref.node_states(), port.node_states())
+    assert dr.membrane_count == dp.membrane_count == d.view.triangle_count
+    assert dr.maximum_absolute_membrane_strain == dp.maximum_absolute_membrane_strain
+    assert dr.maximum_membrane_residual == dp.maximum_membrane_residual
+    assert dr.maximum_membrane_residual > 0.0
+
+
 def test_golden_trajectories():
     """Committed FP64 fixtures produced by the reference build
     (tests/golden/make_golden.py)."""
     path = os.path.join(GOLDEN, "trajectories.npz")
     g = np.load(path)
-    for name in ("patch", "wing"):
+    for name in ("patch", "wing", "membrane_patch"):
         d = _golden_definition(name)
         port = O.PortStructure(d)
         st = step_settings()
@@ -213,4 +275,6 @@ def test_golden_trajectories():
 def _golden_definition(name):
     if name == "patch":
         return sw.generate_patch(nx=17, ny=17, seed=7)
+    if name == "membrane_patch":
+        return sw.generate_patch(nx=12, ny=12, seed=9, membranes=2)
     return sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, seed=3)
