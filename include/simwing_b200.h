@@ -476,7 +476,8 @@ swb_status swb_structure_sweep_order(const swb_structure* structure,
                                      uint64_t count);
 enum {
     SWB_SWEEP_DISTANCE = 0,
-    SWB_SWEEP_DIHEDRAL = 1
+    SWB_SWEEP_DIHEDRAL = 1,
+    SWB_SWEEP_MEMBRANE = 2
 };
 
 /* Shape of the device schedule for reporting. */
@@ -717,6 +718,10 @@ swb_status swb_definition_copy(const swb_structure_definition* source,
 swb_status swb_definition_permute(swb_definition* definition,
                                   const uint64_t* constraint_order,
                                   const uint64_t* dihedral_order);
+/* Reorders the membrane list (an order from swb_structure_sweep_order with
+ * SWB_SWEEP_MEMBRANE). */
+swb_status swb_definition_permute_membranes(swb_definition* definition,
+                                            const uint64_t* membrane_order);
 /* Multiplies the rest length of constraint `index` (any kind) or, when
  * index >= constraint_count, of suspension segment index - constraint_count. */
 swb_status swb_definition_scale_rest(swb_definition* definition,

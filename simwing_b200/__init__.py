@@ -130,12 +130,15 @@ class Definition:
         _check(self._lib.swb_definition_copy(self.pointer, C.byref(out)))
         return Definition(out.value)
 
-    def permuted(self, constraint_order=None, dihedral_order=None) -> "Definition":
+    def permuted(self, constraint_order=None, dihedral_order=None, membrane_order=None) -> "Definition":
         d = self.copy()
         co = None if constraint_order is None else np.ascontiguousarray(constraint_order, dtype=np.uint64)
         ho = None if dihedral_order is None else np.ascontiguousarray(dihedral_order, dtype=np.uint64)
         _check(self._lib.swb_definition_permute(
             d._h, None if co is None else co.ctypes.data, None if ho is None else ho.ctypes.data))
+        if membrane_order is not None:
+            mo = np.ascontiguousarray(membrane_order, dtype=np.uint64)
+            _check(self._lib.swb_definition_permute_membranes(d._h, mo.ctypes.data))
         return d
 
     def scale_rest(self, index: int, factor: float) -> None:
@@ -525,7 +528,8 @@ class Structure:
 
     def sweep_order(self, which: int) -> np.ndarray:
         v = self._definition.view
-        n = v.constraint_count if which == abi.SWEEP_DISTANCE else v.dihedral_count
+        n = v.constraint_count if which == abi.SWEEP_DISTANCE else (
+            v.dihedral_count if which == abi.SWEEP_DIHEDRAL else v.membrane_count)
         out = np.zeros(max(n, 1), dtype=np.uint64)
         _check(self._lib.swb_structure_sweep_order(self._h, which, out.ctypes.data, n))
         return out[:n]
@@ -535,7 +539,9 @@ class Structure:
         sweep order: the reference serial solver run on it performs exactly
         the device's Gauss-Seidel sweep."""
         return self._definition.permuted(self.sweep_order(abi.SWEEP_DISTANCE),
-                                         self.sweep_order(abi.SWEEP_DIHEDRAL))
+                                         self.sweep_order(abi.SWEEP_DIHEDRAL),
+                                         self.sweep_order(abi.SWEEP_MEMBRANE) if self._definition.view.membrane_count
+                                         else None)
 
     def schedule_report(self) -> abi.ScheduleReport:
         r = abi.ScheduleReport()

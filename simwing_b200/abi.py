@@ -196,7 +196,7 @@ OK, INVALID_ARGUMENT, OUT_OF_RANGE, SUSPENSION_ERROR, CONTACT_ERROR, NON_FINITE,
 DISTANCE, CABLE, SUSPENSION_TIE, SEAM_STITCH = 1, 2, 3, 4
 OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID, OPT_SPLIT_STAGES = 1, 2, 4, 8
 BATCH_AUTOTUNE = 1 << 8
-SWEEP_DISTANCE, SWEEP_DIHEDRAL = 0, 1
+SWEEP_DISTANCE, SWEEP_DIHEDRAL, SWEEP_MEMBRANE = 0, 1, 2
 
 P = C.POINTER
 _PROTOTYPES = {
@@ -257,6 +257,7 @@ _PROTOTYPES = {
     "swb_generate_wing": (C.c_int, [P(WingParams), P(C.c_void_p)]),
     "swb_definition_copy": (C.c_int, [P(StructureDefinition), P(C.c_void_p)]),
     "swb_definition_permute": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "swb_definition_permute_membranes": (C.c_int, [C.c_void_p, C.c_void_p]),
     "swb_definition_scale_rest": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double]),
     "swb_definition_view": (P(StructureDefinition), [C.c_void_p]),
     "swb_definition_destroy": (None, [C.c_void_p]),

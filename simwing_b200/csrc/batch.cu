@@ -52,7 +52,8 @@ struct Packing {
     int threads = 0;
     int max_stages = 0;
     uint32_t smem_v = 0, smem_offsets = 0, smem = 0;
-    std::vector<uint32_t> lambda_offset[2];  // per structure
+    std::vector<uint32_t> lambda_offset[3];  // per structure and kind
+    bool membranes = false;                  // a structure carries membrane elements
 };
 
 int initial_ranks(uint64_t nodes, int target, int cluster) {
@@ -145,7 +146,7 @@ void pack(Packing& P, int cluster, int threads_opt, size_t smem_limit) {
         int stages = 0, seam = 0, susp = 0, guard = 0;
         for (size_t i : content[c]) {
             const StructureImpl& m = P.members[i]->s;
-            stages = std::max(stages, m.csched.kinds[0].stages + m.csched.kinds[1].stages);
+            stages = std::max(stages, total_stages(m.csched));
             seam = std::max(seam, m.csched.seam_stages);
             susp |= m.def.has_suspension ? 1 : 0;
             guard |= m.momentum_guard ? 1 : 0;
@@ -179,19 +180,20 @@ void pack(Packing& P, int cluster, int threads_opt, size_t smem_limit) {
         const StructureImpl& m = P.members[i]->s;
         max_patch = std::max(max_patch, m.csched.max_patch);
         lambda_bytes = std::max(lambda_bytes, align16u(m.csched.kinds[0].max_cta_records * 4u) +
-                                                  align16u(m.csched.kinds[1].max_cta_records * 4u));
-        offset_bytes = std::max(offset_bytes,
-                                align16u((m.csched.kinds[0].stages + m.csched.kinds[1].stages + 2) * 4u));
+                                                  align16u(m.csched.kinds[1].max_cta_records * 4u) +
+                                                  align16u(m.csched.kinds[2].max_cta_records * 12u));
+        offset_bytes = std::max(offset_bytes, align16u((total_stages(m.csched) + 3) * 4u));
+        P.membranes = P.membranes || !m.def.membranes.empty();
         threads = std::max(threads, m.threads);
     }
     P.smem_v = align16u(max_patch * 16u);
     const uint32_t lambda_base = P.smem_v + align16u(max_patch * 16u);
-    P.lambda_offset[0].assign(n, 0);
-    P.lambda_offset[1].assign(n, 0);
+    for (int k = 0; k < 3; ++k) P.lambda_offset[k].assign(n, 0);
     for (size_t i = 0; i < n; ++i) {
         const StructureImpl& m = P.members[i]->s;
         P.lambda_offset[0][i] = lambda_base;
         P.lambda_offset[1][i] = lambda_base + align16u(m.csched.kinds[0].max_cta_records * 4u);
+        P.lambda_offset[2][i] = P.lambda_offset[1][i] + align16u(m.csched.kinds[1].max_cta_records * 4u);
     }
     P.smem_offsets = lambda_base + lambda_bytes;
     P.smem = P.smem_offsets + offset_bytes;
@@ -281,6 +283,8 @@ struct BatchImpl {
                     c.recentre = m.def.has_suspension ? 1 : 0;
                     c.kind[0].smem_lambda = P.lambda_offset[0][i];
                     c.kind[1].smem_lambda = P.lambda_offset[1][i];
+                    c.kind[2].smem_lambda = P.lambda_offset[2][i];
+                    c.membrane_residual = m.d_mres[out];
                     rec[(i * 3 + b) * 3 + role] = c;
                 }
         }
@@ -301,7 +305,7 @@ struct BatchImpl {
         // process, so it is set to the device limit, never lowered
         cuda_check(packed_kernel_limits(static_cast<int>(smem_limit), cluster > 8), "batch kernel limits");
         cudaLaunchConfig_t cfg = launch_config();
-        cuda_check(packed_kernel_occupancy(&resident, cfg), "cluster occupancy");
+        cuda_check(packed_kernel_occupancy(&resident, cfg, P.membranes), "cluster occupancy");
         if (resident < 1) raise(SWB_UNSUPPORTED, "the batch's cluster shape cannot be scheduled");
         cuda_check(cudaStreamSynchronize(stream), "batch upload");
     }
@@ -351,7 +355,7 @@ struct BatchImpl {
         cudaLaunchConfig_t cfg = launch_config();
         for (int k = 0; k < launches; ++k) {
             const ClusterParams cp = params(st, k == 0 ? 0 : (k % 2 ? 1 : 2));
-            cuda_check(packed_kernel_launch(cfg, cp), "batch launch");
+            cuda_check(packed_kernel_launch(cfg, cp, P.membranes), "batch launch");
         }
     }
 
@@ -458,10 +462,10 @@ struct BatchImpl {
         cudaLaunchConfig_t cfg = launch_config();
         const ClusterParams cp = params(st, 0);
         for (int k = 0; k < warm; ++k)
-            cuda_check(packed_kernel_launch(cfg, cp), "trial launch");
+            cuda_check(packed_kernel_launch(cfg, cp, P.membranes), "trial launch");
         cuda_check(cudaEventRecord(ev0, stream), "event");
         for (int k = 0; k < timed; ++k)
-            cuda_check(packed_kernel_launch(cfg, cp), "trial launch");
+            cuda_check(packed_kernel_launch(cfg, cp, P.membranes), "trial launch");
         cuda_check(cudaEventRecord(ev1, stream), "event");
         cuda_check(cudaStreamSynchronize(stream), "trial");
         float ms = 0.0f;

@@ -14,6 +14,7 @@
 #include <cooperative_groups.h>
 
 #include "cluster_params.h"
+#include "membrane.cuh"
 #include "step_kernel.cuh"
 
 namespace swb {
@@ -186,6 +187,33 @@ __device__ bool guard_solve(const double* m, const double* rhs, double* out) {
     return true;
 }
 
+// Projects one membrane record: its three corners through the cluster
+// window like apply_record, the step-start positions (damping) from global
+// memory by slot (pbeg = the structure's patch starts).  False when the
+// element's system has no inverse (the corners are then left as they were).
+__device__ __noinline__ bool apply_membrane(const ClusterRecord& r, uint32_t me, uint32_t rank_base,
+                                            uint32_t x_base, float* lam, uint32_t first, const float4* aux,
+                                            const float4* pos_in, const uint32_t* pbeg, float inv_dt,
+                                            float inv_dt2) {
+    const uint32_t ra = r.ab & 0xffffu, rb = r.ab >> 16, rc = r.cd & 0xffffu;
+    const uint32_t pa = node_addr(ra, me, rank_base, x_base);
+    const uint32_t pb = node_addr(rb, me, rank_base, x_base);
+    const uint32_t pc = node_addr(rc, me, rank_base, x_base);
+    float4 A = ld_node(pa), B = ld_node(pb), C = ld_node(pc);
+    const MembraneConst m = load_membrane(aux, r.index);
+    float3 PA = make_float3(0.0f, 0.0f, 0.0f), PB = PA, PC = PA;
+    if (m.damping_time != 0.0f) {
+        PA = f3(__ldg(pos_in + pbeg[ra >> 12] + (ra & 0xfffu)));
+        PB = f3(__ldg(pos_in + pbeg[rb >> 12] + (rb & 0xfffu)));
+        PC = f3(__ldg(pos_in + pbeg[rc >> 12] + (rc & 0xfffu)));
+    }
+    const bool ok = project_membrane(A, B, C, PA, PB, PC, m, lam + 3 * (r.index - first), inv_dt, inv_dt2);
+    st_node(pa, A);
+    st_node(pb, B);
+    st_node(pc, C);
+    return ok;
+}
+
 // Projects one record.  Taping launches first store the record's inputs
 // (node positions and multiplier) at its index in this iteration's tape
 // blocks of `rtotal` entries.
@@ -244,7 +272,9 @@ __device__ __forceinline__ void tape_pilot(PilotTape& t, const DevPayloadState& 
 // kTape = true: one structure per cluster; the step also records the inputs
 // of every projection, line iteration and the pilot finish into p.tape for
 // the reverse sweep of the adjoint.
-template <bool kPacked, bool kTape = false>
+// kMembrane = true: the launch's structures may carry membrane elements
+// (a third record kind); without it their stage count is taken as zero.
+template <bool kPacked, bool kTape = false, bool kMembrane = false>
 __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(const __grid_constant__ ClusterParams p) {
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -253,6 +283,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     __shared__ DevPayloadDef pdef;  // suspension CTA: the payload definition, read on every line iteration
     __shared__ float4* peers[16];
     __shared__ float3 shift_s;
+    __shared__ uint32_t pbeg_s[kClusterMaxCtasDev + 1];  // the structure's patch starts
     __shared__ double mom_scratch[kMaxWarps * kMomentumFields];
     __shared__ double mom_pred[kMomentumFields], mom_cur[kMomentumFields];
     __shared__ double mom_ptot[kMomentumFields], mom_tot[kMomentumFields];
@@ -278,6 +309,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     float4* v = reinterpret_cast<float4*>(smem + p.smem_v);
     float* lam0 = reinterpret_cast<float*>(smem + I.kind[0].smem_lambda);
     float* lam1 = reinterpret_cast<float*>(smem + I.kind[1].smem_lambda);
+    float* lam2 = reinterpret_cast<float*>(smem + I.kind[2].smem_lambda);  // three per membrane record
     const uint32_t base = __ldg(I.patch_begin + me);
     const uint32_t n = __ldg(I.patch_begin + me + 1) - base;
     const bool owner = static_cast<int>(me) == I.susp_cta;
@@ -296,12 +328,13 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         if (n) bulk_load(x, I.pos_in + base, n * 16u, &bar);
     }
     // multipliers restart every substep (soft_body.cpp:1207-1218)
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < (kMembrane ? 3 : 2); ++k) {
         const uint32_t* off = I.kind[k].offsets + static_cast<size_t>(me) * (I.kind[k].stages + 1);
-        const uint32_t cnt = __ldg(off + I.kind[k].stages) - __ldg(off);
-        float* lam = k == 0 ? lam0 : lam1;
+        const uint32_t cnt = (__ldg(off + I.kind[k].stages) - __ldg(off)) * (k == 2 ? 3u : 1u);
+        float* lam = k == 0 ? lam0 : (k == 1 ? lam1 : lam2);
         for (uint32_t i = tid; i < cnt; i += blockDim.x) lam[i] = 0.0f;
     }
+    if (tid <= sctas) pbeg_s[tid] = __ldg(I.patch_begin + tid);
     // pressure gather (ascending triangle order) into v
     for (uint32_t i = tid; i < n; i += blockDim.x) {
         const uint32_t slot = base + i;
@@ -354,33 +387,54 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     cluster.sync();
 
     // ---- constraint iterations ------------------------------------------------
-    // Stages of one iteration: distance colours then dihedral colours.  Each
-    // thread prefetches its first record of the next stage before it works
-    // on the current one, so the record fetch from L2 overlaps the current
-    // stage and its cluster barrier.
-    const int S0 = I.kind[0].stages, S1 = I.kind[1].stages, S = S0 + S1;
+    // Stages of one iteration: distance colours, membrane colours, then
+    // dihedral colours.  Each thread prefetches its first record of the next
+    // stage before it works on the current one, so the record fetch from L2
+    // overlaps the current stage and its cluster barrier.
+    const int S0 = I.kind[0].stages, S1 = I.kind[1].stages, S2 = kMembrane ? I.kind[2].stages : 0,
+              S = S0 + S1 + S2;
     const int stages_c = kPacked ? slot.stages : S;                       // cluster-wide
     const bool susp_c = kPacked ? slot.suspension != 0 : I.susp_cta >= 0;  // cluster-wide
     const int seam_c = kPacked ? slot.seam_stages : I.seam_stages;         // cluster-wide
-    uint32_t* soff = reinterpret_cast<uint32_t*>(smem + p.smem_offsets);  // [S + 2]: stage starts, then ends
-    for (int i = tid; i <= S0; i += blockDim.x)
-        soff[i] = __ldg(I.kind[0].offsets + static_cast<size_t>(me) * (S0 + 1) + i);
-    for (int i = tid; i <= S1; i += blockDim.x)
-        soff[S0 + 1 + i] = __ldg(I.kind[1].offsets + static_cast<size_t>(me) * (S1 + 1) + i);
+    // this CTA's stage offsets, kind by kind: [S0 + 1] distance, [S1 + 1]
+    // dihedral, [S2 + 1] membrane
+    uint32_t* soff = reinterpret_cast<uint32_t*>(smem + p.smem_offsets);
+    for (int k = 0; k < (kMembrane ? 3 : 2); ++k) {
+        const int at = k == 0 ? 0 : (k == 1 ? S0 + 1 : S0 + S1 + 2);
+        for (int i = tid; i <= I.kind[k].stages; i += blockDim.x)
+            soff[at + i] = __ldg(I.kind[k].offsets + static_cast<size_t>(me) * (I.kind[k].stages + 1) + i);
+    }
     __syncthreads();
-    // global stage g -> (kind, [lo, hi)) with first = start of that kind's CTA list
-    auto stage_lo = [&](int g) { return g < S0 ? soff[g] : soff[S0 + 1 + (g - S0)]; };
-    auto stage_hi = [&](int g) { return g < S0 ? soff[g + 1] : soff[S0 + 2 + (g - S0)]; };
-    const uint32_t first0 = soff[0], first1 = soff[S0 + 1];
+    // global stage g -> kind, its stage within the kind, and its offsets
+    // (plain arithmetic: without membranes S2 is the constant 0 and these
+    // reduce to the two-kind forms)
+    auto kind_of = [&](int g) { return g < S0 ? 0 : (g < S0 + S2 ? 2 : 1); };
+    auto local_of = [&](int g) { return g < S0 ? g : (g < S0 + S2 ? g - S0 : g - S0 - S2); };
+    auto stage_at = [&](int g) {
+        return g < S0 ? g : (g < S0 + S2 ? S0 + S1 + 2 + (g - S0) : S0 + 1 + (g - S0 - S2));
+    };
+    auto stage_lo = [&](int g) { return soff[stage_at(g)]; };
+    auto stage_hi = [&](int g) { return soff[stage_at(g) + 1]; };
+    const uint32_t first0 = soff[0], first1 = soff[S0 + 1], first2 = kMembrane ? soff[S0 + S1 + 2] : 0u;
     // record arrays held in registers (the instance record lives in global memory)
     const uint4* rec0 = I.kind[0].rec;
     const uint4* rec1 = I.kind[1].rec;
+    const uint4* rec2 = I.kind[2].rec;
+    auto recs = [&](int k) { return k == 0 ? rec0 : (k == 1 ? rec1 : rec2); };
     auto apply = [&](const ClusterRecord& r, int kind, float* lam, uint32_t first, float4* tape, uint32_t rtotal) {
+        if constexpr (kMembrane) {
+            if (kind == 2) {
+                if (!apply_membrane(r, me, rank_base, x_base, lam, first, I.kind[2].aux, I.pos_in, pbeg_s, p.inv_dt,
+                                    p.inv_dt2))
+                    atomicOr(I.status, kStatusMembrane);
+                return;
+            }
+        }
         apply_record<kTape>(r, kind, me, rank_base, x_base, lam, first, p.inv_dt2, tape, rtotal);
     };
     ClusterRecord next;
     next.index = ~0u;
-    if (p.iterations > 0 && S > 0) next = load_record(S0 > 0 ? rec0 : rec1, stage_lo(0) + tid, stage_hi(0));
+    if (p.iterations > 0 && S > 0) next = load_record(recs(kind_of(0)), stage_lo(0) + tid, stage_hi(0));
     const uint64_t sync0 = I.kind[0].sync_mask, sync1 = I.kind[1].sync_mask;
     const int interior0 = I.kind[0].interior_stages, interior1 = I.kind[1].interior_stages;
     // line iteration beside the last two stages: neither touches a
@@ -394,14 +448,13 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     for (int it = 0; it < p.iterations; ++it) {
         for (int g = 0; g < stages_c; ++g) {
             if (!kPacked || g < S) {
-                const int kind = g < S0 ? 0 : 1;
+                const int kind = kind_of(g);
                 const ClusterRecord cur = next;
                 // prefetch the next stage (wrapping to the next iteration)
                 const int gn = g + 1 < S ? g + 1 : 0;
-                const int kn = gn < S0 ? 0 : 1;
-                next = load_record(kn ? rec1 : rec0, stage_lo(gn) + tid, stage_hi(gn));
-                const uint32_t first = kind ? first1 : first0;
-                float* lam = kind ? lam1 : lam0;
+                next = load_record(recs(kind_of(gn)), stage_lo(gn) + tid, stage_hi(gn));
+                const uint32_t first = kind == 0 ? first0 : (kind == 1 ? first1 : first2);
+                float* lam = kind == 0 ? lam0 : (kind == 1 ? lam1 : lam2);
                 float4* tape = nullptr;
                 uint32_t rtotal = 0;
                 if constexpr (kTape) {
@@ -410,7 +463,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                 }
                 if (cur.index != ~0u) apply(cur, kind, lam, first, tape, rtotal);
                 for (uint32_t i = stage_lo(g) + tid + blockDim.x; i < stage_hi(g); i += blockDim.x)
-                    apply(load_record(kind ? rec1 : rec0, i, stage_hi(g)), kind, lam, first, tape, rtotal);
+                    apply(load_record(recs(kind), i, stage_hi(g)), kind, lam, first, tape, rtotal);
             }
             if (g == line_stage) {
                 if (line_warp) {
@@ -429,11 +482,12 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             } else {
                 // split stages: a cluster barrier where the next stage may read
                 // what another CTA wrote, else a CTA barrier (after the
-                // single-CTA tail's writes to peer nodes are made visible)
-                const int kind = g < S0 ? 0 : 1;
-                const int gl = kind ? g - S0 : g;
-                const uint64_t mask = kind ? sync1 : sync0;
-                if (gl >= 64 || ((mask >> gl) & 1ull)) {
+                // single-CTA tail's writes to peer nodes are made visible);
+                // membrane stages are classic
+                const int kind = kind_of(g);
+                const int gl = local_of(g);
+                const uint64_t mask = kind == 0 ? sync0 : sync1;
+                if (kind == 2 || gl >= 64 || ((mask >> gl) & 1ull)) {
                     cluster.sync();
                 } else {
                     if (gl >= (kind ? interior1 : interior0)) asm volatile("fence.acq_rel.cluster;" ::: "memory");
@@ -470,6 +524,26 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
                 *pb = B;
             }
             cluster.sync();
+        }
+    }
+    // ---- membrane residuals after the iterations (soft_body.cpp:2366-2404) ---
+    if (kMembrane && S2 > 0) {
+        const uint32_t lo = soff[S0 + S1 + 2], hi = soff[S0 + S1 + 2 + S2];
+        for (uint32_t i = lo + tid; i < hi; i += blockDim.x) {
+            const uint4 q = __ldg(rec2 + i);
+            const uint32_t ra = q.x & 0xffffu, rb = q.x >> 16, rc = q.y & 0xffffu;
+            const float4 A = ld_node(node_addr(ra, me, rank_base, x_base));
+            const float4 B = ld_node(node_addr(rb, me, rank_base, x_base));
+            const float4 C = ld_node(node_addr(rc, me, rank_base, x_base));
+            const MembraneConst m = load_membrane(I.kind[2].aux, i);
+            float3 PA = make_float3(0.0f, 0.0f, 0.0f), PB = PA, PC = PA;
+            if (m.damping_time != 0.0f) {
+                PA = f3(__ldg(I.pos_in + pbeg_s[ra >> 12] + (ra & 0xfffu)));
+                PB = f3(__ldg(I.pos_in + pbeg_s[rb >> 12] + (rb & 0xfffu)));
+                PC = f3(__ldg(I.pos_in + pbeg_s[rc >> 12] + (rc & 0xfffu)));
+            }
+            I.membrane_residual[i] = membrane_residual(f3(A), f3(B), f3(C), PA, PB, PC, m, lam2 + 3 * (i - first2),
+                                                       p.inv_dt, p.inv_dt2);
         }
     }
     // ---- finalize (soft_body.cpp:1568-1585) --------------------------------
@@ -585,6 +659,9 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
 // cluster (the batched step).
 inline constexpr auto xpbd_cluster_kernel = &xpbd_cluster_kernel_t<false>;
 inline constexpr auto xpbd_cluster_packed_kernel = &xpbd_cluster_kernel_t<true>;
+// The same with membrane elements.
+inline constexpr auto xpbd_cluster_membrane_kernel = &xpbd_cluster_kernel_t<false, false, true>;
+inline constexpr auto xpbd_cluster_packed_membrane_kernel = &xpbd_cluster_kernel_t<true, false, true>;
 // One structure per cluster, recording the adjoint's tape.
 inline constexpr auto xpbd_cluster_tape_kernel = &xpbd_cluster_kernel_t<false, true>;
 

@@ -10,6 +10,7 @@ namespace swb {
 
 namespace dev {
 constexpr int kClusterMaxThreads = 768;  // threads per CTA of the cluster step kernels
+constexpr int kClusterMaxCtasDev = 16;   // CTAs per cluster at most
 }
 
 struct ClusterKindDev {
@@ -19,8 +20,17 @@ struct ClusterKindDev {
     uint32_t smem_lambda;      // byte offset of this kind's multipliers
     uint64_t sync_mask;        // bit g: a cluster barrier follows stage g (stages >= 64: always)
     int interior_stages;       // stages before this one touch only the CTA's own nodes
-    int pad[3];
+    int pad;
+    const float4* aux;         // membranes: kMembraneAux float4 of element constants per record
 };
+
+// Membrane element constants, per record (float4 each):
+//   0: inverse reference (chart) matrix m00 m01 m10 m11
+//   1: sqrt(reference area), damping time, compression stiffness ratio, warp pre-tension
+//   2: weft pre-tension, compliance xx yy zz
+//   3: compliance xy xz yz, stiffness xx
+//   4: stiffness yy zz xy, 0
+constexpr int kMembraneAux = 5;
 
 // Per-instance tables and state (one cluster each).
 struct ClusterInstance {
@@ -34,7 +44,8 @@ struct ClusterInstance {
     const uint32_t* tri_list;
     const uint4* tri;
     const uint32_t* patch_begin;   // [ctas + 1]
-    ClusterKindDev kind[2];
+    ClusterKindDev kind[3];        // distance, dihedral, membrane (swept distance, membrane, dihedral)
+    float* membrane_residual;      // per membrane record: normalized residual of the last substep
     const uint32_t* seam_offsets;
     const uint32_t* seam_ab;
     int seam_stages;

@@ -178,23 +178,36 @@ void balance_colours(const std::vector<std::array<uint32_t, 4>>& nodes, const st
 
 }  // namespace
 
-// True when a record of global stage g (distance stages, then dihedral
-// stages) has a node flagged in `attached`.
+// Nodes of element i (definition index) of kind k: 2 (distance), 4
+// (dihedral) or 3 (membrane: its triangle's corners); returns the count.
+static int element_nodes(const OwnedDefinition& d, int k, size_t i, uint32_t* nodes) {
+    if (k == 0) {
+        nodes[0] = static_cast<uint32_t>(d.constraints[i].first_node);
+        nodes[1] = static_cast<uint32_t>(d.constraints[i].second_node);
+        return 2;
+    }
+    if (k == 1) {
+        for (int q = 0; q < 4; ++q) nodes[q] = static_cast<uint32_t>(d.dihedrals[i].nodes[q]);
+        return 4;
+    }
+    const swb_triangle_def& t = d.triangles[d.membranes[i].triangle];
+    for (int q = 0; q < 3; ++q) nodes[q] = static_cast<uint32_t>(t.nodes[q]);
+    return 3;
+}
+
+// True when a record of global stage g has a node flagged in `attached`.
 static bool stage_touches(const OwnedDefinition& d, const ClusterSchedule& S, const std::vector<uint8_t>& attached,
                           int g) {
-    const int S0 = S.kinds[0].stages;
-    const int k = g < S0 ? 0 : 1, s = k ? g - S0 : g;
+    int k, s;
+    global_stage(S, g, k, s);
     const ClusterKind& K = S.kinds[k];
     for (int c = 0; c < S.ctas; ++c)
         for (uint32_t r = K.offsets[static_cast<size_t>(c) * (K.stages + 1) + s];
              r < K.offsets[static_cast<size_t>(c) * (K.stages + 1) + s + 1]; ++r) {
-            const uint32_t i = K.def_index[r];
-            if (k == 0) {
-                if (attached[d.constraints[i].first_node] || attached[d.constraints[i].second_node]) return true;
-            } else {
-                for (int q = 0; q < 4; ++q)
-                    if (attached[d.dihedrals[i].nodes[q]]) return true;
-            }
+            uint32_t nodes[4];
+            const int cnt = element_nodes(d, k, K.def_index[r], nodes);
+            for (int q = 0; q < cnt; ++q)
+                if (attached[nodes[q]]) return true;
         }
     return false;
 }
@@ -230,17 +243,14 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
     }
     if (!suspension_nodes.empty()) S.susp_cta = part[suspension_nodes[0]];
 
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < 3; ++k) {
         ClusterKind& K = S.kinds[k];
-        const size_t m = k == 0 ? d.constraints.size() : d.dihedrals.size();
+        const size_t m = k == 0 ? d.constraints.size() : (k == 1 ? d.dihedrals.size() : d.membranes.size());
         std::vector<std::array<uint32_t, 4>> nodes(m);
-        std::vector<int> counts(m, k == 0 ? 2 : 4);
+        std::vector<int> counts(m, 0);
         for (size_t i = 0; i < m; ++i) {
-            if (k == 0)
-                nodes[i] = {static_cast<uint32_t>(d.constraints[i].first_node),
-                            static_cast<uint32_t>(d.constraints[i].second_node), 0, 0};
-            else
-                for (int q = 0; q < 4; ++q) nodes[i][q] = static_cast<uint32_t>(d.dihedrals[i].nodes[q]);
+            nodes[i] = {0, 0, 0, 0};
+            counts[i] = element_nodes(d, k, i, nodes[i].data());
         }
         // executing CTA: owner of most of the constraint's nodes (ties: first)
         std::vector<int> cta_of(m, 0);
@@ -259,7 +269,7 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
             interior[i] = best_count == counts[i];
         }
         std::vector<int> colour(m, 0);  // becomes the stage
-        if (!split || ctas == 1) {
+        if (!split || ctas == 1 || k == 2) {  // membranes: classic stages
             K.stages = dsatur_colour(nodes, counts, colour);
             K.stages = reduce_colours(nodes, counts, N, K.stages, colour, kColourSearchMoves);
             balance_colours(nodes, counts, cta_of, ctas, N, K.stages, colour);
@@ -341,7 +351,11 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
         }
         for (uint32_t i : idx) {
             K.ab.push_back(make_ref(S, nodes[i][0]) | (make_ref(S, nodes[i][1]) << 16));
-            if (k == 1) {
+            if (k == 2) {
+                K.cd.push_back(make_ref(S, nodes[i][2]));
+                K.rest.push_back(0.0f);
+                K.comp.push_back(0.0f);
+            } else if (k == 1) {
                 K.cd.push_back(make_ref(S, nodes[i][2]) | (make_ref(S, nodes[i][3]) << 16));
                 K.rest.push_back(static_cast<float>(d.dihedrals[i].rest_angle));
                 K.comp.push_back(static_cast<float>(d.dihedrals[i].compliance));
@@ -356,7 +370,7 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
             K.def_index.push_back(i);
         }
         // sweep order: stage-major, CTA, record order
-        auto& order = k == 0 ? S.distance_order : S.dihedral_order;
+        auto& order = k == 0 ? S.distance_order : (k == 1 ? S.dihedral_order : S.membrane_order);
         for (int s = 0; s < stages; ++s)
             for (int c = 0; c < ctas; ++c)
                 for (uint32_t r = K.offsets[static_cast<size_t>(c) * (stages + 1) + s];
@@ -370,11 +384,12 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
     if (S.susp_cta >= 0 && !(split && ctas > 1)) {
         std::vector<uint8_t> attached(N, 0);
         for (uint32_t n : suspension_nodes) attached[n] = 1;
-        const int S0 = S.kinds[0].stages, Sg = S0 + S.kinds[1].stages;
+        const int Sg = total_stages(S);
         if (Sg >= 2 && !stage_touches(d, S, attached, Sg - 2) && !stage_touches(d, S, attached, Sg - 1)) {
             S.line_stage = Sg - 2;
             for (int g = Sg - 2; g < Sg; ++g) {
-                const int k = g < S0 ? 0 : 1, s = k ? g - S0 : g;
+                int k, s;
+                global_stage(S, g, k, s);
                 const ClusterKind& K = S.kinds[k];
                 const size_t o = static_cast<size_t>(S.susp_cta) * (K.stages + 1) + s;
                 S.line_owner_records = std::max(S.line_owner_records, K.offsets[o + 1] - K.offsets[o]);
@@ -440,12 +455,13 @@ void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_
             fail("suspension node outside the owner patch");
     }
     if (S.line_stage >= 0) {
-        const int S0 = S.kinds[0].stages, Sg = S0 + S.kinds[1].stages;
+        const int Sg = total_stages(S);
         if (S.susp_cta < 0 || S.line_stage != Sg - 2) fail("line iteration window position");
         std::vector<uint8_t> attached(N, 0);
         for (uint32_t n : suspension_nodes) attached[n] = 1;
         for (int g = Sg - 2; g < Sg; ++g) {
-            const int k = g < S0 ? 0 : 1, s = k ? g - S0 : g;
+            int k, s;
+            global_stage(S, g, k, s);
             if (stage_touches(d, S, attached, g)) fail("line iteration window touches a suspension node");
             if (!S.kinds[k].cluster_sync[s]) fail("line iteration window without cluster barriers");
             const size_t o = static_cast<size_t>(S.susp_cta) * (S.kinds[k].stages + 1) + s;
@@ -459,9 +475,9 @@ void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_
     std::vector<int64_t> run_of(N, -1);
     std::vector<int> run_cta(N, -1);
     int64_t run = 0;
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < 3; ++k) {
         const ClusterKind& K = S.kinds[k];
-        const size_t m = k == 0 ? d.constraints.size() : d.dihedrals.size();
+        const size_t m = k == 0 ? d.constraints.size() : (k == 1 ? d.dihedrals.size() : d.membranes.size());
         std::vector<uint8_t> seen(m, 0);
         if (K.cluster_sync.size() != static_cast<size_t>(K.stages)) fail("barrier kinds per stage");
         if (K.stages > 0 && !K.cluster_sync.back()) fail("a kind must end with a cluster barrier");
@@ -472,18 +488,11 @@ void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_
                      r < K.offsets[static_cast<size_t>(c) * (K.stages + 1) + s + 1]; ++r) {
                     const uint32_t i = K.def_index[r];
                     if (seen[i]++) fail("constraint scheduled twice");
-                    uint32_t refs[4] = {K.ab[r] & 0xffffu, K.ab[r] >> 16, 0, 0};
+                    const uint32_t refs[4] = {K.ab[r] & 0xffffu, K.ab[r] >> 16, k ? (K.cd[r] & 0xffffu) : 0u,
+                                              k ? (K.cd[r] >> 16) : 0u};
                     uint32_t want[4];
-                    int cnt = 2;
-                    if (k == 0) {
-                        want[0] = static_cast<uint32_t>(d.constraints[i].first_node);
-                        want[1] = static_cast<uint32_t>(d.constraints[i].second_node);
-                    } else {
-                        refs[2] = K.cd[r] & 0xffffu;
-                        refs[3] = K.cd[r] >> 16;
-                        cnt = 4;
-                        for (int q = 0; q < 4; ++q) want[q] = static_cast<uint32_t>(d.dihedrals[i].nodes[q]);
-                    }
+                    const int cnt = element_nodes(d, k, i, want);
+                    if (k == 2 && (K.cd[r] >> 16) != 0) fail("membrane record's fourth reference");
                     for (int q = 0; q < cnt; ++q) {
                         const uint32_t n = node_of_ref(refs[q]);
                         if (n != want[q]) fail("reference does not name the constraint's node");

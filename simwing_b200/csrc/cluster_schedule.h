@@ -63,7 +63,10 @@ struct ClusterSchedule {
     std::vector<uint32_t> node_of_slot, slot_of_node;  // slots: patch-major
     std::vector<uint32_t> patch_begin;                 // [ctas + 1]
     uint32_t max_patch = 0;
-    std::array<ClusterKind, 2> kinds;
+    // kinds[0] distance-type constraints, kinds[1] dihedrals, kinds[2]
+    // membrane elements; an iteration runs distance, membrane, then dihedral
+    // stages (soft_body.cpp:1318-1369)
+    std::array<ClusterKind, 3> kinds;
     // seam closing pass: level-scheduled in sweep order, per (cta, stage)
     int seam_stages = 0;
     std::vector<uint32_t> seam_offsets;  // [ctas * (seam_stages + 1)]
@@ -78,8 +81,28 @@ struct ClusterSchedule {
     // suspension CTA's larger record count of the two.
     int line_stage = -1;
     uint32_t line_owner_records = 0;
-    std::vector<uint64_t> distance_order, dihedral_order;
+    std::vector<uint64_t> distance_order, dihedral_order, membrane_order;
 };
+
+// Colour stages per iteration, all kinds.
+inline int total_stages(const ClusterSchedule& s) {
+    return s.kinds[0].stages + s.kinds[1].stages + s.kinds[2].stages;
+}
+// Kind and stage within the kind of global stage g of an iteration
+// (distance stages, membrane stages, dihedral stages).
+inline void global_stage(const ClusterSchedule& s, int g, int& kind, int& local) {
+    const int S0 = s.kinds[0].stages, S2 = s.kinds[2].stages;
+    if (g < S0) {
+        kind = 0;
+        local = g;
+    } else if (g < S0 + S2) {
+        kind = 2;
+        local = g - S0;
+    } else {
+        kind = 1;
+        local = g - S0 - S2;
+    }
+}
 
 // Cluster barriers per constraint iteration (stages followed by one, plus
 // the suspension stage unless the line iteration runs beside two stages).
@@ -91,11 +114,11 @@ inline int cluster_barriers_per_iteration(const ClusterSchedule& s) {
 }
 
 // Dynamic shared memory of the cluster step kernel for this schedule
-// (nodes, forces/velocities, multipliers, stage offsets; with slack for the
-// 16-byte alignment of each array).
+// (nodes, forces/velocities, multipliers -- three per membrane element --,
+// stage offsets; with slack for the 16-byte alignment of each array).
 inline size_t cluster_shared_bytes(const ClusterSchedule& s) {
     return s.max_patch * 32ull + s.kinds[0].max_cta_records * 4ull + s.kinds[1].max_cta_records * 4ull +
-           (s.kinds[0].stages + s.kinds[1].stages + 2) * 4ull + 64;
+           s.kinds[2].max_cta_records * 12ull + (total_stages(s) + 3) * 4ull + 80;
 }
 
 // Returns false (and leaves `out` empty) when the mesh does not fit one

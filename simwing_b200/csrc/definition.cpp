@@ -518,6 +518,23 @@ swb_status swb_definition_permute(swb_definition* definition,
     });
 }
 
+swb_status swb_definition_permute_membranes(swb_definition* definition, const uint64_t* membrane_order) {
+    return guarded([&] {
+        if (!definition) raise(SWB_INVALID_ARGUMENT, "definition is null");
+        OwnedDefinition& d = definition->def;
+        if (!membrane_order) return;
+        std::vector<uint8_t> seen(d.membranes.size(), 0);
+        const auto copy = d.membranes;
+        for (size_t k = 0; k < d.membranes.size(); ++k) {
+            if (membrane_order[k] >= copy.size() || seen[membrane_order[k]])
+                raise(SWB_INVALID_ARGUMENT, "order is not a permutation");
+            seen[membrane_order[k]] = 1;
+            d.membranes[k] = copy[membrane_order[k]];
+        }
+        d.sync_view();
+    });
+}
+
 swb_status swb_definition_scale_rest(swb_definition* definition,
                                      uint64_t index, double factor) {
     return guarded([&] {

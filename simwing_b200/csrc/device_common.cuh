@@ -15,6 +15,7 @@ enum : int {
     kStatusNonFinite = 2,
     kStatusSuspension = 4,
     kStatusCopyTimeout = 8,
+    kStatusMembrane = 16,
 };
 
 enum : int {

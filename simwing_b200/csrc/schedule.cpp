@@ -739,7 +739,7 @@ extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definiti
                 std::memset(out, 0, sizeof(*out));
                 out->blocks = C.ctas;
                 out->cluster_ctas = C.ctas;
-                out->local_stages_per_iteration = C.kinds[0].stages + C.kinds[1].stages;
+                out->local_stages_per_iteration = total_stages(C);
                 out->cluster_barriers_per_iteration = cluster_barriers_per_iteration(C);
                 out->max_patch_nodes = static_cast<int32_t>(C.max_patch);
                 out->shared_bytes = static_cast<int32_t>(bytes);

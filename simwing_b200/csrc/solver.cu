@@ -53,10 +53,13 @@ constexpr int kDiagFields = 16;
 
 __global__ void diagnostics_kernel(const float4* pos, const float4* prev, const float4* vel, uint32_t n,
                                    const uint32_t* ca, const uint32_t* cb, const float* rest, const uint8_t* kind,
-                                   uint32_t m, double* partials) {
+                                   uint32_t m, const uint4* mem, const float4* maux, const float* mres, uint32_t nm,
+                                   double* partials) {
     // fields: 0 dyn count, 1 mass, 2-4 sum m x, 5-7 sum m v, 8 KE, 9 finite(min),
-    //         10 max |distance error|, 11 max cable extension
-    double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0};
+    //         10 max |distance error|, 11 max cable extension,
+    //         12 max |membrane strain component|, 13 max |membrane residual|
+    constexpr int F = 14;
+    double acc[F] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0};
     const uint32_t stride = blockDim.x * gridDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float4 X = pos[i], P = prev[i], V = vel[i];
@@ -80,9 +83,32 @@ __global__ void diagnostics_kernel(const float4* pos, const float4* prev, const 
         if (kind[i] == SWB_CONSTRAINT_CABLE) acc[11] = fmax(acc[11], fmax(0.0, e));
         else acc[10] = fmax(acc[10], fabs(e));
     }
-    __shared__ double red[32][12];
+    // membrane Green strain at the current positions (evaluateMembraneElement,
+    // soft_body.cpp:204-225) and the last substep's residual
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += stride) {
+        const uint4 e = mem[i];
+        const float4 q0 = maux[static_cast<size_t>(e.w) * kMembraneAux];
+        const float4 q1 = maux[static_cast<size_t>(e.w) * kMembraneAux + 1];
+        const float4 q2 = maux[static_cast<size_t>(e.w) * kMembraneAux + 2];
+        const float4 A = pos[e.x], B = pos[e.y], C = pos[e.z];
+        const double e1[3] = {double(B.x) - A.x, double(B.y) - A.y, double(B.z) - A.z};
+        const double e2[3] = {double(C.x) - A.x, double(C.y) - A.y, double(C.z) - A.z};
+        double wa[3], wf[3];
+        for (int k = 0; k < 3; ++k) {
+            wa[k] = q0.x * e1[k] + q0.z * e2[k];
+            wf[k] = q0.y * e1[k] + q0.w * e2[k];
+        }
+        const double sx = 0.5 * (wa[0] * wa[0] + wa[1] * wa[1] + wa[2] * wa[2] - 1.0) + q1.w;
+        const double sy = 0.5 * (wf[0] * wf[0] + wf[1] * wf[1] + wf[2] * wf[2] - 1.0) + q2.x;
+        const double sz = wa[0] * wf[0] + wa[1] * wf[1] + wa[2] * wf[2];
+        const double r = mres[e.w];
+        if (!isfinite(sx) || !isfinite(sy) || !isfinite(sz) || !isfinite(r)) acc[9] = 0.0;
+        acc[12] = fmax(acc[12], fmax(fabs(sx), fmax(fabs(sy), fabs(sz))));
+        acc[13] = fmax(acc[13], fabs(r));
+    }
+    __shared__ double red[32][F];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int f = 0; f < 12; ++f) {
+    for (int f = 0; f < F; ++f) {
         double v = acc[f];
         for (int o = 16; o > 0; o >>= 1) {
             const double u = __shfl_down_sync(0xffffffffu, v, o);
@@ -93,7 +119,7 @@ __global__ void diagnostics_kernel(const float4* pos, const float4* prev, const 
     __syncthreads();
     if (threadIdx.x == 0) {
         const int warps = (blockDim.x + 31) / 32;
-        for (int f = 0; f < 12; ++f) {
+        for (int f = 0; f < F; ++f) {
             double v = red[0][f];
             for (int w = 1; w < warps; ++w)
                 v = f == 9 ? fmin(v, red[w][f]) : (f >= 10 ? fmax(v, red[w][f]) : v + red[w][f]);
@@ -120,7 +146,6 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     validate_definition(def.view);
     fingerprint = definition_fingerprint(def.view);
     if (def.has_contact) raise(SWB_UNSUPPORTED, "fabric self-contact is not available in this build");
-    if (!def.membranes.empty()) raise(SWB_UNSUPPORTED, "membrane elements are not available in this build");
     // Solver-drift momentum restoration of isolated free structures: no
     // suspension, no contact, bending or membranes present, no fixed node.
     momentum_guard = !def.has_suspension && !def.has_contact && (!def.dihedrals.empty() || !def.membranes.empty()) &&
@@ -173,6 +198,8 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     }
     if (!cluster_mode && momentum_guard)
         raise(SWB_UNSUPPORTED, "the momentum guard of a free structure needs the cluster schedule (the mesh does not fit one)");
+    if (!cluster_mode && !def.membranes.empty())
+        raise(SWB_UNSUPPORTED, "membrane elements need the cluster schedule (the mesh does not fit one)");
     uint32_t widest = 32;
     if (cluster_mode) {
         verify_cluster_schedule(def, susp_nodes, csched);
@@ -260,6 +287,36 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     finish_build(opt, prop);
 }
 
+// Device constants of one membrane element (kMembraneAux float4, layout in
+// cluster_params.h): the chart's inverse edge matrix, sqrt(area) and the
+// material's compliance, computed in FP64 as addMembraneElements does
+// (soft_body.cpp:664-690, membrane.cpp:131-271), then rounded.
+static void membrane_constants(const swb_membrane_def& m, float4 out[kMembraneAux]) {
+    const double e1x = m.chart[1][0] - m.chart[0][0], e1y = m.chart[1][1] - m.chart[0][1];
+    const double e2x = m.chart[2][0] - m.chart[0][0], e2y = m.chart[2][1] - m.chart[0][1];
+    const double det = e1x * e2y - e2x * e1y;  // edge matrix [e1x e2x; e1y e2y]
+    const double id = 1.0 / det;
+    const double i00 = e2y * id, i01 = -e2x * id, i10 = -e1y * id, i11 = e1x * id;
+    const swb_membrane_material& q = m.material;
+    const double kxx = q.warp_stiffness, kyy = q.weft_stiffness, kzz = q.shear_stiffness, kxy = q.coupling_stiffness;
+    // symmetric inverse of [kxx kxy 0; kxy kyy 0; 0 0 kzz]
+    const double kdet = kxx * (kyy * kzz) - kxy * (kxy * kzz);
+    const double kid = 1.0 / kdet;
+    const double cxx = (kyy * kzz) * kid, cyy = (kxx * kzz) * kid, czz = (kxx * kyy - kxy * kxy) * kid;
+    const double cxy = (-kxy * kzz) * kid;
+    auto f = [](double v) { return static_cast<float>(v); };
+    out[0] = make_float4(f(i00), f(i01), f(i10), f(i11));
+    out[1] = make_float4(f(std::sqrt(0.5 * det)), f(q.damping_seconds), f(q.compression_stiffness_ratio),
+                         f(q.warp_pretension));
+    out[2] = make_float4(f(q.weft_pretension), f(cxx), f(cyy), f(czz));
+    out[3] = make_float4(f(cxy), 0.0f, 0.0f, f(kxx));
+    out[4] = make_float4(f(kyy), f(kzz), f(kxy), 0.0f);
+}
+
+void (*StructureImpl::step_kernel() const)(ClusterParams) {
+    return def.membranes.empty() ? dev::xpbd_cluster_kernel : dev::xpbd_cluster_membrane_kernel;
+}
+
 void StructureImpl::upload_cluster_tables() {
     ClusterParams& cp = cparams;
     std::memset(&cp, 0, sizeof(cp));
@@ -269,15 +326,25 @@ void StructureImpl::upload_cluster_tables() {
     cp.smem_v = off; off = align16(off + csched.max_patch * 16u);
     ClusterInstance base{};
     base.patch_begin = dupload(owned, csched.patch_begin, stream);
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < 3; ++k) {
         const ClusterKind& K = csched.kinds[k];
         ClusterKindDev& dk = base.kind[k];
         dk.offsets = dupload(owned, K.offsets, stream);
         std::vector<uint4> rec(K.ab.size());
         for (size_t r = 0; r < rec.size(); ++r)
-            rec[r] = make_uint4(K.ab[r], k == 1 ? K.cd[r] : 0u, std::bit_cast<uint32_t>(K.rest[r]),
+            rec[r] = make_uint4(K.ab[r], k >= 1 ? K.cd[r] : 0u, std::bit_cast<uint32_t>(K.rest[r]),
                                 std::bit_cast<uint32_t>(K.comp[r]));
         dk.rec = dupload(owned, rec, stream);
+        if (k == 2) {
+            std::vector<float4> aux(rec.size() * kMembraneAux);
+            for (size_t r = 0; r < rec.size(); ++r) membrane_constants(def.membranes[K.def_index[r]], &aux[r * kMembraneAux]);
+            dk.aux = dupload(owned, aux, stream);
+            for (int b = 0; b < 3; ++b) {
+                d_mres[b] = dalloc<float>(owned, rec.size());
+                cuda_check(cudaMemsetAsync(d_mres[b], 0, std::max<size_t>(rec.size(), 1) * sizeof(float), stream),
+                           "memset");
+            }
+        }
         dk.stages = K.stages;
         dk.smem_lambda = off;
         // stages from 64 on always take a cluster barrier (a superset of any CTA barrier)
@@ -285,10 +352,10 @@ void StructureImpl::upload_cluster_tables() {
         for (int g = 0; g < std::min(K.stages, 64); ++g)
             if (K.cluster_sync[g]) dk.sync_mask |= 1ull << g;
         dk.interior_stages = K.interior_stages;
-        off = align16(off + K.max_cta_records * 4u);
+        off = align16(off + K.max_cta_records * (k == 2 ? 12u : 4u));
     }
     cp.smem_offsets = off;
-    off = align16(off + (csched.kinds[0].stages + csched.kinds[1].stages + 2) * 4u);
+    off = align16(off + (total_stages(csched) + 3) * 4u);
     cluster_smem = off;
     base.seam_offsets = dupload(owned, csched.seam_offsets, stream);
     base.seam_ab = dupload(owned, csched.seam_ab, stream);
@@ -382,6 +449,19 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
         d_diag_rest = dupload(owned, rest, stream);
         d_diag_kind = dupload(owned, kind, stream);
         d_diag_partials = dalloc<double>(owned, static_cast<size_t>(kDiagBlocks) * kDiagFields);
+        // membrane records: corner slots and record index (constants and
+        // residual are per record)
+        if (cluster_mode && !def.membranes.empty()) {
+            const ClusterKind& K = csched.kinds[2];
+            std::vector<uint4> mem(K.def_index.size());
+            for (size_t r = 0; r < mem.size(); ++r) {
+                const swb_triangle_def& t = def.triangles[def.membranes[K.def_index[r]].triangle];
+                mem[r] = make_uint4(static_cast<uint32_t>(slot_of_node[t.nodes[0]]),
+                                    static_cast<uint32_t>(slot_of_node[t.nodes[1]]),
+                                    static_cast<uint32_t>(slot_of_node[t.nodes[2]]), static_cast<uint32_t>(r));
+            }
+            d_diag_mem = dupload(owned, mem, stream);
+        }
     }
 
     // suspension
@@ -495,6 +575,7 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
                 c.payload_def = d_payload_def;
                 c.payload_in = d_payload[in]; c.payload_out = d_payload[out];
                 c.origin_in = d_origin[in]; c.origin_out = d_origin[out];
+                c.membrane_residual = d_mres[out];
                 c.status = d_control->status;
                 c.recentre = def.has_suspension ? 1 : 0;
                 inst[in * 3 + out] = c;
@@ -505,12 +586,12 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
         // the process: it is raised to the device limit, never set to this
         // structure's need (a smaller structure built later would otherwise
         // lower it below what an earlier one launches with).
-        cuda_check(cudaFuncSetAttribute(dev::xpbd_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const auto kernel = step_kernel();
+        cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(smem_limit_)),
                    "shared memory request of the cluster schedule");
         if (G > 8)
-            cuda_check(cudaFuncSetAttribute(dev::xpbd_cluster_kernel,
-                                            cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
+            cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1),
                        "non-portable cluster size");
         cudaLaunchConfig_t cfg{};
         cudaLaunchAttribute attr[1];
@@ -524,7 +605,7 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        cuda_check(cudaOccupancyMaxActiveClusters(&clusters, dev::xpbd_cluster_kernel, &cfg), "cluster occupancy");
+        cuda_check(cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg), "cluster occupancy");
         if (clusters < 1) raise(SWB_UNSUPPORTED, "a cluster of " + std::to_string(G) + " CTAs cannot be scheduled");
     } else {
         // launch feasibility of the cooperative grid
@@ -661,7 +742,7 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out)
         cfg.stream = stream;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        cuda_check(cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_kernel, cp), "cudaLaunchKernelEx (cluster)");
+        cuda_check(cudaLaunchKernelEx(&cfg, step_kernel(), cp), "cudaLaunchKernelEx (cluster)");
         return;
     }
     StepParams p = params;
@@ -690,6 +771,8 @@ size_t dynamic_smem_limit(const cudaDeviceProp& prop) {
     size_t reserve = 2048;
     for (const void* k : {reinterpret_cast<const void*>(dev::xpbd_cluster_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_packed_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_membrane_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_packed_membrane_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_tape_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_kernel_narrow),
@@ -701,19 +784,24 @@ size_t dynamic_smem_limit(const cudaDeviceProp& prop) {
 }
 
 cudaError_t packed_kernel_limits(int max_dynamic_smem, bool non_portable_cluster) {
-    cudaError_t rc = cudaFuncSetAttribute(dev::xpbd_cluster_packed_kernel,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem);
-    if (rc == cudaSuccess && non_portable_cluster)
-        rc = cudaFuncSetAttribute(dev::xpbd_cluster_packed_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaError_t rc = cudaSuccess;
+    for (auto kernel : {dev::xpbd_cluster_packed_kernel, dev::xpbd_cluster_packed_membrane_kernel}) {
+        if (rc == cudaSuccess)
+            rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem);
+        if (rc == cudaSuccess && non_portable_cluster)
+            rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
     return rc;
 }
 
-cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg) {
-    return cudaOccupancyMaxActiveClusters(clusters, dev::xpbd_cluster_packed_kernel, &cfg);
+cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg, bool membranes) {
+    return cudaOccupancyMaxActiveClusters(
+        clusters, membranes ? dev::xpbd_cluster_packed_membrane_kernel : dev::xpbd_cluster_packed_kernel, &cfg);
 }
 
-cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params) {
-    return cudaLaunchKernelEx(&cfg, dev::xpbd_cluster_packed_kernel, params);
+cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params, bool membranes) {
+    return cudaLaunchKernelEx(
+        &cfg, membranes ? dev::xpbd_cluster_packed_membrane_kernel : dev::xpbd_cluster_packed_kernel, params);
 }
 
 cudaError_t plain_cluster_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params) {
@@ -760,6 +848,10 @@ swb_status decode_status(const int status[2], std::string& message) {
     if (status[0] & dev::kStatusCopyTimeout) {
         message = "shared-memory staging timed out";
         return SWB_SYNC_TIMEOUT;
+    }
+    if (status[0] & dev::kStatusMembrane) {
+        message = "membrane system is singular or its right-hand side is not finite";
+        return SWB_INVALID_ARGUMENT;
     }
     if (status[0] & dev::kStatusSuspension) {
         static const char* what[] = {"suspension failure", "line geometry is non-finite or scale-degenerate",
@@ -863,8 +955,10 @@ void StructureImpl::diagnostics(swb_diagnostics* o) const {
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
     const uint32_t N = static_cast<uint32_t>(def.nodes.size());
     const uint32_t M = static_cast<uint32_t>(def.constraints.size());
+    const uint32_t NM = d_diag_mem ? static_cast<uint32_t>(def.membranes.size()) : 0u;
     diagnostics_kernel<<<kDiagBlocks, 256, 0, stream>>>(d_pos[cur], d_prev[cur], d_vel[cur], N, d_diag_a, d_diag_b,
-                                                         d_diag_rest, d_diag_kind, M, d_diag_partials);
+                                                         d_diag_rest, d_diag_kind, M, d_diag_mem,
+                                                         cluster_base.kind[2].aux, d_mres[cur], NM, d_diag_partials);
     cuda_check(cudaGetLastError(), "diagnostics");
     std::vector<double> part(static_cast<size_t>(kDiagBlocks) * kDiagFields);
     DevPayloadState pay{};
@@ -874,13 +968,12 @@ void StructureImpl::diagnostics(swb_diagnostics* o) const {
     cuda_check(cudaMemcpyAsync(&pay, d_payload[cur], sizeof(pay), cudaMemcpyDeviceToHost, stream), "read");
     cuda_check(cudaMemcpyAsync(origin, d_origin[cur], sizeof(origin), cudaMemcpyDeviceToHost, stream), "read");
     cuda_check(cudaStreamSynchronize(stream), "diagnostics");
-    double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0};
+    double acc[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0};
     for (int b = 0; b < kDiagBlocks; ++b) {
         const double* q = &part[static_cast<size_t>(b) * kDiagFields];
         for (int f = 0; f < 9; ++f) acc[f] += q[f];
         acc[9] = std::min(acc[9], q[9]);
-        acc[10] = std::max(acc[10], q[10]);
-        acc[11] = std::max(acc[11], q[11]);
+        for (int f = 10; f < 14; ++f) acc[f] = std::max(acc[f], q[f]);
     }
     std::memset(o, 0, sizeof(*o));
     o->node_count = N;
@@ -925,6 +1018,8 @@ void StructureImpl::diagnostics(swb_diagnostics* o) const {
     o->kinetic_energy = ke;
     o->maximum_distance_error = acc[10];
     o->maximum_cable_extension = acc[11];
+    o->maximum_absolute_membrane_strain = acc[12];
+    o->maximum_membrane_residual = acc[13];
     swb_vec3 pend{0, 0, 0};
     for (const auto& f : pending) {
         pend.x += f.x; pend.y += f.y; pend.z += f.z;
@@ -1184,10 +1279,14 @@ swb_status swb_structure_sweep_order(const swb_structure* s, uint32_t which, uin
     return guarded([&] {
         if (!s || (!order && count)) raise(SWB_INVALID_ARGUMENT, "null argument");
         const StructureImpl& m = s->s;
+        if (which > SWB_SWEEP_MEMBRANE) raise(SWB_INVALID_ARGUMENT, "unknown sweep");
+        static const std::vector<uint64_t> none;
         const auto& v = m.cluster_mode
-                            ? (which == SWB_SWEEP_DISTANCE ? m.csched.distance_order : m.csched.dihedral_order)
-                            : (which == SWB_SWEEP_DISTANCE ? m.sched.distance_order : m.sched.dihedral_order);
-        if (which > SWB_SWEEP_DIHEDRAL) raise(SWB_INVALID_ARGUMENT, "unknown sweep");
+                            ? (which == SWB_SWEEP_DISTANCE
+                                   ? m.csched.distance_order
+                                   : (which == SWB_SWEEP_DIHEDRAL ? m.csched.dihedral_order : m.csched.membrane_order))
+                            : (which == SWB_SWEEP_DISTANCE ? m.sched.distance_order
+                                                           : (which == SWB_SWEEP_DIHEDRAL ? m.sched.dihedral_order : none));
         if (count != v.size()) raise(SWB_INVALID_ARGUMENT, "order count mismatch");
         std::copy(v.begin(), v.end(), order);
     });
@@ -1204,7 +1303,7 @@ swb_status swb_structure_schedule_report(const swb_structure* s, swb_schedule_re
         if (m.cluster_mode) {
             const ClusterSchedule& C = m.csched;
             out->cluster_ctas = C.ctas;
-            out->local_stages_per_iteration = C.kinds[0].stages + C.kinds[1].stages;
+            out->local_stages_per_iteration = total_stages(C);
             out->cluster_barriers_per_iteration = cluster_barriers_per_iteration(C);
             out->max_patch_nodes = static_cast<int32_t>(C.max_patch);
             out->shared_bytes = static_cast<int32_t>(m.cluster_smem);

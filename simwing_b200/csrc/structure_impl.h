@@ -33,8 +33,9 @@ cudaError_t packed_kernel_limits(int max_dynamic_smem, bool non_portable_cluster
 // on this device: the opt-in maximum less the largest static shared memory
 // among those kernels (at least 2 KB).
 size_t dynamic_smem_limit(const cudaDeviceProp& prop);
-cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg);
-cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params);
+// `membranes`: the launch carries membrane elements (the membrane instantiation)
+cudaError_t packed_kernel_occupancy(int* clusters, const cudaLaunchConfig_t& cfg, bool membranes);
+cudaError_t packed_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params, bool membranes);
 // ... and of the single-structure kernels the differentiable rollout drives.
 cudaError_t plain_cluster_launch(const cudaLaunchConfig_t& cfg, const ClusterParams& params);
 cudaError_t tape_kernel_limits(int max_dynamic_smem, bool non_portable_cluster);
@@ -81,6 +82,8 @@ struct StructureImpl {
     uint32_t* d_tri_off = nullptr;
     uint32_t* d_tri_list = nullptr;
     uint32_t* d_diag_a = nullptr;
+    float* d_mres[3] = {nullptr, nullptr, nullptr};  // membrane residual per record, per state buffer
+    uint4* d_diag_mem = nullptr;      // membrane records for the diagnostics: corner slots, record index
     uint32_t* d_diag_b = nullptr;
     float* d_diag_rest = nullptr;
     uint8_t* d_diag_kind = nullptr;
@@ -105,6 +108,9 @@ struct StructureImpl {
     ~StructureImpl();
     void build(const swb_structure_definition& definition, const swb_solver_options* options);
     void upload_cluster_tables();
+    // the cluster step kernel for this structure (the membrane
+    // instantiation when it has membrane elements)
+    void (*step_kernel() const)(ClusterParams);
     void upload_grid_tables();
     void finish_build(const swb_solver_options& opt, const cudaDeviceProp& prop);
     void upload_pressure();
