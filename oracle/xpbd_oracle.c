@@ -17,6 +17,8 @@
  *   evaluate_dihedral  evaluateDihedral                  soft_body.cpp:1648-1711
  *   solve_dihedral     solveDihedralConstraint           soft_body.cpp:1754-1792
  *   measure/restore_momentum                             soft_body.cpp:119-190
+ *   load_path_order    loadPathConstraintOrder           soft_body.cpp:528-629
+ *   cable_pair         solveCablePair (+ distribution)   soft_body.cpp:1265-1317, 1380-1388
  *   membrane_setup     addMembraneElements               soft_body.cpp:664-690
  *   membrane_strain    evaluateMembraneElement (strain)  soft_body.cpp:204-270
  *   solve_membrane     membraneElementCorrections +
@@ -31,8 +33,8 @@
  *   certify/velocity/damping/finish                      suspension.cpp:2324-2610
  *   swo_diagnostics    Structure::diagnostics            structure.cpp:833-959
  *
- * Not restated (the functions return SWB_UNSUPPORTED): contact, load-path
- * cable sweep pairs, suspension controls and ground modes other than Free
+ * Not restated (the functions return SWB_UNSUPPORTED): contact,
+ * suspension controls and ground modes other than Free
  * (the Structure adapter always builds Free, structure.cpp:550), and the
  * equilibrated Cholesky fallback of a symmetric solve whose explicit inverse
  * is rejected (membrane.cpp:247-256).
@@ -273,6 +275,8 @@ typedef struct {
 typedef struct swo_structure {
     uint64_t n, t, m, h, nm;
     Membrane* mem;
+    uint64_t* load_path;     /* cable and tie indices in load-path order  */
+    uint64_t nload;
     Node* nodes;
     uint64_t (*tri)[3];
     double* pressure;
@@ -484,10 +488,110 @@ static int cmp_u64str(uint64_t a, uint64_t b) {
     return strcmp(sa, sb);
 }
 
+/* loadPathConstraintOrder (soft_body.cpp:528-629): the cables and
+ * suspension ties, stable-sorted by graph depth from the structural skin
+ * (fixed nodes and every node of a triangle, distance or seam constraint, or
+ * dihedral); a component with no structural node is rooted at its heaviest
+ * node (the first of the smallest inverse mass). */
+static void load_path_order(swo_structure* s) {
+    const uint64_t n = s->n;
+    uint8_t* structural = calloc(n ? n : 1, 1);
+    uint64_t* deg = calloc(n + 1, sizeof(uint64_t));
+    for (uint64_t i = 0; i < n; ++i) structural[i] = s->nodes[i].w == 0.0;
+    for (uint64_t t = 0; t < s->t; ++t)
+        for (int k = 0; k < 3; ++k) structural[s->tri[t][k]] = 1;
+    s->nload = 0;
+    for (uint64_t i = 0; i < s->m; ++i) {
+        const Distance* c = &s->dist[i];
+        if (c->kind == SWB_CONSTRAINT_DISTANCE || c->kind == SWB_CONSTRAINT_SEAM_STITCH) {
+            structural[c->a] = structural[c->b] = 1;
+            continue;
+        }
+        ++s->nload;
+        ++deg[c->a + 1];
+        ++deg[c->b + 1];
+    }
+    for (uint64_t i = 0; i < s->h; ++i) {
+        structural[s->dih[i].a] = structural[s->dih[i].b] = 1;
+        structural[s->dih[i].c] = structural[s->dih[i].d] = 1;
+    }
+    for (uint64_t v = 0; v < n; ++v) deg[v + 1] += deg[v];
+    /* adjacency in constraint order (each node's neighbours in the order
+     * its load-path constraints appear) */
+    uint64_t* adj = malloc((2 * s->nload + 1) * sizeof(uint64_t));
+    uint64_t* cur = malloc((n + 1) * sizeof(uint64_t));
+    memcpy(cur, deg, (n + 1) * sizeof(uint64_t));
+    free(s->load_path);
+    s->load_path = malloc((s->nload + 1) * sizeof(uint64_t));
+    uint64_t k = 0;
+    for (uint64_t i = 0; i < s->m; ++i) {
+        const Distance* c = &s->dist[i];
+        if (c->kind == SWB_CONSTRAINT_DISTANCE || c->kind == SWB_CONSTRAINT_SEAM_STITCH) continue;
+        s->load_path[k++] = i;
+        adj[cur[c->a]++] = c->b;
+        adj[cur[c->b]++] = c->a;
+    }
+    const uint64_t unknown = ~(uint64_t)0;
+    uint64_t* depth = malloc((n ? n : 1) * sizeof(uint64_t));
+    uint64_t* queue = malloc((n ? n : 1) * sizeof(uint64_t));
+    uint64_t head = 0, tail = 0;
+    for (uint64_t v = 0; v < n; ++v) {
+        depth[v] = unknown;
+        if (structural[v] && deg[v + 1] > deg[v]) {
+            depth[v] = 0;
+            queue[tail++] = v;
+        }
+    }
+    for (;;) {
+        while (head < tail) {
+            const uint64_t v = queue[head++];
+            for (uint64_t e = deg[v]; e < deg[v + 1]; ++e)
+                if (depth[adj[e]] == unknown) {
+                    depth[adj[e]] = depth[v] + 1;
+                    queue[tail++] = adj[e];
+                }
+        }
+        uint64_t root = n;
+        double smallest = INFINITY;
+        for (uint64_t v = 0; v < n; ++v)
+            if (depth[v] == unknown && deg[v + 1] > deg[v] && s->nodes[v].w < smallest) {
+                root = v;
+                smallest = s->nodes[v].w;
+            }
+        if (root == n) break;
+        depth[root] = 0;
+        queue[tail++] = root;
+    }
+    /* stable insertion sort by max(depth[a], depth[b]) */
+    for (uint64_t i = 1; i < s->nload; ++i) {
+        const uint64_t x = s->load_path[i];
+        const uint64_t dx = depth[s->dist[x].a] > depth[s->dist[x].b] ? depth[s->dist[x].a] : depth[s->dist[x].b];
+        uint64_t j = i;
+        while (j > 0) {
+            const uint64_t y = s->load_path[j - 1];
+            const uint64_t dy = depth[s->dist[y].a] > depth[s->dist[y].b] ? depth[s->dist[y].a] : depth[s->dist[y].b];
+            if (dy <= dx) break;
+            s->load_path[j] = y;
+            --j;
+        }
+        s->load_path[j] = x;
+    }
+    free(structural); free(deg); free(adj); free(cur); free(depth); free(queue);
+}
+
+static void project_distance(swo_structure* s, Distance* c, double inv_dt2);
+
+/* solveCablePair (soft_body.cpp:1265-1286): reverse depth order, then
+ * forward depth order */
+static void cable_pair(swo_structure* s, double inv_dt2) {
+    for (uint64_t k = s->nload; k-- > 0;) project_distance(s, &s->dist[s->load_path[k]], inv_dt2);
+    for (uint64_t k = 0; k < s->nload; ++k) project_distance(s, &s->dist[s->load_path[k]], inv_dt2);
+}
+
 void swo_destroy(swo_structure* s) {
     if (!s) return;
     free(s->nodes); free(s->tri); free(s->pressure); free(s->dist);
-    free(s->dih); free(s->pending); free(s->seg); free(s->hang_local); free(s->mem);
+    free(s->dih); free(s->pending); free(s->seg); free(s->hang_local); free(s->mem); free(s->load_path);
     free(s);
 }
 
@@ -523,6 +627,7 @@ swb_status swo_create(const swb_structure_definition* d, swo_structure** out) {
         s->dist[i].compliance =
             c->kind == SWB_CONSTRAINT_SEAM_STITCH ? 0.0 : c->compliance;
     }
+    load_path_order(s);
     s->nm = d->membrane_count;
     s->mem = calloc(s->nm ? s->nm : 1, sizeof(Membrane));
     for (uint64_t i = 0; i < s->nm; ++i)
@@ -1103,7 +1208,15 @@ static swb_status substep(swo_structure* s, double dt, const swb_step_settings* 
     }
     for (uint64_t i = 0; i < s->h; ++i) s->dih[i].lambda = 0.0;
     const double inv_dt2 = 1.0 / (dt * dt);
+    /* three quarters of the cable pairs close the substep, the rest run
+     * before the general sweeps of the first iterations (soft_body.cpp:1288-1317) */
+    const int pairs = st->cable_sweep_pairs;
+    const int closing = pairs > 0 ? pairs - pairs / 4 : 0;
+    const int interleaved = pairs - closing;
+    const int iters = st->constraint_iterations > 1 ? st->constraint_iterations : 1;
     for (int it = 0; it < st->constraint_iterations; ++it) {
+        const int cable_pairs = interleaved / iters + (it < interleaved % iters ? 1 : 0);
+        for (int q = 0; q < cable_pairs; ++q) cable_pair(s, inv_dt2);
         for (uint64_t i = 0; i < s->m; ++i) project_distance(s, &s->dist[i], inv_dt2);
         for (uint64_t i = 0; i < s->nm; ++i)
             if (!solve_membrane(s, &s->mem[i], dt))
@@ -1114,6 +1227,10 @@ static swb_status substep(swo_structure* s, double dt, const swb_step_settings* 
             if (r != SWB_OK) return r;
         }
     }
+    if (st->constraint_iterations > 0)
+        for (int q = 0; q < closing; ++q) cable_pair(s, inv_dt2);
+    else
+        for (int q = 0; q < pairs; ++q) cable_pair(s, inv_dt2);
     if (st->constraint_iterations > 0)
         for (uint64_t i = 0; i < s->m; ++i)
             if (s->dist[i].kind == SWB_CONSTRAINT_SEAM_STITCH)
@@ -1140,8 +1257,6 @@ swb_status swo_step(swo_structure* s, const swb_step_settings* st) {
                         "Coupled structural iterations must equal the registered "
                         "suspension lineIterations contract");
     }
-    if (st->cable_sweep_pairs != 0)
-        return fail(SWB_UNSUPPORTED, "oracle port: load-path cable sweeps not restated");
     /* transactional: snapshot the whole state (structure.cpp:807-831) */
     Saved sv;
     sv.nodes = malloc((s->n ? s->n : 1) * sizeof(Node));

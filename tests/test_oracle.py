@@ -196,6 +196,37 @@ def test_port_matches_reference_on_permuted_definition():
     assert np.array_equal(ref.node_states(), port.node_states())
 
 
+# ---- load-path cable sweeps --------------------------------------------------
+@needs_ref
+@pytest.mark.parametrize("pairs,pilot,permuted", [(1, 1, False), (8, 1, False), (96, 1, True), (96, 0, True)])
+def test_port_matches_reference_bitwise_with_cable_pairs(pairs, pilot, permuted):
+    """Graph-depth load-path sweeps (soft_body.cpp:528-629, 1265-1388):
+    a quarter of the pairs interleaved before the first iterations' general
+    sweeps, the rest closing the substep; on a wing with cascaded lines, with
+    and without the pilot, on the generator's constraint order and on the
+    device sweep order (the load-path order follows the definition's).  The
+    outcome must agree too: where the reference rejects a step (96 pairs
+    stretch the lines past the suspension's residual bound here), the
+    restatement rejects it with the same status and both roll back."""
+    d = sw.generate_wing(cells=6, chordwise=12, spanwise_per_cell=2, rib_layers=3, pilot=pilot)
+    if permuted:
+        _, do, ho = sw.plan_schedule(d)
+        d = d.permuted(do, ho)
+    ref, port = O.RefStructure(d), O.PortStructure(d)
+    st = step_settings()
+    st.cable_sweep_pairs = pairs
+    for _ in range(3):
+        outcome = []
+        for s in (ref, port):
+            try:
+                s.step(st)
+                outcome.append(0)
+            except O.OracleError as e:
+                outcome.append(e.status)
+        assert outcome[0] == outcome[1]
+        assert np.array_equal(ref.node_states(), port.node_states())
+
+
 # ---- membranes ---------------------------------------------------------------
 # material of the reference's membrane tests (softwing_material_test.cpp:30-39,
 # simwing_structure_test.cpp:271-274)
