@@ -21,9 +21,9 @@
 //
 // Differences a caller can observe: the state is FP32 on the device (the
 // boundary stays FP64); `workerThreads` is ignored; fabric self-contact,
-// load-path cable sweeps, and membranes on a mesh too large for one cluster
-// are rejected with simwing_b200::Unsupported (a std::logic_error) at
-// construction or step.
+// and load-path cable sweeps or membranes on a mesh too large for one
+// cluster, are rejected with simwing_b200::Unsupported (a std::logic_error)
+// at construction or step.
 #pragma once
 
 #include "simwing_b200.h"

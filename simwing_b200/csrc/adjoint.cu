@@ -307,6 +307,8 @@ struct RolloutImpl {
 
     void forward(const swb_step_settings& st, const double* target, const double* weights, double* out_loss) {
         S->validate_settings(st);
+        if (st.cable_sweep_pairs != 0)
+            raise(SWB_UNSUPPORTED, "differentiable rollouts with load-path cable sweep pairs are not available");
         if (st.substeps != 1) raise(SWB_UNSUPPORTED, "differentiable rollouts take one substep per step");
         const size_t N = S->def.nodes.size();
         double wsum = 0.0;

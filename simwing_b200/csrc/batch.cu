@@ -398,6 +398,7 @@ struct BatchImpl {
         if (steps < 1) raise(SWB_INVALID_ARGUMENT, "steps must be positive");
         const size_t n = size();
         for (size_t i = 0; i < n; ++i) P.members[i]->s.validate_settings(st);
+        if (st.cable_sweep_pairs != 0) raise(SWB_UNSUPPORTED, "load-path cable sweep pairs are not available in batches");
         cuda_check(cudaSetDevice(device), "cudaSetDevice");
         std::vector<char> alive(n, 1);
         std::vector<swb_status> result(n, SWB_OK);

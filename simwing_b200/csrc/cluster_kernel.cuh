@@ -265,6 +265,24 @@ __device__ __forceinline__ void tape_pilot(PilotTape& t, const DevPayloadState& 
 }
 
 // kPacked = false: one structure per cluster (cluster index = structure).
+// One load-path cable pair (soft_body.cpp:1265-1286): the levels of the
+// reverse and the forward pass over this CTA's cable and tie records, a
+// cluster barrier after each level.  Out of line: only runs with pairs.
+__device__ __noinline__ void run_cable_pair(const ClusterInstance& I, uint32_t me, uint32_t rank_base,
+                                            uint32_t x_base, float* lam0, uint32_t first0, float inv_dt2) {
+    cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+    const uint32_t* off = I.pair_offsets + static_cast<size_t>(me) * (I.pair_stages + 1);
+    for (int l = 0; l < I.pair_stages; ++l) {
+        const uint32_t hi = __ldg(off + l + 1);
+        for (uint32_t i = __ldg(off + l) + threadIdx.x; i < hi; i += blockDim.x) {
+            const uint32_t r = __ldg(I.pair_rec + i);
+            apply_record<false>(load_record(I.kind[0].rec, r, r + 1), 0, me, rank_base, x_base, lam0, first0,
+                                inv_dt2);
+        }
+        cluster.sync();
+    }
+}
+
 // kPacked = true: a cluster carries several structures, each on its own
 // contiguous range of ranks, all in lockstep over the cluster's stage count;
 // the structure's buffers follow the launch role and its committed-buffer
@@ -445,7 +463,18 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     // second stage's barrier, before the next iteration reads them.
     const int line_stage = !kPacked && susp_c ? I.line_stage : -1;
     const bool line_warp = line_stage >= 0 && owner && (tid >> 5) == static_cast<int>(blockDim.x >> 5) - 1;
+    // load-path cable sweeps (soft_body.cpp:1288-1317): a quarter of the
+    // pairs runs before the general sweeps of the first iterations, the rest
+    // closes the substep (all of them without iterations)
+    const int pairs = (kPacked || kTape) ? 0 : p.cable_pairs;
+    const int closing_pairs = pairs > 0 ? pairs - pairs / 4 : 0;
+    const int interleaved_pairs = pairs - closing_pairs;
+    const int pair_iters = p.iterations > 1 ? p.iterations : 1;
     for (int it = 0; it < p.iterations; ++it) {
+        if (pairs > 0) {
+            const int n_pairs = interleaved_pairs / pair_iters + (it < interleaved_pairs % pair_iters ? 1 : 0);
+            for (int q = 0; q < n_pairs; ++q) run_cable_pair(I, me, rank_base, x_base, lam0, first0, p.inv_dt2);
+        }
         for (int g = 0; g < stages_c; ++g) {
             if (!kPacked || g < S) {
                 const int kind = kind_of(g);
@@ -503,6 +532,9 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             cluster.sync();
         }
     }
+    // closing cable pairs
+    for (int q = 0; q < (p.iterations > 0 ? closing_pairs : pairs); ++q)
+        run_cable_pair(I, me, rank_base, x_base, lam0, first0, p.inv_dt2);
     // ---- final seam-stitch projections (soft_body.cpp:1389-1405) ----------
     if (p.iterations > 0) {
         for (int s = 0; s < seam_c; ++s) {

@@ -66,7 +66,12 @@ struct ClusterInstance {
     // contact, bending or membranes present, every node free:
     // soft_body.cpp:1192-1202).  Single-structure launches only.
     int momentum_guard;
-    int pad;
+    // Load-path cable sweeps: levels of one pair (reverse pass, then forward
+    // pass), per CTA and level offsets into pair_rec (distance records this
+    // CTA runs).  Single-structure launches only.
+    int pair_stages;
+    const uint32_t* pair_offsets;  // [ctas * (pair_stages + 1)]
+    const uint32_t* pair_rec;
 };
 
 // Rigid pilot as the adjoint sees it: the suspension endpoint nodes are
@@ -133,6 +138,7 @@ struct ClusterParams {
     float dt, inv_dt, inv_dt2, damping;
     float3 gravity, ref_velocity;
     int iterations;
+    int cable_pairs;               // load-path cable sweep pairs per substep (single-structure launches)
     long long copy_budget;
     uint32_t smem_x, smem_v;       // byte offsets of node and force/velocity arrays
     uint32_t smem_offsets;         // byte offset of the CTA's stage offsets

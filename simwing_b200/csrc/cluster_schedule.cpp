@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <numeric>
 
 namespace swb {
@@ -193,6 +194,118 @@ static int element_nodes(const OwnedDefinition& d, int k, size_t i, uint32_t* no
     const swb_triangle_def& t = d.triangles[d.membranes[i].triangle];
     for (int q = 0; q < 3; ++q) nodes[q] = static_cast<uint32_t>(t.nodes[q]);
     return 3;
+}
+
+// Load-path order of the cables and ties (loadPathConstraintOrder,
+// soft_body.cpp:528-629) in sweep order, then the level schedule of one
+// cable pair (reverse pass, forward pass) over the distance records.
+static void build_load_path(const OwnedDefinition& d, ClusterSchedule& S) {
+    const size_t N = d.nodes.size();
+    std::vector<uint8_t> structural(N, 0);
+    std::vector<std::vector<uint32_t>> adj(N);
+    for (size_t v = 0; v < N; ++v) structural[v] = d.nodes[v].fixed ? 1 : 0;
+    for (const auto& t : d.triangles)
+        for (int k = 0; k < 3; ++k) structural[t.nodes[k]] = 1;
+    std::vector<uint64_t> seq;
+    for (uint64_t i : S.distance_order) {  // the device sweep order
+        const auto& c = d.constraints[i];
+        if (c.kind == SWB_CONSTRAINT_DISTANCE || c.kind == SWB_CONSTRAINT_SEAM_STITCH) continue;
+        seq.push_back(i);
+    }
+    for (const auto& c : d.constraints) {
+        if (c.kind == SWB_CONSTRAINT_DISTANCE || c.kind == SWB_CONSTRAINT_SEAM_STITCH) {
+            structural[c.first_node] = structural[c.second_node] = 1;
+            continue;
+        }
+        adj[c.first_node].push_back(static_cast<uint32_t>(c.second_node));
+        adj[c.second_node].push_back(static_cast<uint32_t>(c.first_node));
+    }
+    for (const auto& h : d.dihedrals)
+        for (int k = 0; k < 4; ++k) structural[h.nodes[k]] = 1;
+    S.pair_stages = 0;
+    S.pair_offsets.assign(static_cast<size_t>(S.ctas), 0);
+    S.pair_rec.clear();
+    if (seq.empty()) return;
+    // breadth-first depth from the structural skin; a component without a
+    // structural node is rooted at its heaviest node (first of the smallest
+    // inverse mass)
+    const uint64_t unknown = ~uint64_t{0};
+    std::vector<uint64_t> depth(N, unknown);
+    std::vector<uint32_t> queue;
+    for (size_t v = 0; v < N; ++v)
+        if (structural[v] && !adj[v].empty()) {
+            depth[v] = 0;
+            queue.push_back(static_cast<uint32_t>(v));
+        }
+    size_t head = 0;
+    for (;;) {
+        while (head < queue.size()) {
+            const uint32_t v = queue[head++];
+            for (uint32_t u : adj[v])
+                if (depth[u] == unknown) {
+                    depth[u] = depth[v] + 1;
+                    queue.push_back(u);
+                }
+        }
+        size_t root = N;
+        double smallest = std::numeric_limits<double>::infinity();
+        for (size_t v = 0; v < N; ++v) {
+            const double w = d.nodes[v].fixed ? 0.0 : 1.0 / d.nodes[v].mass;
+            if (depth[v] == unknown && !adj[v].empty() && w < smallest) {
+                root = v;
+                smallest = w;
+            }
+        }
+        if (root == N) break;
+        depth[root] = 0;
+        queue.push_back(static_cast<uint32_t>(root));
+    }
+    auto cdepth = [&](uint64_t i) {
+        return std::max(depth[d.constraints[i].first_node], depth[d.constraints[i].second_node]);
+    };
+    std::stable_sort(seq.begin(), seq.end(), [&](uint64_t a, uint64_t b) { return cdepth(a) < cdepth(b); });
+    // distance record and executing CTA of each definition index
+    const ClusterKind& K = S.kinds[0];
+    std::vector<uint32_t> rec_of(d.constraints.size(), ~0u);
+    std::vector<int> cta_of_rec(K.def_index.size(), 0);
+    for (int c = 0; c < S.ctas; ++c)
+        for (uint32_t r = K.offsets[static_cast<size_t>(c) * (K.stages + 1)];
+             r < K.offsets[static_cast<size_t>(c) * (K.stages + 1) + K.stages]; ++r) {
+            rec_of[K.def_index[r]] = r;
+            cta_of_rec[r] = c;
+        }
+    // levels of the reverse pass, then of the forward pass
+    struct Item { int level, cta; uint32_t rec; };
+    std::vector<Item> items;
+    int levels = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        std::vector<int> last(N, -1);
+        int top = -1;
+        for (size_t k = 0; k < seq.size(); ++k) {
+            const uint64_t i = pass == 0 ? seq[seq.size() - 1 - k] : seq[k];
+            const auto& c = d.constraints[i];
+            const int level = std::max(last[c.first_node], last[c.second_node]) + 1;
+            last[c.first_node] = last[c.second_node] = level;
+            top = std::max(top, level);
+            items.push_back({levels + level, cta_of_rec[rec_of[i]], rec_of[i]});
+        }
+        levels += top + 1;
+    }
+    S.pair_stages = levels;
+    std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
+        if (a.cta != b.cta) return a.cta < b.cta;
+        return a.level < b.level;
+    });
+    S.pair_offsets.assign(static_cast<size_t>(S.ctas) * (levels + 1), 0);
+    size_t at = 0;
+    for (int c = 0; c < S.ctas; ++c) {
+        for (int l = 0; l <= levels; ++l) {
+            while (at < items.size() && items[at].cta == c && items[at].level < l) ++at;
+            S.pair_offsets[static_cast<size_t>(c) * (levels + 1) + l] = static_cast<uint32_t>(at);
+        }
+        while (at < items.size() && items[at].cta == c) ++at;
+    }
+    for (const Item& it : items) S.pair_rec.push_back(it.rec);
 }
 
 // True when a record of global stage g has a node flagged in `attached`.
@@ -397,6 +510,8 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
         }
     }
 
+    build_load_path(d, S);
+
     // seam closing pass: level scheduling in sweep order, executing CTA =
     // owner of the first node
     {
@@ -508,6 +623,45 @@ void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_
         }
         for (size_t i = 0; i < m; ++i)
             if (!seen[i]) fail("constraint not scheduled");
+    }
+    // cable pairs: node-disjoint levels, each record run by the CTA owning
+    // it, every cable and tie once per pass
+    {
+        const ClusterKind& K = S.kinds[0];
+        std::vector<int> owner_of(K.def_index.size(), -1);
+        for (int c = 0; c < C; ++c)
+            for (uint32_t r = K.offsets[static_cast<size_t>(c) * (K.stages + 1)];
+                 r < K.offsets[static_cast<size_t>(c) * (K.stages + 1) + K.stages]; ++r)
+                owner_of[r] = c;
+        size_t load_path = 0;
+        for (const auto& c : d.constraints)
+            load_path += !(c.kind == SWB_CONSTRAINT_DISTANCE || c.kind == SWB_CONSTRAINT_SEAM_STITCH);
+        if (S.pair_stages > 0 && S.pair_offsets.size() != static_cast<size_t>(C) * (S.pair_stages + 1))
+            fail("pair offsets");
+        if (S.pair_rec.size() != 2 * load_path) fail("every cable and tie once per pass of a pair");
+        std::vector<uint8_t> visits(K.def_index.size(), 0);
+        for (int l = 0; l < S.pair_stages; ++l) {
+            ++epoch;
+            for (int c = 0; c < C; ++c)
+                for (uint32_t i = S.pair_offsets[static_cast<size_t>(c) * (S.pair_stages + 1) + l];
+                     i < S.pair_offsets[static_cast<size_t>(c) * (S.pair_stages + 1) + l + 1]; ++i) {
+                    const uint32_t r = S.pair_rec[i];
+                    if (r >= K.def_index.size() || owner_of[r] != c) fail("pair record run by another CTA");
+                    const auto& con = d.constraints[K.def_index[r]];
+                    if (con.kind == SWB_CONSTRAINT_DISTANCE || con.kind == SWB_CONSTRAINT_SEAM_STITCH)
+                        fail("pair record is not a cable or tie");
+                    ++visits[r];
+                    for (uint64_t n : {con.first_node, con.second_node}) {
+                        if (stamp[n] == epoch) fail("pair level is not node-disjoint");
+                        stamp[n] = epoch;
+                    }
+                }
+        }
+        for (size_t r = 0; r < visits.size(); ++r) {
+            const auto& con = d.constraints[K.def_index[r]];
+            const bool lp = !(con.kind == SWB_CONSTRAINT_DISTANCE || con.kind == SWB_CONSTRAINT_SEAM_STITCH);
+            if (visits[r] != (lp ? 2 : 0)) fail("cable pair visits");
+        }
     }
     for (int s = 0; s < S.seam_stages; ++s) {
         ++epoch;

@@ -82,6 +82,16 @@ struct ClusterSchedule {
     int line_stage = -1;
     uint32_t line_owner_records = 0;
     std::vector<uint64_t> distance_order, dihedral_order, membrane_order;
+    // Load-path cable sweeps (soft_body.cpp:528-629, 1265-1317): one pair is
+    // a reverse then a forward pass over the cables and ties in graph-depth
+    // order; each pass is level-scheduled (a constraint one level after the
+    // last earlier one sharing a node), so a level's constraints share no
+    // node and the levels reproduce the serial pass.  pair_stages = levels of
+    // both passes; pair_offsets [ctas * (pair_stages + 1)] index pair_rec,
+    // the distance records (kind 0) each CTA runs per level (its own: their
+    // multipliers are the general sweep's).
+    int pair_stages = 0;
+    std::vector<uint32_t> pair_offsets, pair_rec;
 };
 
 // Colour stages per iteration, all kinds.

@@ -361,6 +361,9 @@ void StructureImpl::upload_cluster_tables() {
     base.seam_ab = dupload(owned, csched.seam_ab, stream);
     base.seam_stages = csched.seam_stages;
     base.line_stage = csched.line_stage;
+    base.pair_stages = csched.pair_stages;
+    base.pair_offsets = dupload(owned, csched.pair_offsets, stream);
+    base.pair_rec = dupload(owned, csched.pair_rec, stream);
     base.momentum_guard = momentum_guard ? 1 : 0;
     cluster_base = base;
 }
@@ -691,8 +694,8 @@ void StructureImpl::validate_settings(const swb_step_settings& st) const {
     if (def.has_suspension && st.constraint_iterations != def.suspension.solver_iterations)
         raise(SWB_INVALID_ARGUMENT,
               "Coupled structural iterations must equal the registered suspension lineIterations contract");
-    if (st.cable_sweep_pairs != 0)
-        raise(SWB_UNSUPPORTED, "load-path cable sweep pairs are not available in this build");
+    if (st.cable_sweep_pairs != 0 && !cluster_mode)
+        raise(SWB_UNSUPPORTED, "load-path cable sweep pairs need the cluster schedule (the mesh does not fit one)");
 }
 
 // Every device table the kernel dereferences must exist before a launch.
@@ -728,6 +731,7 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out)
         cp.ref_velocity = make_float3(st.damping_reference_velocity.x, st.damping_reference_velocity.y,
                                       st.damping_reference_velocity.z);
         cp.iterations = st.constraint_iterations;
+        cp.cable_pairs = st.cable_sweep_pairs;
         if (!cp.instances || in == out) raise(SWB_CUDA_ERROR, "internal error: cluster instance table");
         cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
         cudaLaunchConfig_t cfg{};

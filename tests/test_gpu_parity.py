@@ -158,6 +158,33 @@ def test_free_structures_are_refused_where_the_guard_is_not_built(cuda_device):
         sw.Structure(d, sw.SolverOptions(flags=sw.abi.OPT_GRID))
 
 
+@pytest.mark.parametrize("pairs,pilot", [(8, 1), (96, 0)])
+def test_wing_cable_pairs_per_step_parity(cuda_device, pairs, pilot):
+    """Load-path cable sweeps (soft_body.cpp:528-629, 1265-1388): the
+    device's level-scheduled passes against the serial sweeps of the oracle
+    on the same depth order (taken from the definition permuted into the
+    device sweep order), one step at a time."""
+    d = sw.generate_wing(cells=6, chordwise=12, spanwise_per_cell=2, rib_layers=3, pilot=pilot)
+    st = step_settings()
+    st.cable_sweep_pairs = pairs
+    errs, dev, orc = per_step_errors(d, 3, st)
+    assert max(errs) <= REL_TOL, errs
+
+
+def test_cable_pairs_are_refused_where_they_are_not_built(cuda_device):
+    d = sw.generate_wing(cells=6, chordwise=12, spanwise_per_cell=2, rib_layers=3)
+    st = step_settings()
+    st.cable_sweep_pairs = 4
+    with pytest.raises(sw.Unsupported):
+        sw.Structure(d, sw.SolverOptions(flags=sw.abi.OPT_GRID)).step(st)
+    with sw.Batch([d]) as batch:
+        with pytest.raises(sw.Unsupported):
+            batch.step(st, 1)
+    r = sw.Rollout(sw.Structure(d), 4)
+    with pytest.raises(sw.Unsupported):
+        r.forward(st, np.zeros((d.node_count, 3)), np.ones(d.node_count))
+
+
 def test_patch_600_steps_settled_shape(cuda_device):
     d = sw.generate_patch()
     dev = sw.Structure(d)
