@@ -52,6 +52,10 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--batch-size", type=int, default=64)
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--only-adjoint", action="store_true",
+                   help="run the adjoint leg alone and print its record (profiling)")
+    p.add_argument("--adjoint-steps", type=int, default=240)
+    p.add_argument("--adjoint-interval", type=int, default=16)
     return p.parse_args()
 
 
@@ -147,13 +151,15 @@ def batched_leg(sw, st, count, rank, world, dist, device):
     return out
 
 
-def adjoint_leg(sw, st, device):
+def adjoint_leg(sw, st, device, steps=240, interval=16):
     """Adjoint calibration workload: the wing generator at 20 cells x 30
-    chordwise, settled for 60 steps; the target is the shape after 240
-    steps with every line's rest length scaled by lognormal(0, 0.02); the
-    loss is the mean squared distance of the fabric (triangle) nodes to it;
-    one gradient = a 240-step forward with a checkpoint every 16 steps plus
-    the backward (segment recompute with tape + reverse sweep)."""
+    chordwise, settled for 60 steps; the target is the shape after `steps`
+    (240) steps with every line's rest length scaled by lognormal(0, 0.02);
+    the loss is the mean squared distance of the fabric (triangle) nodes to
+    it; one gradient = a forward of `steps` steps with a checkpoint every
+    `interval` (16) steps plus the backward (segment recompute with tape +
+    reverse sweep).  Launches: 60 settle and `steps` target steps, then two
+    repetitions of `steps` forward, `steps` taping and `steps` reverse."""
     import numpy as np
 
     d = sw.generate_wing(cells=20, chordwise=30)
@@ -173,14 +179,13 @@ def adjoint_leg(sw, st, device):
     t = sw.Structure(perturbed, opts)
     t.write_node_states(state)
     t.write_payload_state(pilot.center_of_mass, pilot.body_to_world, pilot.linear_velocity, pilot.angular_velocity)
-    steps = 240
     for _ in range(steps):
         t.step(st, diagnostics=False)
     target = t.positions()
     t.close()
     weights = np.zeros(s.node_count)
     weights[d.triangles()["nodes"].astype(np.int64).ravel()] = 1.0
-    r = sw.Rollout(s, steps, 16)
+    r = sw.Rollout(s, steps, interval)
     r.forward(st, target, weights)
     r.backward()  # warm-up (allocates the tapes)
     loss = r.forward(st, target, weights)
@@ -189,10 +194,11 @@ def adjoint_leg(sw, st, device):
     cons = d.constraints()
     line_grad = [float(np.sum(g["d_rest"][x] * cons["rest_length"][x]) / np.sum(cons["rest_length"][x])) for x in lines]
     counts = d.counts()
-    out = {"workload": "wing 20 cells x 30 chordwise, settled 60 steps; 240-step rollout, checkpoint every 16 steps; "
+    out = {"workload": f"wing 20 cells x 30 chordwise, settled 60 steps; {steps}-step rollout, checkpoint every "
+                       f"{interval} steps; "
                        "target from line rest lengths x lognormal(0, 0.02); loss = mean squared distance of the "
                        "fabric nodes",
-           "triangles": counts["triangles"], "nodes": counts["nodes"], "steps": steps, "checkpoint_interval": 16,
+           "triangles": counts["triangles"], "nodes": counts["nodes"], "steps": steps, "checkpoint_interval": interval,
            "parameters": {"line_rest_lengths": len(lines), "compliance_classes": 3,
                           "riser_rest_lengths": int(counts["suspension_segments"]), "pilot_mass": 1},
            "loss": loss, "forward_ms": fwd, "backward_ms": bwd,
@@ -354,6 +360,14 @@ def main():
     torch.cuda.set_device(local)
     if args.warmup < 3:
         raise SystemExit("warmup must be >= 3")
+    if args.only_adjoint:
+        if rank == 0:
+            print(json.dumps({"adjoint": adjoint_leg(sw, settings(sw), local, args.adjoint_steps,
+                                                     args.adjoint_interval)}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     definition = sw.generate_wing()
     st = settings(sw)
@@ -413,7 +427,7 @@ def main():
 
     adjoint = None
     if not args.no_adjoint and rank == 0:
-        adjoint = adjoint_leg(sw, st, local)
+        adjoint = adjoint_leg(sw, st, local, args.adjoint_steps, args.adjoint_interval)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
