@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--batch-size", type=int, default=64)
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-membrane-wing", action="store_true")
     p.add_argument("--only-adjoint", action="store_true",
                    help="run the adjoint leg alone and print its record (profiling)")
     p.add_argument("--adjoint-steps", type=int, default=240)
@@ -78,7 +79,7 @@ def replica_rate(units_per_rank, world, seconds):
 
 
 def wing_config():
-    return {"workload": "plain ram-air wing, 40 cells x 60 chordwise (67,428 tri), 48 iterations, 1 substep, "
+    return {"workload": "plain ram-air wing, 40 cells x 60 chordwise (66,936 tri), 48 iterations, 1 substep, "
                         "dt 1/120 s, 30 Pa + gravity, rigid pilot on 2 risers",
             "cells": 40, "chordwise": 60, "iterations": 48, "substeps": 1,
             "l2": "flushed before every timed step (256 MiB write)"}
@@ -97,6 +98,35 @@ def algorithmic_bytes(definition, iterations=48, substeps=1):
     e_s = v.suspension.contents.segment_count if v.suspension else 0
     return substeps * (144 * n + 52 * t + iterations * (88 * e_d + 160 * e_b + 236 * e_m + 52 * e_s)
                        + 4 * (e_d + e_b) + 12 * e_m)
+
+
+def membrane_wing_leg(sw, st, steps, device, flush):
+    """The same wing with its fabric as the reference's scene assembly builds
+    it: one orthotropic membrane element per skin and rib triangle (66,936)
+    and no fabric edge constraints; seams, lines and pilot as before.  Device
+    steps/s from CUDA events, L2 flushed before every timed step."""
+    import torch
+
+    d = sw.generate_wing(fabric=1)
+    s = sw.Structure(d, sw.SolverOptions(device=device))
+    for _ in range(5):
+        s.step(st, diagnostics=False)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        s.step(st, diagnostics=False)
+        times.append(s.last_step_ms())
+    diag = s.diagnostics()
+    rep = s.schedule_report()
+    s.close()
+    total = float(sum(times))
+    return {"workload": "ram-air wing, 40 cells x 60 chordwise, fabric as membrane elements (66,936), 48 iterations",
+            "membranes": d.counts()["membranes"], "constraints": d.counts()["constraints"],
+            "stages_per_iteration": rep.local_stages_per_iteration, "steps": steps,
+            "ms_per_step": total / steps, "wing_steps_per_s": steps / (total / 1000.0),
+            "max_membrane_strain": diag.maximum_absolute_membrane_strain, "finite": bool(diag.finite)}
 
 
 def batched_leg(sw, st, count, rank, world, dist, device):
@@ -429,6 +459,10 @@ def main():
     if not args.no_adjoint and rank == 0:
         adjoint = adjoint_leg(sw, st, local, args.adjoint_steps, args.adjoint_interval)
 
+    membrane_wing = None
+    if not args.no_membrane_wing and rank == 0:
+        membrane_wing = membrane_wing_leg(sw, st, min(args.steps, 50), local, flush)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu_value, kind, used = cpu_reference_run(definition, args.cpu_sample_steps, 0)
@@ -455,6 +489,7 @@ def main():
             "final_diagnostics": {"finite": bool(diag.finite), "max_distance_error": diag.maximum_distance_error},
             "batched": batched,
             "adjoint": adjoint,
+            "membrane_wing": membrane_wing,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -702,6 +702,13 @@ typedef struct swb_wing_params {
     double aspect_ratio;      /* 0 = derive from span and chord            */
     double compliance_jitter; /* sigma of lognormal compliance multiplier  */
     uint64_t seed;
+    uint32_t fabric;          /* 0 = one distance constraint per skin and
+                                 rib edge; 1 = one orthotropic membrane
+                                 element per skin and rib triangle and no
+                                 fabric edge constraints, as the reference's
+                                 scene assembly builds the canopy
+                                 (scene_structure.cpp:1125-1151)           */
+    uint32_t reserved;
 } swb_wing_params;
 
 void swb_default_patch_params(swb_patch_params* out);

@@ -2,7 +2,9 @@
 
 ctypes loaders for the CPU checkers:
   * PortStructure -- oracle/liboracle.so, the plain-C FP64 restatement of
-    the reference step (oracle/xpbd_oracle.c);
+    the reference step (oracle/xpbd_oracle.c); with float_vectors=True,
+    oracle/liboracle_f32.so, the same step with every vector result rounded
+    to FP32 (the tests' measure of a configuration's FP32 sensitivity);
   * RefStructure  -- oracle/_ref/libswref.so, the reference's own
     softwing core + Structure adapter compiled from source
     (oracle/ref_shim.cpp, oracle/Makefile);
@@ -23,6 +25,7 @@ from simwing_b200 import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_PATH = os.path.join(HERE, "liboracle.so")
+PORT_F32_PATH = os.path.join(HERE, "liboracle_f32.so")
 REF_PATH = os.path.join(HERE, "_ref", "libswref.so")
 ADJOINT_PATH = os.path.join(HERE, "libadjoint.so")
 
@@ -78,10 +81,11 @@ def ref_available() -> bool:
     return os.path.exists(REF_PATH)
 
 
-def port_library() -> C.CDLL:
-    if "port" not in _libs:
-        _libs["port"] = abi.bind(C.CDLL(PORT_PATH), _PORT)
-    return _libs["port"]
+def port_library(float_vectors: bool = False) -> C.CDLL:
+    key = "port_f32" if float_vectors else "port"
+    if key not in _libs:
+        _libs[key] = abi.bind(C.CDLL(PORT_F32_PATH if float_vectors else PORT_PATH), _PORT)
+    return _libs[key]
 
 
 def ref_library() -> C.CDLL:
@@ -143,35 +147,40 @@ class _Base:
 
 
 class PortStructure(_Base):
-    """The C restatement (FP64)."""
+    """The C restatement (FP64; float_vectors=True rounds every vector
+    result to FP32)."""
     _prefix = "swo_"
 
+    def __init__(self, definition, float_vectors: bool = False):
+        self._float_vectors = float_vectors
+        super().__init__(definition)
+
     def _lib(self):
-        return port_library()
+        return port_library(self._float_vectors)
 
     def step(self, settings):
         """One structure step; returns the diagnostics after it (as the
         reference adapter's step does)."""
-        self._check(port_library().swo_step(self._h, C.byref(settings)))
+        self._check(self._lib().swo_step(self._h, C.byref(settings)))
         return self.diagnostics()
 
     def write_node_states(self, states):
         s = np.ascontiguousarray(states, dtype=np.float64)
-        self._check(port_library().swo_write_nodes(self._h, s.ctypes.data, self.node_count))
+        self._check(self._lib().swo_write_nodes(self._h, s.ctypes.data, self.node_count))
 
     def payload(self):
         p = abi.PayloadState()
         w = abi.Wrench()
         r = C.c_double()
-        self._check(port_library().swo_read_payload(self._h, C.byref(p), C.byref(w), C.byref(r)))
+        self._check(self._lib().swo_read_payload(self._h, C.byref(p), C.byref(w), C.byref(r)))
         return p, w, r.value
 
     def write_payload(self, p):
-        self._check(port_library().swo_write_payload(self._h, C.byref(p)))
+        self._check(self._lib().swo_write_payload(self._h, C.byref(p)))
 
     def segment_lambdas(self, n):
         out = np.zeros(n)
-        self._check(port_library().swo_read_segment_lambdas(self._h, out.ctypes.data, n))
+        self._check(self._lib().swo_read_segment_lambdas(self._h, out.ctypes.data, n))
         return out
 
 

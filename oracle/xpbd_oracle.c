@@ -50,7 +50,18 @@ typedef struct { double x, y, z; } V3;
 typedef struct { double w, x, y, z; } Q;
 typedef struct { double v[9]; } M3;
 
+#ifdef SWO_FLOAT_VECTORS
+/* The same algorithm with every vector result (positions, velocities, edges,
+   normals, corrections) rounded to FP32 and the scalar arithmetic in FP64:
+   the tests measure with it how strongly a configuration amplifies FP32
+   rounding, which bounds what an FP32 solver can agree to. */
+static V3 v3(double x, double y, double z) { V3 r = {(float)x, (float)y, (float)z}; return r; }
+/* an FP32-rounded unit direction, checked as the FP32 device checks it */
+static const double kUnitTolerance = 1.0e-5;
+#else
 static V3 v3(double x, double y, double z) { V3 r = {x, y, z}; return r; }
+static const double kUnitTolerance = 1.0e-10; /* suspension.cpp:1140 */
+#endif
 static V3 add(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
 static V3 sub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
 static V3 mul(V3 a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
@@ -1008,7 +1019,7 @@ static swb_status line_iteration(swo_structure* s, double dt) {
         /* projectUnilateralLine (suspension.cpp:1125-1163) */
         if (!(l > 0.0) || !(g->commanded > 0.0) || !(g->stiffness > 0.0) ||
             !(dt > 0.0) || !(g->lambda >= 0.0) || !isfinite(g->lambda) ||
-            fabs(len(fg) - 1.0) > 1.0e-10)
+            fabs(len(fg) - 1.0) > kUnitTolerance)
             return fail(SWB_SUSPENSION_ERROR, "invalid unilateral line projection input");
         const double eff = effective_inverse_mass(fw, fr && !ff, fo, &invI, fg) +
                            effective_inverse_mass(tw, tr && !tf, to, &invI, neg(fg));

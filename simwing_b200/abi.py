@@ -186,7 +186,8 @@ class WingParams(C.Structure):
                 ("bend_rigidity", C.c_double), ("line_compliance_scale", C.c_double), ("pressure", C.c_double),
                 ("line_levels", C.c_uint32), ("line_particles", C.c_uint32), ("line_rows", C.c_uint32),
                 ("pilot", C.c_uint32), ("pilot_mass", C.c_double), ("aspect_ratio", C.c_double),
-                ("compliance_jitter", C.c_double), ("seed", C.c_uint64)]
+                ("compliance_jitter", C.c_double), ("seed", C.c_uint64), ("fabric", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 # status codes

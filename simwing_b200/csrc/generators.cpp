@@ -110,6 +110,34 @@ struct Builder {
             }
     }
 
+    // One membrane element per triangle of [first, last): the chart is the
+    // triangle's own rest shape in its plane, warp along `warp` projected
+    // into the plane (so the element starts unstrained and its chart is
+    // positively oriented).
+    void membranes(size_t first, size_t last, V warp, const swb_membrane_material& material) {
+        for (size_t t = first; t < last; ++t) {
+            const V a = design[d.triangles[t].nodes[0]], b = design[d.triangles[t].nodes[1]],
+                    c = design[d.triangles[t].nodes[2]];
+            V n = cross(b - a, c - a);
+            n = n * (1.0 / length(n));
+            V u = warp - n * dot(warp, n);
+            if (!(length(u) > 1e-9)) u = b - a;
+            u = u * (1.0 / length(u));
+            const V v = cross(n, u);
+            swb_membrane_def m{};
+            m.triangle = t;
+            m.chart[0][0] = 0.0;
+            m.chart[0][1] = 0.0;
+            m.chart[1][0] = dot(b - a, u);
+            m.chart[1][1] = dot(b - a, v);
+            m.chart[2][0] = dot(c - a, u);
+            m.chart[2][1] = dot(c - a, v);
+            m.material = material;
+            m.role = SWB_ROLE_BULK;
+            d.membranes.push_back(m);
+        }
+    }
+
     // assembleBending for one sheet: triangles [first, last).  When
     // `fixed_compliance` >= 0 it replaces the series-strip formula.
     void dihedrals(size_t first, size_t last, double rigidity,
@@ -299,7 +327,7 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
     return guarded([&] {
         if (!p || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
         if (p->cells < 1 || p->chordwise < 4 || p->spanwise_per_cell < 1 ||
-            p->rib_layers < 1 || !(p->root_chord > 0) || !(p->thickness > 0) ||
+            p->rib_layers < 1 || p->fabric > 1 || !(p->root_chord > 0) || !(p->thickness > 0) ||
             !(p->areal_density > 0) || p->skin_compliance < 0 ||
             !(p->bend_rigidity > 0) || p->line_rows > 4 || p->line_levels < 1 ||
             p->line_levels > 6 || p->line_particles > 64)
@@ -365,7 +393,19 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                     b.triangle(A, Cn, D, p->pressure, p->areal_density);
                 }
             const size_t skin_last = def->def.triangles.size();
-            b.edge_constraints(skin_first, skin_last, skin_compliance);
+            // fabric: edge constraints, or membrane elements (ripstop nylon:
+            // warp along the chord, N/m)
+            swb_membrane_material fabric{};
+            fabric.warp_stiffness = 4.0e4;
+            fabric.weft_stiffness = 3.0e4;
+            fabric.coupling_stiffness = 6.0e3;
+            fabric.shear_stiffness = 1.5e3;
+            fabric.compression_stiffness_ratio = 1.0;
+            const V chordwise{1.0, 0.0, 0.0};
+            if (p->fabric == 1)
+                b.membranes(skin_first, skin_last, chordwise, fabric);
+            else
+                b.edge_constraints(skin_first, skin_last, skin_compliance);
             b.dihedrals(skin_first, skin_last, p->bend_rigidity, -1.0);
 
             // Ribs with their own nodes, sewn to the skin.  The last rib
@@ -406,7 +446,10 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                     b.triangle(col[(J - 1) * (L + 1) + l], te, col[(J - 1) * (L + 1) + l + 1],
                                rib_pressure, p->areal_density);
                 const size_t last = def->def.triangles.size();
-                b.edge_constraints(first, last, skin_compliance);
+                if (p->fabric == 1)
+                    b.membranes(first, last, chordwise, fabric);
+                else
+                    b.edge_constraints(first, last, skin_compliance);
                 b.dihedrals(first, last, p->bend_rigidity, -1.0);
                 // Seam: the rib boundary loop (skin loop order, skipping the
                 // skin station next to the trailing edge on both surfaces)

@@ -289,6 +289,39 @@ def test_port_matches_reference_bitwise_on_membrane_patch(option, pinned):
     assert dr.maximum_membrane_residual > 0.0
 
 
+@needs_ref
+def test_port_matches_reference_bitwise_on_membrane_wing():
+    """The wing with its fabric as membrane elements (the reference scene
+    assembly's form), lines and pilot: node states, pilot and membrane
+    diagnostics bit for bit."""
+    d = sw.generate_wing(cells=6, chordwise=12, spanwise_per_cell=2, rib_layers=3, fabric=1)
+    assert d.view.membrane_count == d.view.triangle_count
+    ref, port = O.RefStructure(d), O.PortStructure(d)
+    st = step_settings()
+    for _ in range(3):
+        dr = ref.step(st)
+        dp = port.step(st)
+    assert np.array_equal(ref.node_states(), port.node_states())
+    assert dr.maximum_absolute_membrane_strain == dp.maximum_absolute_membrane_strain
+    assert dr.maximum_membrane_residual == dp.maximum_membrane_residual
+
+
+def test_float_vector_port_rounds_to_fp32_and_stays_close():
+    """The FP32-rounding build of the port (the tests' sensitivity measure)
+    stores FP32-representable positions and stays within FP32 agreement of
+    the FP64 port on a well-conditioned membrane patch."""
+    d = sw.generate_patch(membranes=2)
+    f64, f32 = O.PortStructure(d), O.PortStructure(d, float_vectors=True)
+    st = step_settings()
+    for _ in range(3):
+        f64.step(st)
+        f32.step(st)
+    a, b = f32.node_states()[:, 0, :], f64.node_states()[:, 0, :]
+    assert np.array_equal(a, a.astype(np.float32).astype(np.float64))
+    diff = float(np.abs(a - b).max())
+    assert 0.0 < diff <= 1e-5 * max(1.0, float(np.abs(b).max()))
+
+
 def test_golden_trajectories():
     """Committed FP64 fixtures produced by the reference build
     (tests/golden/make_golden.py)."""
