@@ -745,6 +745,130 @@ uint64_t swb_definition_fingerprint(const swb_structure_definition* definition);
 /* Validation only (structure.cpp:102-455). */
 swb_status swb_validate_definition(const swb_structure_definition* definition);
 
+/* ------------------------------------------------------------------------ */
+/* Contact building blocks on the device, in FP64 (softwing contact.h).      */
+/* The fabric self-contact of a definition (structure.cpp:626-636) is one    */
+/* contact surface over all triangles, paired with itself: vertex-triangle   */
+/* features of every surface vertex against every triangle not holding it,  */
+/* and edge-edge features of every two surface edges that share no node.     */
+/* ------------------------------------------------------------------------ */
+
+/* ContactFeatureKind (contact.h:26-30) */
+#define SWB_FEATURE_VERTEX_TRIANGLE 0u
+#define SWB_FEATURE_EDGE_EDGE 1u
+#define SWB_FEATURE_SEGMENT_TRIANGLE 2u
+
+/* GeometryQueryStatus (contact.h:32-37) */
+#define SWB_GEOMETRY_CERTIFIED 0u
+#define SWB_GEOMETRY_DEGENERATE 1u
+#define SWB_GEOMETRY_NON_FINITE 2u
+#define SWB_GEOMETRY_UNCERTIFIABLE 3u
+
+/* CcdState (contact.h:153-158) */
+#define SWB_CCD_NO_IMPACT 0u
+#define SWB_CCD_IMPACT 1u
+#define SWB_CCD_INITIALLY_PROXIMATE 2u
+#define SWB_CCD_INDETERMINATE 3u
+
+/* ContactFeatureKey (contact.h:95-101); keys order lexicographically by
+ * (pair, kind, first[0..2], second[0..2]).  Vertex-triangle: first =
+ * {vertex, 0, 0}, second = {triangle, 0, 0}; edge-edge: first and second
+ * are the two edges {a, b, 0} (a < b), the lesser edge first. */
+typedef struct swb_contact_key {
+    uint64_t pair;
+    uint32_t kind;
+    uint32_t reserved;
+    uint64_t first[3];
+    uint64_t second[3];
+} swb_contact_key;
+
+/* CcdSettings (contact.h:160-165) */
+typedef struct swb_ccd_settings {
+    int32_t conservative_iterations;   /* 32                                 */
+    int32_t interval_subdivisions;     /* 256; at most SWB_CCD_MAX_SUBDIVISIONS */
+    double time_tolerance;             /* 1e-8                               */
+    double distance_tolerance;         /* 1e-10                              */
+} swb_ccd_settings;
+
+/* The interval fallback keeps its pending intervals in device scratch of
+ * interval_subdivisions + 1 entries per query; larger budgets are refused. */
+#define SWB_CCD_MAX_SUBDIVISIONS 4096
+
+void swb_default_ccd_settings(swb_ccd_settings* out);
+
+/* ClosestFeatureResult (contact.h:53-68); features are ClosestFeatureClass
+ * values (contact.h:39-51: Point 0, SegmentStart 1, SegmentEnd 2,
+ * SegmentInterior 3, TriangleVertex0..2 4-6, TriangleEdge01 7,
+ * TriangleEdge12 8, TriangleEdge20 9, TriangleFace 10). */
+typedef struct swb_closest_result {
+    uint32_t status;
+    uint32_t first_feature;
+    uint32_t second_feature;
+    uint32_t reserved;
+    double first_point[3];
+    double second_point[3];
+    double first_weights[3];
+    double second_weights[3];
+    double normal[3];
+    double distance;
+    double gap;
+} swb_closest_result;
+
+/* CcdResult (contact.h:167-176) */
+typedef struct swb_ccd_result {
+    uint32_t state;
+    int32_t conservative_iterations;
+    int32_t interval_subdivisions;
+    uint32_t used_interval_fallback;
+    double time_of_impact;
+    double bracket_lower;
+    double bracket_upper;
+    swb_closest_result geometry;
+} swb_ccd_result;
+
+/* Candidate features of the definition's fabric self-contact pair for the
+ * motion previous -> current (node_count x 3 doubles each): the eligible
+ * features whose swept, separation-expanded AABBs (sweptExpandedAabb,
+ * contact.cpp:488-526, separation = 2 x half_thickness) overlap on all
+ * three axes, in key order -- the candidate list of SoftBody's contact
+ * iteration (contact.cpp:1057-1290 with sweepAndPruneContactPairs,
+ * contact.cpp:528-668).  possible / excluded count the feature pairs before
+ * and removed by the topology filter.  When the list exceeds `capacity`
+ * only the count is written and the call returns SWB_OUT_OF_RANGE. */
+swb_status swb_contact_candidates(const swb_structure_definition* definition,
+                                  double half_thickness,
+                                  const double* previous,
+                                  const double* current,
+                                  swb_contact_key* keys,
+                                  uint64_t capacity,
+                                  uint64_t* candidate_count,
+                                  uint64_t* possible_count,
+                                  uint64_t* excluded_count);
+
+/* closestVertexTriangle / closestEdgeEdge (contact.cpp:141-305) for `count`
+ * features of one kind.  Each feature reads 3 points (9 doubles) from
+ * `first` and from `second` (unused points ignored: a vertex is first[0],
+ * an edge first[0..1]). */
+swb_status swb_contact_closest(uint32_t kind,
+                               uint64_t count,
+                               const double* first,
+                               const double* second,
+                               double separation,
+                               swb_closest_result* results);
+
+/* sweptContact (contact.cpp:669-945) for `count` features of one kind:
+ * linear motion of each primitive from *_previous to *_current (9 doubles
+ * per feature and side, as above). */
+swb_status swb_contact_sweep(uint32_t kind,
+                             uint64_t count,
+                             const double* first_previous,
+                             const double* first_current,
+                             const double* second_previous,
+                             const double* second_current,
+                             double separation,
+                             const swb_ccd_settings* settings,
+                             swb_ccd_result* results);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -60,6 +60,13 @@ _REF = {
     "swref_read_suspension": (C.c_int, [C.c_void_p, P(abi.PayloadState), C.c_void_p, C.c_uint64]),
     "swref_colouring": (C.c_int, [P(abi.StructureDefinition), C.c_void_p, C.c_void_p, C.c_uint64,
                                   P(C.c_uint64), P(C.c_uint64)]),
+    "swref_contact_candidates": (C.c_int, [P(abi.StructureDefinition), C.c_double, C.c_void_p, C.c_void_p,
+                                           P(abi.ContactKey), C.c_uint64, P(C.c_uint64), P(C.c_uint64),
+                                           P(C.c_uint64)]),
+    "swref_contact_closest": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_double,
+                                        P(abi.ClosestResult)]),
+    "swref_contact_sweep": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_double, P(abi.CcdSettings), P(abi.CcdResult)]),
 }
 
 _ADJ = {
@@ -284,3 +291,44 @@ def rollout_gradient(definition, settings, steps, target, weights, forces=None, 
     out["d_dihedral_comp"], out["d_segment_rest"] = out["d_dihedral_comp"][:h], out["d_segment_rest"][:ns]
     out["loss"], out["d_mass"] = loss.value, mass.value
     return out
+
+
+def _ref_check(status):
+    if status != 0:
+        raise OracleError(status, ref_library().swref_last_error().decode())
+
+
+def ref_contact_candidates(definition, half_thickness, previous, current):
+    """The reference's candidate keys of the fabric self-contact pair (one
+    SoftBody contact iteration, read through its audit hook); returns
+    (keys, possible, excluded)."""
+    lib = ref_library()
+    prev = np.ascontiguousarray(previous, dtype=np.float64)
+    cur = np.ascontiguousarray(current, dtype=np.float64)
+    n, possible, excluded = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    status = lib.swref_contact_candidates(definition.pointer, half_thickness, prev.ctypes.data, cur.ctypes.data,
+                                          None, 0, C.byref(n), C.byref(possible), C.byref(excluded))
+    if status not in (abi.OK, abi.OUT_OF_RANGE):
+        _ref_check(status)
+    keys = (abi.ContactKey * max(n.value, 1))()
+    _ref_check(lib.swref_contact_candidates(definition.pointer, half_thickness, prev.ctypes.data, cur.ctypes.data,
+                                            keys, n.value, C.byref(n), C.byref(possible), C.byref(excluded)))
+    return list(keys)[: n.value], possible.value, excluded.value
+
+
+def ref_contact_closest(kind, first, second, separation):
+    f = np.ascontiguousarray(first, dtype=np.float64).reshape(-1, 9)
+    s = np.ascontiguousarray(second, dtype=np.float64).reshape(-1, 9)
+    out = (abi.ClosestResult * max(len(f), 1))()
+    _ref_check(ref_library().swref_contact_closest(kind, len(f), f.ctypes.data, s.ctypes.data, separation, out))
+    return list(out)[: len(f)]
+
+
+def ref_contact_sweep(kind, first_previous, first_current, second_previous, second_current, separation, settings):
+    arrays = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 9)
+              for a in (first_previous, first_current, second_previous, second_current)]
+    n = len(arrays[0])
+    out = (abi.CcdResult * max(n, 1))()
+    _ref_check(ref_library().swref_contact_sweep(kind, n, *[a.ctypes.data for a in arrays], separation,
+                                                 C.byref(settings), out))
+    return list(out)[:n]

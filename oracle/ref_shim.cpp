@@ -29,6 +29,20 @@
 #include <string>
 #include <vector>
 
+// The reference's own test hook (soft_body.h:22, 504): runs one contact
+// iteration of a body and reads the candidate keys its broadphase streamed.
+namespace softwing {
+struct ContactAuditTestAccess {
+    static void begin(SoftBody& body) { body.beginContactSubstep(); }
+    static void iterate(SoftBody& body, double dt, const StepSettings& settings) {
+        body.solveContactIteration(dt, settings);
+    }
+    static const std::vector<ContactFeatureKey>& candidates(const SoftBody& body) {
+        return body.contactAudit_.iterationCandidateKeys;
+    }
+};
+}  // namespace softwing
+
 namespace {
 
 thread_local std::string g_error;
@@ -454,6 +468,175 @@ swb_status swref_colouring(const swb_structure_definition* d,
         *colour_count =
             view.colourOffsets.empty() ? 0 : view.colourOffsets.size() - 1;
         *parallel_colours = report.parallelColours;
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+// Candidate keys of the fabric self-contact pair (structure.cpp:626-636) for
+// the motion previous -> current: one SoftBody contact iteration
+// (contact.cpp:1057-1290) on a body holding the definition's nodes and
+// triangles, read back through the reference's audit hook.  possible /
+// excluded from SoftBody::contactTopology (contact.cpp:2448).
+swb_status swref_contact_candidates(const swb_structure_definition* d,
+                                    double half_thickness,
+                                    const double* previous,
+                                    const double* current,
+                                    swb_contact_key* keys,
+                                    uint64_t capacity,
+                                    uint64_t* count,
+                                    uint64_t* possible,
+                                    uint64_t* excluded) {
+    try {
+        softwing::SoftBody body;
+        for (uint64_t i = 0; i < d->node_count; ++i) {
+            const swb_node_def& n = d->nodes[i];
+            const softwing::Vec3 p{n.position.x, n.position.y, n.position.z};
+            if (n.fixed)
+                body.addFixedNode(p);
+            else
+                body.addNode(p, n.mass);
+        }
+        for (uint64_t i = 0; i < d->triangle_count; ++i)
+            body.addTriangle(d->triangles[i].nodes[0], d->triangles[i].nodes[1],
+                             d->triangles[i].nodes[2]);
+        const softwing::ContactSurfaceHandle surface = body.addContactSurface(
+            body.surfaceGroup(0, d->triangle_count), half_thickness);
+        const softwing::ContactPairHandle pair = body.addContactPair(
+            surface.collider(), surface.collider(), {0.0, 0.0, 0.0});
+        const softwing::ContactTopologyReport topology = body.contactTopology(pair);
+        for (uint64_t i = 0; i < d->node_count; ++i) {
+            softwing::Node& n = body.nodes()[i];
+            n.previousPosition = {previous[3 * i], previous[3 * i + 1], previous[3 * i + 2]};
+            n.position = {current[3 * i], current[3 * i + 1], current[3 * i + 2]};
+        }
+        softwing::ContactAuditTestAccess::begin(body);
+        softwing::StepSettings settings;
+        try {
+            softwing::ContactAuditTestAccess::iterate(body, 1.0 / 120.0, settings);
+        } catch (const softwing::ContactStepError&) {
+            // The candidate list is complete before any feature is queried.
+        }
+        const auto& found = softwing::ContactAuditTestAccess::candidates(body);
+        *count = found.size();
+        if (possible) *possible = topology.possibleCount;
+        if (excluded) *excluded = topology.excludedCount;
+        if (found.size() > capacity)
+            throw std::out_of_range("candidate capacity too small");
+        for (std::size_t k = 0; k < found.size(); ++k) {
+            swb_contact_key& out = keys[k];
+            std::memset(&out, 0, sizeof out);
+            out.pair = found[k].pair;
+            out.kind = static_cast<uint32_t>(found[k].kind);
+            for (int j = 0; j < 3; ++j) {
+                out.first[j] = found[k].firstPrimitive[j];
+                out.second[j] = found[k].secondPrimitive[j];
+            }
+        }
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+namespace {
+
+softwing::Vec3 vec_at(const double* p, uint64_t feature, int point) {
+    const double* q = p + 9 * feature + 3 * point;
+    return {q[0], q[1], q[2]};
+}
+
+void store_vec(double* out, const softwing::Vec3& v) {
+    out[0] = v.x;
+    out[1] = v.y;
+    out[2] = v.z;
+}
+
+void store_closest(swb_closest_result& o, const softwing::ClosestFeatureResult& r) {
+    std::memset(&o, 0, sizeof o);
+    o.status = static_cast<uint32_t>(r.status);
+    o.first_feature = static_cast<uint32_t>(r.firstFeature);
+    o.second_feature = static_cast<uint32_t>(r.secondFeature);
+    store_vec(o.first_point, r.firstPoint);
+    store_vec(o.second_point, r.secondPoint);
+    for (int k = 0; k < 3; ++k) {
+        o.first_weights[k] = r.firstWeights[k];
+        o.second_weights[k] = r.secondWeights[k];
+    }
+    store_vec(o.normal, r.normal);
+    o.distance = r.distance;
+    o.gap = r.gap;
+}
+
+}  // namespace
+
+// closestVertexTriangle / closestEdgeEdge (contact.h:70-93), per feature.
+swb_status swref_contact_closest(uint32_t kind, uint64_t count,
+                                 const double* first, const double* second,
+                                 double separation,
+                                 swb_closest_result* results) {
+    try {
+        for (uint64_t i = 0; i < count; ++i) {
+            const softwing::ClosestFeatureResult r =
+                kind == SWB_FEATURE_VERTEX_TRIANGLE
+                    ? softwing::closestVertexTriangle(
+                          vec_at(first, i, 0), vec_at(second, i, 0),
+                          vec_at(second, i, 1), vec_at(second, i, 2), separation)
+                    : softwing::closestEdgeEdge(
+                          vec_at(first, i, 0), vec_at(first, i, 1),
+                          vec_at(second, i, 0), vec_at(second, i, 1), separation);
+            store_closest(results[i], r);
+        }
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+// sweptContact (contact.h:265-270), per feature.
+swb_status swref_contact_sweep(uint32_t kind, uint64_t count,
+                               const double* first_previous,
+                               const double* first_current,
+                               const double* second_previous,
+                               const double* second_current,
+                               double separation,
+                               const swb_ccd_settings* settings,
+                               swb_ccd_result* results) {
+    try {
+        softwing::CcdSettings cs;
+        cs.conservativeIterations = settings->conservative_iterations;
+        cs.intervalSubdivisions = settings->interval_subdivisions;
+        cs.timeTolerance = settings->time_tolerance;
+        cs.distanceTolerance = settings->distance_tolerance;
+        const bool vt = kind == SWB_FEATURE_VERTEX_TRIANGLE;
+        const auto kindValue = vt ? softwing::ContactFeatureKind::VertexTriangle
+                                  : softwing::ContactFeatureKind::EdgeEdge;
+        for (uint64_t i = 0; i < count; ++i) {
+            softwing::LinearContactPrimitive f, s;
+            f.count = vt ? 1 : 2;
+            s.count = vt ? 3 : 2;
+            for (std::size_t k = 0; k < f.count; ++k) {
+                f.previous[k] = vec_at(first_previous, i, static_cast<int>(k));
+                f.current[k] = vec_at(first_current, i, static_cast<int>(k));
+            }
+            for (std::size_t k = 0; k < s.count; ++k) {
+                s.previous[k] = vec_at(second_previous, i, static_cast<int>(k));
+                s.current[k] = vec_at(second_current, i, static_cast<int>(k));
+            }
+            const softwing::CcdResult r =
+                softwing::sweptContact(kindValue, f, s, separation, cs);
+            swb_ccd_result& o = results[i];
+            std::memset(&o, 0, sizeof o);
+            o.state = static_cast<uint32_t>(r.state);
+            o.conservative_iterations = r.conservativeIterations;
+            o.interval_subdivisions = r.intervalSubdivisions;
+            o.used_interval_fallback = r.usedIntervalFallback ? 1u : 0u;
+            o.time_of_impact = r.timeOfImpact;
+            o.bracket_lower = r.bracketLower;
+            o.bracket_upper = r.bracketUpper;
+            store_closest(o.geometry, r.geometry);
+        }
         return SWB_OK;
     } catch (...) {
         return translate();

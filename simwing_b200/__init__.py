@@ -372,6 +372,53 @@ def reference_colouring(definition: Definition):
     return order[:m], offsets[: colours.value + 1 if m else 0], int(parallel.value)
 
 
+def CcdSettings(**overrides) -> abi.CcdSettings:
+    s = abi.CcdSettings()
+    abi.library().swb_default_ccd_settings(C.byref(s))
+    for k, v in overrides.items():
+        setattr(s, k, v)
+    return s
+
+
+def contact_candidates(definition: Definition, half_thickness: float, previous, current):
+    """Candidate features of the definition's fabric self-contact pair on the
+    device (swb_contact_candidates); returns (keys, possible, excluded)."""
+    lib = abi.library()
+    prev = np.ascontiguousarray(previous, dtype=np.float64)
+    cur = np.ascontiguousarray(current, dtype=np.float64)
+    n, possible, excluded = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    status = lib.swb_contact_candidates(definition.pointer, half_thickness, prev.ctypes.data, cur.ctypes.data,
+                                        None, 0, C.byref(n), C.byref(possible), C.byref(excluded))
+    if status not in (abi.OK, abi.OUT_OF_RANGE):
+        _check(status)
+    keys = (abi.ContactKey * max(n.value, 1))()
+    _check(lib.swb_contact_candidates(definition.pointer, half_thickness, prev.ctypes.data, cur.ctypes.data, keys,
+                                      n.value, C.byref(n), C.byref(possible), C.byref(excluded)))
+    return list(keys)[: n.value], possible.value, excluded.value
+
+
+def contact_closest(kind: int, first, second, separation: float):
+    """closestVertexTriangle / closestEdgeEdge on the device, 9 doubles per
+    feature and side (swb_contact_closest)."""
+    f = np.ascontiguousarray(first, dtype=np.float64).reshape(-1, 9)
+    s = np.ascontiguousarray(second, dtype=np.float64).reshape(-1, 9)
+    out = (abi.ClosestResult * max(len(f), 1))()
+    _check(abi.library().swb_contact_closest(kind, len(f), f.ctypes.data, s.ctypes.data, separation, out))
+    return list(out)[: len(f)]
+
+
+def contact_sweep(kind: int, first_previous, first_current, second_previous, second_current, separation: float,
+                  settings: abi.CcdSettings | None = None):
+    """sweptContact on the device (swb_contact_sweep)."""
+    arrays = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 9)
+              for a in (first_previous, first_current, second_previous, second_current)]
+    n = len(arrays[0])
+    out = (abi.CcdResult * max(n, 1))()
+    _check(abi.library().swb_contact_sweep(kind, n, *[a.ctypes.data for a in arrays], separation,
+                                           C.byref(settings or CcdSettings()), out))
+    return list(out)[:n]
+
+
 def plan_schedule(definition: Definition, options: abi.SolverOptions | None = None):
     """Host-only schedule build + invariant check; returns (report,
     distance sweep order, dihedral sweep order)."""

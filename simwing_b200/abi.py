@@ -103,6 +103,35 @@ class StructureDefinition(C.Structure):
                 ("suspension", C.POINTER(SuspensionDef))]
 
 
+FEATURE_VERTEX_TRIANGLE, FEATURE_EDGE_EDGE, FEATURE_SEGMENT_TRIANGLE = 0, 1, 2
+GEOMETRY_CERTIFIED, GEOMETRY_DEGENERATE, GEOMETRY_NON_FINITE, GEOMETRY_UNCERTIFIABLE = 0, 1, 2, 3
+CCD_NO_IMPACT, CCD_IMPACT, CCD_INITIALLY_PROXIMATE, CCD_INDETERMINATE = 0, 1, 2, 3
+CCD_MAX_SUBDIVISIONS = 4096
+
+
+class ContactKey(C.Structure):
+    _fields_ = [("pair", C.c_uint64), ("kind", C.c_uint32), ("reserved", C.c_uint32),
+                ("first", C.c_uint64 * 3), ("second", C.c_uint64 * 3)]
+
+
+class CcdSettings(C.Structure):
+    _fields_ = [("conservative_iterations", C.c_int32), ("interval_subdivisions", C.c_int32),
+                ("time_tolerance", C.c_double), ("distance_tolerance", C.c_double)]
+
+
+class ClosestResult(C.Structure):
+    _fields_ = [("status", C.c_uint32), ("first_feature", C.c_uint32), ("second_feature", C.c_uint32),
+                ("reserved", C.c_uint32)] + [(n, C.c_double * 3) for n in (
+                    "first_point", "second_point", "first_weights", "second_weights", "normal")] + [
+                ("distance", C.c_double), ("gap", C.c_double)]
+
+
+class CcdResult(C.Structure):
+    _fields_ = [("state", C.c_uint32), ("conservative_iterations", C.c_int32), ("interval_subdivisions", C.c_int32),
+                ("used_interval_fallback", C.c_uint32), ("time_of_impact", C.c_double),
+                ("bracket_lower", C.c_double), ("bracket_upper", C.c_double), ("geometry", ClosestResult)]
+
+
 class StepSettings(C.Structure):
     _fields_ = [("time_step", C.c_double), ("substeps", C.c_int32), ("constraint_iterations", C.c_int32),
                 ("cable_sweep_pairs", C.c_int32), ("worker_threads", C.c_uint32), ("gravity", Vec3),
@@ -264,6 +293,12 @@ _PROTOTYPES = {
     "swb_definition_destroy": (None, [C.c_void_p]),
     "swb_definition_fingerprint": (C.c_uint64, [P(StructureDefinition)]),
     "swb_validate_definition": (C.c_int, [P(StructureDefinition)]),
+    "swb_default_ccd_settings": (None, [P(CcdSettings)]),
+    "swb_contact_candidates": (C.c_int, [P(StructureDefinition), C.c_double, C.c_void_p, C.c_void_p, P(ContactKey),
+                                         C.c_uint64, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
+    "swb_contact_closest": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_double, P(ClosestResult)]),
+    "swb_contact_sweep": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_double, P(CcdSettings), P(CcdResult)]),
 }
 
 # Entry points the header declares; tests check the library exports each.
