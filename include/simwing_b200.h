@@ -729,6 +729,9 @@ swb_status swb_definition_permute(swb_definition* definition,
  * SWB_SWEEP_MEMBRANE). */
 swb_status swb_definition_permute_membranes(swb_definition* definition,
                                             const uint64_t* membrane_order);
+/* Sets (or, with NULL, removes) the fabric self-contact of a definition. */
+swb_status swb_definition_set_contact(swb_definition* definition,
+                                      const swb_fabric_contact_def* contact);
 /* Multiplies the rest length of constraint `index` (any kind) or, when
  * index >= constraint_count, of suspension segment index - constraint_count. */
 swb_status swb_definition_scale_rest(swb_definition* definition,

@@ -141,6 +141,12 @@ class Definition:
             _check(self._lib.swb_definition_permute_membranes(d._h, mo.ctypes.data))
         return d
 
+    def set_contact(self, contact) -> None:
+        """Fabric self-contact of all triangles: (half_thickness,
+        normal_compliance, static_friction, dynamic_friction), or None."""
+        fc = None if contact is None else abi.FabricContactDef(*[float(x) for x in contact])
+        _check(abi.library().swb_definition_set_contact(self._h, None if fc is None else C.byref(fc)))
+
     def scale_rest(self, index: int, factor: float) -> None:
         _check(self._lib.swb_definition_scale_rest(self._h, index, factor))
 
@@ -196,7 +202,7 @@ class Definition:
 
 
 def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), suspension=None,
-                           membranes=()) -> Definition:
+                           membranes=(), contact=None) -> Definition:
     """Builds an owned Definition from plain Python records.
 
     nodes:       [(x, y, z, mass, fixed), ...]
@@ -212,6 +218,8 @@ def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), su
                  attachments [(id, node)], harness [(id, (x, y, z))],
                  segments [(id, (kind, id), (kind, id), rest, stiffness,
                  damping)], solver_iterations, maximum_line_residual.
+    contact:     (half_thickness, normal_compliance, static_friction,
+                 dynamic_friction): fabric self-contact of all triangles.
     """
     lib = abi.library()
     n = (abi.NodeDef * max(len(nodes), 1))()
@@ -278,6 +286,10 @@ def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), su
         s.maximum_control_work = 1e6
         view.suspension = C.pointer(s)
         keep += [s, a, j, hp, sg]
+    if contact is not None:
+        fc = abi.FabricContactDef(*[float(x) for x in contact])
+        view.fabric_self_contact = C.pointer(fc)
+        keep.append(fc)
     out = C.c_void_p()
     _check(lib.swb_definition_copy(C.byref(view), C.byref(out)))
     del keep

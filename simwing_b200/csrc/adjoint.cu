@@ -112,6 +112,8 @@ struct RolloutImpl {
             raise(SWB_UNSUPPORTED, "differentiable rollouts of free structures (momentum guard) are not available");
         if (!S->def.membranes.empty())
             raise(SWB_UNSUPPORTED, "differentiable rollouts of structures with membrane elements are not available");
+        if (S->def.has_contact)
+            raise(SWB_UNSUPPORTED, "differentiable rollouts of structures with fabric self-contact are not available");
         if (n_steps < 1) raise(SWB_INVALID_ARGUMENT, "a rollout needs at least one step");
         if (every < 1) raise(SWB_INVALID_ARGUMENT, "checkpoint interval must be positive");
         steps = n_steps;

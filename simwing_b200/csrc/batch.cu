@@ -74,6 +74,8 @@ std::unique_ptr<swb_structure> build_member(const swb_structure_definition& def,
         opt.cluster_ctas = r;  // classic stages: a packed cluster takes the same barriers on every rank
         auto m = std::make_unique<swb_structure>();
         try {
+            if (def.fabric_self_contact)
+                raise(SWB_UNSUPPORTED, "fabric self-contact is not available in batches (single structures only)");
             m->s.build(def, &opt);
         } catch (const Error& e) {
             if (e.status == SWB_UNSUPPORTED) continue;

@@ -15,6 +15,7 @@
 
 #include "cluster_params.h"
 #include "membrane.cuh"
+#include "contact_phase.cuh"
 #include "step_kernel.cuh"
 
 namespace swb {
@@ -292,8 +293,9 @@ __device__ __noinline__ void run_cable_pair(const ClusterInstance& I, uint32_t m
 // the reverse sweep of the adjoint.
 // kMembrane = true: the launch's structures may carry membrane elements
 // (a third record kind); without it their stage count is taken as zero.
-template <bool kPacked, bool kTape = false, bool kMembrane = false>
+template <bool kPacked, bool kTape = false, bool kMembrane = false, bool kContact = false>
 __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(const __grid_constant__ ClusterParams p) {
+    static_assert(!(kContact && (kPacked || kTape)), "contact runs in single-structure forward launches only");
     namespace cg = cooperative_groups;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t bar;
@@ -353,6 +355,27 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         for (uint32_t i = tid; i < cnt; i += blockDim.x) lam[i] = 0.0f;
     }
     if (tid <= sctas) pbeg_s[tid] = __ldg(I.patch_begin + tid);
+    ContactCtx cctx{};
+    if constexpr (kContact) {
+        cctx.C = I.contact;
+        cctx.me = me;
+        cctx.ctas = p.ctas;
+        cctx.x = x;
+        cctx.v = v;
+        cctx.base = base;
+        cctx.n = n;
+        cctx.pbeg = pbeg_s;
+        cctx.pos_in = I.pos_in;
+        for (int k = 0; k < 3; ++k) cctx.o[k] = I.origin_in[k];
+        cctx.dt = p.dt64;
+        cctx.status = I.status;
+        // multipliers and records restart every substep (beginContactSubstep,
+        // contact.cpp:1043-1055)
+        if (me == 0 && tid == 0) {
+            I.contact->table_meta[0] = 0;
+            I.contact->table_meta[1] = 0;
+        }
+    }
     // pressure gather (ascending triangle order) into v
     for (uint32_t i = tid; i < n; i += blockDim.x) {
         const uint32_t slot = base + i;
@@ -531,6 +554,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             }
             cluster.sync();
         }
+        if constexpr (kContact) contact_iteration(cctx, cluster);
     }
     // closing cable pairs
     for (int q = 0; q < (p.iterations > 0 ? closing_pairs : pairs); ++q)
@@ -558,6 +582,8 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             cluster.sync();
         }
     }
+    // ---- contact certification of the final state (soft_body.cpp:1411-1418) --
+    if constexpr (kContact) contact_certify(cctx, cluster, I.contact_diag);
     // ---- membrane residuals after the iterations (soft_body.cpp:2366-2404) ---
     if (kMembrane && S2 > 0) {
         const uint32_t lo = soff[S0 + S1 + 2], hi = soff[S0 + S1 + 2 + S2];
@@ -647,6 +673,8 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             __syncthreads();
         }
     }
+    // ---- contact friction on the finalized velocities (soft_body.cpp:1453) ---
+    if constexpr (kContact) contact_friction(cctx, cluster, I.contact_diag);
     if (owner && tid == 0) {
         if constexpr (kTape) tape_pilot(*p.tape.finish, pay, *p.tape.pilot, x, v);
         payload_finish(pdef, pay, *I.payload_in, x, v, p.dt, I.status);
@@ -694,6 +722,9 @@ inline constexpr auto xpbd_cluster_packed_kernel = &xpbd_cluster_kernel_t<true>;
 // The same with membrane elements.
 inline constexpr auto xpbd_cluster_membrane_kernel = &xpbd_cluster_kernel_t<false, false, true>;
 inline constexpr auto xpbd_cluster_packed_membrane_kernel = &xpbd_cluster_kernel_t<true, false, true>;
+// One structure per cluster with fabric self-contact.
+inline constexpr auto xpbd_cluster_contact_kernel = &xpbd_cluster_kernel_t<false, false, false, true>;
+inline constexpr auto xpbd_cluster_contact_membrane_kernel = &xpbd_cluster_kernel_t<false, false, true, true>;
 // One structure per cluster, recording the adjoint's tape.
 inline constexpr auto xpbd_cluster_tape_kernel = &xpbd_cluster_kernel_t<false, true>;
 

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "simwing_b200.h"
 #include "step_params.h"
 
 namespace swb {
@@ -31,6 +32,80 @@ struct ClusterKindDev {
 //   3: compliance xy xz yz, stiffness xx
 //   4: stiffness yy zz xy, 0
 constexpr int kMembraneAux = 5;
+
+// ---- fabric self-contact (single-structure launches) -------------------
+// A feature is coded row << 32 | col: row r < nv is surface vertex r
+// (vertices in node order) against triangle col; row nv + i is edge i
+// (edges in node-pair order) against the later edge col.  Codes order like
+// the reference's ContactFeatureKey (contact.h:95-101).
+
+// Per candidate of the current phase, written in parallel: the swept
+// query's state and normal, and the closest features of the phase's
+// snapshot (contact.cpp:1298-1351).
+struct ContactQuery {
+    double fw[3], sw[3];     // closest-feature weights, first / second primitive
+    double normal[3];        // closest-feature normal (not yet oriented)
+    double ccd_normal[3];    // normal of the swept query's geometry
+    uint32_t ccd_state;      // SWB_CCD_*
+    uint32_t certified;      // the snapshot geometry is certified
+};
+
+// Warm start and record book of one feature over a substep
+// (contactMultipliers_ and contactRecords_, contact.cpp:1320-1468).
+struct ContactEntry {
+    unsigned long long code;
+    double lambda;
+    double normal[3];        // normal of the record's last solver visit
+    uint32_t flags;          // kEntry* bits
+    uint32_t pad;
+};
+enum : uint32_t { kEntryApplied = 1, kEntryRecord = 2, kEntryVisited = 4 };
+
+// A certified record the friction pass consumes (certifyContactState,
+// contact.cpp:1583-2080).
+struct ContactRecordDev {
+    unsigned long long code;
+    double fw[3], sw[3];
+    double normal[3];
+    double lambda;
+    uint32_t active;         // normal multiplier > 0 and swept state not NoImpact
+    uint32_t pad;
+};
+
+struct ContactDiagDev {
+    unsigned long long candidates;     // candidates of the final certification
+    unsigned long long active;         // active certified records
+    unsigned long long records;        // certified + retained records
+    double max_penetration;
+};
+
+struct ContactDev {
+    uint32_t nv, ne, nt, pad;
+    const uint32_t* vid;               // [nv] slot of surface vertex r
+    const uint2* eid;                  // [ne] slots of edge i
+    const uint3* tid;                  // [nt] slots of triangle t
+    double separation;                 // 2 x half thickness
+    double compliance, static_mu, dynamic_mu;
+    swb_ccd_settings ccd;
+    // scratch
+    float4* snapshot;                  // [slots] positions at the phase start
+    double* vbox;                      // [nv][6] swept boxes: lo xyz, hi xyz
+    double* ebox;                      // [ne][6]
+    double* tbox;                      // [nt][6]
+    uint32_t* counts;                  // [nv + ne]
+    unsigned long long* offsets;       // [nv + ne + 1]
+    unsigned long long* cand;          // [cand_cap] codes of the phase's candidates
+    unsigned long long cand_cap;
+    ContactQuery* query;               // [cand_cap]
+    double* queues;                    // [threads][queue_stride][4] swept-query intervals
+    uint32_t queue_stride;
+    uint32_t pad2;
+    ContactEntry* table[2];            // ping-pong, sorted by code
+    uint32_t* table_meta;              // [0] current buffer, [1] entries
+    unsigned long long table_cap;
+    ContactRecordDev* records;         // [record_cap]
+    unsigned long long record_cap;
+};
 
 // Per-instance tables and state (one cluster each).
 struct ClusterInstance {
@@ -72,6 +147,9 @@ struct ClusterInstance {
     int pair_stages;
     const uint32_t* pair_offsets;  // [ctas * (pair_stages + 1)]
     const uint32_t* pair_rec;
+    // Fabric self-contact, or nullptr.  Single-structure launches only.
+    const ContactDev* contact;
+    ContactDiagDev* contact_diag;  // the output state's contact diagnostics
 };
 
 // Rigid pilot as the adjoint sees it: the suspension endpoint nodes are
@@ -136,6 +214,7 @@ struct ClusterParams {
     const int* rotation;               // packed launches: committed buffer per structure
     int role;                          // packed launches: 0 = S->T1, 1 = T1->T2, 2 = T2->T1
     float dt, inv_dt, inv_dt2, damping;
+    double dt64;                   // the substep in FP64 (contact phases)
     float3 gravity, ref_velocity;
     int iterations;
     int cable_pairs;               // load-path cable sweep pairs per substep (single-structure launches)

@@ -77,53 +77,23 @@ __global__ void proxy_boxes_kernel(const double* __restrict__ prev, const double
     *out = contact::swept_box(p, c, count, expansion);
 }
 
-// Row r < nv: the vertex-triangle features of surface vertex r (columns =
-// triangles in index order); row nv + i: the edge-edge features of edge i
-// with every later edge j (columns = j > i).  One warp per row; with
-// `cols` == nullptr the warp counts its row's hits, else it writes their
-// column indices from offsets[row] on, in column order.
+// One warp per candidate row (contact::scan_candidate_row); with `cols` ==
+// nullptr the warp counts its row's hits, else it writes their column
+// indices from offsets[row] on, in column order.
 __global__ void candidate_rows_kernel(uint32_t nv, uint32_t ne, uint32_t nt, const uint32_t* __restrict__ vertices,
                                       const uint2* __restrict__ edges, const uint3* __restrict__ triangles,
                                       const Box* __restrict__ vbox, const Box* __restrict__ ebox,
                                       const Box* __restrict__ tbox, uint32_t* __restrict__ counts,
                                       const unsigned long long* __restrict__ offsets, uint32_t* __restrict__ cols) {
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31;
     const uint32_t rows = nv + ne;
     for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
-        uint32_t hits = 0;
-        unsigned long long base = cols ? offsets[row] : 0;
-        if (row < nv) {
-            const uint32_t v = vertices[row];
-            const Box b = vbox[row];
-            for (uint32_t c0 = 0; c0 < nt; c0 += 32) {
-                const uint32_t t = c0 + lane;
-                bool hit = false;
-                if (t < nt) {
-                    const uint3 tri = triangles[t];
-                    hit = tri.x != v && tri.y != v && tri.z != v && contact::boxes_overlap(b, tbox[t]);
-                }
-                const unsigned mask = __ballot_sync(0xffffffffu, hit);
-                if (cols && hit) cols[base + hits + __popc(mask & ((1u << lane) - 1u))] = t;
-                hits += __popc(mask);
-            }
-        } else {
-            const uint32_t i = row - nv;
-            const uint2 e = edges[i];
-            const Box b = ebox[i];
-            for (uint32_t c0 = i + 1; c0 < ne; c0 += 32) {
-                const uint32_t j = c0 + lane;
-                bool hit = false;
-                if (j < ne) {
-                    const uint2 f = edges[j];
-                    hit = e.x != f.x && e.x != f.y && e.y != f.x && e.y != f.y && contact::boxes_overlap(b, ebox[j]);
-                }
-                const unsigned mask = __ballot_sync(0xffffffffu, hit);
-                if (cols && hit) cols[base + hits + __popc(mask & ((1u << lane) - 1u))] = j;
-                hits += __popc(mask);
-            }
-        }
-        if (!cols && lane == 0) counts[row] = hits;
+        const unsigned long long base = cols ? offsets[row] : 0;
+        const uint32_t hits = contact::scan_candidate_row(row, nv, ne, nt, vertices, edges, triangles, vbox, ebox, tbox,
+                                                          [&](uint32_t col, uint32_t k) {
+                                                              if (cols) cols[base + k] = col;
+                                                          });
+        if (!cols && (threadIdx.x & 31) == 0) counts[row] = hits;
     }
 }
 

@@ -104,7 +104,7 @@ __device__ __forceinline__ bool valid_separation(double s) { return isfinite(s) 
 
 // Closest point of triangle (a, b, c) to `p` by Voronoi regions
 // (closestVertexTriangle, contact.cpp:141-245).
-__device__ __noinline__ Closest closest_vertex_triangle(D3 p, D3 a, D3 b, D3 c, double separation) {
+static __device__ __noinline__ Closest closest_vertex_triangle(D3 p, D3 a, D3 b, D3 c, double separation) {
     Closest r;
     r.first_feature = kPoint;
     r.first_point = p;
@@ -176,7 +176,7 @@ __device__ __noinline__ Closest closest_vertex_triangle(D3 p, D3 a, D3 b, D3 c, 
 }
 
 // Closest points of two segments (closestEdgeEdge, contact.cpp:247-304).
-__device__ __noinline__ Closest closest_edge_edge(D3 p0, D3 p1, D3 q0, D3 q1, double separation) {
+static __device__ __noinline__ Closest closest_edge_edge(D3 p0, D3 p1, D3 q0, D3 q1, double separation) {
     Closest r;
     if (!finite3(p0) || !finite3(p1) || !finite3(q0) || !finite3(q1) || !isfinite(separation)) {
         r.status = SWB_GEOMETRY_NON_FINITE;
@@ -283,7 +283,7 @@ __device__ __forceinline__ bool refine_impact(uint32_t kind, const Linear& f, co
 // Continuous contact over the substep: conservative advancement, then an
 // interval subdivision fallback (sweptContact, contact.cpp:669-945).
 // `queue` holds interval_subdivisions + 1 entries of scratch.
-__device__ __noinline__ Ccd swept_contact(uint32_t kind, const Linear& f, const Linear& s, double separation,
+static __device__ __noinline__ Ccd swept_contact(uint32_t kind, const Linear& f, const Linear& s, double separation,
                                           const swb_ccd_settings& cs, Interval* queue) {
     Ccd r;
     const bool counts = (kind == SWB_FEATURE_VERTEX_TRIANGLE && f.count == 1 && s.count == 3) ||
@@ -457,6 +457,55 @@ __device__ __forceinline__ Box swept_box(const D3* prev, const D3* cur, int coun
 __device__ __forceinline__ bool boxes_overlap(const Box& a, const Box& b) {
     return a.lo[0] <= b.hi[0] && b.lo[0] <= a.hi[0] && a.lo[1] <= b.hi[1] && b.lo[1] <= a.hi[1] &&
            a.lo[2] <= b.hi[2] && b.lo[2] <= a.hi[2];
+}
+
+// One candidate row scanned by a warp (all 32 lanes call it).  Row r < nv:
+// the vertex-triangle features of surface vertex r against every triangle
+// not holding it, in triangle order; row nv + i: the edge-edge features of
+// edge i with every later edge sharing no node, in edge order.  Node
+// identities are whatever the id arrays hold (node indices or slots).
+// emit(col, k) is called by the hitting lane for its k-th hit of the row, in
+// column order; returns the row's hit count.
+template <class Emit>
+__device__ __forceinline__ uint32_t scan_candidate_row(uint32_t row, uint32_t nv, uint32_t ne, uint32_t nt,
+                                                       const uint32_t* __restrict__ vid,
+                                                       const uint2* __restrict__ eid,
+                                                       const uint3* __restrict__ tid3, const Box* __restrict__ vbox,
+                                                       const Box* __restrict__ ebox, const Box* __restrict__ tbox,
+                                                       Emit emit) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t hits = 0;
+    if (row < nv) {
+        const uint32_t v = vid[row];
+        const Box b = vbox[row];
+        for (uint32_t c0 = 0; c0 < nt; c0 += 32) {
+            const uint32_t t = c0 + lane;
+            bool hit = false;
+            if (t < nt) {
+                const uint3 tri = tid3[t];
+                hit = tri.x != v && tri.y != v && tri.z != v && boxes_overlap(b, tbox[t]);
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, hit);
+            if (hit) emit(t, hits + __popc(mask & ((1u << lane) - 1u)));
+            hits += __popc(mask);
+        }
+    } else {
+        const uint32_t i = row - nv;
+        const uint2 e = eid[i];
+        const Box b = ebox[i];
+        for (uint32_t c0 = i + 1; c0 < ne; c0 += 32) {
+            const uint32_t j = c0 + lane;
+            bool hit = false;
+            if (j < ne) {
+                const uint2 f = eid[j];
+                hit = e.x != f.x && e.x != f.y && e.y != f.x && e.y != f.y && boxes_overlap(b, ebox[j]);
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, hit);
+            if (hit) emit(j, hits + __popc(mask & ((1u << lane) - 1u)));
+            hits += __popc(mask);
+        }
+    }
+    return hits;
 }
 
 // ContactFrictionState (contact.h:178-182)

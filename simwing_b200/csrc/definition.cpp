@@ -535,6 +535,16 @@ swb_status swb_definition_permute_membranes(swb_definition* definition, const ui
     });
 }
 
+swb_status swb_definition_set_contact(swb_definition* definition, const swb_fabric_contact_def* contact) {
+    return guarded([&] {
+        if (!definition) raise(SWB_INVALID_ARGUMENT, "definition is null");
+        OwnedDefinition& d = definition->def;
+        d.has_contact = contact != nullptr;
+        d.contact = contact ? *contact : swb_fabric_contact_def{};
+        d.sync_view();
+    });
+}
+
 swb_status swb_definition_scale_rest(swb_definition* definition,
                                      uint64_t index, double factor) {
     return guarded([&] {

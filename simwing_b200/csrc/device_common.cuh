@@ -16,6 +16,7 @@ enum : int {
     kStatusSuspension = 4,
     kStatusCopyTimeout = 8,
     kStatusMembrane = 16,
+    kStatusContact = 32,   // status[1]: a kContact* detail code
 };
 
 enum : int {

@@ -145,7 +145,11 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     def.assign(definition);
     validate_definition(def.view);
     fingerprint = definition_fingerprint(def.view);
-    if (def.has_contact) raise(SWB_UNSUPPORTED, "fabric self-contact is not available in this build");
+    if (def.has_contact) {
+        if (def.has_suspension)
+            raise(SWB_UNSUPPORTED, "fabric self-contact together with a rigid pilot is not available in this build");
+        contact_surface = build_contact_surface(def.view, def.contact.half_thickness);
+    }
     // Solver-drift momentum restoration of isolated free structures: no
     // suspension, no contact, bending or membranes present, no fixed node.
     momentum_guard = !def.has_suspension && !def.has_contact && (!def.dihedrals.empty() || !def.membranes.empty()) &&
@@ -200,6 +204,8 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
         raise(SWB_UNSUPPORTED, "the momentum guard of a free structure needs the cluster schedule (the mesh does not fit one)");
     if (!cluster_mode && !def.membranes.empty())
         raise(SWB_UNSUPPORTED, "membrane elements need the cluster schedule (the mesh does not fit one)");
+    if (!cluster_mode && def.has_contact)
+        raise(SWB_UNSUPPORTED, "fabric self-contact needs the cluster schedule (the mesh does not fit one)");
     uint32_t widest = 32;
     if (cluster_mode) {
         verify_cluster_schedule(def, susp_nodes, csched);
@@ -314,7 +320,65 @@ static void membrane_constants(const swb_membrane_def& m, float4 out[kMembraneAu
 }
 
 void (*StructureImpl::step_kernel() const)(ClusterParams) {
+    if (def.has_contact)
+        return def.membranes.empty() ? dev::xpbd_cluster_contact_kernel : dev::xpbd_cluster_contact_membrane_kernel;
     return def.membranes.empty() ? dev::xpbd_cluster_kernel : dev::xpbd_cluster_membrane_kernel;
+}
+
+// Device tables and scratch of the fabric self-contact phases: the surface
+// by node slot, the candidate list of one phase, the per-thread queues of
+// the swept queries, the ping-pong multiplier table and the record book.
+// Capacities: up to kContactCapacity candidates per phase (and as many
+// warm-started features and records); beyond that the step fails with
+// SWB_CONTACT_ERROR.
+void StructureImpl::setup_contact() {
+    constexpr uint64_t kContactCapacity = uint64_t(1) << 20;
+    const ContactSurface& S = contact_surface;
+    ContactDev c{};
+    c.nv = static_cast<uint32_t>(S.vertices.size());
+    c.ne = static_cast<uint32_t>(S.edges.size());
+    c.nt = static_cast<uint32_t>(S.triangles.size());
+    std::vector<uint32_t> vid(c.nv);
+    std::vector<uint2> eid(c.ne);
+    std::vector<uint3> tid(c.nt);
+    for (uint32_t i = 0; i < c.nv; ++i) vid[i] = slot_of_node[S.vertices[i]];
+    for (uint32_t i = 0; i < c.ne; ++i) eid[i] = make_uint2(slot_of_node[S.edges[i][0]], slot_of_node[S.edges[i][1]]);
+    for (uint32_t i = 0; i < c.nt; ++i)
+        tid[i] = make_uint3(slot_of_node[S.triangles[i][0]], slot_of_node[S.triangles[i][1]],
+                            slot_of_node[S.triangles[i][2]]);
+    c.vid = dupload(owned, vid, stream);
+    c.eid = dupload(owned, eid, stream);
+    c.tid = dupload(owned, tid, stream);
+    c.separation = 2.0 * def.contact.half_thickness;
+    c.compliance = def.contact.normal_compliance;
+    c.static_mu = def.contact.static_friction;
+    c.dynamic_mu = def.contact.dynamic_friction;
+    swb_default_ccd_settings(&c.ccd);  // Structure steps with the default CCD settings
+    c.snapshot = dalloc<float4>(owned, def.nodes.size());
+    c.vbox = dalloc<double>(owned, 6 * static_cast<size_t>(c.nv));
+    c.ebox = dalloc<double>(owned, 6 * static_cast<size_t>(c.ne));
+    c.tbox = dalloc<double>(owned, 6 * static_cast<size_t>(c.nt));
+    c.counts = dalloc<uint32_t>(owned, static_cast<size_t>(c.nv) + c.ne);
+    c.offsets = dalloc<unsigned long long>(owned, static_cast<size_t>(c.nv) + c.ne + 1);
+    cuda_check(cudaMemsetAsync(c.offsets, 0, (static_cast<size_t>(c.nv) + c.ne + 1) * sizeof(unsigned long long),
+                               stream), "memset");
+    const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>(S.possible, kContactCapacity));
+    c.cand_cap = cap;
+    c.cand = dalloc<unsigned long long>(owned, cap);
+    c.query = dalloc<ContactQuery>(owned, cap);
+    c.queue_stride = static_cast<uint32_t>(c.ccd.interval_subdivisions + 1);
+    c.queues = dalloc<double>(owned, static_cast<size_t>(G) * threads * c.queue_stride * 4);
+    for (int b = 0; b < 2; ++b) c.table[b] = dalloc<ContactEntry>(owned, cap);
+    c.table_meta = dalloc<uint32_t>(owned, 2);
+    cuda_check(cudaMemsetAsync(c.table_meta, 0, 2 * sizeof(uint32_t), stream), "memset");
+    c.table_cap = cap;
+    c.records = dalloc<ContactRecordDev>(owned, cap);
+    c.record_cap = cap;
+    d_contact = dupload(owned, std::vector<ContactDev>{c}, stream);
+    for (int b = 0; b < 3; ++b) {
+        d_cdiag[b] = dalloc<ContactDiagDev>(owned, 1);
+        cuda_check(cudaMemsetAsync(d_cdiag[b], 0, sizeof(ContactDiagDev), stream), "memset");
+    }
 }
 
 void StructureImpl::upload_cluster_tables() {
@@ -564,6 +628,7 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
     p.copy_budget = 4000000000LL;
 
     if (cluster_mode) {
+        if (def.has_contact) setup_contact();
         // One instance record per (input, output) buffer pair so a launch
         // only selects a pointer.
         std::vector<ClusterInstance> inst(9);
@@ -579,6 +644,8 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
                 c.payload_in = d_payload[in]; c.payload_out = d_payload[out];
                 c.origin_in = d_origin[in]; c.origin_out = d_origin[out];
                 c.membrane_residual = d_mres[out];
+                c.contact = d_contact;
+                c.contact_diag = d_cdiag[out];
                 c.status = d_control->status;
                 c.recentre = def.has_suspension ? 1 : 0;
                 inst[in * 3 + out] = c;
@@ -724,6 +791,7 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out)
         cp.instances = d_instances + in * 3 + out;
         cp.ctas = G;
         cp.dt = static_cast<float>(dt);
+        cp.dt64 = dt;
         cp.inv_dt = static_cast<float>(1.0 / dt);
         cp.inv_dt2 = static_cast<float>(1.0 / (dt * dt));
         cp.damping = static_cast<float>(std::exp(-st.velocity_damping * dt));
@@ -777,6 +845,8 @@ size_t dynamic_smem_limit(const cudaDeviceProp& prop) {
                           reinterpret_cast<const void*>(dev::xpbd_cluster_packed_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_membrane_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_packed_membrane_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_contact_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_contact_membrane_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_tape_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_kernel_narrow),
@@ -852,6 +922,30 @@ swb_status decode_status(const int status[2], std::string& message) {
     if (status[0] & dev::kStatusCopyTimeout) {
         message = "shared-memory staging timed out";
         return SWB_SYNC_TIMEOUT;
+    }
+    if (status[0] & dev::kStatusContact) {
+        static const char* what[] = {
+            "contact failure",
+            "Contact CCD could not certify a supported feature",
+            "Contact endpoint geometry is not certifiable",
+            "Contact normal is not finite/unit",
+            "Penetrating contact has no movable/compliant response",
+            "Non-finite contact projection",
+            "Non-finite solved contact geometry",
+            "Final contact geometry could not be certified",
+            "Final contact closest geometry is not certifiable",
+            "Final contact geometry is non-finite",
+            "Final contact penetration exceeds the certified gate",
+            "Applied contact impulse lost its supported feature",
+            "Cleared contact final geometry is not certifiable",
+            "Cleared contact failed final geometry certification",
+            "Non-finite/positive contact friction work",
+            "Contact broadphase input failed: positions must be finite",
+            "contact candidates exceed the device list (1,048,576 per phase)",
+            "contact features exceed the device multiplier table",
+            "contact records exceed the device record book"};
+        message = std::string("ContactStepError: ") + what[std::clamp(status[1], 0, 18)];
+        return SWB_CONTACT_ERROR;
     }
     if (status[0] & dev::kStatusMembrane) {
         message = "membrane system is singular or its right-hand side is not finite";
@@ -1024,6 +1118,15 @@ void StructureImpl::diagnostics(swb_diagnostics* o) const {
     o->maximum_cable_extension = acc[11];
     o->maximum_absolute_membrane_strain = acc[12];
     o->maximum_membrane_residual = acc[13];
+    if (def.has_contact) {
+        ContactDiagDev cd{};
+        cuda_check(cudaMemcpyAsync(&cd, d_cdiag[cur], sizeof(cd), cudaMemcpyDeviceToHost, stream), "read");
+        cuda_check(cudaStreamSynchronize(stream), "diagnostics");
+        o->contact_pair_count = 1;
+        o->active_contact_count = cd.active;
+        o->maximum_contact_penetration = cd.max_penetration;
+        finite = finite && std::isfinite(cd.max_penetration);
+    }
     swb_vec3 pend{0, 0, 0};
     for (const auto& f : pending) {
         pend.x += f.x; pend.y += f.y; pend.z += f.z;

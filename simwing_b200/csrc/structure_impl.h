@@ -4,6 +4,7 @@
 #include "cluster_params.h"
 #include "cluster_schedule.h"
 #include "common.h"
+#include "contact_surface.h"
 #include "schedule.h"
 #include "step_params.h"
 
@@ -83,6 +84,11 @@ struct StructureImpl {
     uint32_t* d_tri_list = nullptr;
     uint32_t* d_diag_a = nullptr;
     float* d_mres[3] = {nullptr, nullptr, nullptr};  // membrane residual per record, per state buffer
+    // fabric self-contact: the surface, its device tables and scratch, and
+    // the contact diagnostics per state buffer
+    ContactSurface contact_surface;
+    ContactDev* d_contact = nullptr;
+    ContactDiagDev* d_cdiag[3] = {nullptr, nullptr, nullptr};
     uint4* d_diag_mem = nullptr;      // membrane records for the diagnostics: corner slots, record index
     uint32_t* d_diag_b = nullptr;
     float* d_diag_rest = nullptr;
@@ -108,6 +114,7 @@ struct StructureImpl {
     ~StructureImpl();
     void build(const swb_structure_definition& definition, const swb_solver_options* options);
     void upload_cluster_tables();
+    void setup_contact();
     // the cluster step kernel for this structure (the membrane
     // instantiation when it has membrane elements)
     void (*step_kernel() const)(ClusterParams);

@@ -1,0 +1,151 @@
+"""Steps with fabric self-contact on the device against the reference build.
+
+The reference's Structure (oracle/_ref/libswref.so, with softwing's contact
+code) steps the definition permuted into the device sweep order; both start
+from the definition and run freely.  Contact keys are ordered alike on both
+sides, so the contact projections run in the same order.  Tolerances as for
+the other per-step tests: positions within 1e-5 of the largest coordinate
+(at least 1 m), velocities within that over the step; the largest
+penetration within the position bound; the active contact counts equal.
+
+Hard (zero-compliance) resting contact is decided at a finer scale than an
+FP32 state resolves: the swept query calls a feature in contact when its gap
+is within 1e-10 m (CcdSettings::distanceTolerance), while FP32 positions of
+a sheet 0.35 m from the origin resolve 3e-8 m.  A resting feature is then
+in contact (a record with friction) on one side and not on the other, and
+which of two redundant features ends with a multiplier of 1e-12 rather than
+zero depends on the same rounding; the reference itself moves from 160 to
+157 active features when its input is rounded to FP32.  Hard contact is
+therefore compared without friction and on whether any feature is active;
+compliant contact (1e-3 m/N: resting features sit 1e-5 m inside the
+envelope) is compared exactly, friction, active counts and the step at which
+the reference's query gives up included.
+"""
+import numpy as np
+import pytest
+
+import simwing_b200 as sw
+from oracle import oracle as O
+from tests.conftest import step_settings
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not O.ref_available(), reason="reference build not present")]
+
+REL_TOL = 1e-5
+
+
+def two_sheets():
+    """The reference's contact checkpoint fixture (simwing_structure_test.cpp:
+    297-329): two disconnected triangles 1 cm apart, half thickness 1 cm."""
+    nodes = [(-1, -1, 0, 1.0, 0), (1, -1, 0, 1.0, 0), (0, 1, 0, 1.0, 0),
+             (-1, -1, 0.01, 1.0, 0), (0, 1, 0.01, 1.0, 0), (1, -1, 0.01, 1.0, 0)]
+    return sw.definition_from_arrays(nodes, [(0, 1, 2), (3, 4, 5)], contact=(0.01, 0.0, 0.0, 0.0))
+
+
+def stacked_sheets(n=8, gap=0.003, half=0.002, friction=(0.4, 0.25), spacing=0.05, compliance=0.0):
+    """A free sheet with distance constraints resting 1 mm inside the contact
+    envelope of a pinned sheet below it, shifted so that vertices, edges and
+    faces of the two meet in every feature configuration."""
+    nodes, tris, cons = [], [], []
+    for layer, z in ((0, 0.0), (1, gap)):
+        off = len(nodes)
+        for j in range(n):
+            for i in range(n):
+                x, y = i * spacing, j * spacing
+                if layer:
+                    x, y = x + 0.013, y + 0.007
+                nodes.append((x, y, z, 0.001, layer == 0))
+        for j in range(n - 1):
+            for i in range(n - 1):
+                a = off + j * n + i
+                b, c, d = a + 1, a + n, a + n + 1
+                tris += [(a, b, d), (a, d, c)]
+                if layer:
+                    for u, v in ((a, b), (a, c), (a, d)):
+                        rest = float(np.linalg.norm(np.subtract(nodes[u][:3], nodes[v][:3])))
+                        cons.append((1, u, v, rest, 1e-7))
+        if layer:
+            for j in range(n - 1):
+                a = off + j * n + n - 1
+                cons.append((1, a, a + n, spacing, 1e-7))
+            for i in range(n - 1):
+                a = off + (n - 1) * n + i
+                cons.append((1, a, a + 1, spacing, 1e-7))
+    return sw.definition_from_arrays(nodes, tris, cons, contact=(half, compliance, friction[0], friction[1]))
+
+
+SLIDE = step_settings(iterations=8, gravity=(2.0, 0.0, -9.81))  # tilted gravity: static and dynamic friction
+# (make, settings, steps, exact active count, step at which the reference
+# raises ContactStepError: its swept query cannot certify the resting
+# contact, contact.cpp:1318-1325)
+CASES = {
+    "two_sheets": (two_sheets, step_settings(iterations=4), 6, False, None),
+    "stacked_hard": (lambda: stacked_sheets(friction=(0.0, 0.0)), SLIDE, 3, False, None),
+    "stacked_compliant": (lambda: stacked_sheets(compliance=1e-3), SLIDE, 4, True, 3),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("ctas", [1, 4])
+def test_contact_steps_match_the_reference(cuda_device, name, ctas):
+    make, st, steps, exact_count, fails_at = CASES[name]
+    d = make()
+    dev = sw.Structure(d, sw.SolverOptions(cluster_ctas=ctas))
+    ref = O.RefStructure(dev.oracle_definition())
+    saw_contact = False
+    for k in range(steps):
+        if k == fails_at:
+            before = dev.node_states().copy()
+            with pytest.raises(O.OracleError) as err:
+                ref.step(st)
+            assert err.value.status == sw.abi.CONTACT_ERROR
+            with pytest.raises(sw.ContactStepError):
+                dev.step(st)
+            np.testing.assert_array_equal(dev.node_states(), before)
+            break
+        da = dev.step(st)
+        db = ref.step(st)
+        a, b = dev.node_states(), ref.node_states()
+        scale = max(1.0, float(np.abs(b[:, 0, :]).max()))
+        assert float(np.abs(a[:, 0, :] - b[:, 0, :]).max()) <= REL_TOL * scale
+        assert float(np.abs(a[:, 2, :] - b[:, 2, :]).max()) <= REL_TOL * scale / st.time_step
+        assert da.contact_pair_count == db.contact_pair_count == 1
+        if exact_count:
+            assert da.active_contact_count == db.active_contact_count
+        else:
+            assert (da.active_contact_count > 0) == (db.active_contact_count > 0)
+        assert abs(da.maximum_contact_penetration - db.maximum_contact_penetration) <= REL_TOL * scale
+        assert da.finite and db.finite
+        saw_contact = saw_contact or db.active_contact_count > 0
+    assert saw_contact
+
+
+def test_unresolvable_contact_fails_the_step_and_rolls_back(cuda_device):
+    """Two pinned sheets inside each other's envelope: no movable or
+    compliant response (contact.cpp:1366-1372).  Both solvers raise
+    ContactStepError; the device keeps the pre-step state."""
+    nodes = [(-1, -1, 0, 1.0, 1), (1, -1, 0, 1.0, 1), (0, 1, 0, 1.0, 1),
+             (-1, -1, 0.005, 1.0, 1), (0, 1, 0.005, 1.0, 1), (1, -1, 0.005, 1.0, 1),
+             (3, 3, 3, 1.0, 0)]
+    d = sw.definition_from_arrays(nodes, [(0, 1, 2), (3, 4, 5)], contact=(0.01, 0.0, 0.0, 0.0))
+    st = step_settings(iterations=4)
+    dev = sw.Structure(d)
+    ref = O.RefStructure(dev.oracle_definition())
+    before = dev.node_states().copy()
+    with pytest.raises(sw.ContactStepError):
+        dev.step(st)
+    with pytest.raises(O.OracleError) as err:
+        ref.step(st)
+    assert err.value.status == sw.abi.CONTACT_ERROR
+    np.testing.assert_array_equal(dev.node_states(), before)
+    assert dev.accepted_step_count() == 0
+
+
+def test_contact_is_refused_where_it_is_not_built(cuda_device):
+    d = two_sheets()
+    with pytest.raises(sw.Unsupported):
+        sw.Structure(d, sw.SolverOptions(flags=sw.abi.OPT_GRID))
+    with pytest.raises(sw.Unsupported):
+        sw.Batch([d, two_sheets()])
+    s = sw.Structure(d)
+    with pytest.raises(sw.Unsupported):
+        sw.Rollout(s, 4)
