@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--batch-size", type=int, default=64)
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-membrane-wing", action="store_true")
+    p.add_argument("--no-contact", action="store_true")
     p.add_argument("--only-adjoint", action="store_true",
                    help="run the adjoint leg alone and print its record (profiling)")
     p.add_argument("--adjoint-steps", type=int, default=240)
@@ -127,6 +128,47 @@ def membrane_wing_leg(sw, st, steps, device, flush):
             "stages_per_iteration": rep.local_stages_per_iteration, "steps": steps,
             "ms_per_step": total / steps, "wing_steps_per_s": steps / (total / 1000.0),
             "max_membrane_strain": diag.maximum_absolute_membrane_strain, "finite": bool(diag.finite)}
+
+
+def contact_leg(sw, steps, device, reference_steps, with_reference):
+    """Fabric self-contact: two stacked 16 x 16 sheets (512 nodes, 900
+    triangles), the free one 1 mm inside the contact envelope of the pinned
+    one, compliant contact (1e-3 m/N) with friction, 8 iterations, tilted
+    gravity.  One step from the same initial state, repeated (the state is
+    restored between steps: the reference's swept query gives up on
+    persistent resting contact after a few steps).  Device time from CUDA
+    events; the reference build's Structure timed on the host beside it."""
+    d = sw.stacked_sheets(n=16, compliance=1e-3)
+    st = sw.StepSettings(time_step=1.0 / 120.0, substeps=1, constraint_iterations=8, gravity=(2.0, 0.0, -9.81),
+                         velocity_damping=0.25)
+    s = sw.Structure(d, sw.SolverOptions(device=device))
+    image = s.checkpoint()
+    for _ in range(3):
+        s.step(st, diagnostics=False)
+        s.restore(image)
+    times = []
+    for _ in range(steps):
+        s.step(st, diagnostics=False)
+        times.append(s.last_step_ms())
+        s.restore(image)
+    diag = s.step(st)
+    s.close()
+    out = {"workload": "stacked 16x16 sheets, compliant fabric self-contact with friction, 8 iterations, "
+                       "one step from rest", "nodes": d.counts()["nodes"], "triangles": d.counts()["triangles"],
+           "active_contacts": int(diag.active_contact_count), "steps": steps,
+           "device_ms_per_step": float(sum(times)) / steps}
+    if with_reference:
+        from oracle import oracle as O
+
+        if O.ref_available():
+            ref_times = []
+            for _ in range(reference_steps):
+                ref = O.RefStructure(d)
+                ref.step(st)
+                ref_times.append(ref.last_step_seconds() * 1000.0)
+            out["reference_ms_per_step"] = float(sum(ref_times)) / len(ref_times)
+            out["reference_cores"] = 1
+    return out
 
 
 def batched_leg(sw, st, count, rank, world, dist, device):
@@ -462,6 +504,9 @@ def main():
     membrane_wing = None
     if not args.no_membrane_wing and rank == 0:
         membrane_wing = membrane_wing_leg(sw, st, min(args.steps, 50), local, flush)
+    contact = None
+    if not args.no_contact and rank == 0:
+        contact = contact_leg(sw, min(args.steps, 50), local, 2, not args.no_cpu_baseline)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -490,6 +535,7 @@ def main():
             "batched": batched,
             "adjoint": adjoint,
             "membrane_wing": membrane_wing,
+            "contact": contact,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

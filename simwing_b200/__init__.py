@@ -296,6 +296,41 @@ def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), su
     return Definition(out.value)
 
 
+def stacked_sheets(n: int = 8, gap: float = 0.003, half_thickness: float = 0.002, friction=(0.4, 0.25),
+                   spacing: float = 0.05, compliance: float = 0.0, mass: float = 0.001) -> Definition:
+    """Fabric self-contact scene: a free n x n sheet (distance constraints on
+    its edges, compliance 1e-7) `gap` above a pinned n x n sheet, shifted by
+    (13 mm, 7 mm) so that vertices, edges and faces of the two meet in every
+    feature configuration; contact (half_thickness, compliance, static and
+    dynamic friction) over all triangles."""
+    nodes, tris, cons = [], [], []
+    for layer, z in ((0, 0.0), (1, gap)):
+        off = len(nodes)
+        for j in range(n):
+            for i in range(n):
+                x, y = i * spacing, j * spacing
+                if layer:
+                    x, y = x + 0.013, y + 0.007
+                nodes.append((x, y, z, mass, layer == 0))
+        for j in range(n - 1):
+            for i in range(n - 1):
+                a = off + j * n + i
+                b, c, d = a + 1, a + n, a + n + 1
+                tris += [(a, b, d), (a, d, c)]
+                if layer:
+                    for u, v in ((a, b), (a, c), (a, d)):
+                        rest = float(np.linalg.norm(np.subtract(nodes[u][:3], nodes[v][:3])))
+                        cons.append((1, u, v, rest, 1e-7))
+        if layer:
+            for j in range(n - 1):
+                a = off + j * n + n - 1
+                cons.append((1, a, a + n, spacing, 1e-7))
+            for i in range(n - 1):
+                a = off + (n - 1) * n + i
+                cons.append((1, a, a + 1, spacing, 1e-7))
+    return definition_from_arrays(nodes, tris, cons, contact=(half_thickness, compliance, friction[0], friction[1]))
+
+
 def generate_patch(**overrides) -> Definition:
     """The hanging cloth patch (33 x 33 on 1 m x 1 m by default)."""
     lib = abi.library()

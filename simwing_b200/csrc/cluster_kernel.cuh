@@ -67,19 +67,6 @@ __device__ __forceinline__ uint32_t node_addr(uint32_t ref, uint32_t me, uint32_
     asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank + rank_base));
     return remote;
 }
-__device__ __forceinline__ float4 ld_node(uint32_t addr) {
-    float4 v;
-    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-                 : "r"(addr)
-                 : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_node(uint32_t addr, float4 v) {
-    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z),
-                 "f"(v.w)
-                 : "memory");
-}
 
 // The two halves of a cluster barrier, for a warp that works between its
 // arrival and its wait (arrive releases, wait acquires; every lane of the
@@ -369,6 +356,8 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         for (int k = 0; k < 3; ++k) cctx.o[k] = I.origin_in[k];
         cctx.dt = p.dt64;
         cctx.status = I.status;
+        cctx.x_base = smem_addr(x);
+        cctx.v_delta = smem_addr(v) - smem_addr(x);
         // multipliers and records restart every substep (beginContactSubstep,
         // contact.cpp:1043-1055)
         if (me == 0 && tid == 0) {

@@ -46,8 +46,12 @@ struct ContactQuery {
     double fw[3], sw[3];     // closest-feature weights, first / second primitive
     double normal[3];        // closest-feature normal (not yet oriented)
     double ccd_normal[3];    // normal of the swept query's geometry
+    double eff;              // effective inverse mass sum w_i m_i^-1 w_i
+    uint32_t addr[6];        // cluster shared-memory addresses of the nodes: first, then second primitive
+    float inv[6];            // their inverse masses
     uint32_t ccd_state;      // SWB_CCD_*
     uint32_t certified;      // the snapshot geometry is certified
+    uint32_t fc, sc;         // nodes of the first / second primitive
 };
 
 // Warm start and record book of one feature over a substep
@@ -68,6 +72,10 @@ struct ContactRecordDev {
     double fw[3], sw[3];
     double normal[3];
     double lambda;
+    double eff;              // effective inverse mass
+    uint32_t addr[6];        // node addresses, as in ContactQuery
+    float inv[6];
+    uint32_t fc, sc;
     uint32_t active;         // normal multiplier > 0 and swept state not NoImpact
     uint32_t pad;
 };

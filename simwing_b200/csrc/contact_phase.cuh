@@ -71,20 +71,14 @@ struct ContactCtx {
     double o[3];               // coordinate origin of the state
     double dt;
     int* status;
+    uint32_t x_base;           // shared address of this CTA's node array
+    uint32_t v_delta;          // offset from the node array to the velocity array
 };
 
 using contact::D3;
 
 __device__ __forceinline__ D3 world_of(const ContactCtx& c, float4 X) {
     return {c.o[0] + static_cast<double>(X.x), c.o[1] + static_cast<double>(X.y), c.o[2] + static_cast<double>(X.z)};
-}
-
-// The node of `slot` in its owner CTA's shared memory.
-__device__ __forceinline__ float4* slot_node(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
-                                             float4* local, uint32_t slot) {
-    int r = c.ctas - 1;
-    while (r > 0 && c.pbeg[r] > slot) --r;
-    return cluster.map_shared_rank(local, r) + (slot - c.pbeg[r]);
 }
 
 struct FeatureSlots {
@@ -215,8 +209,20 @@ static __device__ __noinline__ void contact_scan(const ContactCtx& c) {
     }
 }
 
-// Per candidate: the swept query and the snapshot's closest features.
-static __device__ __noinline__ void contact_queries(const ContactCtx& c) {
+// Cluster-window address of the node in `slot` (valid from every CTA).
+__device__ __forceinline__ uint32_t slot_addr(const ContactCtx& c, uint32_t slot) {
+    int r = c.ctas - 1;
+    while (r > 0 && c.pbeg[r] > slot) --r;
+    const uint32_t local = c.x_base + (slot - c.pbeg[r]) * 16u;
+    uint32_t addr;
+    asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(addr) : "r"(local), "r"(r));
+    return addr;
+}
+
+// Per candidate: the swept query, the snapshot's closest features, and what
+// the serial pass needs of the feature's nodes (cluster addresses, inverse
+// masses, effective inverse mass).
+__device__ __noinline__ void contact_queries(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     const unsigned long long count = C.offsets[C.nv + C.ne];
     const uint32_t stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
@@ -228,66 +234,61 @@ static __device__ __noinline__ void contact_queries(const ContactCtx& c) {
         contact::Linear f, s;
         f.count = q.fc;
         s.count = q.sc;
+        ContactQuery& out = C.query[i];
+        double eff = 0.0;
+        const contact::Closest g = [&] {
+            for (int k = 0; k < q.fc; ++k) {
+                f.prev[k] = world_of(c, c.pos_in[q.f[k]]);
+                f.cur[k] = world_of(c, C.snapshot[q.f[k]]);
+            }
+            for (int k = 0; k < q.sc; ++k) {
+                s.prev[k] = world_of(c, c.pos_in[q.s[k]]);
+                s.cur[k] = world_of(c, C.snapshot[q.s[k]]);
+            }
+            return contact::evaluate_current(q.kind, f, s, C.separation);
+        }();
         for (int k = 0; k < q.fc; ++k) {
-            f.prev[k] = world_of(c, c.pos_in[q.f[k]]);
-            f.cur[k] = world_of(c, C.snapshot[q.f[k]]);
+            const float w = C.snapshot[q.f[k]].w;
+            out.addr[k] = slot_addr(c, q.f[k]);
+            out.inv[k] = w;
+            eff += static_cast<double>(w) * g.fw[k] * g.fw[k];
         }
         for (int k = 0; k < q.sc; ++k) {
-            s.prev[k] = world_of(c, c.pos_in[q.s[k]]);
-            s.cur[k] = world_of(c, C.snapshot[q.s[k]]);
+            const float w = C.snapshot[q.s[k]].w;
+            out.addr[q.fc + k] = slot_addr(c, q.s[k]);
+            out.inv[q.fc + k] = w;
+            eff += static_cast<double>(w) * g.sw[k] * g.sw[k];
         }
-        const contact::Ccd ccd = contact::swept_contact(q.kind, f, s, C.separation, C.ccd, queue);
-        const contact::Closest g = contact::evaluate_current(q.kind, f, s, C.separation);
-        ContactQuery& out = C.query[i];
+        out.eff = eff;
+        out.fc = static_cast<uint32_t>(q.fc);
+        out.sc = static_cast<uint32_t>(q.sc);
         for (int k = 0; k < 3; ++k) {
             out.fw[k] = g.fw[k];
             out.sw[k] = g.sw[k];
         }
         out.normal[0] = g.normal.x; out.normal[1] = g.normal.y; out.normal[2] = g.normal.z;
+        out.certified = g.certified() ? 1u : 0u;
+        const contact::Ccd ccd = contact::swept_contact(q.kind, f, s, C.separation, C.ccd, queue);
         out.ccd_normal[0] = ccd.geometry.normal.x;
         out.ccd_normal[1] = ccd.geometry.normal.y;
         out.ccd_normal[2] = ccd.geometry.normal.z;
         out.ccd_state = ccd.state;
-        out.certified = g.certified() ? 1u : 0u;
     }
 }
 
 // ---- serial passes (rank 0, thread 0) ---------------------------------------
 
-struct LiveFeature {
-    float4* f[3];
-    float4* s[3];
-    double fw_inv[3], sw_inv[3];  // inverse masses
-};
-
-__device__ __forceinline__ LiveFeature live_feature(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
-                                                    float4* local, const FeatureSlots& q) {
-    LiveFeature l;
-    for (int k = 0; k < q.fc; ++k) {
-        l.f[k] = slot_node(c, cluster, local, q.f[k]);
-        l.fw_inv[k] = static_cast<double>(slot_node(c, cluster, c.x, q.f[k])->w);
-    }
-    for (int k = 0; k < q.sc; ++k) {
-        l.s[k] = slot_node(c, cluster, local, q.s[k]);
-        l.sw_inv[k] = static_cast<double>(slot_node(c, cluster, c.x, q.s[k])->w);
-    }
-    return l;
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
-// Weighted point of live positions (weightedPoint, contact.cpp:1010-1019).
-__device__ __forceinline__ D3 weighted_point(const ContactCtx& c, float4* const* nodes, int count, const double* w) {
+// Weighted point of a primitive's live nodes (weightedPoint,
+// contact.cpp:1010-1019), streaming the nodes from distributed shared memory.
+__device__ __forceinline__ D3 weighted_live(const ContactCtx& c, const uint32_t* addr, uint32_t n, const double* w) {
     D3 r{0.0, 0.0, 0.0};
-    for (int k = 0; k < count; ++k) r = r + w[k] * world_of(c, *nodes[k]);
+    for (uint32_t k = 0; k < 3; ++k)
+        if (k < n) r = r + w[k] * world_of(c, ld_node(addr[k]));
     return r;
-}
-
-__device__ __forceinline__ void move_node(const ContactCtx& c, float4* node, D3 delta) {
-    float4 X = *node;
-    const D3 p = world_of(c, X) + delta;
-    X.x = static_cast<float>(p.x - c.o[0]);
-    X.y = static_cast<float>(p.y - c.o[1]);
-    X.z = static_cast<float>(p.z - c.o[2]);
-    *node = X;
 }
 
 __device__ __forceinline__ D3 d3_of(const double* v) { return {v[0], v[1], v[2]}; }
@@ -302,9 +303,11 @@ __device__ __forceinline__ bool push_entry(const ContactDev& C, ContactEntry* ou
     return true;
 }
 
+constexpr int kContactPrefetch = 4;  // candidates fetched ahead by the serial passes
+
 // One contact iteration's projections in key order (contact.cpp:1281-1457):
 // warm-started multipliers merged into the other table buffer.
-static __device__ __noinline__ void contact_project_serial(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
+static __device__ __noinline__ void contact_project_serial(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     if (contact_failed(c.status)) return;
     const unsigned long long count = C.offsets[C.nv + C.ne];
@@ -316,12 +319,18 @@ static __device__ __noinline__ void contact_project_serial(const ContactCtx& c, 
     const double alpha = C.compliance / (dt * dt);
     const double margin = contact::dmax(0.1 * C.separation, 8.0 * C.ccd.distance_tolerance);
     for (unsigned long long i = 0; i < count; ++i) {
+        if (i + kContactPrefetch < count) {
+            prefetch_l1(C.query + i + kContactPrefetch);
+            prefetch_l1(reinterpret_cast<const char*>(C.query + i + kContactPrefetch) + 128);
+            prefetch_l1(C.cand + i + kContactPrefetch);
+        }
         const ContactQuery& Q = C.query[i];
-        if (Q.ccd_state == SWB_CCD_INDETERMINATE) {
+        const uint32_t state = Q.ccd_state;
+        if (state == SWB_CCD_INDETERMINATE) {
             contact_fail(c.status, kContactCcd);
             return;
         }
-        if (Q.ccd_state == SWB_CCD_NO_IMPACT) continue;
+        if (state == SWB_CCD_NO_IMPACT) continue;
         const unsigned long long code = C.cand[i];
         while (k < old_n && old[k].code < code)
             if (!push_entry(C, nw, m, old[k++], c.status)) return;
@@ -335,6 +344,7 @@ static __device__ __noinline__ void contact_project_serial(const ContactCtx& c, 
             e.flags = 0;
             e.pad = 0;
         }
+        if (k < old_n) prefetch_l1(old + k);
         if (!Q.certified) {
             contact_fail(c.status, kContactGeometry);
             return;
@@ -345,17 +355,15 @@ static __device__ __noinline__ void contact_project_serial(const ContactCtx& c, 
             contact_fail(c.status, kContactNormal);
             return;
         }
-        const FeatureSlots q = feature_slots(C, code);
-        const LiveFeature L = live_feature(c, cluster, c.x, q);
-        const double gap = contact::dot(weighted_point(c, L.f, q.fc, Q.fw) - weighted_point(c, L.s, q.sc, Q.sw), normal) -
-                           C.separation;
+        const uint32_t fc = Q.fc, sc = Q.sc, n = fc + sc;
+        const double gap =
+            contact::dot(weighted_live(c, Q.addr, fc, Q.fw) - weighted_live(c, Q.addr + fc, sc, Q.sw), normal) -
+            C.separation;
         if (gap > margin && e.lambda == 0.0) {
             if (!push_entry(C, nw, m, e, c.status)) return;
             continue;
         }
-        double eff = 0.0;
-        for (int j = 0; j < q.fc; ++j) eff += L.fw_inv[j] * Q.fw[j] * Q.fw[j];
-        for (int j = 0; j < q.sc; ++j) eff += L.sw_inv[j] * Q.sw[j] * Q.sw[j];
+        const double eff = Q.eff;
         if (!(eff + alpha > 0.0)) {
             if (gap < 0.0) {
                 contact_fail(c.status, kContactNoResponse);
@@ -372,15 +380,19 @@ static __device__ __noinline__ void contact_project_serial(const ContactCtx& c, 
             return;
         }
         e.lambda = next;
-        for (int j = 0; j < q.fc; ++j) {
-            const D3 impulse = (Q.fw[j] * (applied / dt)) * normal;
-            move_node(c, L.f[j], impulse * (L.fw_inv[j] * dt));
+        // impulse w (applied / dt) n on the first primitive, the opposite on
+        // the second; positions move by m^-1 dt impulse (contact.cpp:1404-1417)
+        for (uint32_t j = 0; j < n; ++j) {
+            const double w = j < fc ? Q.fw[j] : -Q.sw[j - fc];
+            const D3 impulse = (w * (applied / dt)) * normal;
+            float4 X = ld_node(Q.addr[j]);
+            const D3 p = world_of(c, X) + impulse * (static_cast<double>(Q.inv[j]) * dt);
+            X.x = static_cast<float>(p.x - c.o[0]);
+            X.y = static_cast<float>(p.y - c.o[1]);
+            X.z = static_cast<float>(p.z - c.o[2]);
+            st_node(Q.addr[j], X);
         }
-        for (int j = 0; j < q.sc; ++j) {
-            const D3 impulse = (-Q.sw[j] * (applied / dt)) * normal;
-            move_node(c, L.s[j], impulse * (L.sw_inv[j] * dt));
-        }
-        const D3 fp = weighted_point(c, L.f, q.fc, Q.fw), sp = weighted_point(c, L.s, q.sc, Q.sw);
+        const D3 fp = weighted_live(c, Q.addr, fc, Q.fw), sp = weighted_live(c, Q.addr + fc, sc, Q.sw);
         const double solved = contact::dot(fp - sp, normal) - C.separation;
         if (!contact::finite3(fp) || !contact::finite3(sp) || !isfinite(solved)) {
             contact_fail(c.status, kContactSolved);
@@ -410,8 +422,7 @@ static __device__ __noinline__ void contact_project_serial(const ContactCtx& c, 
 // The certification of the final state (contact.cpp:1800-2078): certified
 // records of the candidates the swept query finds in contact, retained
 // records of earlier solver visits, in key order.
-static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
-                                                    ContactDiagDev* diag) {
+static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, ContactDiagDev* diag) {
     const ContactDev& C = *c.C;
     if (contact_failed(c.status)) return;
     const unsigned long long count = C.offsets[C.nv + C.ne];
@@ -422,6 +433,10 @@ static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, 
     unsigned long long records = 0, active = 0;
     double max_pen = 0.0;
     for (unsigned long long i = 0; i < count; ++i) {
+        if (i + kContactPrefetch < count) {
+            prefetch_l1(C.query + i + kContactPrefetch);
+            prefetch_l1(C.cand + i + kContactPrefetch);
+        }
         const unsigned long long code = C.cand[i];
         while (k < tn && tab[k].code < code) {
             if (tab[k].flags & kEntryRecord) {
@@ -445,9 +460,8 @@ static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, 
         }
         D3 normal = d3_of(Q.normal);
         if (contact::dot(normal, impact ? d3_of(Q.ccd_normal) : d3_of(e->normal)) < 0.0) normal = -normal;
-        const FeatureSlots q = feature_slots(C, code);
-        const LiveFeature L = live_feature(c, cluster, c.x, q);
-        const D3 fp = weighted_point(c, L.f, q.fc, Q.fw), sp = weighted_point(c, L.s, q.sc, Q.sw);
+        const uint32_t fc = Q.fc, sc = Q.sc;
+        const D3 fp = weighted_live(c, Q.addr, fc, Q.fw), sp = weighted_live(c, Q.addr + fc, sc, Q.sw);
         const double gap = contact::dot(fp - sp, normal) - C.separation;
         if (impact && (!contact::finite3(fp) || !contact::finite3(sp) || !contact::finite3(normal) || !isfinite(gap))) {
             contact_fail(c.status, kContactFinalNonFinite);
@@ -468,6 +482,13 @@ static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, 
             r.fw[j] = Q.fw[j];
             r.sw[j] = Q.sw[j];
         }
+        for (int j = 0; j < 6; ++j) {
+            r.addr[j] = Q.addr[j];
+            r.inv[j] = Q.inv[j];
+        }
+        r.fc = fc;
+        r.sc = sc;
+        r.eff = Q.eff;
         r.normal[0] = normal.x; r.normal[1] = normal.y; r.normal[2] = normal.z;
         r.lambda = e ? e->lambda : 0.0;
         r.active = impact && r.lambda > 0.0 ? 1u : 0u;
@@ -488,45 +509,43 @@ static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, 
 
 // Coulomb friction of the certified records on the finalized velocities,
 // in key order (contact.cpp:2081-2147).
-static __device__ __noinline__ void contact_friction_serial(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
-                                                     const ContactDiagDev* diag) {
+static __device__ __noinline__ void contact_friction_serial(const ContactCtx& c, const ContactDiagDev* diag) {
     const ContactDev& C = *c.C;
     if (contact_failed(c.status)) return;
     const double dt = c.dt;
-    for (unsigned long long i = 0; i < diag->records; ++i) {
+    const unsigned long long records = diag->records;
+    for (unsigned long long i = 0; i < records; ++i) {
+        if (i + kContactPrefetch < records) {
+            prefetch_l1(C.records + i + kContactPrefetch);
+            prefetch_l1(reinterpret_cast<const char*>(C.records + i + kContactPrefetch) + 128);
+        }
         const ContactRecordDev& r = C.records[i];
-        const FeatureSlots q = feature_slots(C, r.code);
-        const LiveFeature V = live_feature(c, cluster, c.v, q);
+        const uint32_t fc = r.fc, sc = r.sc, n = fc + sc;
+        float4 V[6];
+        for (uint32_t j = 0; j < 6; ++j)
+            if (j < n) V[j] = ld_node(r.addr[j] + c.v_delta);
         D3 vf{0.0, 0.0, 0.0}, vs{0.0, 0.0, 0.0};
-        double eff = 0.0;
-        for (int j = 0; j < q.fc; ++j) {
-            const float4 W = *V.f[j];
-            vf = vf + r.fw[j] * D3{W.x, W.y, W.z};
-            eff += V.fw_inv[j] * r.fw[j] * r.fw[j];
+        for (uint32_t j = 0; j < 3; ++j) {
+            if (j < fc) vf = vf + r.fw[j] * D3{V[j].x, V[j].y, V[j].z};
+            if (j < sc) vs = vs + r.sw[j] * D3{V[fc + j].x, V[fc + j].y, V[fc + j].z};
         }
-        for (int j = 0; j < q.sc; ++j) {
-            const float4 W = *V.s[j];
-            vs = vs + r.sw[j] * D3{W.x, W.y, W.z};
-            eff += V.sw_inv[j] * r.sw[j] * r.sw[j];
-        }
-        const contact::Friction fr = contact::coulomb_friction(vf - vs, d3_of(r.normal), eff, r.lambda / dt,
+        const contact::Friction fr = contact::coulomb_friction(vf - vs, d3_of(r.normal), r.eff, r.lambda / dt,
                                                                C.static_mu, C.dynamic_mu, r.active != 0);
         if (!contact::finite3(fr.impulse) || !isfinite(fr.work) ||
             fr.work > 1.0e-12 * contact::dmax(1.0, contact::norm2(fr.initial_tangent))) {
             contact_fail(c.status, kContactFriction);
             return;
         }
-        for (int j = 0; j < q.fc; ++j) {
-            const D3 dv = (r.fw[j] * fr.impulse) * V.fw_inv[j];
-            float4 W = *V.f[j];
-            W.x = static_cast<float>(W.x + dv.x); W.y = static_cast<float>(W.y + dv.y); W.z = static_cast<float>(W.z + dv.z);
-            *V.f[j] = W;
-        }
-        for (int j = 0; j < q.sc; ++j) {
-            const D3 dv = (-r.sw[j] * fr.impulse) * V.sw_inv[j];
-            float4 W = *V.s[j];
-            W.x = static_cast<float>(W.x + dv.x); W.y = static_cast<float>(W.y + dv.y); W.z = static_cast<float>(W.z + dv.z);
-            *V.s[j] = W;
+        if (fr.state == contact::kFrictionInactive) continue;  // no impulse
+        for (uint32_t j = 0; j < 6; ++j) {
+            if (j >= n) break;
+            const double w = j < fc ? r.fw[j] : -r.sw[j - fc];
+            const D3 dv = (w * fr.impulse) * static_cast<double>(r.inv[j]);
+            float4 W = V[j];
+            W.x = static_cast<float>(W.x + dv.x);
+            W.y = static_cast<float>(W.y + dv.y);
+            W.z = static_cast<float>(W.z + dv.z);
+            st_node(r.addr[j] + c.v_delta, W);
         }
     }
 }
@@ -552,21 +571,21 @@ __device__ __forceinline__ void contact_detect(const ContactCtx& c, cooperative_
 
 __device__ __forceinline__ void contact_iteration(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
     contact_detect(c, cluster);
-    if (c.me == 0 && threadIdx.x == 0) contact_project_serial(c, cluster);
+    if (c.me == 0 && threadIdx.x == 0) contact_project_serial(c);
     cluster.sync();
 }
 
 __device__ __forceinline__ void contact_certify(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
                                                 ContactDiagDev* diag) {
     contact_detect(c, cluster);
-    if (c.me == 0 && threadIdx.x == 0) contact_certify_serial(c, cluster, diag);
+    if (c.me == 0 && threadIdx.x == 0) contact_certify_serial(c, diag);
     cluster.sync();
 }
 
 __device__ __forceinline__ void contact_friction(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
                                                  const ContactDiagDev* diag) {
     cluster.sync();  // every CTA has finalized its velocities
-    if (c.me == 0 && threadIdx.x == 0) contact_friction_serial(c, cluster, diag);
+    if (c.me == 0 && threadIdx.x == 0) contact_friction_serial(c, diag);
     cluster.sync();
 }
 

@@ -185,6 +185,9 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
         std::vector<int> candidates;
         if (opt.cluster_ctas > 0) {
             candidates.push_back(opt.cluster_ctas);
+        } else if (def.has_contact) {
+            // the contact phases run over the whole cluster: the widest that fits
+            for (int c = kClusterMaxCtas; c >= 1; c /= 2) candidates.push_back(c);
         } else {
             int c = 1;
             while (c < kClusterMaxCtas && static_cast<uint64_t>(c) * 2048 < N) c *= 2;
@@ -250,6 +253,7 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
                   ? opt.block_threads
                   : static_cast<int>(std::clamp<uint32_t>((widest + 31) / 32 * 32, 64,
                                                           cluster_mode ? dev::kClusterMaxThreads : 512));
+    if (opt.block_threads <= 0 && cluster_mode && def.has_contact) threads = dev::kClusterMaxThreads;
     if (threads % 32 != 0 || threads < 32 || threads > (cluster_mode ? dev::kClusterMaxThreads : 1024))
         raise(SWB_INVALID_ARGUMENT, "block_threads out of range for the chosen schedule");
     if (cluster_mode && csched.line_stage >= 0) {

@@ -41,36 +41,10 @@ def two_sheets():
     return sw.definition_from_arrays(nodes, [(0, 1, 2), (3, 4, 5)], contact=(0.01, 0.0, 0.0, 0.0))
 
 
-def stacked_sheets(n=8, gap=0.003, half=0.002, friction=(0.4, 0.25), spacing=0.05, compliance=0.0):
-    """A free sheet with distance constraints resting 1 mm inside the contact
-    envelope of a pinned sheet below it, shifted so that vertices, edges and
-    faces of the two meet in every feature configuration."""
-    nodes, tris, cons = [], [], []
-    for layer, z in ((0, 0.0), (1, gap)):
-        off = len(nodes)
-        for j in range(n):
-            for i in range(n):
-                x, y = i * spacing, j * spacing
-                if layer:
-                    x, y = x + 0.013, y + 0.007
-                nodes.append((x, y, z, 0.001, layer == 0))
-        for j in range(n - 1):
-            for i in range(n - 1):
-                a = off + j * n + i
-                b, c, d = a + 1, a + n, a + n + 1
-                tris += [(a, b, d), (a, d, c)]
-                if layer:
-                    for u, v in ((a, b), (a, c), (a, d)):
-                        rest = float(np.linalg.norm(np.subtract(nodes[u][:3], nodes[v][:3])))
-                        cons.append((1, u, v, rest, 1e-7))
-        if layer:
-            for j in range(n - 1):
-                a = off + j * n + n - 1
-                cons.append((1, a, a + n, spacing, 1e-7))
-            for i in range(n - 1):
-                a = off + (n - 1) * n + i
-                cons.append((1, a, a + 1, spacing, 1e-7))
-    return sw.definition_from_arrays(nodes, tris, cons, contact=(half, compliance, friction[0], friction[1]))
+def stacked_sheets(**kw):
+    """A free sheet resting 1 mm inside the contact envelope of a pinned sheet
+    below it (simwing_b200.stacked_sheets)."""
+    return sw.stacked_sheets(**kw)
 
 
 SLIDE = step_settings(iterations=8, gravity=(2.0, 0.0, -9.81))  # tilted gravity: static and dynamic friction
