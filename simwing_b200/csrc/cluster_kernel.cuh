@@ -357,6 +357,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         cctx.dt = p.dt64;
         cctx.status = I.status;
         cctx.x_base = smem_addr(x);
+        cctx.node_level = p.smem_levels ? reinterpret_cast<uint32_t*>(smem + p.smem_levels) : I.contact->node_level;
         cctx.v_delta = smem_addr(v) - smem_addr(x);
         // multipliers and records restart every substep (beginContactSubstep,
         // contact.cpp:1043-1055)

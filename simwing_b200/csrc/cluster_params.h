@@ -48,6 +48,7 @@ struct ContactQuery {
     double ccd_normal[3];    // normal of the swept query's geometry
     double eff;              // effective inverse mass sum w_i m_i^-1 w_i
     uint32_t addr[6];        // cluster shared-memory addresses of the nodes: first, then second primitive
+    uint32_t slot[6];        // their slots
     float inv[6];            // their inverse masses
     uint32_t ccd_state;      // SWB_CCD_*
     uint32_t certified;      // the snapshot geometry is certified
@@ -73,7 +74,8 @@ struct ContactRecordDev {
     double normal[3];
     double lambda;
     double eff;              // effective inverse mass
-    uint32_t addr[6];        // node addresses, as in ContactQuery
+    uint32_t addr[6];        // node addresses and slots, as in ContactQuery
+    uint32_t slot[6];
     float inv[6];
     uint32_t fc, sc;
     uint32_t active;         // normal multiplier > 0 and swept state not NoImpact
@@ -113,6 +115,21 @@ struct ContactDev {
     unsigned long long table_cap;
     ContactRecordDev* records;         // [record_cap]
     unsigned long long record_cap;
+    // level schedule of a key-ordered pass: an item's level is one more than
+    // the last level among the earlier items sharing one of its nodes, so
+    // the items of a level share no node and run together
+    uint32_t* node_level;              // [slots]
+    uint32_t* item_level;              // [cand_cap]
+    uint32_t* level_start;             // [cand_cap + 2]
+    uint32_t* level_fill;              // [cand_cap + 2]
+    uint32_t* level_items;             // [cand_cap]
+    uint32_t* level_meta;              // [0] levels
+    uint32_t* hit;                     // [cand_cap] the candidates in contact, in key order
+    uint32_t* mark_a;                  // [cand_cap + 1] per-candidate flags, then their exclusive scan
+    uint32_t* mark_b;                  // [cand_cap + 1] per-table-entry flags, then their exclusive scan
+    ContactEntry* cand_entry;          // [cand_cap] the candidate's table entry after the iteration
+    ContactRecordDev* cand_rec;        // [cand_cap] the candidate's certified record
+    unsigned long long* reduce;        // [2] active records, largest penetration (bits)
 };
 
 // Per-instance tables and state (one cluster each).
@@ -229,6 +246,7 @@ struct ClusterParams {
     long long copy_budget;
     uint32_t smem_x, smem_v;       // byte offsets of node and force/velocity arrays
     uint32_t smem_offsets;         // byte offset of the CTA's stage offsets
+    uint32_t smem_levels;          // contact: byte offset of rank 0's node levels (slots x u32), 0 = global
     TapeStep tape;                 // taping launches: where this step's tape goes
 };
 

@@ -73,6 +73,7 @@ struct ContactCtx {
     int* status;
     uint32_t x_base;           // shared address of this CTA's node array
     uint32_t v_delta;          // offset from the node array to the velocity array
+    uint32_t* node_level;      // rank 0: node levels of the key-ordered passes (shared or global memory)
 };
 
 using contact::D3;
@@ -250,12 +251,14 @@ __device__ __noinline__ void contact_queries(const ContactCtx& c) {
         for (int k = 0; k < q.fc; ++k) {
             const float w = C.snapshot[q.f[k]].w;
             out.addr[k] = slot_addr(c, q.f[k]);
+            out.slot[k] = q.f[k];
             out.inv[k] = w;
             eff += static_cast<double>(w) * g.fw[k] * g.fw[k];
         }
         for (int k = 0; k < q.sc; ++k) {
             const float w = C.snapshot[q.s[k]].w;
             out.addr[q.fc + k] = slot_addr(c, q.s[k]);
+            out.slot[q.fc + k] = q.s[k];
             out.inv[q.fc + k] = w;
             eff += static_cast<double>(w) * g.sw[k] * g.sw[k];
         }
@@ -276,10 +279,11 @@ __device__ __noinline__ void contact_queries(const ContactCtx& c) {
     }
 }
 
-// ---- serial passes (rank 0, thread 0) ---------------------------------------
+// ---- key-ordered passes, level by level ---------------------------------------
 
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+__device__ __forceinline__ uint32_t cluster_tid(const ContactCtx& c) { return c.me * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint32_t cluster_threads(const ContactCtx& c) {
+    return static_cast<uint32_t>(c.ctas) * blockDim.x;
 }
 
 // Weighted point of a primitive's live nodes (weightedPoint,
@@ -293,170 +297,373 @@ __device__ __forceinline__ D3 weighted_live(const ContactCtx& c, const uint32_t*
 
 __device__ __forceinline__ D3 d3_of(const double* v) { return {v[0], v[1], v[2]}; }
 
-__device__ __forceinline__ bool push_entry(const ContactDev& C, ContactEntry* out, uint32_t& m, const ContactEntry& e,
-                                           int* status) {
-    if (m >= C.table_cap) {
-        contact_fail(status, kContactTable);
-        return false;
+// First index in the sorted codes[0..n) whose code is not below `code`.
+template <class Code>
+__device__ __forceinline__ uint32_t lower_bound_code(Code code_at, uint32_t n, unsigned long long code) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (code_at(mid) < code) lo = mid + 1;
+        else hi = mid;
     }
-    out[m++] = e;
-    return true;
+    return lo;
 }
 
-constexpr int kContactPrefetch = 4;  // candidates fetched ahead by the serial passes
+// Exclusive scan of in[0..n) into out[0..n] (in place allowed) by the
+// calling block.
+__device__ __noinline__ void block_scan(const uint32_t* in, uint32_t n, uint32_t* out) {
+    __shared__ uint32_t warp_total[32];
+    const uint32_t t = threadIdx.x, threads = blockDim.x;
+    const uint32_t chunk = (n + threads - 1) / threads;
+    const uint32_t lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    uint32_t own = 0;
+    for (uint32_t i = lo; i < hi; ++i) own += in[i];
+    uint32_t incl = own;
+    const uint32_t lane = t & 31, warp = t >> 5;
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= static_cast<uint32_t>(d)) incl += y;
+    }
+    if (lane == 31) warp_total[warp] = incl;
+    __syncthreads();
+    if (t == 0) {
+        uint32_t run = 0;
+        for (uint32_t w = 0; w < (threads + 31) / 32; ++w) {
+            const uint32_t y = warp_total[w];
+            warp_total[w] = run;
+            run += y;
+        }
+    }
+    __syncthreads();
+    uint32_t at = warp_total[warp] + incl - own;
+    for (uint32_t i = lo; i < hi; ++i) {
+        const uint32_t v = in[i];
+        out[i] = at;
+        at += v;
+    }
+    if (t == threads - 1) out[n] = at;
+    __syncthreads();
+}
 
-// One contact iteration's projections in key order (contact.cpp:1281-1457):
-// warm-started multipliers merged into the other table buffer.
-static __device__ __noinline__ void contact_project_serial(const ContactCtx& c) {
+// Folds a batch of up to 32 items, one per lane of the calling warp, into
+// the node levels in lane order (lane 0 does the folding); returns the
+// largest level so far.
+static __device__ __noinline__ uint32_t fold_levels(uint32_t* level, uint32_t* item_level, uint32_t batch,
+                                                    uint32_t mine_n, const uint32_t* mine, uint32_t levels) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t m0 = mine[0], m1 = mine[1], m2 = mine[2], m3 = mine[3], m4 = mine[4], m5 = mine[5];
+    for (uint32_t k = 0; k < batch; ++k) {
+        const uint32_t n = __shfl_sync(0xffffffffu, mine_n, k);
+        const uint32_t s0 = __shfl_sync(0xffffffffu, m0, k), s1 = __shfl_sync(0xffffffffu, m1, k);
+        const uint32_t s2 = __shfl_sync(0xffffffffu, m2, k), s3 = __shfl_sync(0xffffffffu, m3, k);
+        const uint32_t s4 = __shfl_sync(0xffffffffu, m4, k), s5 = __shfl_sync(0xffffffffu, m5, k);
+        if (lane == 0) {
+            uint32_t l = 0;
+            if (n) {
+                l = level[s0];
+                if (n > 1) l = max(l, level[s1]);
+                if (n > 2) l = max(l, level[s2]);
+                if (n > 3) l = max(l, level[s3]);
+                if (n > 4) l = max(l, level[s4]);
+                if (n > 5) l = max(l, level[s5]);
+                ++l;
+                level[s0] = l;
+                if (n > 1) level[s1] = l;
+                if (n > 2) level[s2] = l;
+                if (n > 3) level[s3] = l;
+                if (n > 4) level[s4] = l;
+                if (n > 5) level[s5] = l;
+                levels = max(levels, l);
+            }
+            item_level[k] = l;
+        }
+    }
+    return levels;
+}
+
+// Levels of `items` in order (rank 0's block): get(i, slots) returns the
+// item's nodes (0: the item takes no level).  The lanes of warp 0 fetch the
+// nodes of 32 consecutive items at once and lane 0 folds them into the node
+// levels in order; the level sizes are then counted by the block and
+// scanned.  Leaves the levels' starts in level_start[1 .. levels + 1] and the
+// level count in level_meta[0].
+template <class Get>
+__device__ __forceinline__ void assign_levels(const ContactCtx& c, uint32_t items, uint32_t slots, Get get) {
     const ContactDev& C = *c.C;
-    if (contact_failed(c.status)) return;
-    const unsigned long long count = C.offsets[C.nv + C.ne];
-    const uint32_t sel = C.table_meta[0], old_n = C.table_meta[1];
-    const ContactEntry* old = C.table[sel];
-    ContactEntry* nw = C.table[sel ^ 1u];
-    uint32_t k = 0, m = 0;
+    uint32_t* level = c.node_level;
+    for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) level[i] = 0;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const uint32_t lane = threadIdx.x;
+        uint32_t levels = 0;
+        for (uint32_t base = 0; base < items; base += 32) {
+            uint32_t mine[6] = {0, 0, 0, 0, 0, 0};
+            const uint32_t mine_n = base + lane < items ? get(base + lane, mine) : 0u;
+            const uint32_t batch = min(32u, items - base);
+            levels = fold_levels(level, C.item_level + base, batch, mine_n, mine, levels);
+        }
+        if (lane == 0) C.level_meta[0] = levels;
+    }
+    __syncthreads();
+    const uint32_t levels = C.level_meta[0];
+    for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) {
+        const uint32_t l = C.item_level[i];
+        if (l) atomicAdd(&C.level_start[l], 1u);
+    }
+    __syncthreads();
+    block_scan(C.level_start + 1, levels, C.level_start + 1);
+}
+
+// Clears the level tables for `items` items (every thread of the cluster).
+__device__ __forceinline__ void reset_levels(const ContactCtx& c, uint32_t items, uint32_t slots) {
+    const ContactDev& C = *c.C;
+    const uint32_t gt = cluster_tid(c), stride = cluster_threads(c);
+    (void)slots;
+    for (uint32_t i = gt; i < items + 2; i += stride) {
+        C.level_start[i] = 0;
+        C.level_fill[i] = 0;
+    }
+}
+
+// Buckets the items by level (every thread of the calling block); a bucket
+// holds id[item], or the item itself without `id`.
+__device__ __forceinline__ void scatter_levels(const ContactDev& C, uint32_t items, const uint32_t* id = nullptr) {
+    for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) {
+        const uint32_t l = C.item_level[i];
+        if (l) C.level_items[C.level_start[l] + atomicAdd(&C.level_fill[l], 1u)] = id ? id[i] : i;
+    }
+    __syncthreads();
+}
+
+// Runs work(item) level by level inside the calling block: the items of a
+// level touch disjoint nodes.  The nodes may live in any CTA of the
+// cluster, but only this block's threads touch them until the cluster
+// barrier that follows, so a block barrier orders one level's writes before
+// the next level's reads.
+template <class Work>
+__device__ __forceinline__ void run_levels(const ContactDev& C, Work work) {
+    const uint32_t levels = C.level_meta[0];
+    for (uint32_t l = 1; l <= levels; ++l) {
+        const uint32_t lo = C.level_start[l], hi = C.level_start[l + 1];
+        for (uint32_t k = lo + threadIdx.x; k < hi; k += blockDim.x) work(C.level_items[k]);
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ bool impact_state(uint32_t s) {
+    return s == SWB_CCD_IMPACT || s == SWB_CCD_INITIALLY_PROXIMATE;
+}
+
+// The record book's flags after an iteration in which the entry was not
+// visited: it stays a record only when it applied an impulse
+// (contact.cpp:1462-1495).
+__device__ __forceinline__ uint32_t carried_flags(uint32_t f) {
+    return ((f & kEntryRecord) && (f & kEntryApplied)) ? (kEntryRecord | kEntryApplied) : 0u;
+}
+
+// One candidate's projection (contact.cpp:1318-1457): warm start from its
+// entry of the previous table (copied into cand_entry beforehand), the XPBD
+// normal projection on the live nodes, its entry for the next table.
+static __device__ __noinline__ void project_one(const ContactCtx& c, uint32_t i) {
+    const ContactDev& C = *c.C;
+    const ContactQuery& Q = C.query[i];
+    ContactEntry& out = C.cand_entry[i];
+    ContactEntry e = out;  // the warm start
+    if (!Q.certified) {
+        contact_fail(c.status, kContactGeometry);
+        return;
+    }
+    D3 normal = d3_of(Q.normal);
+    if (contact::dot(normal, d3_of(Q.ccd_normal)) < 0.0) normal = -normal;
+    if (!contact::finite3(normal) || fabs(contact::norm2(normal) - 1.0) > 1.0e-8) {
+        contact_fail(c.status, kContactNormal);
+        return;
+    }
     const double dt = c.dt;
     const double alpha = C.compliance / (dt * dt);
     const double margin = contact::dmax(0.1 * C.separation, 8.0 * C.ccd.distance_tolerance);
-    for (unsigned long long i = 0; i < count; ++i) {
-        if (i + kContactPrefetch < count) {
-            prefetch_l1(C.query + i + kContactPrefetch);
-            prefetch_l1(reinterpret_cast<const char*>(C.query + i + kContactPrefetch) + 128);
-            prefetch_l1(C.cand + i + kContactPrefetch);
-        }
-        const ContactQuery& Q = C.query[i];
-        const uint32_t state = Q.ccd_state;
-        if (state == SWB_CCD_INDETERMINATE) {
-            contact_fail(c.status, kContactCcd);
-            return;
-        }
-        if (state == SWB_CCD_NO_IMPACT) continue;
-        const unsigned long long code = C.cand[i];
-        while (k < old_n && old[k].code < code)
-            if (!push_entry(C, nw, m, old[k++], c.status)) return;
-        ContactEntry e;
-        if (k < old_n && old[k].code == code) {
-            e = old[k++];
-        } else {
-            e.code = code;
-            e.lambda = 0.0;
-            e.normal[0] = e.normal[1] = e.normal[2] = 0.0;
-            e.flags = 0;
-            e.pad = 0;
-        }
-        if (k < old_n) prefetch_l1(old + k);
-        if (!Q.certified) {
-            contact_fail(c.status, kContactGeometry);
-            return;
-        }
-        D3 normal = d3_of(Q.normal);
-        if (contact::dot(normal, d3_of(Q.ccd_normal)) < 0.0) normal = -normal;
-        if (!contact::finite3(normal) || fabs(contact::norm2(normal) - 1.0) > 1.0e-8) {
-            contact_fail(c.status, kContactNormal);
-            return;
-        }
-        const uint32_t fc = Q.fc, sc = Q.sc, n = fc + sc;
-        const double gap =
-            contact::dot(weighted_live(c, Q.addr, fc, Q.fw) - weighted_live(c, Q.addr + fc, sc, Q.sw), normal) -
-            C.separation;
-        if (gap > margin && e.lambda == 0.0) {
-            if (!push_entry(C, nw, m, e, c.status)) return;
-            continue;
-        }
-        const double eff = Q.eff;
-        if (!(eff + alpha > 0.0)) {
-            if (gap < 0.0) {
-                contact_fail(c.status, kContactNoResponse);
-                return;
-            }
-            if (!push_entry(C, nw, m, e, c.status)) return;
-            continue;
-        }
-        const double delta = (-gap - alpha * e.lambda) / (eff + alpha);
-        const double next = contact::dmax(0.0, e.lambda + delta);
-        const double applied = next - e.lambda;
-        if (!isfinite(next) || !isfinite(applied)) {
-            contact_fail(c.status, kContactProjection);
-            return;
-        }
-        e.lambda = next;
-        // impulse w (applied / dt) n on the first primitive, the opposite on
-        // the second; positions move by m^-1 dt impulse (contact.cpp:1404-1417)
-        for (uint32_t j = 0; j < n; ++j) {
-            const double w = j < fc ? Q.fw[j] : -Q.sw[j - fc];
-            const D3 impulse = (w * (applied / dt)) * normal;
-            float4 X = ld_node(Q.addr[j]);
-            const D3 p = world_of(c, X) + impulse * (static_cast<double>(Q.inv[j]) * dt);
-            X.x = static_cast<float>(p.x - c.o[0]);
-            X.y = static_cast<float>(p.y - c.o[1]);
-            X.z = static_cast<float>(p.z - c.o[2]);
-            st_node(Q.addr[j], X);
-        }
-        const D3 fp = weighted_live(c, Q.addr, fc, Q.fw), sp = weighted_live(c, Q.addr + fc, sc, Q.sw);
-        const double solved = contact::dot(fp - sp, normal) - C.separation;
-        if (!contact::finite3(fp) || !contact::finite3(sp) || !isfinite(solved)) {
-            contact_fail(c.status, kContactSolved);
-            return;
-        }
-        // a record continuing from the previous iteration keeps its impulse
-        // ledger; a new one starts it (contact.cpp:1391-1401)
-        const bool ledger = (e.flags & kEntryRecord) && (e.flags & kEntryApplied);
-        e.flags = (e.flags & kEntryRecord) | kEntryVisited | ((ledger || applied != 0.0) ? kEntryApplied : 0u);
-        e.normal[0] = normal.x; e.normal[1] = normal.y; e.normal[2] = normal.z;
-        if (!push_entry(C, nw, m, e, c.status)) return;
+    const uint32_t fc = Q.fc, sc = Q.sc;
+    // the first primitive's nodes in A, the second's in B (constant indices)
+    float4 A[3], B[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (k < static_cast<int>(fc)) A[k] = ld_node(Q.addr[k]);
+        if (k < static_cast<int>(sc)) B[k] = ld_node(Q.addr[fc + k]);
     }
-    while (k < old_n)
-        if (!push_entry(C, nw, m, old[k++], c.status)) return;
-    // the record book after the iteration: this iteration's visits plus the
-    // earlier records that applied an impulse (contact.cpp:1462-1495)
-    for (uint32_t j = 0; j < m; ++j) {
-        uint32_t f = nw[j].flags;
-        const bool record = (f & kEntryVisited) || ((f & kEntryRecord) && (f & kEntryApplied));
-        f = record ? ((f & kEntryApplied) | kEntryRecord) : 0u;
-        nw[j].flags = f;
+    auto point = [&](const float4* P, uint32_t count, const double* w) {
+        D3 r{0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (k < static_cast<int>(count)) r = r + w[k] * world_of(c, P[k]);
+        return r;
+    };
+    const double gap = contact::dot(point(A, fc, Q.fw) - point(B, sc, Q.sw), normal) - C.separation;
+    const double eff = Q.eff;
+    if ((gap > margin && e.lambda == 0.0) || !(eff + alpha > 0.0)) {
+        if (!(eff + alpha > 0.0) && gap < 0.0 && !(gap > margin && e.lambda == 0.0)) {
+            contact_fail(c.status, kContactNoResponse);
+            return;
+        }
+        e.flags = carried_flags(e.flags);
+        out = e;
+        return;
     }
-    C.table_meta[0] = sel ^ 1u;
-    C.table_meta[1] = m;
+    const double delta = (-gap - alpha * e.lambda) / (eff + alpha);
+    const double next = contact::dmax(0.0, e.lambda + delta);
+    const double applied = next - e.lambda;
+    if (!isfinite(next) || !isfinite(applied)) {
+        contact_fail(c.status, kContactProjection);
+        return;
+    }
+    // impulse w (applied / dt) n on the first primitive, the opposite on the
+    // second; positions move by m^-1 dt impulse (contact.cpp:1404-1417)
+    auto move = [&](float4& X, double w, float inv, uint32_t addr) {
+        const D3 impulse = (w * (applied / dt)) * normal;
+        const D3 p = world_of(c, X) + impulse * (static_cast<double>(inv) * dt);
+        X.x = static_cast<float>(p.x - c.o[0]);
+        X.y = static_cast<float>(p.y - c.o[1]);
+        X.z = static_cast<float>(p.z - c.o[2]);
+        st_node(addr, X);
+    };
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (k < static_cast<int>(fc)) move(A[k], Q.fw[k], Q.inv[k], Q.addr[k]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (k < static_cast<int>(sc)) move(B[k], -Q.sw[k], Q.inv[fc + k], Q.addr[fc + k]);
+    const D3 fp = point(A, fc, Q.fw), sp = point(B, sc, Q.sw);
+    const double solved = contact::dot(fp - sp, normal) - C.separation;
+    if (!contact::finite3(fp) || !contact::finite3(sp) || !isfinite(solved)) {
+        contact_fail(c.status, kContactSolved);
+        return;
+    }
+    // a record continuing from the previous iteration keeps its impulse
+    // ledger; a new one starts it (contact.cpp:1391-1401); visited, it is a
+    // record of this iteration
+    const bool ledger = (e.flags & kEntryRecord) && (e.flags & kEntryApplied);
+    e.lambda = next;
+    e.flags = kEntryRecord | ((ledger || applied != 0.0) ? kEntryApplied : 0u);
+    e.normal[0] = normal.x; e.normal[1] = normal.y; e.normal[2] = normal.z;
+    out = e;
 }
 
-// The certification of the final state (contact.cpp:1800-2078): certified
-// records of the candidates the swept query finds in contact, retained
-// records of earlier solver visits, in key order.
-static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, ContactDiagDev* diag) {
+// The contact iteration's projections in key order, level by level, and the
+// next multiplier table (the merge of this iteration's candidates in
+// contact with the previous table's other entries).
+__device__ __noinline__ void contact_project(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
     const ContactDev& C = *c.C;
-    if (contact_failed(c.status)) return;
-    const unsigned long long count = C.offsets[C.nv + C.ne];
+    const bool skip = contact_failed(c.status);
+    const uint32_t count = skip ? 0u : static_cast<uint32_t>(C.offsets[C.nv + C.ne]);
+    const uint32_t sel = C.table_meta[0], old_n = C.table_meta[1];
+    const ContactEntry* old = C.table[sel];
+    ContactEntry* nw = C.table[sel ^ 1u];
+    const uint32_t gt = cluster_tid(c), stride = cluster_threads(c);
+    const uint32_t slots = c.pbeg[c.ctas];
+    // reset
+    reset_levels(c, count, slots);
+    for (uint32_t k = gt; k < old_n; k += stride) C.mark_b[k] = 1u;
+    cluster.sync();
+    // in contact or not; warm-start entry; previous entries taken over
+    for (uint32_t i = gt; i < count; i += stride) {
+        const uint32_t s = C.query[i].ccd_state;
+        if (s == SWB_CCD_INDETERMINATE) contact_fail(c.status, kContactCcd);
+        const bool hit = impact_state(s);
+        C.mark_a[i] = hit ? 1u : 0u;
+        if (hit) {
+            const unsigned long long code = C.cand[i];
+            const uint32_t k = lower_bound_code([&](uint32_t m) { return old[m].code; }, old_n, code);
+            ContactEntry e;
+            if (k < old_n && old[k].code == code) {
+                e = old[k];
+                C.mark_b[k] = 0u;
+            } else {
+                e.code = code;
+                e.lambda = 0.0;
+                e.normal[0] = e.normal[1] = e.normal[2] = 0.0;
+                e.flags = 0;
+                e.pad = 0;
+            }
+            C.cand_entry[i] = e;  // the warm start, replaced by the projection's result
+        }
+    }
+    cluster.sync();
+    // ranks of the two merged lists; the candidates in contact, their levels
+    // and their projections, level by level (rank 0's block)
+    if (c.me == 0) {
+        block_scan(C.mark_a, count, C.mark_a);
+        block_scan(C.mark_b, old_n, C.mark_b);
+        if (!contact_failed(c.status)) {
+            const uint32_t hits = C.mark_a[count];
+            for (uint32_t i = threadIdx.x; i < count; i += blockDim.x)
+                if (C.mark_a[i + 1] != C.mark_a[i]) C.hit[C.mark_a[i]] = i;
+            __syncthreads();
+            assign_levels(c, hits, slots, [&](uint32_t h, uint32_t* s) -> uint32_t {
+                const ContactQuery& Q = C.query[C.hit[h]];
+                const uint32_t n = Q.fc + Q.sc;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) s[j] = j < static_cast<int>(n) ? Q.slot[j] : 0u;
+                return n;
+            });
+            scatter_levels(C, hits, C.hit);
+            run_levels(C, [&](uint32_t i) { project_one(c, i); });
+        }
+    }
+    cluster.sync();
+    if (contact_failed(c.status)) return;  // uniform: read after the barrier
+    // the next table: sorted union of the candidates in contact and the
+    // previous entries they did not take over (codes are disjoint)
+    const uint32_t hits = C.mark_a[count], kept = C.mark_b[old_n];
+    if (hits + kept > C.table_cap) {
+        if (gt == 0) contact_fail(c.status, kContactTable);
+        return;
+    }
+    for (uint32_t i = gt; i < count; i += stride) {
+        if (C.mark_a[i + 1] == C.mark_a[i]) continue;
+        const unsigned long long code = C.cand[i];
+        const uint32_t k = lower_bound_code([&](uint32_t m) { return old[m].code; }, old_n, code);
+        nw[C.mark_a[i] + C.mark_b[k]] = C.cand_entry[i];
+    }
+    for (uint32_t k = gt; k < old_n; k += stride) {
+        if (C.mark_b[k + 1] == C.mark_b[k]) continue;
+        ContactEntry e = old[k];
+        e.flags = carried_flags(e.flags);
+        const uint32_t i = lower_bound_code([&](uint32_t m) { return C.cand[m]; }, count, e.code);
+        nw[C.mark_b[k] + C.mark_a[i]] = e;
+    }
+    cluster.sync();
+    if (c.me == 0 && threadIdx.x == 0) {
+        C.table_meta[0] = sel ^ 1u;
+        C.table_meta[1] = hits + kept;
+    }
+}
+
+// The certification of the final state (contact.cpp:1800-2078): the
+// certified records of the candidates the swept query finds in contact and
+// the retained records of earlier solver visits, in key order.
+__device__ __noinline__ void contact_certify_all(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
+                                                 ContactDiagDev* diag) {
+    const ContactDev& C = *c.C;
+    const bool skip = contact_failed(c.status);
+    const uint32_t count = skip ? 0u : static_cast<uint32_t>(C.offsets[C.nv + C.ne]);
     const uint32_t sel = C.table_meta[0], tn = C.table_meta[1];
     const ContactEntry* tab = C.table[sel];
+    const uint32_t gt = cluster_tid(c), stride = cluster_threads(c);
     const double limit = contact::dmax(0.02 * C.separation, 1.0e-8);
-    uint32_t k = 0;
-    unsigned long long records = 0, active = 0;
-    double max_pen = 0.0;
-    for (unsigned long long i = 0; i < count; ++i) {
-        if (i + kContactPrefetch < count) {
-            prefetch_l1(C.query + i + kContactPrefetch);
-            prefetch_l1(C.cand + i + kContactPrefetch);
-        }
-        const unsigned long long code = C.cand[i];
-        while (k < tn && tab[k].code < code) {
-            if (tab[k].flags & kEntryRecord) {
-                contact_fail(c.status, kContactLost);
-                return;
-            }
-            ++k;
-        }
-        const ContactEntry* e = (k < tn && tab[k].code == code) ? &tab[k] : nullptr;
-        if (e) ++k;
+    for (uint32_t i = gt; i < count; i += stride) {
+        C.mark_a[i] = 0u;
         const ContactQuery& Q = C.query[i];
+        const unsigned long long code = C.cand[i];
         if (Q.ccd_state == SWB_CCD_INDETERMINATE) {
             contact_fail(c.status, kContactFinalCcd);
-            return;
+            continue;
         }
+        const uint32_t k = lower_bound_code([&](uint32_t m) { return tab[m].code; }, tn, code);
+        const ContactEntry* e = (k < tn && tab[k].code == code) ? &tab[k] : nullptr;
         const bool impact = Q.ccd_state != SWB_CCD_NO_IMPACT;
         if (!impact && !(e && (e->flags & kEntryRecord))) continue;
         if (!Q.certified) {
             contact_fail(c.status, impact ? kContactFinalGeometry : kContactCleared);
-            return;
+            continue;
         }
         D3 normal = d3_of(Q.normal);
         if (contact::dot(normal, impact ? d3_of(Q.ccd_normal) : d3_of(e->normal)) < 0.0) normal = -normal;
@@ -465,18 +672,14 @@ static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, 
         const double gap = contact::dot(fp - sp, normal) - C.separation;
         if (impact && (!contact::finite3(fp) || !contact::finite3(sp) || !contact::finite3(normal) || !isfinite(gap))) {
             contact_fail(c.status, kContactFinalNonFinite);
-            return;
+            continue;
         }
         const double pen = contact::dmax(0.0, -gap);
         if ((!impact && !isfinite(gap)) || pen > limit) {
             contact_fail(c.status, impact ? kContactPenetration : kContactClearedGate);
-            return;
+            continue;
         }
-        if (records >= C.record_cap) {
-            contact_fail(c.status, kContactRecords);
-            return;
-        }
-        ContactRecordDev& r = C.records[records++];
+        ContactRecordDev& r = C.cand_rec[i];
         r.code = code;
         for (int j = 0; j < 3; ++j) {
             r.fw[j] = Q.fw[j];
@@ -484,6 +687,7 @@ static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, 
         }
         for (int j = 0; j < 6; ++j) {
             r.addr[j] = Q.addr[j];
+            r.slot[j] = Q.slot[j];
             r.inv[j] = Q.inv[j];
         }
         r.fc = fc;
@@ -493,61 +697,69 @@ static __device__ __noinline__ void contact_certify_serial(const ContactCtx& c, 
         r.lambda = e ? e->lambda : 0.0;
         r.active = impact && r.lambda > 0.0 ? 1u : 0u;
         r.pad = 0;
-        active += r.active;
-        max_pen = contact::dmax(max_pen, pen);
+        C.mark_a[i] = 1u;
+        if (r.active) atomicAdd(&C.reduce[0], 1ull);
+        atomicMax(&C.reduce[1], static_cast<unsigned long long>(__double_as_longlong(pen)));  // pen >= 0
     }
-    for (; k < tn; ++k)
-        if (tab[k].flags & kEntryRecord) {
-            contact_fail(c.status, kContactLost);
-            return;
+    // every record of the solver must still be a supported feature
+    for (uint32_t k = gt; k < tn; k += stride) {
+        if (!(tab[k].flags & kEntryRecord)) continue;
+        const uint32_t i = lower_bound_code([&](uint32_t m) { return C.cand[m]; }, count, tab[k].code);
+        if (!(i < count && C.cand[i] == tab[k].code)) contact_fail(c.status, kContactLost);
+    }
+    cluster.sync();
+    if (c.me == 0) {
+        block_scan(C.mark_a, count, C.mark_a);
+        if (threadIdx.x == 0) {
+            diag->candidates = count;
+            diag->active = C.reduce[0];
+            diag->records = C.mark_a[count];
+            diag->max_penetration = __longlong_as_double(static_cast<long long>(C.reduce[1]));
         }
-    diag->candidates = count;
-    diag->active = active;
-    diag->records = records;
-    diag->max_penetration = max_pen;
+    }
+    cluster.sync();
+    for (uint32_t i = gt; i < count; i += stride)
+        if (C.mark_a[i + 1] != C.mark_a[i]) C.records[C.mark_a[i]] = C.cand_rec[i];
 }
 
-// Coulomb friction of the certified records on the finalized velocities,
-// in key order (contact.cpp:2081-2147).
-static __device__ __noinline__ void contact_friction_serial(const ContactCtx& c, const ContactDiagDev* diag) {
+// Coulomb friction of one certified record on the finalized velocities
+// (contact.cpp:2081-2147).
+static __device__ __noinline__ void friction_one(const ContactCtx& c, const ContactRecordDev& r) {
     const ContactDev& C = *c.C;
-    if (contact_failed(c.status)) return;
-    const double dt = c.dt;
-    const unsigned long long records = diag->records;
-    for (unsigned long long i = 0; i < records; ++i) {
-        if (i + kContactPrefetch < records) {
-            prefetch_l1(C.records + i + kContactPrefetch);
-            prefetch_l1(reinterpret_cast<const char*>(C.records + i + kContactPrefetch) + 128);
-        }
-        const ContactRecordDev& r = C.records[i];
-        const uint32_t fc = r.fc, sc = r.sc, n = fc + sc;
-        float4 V[6];
-        for (uint32_t j = 0; j < 6; ++j)
-            if (j < n) V[j] = ld_node(r.addr[j] + c.v_delta);
-        D3 vf{0.0, 0.0, 0.0}, vs{0.0, 0.0, 0.0};
-        for (uint32_t j = 0; j < 3; ++j) {
-            if (j < fc) vf = vf + r.fw[j] * D3{V[j].x, V[j].y, V[j].z};
-            if (j < sc) vs = vs + r.sw[j] * D3{V[fc + j].x, V[fc + j].y, V[fc + j].z};
-        }
-        const contact::Friction fr = contact::coulomb_friction(vf - vs, d3_of(r.normal), r.eff, r.lambda / dt,
-                                                               C.static_mu, C.dynamic_mu, r.active != 0);
-        if (!contact::finite3(fr.impulse) || !isfinite(fr.work) ||
-            fr.work > 1.0e-12 * contact::dmax(1.0, contact::norm2(fr.initial_tangent))) {
-            contact_fail(c.status, kContactFriction);
-            return;
-        }
-        if (fr.state == contact::kFrictionInactive) continue;  // no impulse
-        for (uint32_t j = 0; j < 6; ++j) {
-            if (j >= n) break;
-            const double w = j < fc ? r.fw[j] : -r.sw[j - fc];
-            const D3 dv = (w * fr.impulse) * static_cast<double>(r.inv[j]);
-            float4 W = V[j];
-            W.x = static_cast<float>(W.x + dv.x);
-            W.y = static_cast<float>(W.y + dv.y);
-            W.z = static_cast<float>(W.z + dv.z);
-            st_node(r.addr[j] + c.v_delta, W);
-        }
+    const uint32_t fc = r.fc, sc = r.sc;
+    float4 A[3], B[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (k < static_cast<int>(fc)) A[k] = ld_node(r.addr[k] + c.v_delta);
+        if (k < static_cast<int>(sc)) B[k] = ld_node(r.addr[fc + k] + c.v_delta);
     }
+    D3 vf{0.0, 0.0, 0.0}, vs{0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (k < static_cast<int>(fc)) vf = vf + r.fw[k] * D3{A[k].x, A[k].y, A[k].z};
+        if (k < static_cast<int>(sc)) vs = vs + r.sw[k] * D3{B[k].x, B[k].y, B[k].z};
+    }
+    const contact::Friction fr = contact::coulomb_friction(vf - vs, d3_of(r.normal), r.eff, r.lambda / c.dt,
+                                                           C.static_mu, C.dynamic_mu, r.active != 0);
+    if (!contact::finite3(fr.impulse) || !isfinite(fr.work) ||
+        fr.work > 1.0e-12 * contact::dmax(1.0, contact::norm2(fr.initial_tangent))) {
+        contact_fail(c.status, kContactFriction);
+        return;
+    }
+    if (fr.state == contact::kFrictionInactive) return;  // no impulse
+    auto kick = [&](float4& V, double w, float inv, uint32_t addr) {
+        const D3 dv = (w * fr.impulse) * static_cast<double>(inv);
+        V.x = static_cast<float>(V.x + dv.x);
+        V.y = static_cast<float>(V.y + dv.y);
+        V.z = static_cast<float>(V.z + dv.z);
+        st_node(addr + c.v_delta, V);
+    };
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (k < static_cast<int>(fc)) kick(A[k], r.fw[k], r.inv[k], r.addr[k]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (k < static_cast<int>(sc)) kick(B[k], -r.sw[k], r.inv[fc + k], r.addr[fc + k]);
 }
 
 // ---- the three contact steps of a substep ------------------------------------
@@ -571,21 +783,40 @@ __device__ __forceinline__ void contact_detect(const ContactCtx& c, cooperative_
 
 __device__ __forceinline__ void contact_iteration(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
     contact_detect(c, cluster);
-    if (c.me == 0 && threadIdx.x == 0) contact_project_serial(c);
+    contact_project(c, cluster);
     cluster.sync();
 }
 
 __device__ __forceinline__ void contact_certify(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
                                                 ContactDiagDev* diag) {
+    if (c.me == 0 && threadIdx.x == 0) {
+        c.C->reduce[0] = 0ull;
+        c.C->reduce[1] = 0ull;
+    }
     contact_detect(c, cluster);
-    if (c.me == 0 && threadIdx.x == 0) contact_certify_serial(c, diag);
+    contact_certify_all(c, cluster, diag);
     cluster.sync();
 }
 
 __device__ __forceinline__ void contact_friction(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
                                                  const ContactDiagDev* diag) {
+    const ContactDev& C = *c.C;
     cluster.sync();  // every CTA has finalized its velocities
-    if (c.me == 0 && threadIdx.x == 0) contact_friction_serial(c, diag);
+    const bool skip = contact_failed(c.status);
+    const uint32_t records = skip ? 0u : static_cast<uint32_t>(diag->records);
+    reset_levels(c, records, c.pbeg[c.ctas]);
+    cluster.sync();
+    if (c.me == 0) {
+        assign_levels(c, records, c.pbeg[c.ctas], [&](uint32_t i, uint32_t* s) -> uint32_t {
+            const ContactRecordDev& r = C.records[i];
+            const uint32_t n = r.fc + r.sc;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) s[j] = j < static_cast<int>(n) ? r.slot[j] : 0u;
+            return n;
+        });
+        scatter_levels(C, records);
+        run_levels(C, [&](uint32_t i) { friction_one(c, C.records[i]); });
+    }
     cluster.sync();
 }
 

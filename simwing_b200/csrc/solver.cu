@@ -178,6 +178,7 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
         raise(SWB_UNSUPPORTED, "more than 8 suspension segments or harness points");
     const std::vector<uint32_t> susp_nodes = suspension_endpoint_nodes(def);
     const size_t smem_limit = dynamic_smem_limit(prop);
+    smem_cap = smem_limit;
     cluster_mode = false;
     if (!(opt.flags & (SWB_OPT_GRID | SWB_OPT_GLOBAL_ONLY))) {
         if (opt.cluster_ctas < 0 || opt.cluster_ctas > kClusterMaxCtas)
@@ -378,6 +379,18 @@ void StructureImpl::setup_contact() {
     c.table_cap = cap;
     c.records = dalloc<ContactRecordDev>(owned, cap);
     c.record_cap = cap;
+    c.node_level = dalloc<uint32_t>(owned, def.nodes.size());
+    c.item_level = dalloc<uint32_t>(owned, cap);
+    c.level_start = dalloc<uint32_t>(owned, cap + 2);
+    c.level_fill = dalloc<uint32_t>(owned, cap + 2);
+    c.level_items = dalloc<uint32_t>(owned, cap);
+    c.level_meta = dalloc<uint32_t>(owned, 2);
+    c.hit = dalloc<uint32_t>(owned, cap);
+    c.mark_a = dalloc<uint32_t>(owned, cap + 1);
+    c.mark_b = dalloc<uint32_t>(owned, cap + 1);
+    c.cand_entry = dalloc<ContactEntry>(owned, cap);
+    c.cand_rec = dalloc<ContactRecordDev>(owned, cap);
+    c.reduce = dalloc<unsigned long long>(owned, 2);
     d_contact = dupload(owned, std::vector<ContactDev>{c}, stream);
     for (int b = 0; b < 3; ++b) {
         d_cdiag[b] = dalloc<ContactDiagDev>(owned, 1);
@@ -424,6 +437,13 @@ void StructureImpl::upload_cluster_tables() {
     }
     cp.smem_offsets = off;
     off = align16(off + (total_stages(csched) + 3) * 4u);
+    // contact: rank 0 keeps the node levels of its key-ordered passes in
+    // shared memory when they fit (else in global memory)
+    const uint32_t levels_bytes = align16(static_cast<uint32_t>(def.nodes.size()) * 4u);
+    if (def.has_contact && off + levels_bytes <= smem_cap) {
+        cp.smem_levels = off;
+        off += levels_bytes;
+    }
     cluster_smem = off;
     base.seam_offsets = dupload(owned, csched.seam_offsets, stream);
     base.seam_ab = dupload(owned, csched.seam_ab, stream);
