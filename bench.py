@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--no-contact", action="store_true")
     p.add_argument("--only-adjoint", action="store_true",
                    help="run the adjoint leg alone and print its record (profiling)")
+    p.add_argument("--only-contact", action="store_true",
+                   help="run the fabric self-contact leg alone and print its record (profiling)")
     p.add_argument("--adjoint-steps", type=int, default=240)
     p.add_argument("--adjoint-interval", type=int, default=16)
     return p.parse_args()
@@ -432,6 +434,13 @@ def main():
     torch.cuda.set_device(local)
     if args.warmup < 3:
         raise SystemExit("warmup must be >= 3")
+    if args.only_contact:
+        if rank == 0:
+            print(json.dumps({"contact": contact_leg(sw, args.steps, local, 1, False)}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
     if args.only_adjoint:
         if rank == 0:
             print(json.dumps({"adjoint": adjoint_leg(sw, settings(sw), local, args.adjoint_steps,
