@@ -872,6 +872,15 @@ swb_status swb_contact_sweep(uint32_t kind,
                              const swb_ccd_settings* settings,
                              swb_ccd_result* results);
 
+/* The candidate features of the last step's contact certification
+ * (contact.cpp:1583-1798: the final broadphase, in key order), for
+ * inspection; valid until the next step.  SWB_OUT_OF_RANGE (count written)
+ * when they exceed `capacity`; SWB_UNSUPPORTED without fabric self-contact. */
+swb_status swb_structure_contact_candidates(const swb_structure* structure,
+                                            swb_contact_key* keys,
+                                            uint64_t capacity,
+                                            uint64_t* count);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

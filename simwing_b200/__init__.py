@@ -637,6 +637,17 @@ class Structure:
                                          self.sweep_order(abi.SWEEP_MEMBRANE) if self._definition.view.membrane_count
                                          else None)
 
+    def contact_candidates(self) -> list:
+        """Candidate features of the last step's contact certification, in
+        key order (swb_structure_contact_candidates)."""
+        n = C.c_uint64()
+        status = self._lib.swb_structure_contact_candidates(self._h, None, 0, C.byref(n))
+        if status not in (abi.OK, abi.OUT_OF_RANGE):
+            _check(status)
+        keys = (abi.ContactKey * max(n.value, 1))()
+        _check(self._lib.swb_structure_contact_candidates(self._h, keys, n.value, C.byref(n)))
+        return list(keys)[: n.value]
+
     def schedule_report(self) -> abi.ScheduleReport:
         r = abi.ScheduleReport()
         _check(self._lib.swb_structure_schedule_report(self._h, C.byref(r)))

@@ -125,6 +125,18 @@ struct ContactDev {
     uint32_t* level_items;             // [cand_cap]
     uint32_t* level_meta;              // [0] levels
     uint32_t* hit;                     // [cand_cap] the candidates in contact, in key order
+    // binned broadphase: the triangles (for vertex rows) and the edges (for
+    // edge rows) bucketed by the low end of their boxes along `axis`
+    int axis;
+    uint32_t bins_cap;                 // bins per column set at most
+    uint32_t* tbin;                    // [bins_cap + 1] counts, then starts
+    uint32_t* tbin_fill;               // [bins_cap + 1]
+    uint32_t* tbin_items;              // [nt]
+    uint32_t* ebin;                    // [bins_cap + 1]
+    uint32_t* ebin_fill;               // [bins_cap + 1]
+    uint32_t* ebin_items;              // [ne]
+    unsigned long long* range;         // [6] order keys: triangle lo min, lo max, extent max; the same for edges
+    uint32_t* cand_tmp;                // [cand_cap] a row's hits before they are ordered
     uint32_t* mark_a;                  // [cand_cap + 1] per-candidate flags, then their exclusive scan
     uint32_t* mark_b;                  // [cand_cap + 1] per-table-entry flags, then their exclusive scan
     ContactEntry* cand_entry;          // [cand_cap] the candidate's table entry after the iteration

@@ -108,68 +108,231 @@ __device__ __forceinline__ FeatureSlots feature_slots(const ContactDev& C, unsig
     return q;
 }
 
+// Order key of a double, monotone for every non-NaN value, so that
+// unsigned 64-bit atomics take minima and maxima of doubles.
+__device__ __forceinline__ unsigned long long order_key(double d) {
+    const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(d));
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_order_key(unsigned long long k) {
+    const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double(static_cast<long long>(b));
+}
+
+// Warp-reduced atomic minimum / maximum of order keys (every lane calls,
+// `valid` marks the lanes that contribute).
+__device__ __forceinline__ void warp_atomic_range(unsigned long long* lo_min, unsigned long long* lo_max,
+                                                  unsigned long long* ext_max, bool valid, unsigned long long lo,
+                                                  unsigned long long ext) {
+    unsigned long long mn = valid ? lo : ~0ull, mx = valid ? lo : 0ull, ex = valid ? ext : 0ull;
+    for (int d = 16; d > 0; d >>= 1) {
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+        ex = max(ex, __shfl_xor_sync(0xffffffffu, ex, d));
+    }
+    const bool any = __any_sync(0xffffffffu, valid);  // every lane takes part
+    if ((threadIdx.x & 31) == 0 && any) {
+        atomicMin(lo_min, mn);
+        atomicMax(lo_max, mx);
+        atomicMax(ext_max, ex);
+    }
+}
+
+// Bins of one column set (triangles or edges) along the broadphase axis:
+// width at least the widest column box, so that the columns a row's box can
+// overlap lie in the bins from bin(lo - widest) to bin(hi).
+struct Bins {
+    double lo, width, widest;
+    uint32_t count;
+    __device__ uint32_t of(double x) const {
+        if (!(x > lo)) return 0u;
+        const double q = floor((x - lo) / width);
+        return q >= static_cast<double>(count - 1) ? count - 1 : static_cast<uint32_t>(q);
+    }
+};
+
+__device__ __forceinline__ Bins make_bins(const unsigned long long* range, uint32_t cap) {
+    Bins b;
+    b.lo = from_order_key(range[0]);
+    const double hi = from_order_key(range[1]);
+    b.widest = from_order_key(range[2]);
+    if (!isfinite(b.lo) || !isfinite(hi) || !isfinite(b.widest) || hi < b.lo) {
+        // no column contributed (an empty set): one bin
+        b.lo = 0.0;
+        b.width = 1.0;
+        b.widest = 0.0;
+        b.count = 1;
+        return b;
+    }
+    const double span = hi - b.lo;
+    b.width = fmax(b.widest, span / static_cast<double>(cap));
+    if (!(b.width > 0.0)) b.width = 1.0;
+    const double n = floor(span / b.width) + 1.0;
+    b.count = n >= static_cast<double>(cap) ? cap : static_cast<uint32_t>(n);
+    if (b.count == 0) b.count = 1;
+    return b;
+}
+
 // ---- parallel phases (every thread of the cluster; a barrier after each) ----
 
 __device__ __forceinline__ void contact_snapshot(const ContactCtx& c) {
-    for (uint32_t i = threadIdx.x; i < c.n; i += blockDim.x) c.C->snapshot[c.base + i] = c.x[i];
+    const ContactDev& C = *c.C;
+    for (uint32_t i = threadIdx.x; i < c.n; i += blockDim.x) C.snapshot[c.base + i] = c.x[i];
+    const uint32_t gt = c.me * blockDim.x + threadIdx.x, stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
+    for (uint32_t i = gt; i <= C.bins_cap; i += stride) {
+        C.tbin[i] = 0u;
+        C.tbin_fill[i] = 0u;
+        C.ebin[i] = 0u;
+        C.ebin_fill[i] = 0u;
+    }
+    if (gt < 6) C.range[gt] = (gt % 3 == 0) ? ~0ull : 0ull;
 }
 
 static __device__ __noinline__ void contact_boxes(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     const uint32_t total = C.nv + C.ne + C.nt;
     const uint32_t stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
-    for (uint32_t i = c.me * blockDim.x + threadIdx.x; i < total; i += stride) {
-        uint32_t s[3];
-        int count;
-        double* out;
-        if (i < C.nv) {
-            s[0] = C.vid[i];
-            count = 1;
-            out = C.vbox + 6 * static_cast<size_t>(i);
-        } else if (i < C.nv + C.ne) {
-            const uint2 e = C.eid[i - C.nv];
-            s[0] = e.x; s[1] = e.y;
-            count = 2;
-            out = C.ebox + 6 * static_cast<size_t>(i - C.nv);
-        } else {
-            const uint3 t = C.tid[i - C.nv - C.ne];
-            s[0] = t.x; s[1] = t.y; s[2] = t.z;
-            count = 3;
-            out = C.tbox + 6 * static_cast<size_t>(i - C.nv - C.ne);
+    const int a = C.axis;
+    // warp-uniform trip count: every lane takes part in the warp reductions
+    for (uint32_t base = c.me * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        bool tri = false, edge = false;
+        unsigned long long lo_key = 0, ext_key = 0;
+        if (i < total) {
+            uint32_t s[3];
+            int count;
+            double* out;
+            if (i < C.nv) {
+                s[0] = C.vid[i];
+                count = 1;
+                out = C.vbox + 6 * static_cast<size_t>(i);
+            } else if (i < C.nv + C.ne) {
+                const uint2 e = C.eid[i - C.nv];
+                s[0] = e.x; s[1] = e.y;
+                count = 2;
+                out = C.ebox + 6 * static_cast<size_t>(i - C.nv);
+                edge = true;
+            } else {
+                const uint3 t = C.tid[i - C.nv - C.ne];
+                s[0] = t.x; s[1] = t.y; s[2] = t.z;
+                count = 3;
+                out = C.tbox + 6 * static_cast<size_t>(i - C.nv - C.ne);
+                tri = true;
+            }
+            D3 prev[3], cur[3];
+            bool finite = true;
+            for (int k = 0; k < count; ++k) {
+                prev[k] = world_of(c, c.pos_in[s[k]]);
+                cur[k] = world_of(c, C.snapshot[s[k]]);
+                finite = finite && contact::finite3(prev[k]) && contact::finite3(cur[k]);
+            }
+            if (!finite) contact_fail(c.status, kContactInput);
+            const contact::Box b = contact::swept_box(prev, cur, count, C.separation);
+            for (int k = 0; k < 3; ++k) {
+                out[k] = b.lo[k];
+                out[3 + k] = b.hi[k];
+            }
+            lo_key = order_key(b.lo[a]);
+            ext_key = order_key(b.hi[a] - b.lo[a]);
+            if (!finite) tri = edge = false;
         }
-        D3 prev[3], cur[3];
-        bool finite = true;
-        for (int k = 0; k < count; ++k) {
-            prev[k] = world_of(c, c.pos_in[s[k]]);
-            cur[k] = world_of(c, C.snapshot[s[k]]);
-            finite = finite && contact::finite3(prev[k]) && contact::finite3(cur[k]);
-        }
-        if (!finite) contact_fail(c.status, kContactInput);
-        const contact::Box b = contact::swept_box(prev, cur, count, C.separation);
-        for (int k = 0; k < 3; ++k) {
-            out[k] = b.lo[k];
-            out[3 + k] = b.hi[k];
-        }
+        warp_atomic_range(C.range + 0, C.range + 1, C.range + 2, tri, lo_key, ext_key);
+        warp_atomic_range(C.range + 3, C.range + 4, C.range + 5, edge, lo_key, ext_key);
     }
 }
 
-// Count (write == false) or write the candidate rows, one warp per row.
-static __device__ __noinline__ void contact_rows(const ContactCtx& c, bool write) {
+// Bucket counts of the columns (every thread of the cluster).
+__device__ __noinline__ void contact_bin_counts(const ContactCtx& c) {
+    const ContactDev& C = *c.C;
+    const uint32_t gt = c.me * blockDim.x + threadIdx.x, stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
+    const int a = C.axis;
+    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 3, C.bins_cap);
+    for (uint32_t t = gt; t < C.nt; t += stride) atomicAdd(&C.tbin[bt.of(C.tbox[6 * static_cast<size_t>(t) + a])], 1u);
+    for (uint32_t e = gt; e < C.ne; e += stride) atomicAdd(&C.ebin[be.of(C.ebox[6 * static_cast<size_t>(e) + a])], 1u);
+}
+
+// Columns into their buckets (every thread of the cluster).
+__device__ __noinline__ void contact_bin_scatter(const ContactCtx& c) {
+    const ContactDev& C = *c.C;
+    const uint32_t gt = c.me * blockDim.x + threadIdx.x, stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
+    const int a = C.axis;
+    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 3, C.bins_cap);
+    for (uint32_t t = gt; t < C.nt; t += stride) {
+        const uint32_t b = bt.of(C.tbox[6 * static_cast<size_t>(t) + a]);
+        C.tbin_items[C.tbin[b] + atomicAdd(&C.tbin_fill[b], 1u)] = t;
+    }
+    for (uint32_t e = gt; e < C.ne; e += stride) {
+        const uint32_t b = be.of(C.ebox[6 * static_cast<size_t>(e) + a]);
+        C.ebin_items[C.ebin[b] + atomicAdd(&C.ebin_fill[b], 1u)] = e;
+    }
+}
+
+// Count (write == false) or write the candidate rows, one warp per row.  A
+// row tests only the columns of the bins its box can reach along the
+// broadphase axis: every column whose box can overlap the row's.  The
+// write pass collects the row's hits, then orders them by column (a rank
+// sort of the row's segment), so the list is the exhaustive one in key
+// order.
+__device__ __noinline__ void contact_rows(const ContactCtx& c, bool write) {
     const ContactDev& C = *c.C;
     const uint32_t rows = C.nv + C.ne;
     const uint32_t warps = (static_cast<uint32_t>(c.ctas) * blockDim.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    const int a = C.axis;
     const contact::Box* vb = reinterpret_cast<const contact::Box*>(C.vbox);
     const contact::Box* eb = reinterpret_cast<const contact::Box*>(C.ebox);
     const contact::Box* tb = reinterpret_cast<const contact::Box*>(C.tbox);
+    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 3, C.bins_cap);
     for (uint32_t row = (c.me * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
+        const bool vertex_row = row < C.nv;
+        const contact::Box b = vertex_row ? vb[row] : eb[row - C.nv];
+        const Bins& bins = vertex_row ? bt : be;
+        const uint32_t* bin_start = vertex_row ? C.tbin : C.ebin;
+        const uint32_t* items = vertex_row ? C.tbin_items : C.ebin_items;
+        // the window's lower end, widened by a relative margin against the
+        // rounding of the columns' extents (the overlap test decides)
+        const double reach = b.lo[a] - bins.widest - 1.0e-9 * (fabs(b.lo[a]) + bins.widest);
+        const uint32_t lo = bin_start[bins.of(reach)];
+        const uint32_t hi = bin_start[bins.of(b.hi[a]) + 1];
+        uint32_t v = 0;
+        uint2 e = make_uint2(0, 0);
+        if (vertex_row) v = C.vid[row];
+        else e = C.eid[row - C.nv];
+        const uint32_t i = row - C.nv;
         const unsigned long long base = write ? C.offsets[row] : 0ull;
-        const unsigned long long hi = static_cast<unsigned long long>(row) << 32;
-        const uint32_t hits =
-            contact::scan_candidate_row(row, C.nv, C.ne, C.nt, C.vid, C.eid, C.tid, vb, eb, tb,
-                                        [&](uint32_t col, uint32_t k) {
-                                            if (write) C.cand[base + k] = hi | col;
-                                        });
-        if (!write && (threadIdx.x & 31) == 0) C.counts[row] = hits;
+        uint32_t hits = 0;
+        for (uint32_t k0 = lo; k0 < hi; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            bool hit = false;
+            uint32_t col = 0;
+            if (k < hi) {
+                col = items[k];
+                if (vertex_row) {
+                    const uint3 t = C.tid[col];
+                    hit = t.x != v && t.y != v && t.z != v && contact::boxes_overlap(b, tb[col]);
+                } else {
+                    const uint2 f = C.eid[col];
+                    hit = col > i && e.x != f.x && e.x != f.y && e.y != f.x && e.y != f.y &&
+                          contact::boxes_overlap(b, eb[col]);
+                }
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, hit);
+            if (write && hit) C.cand_tmp[base + hits + __popc(mask & ((1u << lane) - 1u))] = col;
+            hits += __popc(mask);
+        }
+        if (!write) {
+            if (lane == 0) C.counts[row] = hits;
+            continue;
+        }
+        __syncwarp();
+        // rank sort of the row's hits (columns are distinct)
+        const unsigned long long code_hi = static_cast<unsigned long long>(row) << 32;
+        for (uint32_t p = lane; p < hits; p += 32) {
+            const uint32_t mine = C.cand_tmp[base + p];
+            uint32_t rank = 0;
+            for (uint32_t q = 0; q < hits; ++q) rank += C.cand_tmp[base + q] < mine ? 1u : 0u;
+            C.cand[base + rank] = code_hi | mine;
+        }
     }
 }
 
@@ -764,12 +927,24 @@ static __device__ __noinline__ void friction_one(const ContactCtx& c, const Cont
 
 // ---- the three contact steps of a substep ------------------------------------
 
+__device__ __forceinline__ uint32_t* C_bins_t(const ContactCtx& c) { return c.C->tbin; }
+__device__ __forceinline__ uint32_t* C_bins_e(const ContactCtx& c) { return c.C->ebin; }
+
 // Broadphase and queries of the current state (phases snapshot .. queries).
 __device__ __forceinline__ void contact_detect(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
     cluster.sync();  // every CTA's projections (local and remote) are done
     contact_snapshot(c);
     cluster.sync();
     contact_boxes(c);
+    cluster.sync();
+    if (!contact_failed(c.status)) contact_bin_counts(c);
+    cluster.sync();
+    if (c.me == 0 && !contact_failed(c.status)) {
+        block_scan(C_bins_t(c), make_bins(c.C->range, c.C->bins_cap).count, C_bins_t(c));
+        block_scan(C_bins_e(c), make_bins(c.C->range + 3, c.C->bins_cap).count, C_bins_e(c));
+    }
+    cluster.sync();
+    if (!contact_failed(c.status)) contact_bin_scatter(c);
     cluster.sync();
     if (!contact_failed(c.status)) contact_rows(c, false);
     cluster.sync();

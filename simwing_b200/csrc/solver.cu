@@ -386,12 +386,36 @@ void StructureImpl::setup_contact() {
     c.level_items = dalloc<uint32_t>(owned, cap);
     c.level_meta = dalloc<uint32_t>(owned, 2);
     c.hit = dalloc<uint32_t>(owned, cap);
+    // binned broadphase along the longest extent of the initial geometry
+    {
+        double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        for (size_t i = 0; i < def.nodes.size(); ++i) {
+            const double q[3] = {def.nodes[i].position.x, def.nodes[i].position.y, def.nodes[i].position.z};
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = i ? std::min(lo[k], q[k]) : q[k];
+                hi[k] = i ? std::max(hi[k], q[k]) : q[k];
+            }
+        }
+        c.axis = 0;
+        for (int k = 1; k < 3; ++k)
+            if (hi[k] - lo[k] > hi[c.axis] - lo[c.axis]) c.axis = k;
+    }
+    c.bins_cap = 1u << 16;
+    c.tbin = dalloc<uint32_t>(owned, c.bins_cap + 1);
+    c.tbin_fill = dalloc<uint32_t>(owned, c.bins_cap + 1);
+    c.tbin_items = dalloc<uint32_t>(owned, std::max<uint32_t>(c.nt, 1));
+    c.ebin = dalloc<uint32_t>(owned, c.bins_cap + 1);
+    c.ebin_fill = dalloc<uint32_t>(owned, c.bins_cap + 1);
+    c.ebin_items = dalloc<uint32_t>(owned, std::max<uint32_t>(c.ne, 1));
+    c.range = dalloc<unsigned long long>(owned, 6);
+    c.cand_tmp = dalloc<uint32_t>(owned, cap);
     c.mark_a = dalloc<uint32_t>(owned, cap + 1);
     c.mark_b = dalloc<uint32_t>(owned, cap + 1);
     c.cand_entry = dalloc<ContactEntry>(owned, cap);
     c.cand_rec = dalloc<ContactRecordDev>(owned, cap);
     c.reduce = dalloc<unsigned long long>(owned, 2);
     d_contact = dupload(owned, std::vector<ContactDev>{c}, stream);
+    contact_host = c;
     for (int b = 0; b < 3; ++b) {
         d_cdiag[b] = dalloc<ContactDiagDev>(owned, 1);
         cuda_check(cudaMemsetAsync(d_cdiag[b], 0, sizeof(ContactDiagDev), stream), "memset");
@@ -1420,6 +1444,43 @@ swb_status swb_structure_sweep_order(const swb_structure* s, uint32_t which, uin
                                                            : (which == SWB_SWEEP_DIHEDRAL ? m.sched.dihedral_order : none));
         if (count != v.size()) raise(SWB_INVALID_ARGUMENT, "order count mismatch");
         std::copy(v.begin(), v.end(), order);
+    });
+}
+
+swb_status swb_structure_contact_candidates(const swb_structure* s, swb_contact_key* keys, uint64_t capacity,
+                                            uint64_t* count) {
+    return guarded([&] {
+        if (!s || !count || (capacity && !keys)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        const StructureImpl& m = s->s;
+        if (!m.def.has_contact) raise(SWB_UNSUPPORTED, "the structure has no fabric self-contact");
+        cuda_check(cudaSetDevice(m.device), "cudaSetDevice");
+        ContactDiagDev cd{};
+        cuda_check(cudaMemcpyAsync(&cd, m.d_cdiag[m.cur], sizeof(cd), cudaMemcpyDeviceToHost, m.stream), "read");
+        cuda_check(cudaStreamSynchronize(m.stream), "read");
+        *count = cd.candidates;
+        if (cd.candidates > capacity) raise(SWB_OUT_OF_RANGE, "candidate capacity too small");
+        std::vector<unsigned long long> codes(cd.candidates);
+        if (!codes.empty())
+            cuda_check(cudaMemcpy(codes.data(), m.contact_host.cand, codes.size() * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost), "read");
+        const ContactSurface& S = m.contact_surface;
+        const size_t nv = S.vertices.size();
+        for (size_t k = 0; k < codes.size(); ++k) {
+            const uint64_t row = codes[k] >> 32, col = codes[k] & 0xffffffffull;
+            swb_contact_key& key = keys[k];
+            std::memset(&key, 0, sizeof key);
+            if (row < nv) {
+                key.kind = SWB_FEATURE_VERTEX_TRIANGLE;
+                key.first[0] = S.vertices[row];
+                key.second[0] = col;
+            } else {
+                key.kind = SWB_FEATURE_EDGE_EDGE;
+                key.first[0] = S.edges[row - nv][0];
+                key.first[1] = S.edges[row - nv][1];
+                key.second[0] = S.edges[col][0];
+                key.second[1] = S.edges[col][1];
+            }
+        }
     });
 }
 

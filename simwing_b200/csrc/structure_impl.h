@@ -88,6 +88,7 @@ struct StructureImpl {
     // the contact diagnostics per state buffer
     ContactSurface contact_surface;
     ContactDev* d_contact = nullptr;
+    ContactDev contact_host{};  // host copy of *d_contact (device pointers)
     size_t smem_cap = 0;  // dynamic shared memory a step kernel may request on this device
     ContactDiagDev* d_cdiag[3] = {nullptr, nullptr, nullptr};
     uint4* d_diag_mem = nullptr;      // membrane records for the diagnostics: corner slots, record index

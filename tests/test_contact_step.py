@@ -123,3 +123,25 @@ def test_contact_is_refused_where_it_is_not_built(cuda_device):
     s = sw.Structure(d)
     with pytest.raises(sw.Unsupported):
         sw.Rollout(s, 4)
+
+
+def key_tuple(k):
+    return (k.pair, k.kind, tuple(k.first), tuple(k.second))
+
+
+@pytest.mark.parametrize("make", [lambda: sw.stacked_sheets(n=16, compliance=1e-3),
+                                  lambda: sw.stacked_sheets(n=12, gap=0.001, half_thickness=0.003)])
+def test_binned_broadphase_equals_the_exhaustive_list(cuda_device, make):
+    """The step's broadphase bins the columns along one axis; its list (the
+    certification's, for the last step's start and end positions) must be
+    the exhaustive one (swb_contact_candidates), key for key."""
+    d = make()
+    dev = sw.Structure(d)
+    st = SLIDE
+    dev.step(st)
+    states = dev.node_states()
+    keys = dev.contact_candidates()
+    h = d.view.fabric_self_contact.contents.half_thickness
+    full, _, _ = sw.contact_candidates(d, h, states[:, 1, :], states[:, 0, :])
+    assert [key_tuple(k) for k in keys] == [key_tuple(k) for k in full]
+    assert len(keys) > 1000
