@@ -20,10 +20,10 @@
 // simwing_b200::DeviceStepError (a std::runtime_error) with the status.
 //
 // Differences a caller can observe: the state is FP32 on the device (the
-// boundary stays FP64); `workerThreads` is ignored; fabric self-contact
-// together with a rigid pilot, and fabric self-contact, load-path cable
-// sweeps or membranes on a mesh too large for one cluster, are rejected with
-// simwing_b200::Unsupported (a std::logic_error) at construction or step.
+// boundary stays FP64); `workerThreads` is ignored; fabric self-contact,
+// load-path cable sweeps or membranes on a mesh too large for one cluster
+// are rejected with simwing_b200::Unsupported (a std::logic_error) at
+// construction or step.
 #pragma once
 
 #include "simwing_b200.h"

@@ -297,12 +297,14 @@ def definition_from_arrays(nodes, triangles=(), constraints=(), dihedrals=(), su
 
 
 def stacked_sheets(n: int = 8, gap: float = 0.003, half_thickness: float = 0.002, friction=(0.4, 0.25),
-                   spacing: float = 0.05, compliance: float = 0.0, mass: float = 0.001) -> Definition:
+                   spacing: float = 0.05, compliance: float = 0.0, mass: float = 0.001,
+                   suspension=None) -> Definition:
     """Fabric self-contact scene: a free n x n sheet (distance constraints on
     its edges, compliance 1e-7) `gap` above a pinned n x n sheet, shifted by
     (13 mm, 7 mm) so that vertices, edges and faces of the two meet in every
     feature configuration; contact (half_thickness, compliance, static and
-    dynamic friction) over all triangles."""
+    dynamic friction) over all triangles.  `suspension` as for
+    definition_from_arrays (node indices: the pinned sheet first)."""
     nodes, tris, cons = [], [], []
     for layer, z in ((0, 0.0), (1, gap)):
         off = len(nodes)
@@ -328,7 +330,8 @@ def stacked_sheets(n: int = 8, gap: float = 0.003, half_thickness: float = 0.002
             for i in range(n - 1):
                 a = off + (n - 1) * n + i
                 cons.append((1, a, a + 1, spacing, 1e-7))
-    return definition_from_arrays(nodes, tris, cons, contact=(half_thickness, compliance, friction[0], friction[1]))
+    return definition_from_arrays(nodes, tris, cons, suspension=suspension,
+                                  contact=(half_thickness, compliance, friction[0], friction[1]))
 
 
 def generate_patch(**overrides) -> Definition:

@@ -663,11 +663,21 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             __syncthreads();
         }
     }
-    // ---- contact friction on the finalized velocities (soft_body.cpp:1453) ---
-    if constexpr (kContact) contact_friction(cctx, cluster, I.contact_diag);
+    // ---- the payload's velocity and line damping, contact friction on the
+    // finalized velocities, the payload's certification (soft_body.cpp:
+    // 1447-1457)
+    bool finish_ok = true;
+    if constexpr (kContact) {
+        if (owner && tid == 0) finish_ok = payload_reconstruct_damp(pdef, pay, *I.payload_in, x, v, p.dt, I.status);
+        contact_friction(cctx, cluster, I.contact_diag);
+    }
     if (owner && tid == 0) {
         if constexpr (kTape) tape_pilot(*p.tape.finish, pay, *p.tape.pilot, x, v);
-        payload_finish(pdef, pay, *I.payload_in, x, v, p.dt, I.status);
+        if constexpr (kContact) {
+            if (finish_ok) payload_certify_finish(pdef, pay, x, v, p.dt, I.status);
+        } else {
+            payload_finish(pdef, pay, *I.payload_in, x, v, p.dt, I.status);
+        }
         float3 s = make_float3(0.0f, 0.0f, 0.0f);
         if (I.recentre && finite3(pay.com) &&
             fmaxf(fabsf(pay.com.x), fmaxf(fabsf(pay.com.y), fabsf(pay.com.z))) > 0.25f)

@@ -145,11 +145,7 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     def.assign(definition);
     validate_definition(def.view);
     fingerprint = definition_fingerprint(def.view);
-    if (def.has_contact) {
-        if (def.has_suspension)
-            raise(SWB_UNSUPPORTED, "fabric self-contact together with a rigid pilot is not available in this build");
-        contact_surface = build_contact_surface(def.view, def.contact.half_thickness);
-    }
+    if (def.has_contact) contact_surface = build_contact_surface(def.view, def.contact.half_thickness);
     // Solver-drift momentum restoration of isolated free structures: no
     // suspension, no contact, bending or membranes present, no fixed node.
     momentum_guard = !def.has_suspension && !def.has_contact && (!def.dihedrals.empty() || !def.membranes.empty()) &&

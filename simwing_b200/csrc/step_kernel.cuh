@@ -343,12 +343,33 @@ __device__ __noinline__ void line_iteration(const DevPayloadDef& d, DevPayloadSt
 // half angle of the orientation increment is evaluated as
 // atan2(|xyz|, w), which equals the reference's acos(w) on unit
 // quaternions and keeps FP32 accuracy for small rotations.
-__device__ void payload_finish(const DevPayloadDef& d, DevPayloadState& s, const DevPayloadState& start,
-                               const float4* x, float4* v, float dt, int* status) {
+// A suspension endpoint's position and velocity: a node, or a harness point
+// of the payload.
+__device__ __forceinline__ bool payload_endpoint(const DevPayloadDef& d, const DevPayloadState& s, const float4* x,
+                                                 const float4* v, int node, int point, float3& pos, float3& vel) {
+    if (node >= 0) {
+        pos = f3(x[node]);
+        vel = f3(v[node]);
+        return true;
+    }
+    const float3 local = d.hang_local[point] - d.com_local;
+    M3 RR;
+    if (!q_rotation(s.q, RR)) return false;
+    const float3 offset = m3v(RR, local);
+    pos = s.com + offset;
+    vel = s.v + cross(s.w, offset);
+    return true;
+}
+
+// reconstructPayloadVelocity and applyLineDamping (suspension.cpp:2413-2479):
+// the first half of the payload's substep finish.  Returns false after a
+// failure (status set).
+__device__ bool payload_reconstruct_damp(const DevPayloadDef& d, DevPayloadState& s, const DevPayloadState& start,
+                                         const float4* x, float4* v, float dt, int* status) {
     s.v = (s.com - start.com) / dt;
     float4 delta;
     const float4 conj = make_float4(start.q.x, -start.q.y, -start.q.z, -start.q.w);
-    if (!q_canon(q_mul(s.q, conj), delta)) { susp_fail(status, kSuspOrientation); return; }
+    if (!q_canon(q_mul(s.q, conj), delta)) { susp_fail(status, kSuspOrientation); return false; }
     const float sn = sqrtf(delta.y * delta.y + delta.z * delta.z + delta.w * delta.w);
     const float half = atan2f(sn, delta.x);
     if (sn < 1.0e-12f) {
@@ -357,22 +378,11 @@ __device__ void payload_finish(const DevPayloadDef& d, DevPayloadState& s, const
         s.w = make_float3(delta.y, delta.z, delta.w) * (2.0f * half / (dt * sn));
     }
     M3 R, I, invI;
-    if (!q_rotation(s.q, R)) { susp_fail(status, kSuspOrientation); return; }
+    if (!q_rotation(s.q, R)) { susp_fail(status, kSuspOrientation); return false; }
     I = world_inertia(R, d.inertia);
-    if (!m3_inverse(I, invI)) { susp_fail(status, kSuspPayload); return; }
+    if (!m3_inverse(I, invI)) { susp_fail(status, kSuspPayload); return false; }
     auto endpoint = [&](int node, int point, float3& pos, float3& vel) -> bool {
-        if (node >= 0) {
-            pos = f3(x[node]);
-            vel = f3(v[node]);
-            return true;
-        }
-        const float3 local = d.hang_local[point] - d.com_local;
-        M3 RR;
-        if (!q_rotation(s.q, RR)) return false;
-        const float3 offset = m3v(RR, local);
-        pos = s.com + offset;
-        vel = s.v + cross(s.w, offset);
-        return true;
+        return payload_endpoint(d, s, x, v, node, point, pos, vel);
     };
     // applyLineDamping (suspension.cpp:2413-2479)
     for (int k = 0; k < d.segments; ++k) {
@@ -380,7 +390,7 @@ __device__ void payload_finish(const DevPayloadDef& d, DevPayloadState& s, const
         float3 from, to, vf, vt;
         if (!endpoint(d.from_node[k], d.from_point[k], from, vf) || !endpoint(d.to_node[k], d.to_point[k], to, vt)) {
             susp_fail(status, kSuspOrientation);
-            return;
+            return false;
         }
         const float3 df = to - from;
         const float m = length(df);
@@ -416,6 +426,16 @@ __device__ void payload_finish(const DevPayloadDef& d, DevPayloadState& s, const
             }
         }
     }
+    return true;
+}
+
+// certifySubstep and finishSubstep (suspension.cpp:2324-2359, 2481-2610):
+// the second half of the payload's substep finish.
+__device__ void payload_certify_finish(const DevPayloadDef& d, DevPayloadState& s, const float4* x, const float4* v,
+                                       float dt, int* status) {
+    auto endpoint = [&](int node, int point, float3& pos, float3& vel) -> bool {
+        return payload_endpoint(d, s, x, v, node, point, pos, vel);
+    };
     // certifySubstep (suspension.cpp:2324-2359); the unit-norm gate uses an
     // FP32 tolerance.
     const float qn = s.q.x * s.q.x + s.q.y * s.q.y + s.q.z * s.q.z + s.q.w * s.q.w;
@@ -449,6 +469,14 @@ __device__ void payload_finish(const DevPayloadDef& d, DevPayloadState& s, const
     }
     s.max_residual = maxres;
     if (maxres > d.max_residual) susp_fail(status, kSuspResidual);
+}
+
+
+// The payload's substep finish: velocity reconstruction, line damping,
+// certification and the line wrench.
+__device__ void payload_finish(const DevPayloadDef& d, DevPayloadState& s, const DevPayloadState& start,
+                               const float4* x, float4* v, float dt, int* status) {
+    if (payload_reconstruct_damp(d, s, start, x, v, dt, status)) payload_certify_finish(d, s, x, v, dt, status);
 }
 
 // ---- the kernel -------------------------------------------------------------

@@ -123,6 +123,9 @@ def test_contact_is_refused_where_it_is_not_built(cuda_device):
     s = sw.Structure(d)
     with pytest.raises(sw.Unsupported):
         sw.Rollout(s, 4)
+    with pytest.raises(sw.Unsupported):
+        sw.contact_sweep(sw.abi.FEATURE_SEGMENT_TRIANGLE, np.zeros((1, 9)), np.zeros((1, 9)), np.zeros((1, 9)),
+                         np.zeros((1, 9)), 0.0)
 
 
 def key_tuple(k):
@@ -145,3 +148,51 @@ def test_binned_broadphase_equals_the_exhaustive_list(cuda_device, make):
     full, _, _ = sw.contact_candidates(d, h, states[:, 1, :], states[:, 0, :])
     assert [key_tuple(k) for k in keys] == [key_tuple(k) for k in full]
     assert len(keys) > 1000
+
+
+def pilot_sheets():
+    """The compliant stacked sheets with a light rigid pilot hanging from
+    two nodes of the free sheet by two risers (the payload's line damping
+    precedes contact friction, friction precedes the payload's
+    certification: soft_body.cpp:1447-1457)."""
+    n, spacing = 8, 0.05
+    a, b = n * n + 2 * n + 2, n * n + 5 * n + 5
+    pa = np.array([2 * spacing + 0.013, 2 * spacing + 0.007, 0.003])
+    pb = np.array([5 * spacing + 0.013, 5 * spacing + 0.007, 0.003])
+    com = np.array([0.5 * (pa[0] + pb[0]), 0.5 * (pa[1] + pb[1]), -0.6])
+    ha, hb = np.array([-0.05, 0.0, 0.2]), np.array([0.05, 0.0, 0.2])
+    ra, rb = float(np.linalg.norm(pa - (com + ha))), float(np.linalg.norm(pb - (com + hb)))
+    susp = dict(pilot_mass=0.05, pilot_com_world=tuple(com), pilot_inertia=(0.002, 0.002, 0.001),
+                attachments=[(1, a), (2, b)], harness=[(1, tuple(ha)), (2, tuple(hb))],
+                segments=[(1, (1, 1), (3, 1), ra, 1e3, 0.5), (2, (1, 2), (3, 2), rb, 1e3, 0.5)],
+                solver_iterations=8, maximum_line_residual=1e-2)
+    return sw.stacked_sheets(n=n, compliance=1e-3, suspension=susp)
+
+
+@pytest.mark.parametrize("ctas", [1, 4])
+def test_contact_with_a_pilot_matches_the_reference(cuda_device, ctas):
+    d = pilot_sheets()
+    dev = sw.Structure(d, sw.SolverOptions(cluster_ctas=ctas))
+    ref = O.RefStructure(dev.oracle_definition())
+    da = dev.step(SLIDE)
+    db = ref.step(SLIDE)
+    a, b = dev.node_states(), ref.node_states()
+    assert float(np.abs(a[:, 0, :] - b[:, 0, :]).max()) <= REL_TOL
+    assert float(np.abs(a[:, 2, :] - b[:, 2, :]).max()) <= REL_TOL / SLIDE.time_step
+    assert da.active_contact_count == db.active_contact_count > 0
+    assert abs(da.maximum_contact_penetration - db.maximum_contact_penetration) <= REL_TOL
+    pd, pr = dev.suspension_state(), ref.payload()[0]
+    np.testing.assert_allclose(pd.center_of_mass, [pr.center_of_mass.x, pr.center_of_mass.y, pr.center_of_mass.z],
+                               atol=REL_TOL)
+    np.testing.assert_allclose(pd.linear_velocity,
+                               [pr.linear_velocity.x, pr.linear_velocity.y, pr.linear_velocity.z],
+                               atol=REL_TOL / SLIDE.time_step)
+    assert abs(da.maximum_suspension_residual - db.maximum_suspension_residual) <= REL_TOL
+    # the resting contact the pilot presses: the reference's swept query gives up
+    before = dev.node_states().copy()
+    with pytest.raises(O.OracleError) as err:
+        ref.step(SLIDE)
+    assert err.value.status == sw.abi.CONTACT_ERROR
+    with pytest.raises(sw.ContactStepError):
+        dev.step(SLIDE)
+    np.testing.assert_array_equal(dev.node_states(), before)
