@@ -872,6 +872,43 @@ swb_status swb_contact_sweep(uint32_t kind,
                              const swb_ccd_settings* settings,
                              swb_ccd_result* results);
 
+/* ------------------------------------------------------------------------ */
+/* Coupling callers with device-resident loads: the structural side of      */
+/* simwing::fsi::ConservativeMacroStepCoupling::advanceStructure and        */
+/* advanceStructureWithEndpointLoads (src/fsi/coupling.cpp:806-911).  A     */
+/* coupling binds interface node i to structure node structure_nodes[i];    */
+/* several interface nodes may load one structure node.                     */
+/* ------------------------------------------------------------------------ */
+typedef struct swb_coupling swb_coupling;
+
+/* SWB_OUT_OF_RANGE when a binding names an unknown structure node. */
+swb_status swb_coupling_create(swb_structure* structure,
+                               const uint64_t* structure_nodes,
+                               uint64_t bindings,
+                               swb_coupling** out);
+void swb_coupling_destroy(swb_coupling* coupling);
+
+/* One structure step on the time-integrated interface impulses `impulses`
+ * (DEVICE memory, bindings x 3 doubles, N s) over `duration` seconds, which
+ * must equal settings->time_step: each binding adds impulse / duration to
+ * its structure node, in binding order, on top of the loads already
+ * pending.  Non-finite loads: SWB_INVALID_ARGUMENT before stepping; a failed
+ * step leaves the pending loads as they were (the reference restores its
+ * pre-call checkpoint). */
+swb_status swb_coupling_advance_impulses(swb_coupling* coupling,
+                                         const double* impulses,
+                                         double duration,
+                                         const swb_step_settings* settings,
+                                         swb_diagnostics* out);
+
+/* The same with endpoint tractions (DEVICE memory, bindings x 3 doubles
+ * each, N): each binding adds the mean of its start and end load. */
+swb_status swb_coupling_advance_endpoint_loads(swb_coupling* coupling,
+                                               const double* start_loads,
+                                               const double* end_loads,
+                                               const swb_step_settings* settings,
+                                               swb_diagnostics* out);
+
 /* The candidate features of the last step's contact certification
  * (contact.cpp:1583-1798: the final broadphase, in key order), for
  * inspection; valid until the next step.  SWB_OUT_OF_RANGE (count written)

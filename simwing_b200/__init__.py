@@ -660,6 +660,45 @@ class Structure:
         return float(self._lib.swb_structure_last_step_ms(self._h))
 
 
+class Coupling:
+    """The structural side of ConservativeMacroStepCoupling
+    (src/fsi/coupling.cpp:806-911) with device-resident loads: interface node
+    i loads structure node structure_nodes[i].  The load arrays are device
+    addresses (integers) or CUDA tensors of bindings x 3 doubles."""
+
+    def __init__(self, structure: "Structure", structure_nodes):
+        self._lib = abi.library()
+        self._structure = structure  # keep alive
+        nodes = np.ascontiguousarray(structure_nodes, dtype=np.uint64)
+        h = C.c_void_p()
+        _check(self._lib.swb_coupling_create(structure.handle, nodes.ctypes.data, nodes.size, C.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def _ptr(a):
+        return a.data_ptr() if hasattr(a, "data_ptr") else int(a)
+
+    def advance_impulses(self, impulses, duration: float, settings: abi.StepSettings) -> abi.Diagnostics:
+        d = abi.Diagnostics()
+        _check(self._lib.swb_coupling_advance_impulses(self._h, self._ptr(impulses), duration, C.byref(settings),
+                                                       C.byref(d)))
+        return d
+
+    def advance_endpoint_loads(self, start_loads, end_loads, settings: abi.StepSettings) -> abi.Diagnostics:
+        d = abi.Diagnostics()
+        _check(self._lib.swb_coupling_advance_endpoint_loads(self._h, self._ptr(start_loads), self._ptr(end_loads),
+                                                             C.byref(settings), C.byref(d)))
+        return d
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.swb_coupling_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+
 def BatchOptions(**overrides) -> abi.BatchOptions:
     o = abi.BatchOptions()
     abi.library().swb_default_batch_options(C.byref(o))

@@ -296,6 +296,11 @@ _PROTOTYPES = {
     "swb_default_ccd_settings": (None, [P(CcdSettings)]),
     "swb_definition_set_contact": (C.c_int, [C.c_void_p, P(FabricContactDef)]),
     "swb_structure_contact_candidates": (C.c_int, [C.c_void_p, P(ContactKey), C.c_uint64, P(C.c_uint64)]),
+    "swb_coupling_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, P(C.c_void_p)]),
+    "swb_coupling_destroy": (None, [C.c_void_p]),
+    "swb_coupling_advance_impulses": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, P(StepSettings), P(Diagnostics)]),
+    "swb_coupling_advance_endpoint_loads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, P(StepSettings),
+                                                      P(Diagnostics)]),
     "swb_contact_candidates": (C.c_int, [P(StructureDefinition), C.c_double, C.c_void_p, C.c_void_p, P(ContactKey),
                                          C.c_uint64, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
     "swb_contact_closest": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_double, P(ClosestResult)]),

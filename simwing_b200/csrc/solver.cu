@@ -1033,7 +1033,7 @@ swb_status StructureImpl::step(const swb_step_settings& st, int steps, swb_diagn
     if (steps < 1) raise(SWB_INVALID_ARGUMENT, "steps must be positive");
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
     if (pressure_dirty) upload_pressure();
-    if (forces_dirty) upload_forces();
+    if (forces_dirty && !device_forces) upload_forces();
     const int start = cur;
     const int total = steps * st.substeps;
     // Transaction: substeps ping-pong between buffers `start` and `other`;

@@ -117,6 +117,9 @@ struct StructureImpl {
     void build(const swb_structure_definition& definition, const swb_solver_options* options);
     void upload_cluster_tables();
     void setup_contact();
+    // The step with the force buffer already written on the device (the
+    // coupling's impulse gather): skips the upload of the pending loads.
+    bool device_forces = false;
     // the cluster step kernel for this structure (the membrane
     // instantiation when it has membrane elements)
     void (*step_kernel() const)(ClusterParams);
