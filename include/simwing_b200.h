@@ -909,6 +909,45 @@ swb_status swb_coupling_advance_endpoint_loads(swb_coupling* coupling,
                                                const swb_step_settings* settings,
                                                swb_diagnostics* out);
 
+/* ------------------------------------------------------------------------ */
+/* Closed cell (bay) volumes, the geometric input of the canopy's cell-air   */
+/* pressure model: softwing::estimateClosedCellVolume (cell_volume.h:38-44, */
+/* cell_volume.cpp:161-306) for many cells at once, on the device in FP64.  */
+/* ------------------------------------------------------------------------ */
+
+/* One cell: skin faces face_indices[face_begin, +face_count) and the two rib
+ * loops (ordered closed polygons, first node not repeated)
+ * loop_nodes[low_begin, +low_count) and loop_nodes[high_begin, +high_count). */
+typedef struct swb_cell_def {
+    uint64_t face_begin, face_count;
+    uint64_t low_begin, low_count;
+    uint64_t high_begin, high_count;
+} swb_cell_def;
+
+/* ClosedCellVolumeEstimate (cell_volume.h:14-32) */
+typedef struct swb_cell_volume {
+    double signed_volume;
+    double volume;
+    uint64_t skin_boundary_edges;
+    uint64_t cap_boundary_edges_matched;
+    uint64_t non_manifold_skin_edges;
+    uint64_t degenerate_skin_faces;
+    uint32_t valid;
+    uint32_t watertight_after_capping;
+    uint32_t used_geometric_orientation_fallback;
+    uint32_t ambiguous_skin_orientation;
+} swb_cell_volume;
+
+/* Volumes of `cell_count` cells of the definition's triangles at `positions`
+ * (node_count x 3 doubles, host); bit for bit the reference's estimates. */
+swb_status swb_cell_volumes(const swb_structure_definition* definition,
+                            const uint64_t* face_indices,
+                            const uint64_t* loop_nodes,
+                            const swb_cell_def* cells,
+                            uint64_t cell_count,
+                            const double* positions,
+                            swb_cell_volume* out);
+
 /* The candidate features of the last step's contact certification
  * (contact.cpp:1583-1798: the final broadphase, in key order), for
  * inspection; valid until the next step.  SWB_OUT_OF_RANGE (count written)

@@ -19,6 +19,7 @@
 #include <softwing/parallel.h>
 #include <softwing/soft_body.h>
 #include <softwing/suspension.h>
+#include <softwing/cell_volume.h>
 
 #include <chrono>
 #include <cmath>
@@ -636,6 +637,53 @@ swb_status swref_contact_sweep(uint32_t kind, uint64_t count,
             o.bracket_lower = r.bracketLower;
             o.bracket_upper = r.bracketUpper;
             store_closest(o.geometry, r.geometry);
+        }
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+// softwing::estimateClosedCellVolume (cell_volume.h:38-44) per cell, on the
+// definition's triangles at `positions`.
+swb_status swref_cell_volumes(const swb_structure_definition* d,
+                              const uint64_t* face_indices,
+                              const uint64_t* loop_nodes,
+                              const swb_cell_def* cells,
+                              uint64_t cell_count,
+                              const double* positions,
+                              swb_cell_volume* out) {
+    try {
+        std::vector<softwing::Node> nodes(d->node_count);
+        for (uint64_t i = 0; i < d->node_count; ++i)
+            nodes[i].position = {positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]};
+        std::vector<softwing::Triangle> triangles(d->triangle_count);
+        for (uint64_t t = 0; t < d->triangle_count; ++t) {
+            triangles[t].a = d->triangles[t].nodes[0];
+            triangles[t].b = d->triangles[t].nodes[1];
+            triangles[t].c = d->triangles[t].nodes[2];
+        }
+        for (uint64_t k = 0; k < cell_count; ++k) {
+            const swb_cell_def& c = cells[k];
+            const std::vector<std::size_t> faces(face_indices + c.face_begin,
+                                                 face_indices + c.face_begin + c.face_count);
+            const std::vector<std::size_t> low(loop_nodes + c.low_begin, loop_nodes + c.low_begin + c.low_count);
+            const std::vector<std::size_t> high(loop_nodes + c.high_begin,
+                                                loop_nodes + c.high_begin + c.high_count);
+            const softwing::ClosedCellVolumeEstimate e =
+                softwing::estimateClosedCellVolume(nodes, triangles, faces, low, high);
+            swb_cell_volume& o = out[k];
+            std::memset(&o, 0, sizeof o);
+            o.signed_volume = e.signedVolume;
+            o.volume = e.volume;
+            o.skin_boundary_edges = e.skinBoundaryEdges;
+            o.cap_boundary_edges_matched = e.capBoundaryEdgesMatched;
+            o.non_manifold_skin_edges = e.nonManifoldSkinEdges;
+            o.degenerate_skin_faces = e.degenerateSkinFaces;
+            o.valid = e.valid;
+            o.watertight_after_capping = e.watertightAfterCapping;
+            o.used_geometric_orientation_fallback = e.usedGeometricOrientationFallback;
+            o.ambiguous_skin_orientation = e.ambiguousSkinOrientation;
         }
         return SWB_OK;
     } catch (...) {
