@@ -127,15 +127,16 @@ struct ContactDev {
     uint32_t* hit;                     // [cand_cap] the candidates in contact, in key order
     // binned broadphase: the triangles (for vertex rows) and the edges (for
     // edge rows) bucketed by the low end of their boxes along `axis`
-    int axis;
-    uint32_t bins_cap;                 // bins per column set at most
+    int axis, axis2;                   // the grid's axes: the longest and second-longest extents
+    uint32_t bins_cap;                 // grid cells per column set at most
     uint32_t* tbin;                    // [bins_cap + 1] counts, then starts
     uint32_t* tbin_fill;               // [bins_cap + 1]
     uint32_t* tbin_items;              // [nt]
     uint32_t* ebin;                    // [bins_cap + 1]
     uint32_t* ebin_fill;               // [bins_cap + 1]
     uint32_t* ebin_items;              // [ne]
-    unsigned long long* range;         // [6] order keys: triangle lo min, lo max, extent max; the same for edges
+    unsigned long long* range;         // [12] order keys per column set (triangles, then edges): on each
+                                       // axis the low ends' minimum and maximum and the largest extent
     uint32_t* cand_tmp;                // [cand_cap] a row's hits before they are ordered
     uint32_t* mark_a;                  // [cand_cap + 1] per-candidate flags, then their exclusive scan
     uint32_t* mark_b;                  // [cand_cap + 1] per-table-entry flags, then their exclusive scan

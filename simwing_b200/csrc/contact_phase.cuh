@@ -138,10 +138,10 @@ __device__ __forceinline__ void warp_atomic_range(unsigned long long* lo_min, un
     }
 }
 
-// Bins of one column set (triangles or edges) along the broadphase axis:
-// width at least the widest column box, so that the columns a row's box can
-// overlap lie in the bins from bin(lo - widest) to bin(hi).
-struct Bins {
+// One axis of a column set's grid: cell width at least the widest column
+// box on that axis, so that the columns a row's box can overlap have their
+// low ends in the cells from of(lo - widest) to of(hi).
+struct Axis {
     double lo, width, widest;
     uint32_t count;
     __device__ uint32_t of(double x) const {
@@ -151,13 +151,13 @@ struct Bins {
     }
 };
 
-__device__ __forceinline__ Bins make_bins(const unsigned long long* range, uint32_t cap) {
-    Bins b;
+__device__ __forceinline__ Axis make_axis(const unsigned long long* range, uint32_t cap) {
+    Axis b;
     b.lo = from_order_key(range[0]);
     const double hi = from_order_key(range[1]);
     b.widest = from_order_key(range[2]);
     if (!isfinite(b.lo) || !isfinite(hi) || !isfinite(b.widest) || hi < b.lo) {
-        // no column contributed (an empty set): one bin
+        // no column contributed (an empty set): one cell
         b.lo = 0.0;
         b.width = 1.0;
         b.widest = 0.0;
@@ -173,6 +173,24 @@ __device__ __forceinline__ Bins make_bins(const unsigned long long* range, uint3
     return b;
 }
 
+// A column set's grid on the two broadphase axes; cells numbered a-major,
+// so the cells of one a-index form a contiguous run of bucketed columns.
+struct Bins {
+    Axis a, b;
+    __device__ uint32_t count() const { return a.count * b.count; }
+    __device__ uint32_t of(double xa, double xb) const { return a.of(xa) * b.count + b.of(xb); }
+};
+
+// range: the set's six keys (axis a: lo min, lo max, widest; axis b: the same)
+__device__ __forceinline__ Bins make_bins(const unsigned long long* range, uint32_t cap) {
+    uint32_t side = 1;
+    while ((side + 1) * (side + 1) <= cap) ++side;
+    Bins g;
+    g.a = make_axis(range, side);
+    g.b = make_axis(range + 3, side);
+    return g;
+}
+
 // ---- parallel phases (every thread of the cluster; a barrier after each) ----
 
 __device__ __forceinline__ void contact_snapshot(const ContactCtx& c) {
@@ -185,19 +203,19 @@ __device__ __forceinline__ void contact_snapshot(const ContactCtx& c) {
         C.ebin[i] = 0u;
         C.ebin_fill[i] = 0u;
     }
-    if (gt < 6) C.range[gt] = (gt % 3 == 0) ? ~0ull : 0ull;
+    if (gt < 12) C.range[gt] = (gt % 3 == 0) ? ~0ull : 0ull;
 }
 
 static __device__ __noinline__ void contact_boxes(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     const uint32_t total = C.nv + C.ne + C.nt;
     const uint32_t stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
-    const int a = C.axis;
+    const int a = C.axis, a2 = C.axis2;
     // warp-uniform trip count: every lane takes part in the warp reductions
     for (uint32_t base = c.me * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
         const uint32_t i = base + (threadIdx.x & 31);
         bool tri = false, edge = false;
-        unsigned long long lo_key = 0, ext_key = 0;
+        unsigned long long lo_key = 0, ext_key = 0, lo_key2 = 0, ext_key2 = 0;
         if (i < total) {
             uint32_t s[3];
             int count;
@@ -234,42 +252,55 @@ static __device__ __noinline__ void contact_boxes(const ContactCtx& c) {
             }
             lo_key = order_key(b.lo[a]);
             ext_key = order_key(b.hi[a] - b.lo[a]);
+            lo_key2 = order_key(b.lo[a2]);
+            ext_key2 = order_key(b.hi[a2] - b.lo[a2]);
             if (!finite) tri = edge = false;
         }
         warp_atomic_range(C.range + 0, C.range + 1, C.range + 2, tri, lo_key, ext_key);
-        warp_atomic_range(C.range + 3, C.range + 4, C.range + 5, edge, lo_key, ext_key);
+        warp_atomic_range(C.range + 3, C.range + 4, C.range + 5, tri, lo_key2, ext_key2);
+        warp_atomic_range(C.range + 6, C.range + 7, C.range + 8, edge, lo_key, ext_key);
+        warp_atomic_range(C.range + 9, C.range + 10, C.range + 11, edge, lo_key2, ext_key2);
     }
 }
 
-// Bucket counts of the columns (every thread of the cluster).
+// Bucket counts of the columns by the grid cell of their box's low corner
+// (every thread of the cluster).
 __device__ __noinline__ void contact_bin_counts(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     const uint32_t gt = c.me * blockDim.x + threadIdx.x, stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
-    const int a = C.axis;
-    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 3, C.bins_cap);
-    for (uint32_t t = gt; t < C.nt; t += stride) atomicAdd(&C.tbin[bt.of(C.tbox[6 * static_cast<size_t>(t) + a])], 1u);
-    for (uint32_t e = gt; e < C.ne; e += stride) atomicAdd(&C.ebin[be.of(C.ebox[6 * static_cast<size_t>(e) + a])], 1u);
+    const int a = C.axis, a2 = C.axis2;
+    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 6, C.bins_cap);
+    for (uint32_t t = gt; t < C.nt; t += stride) {
+        const double* q = C.tbox + 6 * static_cast<size_t>(t);
+        atomicAdd(&C.tbin[bt.of(q[a], q[a2])], 1u);
+    }
+    for (uint32_t e = gt; e < C.ne; e += stride) {
+        const double* q = C.ebox + 6 * static_cast<size_t>(e);
+        atomicAdd(&C.ebin[be.of(q[a], q[a2])], 1u);
+    }
 }
 
 // Columns into their buckets (every thread of the cluster).
 __device__ __noinline__ void contact_bin_scatter(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     const uint32_t gt = c.me * blockDim.x + threadIdx.x, stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
-    const int a = C.axis;
-    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 3, C.bins_cap);
+    const int a = C.axis, a2 = C.axis2;
+    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 6, C.bins_cap);
     for (uint32_t t = gt; t < C.nt; t += stride) {
-        const uint32_t b = bt.of(C.tbox[6 * static_cast<size_t>(t) + a]);
+        const double* q = C.tbox + 6 * static_cast<size_t>(t);
+        const uint32_t b = bt.of(q[a], q[a2]);
         C.tbin_items[C.tbin[b] + atomicAdd(&C.tbin_fill[b], 1u)] = t;
     }
     for (uint32_t e = gt; e < C.ne; e += stride) {
-        const uint32_t b = be.of(C.ebox[6 * static_cast<size_t>(e) + a]);
+        const double* q = C.ebox + 6 * static_cast<size_t>(e);
+        const uint32_t b = be.of(q[a], q[a2]);
         C.ebin_items[C.ebin[b] + atomicAdd(&C.ebin_fill[b], 1u)] = e;
     }
 }
 
 // Count (write == false) or write the candidate rows, one warp per row.  A
-// row tests only the columns of the bins its box can reach along the
-// broadphase axis: every column whose box can overlap the row's.  The
+// row tests only the columns of the grid cells its box can reach on the two
+// broadphase axes: every column whose box can overlap the row's.  The
 // write pass collects the row's hits, then orders them by column (a rank
 // sort of the row's segment), so the list is the exhaustive one in key
 // order.
@@ -282,18 +313,20 @@ __device__ __noinline__ void contact_rows(const ContactCtx& c, bool write) {
     const contact::Box* vb = reinterpret_cast<const contact::Box*>(C.vbox);
     const contact::Box* eb = reinterpret_cast<const contact::Box*>(C.ebox);
     const contact::Box* tb = reinterpret_cast<const contact::Box*>(C.tbox);
-    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 3, C.bins_cap);
+    const int a2 = C.axis2;
+    const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 6, C.bins_cap);
     for (uint32_t row = (c.me * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
         const bool vertex_row = row < C.nv;
         const contact::Box b = vertex_row ? vb[row] : eb[row - C.nv];
-        const Bins& bins = vertex_row ? bt : be;
-        const uint32_t* bin_start = vertex_row ? C.tbin : C.ebin;
+        const Bins& g = vertex_row ? bt : be;
+        const uint32_t* cell_start = vertex_row ? C.tbin : C.ebin;
         const uint32_t* items = vertex_row ? C.tbin_items : C.ebin_items;
-        // the window's lower end, widened by a relative margin against the
+        // the window's low ends, widened by a relative margin against the
         // rounding of the columns' extents (the overlap test decides)
-        const double reach = b.lo[a] - bins.widest - 1.0e-9 * (fabs(b.lo[a]) + bins.widest);
-        const uint32_t lo = bin_start[bins.of(reach)];
-        const uint32_t hi = bin_start[bins.of(b.hi[a]) + 1];
+        const double reach_a = b.lo[a] - g.a.widest - 1.0e-9 * (fabs(b.lo[a]) + g.a.widest);
+        const double reach_b = b.lo[a2] - g.b.widest - 1.0e-9 * (fabs(b.lo[a2]) + g.b.widest);
+        const uint32_t ia0 = g.a.of(reach_a), ia1 = g.a.of(b.hi[a]);
+        const uint32_t ib0 = g.b.of(reach_b), ib1 = g.b.of(b.hi[a2]);
         uint32_t v = 0;
         uint2 e = make_uint2(0, 0);
         if (vertex_row) v = C.vid[row];
@@ -301,24 +334,28 @@ __device__ __noinline__ void contact_rows(const ContactCtx& c, bool write) {
         const uint32_t i = row - C.nv;
         const unsigned long long base = write ? C.offsets[row] : 0ull;
         uint32_t hits = 0;
-        for (uint32_t k0 = lo; k0 < hi; k0 += 32) {
-            const uint32_t k = k0 + lane;
-            bool hit = false;
-            uint32_t col = 0;
-            if (k < hi) {
-                col = items[k];
-                if (vertex_row) {
-                    const uint3 t = C.tid[col];
-                    hit = t.x != v && t.y != v && t.z != v && contact::boxes_overlap(b, tb[col]);
-                } else {
-                    const uint2 f = C.eid[col];
-                    hit = col > i && e.x != f.x && e.x != f.y && e.y != f.x && e.y != f.y &&
-                          contact::boxes_overlap(b, eb[col]);
+        for (uint32_t ia = ia0; ia <= ia1; ++ia) {
+            const uint32_t lo = cell_start[ia * g.b.count + ib0];
+            const uint32_t hi = cell_start[ia * g.b.count + ib1 + 1];
+            for (uint32_t k0 = lo; k0 < hi; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                bool hit = false;
+                uint32_t col = 0;
+                if (k < hi) {
+                    col = items[k];
+                    if (vertex_row) {
+                        const uint3 t = C.tid[col];
+                        hit = t.x != v && t.y != v && t.z != v && contact::boxes_overlap(b, tb[col]);
+                    } else {
+                        const uint2 f = C.eid[col];
+                        hit = col > i && e.x != f.x && e.x != f.y && e.y != f.x && e.y != f.y &&
+                              contact::boxes_overlap(b, eb[col]);
+                    }
                 }
+                const unsigned mask = __ballot_sync(0xffffffffu, hit);
+                if (write && hit) C.cand_tmp[base + hits + __popc(mask & ((1u << lane) - 1u))] = col;
+                hits += __popc(mask);
             }
-            const unsigned mask = __ballot_sync(0xffffffffu, hit);
-            if (write && hit) C.cand_tmp[base + hits + __popc(mask & ((1u << lane) - 1u))] = col;
-            hits += __popc(mask);
         }
         if (!write) {
             if (lane == 0) C.counts[row] = hits;
@@ -940,8 +977,8 @@ __device__ __forceinline__ void contact_detect(const ContactCtx& c, cooperative_
     if (!contact_failed(c.status)) contact_bin_counts(c);
     cluster.sync();
     if (c.me == 0 && !contact_failed(c.status)) {
-        block_scan(C_bins_t(c), make_bins(c.C->range, c.C->bins_cap).count, C_bins_t(c));
-        block_scan(C_bins_e(c), make_bins(c.C->range + 3, c.C->bins_cap).count, C_bins_e(c));
+        block_scan(C_bins_t(c), make_bins(c.C->range, c.C->bins_cap).count(), C_bins_t(c));
+        block_scan(C_bins_e(c), make_bins(c.C->range + 6, c.C->bins_cap).count(), C_bins_e(c));
     }
     cluster.sync();
     if (!contact_failed(c.status)) contact_bin_scatter(c);

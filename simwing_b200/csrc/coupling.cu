@@ -155,6 +155,8 @@ swb_status swb_coupling_create(swb_structure* structure, const uint64_t* structu
                                swb_coupling** out) {
     return guarded([&] {
         if (!structure || !out || (bindings && !structure_nodes)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        if (structure->borrowed)
+            raise(SWB_UNSUPPORTED, "a structure of a batch steps with its batch; couple a plain structure");
         StructureImpl& S = structure->s;
         const uint64_t N = S.def.nodes.size();
         auto c = std::make_unique<swb_coupling>();

@@ -392,9 +392,10 @@ void StructureImpl::setup_contact() {
                 hi[k] = i ? std::max(hi[k], q[k]) : q[k];
             }
         }
-        c.axis = 0;
-        for (int k = 1; k < 3; ++k)
-            if (hi[k] - lo[k] > hi[c.axis] - lo[c.axis]) c.axis = k;
+        int order[3] = {0, 1, 2};
+        std::sort(order, order + 3, [&](int a, int b) { return hi[a] - lo[a] > hi[b] - lo[b]; });
+        c.axis = order[0];
+        c.axis2 = order[1];
     }
     c.bins_cap = 1u << 16;
     c.tbin = dalloc<uint32_t>(owned, c.bins_cap + 1);
@@ -403,7 +404,7 @@ void StructureImpl::setup_contact() {
     c.ebin = dalloc<uint32_t>(owned, c.bins_cap + 1);
     c.ebin_fill = dalloc<uint32_t>(owned, c.bins_cap + 1);
     c.ebin_items = dalloc<uint32_t>(owned, std::max<uint32_t>(c.ne, 1));
-    c.range = dalloc<unsigned long long>(owned, 6);
+    c.range = dalloc<unsigned long long>(owned, 12);
     c.cand_tmp = dalloc<uint32_t>(owned, cap);
     c.mark_a = dalloc<uint32_t>(owned, cap + 1);
     c.mark_b = dalloc<uint32_t>(owned, cap + 1);
