@@ -196,3 +196,9 @@ def test_contact_with_a_pilot_matches_the_reference(cuda_device, ctas):
     with pytest.raises(sw.ContactStepError):
         dev.step(SLIDE)
     np.testing.assert_array_equal(dev.node_states(), before)
+
+
+def test_candidate_inspection_needs_contact(cuda_device):
+    s = sw.Structure(sw.generate_patch(nx=8, ny=8))
+    with pytest.raises(sw.Unsupported):
+        s.contact_candidates()

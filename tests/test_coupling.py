@@ -98,3 +98,11 @@ def test_invalid_transfers_are_refused_and_keep_the_pending_loads(cuda_device):
     np.testing.assert_array_equal(dev.node_states(), host.node_states())
     with pytest.raises(sw.OutOfRange):
         sw.Coupling(dev, [d.view.node_count])
+
+
+def test_a_batch_structure_is_not_coupled(cuda_device):
+    """A structure of a batch steps with its batch's launches."""
+    defs = [sw.generate_patch(nx=8, ny=8, seed=1), sw.generate_patch(nx=9, ny=9, seed=2)]
+    with sw.Batch(defs) as batch:
+        with pytest.raises(sw.Unsupported):
+            sw.Coupling(batch.structure(0), [0, 1, 2])
