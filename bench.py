@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-membrane-wing", action="store_true")
     p.add_argument("--no-contact", action="store_true")
+    p.add_argument("--no-coupling", action="store_true")
     p.add_argument("--only-adjoint", action="store_true",
                    help="run the adjoint leg alone and print its record (profiling)")
     p.add_argument("--only-contact", action="store_true",
@@ -170,6 +171,50 @@ def contact_leg(sw, steps, device, reference_steps, with_reference):
                 ref_times.append(ref.last_step_seconds() * 1000.0)
             out["reference_ms_per_step"] = float(sum(ref_times)) / len(ref_times)
             out["reference_cores"] = 1
+    return out
+
+
+def coupling_leg(sw, st, steps, device):
+    """A macro-step of the coupling caller (ConservativeMacroStepCoupling::
+    advanceStructure) on the wing, one interface node per structure node:
+    the interface impulses handed over from device memory
+    (swb_coupling_advance_impulses) against the same loads handed over from
+    host memory (set_external_forces, then step).  Wall-clock time per
+    macro-step, each call synchronised."""
+    import time
+
+    import numpy as np
+    import torch
+
+    d = sw.generate_wing()
+    n = d.view.node_count
+    rng = np.random.default_rng(11)
+    impulses = rng.normal(scale=1e-4, size=(n, 3))
+    forces = impulses * (1.0 / st.time_step)
+    d_impulses = torch.tensor(impulses, dtype=torch.float64, device=f"cuda:{device}")
+    out = {"workload": "ram-air wing, 38,417 interface nodes bound one to one, 48 iterations", "steps": steps}
+    s = sw.Structure(d, sw.SolverOptions(device=device))
+    coupling = sw.Coupling(s, np.arange(n, dtype=np.uint64))
+    for _ in range(3):
+        coupling.advance_impulses(d_impulses, st.time_step, st)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(steps):
+        coupling.advance_impulses(d_impulses, st.time_step, st)
+    out["device_loads_ms_per_step"] = (time.perf_counter() - t) * 1000.0 / steps
+    coupling.close()
+    s.close()
+    s = sw.Structure(d, sw.SolverOptions(device=device))
+    for _ in range(3):
+        s.set_external_forces(forces)
+        s.step(st)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(steps):
+        s.set_external_forces(forces)
+        s.step(st)
+    out["host_loads_ms_per_step"] = (time.perf_counter() - t) * 1000.0 / steps
+    s.close()
     return out
 
 
@@ -513,6 +558,9 @@ def main():
     membrane_wing = None
     if not args.no_membrane_wing and rank == 0:
         membrane_wing = membrane_wing_leg(sw, st, min(args.steps, 50), local, flush)
+    coupling = None
+    if not args.no_coupling and rank == 0:
+        coupling = coupling_leg(sw, st, min(args.steps, 50), local)
     contact = None
     if not args.no_contact and rank == 0:
         contact = contact_leg(sw, min(args.steps, 50), local, 2, not args.no_cpu_baseline)
@@ -545,6 +593,7 @@ def main():
             "adjoint": adjoint,
             "membrane_wing": membrane_wing,
             "contact": contact,
+            "coupling": coupling,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

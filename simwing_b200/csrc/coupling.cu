@@ -24,6 +24,7 @@ struct swb_coupling {
     double* d_pending = nullptr;    // [slots][3] the loads pending before the call
     double* d_applied = nullptr;    // [3] the total applied force (node order)
     int* d_flag = nullptr;          // 1: a non-finite load
+    std::vector<double> pending_host;  // staging of the pending loads
     std::vector<void*> owned;
     ~swb_coupling() {
         for (void* p : owned) cudaFree(p);
@@ -68,20 +69,33 @@ __global__ void gather_loads_kernel(uint32_t slots, const uint32_t* __restrict__
     total64[3 * s + 2] = f[2];
 }
 
-// Sum of the applied forces in node order (one thread: the order of the
-// reference's diagnostics sum).
+// Total of the applied forces: each thread sums a contiguous run of nodes in
+// node order, then the partial sums are added in thread order (one block, a
+// fixed order: the same total on every call).
 __global__ void applied_total_kernel(uint64_t nodes, const uint32_t* __restrict__ slot_of_node,
                                      const double* __restrict__ total64, double* out) {
+    __shared__ double part[3][1024];
+    const uint32_t t = threadIdx.x, threads = blockDim.x;
+    const uint64_t chunk = (nodes + threads - 1) / threads;
+    const uint64_t start = static_cast<uint64_t>(t) * chunk;
+    const uint64_t lo = start < nodes ? start : nodes;
+    const uint64_t hi = lo + chunk < nodes ? lo + chunk : nodes;
     double x = 0.0, y = 0.0, z = 0.0;
-    for (uint64_t n = 0; n < nodes; ++n) {
+    for (uint64_t n = lo; n < hi; ++n) {
         const uint32_t s = slot_of_node[n];
         x += total64[3 * s];
         y += total64[3 * s + 1];
         z += total64[3 * s + 2];
     }
-    out[0] = x;
-    out[1] = y;
-    out[2] = z;
+    part[0][t] = x;
+    part[1][t] = y;
+    part[2][t] = z;
+    __syncthreads();
+    if (t < 3) {
+        double sum = 0.0;
+        for (uint32_t k = 0; k < threads; ++k) sum += part[t][k];
+        out[t] = sum;
+    }
 }
 
 template <class T>
@@ -99,16 +113,24 @@ swb_status advance(swb_coupling* c, const double* a, const double* b, double sca
         S.validate_settings(*settings);
         cuda_check(cudaSetDevice(S.device), "cudaSetDevice");
         const uint32_t slots = static_cast<uint32_t>(S.def.nodes.size());
-        // the loads pending before the call, by slot
-        std::vector<double> pending(3 * static_cast<size_t>(slots));
-        for (uint64_t n = 0; n < S.def.nodes.size(); ++n) {
-            const uint32_t s = S.slot_of_node[n];
-            pending[3 * s] = S.pending[n].x;
-            pending[3 * s + 1] = S.pending[n].y;
-            pending[3 * s + 2] = S.pending[n].z;
+        // the loads pending before the call, by slot (cleared when none is)
+        const bool any_pending = std::any_of(S.pending.begin(), S.pending.end(), [](const swb_vec3& f) {
+            return f.x != 0.0 || f.y != 0.0 || f.z != 0.0;
+        });
+        if (any_pending) {
+            c->pending_host.assign(3 * static_cast<size_t>(slots), 0.0);
+            for (uint64_t n = 0; n < S.def.nodes.size(); ++n) {
+                const uint32_t s = S.slot_of_node[n];
+                c->pending_host[3 * s] = S.pending[n].x;
+                c->pending_host[3 * s + 1] = S.pending[n].y;
+                c->pending_host[3 * s + 2] = S.pending[n].z;
+            }
+            cuda_check(cudaMemcpy(c->d_pending, c->pending_host.data(), c->pending_host.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice), "pending upload");
+        } else {
+            cuda_check(cudaMemsetAsync(c->d_pending, 0, 3 * static_cast<size_t>(slots) * sizeof(double), S.stream),
+                       "memset");
         }
-        cuda_check(cudaMemcpyAsync(c->d_pending, pending.data(), pending.size() * sizeof(double),
-                                   cudaMemcpyHostToDevice, S.stream), "pending upload");
         cuda_check(cudaMemsetAsync(c->d_flag, 0, sizeof(int), S.stream), "memset");
         double* total64 = c->d_pending;  // overwritten in place, slot by slot
         gather_loads_kernel<<<(slots + 255) / 256, 256, 0, S.stream>>>(slots, c->d_offsets, c->d_items,
@@ -133,8 +155,8 @@ swb_status advance(swb_coupling* c, const double* a, const double* b, double sca
         S.device_forces = false;
         // the step consumed the loads: the applied total, in node order
         static_assert(sizeof(swb_vec3) == 3 * sizeof(double), "swb_vec3 layout");
-        applied_total_kernel<<<1, 1, 0, S.stream>>>(S.def.nodes.size(), c->d_items + c->bindings, total64,
-                                                    c->d_applied);
+        applied_total_kernel<<<1, 1024, 0, S.stream>>>(S.def.nodes.size(), c->d_items + c->bindings, total64,
+                                                       c->d_applied);
         cuda_check(cudaGetLastError(), "applied_total_kernel");
         swb_vec3 applied{};
         cuda_check(cudaMemcpyAsync(&applied, c->d_applied, sizeof(applied), cudaMemcpyDeviceToHost, S.stream),
