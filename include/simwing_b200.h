@@ -948,6 +948,59 @@ swb_status swb_cell_volumes(const swb_structure_definition* definition,
                             const double* positions,
                             swb_cell_volume* out);
 
+/* ---- Pneumatic port mass flows --------------------------------------- */
+/* evaluateOrificeMassFlow / evaluateConductanceMassFlow (pneumatics.cpp:   */
+/* 132-232, pneumatics.h:46-92): the flow laws that move air between the    */
+/* cells, inlets and reservoirs of the cell-air model, evaluated for many   */
+/* ports in one launch.                                                     */
+#define SWB_PORT_ORIFICE 0u     /* compressible orifice, choked or not     */
+#define SWB_PORT_CONDUCTANCE 1u /* linear mass conductance                  */
+#define SWB_FLOW_EQUILIBRIUM 0u
+#define SWB_FLOW_FIRST_TO_SECOND 1u
+#define SWB_FLOW_SECOND_TO_FIRST 2u
+
+typedef struct swb_air_properties {      /* AirProperties                */
+    double specific_gas_constant;        /* J/(kg K), 287.05 dry air     */
+    double heat_capacity_ratio;          /* gamma, 1.4 dry air           */
+} swb_air_properties;
+
+typedef struct swb_flow_zone_state {     /* FlowZoneState                */
+    double absolute_pressure;            /* Pa                           */
+    double absolute_temperature;         /* K                            */
+} swb_flow_zone_state;
+
+typedef struct swb_port_def {
+    uint32_t kind;                       /* SWB_PORT_*                   */
+    uint32_t reserved;                   /* 0                            */
+    uint64_t first, second;              /* zone indices                 */
+    double discharge_coefficient;        /* orifice: 0 < Cd <= 1         */
+    double effective_area;               /* orifice: m^2                 */
+    double mass_conductance;             /* conductance: kg/(s Pa)       */
+    double opening_fraction;             /* [0, 1]                       */
+} swb_port_def;
+
+typedef struct swb_mass_flow {           /* MassFlowEvaluation           */
+    double signed_mass_rate;             /* kg/s, positive first->second */
+    double magnitude;
+    double pressure_ratio;
+    double critical_pressure_ratio;
+    uint32_t direction;                  /* SWB_FLOW_*                   */
+    uint32_t choked;
+} swb_mass_flow;
+
+/* One evaluation per port, from the zones' states (host arrays).  A port
+ * the reference would refuse (invalid air, zone state, opening or port
+ * constants, a non-finite flow) makes the call return SWB_INVALID_ARGUMENT
+ * with the first such port in *failed_port (nullable; port_count when none);
+ * `out` is then unspecified.  A zone index past zone_count: SWB_OUT_OF_RANGE. */
+swb_status swb_port_mass_flows(const swb_air_properties* air,
+                               const swb_flow_zone_state* zones,
+                               uint64_t zone_count,
+                               const swb_port_def* ports,
+                               uint64_t port_count,
+                               swb_mass_flow* out,
+                               uint64_t* failed_port);
+
 /* The candidate features of the last step's contact certification
  * (contact.cpp:1583-1798: the final broadphase, in key order), for
  * inspection; valid until the next step.  SWB_OUT_OF_RANGE (count written)

@@ -63,6 +63,8 @@ _REF = {
     "swref_contact_candidates": (C.c_int, [P(abi.StructureDefinition), C.c_double, C.c_void_p, C.c_void_p,
                                            P(abi.ContactKey), C.c_uint64, P(C.c_uint64), P(C.c_uint64),
                                            P(C.c_uint64)]),
+    "swref_port_mass_flows": (C.c_int, [P(abi.AirProperties), C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                        C.c_void_p, P(C.c_uint64)]),
     "swref_contact_closest": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_double,
                                         P(abi.ClosestResult)]),
     "swref_contact_sweep": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -332,3 +334,16 @@ def ref_contact_sweep(kind, first_previous, first_current, second_previous, seco
     _ref_check(ref_library().swref_contact_sweep(kind, n, *[a.ctypes.data for a in arrays], separation,
                                                  C.byref(settings), out))
     return list(out)[:n]
+
+
+def ref_port_mass_flows(zones, ports, air=(287.05, 1.4)):
+    """The reference's flow laws over many ports (swref_port_mass_flows):
+    returns (status, flows, first refusing port)."""
+    z = np.array(zones, dtype=abi.ZONE_DTYPE).reshape(-1)
+    p = np.array(ports, dtype=abi.PORT_DTYPE).reshape(-1)
+    out = np.zeros(len(p), dtype=abi.FLOW_DTYPE)
+    failed = C.c_uint64(0)
+    a = abi.AirProperties(*air)
+    status = ref_library().swref_port_mass_flows(C.byref(a), z.ctypes.data, len(z), p.ctypes.data, len(p),
+                                                 out.ctypes.data, C.byref(failed))
+    return status, out, failed.value

@@ -20,6 +20,7 @@
 #include <softwing/soft_body.h>
 #include <softwing/suspension.h>
 #include <softwing/cell_volume.h>
+#include <softwing/pneumatics.h>
 
 #include <chrono>
 #include <cmath>
@@ -692,3 +693,53 @@ swb_status swref_cell_volumes(const swb_structure_definition* d,
 }
 
 }  // extern "C"
+
+// evaluateOrificeMassFlow / evaluateConductanceMassFlow (pneumatics.cpp:
+// 132-232) over many ports, with swb_port_mass_flows's conventions: the first
+// port the reference refuses is reported, as SWB_INVALID_ARGUMENT.
+extern "C" swb_status swref_port_mass_flows(const swb_air_properties* air,
+                                            const swb_flow_zone_state* zones,
+                                            uint64_t zone_count,
+                                            const swb_port_def* ports,
+                                            uint64_t port_count,
+                                            swb_mass_flow* out,
+                                            uint64_t* failed_port) {
+    if (failed_port) *failed_port = port_count;
+    softwing::AirProperties a;
+    a.specificGasConstant = air->specific_gas_constant;
+    a.heatCapacityRatio = air->heat_capacity_ratio;
+    for (uint64_t i = 0; i < port_count; ++i)
+        if (ports[i].first >= zone_count || ports[i].second >= zone_count) return SWB_OUT_OF_RANGE;
+    for (uint64_t i = 0; i < port_count; ++i) {
+        const swb_port_def& p = ports[i];
+        softwing::FlowZoneState first{zones[p.first].absolute_pressure, zones[p.first].absolute_temperature};
+        softwing::FlowZoneState second{zones[p.second].absolute_pressure, zones[p.second].absolute_temperature};
+        try {
+            if (p.reserved != 0 || p.kind > SWB_PORT_CONDUCTANCE) throw std::invalid_argument("port kind");
+            softwing::MassFlowEvaluation e;
+            if (p.kind == SWB_PORT_ORIFICE) {
+                softwing::OrificeDefinition d;
+                d.dischargeCoefficient = p.discharge_coefficient;
+                d.effectiveArea = p.effective_area;
+                d.openingFraction = p.opening_fraction;
+                e = softwing::evaluateOrificeMassFlow(first, second, a, d);
+            } else {
+                softwing::ConductanceDefinition d;
+                d.massConductance = p.mass_conductance;
+                d.openingFraction = p.opening_fraction;
+                e = softwing::evaluateConductanceMassFlow(first, second, d);
+            }
+            swb_mass_flow& o = out[i];
+            std::memset(&o, 0, sizeof o);
+            o.signed_mass_rate = e.signedMassRate;
+            o.magnitude = e.magnitude;
+            o.pressure_ratio = e.pressureRatio;
+            o.critical_pressure_ratio = e.criticalPressureRatio;
+            o.direction = static_cast<uint32_t>(e.direction);
+            o.choked = e.choked ? 1u : 0u;
+        } catch (const std::invalid_argument&) {
+            if (failed_port && *failed_port == port_count) *failed_port = i;
+        }
+    }
+    return failed_port && *failed_port != port_count ? SWB_INVALID_ARGUMENT : SWB_OK;
+}

@@ -24,6 +24,7 @@ from .abi import Vec3
 __all__ = [
     "Structure", "Definition", "StepSettings", "SolverOptions", "generate_patch", "generate_wing",
     "SimwingError", "InvalidArgument", "OutOfRange", "SuspensionError", "ContactStepError",
+    "port_mass_flows",
     "NonFiniteState", "SyncTimeout", "CudaError", "Unsupported", "reference_colouring",
     "definition_from_arrays", "plan_schedule",
 ]
@@ -445,6 +446,29 @@ def contact_candidates(definition: Definition, half_thickness: float, previous, 
     _check(lib.swb_contact_candidates(definition.pointer, half_thickness, prev.ctypes.data, cur.ctypes.data, keys,
                                       n.value, C.byref(n), C.byref(possible), C.byref(excluded)))
     return list(keys)[: n.value], possible.value, excluded.value
+
+
+def port_mass_flows(zones, ports, air=(287.05, 1.4)):
+    """Mass flow through each pneumatic port between two zones
+    (evaluateOrificeMassFlow / evaluateConductanceMassFlow,
+    pneumatics.cpp:132-232), one device thread per port.  `zones` are
+    (absolute pressure Pa, absolute temperature K) records, `ports` records
+    of abi.PORT_DTYPE, `air` (R, gamma).  Returns abi.FLOW_DTYPE records.
+    Raises InvalidArgument where the reference throws, with the first
+    refusing port in the exception's `port`."""
+    z = np.array(zones, dtype=abi.ZONE_DTYPE).reshape(-1)
+    p = np.array(ports, dtype=abi.PORT_DTYPE).reshape(-1)
+    out = np.zeros(len(p), dtype=abi.FLOW_DTYPE)
+    failed = C.c_uint64(0)
+    a = abi.AirProperties(*air)
+    status = abi.library().swb_port_mass_flows(C.byref(a), z.ctypes.data, len(z), p.ctypes.data, len(p),
+                                               out.ctypes.data, C.byref(failed))
+    try:
+        _check(status)
+    except InvalidArgument as e:
+        e.port = failed.value
+        raise
+    return out
 
 
 def contact_closest(kind: int, first, second, separation: float):

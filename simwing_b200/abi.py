@@ -7,6 +7,8 @@ C or C++ host binds.
 from __future__ import annotations
 
 import ctypes as C
+
+import numpy as np
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -112,6 +114,21 @@ CCD_MAX_SUBDIVISIONS = 4096
 class ContactKey(C.Structure):
     _fields_ = [("pair", C.c_uint64), ("kind", C.c_uint32), ("reserved", C.c_uint32),
                 ("first", C.c_uint64 * 3), ("second", C.c_uint64 * 3)]
+
+
+class AirProperties(C.Structure):
+    _fields_ = [("specific_gas_constant", C.c_double), ("heat_capacity_ratio", C.c_double)]
+
+
+# swb_flow_zone_state, swb_port_def and swb_mass_flow as numpy records
+ZONE_DTYPE = np.dtype([("absolute_pressure", "<f8"), ("absolute_temperature", "<f8")])
+PORT_DTYPE = np.dtype([("kind", "<u4"), ("reserved", "<u4"), ("first", "<u8"), ("second", "<u8"),
+                       ("discharge_coefficient", "<f8"), ("effective_area", "<f8"), ("mass_conductance", "<f8"),
+                       ("opening_fraction", "<f8")])
+FLOW_DTYPE = np.dtype([("signed_mass_rate", "<f8"), ("magnitude", "<f8"), ("pressure_ratio", "<f8"),
+                       ("critical_pressure_ratio", "<f8"), ("direction", "<u4"), ("choked", "<u4")])
+PORT_ORIFICE, PORT_CONDUCTANCE = 0, 1
+FLOW_EQUILIBRIUM, FLOW_FIRST_TO_SECOND, FLOW_SECOND_TO_FIRST = 0, 1, 2
 
 
 class CcdSettings(C.Structure):
@@ -303,6 +320,8 @@ _PROTOTYPES = {
                                                       P(Diagnostics)]),
     "swb_contact_candidates": (C.c_int, [P(StructureDefinition), C.c_double, C.c_void_p, C.c_void_p, P(ContactKey),
                                          C.c_uint64, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
+    "swb_port_mass_flows": (C.c_int, [P(AirProperties), C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p,
+                                      P(C.c_uint64)]),
     "swb_contact_closest": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_double, P(ClosestResult)]),
     "swb_contact_sweep": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_double, P(CcdSettings), P(CcdResult)]),
