@@ -14,9 +14,11 @@ generator); the reference's wing meshes are not shipped.
           uploads that step's external forces from host memory
           (swb_structure_set_external_forces) and reads the step's
           diagnostics back (swb_structure_step with a diagnostics output);
-  roofline  algorithmic bytes per step (the per-visit byte model in
-          DESIGN.md) over the device time per step, against the measured
-          HBM copy bandwidth;
+  roofline  algorithmic bytes per step (the per-visit byte model:
+          S*[144 N + 52 T + I*(88 E_d + 160 E_b + 52 E_s) + 4 (E_d + E_b)])
+          over the device time per step, against the measured HBM copy
+          bandwidth; `traffic` is the DRAM bytes per launch of the committed
+          ncu capture of this workload (profiles/), not measured in the run;
   cpu_baseline  the reference Structure::step (oracle/_ref, serial) on a
           bounded sample of the same workload, timed on this host.
 
@@ -83,15 +85,25 @@ def replica_rate(units_per_rank, world, seconds):
 
 
 def wing_config():
-    return {"workload": "plain ram-air wing, 40 cells x 60 chordwise (66,936 tri), 48 iterations, 1 substep, "
+    return {"workload": "plain ram-air wing, 40 cells x 60 chordwise (68,412 tri, 39,155 nodes), 48 iterations, 1 substep, "
                         "dt 1/120 s, 30 Pa + gravity, rigid pilot on 2 risers",
             "cells": 40, "chordwise": 60, "iterations": 48, "substeps": 1,
             "l2": "flushed before every timed step (256 MiB write)"}
 
 
-def settings(sw):
-    return sw.StepSettings(time_step=1.0 / 120.0, substeps=1, constraint_iterations=48, gravity=(0.0, 0.0, -9.81),
-                           velocity_damping=0.25)
+def settings(sw=None):
+    """The workload's step settings (dt 1/120 s, 1 substep, 48 iterations,
+    gravity, damping 0.25; no cable sweep pairs, serial), filled in plain
+    ctypes so that the reference arm needs no product library."""
+    from simwing_b200 import abi
+
+    s = abi.StepSettings()
+    s.time_step = 1.0 / 120.0
+    s.substeps = 1
+    s.constraint_iterations = 48
+    s.gravity = abi.Vec3(0.0, 0.0, -9.81)
+    s.velocity_damping = 0.25
+    return s
 
 
 def algorithmic_bytes(definition, iterations=48, substeps=1):
@@ -106,7 +118,7 @@ def algorithmic_bytes(definition, iterations=48, substeps=1):
 
 def membrane_wing_leg(sw, st, steps, device, flush):
     """The same wing with its fabric as the reference's scene assembly builds
-    it: one orthotropic membrane element per skin and rib triangle (66,936)
+    it: one orthotropic membrane element per skin and rib triangle (68,412)
     and no fabric edge constraints; seams, lines and pilot as before.  Device
     steps/s from CUDA events, L2 flushed before every timed step."""
     import torch
@@ -126,7 +138,7 @@ def membrane_wing_leg(sw, st, steps, device, flush):
     rep = s.schedule_report()
     s.close()
     total = float(sum(times))
-    return {"workload": "ram-air wing, 40 cells x 60 chordwise, fabric as membrane elements (66,936), 48 iterations",
+    return {"workload": "ram-air wing, 40 cells x 60 chordwise, fabric as membrane elements (68,412), 48 iterations",
             "membranes": d.counts()["membranes"], "constraints": d.counts()["constraints"],
             "stages_per_iteration": rep.local_stages_per_iteration, "steps": steps,
             "ms_per_step": total / steps, "wing_steps_per_s": steps / (total / 1000.0),
@@ -192,7 +204,7 @@ def coupling_leg(sw, st, steps, device):
     impulses = rng.normal(scale=1e-4, size=(n, 3))
     forces = impulses * (1.0 / st.time_step)
     d_impulses = torch.tensor(impulses, dtype=torch.float64, device=f"cuda:{device}")
-    out = {"workload": "ram-air wing, 38,417 interface nodes bound one to one, 48 iterations", "steps": steps}
+    out = {"workload": "ram-air wing, 39,155 interface nodes bound one to one, 48 iterations", "steps": steps}
     s = sw.Structure(d, sw.SolverOptions(device=device))
     coupling = sw.Coupling(s, np.arange(n, dtype=np.uint64))
     for _ in range(3):
@@ -403,9 +415,8 @@ def cpu_reference_run(definition, steps, threads):
     """Reference Structure::step on this host (oracle/_ref when built,
     otherwise the C restatement)."""
     from oracle import oracle as O
-    import simwing_b200 as sw
 
-    st = settings(sw)
+    st = settings()
     st.worker_threads = threads
     if O.ref_available():
         ref = O.RefStructure(definition)
@@ -438,9 +449,19 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import simwing_b200 as sw
+    import tempfile
 
-    definition = sw.generate_wing()
+    from oracle import definition_file
+
+    # The wing comes from the product's generator, run in a child process
+    # that writes it to a file: this process maps only the reference build.
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "wing.npz")
+        subprocess.run([sys.executable, "-c",
+                        "import sys; sys.path.insert(0, sys.argv[1]); import simwing_b200 as sw; "
+                        "from oracle import definition_file as F; F.save(sw.generate_wing(), sys.argv[2])",
+                        ROOT, path], check=True)
+        definition = definition_file.FileDefinition(path)
     cores = physical_cores()
     sample = max(1, min(args.steps, 8))
     value, kind, used = cpu_reference_run(definition, sample, cores)

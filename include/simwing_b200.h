@@ -785,6 +785,45 @@ typedef struct swb_contact_key {
     uint64_t second[3];
 } swb_contact_key;
 
+/* ------------------------------------------------------------------------ */
+/* Details of the last failure on this thread, for the callers that read    */
+/* them off the reference's exceptions: SuspensionError::phase() and        */
+/* entity() (src/softwing/include/softwing/suspension.h:27-53) and          */
+/* ContactStepError::key() (src/softwing/include/softwing/contact.h:        */
+/* 262-270).                                                                 */
+/* ------------------------------------------------------------------------ */
+/* softwing::SuspensionPhase, in declaration order. */
+#define SWB_PHASE_PARSE 0u
+#define SWB_PHASE_VALIDATION 1u
+#define SWB_PHASE_ATTACHMENT_RESOLUTION 2u
+#define SWB_PHASE_GRAPH_CONSTRUCTION 3u
+#define SWB_PHASE_CONTROL 4u
+#define SWB_PHASE_PREDICTION 5u
+#define SWB_PHASE_LINE_SOLVE 6u
+#define SWB_PHASE_GROUND_SOLVE 7u
+#define SWB_PHASE_CERTIFICATION 8u
+#define SWB_PHASE_DIAGNOSTICS 9u
+
+typedef struct swb_error_detail {
+    uint32_t status;              /* status of the failure described        */
+    uint32_t suspension_phase;    /* SWB_SUSPENSION_ERROR: SWB_PHASE_*       */
+    char suspension_entity[128];  /* SWB_SUSPENSION_ERROR: the entity, e.g.
+                                     "segment:<stable id>", "line-residual",
+                                     "payload", "payload-step"             */
+    uint32_t has_contact_key;     /* SWB_CONTACT_ERROR: 1 when the failure
+                                     belongs to a feature; 0 gives the
+                                     reference's default-constructed key   */
+    uint32_t reserved;
+    swb_contact_key contact_key;  /* SWB_CONTACT_ERROR: the failing feature
+                                     first in key order (the one the
+                                     reference's key-ordered sweep throws
+                                     at)                                    */
+} swb_error_detail;
+
+/* Copies the details of the last failing call on this thread (zeroed with
+ * `status` SWB_OK when the last failure had none to give). */
+swb_status swb_last_error_detail(swb_error_detail* out);
+
 /* CcdSettings (contact.h:160-165) */
 typedef struct swb_ccd_settings {
     int32_t conservative_iterations;   /* 32                                 */

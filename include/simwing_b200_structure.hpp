@@ -43,18 +43,62 @@
 
 namespace softwing {
 
-// softwing::SuspensionError (src/softwing/include/softwing/suspension.h:40)
-// without the phase/entity details, which the device status does not carry.
-class SuspensionError : public std::runtime_error {
-public:
-    using std::runtime_error::runtime_error;
+// softwing::SuspensionPhase (src/softwing/include/softwing/suspension.h:27-38),
+// in the same order as SWB_PHASE_*.
+enum class SuspensionPhase {
+    Parse,
+    Validation,
+    AttachmentResolution,
+    GraphConstruction,
+    Control,
+    Prediction,
+    LineSolve,
+    GroundSolve,
+    Certification,
+    Diagnostics,
 };
 
-// softwing::ContactStepError (src/softwing/include/softwing/contact.h:262)
-// without the failing feature key.
+// softwing::SuspensionError (src/softwing/include/softwing/suspension.h:40-53).
+class SuspensionError : public std::runtime_error {
+public:
+    SuspensionError(SuspensionPhase phase, std::string entity, const std::string& message)
+        : std::runtime_error(message), phase_(phase), entity_(std::move(entity)) {}
+
+    [[nodiscard]] SuspensionPhase phase() const { return phase_; }
+    [[nodiscard]] const std::string& entity() const { return entity_; }
+
+private:
+    SuspensionPhase phase_;
+    std::string entity_;
+};
+
+// softwing::ContactFeatureKind and ContactFeatureKey
+// (src/softwing/include/softwing/contact.h:27-31, 95-101).
+enum class ContactFeatureKind {
+    VertexTriangle,
+    EdgeEdge,
+    SegmentTriangle,
+};
+
+struct ContactFeatureKey {
+    std::size_t pair = 0;
+    ContactFeatureKind kind = ContactFeatureKind::VertexTriangle;
+    std::array<std::size_t, 3> firstPrimitive{};
+    std::array<std::size_t, 3> secondPrimitive{};
+
+    auto operator<=>(const ContactFeatureKey&) const = default;
+};
+
+// softwing::ContactStepError (src/softwing/include/softwing/contact.h:262-270).
 class ContactStepError : public std::runtime_error {
 public:
-    using std::runtime_error::runtime_error;
+    ContactStepError(const ContactFeatureKey& key, const std::string& message)
+        : std::runtime_error(message), key_(key) {}
+
+    [[nodiscard]] const ContactFeatureKey& key() const { return key_; }
+
+private:
+    ContactFeatureKey key_;
 };
 
 }  // namespace softwing
@@ -75,15 +119,34 @@ public:
     using std::logic_error::logic_error;
 };
 
-// Throws the exception the reference adapter throws for `status`.
+// Throws the exception the reference adapter throws for `status`, with the
+// suspension phase and entity or the contact feature key of the failure.
 inline void check(swb_status status) {
     if (status == SWB_OK) return;
     const std::string what = swb_last_error() ? swb_last_error() : "simwing_b200 error";
+    swb_error_detail detail{};
+    if (swb_last_error_detail(&detail) != SWB_OK || detail.status != static_cast<uint32_t>(status))
+        detail = swb_error_detail{};
     switch (status) {
     case SWB_INVALID_ARGUMENT: throw std::invalid_argument(what);
     case SWB_OUT_OF_RANGE: throw std::out_of_range(what);
-    case SWB_SUSPENSION_ERROR: throw softwing::SuspensionError(what);
-    case SWB_CONTACT_ERROR: throw softwing::ContactStepError(what);
+    case SWB_SUSPENSION_ERROR: {
+        const char* entity = detail.status ? detail.suspension_entity : "";
+        throw softwing::SuspensionError(static_cast<softwing::SuspensionPhase>(detail.suspension_phase),
+                                        std::string(entity, strnlen(entity, sizeof detail.suspension_entity)), what);
+    }
+    case SWB_CONTACT_ERROR: {
+        softwing::ContactFeatureKey key{};
+        if (detail.has_contact_key) {
+            key.pair = static_cast<std::size_t>(detail.contact_key.pair);
+            key.kind = static_cast<softwing::ContactFeatureKind>(detail.contact_key.kind);
+            for (int i = 0; i < 3; ++i) {
+                key.firstPrimitive[i] = static_cast<std::size_t>(detail.contact_key.first[i]);
+                key.secondPrimitive[i] = static_cast<std::size_t>(detail.contact_key.second[i]);
+            }
+        }
+        throw softwing::ContactStepError(key, what);
+    }
     case SWB_UNSUPPORTED: throw Unsupported(what);
     case SWB_OUT_OF_MEMORY: throw std::bad_alloc();
     default: throw DeviceStepError(status, what);

@@ -48,6 +48,7 @@ _PORT = {
 _REF = {
     "swref_last_error": (C.c_char_p, []),
     "swref_physical_cores": (C.c_uint, []),
+    "swref_last_error_detail": (C.c_int, [P(abi.ErrorDetail)]),
     "swref_create": (C.c_int, [P(abi.StructureDefinition), P(C.c_void_p)]),
     "swref_destroy": (None, [C.c_void_p]),
     "swref_fingerprint": (C.c_uint64, [C.c_void_p]),
@@ -104,9 +105,14 @@ def ref_library() -> C.CDLL:
 
 
 class OracleError(RuntimeError):
-    def __init__(self, status, message):
+    """A checker's failure; for the reference build's SuspensionError and
+    ContactStepError also `phase`/`entity` or `key`, as the product's
+    exceptions carry them."""
+
+    def __init__(self, status, message, phase=None, entity=None, key=None):
         super().__init__(f"status {status}: {message}")
         self.status = status
+        self.phase, self.entity, self.key = phase, entity, key
 
 
 class _Base:
@@ -117,7 +123,18 @@ class _Base:
 
     def _check(self, status):
         if status != 0:
-            raise OracleError(status, getattr(self._lib(), self._prefix + "last_error")().decode())
+            message = getattr(self._lib(), self._prefix + "last_error")().decode()
+            phase = entity = key = None
+            if self._prefix == "swref_" and status in (abi.SUSPENSION_ERROR, abi.CONTACT_ERROR):
+                d = abi.ErrorDetail()
+                ref_library().swref_last_error_detail(C.byref(d))
+                if status == abi.SUSPENSION_ERROR:
+                    phase = abi.SUSPENSION_PHASES[d.suspension_phase]
+                    entity = d.suspension_entity.decode(errors="replace")
+                else:
+                    k = d.contact_key
+                    key = (int(k.pair), int(k.kind), tuple(int(x) for x in k.first), tuple(int(x) for x in k.second))
+            raise OracleError(status, message, phase, entity, key)
 
     def __init__(self, definition):
         self._definition = definition  # keep alive

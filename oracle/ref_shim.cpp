@@ -24,6 +24,7 @@
 
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -48,6 +49,9 @@ struct ContactAuditTestAccess {
 namespace {
 
 thread_local std::string g_error;
+// The reference's exception details of the last failure (SuspensionError
+// phase/entity, ContactStepError key), for comparison with the device's.
+thread_local swb_error_detail g_detail{};
 
 using namespace simwing::fsi;
 
@@ -175,6 +179,7 @@ struct RefHandle {
 
 swb_status fail(swb_status status, const std::exception& error) {
     g_error = error.what();
+    g_detail = swb_error_detail{};
     return status;
 }
 
@@ -182,9 +187,23 @@ swb_status translate() {
     try {
         throw;
     } catch (const softwing::SuspensionError& e) {
-        return fail(SWB_SUSPENSION_ERROR, e);
+        const swb_status st = fail(SWB_SUSPENSION_ERROR, e);
+        g_detail.status = st;
+        g_detail.suspension_phase = static_cast<uint32_t>(e.phase());
+        std::snprintf(g_detail.suspension_entity, sizeof g_detail.suspension_entity, "%s", e.entity().c_str());
+        return st;
     } catch (const softwing::ContactStepError& e) {
-        return fail(SWB_CONTACT_ERROR, e);
+        const swb_status st = fail(SWB_CONTACT_ERROR, e);
+        const softwing::ContactFeatureKey& k = e.key();
+        g_detail.status = st;
+        g_detail.has_contact_key = 1;
+        g_detail.contact_key.pair = k.pair;
+        g_detail.contact_key.kind = static_cast<uint32_t>(k.kind);
+        for (int i = 0; i < 3; ++i) {
+            g_detail.contact_key.first[i] = k.firstPrimitive[i];
+            g_detail.contact_key.second[i] = k.secondPrimitive[i];
+        }
+        return st;
     } catch (const std::out_of_range& e) {
         return fail(SWB_OUT_OF_RANGE, e);
     } catch (const std::invalid_argument& e) {
@@ -251,6 +270,12 @@ StructureStepSettings convert(const swb_step_settings& s) {
 extern "C" {
 
 const char* swref_last_error(void) { return g_error.c_str(); }
+
+int swref_last_error_detail(swb_error_detail* out) {
+    if (!out) return SWB_INVALID_ARGUMENT;
+    *out = g_detail;
+    return SWB_OK;
+}
 
 unsigned swref_physical_cores(void) {
     return softwing::hardwarePhysicalCoreCount();

@@ -43,11 +43,19 @@ class OutOfRange(SimwingError, IndexError):
 
 
 class SuspensionError(SimwingError):
+    """softwing::SuspensionError: `phase` (a SuspensionPhase name) and
+    `entity`, as its phase() and entity() give them."""
     status = abi.SUSPENSION_ERROR
+    phase = None
+    entity = None
 
 
 class ContactStepError(SimwingError):
+    """softwing::ContactStepError: `key`, its ContactFeatureKey as (pair,
+    kind, first, second) -- the default key (0, 0, (0, 0, 0), (0, 0, 0))
+    when the failure belongs to no feature."""
     status = abi.CONTACT_ERROR
+    key = None
 
 
 class NonFiniteState(SimwingError):
@@ -76,8 +84,20 @@ _ERRORS = {cls.status: cls for cls in (InvalidArgument, OutOfRange, SuspensionEr
 
 def _check(status: int) -> None:
     if status != abi.OK:
-        message = abi.library().swb_last_error().decode(errors="replace")
-        raise _ERRORS.get(status, SimwingError)(message)
+        lib = abi.library()
+        message = lib.swb_last_error().decode(errors="replace")
+        error = _ERRORS.get(status, SimwingError)(message)
+        if status in (abi.SUSPENSION_ERROR, abi.CONTACT_ERROR):
+            d = abi.ErrorDetail()
+            lib.swb_last_error_detail(C.byref(d))
+            if d.status == status and status == abi.SUSPENSION_ERROR:
+                error.phase = abi.SUSPENSION_PHASES[d.suspension_phase]
+                error.entity = d.suspension_entity.decode(errors="replace")
+            elif d.status == status:
+                k = d.contact_key
+                error.key = (int(k.pair), int(k.kind), tuple(int(x) for x in k.first),
+                             tuple(int(x) for x in k.second))
+        raise error
 
 
 def StepSettings(**overrides) -> abi.StepSettings:

@@ -116,6 +116,16 @@ class ContactKey(C.Structure):
                 ("first", C.c_uint64 * 3), ("second", C.c_uint64 * 3)]
 
 
+# softwing::SuspensionPhase in declaration order (suspension.h:27-38)
+SUSPENSION_PHASES = ("Parse", "Validation", "AttachmentResolution", "GraphConstruction", "Control", "Prediction",
+                     "LineSolve", "GroundSolve", "Certification", "Diagnostics")
+
+
+class ErrorDetail(C.Structure):
+    _fields_ = [("status", C.c_uint32), ("suspension_phase", C.c_uint32), ("suspension_entity", C.c_char * 128),
+                ("has_contact_key", C.c_uint32), ("reserved", C.c_uint32), ("contact_key", ContactKey)]
+
+
 class AirProperties(C.Structure):
     _fields_ = [("specific_gas_constant", C.c_double), ("heat_capacity_ratio", C.c_double)]
 
@@ -248,6 +258,7 @@ SWEEP_DISTANCE, SWEEP_DIHEDRAL, SWEEP_MEMBRANE = 0, 1, 2
 P = C.POINTER
 _PROTOTYPES = {
     "swb_last_error": (C.c_char_p, []),
+    "swb_last_error_detail": (C.c_int, [C.POINTER(ErrorDetail)]),
     "swb_abi_version": (C.c_uint32, []),
     "swb_default_step_settings": (None, [P(StepSettings)]),
     "swb_default_solver_options": (None, [P(SolverOptions)]),

@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     }
     if (owner && tid == 0) {
         for (int k = 0; k < 8; ++k) pay.lambda[k] = 0.0f;
-        if (!payload_predict(pdef, pay, p.dt, p.gravity)) susp_fail(I.status, kSuspPayload);
+        if (!payload_predict(pdef, pay, p.dt, p.gravity)) susp_fail(I.status, kSuspPredict);
     }
     if (guard) {
         // momentum of the predicted state (the guard's target)

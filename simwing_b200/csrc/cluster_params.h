@@ -143,6 +143,8 @@ struct ContactDev {
     ContactEntry* cand_entry;          // [cand_cap] the candidate's table entry after the iteration
     ContactRecordDev* cand_rec;        // [cand_cap] the candidate's certified record
     unsigned long long* reduce;        // [2] active records, largest penetration (bits)
+    unsigned long long* fail;          // [1] the failing feature first in key order, packed with its
+                                       // detail code (contact_fail_at); all ones when none failed
 };
 
 // Per-instance tables and state (one cluster each).

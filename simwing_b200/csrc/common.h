@@ -11,11 +11,19 @@
 namespace swb {
 
 // Error carrying an swb_status; every C-ABI entry point catches it and
-// stores the message for swb_last_error().
+// stores the message for swb_last_error() and, when the failure has one,
+// its detail (suspension phase and entity, contact feature key) for
+// swb_last_error_detail().
 struct Error : std::runtime_error {
     swb_status status;
+    bool has_detail = false;
+    swb_error_detail detail{};
     Error(swb_status s, const std::string& message)
         : std::runtime_error(message), status(s) {}
+    Error(swb_status s, const std::string& message, const swb_error_detail& d)
+        : std::runtime_error(message), status(s), has_detail(true), detail(d) {
+        detail.status = static_cast<uint32_t>(s);
+    }
 };
 
 [[noreturn]] inline void raise(swb_status status, const std::string& message) {
@@ -23,6 +31,7 @@ struct Error : std::runtime_error {
 }
 
 void set_last_error(const std::string& message);
+void set_last_error_detail(const swb_error_detail* detail);  // nullptr clears it
 
 // Runs `body` and converts exceptions into a status + thread-local message.
 template <class F>
@@ -32,6 +41,7 @@ swb_status guarded(F&& body) {
         return SWB_OK;
     } catch (const Error& e) {
         set_last_error(e.what());
+        set_last_error_detail(e.has_detail ? &e.detail : nullptr);
         return e.status;
     } catch (const std::bad_alloc&) {
         set_last_error("out of host memory");

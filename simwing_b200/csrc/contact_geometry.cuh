@@ -253,11 +253,22 @@ struct Interval {
 // Bisection of [safe, impact] to the time tolerance (sweptContact's
 // refineImpact, contact.cpp:778-804).  Returns false on an uncertifiable
 // midpoint (state Indeterminate).
+//
+// A tolerance below the spacing of doubles near the impact time lets the
+// midpoint round onto an end of the interval.  When the update then leaves
+// the interval as it was, every later pass would evaluate the same midpoint
+// and change nothing again (the reference's loop spins there for good), so
+// the search stops with the interval it has.  Wherever the reference's loop
+// ends, every pass changes the interval and the result is the same.  A pass
+// that changes the interval roughly halves it, so the search takes at most
+// about 1,100 passes; kMaxRefinePasses bounds it regardless.
+constexpr int kMaxRefinePasses = 4096;
+
 __device__ __forceinline__ bool refine_impact(uint32_t kind, const Linear& f, const Linear& s, double separation,
                                               const swb_ccd_settings& cs, double safe, double impact,
                                               Closest impact_geometry, Ccd& out) {
     double lower = safe, upper = impact;
-    while (upper - lower > cs.time_tolerance) {
+    for (int pass = 0; upper - lower > cs.time_tolerance && pass < kMaxRefinePasses; ++pass) {
         const double middle = 0.5 * (lower + upper);
         const Closest g = evaluate_at(kind, f, s, middle, separation);
         if (!g.certified()) {
@@ -265,12 +276,14 @@ __device__ __forceinline__ bool refine_impact(uint32_t kind, const Linear& f, co
             out.geometry = g;
             return false;
         }
+        const double was_lower = lower, was_upper = upper;
         if (g.gap <= cs.distance_tolerance) {
             upper = middle;
             impact_geometry = g;
         } else {
             lower = middle;
         }
+        if (lower == was_lower && upper == was_upper) break;
     }
     out.state = SWB_CCD_IMPACT;
     out.toi = upper;

@@ -55,6 +55,20 @@ __device__ __forceinline__ void contact_fail(int* status, int code) {
     if ((atomicOr(status, kStatusContact) & kStatusContact) == 0) status[1] = code;
 }
 
+// A failure that belongs to a candidate feature also records the feature.
+// The reference's sweeps are key-ordered and throw at their first failing
+// feature, so the device keeps the failing feature first in key order: the
+// candidate code (row << 32 | col) packed with the detail code as
+// row << 37 | col << 5 | detail (rows stay below 2^27), kept by atomicMin
+// in C.fail, which is reset before every step.
+__device__ __forceinline__ void contact_fail_at(const ContactDev& C, int* status, int detail,
+                                                unsigned long long code) {
+    const unsigned long long packed =
+        ((code >> 32) << 37) | ((code & 0xffffffffull) << 5) | static_cast<unsigned long long>(detail);
+    atomicMin(C.fail, packed);
+    contact_fail(status, detail);
+}
+
 __device__ __forceinline__ bool contact_failed(const int* status) {
     return (*reinterpret_cast<const volatile int*>(status) & kStatusContact) != 0;
 }
@@ -670,7 +684,7 @@ static __device__ __noinline__ void project_one(const ContactCtx& c, uint32_t i)
     ContactEntry& out = C.cand_entry[i];
     ContactEntry e = out;  // the warm start
     if (!Q.certified) {
-        contact_fail(c.status, kContactGeometry);
+        contact_fail_at(C, c.status, kContactGeometry, C.cand[i]);
         return;
     }
     D3 normal = d3_of(Q.normal);
@@ -701,7 +715,7 @@ static __device__ __noinline__ void project_one(const ContactCtx& c, uint32_t i)
     const double eff = Q.eff;
     if ((gap > margin && e.lambda == 0.0) || !(eff + alpha > 0.0)) {
         if (!(eff + alpha > 0.0) && gap < 0.0 && !(gap > margin && e.lambda == 0.0)) {
-            contact_fail(c.status, kContactNoResponse);
+            contact_fail_at(C, c.status, kContactNoResponse, C.cand[i]);
             return;
         }
         e.flags = carried_flags(e.flags);
@@ -712,7 +726,7 @@ static __device__ __noinline__ void project_one(const ContactCtx& c, uint32_t i)
     const double next = contact::dmax(0.0, e.lambda + delta);
     const double applied = next - e.lambda;
     if (!isfinite(next) || !isfinite(applied)) {
-        contact_fail(c.status, kContactProjection);
+        contact_fail_at(C, c.status, kContactProjection, C.cand[i]);
         return;
     }
     // impulse w (applied / dt) n on the first primitive, the opposite on the
@@ -734,7 +748,7 @@ static __device__ __noinline__ void project_one(const ContactCtx& c, uint32_t i)
     const D3 fp = point(A, fc, Q.fw), sp = point(B, sc, Q.sw);
     const double solved = contact::dot(fp - sp, normal) - C.separation;
     if (!contact::finite3(fp) || !contact::finite3(sp) || !isfinite(solved)) {
-        contact_fail(c.status, kContactSolved);
+        contact_fail_at(C, c.status, kContactSolved, C.cand[i]);
         return;
     }
     // a record continuing from the previous iteration keeps its impulse
@@ -766,7 +780,7 @@ __device__ __noinline__ void contact_project(const ContactCtx& c, cooperative_gr
     // in contact or not; warm-start entry; previous entries taken over
     for (uint32_t i = gt; i < count; i += stride) {
         const uint32_t s = C.query[i].ccd_state;
-        if (s == SWB_CCD_INDETERMINATE) contact_fail(c.status, kContactCcd);
+        if (s == SWB_CCD_INDETERMINATE) contact_fail_at(C, c.status, kContactCcd, C.cand[i]);
         const bool hit = impact_state(s);
         C.mark_a[i] = hit ? 1u : 0u;
         if (hit) {
@@ -854,7 +868,7 @@ __device__ __noinline__ void contact_certify_all(const ContactCtx& c, cooperativ
         const ContactQuery& Q = C.query[i];
         const unsigned long long code = C.cand[i];
         if (Q.ccd_state == SWB_CCD_INDETERMINATE) {
-            contact_fail(c.status, kContactFinalCcd);
+            contact_fail_at(C, c.status, kContactFinalCcd, code);
             continue;
         }
         const uint32_t k = lower_bound_code([&](uint32_t m) { return tab[m].code; }, tn, code);
@@ -862,7 +876,7 @@ __device__ __noinline__ void contact_certify_all(const ContactCtx& c, cooperativ
         const bool impact = Q.ccd_state != SWB_CCD_NO_IMPACT;
         if (!impact && !(e && (e->flags & kEntryRecord))) continue;
         if (!Q.certified) {
-            contact_fail(c.status, impact ? kContactFinalGeometry : kContactCleared);
+            contact_fail_at(C, c.status, impact ? kContactFinalGeometry : kContactCleared, code);
             continue;
         }
         D3 normal = d3_of(Q.normal);
@@ -871,12 +885,12 @@ __device__ __noinline__ void contact_certify_all(const ContactCtx& c, cooperativ
         const D3 fp = weighted_live(c, Q.addr, fc, Q.fw), sp = weighted_live(c, Q.addr + fc, sc, Q.sw);
         const double gap = contact::dot(fp - sp, normal) - C.separation;
         if (impact && (!contact::finite3(fp) || !contact::finite3(sp) || !contact::finite3(normal) || !isfinite(gap))) {
-            contact_fail(c.status, kContactFinalNonFinite);
+            contact_fail_at(C, c.status, kContactFinalNonFinite, code);
             continue;
         }
         const double pen = contact::dmax(0.0, -gap);
         if ((!impact && !isfinite(gap)) || pen > limit) {
-            contact_fail(c.status, impact ? kContactPenetration : kContactClearedGate);
+            contact_fail_at(C, c.status, impact ? kContactPenetration : kContactClearedGate, code);
             continue;
         }
         ContactRecordDev& r = C.cand_rec[i];
@@ -905,7 +919,7 @@ __device__ __noinline__ void contact_certify_all(const ContactCtx& c, cooperativ
     for (uint32_t k = gt; k < tn; k += stride) {
         if (!(tab[k].flags & kEntryRecord)) continue;
         const uint32_t i = lower_bound_code([&](uint32_t m) { return C.cand[m]; }, count, tab[k].code);
-        if (!(i < count && C.cand[i] == tab[k].code)) contact_fail(c.status, kContactLost);
+        if (!(i < count && C.cand[i] == tab[k].code)) contact_fail_at(C, c.status, kContactLost, tab[k].code);
     }
     cluster.sync();
     if (c.me == 0) {
@@ -943,7 +957,7 @@ static __device__ __noinline__ void friction_one(const ContactCtx& c, const Cont
                                                            C.static_mu, C.dynamic_mu, r.active != 0);
     if (!contact::finite3(fr.impulse) || !isfinite(fr.work) ||
         fr.work > 1.0e-12 * contact::dmax(1.0, contact::norm2(fr.initial_tangent))) {
-        contact_fail(c.status, kContactFriction);
+        contact_fail_at(C, c.status, kContactFriction, r.code);
         return;
     }
     if (fr.state == contact::kFrictionInactive) return;  // no impulse

@@ -80,4 +80,21 @@ ContactSurface build_contact_surface(const swb_structure_definition& d, double h
     return s;
 }
 
+swb_contact_key contact_key_of(const ContactSurface& S, uint64_t row, uint64_t col) {
+    swb_contact_key key{};
+    const size_t nv = S.vertices.size();
+    if (row < nv) {
+        key.kind = SWB_FEATURE_VERTEX_TRIANGLE;
+        key.first[0] = S.vertices[row];
+        key.second[0] = col;
+    } else {
+        key.kind = SWB_FEATURE_EDGE_EDGE;
+        key.first[0] = S.edges[row - nv][0];
+        key.first[1] = S.edges[row - nv][1];
+        key.second[0] = S.edges[col][0];
+        key.second[1] = S.edges[col][1];
+    }
+    return key;
+}
+
 }  // namespace swb

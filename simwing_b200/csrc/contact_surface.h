@@ -34,6 +34,11 @@ struct CandidateRows {
     std::vector<uint32_t> cols;
 };
 
+// The ContactFeatureKey (contact.h:95-101) of the candidate in `row`
+// against column `col`: vertex-triangle {vertex} x {triangle}, edge-edge
+// {a, b} x {c, d}.
+swb_contact_key contact_key_of(const ContactSurface& surface, uint64_t row, uint64_t col);
+
 CandidateRows contact_candidate_rows(const ContactSurface& surface, const double* prev, const double* cur,
                                      uint64_t node_count, double separation);
 

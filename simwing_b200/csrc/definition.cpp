@@ -12,7 +12,16 @@ namespace swb {
 
 thread_local std::string g_last_error;
 
-void set_last_error(const std::string& message) { g_last_error = message; }
+thread_local swb_error_detail g_last_detail{};
+
+void set_last_error(const std::string& message) {
+    g_last_error = message;
+    g_last_detail = swb_error_detail{};
+}
+
+void set_last_error_detail(const swb_error_detail* detail) {
+    g_last_detail = detail ? *detail : swb_error_detail{};
+}
 
 void OwnedDefinition::assign(const swb_structure_definition& s) {
     if ((s.node_count && !s.nodes) || (s.triangle_count && !s.triangles) ||
@@ -452,6 +461,12 @@ using namespace swb;
 extern "C" {
 
 const char* swb_last_error(void) { return swb::g_last_error.c_str(); }
+
+swb_status swb_last_error_detail(swb_error_detail* out) {
+    if (!out) return SWB_INVALID_ARGUMENT;
+    *out = swb::g_last_detail;
+    return SWB_OK;
+}
 
 uint32_t swb_abi_version(void) { return SWB_ABI_VERSION; }
 

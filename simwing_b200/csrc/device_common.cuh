@@ -9,7 +9,8 @@ namespace swb {
 namespace dev {
 
 // Status bits written by kernels (atomicOr into status[0]); status[1] holds
-// a detail code of the first suspension failure.
+// a detail code of the first suspension failure (low byte; the failing
+// segment + 1 above it, where the failure belongs to a segment).
 enum : int {
     kStatusSyncTimeout = 1,
     kStatusNonFinite = 2,
@@ -19,13 +20,18 @@ enum : int {
     kStatusContact = 32,   // status[1]: a kContact* detail code
 };
 
+// Suspension detail codes, each one (phase, entity) of the reference's
+// SuspensionError (suspension.cpp):
 enum : int {
-    kSuspLineGeometry = 1,
-    kSuspLineInput = 2,
-    kSuspEffectiveMass = 3,
-    kSuspPayload = 4,
-    kSuspResidual = 5,
-    kSuspOrientation = 6,
+    kSuspLineGeometry = 1,   // LineSolve, the segment (:2247-2252)
+    kSuspLineInput = 2,      // LineSolve, "line-projection" (:1141-1150)
+    kSuspEffectiveMass = 3,  // LineSolve, "effective-mass" (:1110-1120)
+    kSuspPayload = 4,        // Certification, "payload" (:2325-2333)
+    kSuspResidual = 5,       // Certification, "line-residual" (:2350-2358)
+    kSuspOrientation = 6,    // LineSolve, "payload": the pilot's pose is unusable
+    kSuspPredict = 7,        // Prediction, "payload-step" (:1080-1100)
+    kSuspCertifyLength = 8,  // Certification, the segment (:2339-2341)
+    kSuspFinish = 9,         // Certification, "payload": velocity reconstruction or line damping
 };
 
 __device__ __forceinline__ float3 f3(float4 v) { return make_float3(v.x, v.y, v.z); }

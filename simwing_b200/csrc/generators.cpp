@@ -211,13 +211,13 @@ void swb_default_wing_params(swb_wing_params* p) {
     p->cells = 40;
     p->chordwise = 60;
     p->spanwise_per_cell = 4;
-    p->rib_layers = 6;
+    p->rib_layers = 10;
     p->span = 11.0;
     p->root_chord = 2.6;
     p->thickness = 0.15;
     p->areal_density = 0.045;
     p->skin_compliance = 1.0e-7;
-    p->bend_rigidity = 1.0;
+    p->bend_rigidity = 1.0e-3;
     p->line_compliance_scale = 1.0;
     p->pressure = 30.0;
     p->line_levels = 4;
@@ -411,40 +411,64 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
             // Ribs with their own nodes, sewn to the skin.  The last rib
             // column is one station before the trailing edge (the section is
             // thinnest there); the rib fans from it to the trailing-edge node,
-            // and the skin station between them is not sewn.
+            // and the skin station between them is not sewn.  Each column is
+            // split through the thickness into as many layers as keep its
+            // elements about as tall as the chordwise station spacing (at
+            // most rib_layers, at least one), and neighbouring columns are
+            // joined by a strip that advances along the shorter diagonal, so
+            // no rib element is a sliver where the section thins towards the
+            // trailing edge.  The two end ribs close the end cells and carry
+            // the outward pressure jump; the inner ribs separate pressurised
+            // cells and carry none.
             const uint32_t L = p->rib_layers;
             const uint32_t J = C - 1;  // rib columns 1 .. J-1, fan from J-1 to the trailing edge
             const double seam_ea = 1.0e5;
             for (uint32_t r = 0; r <= p->cells; ++r) {
                 const uint32_t s = r * p->spanwise_per_cell;
                 const Station st = station(s);
-                std::vector<uint64_t> col((C + 1) * (L + 1), 0);
+                std::vector<std::vector<uint64_t>> col(C + 1);
                 const uint64_t le = b.node(surface_point(st, 0.0, 1.0));
                 const uint64_t te = b.node(surface_point(st, 1.0, 1.0));
                 for (uint32_t j = 1; j < J; ++j) {
                     const V lo = surface_point(st, xi[j], -1.0);
                     const V hi = surface_point(st, xi[j], 1.0);
-                    for (uint32_t l = 0; l <= L; ++l)
-                        col[j * (L + 1) + l] = b.node(lo + (hi - lo) * (double(l) / L));
+                    const double spacing = 0.5 * (xi[j + 1] - xi[j - 1]) * st.chord;
+                    const double want = std::round(length(hi - lo) / spacing);
+                    const uint32_t layers =
+                        static_cast<uint32_t>(std::clamp(want, 1.0, static_cast<double>(L)));
+                    for (uint32_t l = 0; l <= layers; ++l)
+                        col[j].push_back(b.node(lo + (hi - lo) * (double(l) / layers)));
                 }
-                // Ribs separate pressurised cells and carry no pressure jump.
-                const double rib_pressure = 0.0;
+                // End ribs: the normal of the fans and strips below points
+                // to -y (the r = 0 side); the far end rib takes the jump with
+                // the opposite sign so that both push outwards.
+                const double rib_pressure =
+                    r == 0 ? p->pressure : (r == p->cells ? -p->pressure : 0.0);
                 const size_t first = def->def.triangles.size();
-                for (uint32_t l = 0; l < L; ++l)
-                    b.triangle(le, col[1 * (L + 1) + l], col[1 * (L + 1) + l + 1], rib_pressure,
-                               p->areal_density);
-                for (uint32_t j = 1; j + 1 < J; ++j)
-                    for (uint32_t l = 0; l < L; ++l) {
-                        const uint64_t a = col[j * (L + 1) + l];
-                        const uint64_t bb = col[(j + 1) * (L + 1) + l];
-                        const uint64_t c = col[(j + 1) * (L + 1) + l + 1];
-                        const uint64_t dd = col[j * (L + 1) + l + 1];
-                        b.triangle(a, bb, c, rib_pressure, p->areal_density);
-                        b.triangle(a, c, dd, rib_pressure, p->areal_density);
+                for (size_t l = 0; l + 1 < col[1].size(); ++l)
+                    b.triangle(le, col[1][l], col[1][l + 1], rib_pressure, p->areal_density);
+                for (uint32_t j = 1; j + 1 < J; ++j) {
+                    const std::vector<uint64_t>& u = col[j];
+                    const std::vector<uint64_t>& w = col[j + 1];
+                    size_t a = 0, c = 0;
+                    while (a + 1 < u.size() || c + 1 < w.size()) {
+                        bool advance_u;
+                        if (a + 1 == u.size()) advance_u = false;
+                        else if (c + 1 == w.size()) advance_u = true;
+                        else
+                            advance_u = length(b.design[u[a + 1]] - b.design[w[c]]) <=
+                                        length(b.design[u[a]] - b.design[w[c + 1]]);
+                        if (advance_u) {
+                            b.triangle(u[a], w[c], u[a + 1], rib_pressure, p->areal_density);
+                            ++a;
+                        } else {
+                            b.triangle(u[a], w[c], w[c + 1], rib_pressure, p->areal_density);
+                            ++c;
+                        }
                     }
-                for (uint32_t l = 0; l < L; ++l)
-                    b.triangle(col[(J - 1) * (L + 1) + l], te, col[(J - 1) * (L + 1) + l + 1],
-                               rib_pressure, p->areal_density);
+                }
+                for (size_t l = 0; l + 1 < col[J - 1].size(); ++l)
+                    b.triangle(col[J - 1][l], te, col[J - 1][l + 1], rib_pressure, p->areal_density);
                 const size_t last = def->def.triangles.size();
                 if (p->fabric == 1)
                     b.membranes(first, last, chordwise, fabric);
@@ -460,8 +484,8 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                     skin_loop.push_back(skin[s * loop + k]);
                     if (k == 0) rib_loop.push_back(te);
                     else if (k == C) rib_loop.push_back(le);
-                    else if (k < C) rib_loop.push_back(col[(C - k) * (L + 1) + 0]);
-                    else rib_loop.push_back(col[(k - C) * (L + 1) + L]);
+                    else if (k < C) rib_loop.push_back(col[C - k].front());
+                    else rib_loop.push_back(col[k - C].back());
                 }
                 const size_t seam = rib_loop.size();
                 for (size_t k = 0; k < seam; ++k)

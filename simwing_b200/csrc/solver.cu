@@ -48,6 +48,32 @@ uint32_t align16(uint32_t v) { return (v + 15u) & ~15u; }
 // (suspension.cpp:1000-1006), i.e. by the decimal spelling of the id.
 bool id_string_less(uint64_t a, uint64_t b) { return std::to_string(a) < std::to_string(b); }
 
+// The fabric self-contact multiplier table is part of the step transaction,
+// as the reference's contactMultipliers_ / contactRecords_ are
+// (soft_body.cpp:1090-1112): the step's contact iterations ping-pong the
+// table, so the committed table is copied aside before a step and put back
+// when the step fails.  Both kernels read the entry count on the device.
+__global__ void contact_table_save(const ContactDev* c, ContactEntry* out, uint32_t* meta_out) {
+    const uint32_t sel = c->table_meta[0], n = c->table_meta[1];
+    const ContactEntry* src = c->table[sel];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = src[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        meta_out[0] = 0u;
+        meta_out[1] = n;
+        *c->fail = ~0ull;  // no failing feature yet
+    }
+}
+
+__global__ void contact_table_restore(const ContactDev* c, const ContactEntry* in, const uint32_t* meta_in) {
+    const uint32_t n = meta_in[1];
+    ContactEntry* dst = c->table[0];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = in[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        c->table_meta[0] = 0u;
+        c->table_meta[1] = n;
+    }
+}
+
 // Diagnostics partial sums per CTA (double).
 constexpr int kDiagFields = 16;
 
@@ -411,8 +437,16 @@ void StructureImpl::setup_contact() {
     c.cand_entry = dalloc<ContactEntry>(owned, cap);
     c.cand_rec = dalloc<ContactRecordDev>(owned, cap);
     c.reduce = dalloc<unsigned long long>(owned, 2);
+    // a failing feature is packed as row << 37 | col << 5 | detail
+    if (static_cast<uint64_t>(c.nv) + c.ne >= (uint64_t(1) << 27))
+        raise(SWB_UNSUPPORTED, "fabric self-contact surface too large for the device feature codes");
+    c.fail = dalloc<unsigned long long>(owned, 1);
+    cuda_check(cudaMemsetAsync(c.fail, 0xff, sizeof(unsigned long long), stream), "memset");
     d_contact = dupload(owned, std::vector<ContactDev>{c}, stream);
     contact_host = c;
+    d_table_commit = dalloc<ContactEntry>(owned, cap);
+    d_meta_commit = dalloc<uint32_t>(owned, 2);
+    cuda_check(cudaMemsetAsync(d_meta_commit, 0, 2 * sizeof(uint32_t), stream), "memset");
     for (int b = 0; b < 3; ++b) {
         d_cdiag[b] = dalloc<ContactDiagDev>(owned, 1);
         cuda_check(cudaMemsetAsync(d_cdiag[b], 0, sizeof(ContactDiagDev), stream), "memset");
@@ -1000,8 +1034,11 @@ swb_status decode_status(const int status[2], std::string& message) {
         static const char* what[] = {"suspension failure", "line geometry is non-finite or scale-degenerate",
                                      "invalid unilateral line projection input", "zero generalized effective mass",
                                      "payload trial state is non-finite or unnormalized",
-                                     "maximum line residual exceeds configured bound", "invalid payload orientation"};
-        message = std::string("SuspensionError: ") + what[std::clamp(status[1], 0, 6)];
+                                     "maximum line residual exceeds configured bound", "invalid payload orientation",
+                                     "payload integration produced non-finite state",
+                                     "line trial length is non-finite",
+                                     "payload velocity reconstruction or line damping failed"};
+        message = std::string("SuspensionError: ") + what[std::clamp(status[1] & 0xff, 0, 9)];
         return SWB_SUSPENSION_ERROR;
     }
     message = "trial step produced a non-finite state";
@@ -1012,7 +1049,46 @@ swb_status StructureImpl::read_status(std::string& message) {
     Control c{};
     cuda_check(cudaMemcpyAsync(&c, d_control, sizeof(Control), cudaMemcpyDeviceToHost, stream), "status");
     cuda_check(cudaStreamSynchronize(stream), "step");
+    last_status[0] = c.status[0];
+    last_status[1] = c.status[1];
     return decode_status(c.status, message);
+}
+
+// The reference's exception details for a failed step: the phase and entity
+// of a SuspensionError (suspension.cpp fail sites, one per device detail
+// code) and the feature key of a ContactStepError.  The contact message is
+// that of the failing feature first in key order.
+swb_error_detail StructureImpl::failure_detail(swb_status status, std::string& message) {
+    swb_error_detail d{};
+    d.status = static_cast<uint32_t>(status);
+    if (status == SWB_SUSPENSION_ERROR) {
+        struct Site { uint32_t phase; const char* entity; };
+        static const Site sites[] = {
+            {SWB_PHASE_CERTIFICATION, "unknown"},          {SWB_PHASE_LINE_SOLVE, nullptr},
+            {SWB_PHASE_LINE_SOLVE, "line-projection"},     {SWB_PHASE_LINE_SOLVE, "effective-mass"},
+            {SWB_PHASE_CERTIFICATION, "payload"},          {SWB_PHASE_CERTIFICATION, "line-residual"},
+            {SWB_PHASE_LINE_SOLVE, "payload"},             {SWB_PHASE_PREDICTION, "payload-step"},
+            {SWB_PHASE_CERTIFICATION, nullptr},            {SWB_PHASE_CERTIFICATION, "payload"}};
+        const int code = std::clamp(last_status[1] & 0xff, 0, 9);
+        const int segment = (last_status[1] >> 8) - 1;
+        d.suspension_phase = sites[code].phase;
+        std::string entity = sites[code].entity ? sites[code].entity : "segment";
+        if (!sites[code].entity && segment >= 0 && static_cast<size_t>(segment) < segment_order.size())
+            entity = "segment:" + std::to_string(def.segments[segment_order[segment]].stable_id);
+        std::snprintf(d.suspension_entity, sizeof d.suspension_entity, "%s", entity.c_str());
+    } else if (status == SWB_CONTACT_ERROR && d_contact) {
+        unsigned long long packed = ~0ull;
+        cuda_check(cudaMemcpy(&packed, contact_host.fail, sizeof packed, cudaMemcpyDeviceToHost), "read");
+        if (packed != ~0ull) {
+            const uint64_t row = packed >> 37, col = (packed >> 5) & 0xffffffffull;
+            const int detail = static_cast<int>(packed & 31u);
+            d.has_contact_key = 1;
+            d.contact_key = contact_key_of(contact_surface, row, col);
+            const int raw[2] = {dev::kStatusContact, detail};
+            decode_status(raw, message);
+        }
+    }
+    return d;
 }
 
 void StructureImpl::commit(int new_cur, int steps, const swb_step_settings& st) {
@@ -1047,6 +1123,10 @@ swb_status StructureImpl::step(const swb_step_settings& st, int steps, swb_diagn
         backup = 3 - a - b;
         copy_state(a, backup);
     }
+    if (d_contact) {
+        contact_table_save<<<kDiagBlocks, 256, 0, stream>>>(d_contact, d_table_commit, d_meta_commit);
+        cuda_check(cudaGetLastError(), "contact_table_save");
+    }
     cuda_check(cudaEventRecord(ev0, stream), "event");
     for (int k = 0; k < total; ++k) {
         launch_substep(st, a, b);
@@ -1059,11 +1139,17 @@ swb_status StructureImpl::step(const swb_step_settings& st, int steps, swb_diagn
     cudaEventElapsedTime(&ms, ev0, ev1);
     last_ms = ms;
     if (status != SWB_OK) {
-        if (backup >= 0) {
-            copy_state(backup, start);
-            cuda_check(cudaStreamSynchronize(stream), "restore");
+        if (backup >= 0) copy_state(backup, start);
+        if (d_contact) {
+            contact_table_restore<<<kDiagBlocks, 256, 0, stream>>>(d_contact, d_table_commit, d_meta_commit);
+            cuda_check(cudaGetLastError(), "contact_table_restore");
         }
+        if (backup >= 0 || d_contact) cuda_check(cudaStreamSynchronize(stream), "restore");
         cur = start;
+        if (status == SWB_SUSPENSION_ERROR || status == SWB_CONTACT_ERROR) {
+            const swb_error_detail detail = failure_detail(status, message);
+            throw Error(status, message, detail);
+        }
         raise(status, message);
     }
     commit(a, steps, st);
@@ -1460,24 +1546,8 @@ swb_status swb_structure_contact_candidates(const swb_structure* s, swb_contact_
         if (!codes.empty())
             cuda_check(cudaMemcpy(codes.data(), m.contact_host.cand, codes.size() * sizeof(unsigned long long),
                                   cudaMemcpyDeviceToHost), "read");
-        const ContactSurface& S = m.contact_surface;
-        const size_t nv = S.vertices.size();
-        for (size_t k = 0; k < codes.size(); ++k) {
-            const uint64_t row = codes[k] >> 32, col = codes[k] & 0xffffffffull;
-            swb_contact_key& key = keys[k];
-            std::memset(&key, 0, sizeof key);
-            if (row < nv) {
-                key.kind = SWB_FEATURE_VERTEX_TRIANGLE;
-                key.first[0] = S.vertices[row];
-                key.second[0] = col;
-            } else {
-                key.kind = SWB_FEATURE_EDGE_EDGE;
-                key.first[0] = S.edges[row - nv][0];
-                key.first[1] = S.edges[row - nv][1];
-                key.second[0] = S.edges[col][0];
-                key.second[1] = S.edges[col][1];
-            }
-        }
+        for (size_t k = 0; k < codes.size(); ++k)
+            keys[k] = contact_key_of(m.contact_surface, codes[k] >> 32, codes[k] & 0xffffffffull);
     });
 }
 

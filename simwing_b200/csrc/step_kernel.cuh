@@ -268,7 +268,7 @@ __device__ __noinline__ void line_iteration(const DevPayloadDef& d, DevPayloadSt
     M3 R, I, invI;
     if (!q_rotation(s.q, R)) { susp_fail(status, kSuspOrientation); return; }
     I = world_inertia(R, d.inertia);
-    if (!m3_inverse(I, invI)) { susp_fail(status, kSuspPayload); return; }
+    if (!m3_inverse(I, invI)) { susp_fail(status, kSuspEffectiveMass); return; }
     const float wp = 1.0f / d.mass;
     for (int k = 0; k < d.segments; ++k) {
         float3 p[2], off[2];
@@ -294,7 +294,7 @@ __device__ __noinline__ void line_iteration(const DevPayloadDef& d, DevPayloadSt
         }
         const float3 diff = p[1] - p[0];
         const float l = length(diff);
-        if (!isfinite(l) || l <= d.min_length) { susp_fail(status, kSuspLineGeometry); return; }
+        if (!isfinite(l) || l <= d.min_length) { susp_fail(status, kSuspLineGeometry | ((k + 1) << 8)); return; }
         const float3 dir = diff * fast_rcp(l);
         const float lam = s.lambda[k];
         // projectUnilateralLine (suspension.cpp:1125-1163).  The unit-gradient
@@ -369,7 +369,7 @@ __device__ bool payload_reconstruct_damp(const DevPayloadDef& d, DevPayloadState
     s.v = (s.com - start.com) / dt;
     float4 delta;
     const float4 conj = make_float4(start.q.x, -start.q.y, -start.q.z, -start.q.w);
-    if (!q_canon(q_mul(s.q, conj), delta)) { susp_fail(status, kSuspOrientation); return false; }
+    if (!q_canon(q_mul(s.q, conj), delta)) { susp_fail(status, kSuspFinish); return false; }
     const float sn = sqrtf(delta.y * delta.y + delta.z * delta.z + delta.w * delta.w);
     const float half = atan2f(sn, delta.x);
     if (sn < 1.0e-12f) {
@@ -378,9 +378,9 @@ __device__ bool payload_reconstruct_damp(const DevPayloadDef& d, DevPayloadState
         s.w = make_float3(delta.y, delta.z, delta.w) * (2.0f * half / (dt * sn));
     }
     M3 R, I, invI;
-    if (!q_rotation(s.q, R)) { susp_fail(status, kSuspOrientation); return false; }
+    if (!q_rotation(s.q, R)) { susp_fail(status, kSuspFinish); return false; }
     I = world_inertia(R, d.inertia);
-    if (!m3_inverse(I, invI)) { susp_fail(status, kSuspPayload); return false; }
+    if (!m3_inverse(I, invI)) { susp_fail(status, kSuspFinish); return false; }
     auto endpoint = [&](int node, int point, float3& pos, float3& vel) -> bool {
         return payload_endpoint(d, s, x, v, node, point, pos, vel);
     };
@@ -389,7 +389,7 @@ __device__ bool payload_reconstruct_damp(const DevPayloadDef& d, DevPayloadState
         if (!(s.lambda[k] > 0.0f) || !(d.damping[k] > 0.0f)) continue;
         float3 from, to, vf, vt;
         if (!endpoint(d.from_node[k], d.from_point[k], from, vf) || !endpoint(d.to_node[k], d.to_point[k], to, vt)) {
-            susp_fail(status, kSuspOrientation);
+            susp_fail(status, kSuspFinish);
             return false;
         }
         const float3 df = to - from;
@@ -452,7 +452,7 @@ __device__ void payload_certify_finish(const DevPayloadDef& d, DevPayloadState& 
         endpoint(d.to_node[k], d.to_point[k], to, vt);
         const float3 df = to - from;
         const float l = length(df);
-        if (!isfinite(l)) { susp_fail(status, kSuspLineGeometry); return; }
+        if (!isfinite(l)) { susp_fail(status, kSuspCertifyLength | ((k + 1) << 8)); return; }
         const float stretch = fmaxf(0.0f, l - d.rest[k]);
         const float cs = s.lambda[k] / (d.stiffness[k] * dt * dt);
         maxres = fmaxf(maxres, fabsf(stretch - cs));
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(1024) xpbd_step_kernel(const __grid_constant__
     }
     if (owner && tid == 0) {
         for (int k = 0; k < 8; ++k) pay.lambda[k] = 0.0f;
-        if (!payload_predict(*p.payload_def, pay, p.dt, p.gravity)) susp_fail(p.status, kSuspPayload);
+        if (!payload_predict(*p.payload_def, pay, p.dt, p.gravity)) susp_fail(p.status, kSuspPredict);
     }
     __syncthreads();
 

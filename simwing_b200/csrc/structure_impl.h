@@ -91,6 +91,9 @@ struct StructureImpl {
     ContactDev contact_host{};  // host copy of *d_contact (device pointers)
     size_t smem_cap = 0;  // dynamic shared memory a step kernel may request on this device
     ContactDiagDev* d_cdiag[3] = {nullptr, nullptr, nullptr};
+    // the committed multiplier table while a step runs (restored on failure)
+    ContactEntry* d_table_commit = nullptr;
+    uint32_t* d_meta_commit = nullptr;
     uint4* d_diag_mem = nullptr;      // membrane records for the diagnostics: corner slots, record index
     uint32_t* d_diag_b = nullptr;
     float* d_diag_rest = nullptr;
@@ -128,6 +131,10 @@ struct StructureImpl {
     void upload_pressure();
     void upload_forces();
     void validate_settings(const swb_step_settings& st) const;
+    // the raw status words of the last step and the exception details of a
+    // failed one
+    int last_status[2] = {0, 0};
+    swb_error_detail failure_detail(swb_status status, std::string& message);
     void launch_substep(const swb_step_settings& st, int in, int out);
     swb_status read_status(std::string& message);
     // Accepts `steps` steps that left the state in buffer `new_cur`: the

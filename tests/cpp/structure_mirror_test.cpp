@@ -237,6 +237,46 @@ void gpu_checks() {
     const double qn = p.bodyToWorld.w * p.bodyToWorld.w + p.bodyToWorld.x * p.bodyToWorld.x +
                       p.bodyToWorld.y * p.bodyToWorld.y + p.bodyToWorld.z * p.bodyToWorld.z;
     expect(std::fabs(qn - 1.0) < 1e-5, "payload orientation stays a unit quaternion");
+
+    // typed step failures with the reference's details; the caller compares
+    // the printed details with what the reference build throws on the same
+    // definitions (tests/test_cpp_mirror.py)
+    StructureDefinition strict = small_wing_definition();
+    strict.suspension->maximumLineResidualMeters = 0.0;
+    Structure sw(strict);
+    bool caught = false;
+    try {
+        for (int i = 0; i < 20; ++i) (void)sw.step(settings());
+    } catch (const softwing::SuspensionError& e) {
+        caught = true;
+        std::printf("detail suspension %d %s\n", static_cast<int>(e.phase()), e.entity().c_str());
+    }
+    expect(caught, "a zero line residual bound throws SuspensionError");
+    StructureDefinition pinned;
+    const double z[2] = {0.0, 0.005};
+    for (int sheet = 0; sheet < 2; ++sheet) {
+        pinned.nodes.push_back({{-1.0, -1.0, z[sheet]}, 1.0, true});
+        pinned.nodes.push_back({{sheet ? 0.0 : 1.0, sheet ? 1.0 : -1.0, z[sheet]}, 1.0, true});
+        pinned.nodes.push_back({{sheet ? 1.0 : 0.0, sheet ? -1.0 : 1.0, z[sheet]}, 1.0, true});
+    }
+    pinned.nodes.push_back({{3.0, 3.0, 3.0}, 1.0, false});
+    pinned.triangles.push_back({{0, 1, 2}});
+    pinned.triangles.push_back({{3, 4, 5}});
+    pinned.fabricSelfContact = StructureFabricContactDefinition{0.01, 0.0, 0.0, 0.0};
+    Structure sc(pinned);
+    StructureStepSettings four = settings();
+    four.constraintIterations = 4;
+    caught = false;
+    try {
+        (void)sc.step(four);
+    } catch (const softwing::ContactStepError& e) {
+        caught = true;
+        const softwing::ContactFeatureKey& k = e.key();
+        std::printf("detail contact %zu %d %zu %zu %zu %zu %zu %zu\n", k.pair, static_cast<int>(k.kind),
+                    k.firstPrimitive[0], k.firstPrimitive[1], k.firstPrimitive[2], k.secondPrimitive[0],
+                    k.secondPrimitive[1], k.secondPrimitive[2]);
+    }
+    expect(caught, "unresolvable contact throws ContactStepError");
 }
 
 }  // namespace

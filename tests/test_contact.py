@@ -252,3 +252,28 @@ def test_device_swept_contact_equals_the_reference_bytewise(cuda_device, kind, s
         states = {r.state for r in ref}
         assert {abi.CCD_NO_IMPACT, abi.CCD_IMPACT, abi.CCD_INITIALLY_PROXIMATE} <= states
         assert any(r.used_interval_fallback for r in ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", [abi.FEATURE_VERTEX_TRIANGLE, abi.FEATURE_EDGE_EDGE])
+def test_swept_contact_with_a_tolerance_below_double_spacing_returns(cuda_device, kind):
+    """A time tolerance finer than the spacing of doubles near the impact
+    time: the bisection of sweptContact (contact.cpp:778-804) reaches an
+    interval whose midpoint rounds onto one of its ends, where the
+    reference's loop would never end.  The device stops there with the
+    interval refined to double resolution; the states are those of a
+    tolerance the reference handles."""
+    rng = np.random.default_rng(31 + kind)
+    parts = [random_motions(rng, 400, kind, s) for s in (0.05, 0.3)]
+    fp, fc, sp, sc = (np.concatenate([p[i] for p in parts]) for i in range(4))
+    fine = sw.contact_sweep(kind, fp, fc, sp, sc, 0.05, sw.CcdSettings(time_tolerance=1e-300))
+    coarse = sw.contact_sweep(kind, fp, fc, sp, sc, 0.05, sw.CcdSettings(time_tolerance=1e-12))
+    impacts = 0
+    for a, b in zip(fine, coarse):
+        assert a.state == b.state
+        if a.state == abi.CCD_IMPACT:
+            impacts += 1
+            assert a.bracket_lower <= a.time_of_impact <= a.bracket_upper
+            assert a.bracket_upper - a.bracket_lower <= 1e-12
+            assert abs(a.time_of_impact - b.time_of_impact) <= 2e-12
+    assert impacts > 0

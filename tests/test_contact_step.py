@@ -72,8 +72,9 @@ def test_contact_steps_match_the_reference(cuda_device, name, ctas):
             with pytest.raises(O.OracleError) as err:
                 ref.step(st)
             assert err.value.status == sw.abi.CONTACT_ERROR
-            with pytest.raises(sw.ContactStepError):
+            with pytest.raises(sw.ContactStepError) as dev_err:
                 dev.step(st)
+            assert dev_err.value.key == err.value.key
             np.testing.assert_array_equal(dev.node_states(), before)
             break
         da = dev.step(st)
@@ -105,11 +106,14 @@ def test_unresolvable_contact_fails_the_step_and_rolls_back(cuda_device):
     dev = sw.Structure(d)
     ref = O.RefStructure(dev.oracle_definition())
     before = dev.node_states().copy()
-    with pytest.raises(sw.ContactStepError):
+    with pytest.raises(sw.ContactStepError) as dev_err:
         dev.step(st)
     with pytest.raises(O.OracleError) as err:
         ref.step(st)
     assert err.value.status == sw.abi.CONTACT_ERROR
+    # ContactStepError::key(): the feature the reference's key-ordered
+    # projection throws at
+    assert dev_err.value.key == err.value.key
     np.testing.assert_array_equal(dev.node_states(), before)
     assert dev.accepted_step_count() == 0
 
@@ -202,3 +206,51 @@ def test_candidate_inspection_needs_contact(cuda_device):
     s = sw.Structure(sw.generate_patch(nx=8, ny=8))
     with pytest.raises(sw.Unsupported):
         s.contact_candidates()
+
+
+def test_contact_checkpoint_replay_is_bitwise(cuda_device):
+    """The checkpoint image carries the contact multiplier table (the warm
+    starts and the record book that carry over between steps, as
+    SoftBodyCheckpoint::State holds contactMultipliers and contactRecords)
+    and the contact diagnostics: replay after a restore is bit for bit."""
+    d = stacked_sheets(compliance=1e-3)
+    s = sw.Structure(d)
+    s.step(SLIDE)
+    image = s.checkpoint()
+    first = [s.step(SLIDE) for _ in range(2)]
+    states = s.node_states()
+    s.restore(image)
+    assert s.checkpoint() == image
+    again = [s.step(SLIDE) for _ in range(2)]
+    np.testing.assert_array_equal(s.node_states(), states)
+    for a, b in zip(first, again):
+        assert a.active_contact_count == b.active_contact_count > 0
+        assert a.maximum_contact_penetration == b.maximum_contact_penetration
+    # a tampered table entry is refused, the state untouched
+    bad = bytearray(image)
+    bad[-120] ^= 0x40
+    with pytest.raises(sw.InvalidArgument):
+        s.restore(bytes(bad))
+    np.testing.assert_array_equal(s.node_states(), states)
+
+
+@pytest.mark.parametrize("failure", ["contact", "non_finite"])
+def test_failed_contact_step_restores_the_multiplier_table(cuda_device, failure):
+    """A failed step rolls the contact multiplier table back with the nodes
+    (soft_body.cpp:1090-1112): afterwards the structure is byte for byte the
+    one that never tried the step."""
+    d = stacked_sheets(compliance=1e-3)
+    tried, twin = sw.Structure(d), sw.Structure(d)
+    steps = 3 if failure == "contact" else 2
+    for _ in range(steps):
+        tried.step(SLIDE)
+        twin.step(SLIDE)
+    if failure == "non_finite":
+        for s in (tried, twin):
+            s.add_external_force(3, (3.0e38, 3.0e38, 3.0e38))
+    before = tried.checkpoint()
+    # the compliant stacked sheets' fourth step fails in the swept query, as
+    # the reference's does (see CASES)
+    with pytest.raises(sw.ContactStepError if failure == "contact" else sw.NonFiniteState):
+        tried.step(SLIDE)
+    assert tried.checkpoint() == before == twin.checkpoint()

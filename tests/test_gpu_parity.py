@@ -260,10 +260,19 @@ def test_suspension_certification_failure_rolls_back(cuda_device):
     s = sw.Structure(d)
     before = s.node_states()
     # a zero residual bound fails certification once the risers load
-    with pytest.raises(sw.SuspensionError):
+    with pytest.raises(sw.SuspensionError) as err:
         for _ in range(20):
             s.step(step_settings())
     assert s.accepted_step_count() < 20
+    # SuspensionError::phase() / entity() as the reference's certifySubstep
+    # raises them (suspension.cpp:2350-2358)
+    assert (err.value.phase, err.value.entity) == ("Certification", "line-residual")
+    if O.ref_available():
+        ref = O.RefStructure(d)
+        with pytest.raises(O.OracleError) as ref_err:
+            for _ in range(20):
+                ref.step(step_settings())
+        assert (ref_err.value.phase, ref_err.value.entity) == (err.value.phase, err.value.entity)
 
 
 def test_barrier_timeout_reports_and_restores(cuda_device):

@@ -195,3 +195,13 @@ def test_full_wing_schedule_invariants():
     total = d.view.constraint_count + d.view.dihedral_count
     assert sum(r.level_constraints) + r.global_constraints == total
     assert r.max_patch_nodes < 65536
+
+
+def test_bench_workload_counts_match_the_generator():
+    """The bench line names the wing by its counts; they must be the
+    generator's."""
+    import bench
+
+    c = sw.generate_wing().counts()
+    text = bench.wing_config()["workload"]
+    assert f"{c['triangles']:,} tri" in text and f"{c['nodes']:,} nodes" in text
