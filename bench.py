@@ -284,7 +284,8 @@ def batched_leg(sw, st, count, rank, world, dist, device):
 
 def adjoint_leg(sw, st, device, steps=240, interval=16):
     """Adjoint calibration workload: the wing generator at 20 cells x 30
-    chordwise, settled for 60 steps; the target is the shape after `steps`
+    chordwise with two line attachments per cell and row (13,338 triangles,
+    266 line rest lengths), settled for 60 steps; the target is the shape after `steps`
     (240) steps with every line's rest length scaled by lognormal(0, 0.02);
     the loss is the mean squared distance of the fabric (triangle) nodes to
     it; one gradient = a forward of `steps` steps with a checkpoint every
@@ -293,7 +294,7 @@ def adjoint_leg(sw, st, device, steps=240, interval=16):
     repetitions of `steps` forward, `steps` taping and `steps` reverse."""
     import numpy as np
 
-    d = sw.generate_wing(cells=20, chordwise=30)
+    d = sw.generate_calibration_wing()
     opts = sw.SolverOptions(device=device)
     s = sw.Structure(d, opts)
     for _ in range(60):
@@ -325,7 +326,7 @@ def adjoint_leg(sw, st, device, steps=240, interval=16):
     cons = d.constraints()
     line_grad = [float(np.sum(g["d_rest"][x] * cons["rest_length"][x]) / np.sum(cons["rest_length"][x])) for x in lines]
     counts = d.counts()
-    out = {"workload": f"wing 20 cells x 30 chordwise, settled 60 steps; {steps}-step rollout, checkpoint every "
+    out = {"workload": f"wing 20 cells x 30 chordwise, 2 line attachments per cell, settled 60 steps; {steps}-step rollout, checkpoint every "
                        f"{interval} steps; "
                        "target from line rest lengths x lognormal(0, 0.02); loss = mean squared distance of the "
                        "fabric nodes",

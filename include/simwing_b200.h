@@ -708,7 +708,9 @@ typedef struct swb_wing_params {
                                  fabric edge constraints, as the reference's
                                  scene assembly builds the canopy
                                  (scene_structure.cpp:1125-1151)           */
-    uint32_t reserved;
+    uint32_t attachments_per_cell; /* line attachment stations per cell on
+                                 each row (0 or 1 = one per rib; must
+                                 divide spanwise_per_cell)                 */
 } swb_wing_params;
 
 void swb_default_patch_params(swb_patch_params* out);
@@ -987,6 +989,35 @@ swb_status swb_cell_volumes(const swb_structure_definition* definition,
                             const double* positions,
                             swb_cell_volume* out);
 
+/* Device-resident form for a step loop: the cells' topology is computed and
+ * uploaded once, at plan creation (the only allocations); each evaluation
+ * then launches one kernel on the caller's stream, allocates nothing and
+ * does not synchronise.  The plan lives on `device`. */
+typedef struct swb_cell_volume_plan swb_cell_volume_plan;
+swb_status swb_cell_volume_plan_create(const swb_structure_definition* definition,
+                                       const uint64_t* face_indices,
+                                       const uint64_t* loop_nodes,
+                                       const swb_cell_def* cells,
+                                       uint64_t cell_count,
+                                       int device,
+                                       swb_cell_volume_plan** out);
+void swb_cell_volume_plan_destroy(swb_cell_volume_plan* plan);
+/* `positions` (node_count x 3 doubles) and `out` (cell_count entries) in
+ * DEVICE memory; `stream` a cudaStream_t (NULL: the legacy stream). */
+swb_status swb_cell_volumes_device(const swb_cell_volume_plan* plan,
+                                   const double* positions,
+                                   swb_cell_volume* out,
+                                   void* stream);
+
+/* The same at a structure's committed state, read where it lives (its FP32
+ * offsets from the FP64 frame origin, widened to FP64 world positions):
+ * `out` in DEVICE memory, on the structure's stream, no host copy.  The
+ * plan must come from the structure's definition and device; its first use
+ * with a structure uploads that structure's node order once. */
+swb_status swb_structure_cell_volumes(const swb_structure* structure,
+                                      swb_cell_volume_plan* plan,
+                                      swb_cell_volume* out);
+
 /* ---- Pneumatic port mass flows --------------------------------------- */
 /* evaluateOrificeMassFlow / evaluateConductanceMassFlow (pneumatics.cpp:   */
 /* 132-232, pneumatics.h:46-92): the flow laws that move air between the    */
@@ -1039,6 +1070,21 @@ swb_status swb_port_mass_flows(const swb_air_properties* air,
                                uint64_t port_count,
                                swb_mass_flow* out,
                                uint64_t* failed_port);
+
+/* The same on DEVICE arrays (zones, ports, out and the one-word
+ * `failed_port`), for a network advanced on the device: two kernels on
+ * `stream` (a cudaStream_t; NULL: the legacy stream), no allocation, no
+ * synchronisation.  Every refusal -- a zone index past zone_count included
+ * -- is reported through *failed_port (the first refused port, or
+ * port_count when none), which the caller reads when it needs it. */
+swb_status swb_port_mass_flows_device(const swb_air_properties* air,
+                                      const swb_flow_zone_state* zones,
+                                      uint64_t zone_count,
+                                      const swb_port_def* ports,
+                                      uint64_t port_count,
+                                      swb_mass_flow* out,
+                                      uint64_t* failed_port,
+                                      void* stream);
 
 /* The candidate features of the last step's contact certification
  * (contact.cpp:1583-1798: the final broadphase, in key order), for

@@ -379,6 +379,17 @@ def generate_wing(**overrides) -> Definition:
     return Definition(out.value)
 
 
+# The adjoint calibration wing: 20 cells x 30 chordwise (13,338 triangles)
+# with two line attachment stations per cell and row (266 line rest
+# lengths).
+CALIBRATION_WING = dict(cells=20, chordwise=30, attachments_per_cell=2)
+
+
+def generate_calibration_wing(**overrides) -> Definition:
+    """The adjoint calibration wing (CALIBRATION_WING)."""
+    return generate_wing(**dict(CALIBRATION_WING, **overrides))
+
+
 def wing_batch_parameters(count: int = 64, seed: int = 2024):
     """Seeded uneven wing sizes of the batched workload: cells ~ U{20..60},
     chordwise in {30, 45, 60}, aspect ratio ~ U(4.5, 7), per-wing compliance

@@ -243,7 +243,7 @@ class WingParams(C.Structure):
                 ("line_levels", C.c_uint32), ("line_particles", C.c_uint32), ("line_rows", C.c_uint32),
                 ("pilot", C.c_uint32), ("pilot_mass", C.c_double), ("aspect_ratio", C.c_double),
                 ("compliance_jitter", C.c_double), ("seed", C.c_uint64), ("fabric", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("attachments_per_cell", C.c_uint32)]
 
 
 # status codes
@@ -333,6 +333,13 @@ _PROTOTYPES = {
                                          C.c_uint64, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
     "swb_port_mass_flows": (C.c_int, [P(AirProperties), C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p,
                                       P(C.c_uint64)]),
+    "swb_port_mass_flows_device": (C.c_int, [P(AirProperties), C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]),
+    "swb_cell_volume_plan_create": (C.c_int, [P(StructureDefinition), C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                              C.c_int, P(C.c_void_p)]),
+    "swb_cell_volume_plan_destroy": (None, [C.c_void_p]),
+    "swb_cell_volumes_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "swb_structure_cell_volumes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "swb_contact_closest": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_double, P(ClosestResult)]),
     "swb_contact_sweep": (C.c_int, [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_double, P(CcdSettings), P(CcdResult)]),

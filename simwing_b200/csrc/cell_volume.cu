@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <memory>
 #include <set>
 #include <vector>
 
@@ -268,6 +269,100 @@ struct DeviceBuffer {
 }  // namespace
 }  // namespace swb
 
+namespace swb {
+namespace {
+
+// The position-independent tables of a set of cells, ready for upload: the
+// per-cell topology, the triangles' node triples, the face and loop index
+// lists (indices clamped into range: out-of-range ones only reach the
+// device in faces or loops the topology rejects).
+struct CellTables {
+    std::vector<CellTopology> topo;
+    std::vector<uint3> tri;
+    std::vector<uint32_t> faces, loops;
+};
+
+CellTables cell_tables(const swb_structure_definition* definition, const uint64_t* face_indices,
+                       const uint64_t* loop_nodes, const swb_cell_def* cells, uint64_t cell_count) {
+    if (definition->node_count > 0xffffffffu || definition->triangle_count > 0xffffffffu)
+        raise(SWB_INVALID_ARGUMENT, "definition too large for 32-bit indices");
+    uint64_t faces_total = 0, loops_total = 0;
+    for (uint64_t k = 0; k < cell_count; ++k) {
+        faces_total = std::max(faces_total, cells[k].face_begin + cells[k].face_count);
+        loops_total = std::max({loops_total, cells[k].low_begin + cells[k].low_count,
+                                cells[k].high_begin + cells[k].high_count});
+    }
+    if ((faces_total && !face_indices) || (loops_total && !loop_nodes)) raise(SWB_INVALID_ARGUMENT, "null argument");
+    if (faces_total > 0xffffffffu || loops_total > 0xffffffffu)
+        raise(SWB_INVALID_ARGUMENT, "cell tables too large for 32-bit indices");
+    CellTables t;
+    t.topo.resize(cell_count);
+    for (uint64_t k = 0; k < cell_count; ++k) t.topo[k] = cell_topology(*definition, face_indices, loop_nodes, cells[k]);
+    t.tri.resize(definition->triangle_count);
+    for (uint64_t i = 0; i < t.tri.size(); ++i) {
+        const uint64_t* n = definition->triangles[i].nodes;
+        t.tri[i] = make_uint3(static_cast<uint32_t>(std::min<uint64_t>(n[0], definition->node_count - 1)),
+                              static_cast<uint32_t>(std::min<uint64_t>(n[1], definition->node_count - 1)),
+                              static_cast<uint32_t>(std::min<uint64_t>(n[2], definition->node_count - 1)));
+    }
+    t.faces.resize(faces_total);
+    t.loops.resize(loops_total);
+    for (uint64_t i = 0; i < faces_total; ++i)
+        t.faces[i] = static_cast<uint32_t>(std::min<uint64_t>(face_indices[i], std::max<uint64_t>(t.tri.size(), 1) - 1));
+    for (uint64_t i = 0; i < loops_total; ++i)
+        t.loops[i] = static_cast<uint32_t>(std::min<uint64_t>(loop_nodes[i], definition->node_count - 1));
+    return t;
+}
+
+void require_gpu() {
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+        raise(SWB_CUDA_ERROR, "no CUDA device: the cell volume kernel needs a GPU");
+}
+
+template <class T>
+T* upload_owned(std::vector<void*>& owned, const std::vector<T>& host) {
+    T* p = nullptr;
+    cuda_check(cudaMalloc(&p, std::max<size_t>(host.size(), 1) * sizeof(T)), "cudaMalloc (cell volume plan)");
+    owned.push_back(p);
+    if (!host.empty()) cuda_check(cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    return p;
+}
+
+// World positions in FP64 from a structure's device state: node n is slot
+// slot_of_node[n], stored as an FP32 offset from the state's FP64 origin.
+__global__ void gather_world_positions(const float4* __restrict__ pos, const double* __restrict__ origin,
+                                       const uint32_t* __restrict__ slot_of_node, uint32_t n, double* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 x = pos[slot_of_node[i]];
+    out[3 * i] = origin[0] + static_cast<double>(x.x);
+    out[3 * i + 1] = origin[1] + static_cast<double>(x.y);
+    out[3 * i + 2] = origin[2] + static_cast<double>(x.z);
+}
+
+}  // namespace
+}  // namespace swb
+
+// A set of cells whose tables live on one device.
+struct swb_cell_volume_plan {
+    int device = 0;
+    uint32_t cells = 0;
+    uint64_t node_count = 0;
+    swb::CellTopology* topo = nullptr;
+    uint3* tri = nullptr;
+    uint32_t* faces = nullptr;
+    uint32_t* loops = nullptr;
+    // the structure form's world positions, node-major
+    double* world = nullptr;
+    uint32_t* slot_of_node = nullptr;
+    const void* structure = nullptr;  // the structure `slot_of_node` belongs to
+    std::vector<void*> owned;
+    ~swb_cell_volume_plan() {
+        for (void* p : owned) cudaFree(p);
+    }
+};
+
 using namespace swb;
 
 swb_status swb_cell_volumes(const swb_structure_definition* definition, const uint64_t* face_indices,
@@ -280,39 +375,12 @@ swb_status swb_cell_volumes(const swb_structure_definition* definition, const ui
             for (uint64_t k = 0; k < cell_count; ++k) out[k] = swb_cell_volume{};
             return;
         }
-        if (definition->node_count > 0xffffffffu || definition->triangle_count > 0xffffffffu)
-            raise(SWB_INVALID_ARGUMENT, "definition too large for 32-bit indices");
-        uint64_t faces_total = 0, loops_total = 0;
-        for (uint64_t k = 0; k < cell_count; ++k) {
-            faces_total = std::max(faces_total, cells[k].face_begin + cells[k].face_count);
-            loops_total = std::max({loops_total, cells[k].low_begin + cells[k].low_count,
-                                    cells[k].high_begin + cells[k].high_count});
-        }
-        if ((faces_total && !face_indices) || (loops_total && !loop_nodes)) raise(SWB_INVALID_ARGUMENT, "null argument");
-        if (faces_total > 0xffffffffu || loops_total > 0xffffffffu)
-            raise(SWB_INVALID_ARGUMENT, "cell tables too large for 32-bit indices");
-        int devices = 0;
-        if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
-            raise(SWB_CUDA_ERROR, "no CUDA device: the cell volume kernel needs a GPU");
-        std::vector<CellTopology> topo(cell_count);
-        for (uint64_t k = 0; k < cell_count; ++k) topo[k] = cell_topology(*definition, face_indices, loop_nodes, cells[k]);
-        std::vector<uint3> tri(definition->triangle_count);
-        for (uint64_t t = 0; t < tri.size(); ++t) {
-            const uint64_t* n = definition->triangles[t].nodes;
-            // out-of-range nodes only reach the device in faces the topology rejects
-            tri[t] = make_uint3(static_cast<uint32_t>(std::min<uint64_t>(n[0], definition->node_count - 1)),
-                                static_cast<uint32_t>(std::min<uint64_t>(n[1], definition->node_count - 1)),
-                                static_cast<uint32_t>(std::min<uint64_t>(n[2], definition->node_count - 1)));
-        }
-        std::vector<uint32_t> faces(faces_total), loops(loops_total);
-        for (uint64_t i = 0; i < faces_total; ++i)
-            faces[i] = static_cast<uint32_t>(std::min<uint64_t>(face_indices[i], std::max<uint64_t>(tri.size(), 1) - 1));
-        for (uint64_t i = 0; i < loops_total; ++i)
-            loops[i] = static_cast<uint32_t>(std::min<uint64_t>(loop_nodes[i], definition->node_count - 1));
+        require_gpu();
+        const CellTables t = cell_tables(definition, face_indices, loop_nodes, cells, cell_count);
         std::vector<double> p(positions, positions + 3 * definition->node_count);
-        DeviceBuffer<CellTopology> d_topo(topo);
-        DeviceBuffer<uint3> d_tri(tri);
-        DeviceBuffer<uint32_t> d_faces(faces), d_loops(loops);
+        DeviceBuffer<CellTopology> d_topo(t.topo);
+        DeviceBuffer<uint3> d_tri(t.tri);
+        DeviceBuffer<uint32_t> d_faces(t.faces), d_loops(t.loops);
         DeviceBuffer<double> d_p(p);
         std::vector<swb_cell_volume> result(cell_count);
         DeviceBuffer<swb_cell_volume> d_out(result);
@@ -320,5 +388,72 @@ swb_status swb_cell_volumes(const swb_structure_definition* definition, const ui
             static_cast<uint32_t>(cell_count), d_topo.ptr, d_tri.ptr, d_faces.ptr, d_loops.ptr, d_p.ptr, d_out.ptr);
         cuda_check(cudaGetLastError(), "cell_volume_kernel");
         cuda_check(cudaMemcpy(out, d_out.ptr, cell_count * sizeof(swb_cell_volume), cudaMemcpyDeviceToHost), "download");
+    });
+}
+
+swb_status swb_cell_volume_plan_create(const swb_structure_definition* definition, const uint64_t* face_indices,
+                                       const uint64_t* loop_nodes, const swb_cell_def* cells, uint64_t cell_count,
+                                       int device, swb_cell_volume_plan** out) {
+    return guarded([&] {
+        if (!definition || !out || (cell_count && !cells)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        if (cell_count > 0xffffffffu) raise(SWB_INVALID_ARGUMENT, "too many cells");
+        if (definition->node_count == 0) raise(SWB_INVALID_ARGUMENT, "definition has no node");
+        require_gpu();
+        const CellTables t = cell_tables(definition, face_indices, loop_nodes, cells, cell_count);
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        auto plan = std::make_unique<swb_cell_volume_plan>();
+        plan->device = device;
+        plan->cells = static_cast<uint32_t>(cell_count);
+        plan->node_count = definition->node_count;
+        plan->topo = upload_owned(plan->owned, t.topo);
+        plan->tri = upload_owned(plan->owned, t.tri);
+        plan->faces = upload_owned(plan->owned, t.faces);
+        plan->loops = upload_owned(plan->owned, t.loops);
+        plan->world = upload_owned(plan->owned, std::vector<double>(3 * definition->node_count));
+        plan->slot_of_node = upload_owned(plan->owned, std::vector<uint32_t>(definition->node_count));
+        *out = plan.release();
+    });
+}
+
+void swb_cell_volume_plan_destroy(swb_cell_volume_plan* plan) {
+    if (!plan) return;
+    cudaSetDevice(plan->device);
+    delete plan;
+}
+
+swb_status swb_cell_volumes_device(const swb_cell_volume_plan* plan, const double* positions, swb_cell_volume* out,
+                                   void* stream) {
+    return guarded([&] {
+        if (!plan || !positions || (plan->cells && !out)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        if (!plan->cells) return;
+        cuda_check(cudaSetDevice(plan->device), "cudaSetDevice");
+        cell_volume_kernel<<<(plan->cells + 63) / 64, 64, 0, static_cast<cudaStream_t>(stream)>>>(
+            plan->cells, plan->topo, plan->tri, plan->faces, plan->loops, positions, out);
+        cuda_check(cudaGetLastError(), "cell_volume_kernel");
+    });
+}
+
+swb_status swb_structure_cell_volumes(const swb_structure* s, swb_cell_volume_plan* plan, swb_cell_volume* out) {
+    return guarded([&] {
+        if (!s || !plan || (plan->cells && !out)) raise(SWB_INVALID_ARGUMENT, "null argument");
+        const StructureImpl& m = s->s;
+        if (m.def.nodes.size() != plan->node_count) raise(SWB_INVALID_ARGUMENT, "plan belongs to another definition");
+        if (m.device != plan->device) raise(SWB_INVALID_ARGUMENT, "plan and structure are on different devices");
+        cuda_check(cudaSetDevice(plan->device), "cudaSetDevice");
+        if (plan->structure != s) {
+            // first use with this structure: its node -> slot table
+            cuda_check(cudaMemcpy(plan->slot_of_node, m.slot_of_node.data(), plan->node_count * sizeof(uint32_t),
+                                  cudaMemcpyHostToDevice), "upload");
+            plan->structure = s;
+        }
+        const uint32_t n = static_cast<uint32_t>(plan->node_count);
+        gather_world_positions<<<(n + 255) / 256, 256, 0, m.stream>>>(m.d_pos[m.cur], m.d_origin[m.cur],
+                                                                       plan->slot_of_node, n, plan->world);
+        cuda_check(cudaGetLastError(), "gather_world_positions");
+        if (!plan->cells) return;
+        cell_volume_kernel<<<(plan->cells + 63) / 64, 64, 0, m.stream>>>(plan->cells, plan->topo, plan->tri,
+                                                                          plan->faces, plan->loops, plan->world, out);
+        cuda_check(cudaGetLastError(), "cell_volume_kernel");
     });
 }

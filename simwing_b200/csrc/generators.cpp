@@ -330,7 +330,8 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
             p->rib_layers < 1 || p->fabric > 1 || !(p->root_chord > 0) || !(p->thickness > 0) ||
             !(p->areal_density > 0) || p->skin_compliance < 0 ||
             !(p->bend_rigidity > 0) || p->line_rows > 4 || p->line_levels < 1 ||
-            p->line_levels > 6 || p->line_particles > 64)
+            p->line_levels > 6 || p->line_particles > 64 ||
+            (p->attachments_per_cell > 1 && p->spanwise_per_cell % p->attachments_per_cell != 0))
             raise(SWB_INVALID_ARGUMENT, "invalid wing parameters");
         auto* def = new swb_definition;
         try {
@@ -530,17 +531,22 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                     b.mass[to] += 0.5 * line_density * piece;
                 };
                 const double row_x[4] = {0.10, 0.35, 0.60, 1.0};
+                // Attachment stations: every rib, or `attachments_per_cell`
+                // evenly spaced stations per cell.
+                const uint32_t per_cell = p->attachments_per_cell ? p->attachments_per_cell : 1u;
+                const uint32_t stride = p->spanwise_per_cell / per_cell;
+                const uint32_t stations = p->cells * per_cell;
                 for (uint32_t row = 0; row < p->line_rows; ++row) {
                     for (int side = 0; side < 2; ++side) {
                         // Attachments of this row and side, ordered from the
                         // centre outwards.
                         std::vector<uint64_t> level;
                         const bool brake = row == 3;
-                        for (uint32_t r = 0; r <= p->cells; ++r) {
-                            const double eta = -1.0 + 2.0 * r / p->cells;
+                        for (uint32_t r = 0; r <= stations; ++r) {
+                            const double eta = -1.0 + 2.0 * r / stations;
                             if ((side == 0) != (eta <= 0.0)) continue;
                             if (brake && (r % 2) != 0) continue;
-                            const uint32_t s = r * p->spanwise_per_cell;
+                            const uint32_t s = r * stride;
                             uint32_t best = 0;
                             for (uint32_t k = 0; k <= C; ++k)
                                 if (std::fabs(xi[C - k] - row_x[row]) <

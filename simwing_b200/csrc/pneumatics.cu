@@ -87,9 +87,12 @@ __device__ bool conductance_flow(const swb_flow_zone_state& first, const swb_flo
     return isfinite(r.signed_mass_rate);
 }
 
+// `zone_count`: ports naming a zone past it are refused (the host entry
+// point rejects them before the launch; the device-array form has no host
+// copy of the ports to check).
 __global__ void port_flow_kernel(swb_air_properties air, const swb_flow_zone_state* __restrict__ zones,
-                                 const swb_port_def* __restrict__ ports, uint64_t count, swb_mass_flow* out,
-                                 unsigned long long* failed) {
+                                 uint64_t zone_count, const swb_port_def* __restrict__ ports, uint64_t count,
+                                 swb_mass_flow* out, unsigned long long* failed) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (i >= count) return;
     const swb_port_def port = ports[i];
@@ -97,7 +100,7 @@ __global__ void port_flow_kernel(swb_air_properties air, const swb_flow_zone_sta
     r.pressure_ratio = 1.0;
     r.critical_pressure_ratio = 1.0;
     bool ok = false;
-    if (port.reserved == 0u) {
+    if (port.reserved == 0u && port.first < zone_count && port.second < zone_count) {
         const swb_flow_zone_state first = zones[port.first], second = zones[port.second];
         if (port.kind == SWB_PORT_ORIFICE) ok = orifice_flow(first, second, air, port, r);
         else if (port.kind == SWB_PORT_CONDUCTANCE) ok = conductance_flow(first, second, port, r);
@@ -105,6 +108,8 @@ __global__ void port_flow_kernel(swb_air_properties air, const swb_flow_zone_sta
     out[i] = r;
     if (!ok) atomicMin(failed, static_cast<unsigned long long>(i));
 }
+
+__global__ void set_word(unsigned long long* word, unsigned long long value) { *word = value; }
 
 template <class T>
 struct Scratch {
@@ -143,8 +148,8 @@ swb_status swb_port_mass_flows(const swb_air_properties* air, const swb_flow_zon
         cuda_check(cudaMemcpy(d_ports.ptr, ports, port_count * sizeof(swb_port_def), cudaMemcpyHostToDevice),
                    "upload ports");
         cuda_check(cudaMemcpy(d_failed.ptr, &none, sizeof none, cudaMemcpyHostToDevice), "upload");
-        port_flow_kernel<<<static_cast<unsigned>((port_count + 255) / 256), 256>>>(*air, d_zones.ptr, d_ports.ptr,
-                                                                                    port_count, d_out.ptr, d_failed.ptr);
+        port_flow_kernel<<<static_cast<unsigned>((port_count + 255) / 256), 256>>>(
+            *air, d_zones.ptr, zone_count, d_ports.ptr, port_count, d_out.ptr, d_failed.ptr);
         cuda_check(cudaGetLastError(), "port_flow_kernel");
         unsigned long long failed = none;
         cuda_check(cudaMemcpy(&failed, d_failed.ptr, sizeof failed, cudaMemcpyDeviceToHost), "download");
@@ -155,5 +160,23 @@ swb_status swb_port_mass_flows(const swb_air_properties* air, const swb_flow_zon
             raise(SWB_INVALID_ARGUMENT, "pneumatic port flow refused (invalid air, zone state, opening, port "
                                         "constants or a non-finite flow)");
         }
+    });
+}
+
+swb_status swb_port_mass_flows_device(const swb_air_properties* air, const swb_flow_zone_state* zones,
+                                      uint64_t zone_count, const swb_port_def* ports, uint64_t port_count,
+                                      swb_mass_flow* out, uint64_t* failed_port, void* stream) {
+    return guarded([&] {
+        if (!air || !failed_port || (port_count && (!ports || !out || !zones)))
+            raise(SWB_INVALID_ARGUMENT, "null argument");
+        static_assert(sizeof(uint64_t) == sizeof(unsigned long long), "64-bit word");
+        auto* failed = reinterpret_cast<unsigned long long*>(failed_port);
+        const cudaStream_t s = static_cast<cudaStream_t>(stream);
+        set_word<<<1, 1, 0, s>>>(failed, port_count);
+        cuda_check(cudaGetLastError(), "set_word");
+        if (!port_count) return;
+        port_flow_kernel<<<static_cast<unsigned>((port_count + 255) / 256), 256, 0, s>>>(
+            *air, zones, zone_count, ports, port_count, out, failed);
+        cuda_check(cudaGetLastError(), "port_flow_kernel");
     });
 }

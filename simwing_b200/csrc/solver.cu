@@ -863,7 +863,11 @@ void check_params(const StepParams& p) {
     if (!ok) raise(SWB_CUDA_ERROR, "internal error: a device table is missing; launch refused");
 }
 
-void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out) {
+// `first`: the first substep of a step clears the status words; later
+// substeps keep them, so a failure in any substep fails the whole step (and
+// a timed-out grid barrier makes the later substeps' barriers return at
+// once).
+void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out, bool first) {
     const double dt = st.time_step / st.substeps;
     if (cluster_mode) {
         ClusterParams cp = cparams;
@@ -880,7 +884,7 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out)
         cp.iterations = st.constraint_iterations;
         cp.cable_pairs = st.cable_sweep_pairs;
         if (!cp.instances || in == out) raise(SWB_CUDA_ERROR, "internal error: cluster instance table");
-        cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
+        if (first) cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
         cudaLaunchConfig_t cfg{};
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -911,7 +915,7 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out)
                                  st.damping_reference_velocity.z);
     p.iterations = st.constraint_iterations;
     check_params(p);
-    cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
+    if (first) cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
     void* args[] = {&p};
     cuda_check(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dev::xpbd_step_kernel), dim3(G), dim3(threads),
                                            args, p.smem_total, stream),
@@ -1129,7 +1133,7 @@ swb_status StructureImpl::step(const swb_step_settings& st, int steps, swb_diagn
     }
     cuda_check(cudaEventRecord(ev0, stream), "event");
     for (int k = 0; k < total; ++k) {
-        launch_substep(st, a, b);
+        launch_substep(st, a, b, k == 0);
         std::swap(a, b);
     }
     cuda_check(cudaEventRecord(ev1, stream), "event");

@@ -135,7 +135,7 @@ struct StructureImpl {
     // failed one
     int last_status[2] = {0, 0};
     swb_error_detail failure_detail(swb_status status, std::string& message);
-    void launch_substep(const swb_step_settings& st, int in, int out);
+    void launch_substep(const swb_step_settings& st, int in, int out, bool first);
     swb_status read_status(std::string& message);
     // Accepts `steps` steps that left the state in buffer `new_cur`: the
     // pending loads are consumed, the counters advance.

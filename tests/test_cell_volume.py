@@ -142,3 +142,70 @@ def test_device_cell_volumes_equal_the_reference_bytewise(cuda_device):
                   b.ambiguous_skin_orientation))
     # valid watertight, valid with fallback, invalid ambiguous, and the early returns
     assert (1, 1, 0, 0) in seen and (1, 0, 1, 0) in seen and (0, 0, 1, 1) in seen and (0, 0, 0, 0) in seen
+
+
+def plan_for(case):
+    p, t, faces, lo, hi = case
+    d = sw.definition_from_arrays([(x, y, z, 1.0, 0) for x, y, z in np.nan_to_num(p)], t)
+    cell = (CellDef * 1)(CellDef(0, len(faces), 0, len(lo), len(lo), len(hi)))
+    f = np.array(faces, dtype=np.uint64)
+    loops = np.array(list(lo) + list(hi), dtype=np.uint64)
+    plan = C.c_void_p()
+    sw._check(abi.library().swb_cell_volume_plan_create(d.pointer, f.ctypes.data, loops.ctypes.data,
+                                                         C.cast(cell, C.c_void_p), 1, 0, C.byref(plan)))
+    return d, plan
+
+
+@pytest.mark.gpu
+def test_device_resident_cell_volumes_equal_the_host_form(cuda_device):
+    """swb_cell_volumes_device (tables uploaded once at plan creation,
+    positions and results in device memory, one launch on the caller's
+    stream) gives the host form's estimates byte for byte."""
+    import torch
+
+    lib = abi.library()
+    host = bind(lib, "swb_cell_volumes")
+    stream = torch.cuda.Stream()
+    for k, case in enumerate(build_cases()):
+        d, plan = plan_for(case)
+        try:
+            pos = torch.tensor(np.ascontiguousarray(case[0], dtype=np.float64), device="cuda")
+            out = torch.zeros(C.sizeof(CellVolume), dtype=torch.uint8, device="cuda")
+            for _ in range(2):  # the plan is reused
+                sw._check(lib.swb_cell_volumes_device(plan, pos.data_ptr(), out.data_ptr(),
+                                                      C.c_void_p(stream.cuda_stream)))
+            stream.synchronize()
+            got = CellVolume.from_buffer_copy(out.cpu().numpy().tobytes())
+            assert bytes(got) == bytes(run(host, case)), f"case {k}"
+        finally:
+            lib.swb_cell_volume_plan_destroy(plan)
+
+
+@pytest.mark.gpu
+def test_structure_cell_volumes_at_the_device_state(cuda_device):
+    """swb_structure_cell_volumes reads a structure's committed state where
+    it lives: the estimates equal the host form's on the node states the
+    structure reports (the same FP32 offsets widened to FP64 world
+    positions)."""
+    import torch
+
+    lib = abi.library()
+    p, t, lo, hi = tube(rng=np.random.default_rng(9))
+    faces = list(range(len(t)))
+    case = (p, t, faces, lo, hi)
+    d, plan = plan_for(case)
+    try:
+        s = sw.Structure(d)
+        st = sw.StepSettings(time_step=1.0 / 120.0, substeps=1, constraint_iterations=4, gravity=(0.0, 0.0, -9.81))
+        out = torch.zeros(C.sizeof(CellVolume), dtype=torch.uint8, device="cuda")
+        for _ in range(3):
+            s.step(st, diagnostics=False)
+            sw._check(lib.swb_structure_cell_volumes(s.handle, plan, out.data_ptr()))
+            torch.cuda.synchronize()
+            got = CellVolume.from_buffer_copy(out.cpu().numpy().tobytes())
+            want = run(bind(lib, "swb_cell_volumes"), (s.positions(), t, faces, lo, hi))
+            assert bytes(got) == bytes(want)
+            assert got.valid and got.watertight_after_capping
+        s.close()
+    finally:
+        lib.swb_cell_volume_plan_destroy(plan)

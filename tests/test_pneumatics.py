@@ -130,3 +130,42 @@ def test_device_refuses_the_ports_the_reference_refuses(cuda_device):
             sw.port_mass_flows(zones, ports, air)
         assert e.value.port == k
     assert len(sw.port_mass_flows([], [], AIR)) == 0
+
+
+@pytest.mark.gpu
+def test_device_array_port_flows_equal_the_host_form(cuda_device):
+    """swb_port_mass_flows_device on device arrays (no allocation, no
+    synchronisation) gives the host form's flows byte for byte, and reports
+    the first refused port -- a zone index past the zone count included --
+    through the device word."""
+    import ctypes as C
+
+    import torch
+
+    zones, ports = random_case(n=3000, seed=5)
+    z = np.array(zones, dtype=abi.ZONE_DTYPE)
+    p = np.array(ports, dtype=abi.PORT_DTYPE)
+    lib = abi.library()
+    air = abi.AirProperties(*AIR)
+    stream = torch.cuda.Stream()
+
+    def device_flows(pp):
+        dz = torch.from_numpy(z.view(np.uint8).copy()).cuda()
+        dp = torch.from_numpy(pp.view(np.uint8).copy()).cuda()
+        out = torch.zeros(len(pp) * abi.FLOW_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        failed = torch.zeros(1, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        sw._check(lib.swb_port_mass_flows_device(C.byref(air), dz.data_ptr(), len(z), dp.data_ptr(), len(pp),
+                                                 out.data_ptr(), failed.data_ptr(), C.c_void_p(stream.cuda_stream)))
+        stream.synchronize()
+        return out.cpu().numpy().view(abi.FLOW_DTYPE), int(failed.cpu().item())
+
+    good = p[[k for k in range(len(p)) if p[k]["opening_fraction"] > 0.0]]
+    flows, failed = device_flows(good)
+    assert failed == len(good)
+    assert flows.tobytes() == sw.port_mass_flows(z, good, AIR).tobytes()
+    bad = good.copy()
+    bad[100]["second"] = len(z) + 3  # unknown zone
+    bad[700]["discharge_coefficient"] = 2.0  # refused constant
+    _, failed = device_flows(bad)
+    assert failed == 100
