@@ -509,6 +509,11 @@ swb_status swb_plan_schedule(const swb_structure_definition* definition,
                              swb_schedule_report* out,
                              uint64_t* distance_order,
                              uint64_t* dihedral_order);
+/* The membrane sweep order of the same host-built schedule (membrane_count
+ * entries).  No reference counterpart. */
+swb_status swb_plan_membrane_order(const swb_structure_definition* definition,
+                                   const swb_solver_options* options,
+                                   uint64_t* membrane_order);
 
 /* Device time of the most recent step's kernels in milliseconds, measured
  * with CUDA events on the solver's stream. */

@@ -537,6 +537,16 @@ def plan_schedule(definition: Definition, options: abi.SolverOptions | None = No
     return r, do[: v.constraint_count], ho[: v.dihedral_count]
 
 
+def plan_membrane_order(definition: Definition, options: abi.SolverOptions | None = None) -> np.ndarray:
+    """The membrane sweep order of the host-built schedule (as
+    Structure.sweep_order(SWEEP_MEMBRANE) gives it on the device)."""
+    n = definition.view.membrane_count
+    out = np.zeros(max(n, 1), dtype=np.uint64)
+    _check(abi.library().swb_plan_membrane_order(definition.pointer, None if options is None else C.byref(options),
+                                                 out.ctypes.data))
+    return out[:n]
+
+
 @dataclass
 class SuspensionState:
     center_of_mass: np.ndarray

@@ -292,6 +292,7 @@ _PROTOTYPES = {
     "swb_structure_last_step_ms": (C.c_double, [C.c_void_p]),
     "swb_plan_schedule": (C.c_int, [P(StructureDefinition), P(SolverOptions), P(ScheduleReport), C.c_void_p,
                                     C.c_void_p]),
+    "swb_plan_membrane_order": (C.c_int, [P(StructureDefinition), P(SolverOptions), C.c_void_p]),
     "swb_default_batch_options": (None, [P(BatchOptions)]),
     "swb_batch_create": (C.c_int, [C.c_void_p, C.c_uint64, P(BatchOptions), P(C.c_void_p)]),
     "swb_batch_destroy": (None, [C.c_void_p]),

@@ -415,10 +415,8 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
             // and the skin station between them is not sewn.  Each column is
             // split through the thickness into as many layers as keep its
             // elements about as tall as the chordwise station spacing (at
-            // most rib_layers, at least one), and neighbouring columns are
-            // joined by a strip that advances along the shorter diagonal, so
-            // no rib element is a sliver where the section thins towards the
-            // trailing edge.  The two end ribs close the end cells and carry
+            // most rib_layers, at least one), so no rib element is a sliver
+            // where the section thins towards the trailing edge.  The two end ribs close the end cells and carry
             // the outward pressure jump; the inner ribs separate pressurised
             // cells and carry none.
             const uint32_t L = p->rib_layers;
@@ -430,15 +428,24 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                 std::vector<std::vector<uint64_t>> col(C + 1);
                 const uint64_t le = b.node(surface_point(st, 0.0, 1.0));
                 const uint64_t te = b.node(surface_point(st, 1.0, 1.0));
+                // layers per column: about the section height over the
+                // station spacing, graded so that neighbouring columns differ
+                // by at most one layer (a strip then adds at most one
+                // triangle)
+                std::vector<uint32_t> layers(C + 1, 1);
+                for (uint32_t j = 1; j < J; ++j) {
+                    const double height = length(surface_point(st, xi[j], 1.0) - surface_point(st, xi[j], -1.0));
+                    const double spacing = 0.5 * (xi[j + 1] - xi[j - 1]) * st.chord;
+                    layers[j] = static_cast<uint32_t>(
+                        std::clamp(std::round(height / spacing), 1.0, static_cast<double>(L)));
+                }
+                for (uint32_t j = 2; j < J; ++j) layers[j] = std::min(layers[j], layers[j - 1] + 1);
+                for (uint32_t j = J - 2; j >= 1; --j) layers[j] = std::min(layers[j], layers[j + 1] + 1);
                 for (uint32_t j = 1; j < J; ++j) {
                     const V lo = surface_point(st, xi[j], -1.0);
                     const V hi = surface_point(st, xi[j], 1.0);
-                    const double spacing = 0.5 * (xi[j + 1] - xi[j - 1]) * st.chord;
-                    const double want = std::round(length(hi - lo) / spacing);
-                    const uint32_t layers =
-                        static_cast<uint32_t>(std::clamp(want, 1.0, static_cast<double>(L)));
-                    for (uint32_t l = 0; l <= layers; ++l)
-                        col[j].push_back(b.node(lo + (hi - lo) * (double(l) / layers)));
+                    for (uint32_t l = 0; l <= layers[j]; ++l)
+                        col[j].push_back(b.node(lo + (hi - lo) * (double(l) / layers[j])));
                 }
                 // End ribs: the normal of the fans and strips below points
                 // to -y (the r = 0 side); the far end rib takes the jump with
@@ -451,14 +458,13 @@ swb_status swb_generate_wing(const swb_wing_params* p, swb_definition** out) {
                 for (uint32_t j = 1; j + 1 < J; ++j) {
                     const std::vector<uint64_t>& u = col[j];
                     const std::vector<uint64_t>& w = col[j + 1];
+                    // advance the column with more layers left: the extra
+                    // triangle of a graded strip sits at the bottom boundary,
+                    // whose nodes have the fewest triangles, so no rib node
+                    // gathers more than six; quads split along one diagonal
                     size_t a = 0, c = 0;
                     while (a + 1 < u.size() || c + 1 < w.size()) {
-                        bool advance_u;
-                        if (a + 1 == u.size()) advance_u = false;
-                        else if (c + 1 == w.size()) advance_u = true;
-                        else
-                            advance_u = length(b.design[u[a + 1]] - b.design[w[c]]) <=
-                                        length(b.design[u[a]] - b.design[w[c + 1]]);
+                        const bool advance_u = u.size() - a > w.size() - c;
                         if (advance_u) {
                             b.triangle(u[a], w[c], u[a + 1], rib_pressure, p->areal_density);
                             ++a;

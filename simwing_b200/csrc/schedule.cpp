@@ -709,9 +709,29 @@ void verify_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& susp
 
 }  // namespace swb
 
+namespace {
+swb_status plan(const swb_structure_definition* definition, const swb_solver_options* options,
+                swb_schedule_report* out, uint64_t* distance_order, uint64_t* dihedral_order,
+                uint64_t* membrane_order);
+}  // namespace
+
 extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definition,
                                         const swb_solver_options* options, swb_schedule_report* out,
                                         uint64_t* distance_order, uint64_t* dihedral_order) {
+    return plan(definition, options, out, distance_order, dihedral_order, nullptr);
+}
+
+extern "C" swb_status swb_plan_membrane_order(const swb_structure_definition* definition,
+                                              const swb_solver_options* options, uint64_t* membrane_order) {
+    swb_schedule_report report;
+    if (!membrane_order && definition && definition->membrane_count) return SWB_INVALID_ARGUMENT;
+    return plan(definition, options, &report, nullptr, nullptr, membrane_order);
+}
+
+namespace {
+swb_status plan(const swb_structure_definition* definition, const swb_solver_options* options,
+                swb_schedule_report* out, uint64_t* distance_order, uint64_t* dihedral_order,
+                uint64_t* membrane_order) {
     using namespace swb;
     return guarded([&] {
         if (!definition || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
@@ -746,6 +766,7 @@ extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definiti
                 out->level_constraints[0] = def.constraints.size() + def.dihedrals.size();
                 if (distance_order) std::copy(C.distance_order.begin(), C.distance_order.end(), distance_order);
                 if (dihedral_order) std::copy(C.dihedral_order.begin(), C.dihedral_order.end(), dihedral_order);
+                if (membrane_order) std::copy(C.membrane_order.begin(), C.membrane_order.end(), membrane_order);
                 return;
             }
             if (options && options->cluster_ctas > 0)
@@ -778,7 +799,10 @@ extern "C" swb_status swb_plan_schedule(const swb_structure_definition* definiti
         out->max_patch_nodes = S.max_patch_nodes;
         for (int l = 0; l < 4; ++l) out->level_constraints[l] = S.level_constraints[l];
         out->global_constraints = S.global_constraints;
+        if (membrane_order && !def.membranes.empty())
+            raise(SWB_UNSUPPORTED, "membrane elements need the cluster schedule");
         if (distance_order) std::copy(S.distance_order.begin(), S.distance_order.end(), distance_order);
         if (dihedral_order) std::copy(S.dihedral_order.begin(), S.dihedral_order.end(), dihedral_order);
     });
 }
+}  // namespace
