@@ -258,8 +258,9 @@ def batched_leg(sw, st, count, rank, world, dist, device):
            "target_patch_nodes": rep.target_patch_nodes, "clusters": rep.clusters,
            "cluster_ctas": rep.cluster_ctas, "resident_clusters": rep.resident_clusters,
            "block_threads": rep.block_threads,
-           "autotune_ms_per_step": {str(rep.candidate_patch_nodes[k]): rep.candidate_ms_per_step[k]
-                                    for k in range(rep.autotune_candidates)}}
+           "autotune_ms_per_step": {f"patch {rep.candidate_patch_nodes[k]}, "
+                                    f"{rep.candidate_block_threads[k] or 'widest-stage'} threads":
+                                    rep.candidate_ms_per_step[k] for k in range(rep.autotune_candidates)}}
     batch.close()
     if rank == 0:
         # the same wings, one plain structure after another
@@ -519,7 +520,9 @@ def main():
 
     definition = sw.generate_wing()
     st = settings(sw)
-    structure = sw.Structure(definition, sw.SolverOptions(device=local))
+    # the autotuner picks block size, split stages and cluster width at
+    # creation (trial substeps that leave the state untouched)
+    structure = sw.Structure(definition, sw.SolverOptions(device=local, flags=sw.abi.OPT_AUTOTUNE))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
     # warm-up
@@ -609,7 +612,8 @@ def main():
                          "cluster_ctas": report.cluster_ctas,
                          "cluster_barriers_per_iteration": report.cluster_barriers_per_iteration,
                          "stages_per_iteration": report.local_stages_per_iteration,
-                         "shared_bytes": report.shared_bytes},
+                         "shared_bytes": report.shared_bytes,
+                         "autotune": structure.autotune_report()},
             "final_diagnostics": {"finite": bool(diag.finite), "max_distance_error": diag.maximum_distance_error},
             "batched": batched,
             "adjoint": adjoint,

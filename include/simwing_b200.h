@@ -321,11 +321,24 @@ enum {
                                       phase (comparison/debug)               */
     SWB_OPT_NO_GRAPH = 1u << 1,    /* batched: launch without CUDA graphs    */
     SWB_OPT_GRID = 1u << 2,        /* force the grid schedule                */
-    SWB_OPT_SPLIT_STAGES = 1u << 3 /* cluster schedule with split stages:
+    SWB_OPT_SPLIT_STAGES = 1u << 3, /* cluster schedule with split stages:
                                       interior constraints coloured per CTA
                                       behind CTA barriers, cluster barriers
                                       only where constraints span CTAs (fewer
                                       cluster barriers, more stages)         */
+    SWB_OPT_AUTOTUNE = 1u << 4     /* swb_structure_create builds the cluster
+                                      schedule for several block sizes (the
+                                      widest stage, 512, 768 threads), with
+                                      and without split stages and on the
+                                      smallest and the next wider cluster
+                                      that fit, times trial substeps of each
+                                      (which leave the state untouched) and
+                                      keeps the fastest; the other options
+                                      fields fix what they set.  Ignored for
+                                      fabric self-contact (the widest cluster
+                                      and 768 threads) and with SWB_OPT_GRID.
+                                      swb_structure_autotune_report lists
+                                      the candidates.                         */
 };
 
 void swb_default_solver_options(swb_solver_options* out);
@@ -495,6 +508,25 @@ typedef struct swb_schedule_report {
     int32_t cluster_ctas;                /* 0 = grid schedule                */
     int32_t cluster_barriers_per_iteration;
 } swb_schedule_report;
+/* The autotuner's candidates (SWB_OPT_AUTOTUNE) and its choice; zero
+ * candidates when the structure was not tuned.  No reference counterpart. */
+#define SWB_AUTOTUNE_MAX_CANDIDATES 16
+typedef struct swb_autotune_candidate {
+    int32_t cluster_ctas;
+    int32_t block_threads;
+    uint32_t split_stages;          /* 1: SWB_OPT_SPLIT_STAGES               */
+    int32_t stages_per_iteration;
+    double ms_per_substep;          /* trial substep, device time            */
+} swb_autotune_candidate;
+typedef struct swb_autotune_report {
+    uint32_t candidates;
+    uint32_t chosen;                /* index of the kept candidate            */
+    uint32_t iterations;            /* constraint iterations of the trials    */
+    uint32_t reserved;
+    swb_autotune_candidate entries[SWB_AUTOTUNE_MAX_CANDIDATES];
+} swb_autotune_report;
+swb_status swb_structure_autotune_report(const swb_structure* structure, swb_autotune_report* out);
+
 swb_status swb_structure_schedule_report(const swb_structure* structure,
                                          swb_schedule_report* out);
 
@@ -587,10 +619,12 @@ typedef struct swb_batch_report {
     int32_t max_cluster_stages;  /* colour stages per iteration, worst cluster */
     int32_t resident_clusters;   /* clusters the device holds at once        */
     int32_t colours_per_sync;    /* colour stages between cluster barriers   */
-    int32_t autotune_candidates; /* patch sizes timed at creation            */
+    int32_t autotune_candidates; /* patch size x block size pairs timed at
+                                    creation                                 */
     int32_t reserved;
     int32_t candidate_patch_nodes[8];
     double candidate_ms_per_step[8];
+    int32_t candidate_block_threads[8]; /* 0: enough for the widest stage    */
 } swb_batch_report;
 swb_status swb_batch_get_report(const swb_batch* batch, swb_batch_report* out);
 

@@ -716,6 +716,19 @@ class Structure:
         _check(self._lib.swb_structure_contact_candidates(self._h, keys, n.value, C.byref(n)))
         return list(keys)[: n.value]
 
+    def autotune_report(self) -> list:
+        """The autotuner's candidates (SolverOptions flags OPT_AUTOTUNE), each
+        a dict with `chosen` set on the one kept; empty when not tuned."""
+        r = abi.AutotuneReport()
+        _check(self._lib.swb_structure_autotune_report(self._h, C.byref(r)))
+        out = []
+        for k in range(r.candidates):
+            e = r.entries[k]
+            out.append({"cluster_ctas": e.cluster_ctas, "block_threads": e.block_threads,
+                        "split_stages": bool(e.split_stages), "stages_per_iteration": e.stages_per_iteration,
+                        "ms_per_substep": e.ms_per_substep, "chosen": k == r.chosen})
+        return out
+
     def schedule_report(self) -> abi.ScheduleReport:
         r = abi.ScheduleReport()
         _check(self._lib.swb_structure_schedule_report(self._h, C.byref(r)))

@@ -220,7 +220,8 @@ class BatchReport(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "structures", "clusters", "cluster_ctas", "idle_ctas", "block_threads", "target_patch_nodes",
         "shared_bytes", "max_cluster_stages", "resident_clusters", "colours_per_sync", "autotune_candidates",
-        "reserved")] + [("candidate_patch_nodes", C.c_int32 * 8), ("candidate_ms_per_step", C.c_double * 8)]
+        "reserved")] + [("candidate_patch_nodes", C.c_int32 * 8), ("candidate_ms_per_step", C.c_double * 8),
+                        ("candidate_block_threads", C.c_int32 * 8)]
 
 
 class RolloutGradient(C.Structure):
@@ -251,7 +252,17 @@ OK, INVALID_ARGUMENT, OUT_OF_RANGE, SUSPENSION_ERROR, CONTACT_ERROR, NON_FINITE,
     CUDA_ERROR, UNSUPPORTED, OUT_OF_MEMORY = range(10)
 
 DISTANCE, CABLE, SUSPENSION_TIE, SEAM_STITCH = 1, 2, 3, 4
-OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID, OPT_SPLIT_STAGES = 1, 2, 4, 8
+OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID, OPT_SPLIT_STAGES, OPT_AUTOTUNE = 1, 2, 4, 8, 16
+
+
+class AutotuneCandidate(C.Structure):
+    _fields_ = [("cluster_ctas", C.c_int32), ("block_threads", C.c_int32), ("split_stages", C.c_uint32),
+                ("stages_per_iteration", C.c_int32), ("ms_per_substep", C.c_double)]
+
+
+class AutotuneReport(C.Structure):
+    _fields_ = [("candidates", C.c_uint32), ("chosen", C.c_uint32), ("iterations", C.c_uint32),
+                ("reserved", C.c_uint32), ("entries", AutotuneCandidate * 16)]
 BATCH_AUTOTUNE = 1 << 8
 SWEEP_DISTANCE, SWEEP_DIHEDRAL, SWEEP_MEMBRANE = 0, 1, 2
 
@@ -293,6 +304,7 @@ _PROTOTYPES = {
     "swb_plan_schedule": (C.c_int, [P(StructureDefinition), P(SolverOptions), P(ScheduleReport), C.c_void_p,
                                     C.c_void_p]),
     "swb_plan_membrane_order": (C.c_int, [P(StructureDefinition), P(SolverOptions), C.c_void_p]),
+    "swb_structure_autotune_report": (C.c_int, [C.c_void_p, P(AutotuneReport)]),
     "swb_default_batch_options": (None, [P(BatchOptions)]),
     "swb_batch_create": (C.c_int, [C.c_void_p, C.c_uint64, P(BatchOptions), P(C.c_void_p)]),
     "swb_batch_destroy": (None, [C.c_void_p]),

@@ -227,6 +227,7 @@ struct BatchImpl {
     cudaLaunchAttribute launch_attr[1] = {};
     double last_ms = 0.0;
     std::vector<int> candidates;
+    std::vector<int> candidate_threads;
     std::vector<double> candidate_ms;
     // captured graph and what it was captured for
     cudaGraphExec_t graph = nullptr;
@@ -538,32 +539,47 @@ swb_status swb_batch_create(const swb_structure_definition* const* definitions, 
         swb_default_step_settings(&trial);
         trial.substeps = 1;
         trial.constraint_iterations = opt.autotune_iterations > 0 ? opt.autotune_iterations : 48;
+        // block sizes: the caller's, or with the autotuner also 512 threads
+        // beside enough for the widest stage
+        std::vector<int> thread_choices = {opt.block_threads};
+        if ((opt.flags & SWB_BATCH_AUTOTUNE) && opt.block_threads == 0) thread_choices.push_back(512);
+        const bool tuning = targets.size() * thread_choices.size() > 1;
         double best = 1e300;
         Packing best_packing;
-        for (int target : targets) {
+        for (const int target : targets) {
             Packing P;
             build_members(defs, B.device, target, B.cluster, P);
-            pack(P, B.cluster, opt.block_threads, smem_limit);
-            if (targets.size() == 1) {
+            if (!tuning) {
+                pack(P, B.cluster, thread_choices[0], smem_limit);
                 best_packing = std::move(P);
                 break;
             }
-            B.P = std::move(P);
-            B.upload_tables();
             // the trial settings must be valid for every structure (a pilot
             // fixes the iteration count)
             swb_step_settings st = trial;
-            for (const auto& m : B.P.members)
+            for (const auto& m : P.members)
                 if (m->s.def.has_suspension) st.constraint_iterations = m->s.def.suspension.solver_iterations;
-            const double ms = B.time_trial(st, 2, 3);
-            B.candidates.push_back(target);
-            B.candidate_ms.push_back(ms);
-            if (ms < best) {
-                best = ms;
-                best_packing = std::move(B.P);
+            int best_threads = -1;
+            for (const int block_threads : thread_choices) {
+                pack(P, B.cluster, block_threads, smem_limit);
+                B.P = std::move(P);
+                B.upload_tables();
+                const double ms = B.time_trial(st, 2, 3);
+                B.release_tables();
+                P = std::move(B.P);
+                B.P = Packing{};
+                B.candidates.push_back(target);
+                B.candidate_threads.push_back(block_threads);
+                B.candidate_ms.push_back(ms);
+                if (ms < best) {
+                    best = ms;
+                    best_threads = block_threads;
+                }
             }
-            B.release_tables();
-            B.P = Packing{};
+            if (best_threads >= 0) {
+                pack(P, B.cluster, best_threads, smem_limit);
+                best_packing = std::move(P);
+            }
         }
         B.P = std::move(best_packing);
         B.upload_tables();
@@ -611,6 +627,7 @@ swb_status swb_batch_get_report(const swb_batch* batch, swb_batch_report* out) {
         for (int k = 0; k < out->autotune_candidates; ++k) {
             out->candidate_patch_nodes[k] = B.candidates[k];
             out->candidate_ms_per_step[k] = B.candidate_ms[k];
+            out->candidate_block_threads[k] = B.candidate_threads[k];
         }
     });
 }

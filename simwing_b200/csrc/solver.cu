@@ -8,6 +8,7 @@
 #include "structure_impl.h"
 
 #include <algorithm>
+#include <limits>
 #include <bit>
 #include <cmath>
 #include <cstring>
@@ -1282,13 +1283,128 @@ void swb_default_solver_options(swb_solver_options* out) {
     std::memset(out, 0, sizeof(*out));
 }
 
+double StructureImpl::time_trial(const swb_step_settings& st, int warm, int reps) {
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    if (pressure_dirty) upload_pressure();
+    if (forces_dirty && !device_forces) upload_forces();
+    const int spare = (cur + 1) % 3;
+    for (int k = 0; k < warm; ++k) launch_substep(st, cur, spare, true);
+    cuda_check(cudaEventRecord(ev0, stream), "event");
+    for (int k = 0; k < reps; ++k) launch_substep(st, cur, spare, true);
+    cuda_check(cudaEventRecord(ev1, stream), "event");
+    cuda_check(cudaStreamSynchronize(stream), "trial");
+    float ms = 0.0f;
+    cuda_check(cudaEventElapsedTime(&ms, ev0, ev1), "event");
+    std::string message;
+    const swb_status status = read_status(message);
+    // the next step clears the status words before its first substep
+    return status == SWB_OK ? ms / reps : std::numeric_limits<double>::infinity();
+}
+
+namespace swb {
+namespace {
+
+// The autotuner (SWB_OPT_AUTOTUNE): cluster schedules for block sizes
+// (the widest stage, 512 and 768 threads), classic and split stages, the
+// smallest cluster that fits and the next wider one; each candidate is
+// built in full (its schedule verified) and timed over trial substeps from
+// the definition's state; the fastest is kept.  Candidates that do not fit
+// or fail to build are skipped.  Options the caller sets (block_threads,
+// cluster_ctas) are kept fixed.
+std::unique_ptr<swb_structure> autotuned(const swb_structure_definition& definition, swb_solver_options opt) {
+    opt.flags &= ~static_cast<uint32_t>(SWB_OPT_AUTOTUNE);
+    auto first = std::make_unique<swb_structure>();
+    first->s.build(definition, &opt);
+    StructureImpl& base = first->s;
+    if (!base.cluster_mode || base.def.has_contact) return first;
+    swb_step_settings st;
+    swb_default_step_settings(&st);
+    st.substeps = 1;
+    st.constraint_iterations = base.def.has_suspension ? base.def.suspension.solver_iterations : 48;
+    std::vector<int> ctas = {opt.cluster_ctas > 0 ? opt.cluster_ctas : base.G};
+    if (opt.cluster_ctas <= 0 && base.G * 2 <= kClusterMaxCtas) ctas.push_back(base.G * 2);
+    std::vector<int> threads = {opt.block_threads};
+    if (opt.block_threads <= 0)
+        for (int t : {512, 768}) threads.push_back(t);
+    swb_autotune_report report{};
+    report.iterations = static_cast<uint32_t>(st.constraint_iterations);
+    std::unique_ptr<swb_structure> best;
+    double best_ms = std::numeric_limits<double>::infinity();
+    for (int c : ctas)
+        for (uint32_t split : {0u, 1u})
+            for (int t : threads) {
+                if (report.candidates == SWB_AUTOTUNE_MAX_CANDIDATES) break;
+                swb_solver_options o = opt;
+                o.cluster_ctas = c;
+                o.block_threads = t;
+                o.flags = (opt.flags & ~static_cast<uint32_t>(SWB_OPT_SPLIT_STAGES)) |
+                          (split ? static_cast<uint32_t>(SWB_OPT_SPLIT_STAGES) : 0u);
+                std::unique_ptr<swb_structure> cand;
+                if (first && c == base.G && t == opt.block_threads &&
+                    split == ((opt.flags & SWB_OPT_SPLIT_STAGES) ? 1u : 0u)) {
+                    cand = std::move(first);
+                } else {
+                    cand = std::make_unique<swb_structure>();
+                    try {
+                        cand->s.build(definition, &o);
+                    } catch (const Error& e) {
+                        if (e.status == SWB_UNSUPPORTED || e.status == SWB_INVALID_ARGUMENT) continue;
+                        throw;
+                    }
+                    if (!cand->s.cluster_mode) continue;
+                }
+                // duplicates (a block size the default already chose)
+                bool seen = false;
+                for (uint32_t k = 0; k < report.candidates; ++k) {
+                    const swb_autotune_candidate& e = report.entries[k];
+                    seen = seen || (e.cluster_ctas == cand->s.G && e.block_threads == cand->s.threads &&
+                                    e.split_stages == split);
+                }
+                if (seen) continue;
+                const double ms = cand->s.time_trial(st, 2, 5);
+                swb_autotune_candidate& e = report.entries[report.candidates];
+                e.cluster_ctas = cand->s.G;
+                e.block_threads = cand->s.threads;
+                e.split_stages = split;
+                e.stages_per_iteration = 0;
+                for (int k = 0; k < 3; ++k) e.stages_per_iteration += cand->s.csched.kinds[k].stages;
+                e.ms_per_substep = ms;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = std::move(cand);
+                    report.chosen = report.candidates;
+                }
+                ++report.candidates;
+            }
+    if (!best) return first ? std::move(first) : nullptr;
+    best->s.tune = report;
+    return best;
+}
+
+}  // namespace
+}  // namespace swb
+
 swb_status swb_structure_create(const swb_structure_definition* definition, const swb_solver_options* options,
                                 swb_structure** out) {
     return guarded([&] {
         if (!definition || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
+        if (options && (options->flags & SWB_OPT_AUTOTUNE) &&
+            !(options->flags & (SWB_OPT_GRID | SWB_OPT_GLOBAL_ONLY))) {
+            auto tuned = autotuned(*definition, *options);
+            if (!tuned) raise(SWB_UNSUPPORTED, "no autotuner candidate could be built");
+            *out = tuned.release();
+            return;
+        }
         auto impl = std::make_unique<swb_structure>();
         impl->s.build(*definition, options);
         *out = impl.release();
+    });
+}
+
+swb_status swb_structure_autotune_report(const swb_structure* s, swb_autotune_report* out) {
+    return guarded([&] {
+        if (!s || !out) raise(SWB_INVALID_ARGUMENT, "null argument");
+        *out = s->s.tune;
     });
 }
 

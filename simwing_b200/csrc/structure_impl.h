@@ -134,6 +134,11 @@ struct StructureImpl {
     // the raw status words of the last step and the exception details of a
     // failed one
     int last_status[2] = {0, 0};
+    // autotuner: candidates and choice (empty when not tuned); device time
+    // of `reps` trial substeps from the committed state into the spare
+    // buffer, which leave the state untouched
+    swb_autotune_report tune{};
+    double time_trial(const swb_step_settings& st, int warm, int reps);
     swb_error_detail failure_detail(swb_status status, std::string& message);
     void launch_substep(const swb_step_settings& st, int in, int out, bool first);
     swb_status read_status(std::string& message);

@@ -291,3 +291,28 @@ def test_multi_substep_step_and_rollback(cuda_device):
     s.step(st)
     orc.step(st)
     assert rel_error(s.node_states(), orc.node_states()) <= REL_TOL
+
+
+@pytest.mark.parametrize("case", ["patch", "small wing"])
+def test_autotuned_structure_keeps_parity(cuda_device, case):
+    """SWB_OPT_AUTOTUNE: the candidates are reported, the fastest is kept,
+    every candidate's schedule passed the verifier on construction, and the
+    chosen one steps like the oracle in its own sweep order."""
+    d = sw.generate_patch() if case == "patch" else \
+        sw.generate_wing(cells=8, chordwise=20, spanwise_per_cell=2, rib_layers=3)
+    opts = sw.SolverOptions(flags=sw.abi.OPT_AUTOTUNE)
+    dev = sw.Structure(d, opts)
+    report = dev.autotune_report()
+    assert len(report) >= 2 and sum(c["chosen"] for c in report) == 1
+    chosen = next(c for c in report if c["chosen"])
+    assert chosen["ms_per_substep"] == min(c["ms_per_substep"] for c in report)
+    r = dev.schedule_report()
+    assert (r.cluster_ctas, r.block_threads) == (chosen["cluster_ctas"], chosen["block_threads"])
+    orc = O.PortStructure(dev.oracle_definition())
+    st = step_settings()
+    for _ in range(3):
+        sync_oracle_to_device(dev, orc)
+        dev.step(st, diagnostics=False)
+        orc.step(st)
+        assert rel_error(dev.node_states(), orc.node_states()) <= REL_TOL
+    assert sw.Structure(d).autotune_report() == []
