@@ -552,9 +552,10 @@ inline swb_step_settings to_swb(const StructureStepSettings& s) {
 }
 
 // Reads the public fields of a checkpoint image (layout written by
-// swb_structure_checkpoint: magic, version, suspension flag, fingerprint,
-// accepted steps, time, last dt, origin, node count, per node position /
-// previous / velocity, pending forces, last applied force, ...).
+// swb_structure_checkpoint: magic, version, suspension flag, contact flag,
+// a reserved word, fingerprint, accepted steps, time, last dt, origin, node
+// count, per node position / previous / velocity, pending forces, last
+// applied force, ...).
 class ImageReader {
 public:
     explicit ImageReader(const std::vector<std::uint8_t>& b) : b_(b) {}
@@ -671,7 +672,7 @@ public:
         simwing_b200::check(swb_structure_checkpoint(h(), det->image.data(), bytes));
         StructureCheckpoint c;
         detail::ImageReader r(det->image);
-        r.skip(8 + 4 + 4);
+        r.skip(8 + 4 + 4 + 4 + 4);
         c.definitionFingerprint = r.get<std::uint64_t>();
         c.acceptedStepCount = r.get<std::uint64_t>();
         c.simulationTimeSeconds = r.get<double>();

@@ -266,6 +266,7 @@ struct RolloutImpl {
         cp.inv_dt = static_cast<float>(1.0 / dt);
         cp.inv_dt2 = static_cast<float>(1.0 / (dt * dt));
         cp.damping = static_cast<float>(std::exp(-settings.velocity_damping * dt));
+        cp.damping_loss = static_cast<float>(-std::expm1(-settings.velocity_damping * dt));
         cp.gravity = make_float3(settings.gravity.x, settings.gravity.y, settings.gravity.z);
         cp.ref_velocity = make_float3(settings.damping_reference_velocity.x, settings.damping_reference_velocity.y,
                                       settings.damping_reference_velocity.z);

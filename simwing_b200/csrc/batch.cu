@@ -341,6 +341,7 @@ struct BatchImpl {
         cp.inv_dt = static_cast<float>(1.0 / dt);
         cp.inv_dt2 = static_cast<float>(1.0 / (dt * dt));
         cp.damping = static_cast<float>(std::exp(-st.velocity_damping * dt));
+        cp.damping_loss = static_cast<float>(-std::expm1(-st.velocity_damping * dt));
         cp.gravity = make_float3(st.gravity.x, st.gravity.y, st.gravity.z);
         cp.ref_velocity = make_float3(st.damping_reference_velocity.x, st.damping_reference_velocity.y,
                                       st.damping_reference_velocity.z);

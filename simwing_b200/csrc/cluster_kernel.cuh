@@ -397,9 +397,12 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         const float4 V0 = __ldg(I.vel_in + base + i);
         const float4 F = v[i];
         const float ax = p.gravity.x + F.x * X.w, ay = p.gravity.y + F.y * X.w, az = p.gravity.z + F.z * X.w;
-        const float vx = p.ref_velocity.x + ((V0.x + ax * p.dt) - p.ref_velocity.x) * p.damping;
-        const float vy = p.ref_velocity.y + ((V0.y + ay * p.dt) - p.ref_velocity.y) * p.damping;
-        const float vz = p.ref_velocity.z + ((V0.z + az * p.dt) - p.ref_velocity.z) * p.damping;
+        const float wx = (V0.x + ax * p.dt) - p.ref_velocity.x;
+        const float vx = p.ref_velocity.x + (wx - wx * p.damping_loss);
+        const float wy = (V0.y + ay * p.dt) - p.ref_velocity.y;
+        const float vy = p.ref_velocity.y + (wy - wy * p.damping_loss);
+        const float wz = (V0.z + az * p.dt) - p.ref_velocity.z;
+        const float vz = p.ref_velocity.z + (wz - wz * p.damping_loss);
         X.x += vx * p.dt;
         X.y += vy * p.dt;
         X.z += vz * p.dt;

@@ -145,6 +145,15 @@ struct ContactDev {
     unsigned long long* reduce;        // [2] active records, largest penetration (bits)
     unsigned long long* fail;          // [1] the failing feature first in key order, packed with its
                                        // detail code (contact_fail_at); all ones when none failed
+    // cluster-wide levels of a key-ordered pass (cluster_levels): node
+    // buckets of the (node, item) pairs, each item's predecessors through
+    // its nodes, and the round flags of the longest-path relaxation
+    uint32_t* lv_node_start;           // [slots + 1] counts, then bucket starts
+    uint32_t* lv_node_fill;            // [slots]
+    uint32_t* lv_pairs;                // [6 * cand_cap]
+    uint32_t* lv_pred;                 // [6 * cand_cap]
+    uint32_t* lv_npred;                // [cand_cap]
+    uint32_t* lv_flag;                 // [3]
 };
 
 // Per-instance tables and state (one cluster each).
@@ -254,6 +263,7 @@ struct ClusterParams {
     const int* rotation;               // packed launches: committed buffer per structure
     int role;                          // packed launches: 0 = S->T1, 1 = T1->T2, 2 = T2->T1
     float dt, inv_dt, inv_dt2, damping;
+    float damping_loss;            // 1 - damping from FP64 (see StepParams)
     double dt64;                   // the substep in FP64 (contact phases)
     float3 gravity, ref_velocity;
     int iterations;

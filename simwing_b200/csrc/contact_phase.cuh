@@ -628,6 +628,100 @@ __device__ __forceinline__ void assign_levels(const ContactCtx& c, uint32_t item
     block_scan(C.level_start + 1, levels, C.level_start + 1);
 }
 
+// Levels of `items` in order, over the whole cluster (every thread of every
+// CTA calls it): get(i, slots) returns item i's nodes (0: the item takes no
+// level).  An item's level is one more than the largest level among the
+// earlier items sharing one of its nodes (1 without one), as a serial fold
+// in item order gives it.  The (node, item) pairs are bucketed by node with
+// a counting sort and each bucket is put in item order, so an item's
+// predecessors are the items just before it in its nodes' buckets; the
+// longest path over these links is then relaxed in rounds, each lifting
+// every item to one more than its predecessors' largest level, until a
+// round changes nothing (at most `items` rounds: a path has at most `items`
+// links).  Leaves item_level[], the level count in level_meta[0] and the
+// levels' starts in level_start[1 .. levels + 1], as the serial fold does.
+template <class Get>
+__device__ __noinline__ void cluster_levels(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
+                                            uint32_t items, uint32_t slots, Get get) {
+    const ContactDev& C = *c.C;
+    const uint32_t gt = cluster_tid(c), stride = cluster_threads(c);
+    uint32_t* count = C.lv_node_start;  // counts, then (scanned in place) bucket starts
+    for (uint32_t i = gt; i <= slots; i += stride) count[i] = 0;
+    for (uint32_t i = gt; i < slots; i += stride) C.lv_node_fill[i] = 0;
+    for (uint32_t i = gt; i < items; i += stride) C.lv_npred[i] = 0;
+    if (gt == 0) {
+        C.level_meta[0] = 0;
+        C.lv_flag[0] = C.lv_flag[1] = C.lv_flag[2] = 0;
+    }
+    cluster.sync();
+    uint32_t s6[6];
+    for (uint32_t i = gt; i < items; i += stride) {
+        const uint32_t n = get(i, s6);
+        for (uint32_t q = 0; q < n; ++q) atomicAdd(&count[s6[q]], 1u);
+        C.item_level[i] = n ? 1u : 0u;
+    }
+    cluster.sync();
+    if (c.me == 0) block_scan(count, slots, count);
+    cluster.sync();
+    for (uint32_t i = gt; i < items; i += stride) {
+        const uint32_t n = get(i, s6);
+        for (uint32_t q = 0; q < n; ++q) C.lv_pairs[count[s6[q]] + atomicAdd(&C.lv_node_fill[s6[q]], 1u)] = i;
+    }
+    cluster.sync();
+    // each node's bucket in item order; an item's predecessor through the
+    // node is the item before it there
+    for (uint32_t v = gt; v < slots; v += stride) {
+        const uint32_t lo = count[v], hi = count[v + 1];
+        for (uint32_t a = lo + 1; a < hi; ++a) {
+            const uint32_t x = C.lv_pairs[a];
+            uint32_t b = a;
+            while (b > lo && C.lv_pairs[b - 1] > x) {
+                C.lv_pairs[b] = C.lv_pairs[b - 1];
+                --b;
+            }
+            C.lv_pairs[b] = x;
+        }
+        for (uint32_t a = lo + 1; a < hi; ++a) {
+            const uint32_t j = C.lv_pairs[a];
+            C.lv_pred[static_cast<size_t>(j) * 6 + atomicAdd(&C.lv_npred[j], 1u)] = C.lv_pairs[a - 1];
+        }
+    }
+    cluster.sync();
+    // longest path: rounds until one changes nothing; round r reports on
+    // flag r % 3 and clears the flag round r + 1 will use (last read two
+    // barriers ago)
+    for (uint32_t r = 0; r <= items; ++r) {
+        bool changed = false;
+        for (uint32_t i = gt; i < items; i += stride) {
+            const uint32_t np = C.lv_npred[i];
+            if (!np) continue;
+            uint32_t l = 0;
+            for (uint32_t k = 0; k < np; ++k) l = max(l, __ldcg(C.item_level + C.lv_pred[static_cast<size_t>(i) * 6 + k]));
+            ++l;
+            if (l > __ldcg(C.item_level + i)) {
+                __stcg(C.item_level + i, l);
+                changed = true;
+            }
+        }
+        if (changed) C.lv_flag[r % 3] = 1u;
+        if (gt == 0) C.lv_flag[(r + 1) % 3] = 0u;
+        cluster.sync();
+        if (*reinterpret_cast<const volatile uint32_t*>(C.lv_flag + r % 3) == 0u) break;
+    }
+    // the levels' sizes and starts (rank 0's block)
+    if (c.me == 0) {
+        for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) atomicMax(C.level_meta, __ldcg(C.item_level + i));
+        __syncthreads();
+        const uint32_t levels = C.level_meta[0];
+        for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) {
+            const uint32_t l = __ldcg(C.item_level + i);
+            if (l) atomicAdd(&C.level_start[l], 1u);
+        }
+        __syncthreads();
+        block_scan(C.level_start + 1, levels, C.level_start + 1);
+    }
+}
+
 // Clears the level tables for `items` items (every thread of the cluster).
 __device__ __forceinline__ void reset_levels(const ContactCtx& c, uint32_t items, uint32_t slots) {
     const ContactDev& C = *c.C;
@@ -643,7 +737,7 @@ __device__ __forceinline__ void reset_levels(const ContactCtx& c, uint32_t items
 // holds id[item], or the item itself without `id`.
 __device__ __forceinline__ void scatter_levels(const ContactDev& C, uint32_t items, const uint32_t* id = nullptr) {
     for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) {
-        const uint32_t l = C.item_level[i];
+        const uint32_t l = __ldcg(C.item_level + i);  // written by every CTA of the cluster
         if (l) C.level_items[C.level_start[l] + atomicAdd(&C.level_fill[l], 1u)] = id ? id[i] : i;
     }
     __syncthreads();
@@ -690,7 +784,7 @@ static __device__ __noinline__ void project_one(const ContactCtx& c, uint32_t i)
     D3 normal = d3_of(Q.normal);
     if (contact::dot(normal, d3_of(Q.ccd_normal)) < 0.0) normal = -normal;
     if (!contact::finite3(normal) || fabs(contact::norm2(normal) - 1.0) > 1.0e-8) {
-        contact_fail(c.status, kContactNormal);
+        contact_fail_at(C, c.status, kContactNormal, C.cand[i]);
         return;
     }
     const double dt = c.dt;
@@ -801,23 +895,27 @@ __device__ __noinline__ void contact_project(const ContactCtx& c, cooperative_gr
         }
     }
     cluster.sync();
-    // ranks of the two merged lists; the candidates in contact, their levels
-    // and their projections, level by level (rank 0's block)
+    // ranks of the two merged lists and the candidates in contact (rank 0's
+    // block); their levels (the cluster); their projections, level by level
+    // (rank 0's block)
     if (c.me == 0) {
         block_scan(C.mark_a, count, C.mark_a);
         block_scan(C.mark_b, old_n, C.mark_b);
-        if (!contact_failed(c.status)) {
-            const uint32_t hits = C.mark_a[count];
+        if (!contact_failed(c.status))
             for (uint32_t i = threadIdx.x; i < count; i += blockDim.x)
                 if (C.mark_a[i + 1] != C.mark_a[i]) C.hit[C.mark_a[i]] = i;
-            __syncthreads();
-            assign_levels(c, hits, slots, [&](uint32_t h, uint32_t* s) -> uint32_t {
-                const ContactQuery& Q = C.query[C.hit[h]];
-                const uint32_t n = Q.fc + Q.sc;
+    }
+    cluster.sync();
+    if (!contact_failed(c.status)) {  // uniform: read after the barrier
+        const uint32_t hits = C.mark_a[count];
+        cluster_levels(c, cluster, hits, slots, [&](uint32_t h, uint32_t* s) -> uint32_t {
+            const ContactQuery& Q = C.query[C.hit[h]];
+            const uint32_t n = Q.fc + Q.sc;
 #pragma unroll
-                for (int j = 0; j < 6; ++j) s[j] = j < static_cast<int>(n) ? Q.slot[j] : 0u;
-                return n;
-            });
+            for (int j = 0; j < 6; ++j) s[j] = j < static_cast<int>(n) ? Q.slot[j] : 0u;
+            return n;
+        });
+        if (c.me == 0) {
             scatter_levels(C, hits, C.hit);
             run_levels(C, [&](uint32_t i) { project_one(c, i); });
         }
@@ -1032,14 +1130,14 @@ __device__ __forceinline__ void contact_friction(const ContactCtx& c, cooperativ
     const uint32_t records = skip ? 0u : static_cast<uint32_t>(diag->records);
     reset_levels(c, records, c.pbeg[c.ctas]);
     cluster.sync();
-    if (c.me == 0) {
-        assign_levels(c, records, c.pbeg[c.ctas], [&](uint32_t i, uint32_t* s) -> uint32_t {
-            const ContactRecordDev& r = C.records[i];
-            const uint32_t n = r.fc + r.sc;
+    cluster_levels(c, cluster, records, c.pbeg[c.ctas], [&](uint32_t i, uint32_t* s) -> uint32_t {
+        const ContactRecordDev& r = C.records[i];
+        const uint32_t n = r.fc + r.sc;
 #pragma unroll
-            for (int j = 0; j < 6; ++j) s[j] = j < static_cast<int>(n) ? r.slot[j] : 0u;
-            return n;
-        });
+        for (int j = 0; j < 6; ++j) s[j] = j < static_cast<int>(n) ? r.slot[j] : 0u;
+        return n;
+    });
+    if (c.me == 0) {
         scatter_levels(C, records);
         run_levels(C, [&](uint32_t i) { friction_one(c, C.records[i]); });
     }

@@ -441,6 +441,12 @@ void StructureImpl::setup_contact() {
     // a failing feature is packed as row << 37 | col << 5 | detail
     if (static_cast<uint64_t>(c.nv) + c.ne >= (uint64_t(1) << 27))
         raise(SWB_UNSUPPORTED, "fabric self-contact surface too large for the device feature codes");
+    c.lv_node_start = dalloc<uint32_t>(owned, def.nodes.size() + 1);
+    c.lv_node_fill = dalloc<uint32_t>(owned, std::max<size_t>(def.nodes.size(), 1));
+    c.lv_pairs = dalloc<uint32_t>(owned, 6 * cap);
+    c.lv_pred = dalloc<uint32_t>(owned, 6 * cap);
+    c.lv_npred = dalloc<uint32_t>(owned, cap);
+    c.lv_flag = dalloc<uint32_t>(owned, 3);
     c.fail = dalloc<unsigned long long>(owned, 1);
     cuda_check(cudaMemsetAsync(c.fail, 0xff, sizeof(unsigned long long), stream), "memset");
     d_contact = dupload(owned, std::vector<ContactDev>{c}, stream);
@@ -879,6 +885,7 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out,
         cp.inv_dt = static_cast<float>(1.0 / dt);
         cp.inv_dt2 = static_cast<float>(1.0 / (dt * dt));
         cp.damping = static_cast<float>(std::exp(-st.velocity_damping * dt));
+        cp.damping_loss = static_cast<float>(-std::expm1(-st.velocity_damping * dt));
         cp.gravity = make_float3(st.gravity.x, st.gravity.y, st.gravity.z);
         cp.ref_velocity = make_float3(st.damping_reference_velocity.x, st.damping_reference_velocity.y,
                                       st.damping_reference_velocity.z);
@@ -911,6 +918,7 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out,
     p.inv_dt = static_cast<float>(1.0 / dt);
     p.inv_dt2 = static_cast<float>(1.0 / (dt * dt));
     p.damping = static_cast<float>(std::exp(-st.velocity_damping * dt));
+    p.damping_loss = static_cast<float>(-std::expm1(-st.velocity_damping * dt));
     p.gravity = make_float3(st.gravity.x, st.gravity.y, st.gravity.z);
     p.ref_velocity = make_float3(st.damping_reference_velocity.x, st.damping_reference_velocity.y,
                                  st.damping_reference_velocity.z);

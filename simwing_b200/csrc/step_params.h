@@ -86,6 +86,11 @@ struct StepParams {
     const uint32_t* seam_b;
     // physics
     float dt, inv_dt, inv_dt2, damping;
+    // 1 - damping, from FP64: the predicted velocity is w - w * damping_loss
+    // (w the undamped one), which FP32 keeps unbiased where w * damping
+    // would carry the rounding of the factor close to 1, magnified
+    // 1 / (1 - damping) times in the velocity it settles to
+    float damping_loss;
     float3 gravity, ref_velocity;
     int iterations;
     // suspension

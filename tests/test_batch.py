@@ -103,13 +103,21 @@ def test_batch_failure_is_isolated_and_rolled_back(cuda_device):
 
 
 def test_batch_autotune_times_candidates(cuda_device):
+    """The batch autotuner times three patch sizes, each with two block
+    sizes (enough threads for the widest stage, and 512), and keeps the
+    fastest pair."""
     defs = mixed_definitions()[:3]
     with sw.Batch(defs, sw.BatchOptions(flags=abi.BATCH_AUTOTUNE)) as batch:
         rep = batch.report()
-        assert rep.autotune_candidates == 3
-        ms = [rep.candidate_ms_per_step[k] for k in range(3)]
+        n = rep.autotune_candidates
+        assert n == 6
+        pairs = {(rep.candidate_patch_nodes[k], rep.candidate_block_threads[k]) for k in range(n)}
+        assert pairs == {(p, t) for p in (1024, 2048, 4096) for t in (0, 512)}
+        ms = [rep.candidate_ms_per_step[k] for k in range(n)]
         assert all(m > 0 for m in ms)
-        best = min(range(3), key=lambda k: ms[k])
+        best = min(range(n), key=lambda k: ms[k])
         assert rep.target_patch_nodes == rep.candidate_patch_nodes[best]
+        if rep.candidate_block_threads[best]:
+            assert rep.block_threads == rep.candidate_block_threads[best]
         batch.step(step_settings(), 2)
         assert all(batch.structure(i).accepted_step_count() == 2 for i in range(len(defs)))
