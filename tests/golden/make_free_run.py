@@ -19,7 +19,16 @@ are stored in FP32 (the tests compare at 1e-3 m).  A hash of each case's
 sweep order is stored too: the tests check that the device still sweeps in
 that order.
 
-    python tests/golden/make_free_run.py       (about 10 minutes)
+Each case also runs a second time in FP64 from the same state with every
+position moved by N(0, 1e-7 m) (about the rounding of an FP32 position of
+a metre): how far that run ends from the first measures how strongly the
+configuration itself amplifies a perturbation of the size FP32 rounding
+makes.  Stored per case: the largest deviation of the fabric (triangle)
+nodes and of the other (line) nodes from the first run's shape at the
+position steps (each relative to its centre of mass), and the largest
+differences of the two norms and of the centre of mass over all steps.
+
+    python tests/golden/make_free_run.py       (about 10 minutes, 6 cores)
 """
 import hashlib
 import multiprocessing as mp
@@ -50,7 +59,14 @@ def order_hash(*orders):
     return h.hexdigest()
 
 
-def run_case(name):
+PERTURBATION = 1e-7
+
+
+def run_case(job):
+    """One FP64 run of a case; `perturbed` moves every initial position by
+    N(0, PERTURBATION).  Returns the per-step diagnostics and the positions
+    (FP64) at the position steps."""
+    name, perturbed = job
     import simwing_b200 as sw
     from oracle import oracle as O
 
@@ -64,30 +80,49 @@ def run_case(name):
     st = sw.StepSettings(time_step=1.0 / 120.0, substeps=1, constraint_iterations=48, gravity=(0.0, 0.0, -9.81),
                          velocity_damping=0.25)
     orc = O.PortStructure(od)
-    out = {}
-    diag = []
+    if perturbed:
+        s0 = orc.node_states()
+        s0[:, 0, :] += np.random.default_rng(1).normal(0.0, PERTURBATION, s0[:, 0, :].shape)
+        s0[:, 1, :] = s0[:, 0, :]
+        orc.write_node_states(s0)
+    positions, diag = {}, []
     t0 = time.time()
     for k in range(1, steps + 1):
         g = orc.step(st)
         diag.append((g.maximum_distance_error, g.maximum_cable_extension, g.maximum_absolute_membrane_strain,
                      g.center_of_mass.x, g.center_of_mass.y, g.center_of_mass.z))
         if k in keep:
-            out[f"{name}_x{k}"] = orc.positions().astype(np.float32)
-    out[f"{name}_diag"] = np.array(diag)
-    out[f"{name}_order_hash"] = np.array(order_hash(*orders))
-    out[f"{name}_steps"] = np.array(steps)
-    print(name, "%.0f s" % (time.time() - t0), diag[-1][:3], flush=True)
-    return out
+            positions[k] = orc.positions()
+    fabric = np.zeros(d.node_count, dtype=bool)
+    fabric[d.triangles()["nodes"].astype(np.int64).ravel()] = True
+    print(name, "perturbed" if perturbed else "", "%.0f s" % (time.time() - t0), diag[-1][:3], flush=True)
+    return {"diag": np.array(diag), "positions": positions, "order_hash": order_hash(*orders), "fabric": fabric}
 
 
 def main():
-    with mp.get_context("spawn").Pool(len(CASES)) as pool:
-        parts = pool.map(run_case, list(CASES))
+    jobs = [(name, p) for name in CASES for p in (False, True)]
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+        runs = dict(zip(jobs, pool.map(run_case, jobs)))
     out = {}
-    for p in parts:
-        out.update(p)
+    for name, (_, steps, keep) in CASES.items():
+        a, b = runs[(name, False)], runs[(name, True)]
+        out[f"{name}_diag"] = a["diag"]
+        out[f"{name}_order_hash"] = np.array(a["order_hash"])
+        out[f"{name}_steps"] = np.array(steps)
+        out[f"{name}_fabric"] = a["fabric"]
+        shape_fabric, shape_lines = [], []
+        for k in keep:
+            out[f"{name}_x{k}"] = a["positions"][k].astype(np.float32)
+            dev = np.abs((b["positions"][k] - b["diag"][k - 1, 3:6]) -
+                         (a["positions"][k] - a["diag"][k - 1, 3:6])).max(axis=1)
+            shape_fabric.append(float(dev[a["fabric"]].max()))
+            shape_lines.append(float(dev[~a["fabric"]].max()) if (~a["fabric"]).any() else 0.0)
+        out[f"{name}_sens_shape_fabric"] = np.array(shape_fabric)
+        out[f"{name}_sens_shape_lines"] = np.array(shape_lines)
+        out[f"{name}_sens_norms"] = np.array(float(np.abs(b["diag"][:, :2] - a["diag"][:, :2]).max()))
+        out[f"{name}_sens_com"] = np.array(float(np.abs(b["diag"][:, 3:6] - a["diag"][:, 3:6]).max()))
     np.savez_compressed(OUT, **out)
-    print("wrote", OUT, sorted(out))
+    print("wrote", OUT, {k: out[k] for k in out if "sens" in k})
 
 
 if __name__ == "__main__":
