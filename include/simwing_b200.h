@@ -758,6 +758,152 @@ swb_status swb_generate_patch(const swb_patch_params* params,
                               swb_definition** out);
 swb_status swb_generate_wing(const swb_wing_params* params,
                              swb_definition** out);
+/* ------------------------------------------------------------------------ */
+/* Scene assembly: simwing::fsi::assembleSceneStructure                     */
+/* (src/fsi/scene_structure.h:127-196, scene_structure.cpp:278-1284) --     */
+/* authored scene-v2 geometry (src/fsi/scene.h:77-233) to a definition:     */
+/* fabric mass lumped from each triangle's material-chart area, one Bulk    */
+/* membrane per triangle, one dihedral per consistently oriented manifold   */
+/* edge of one sheet with compliance h0/(2 D0 L0) + h1/(2 D1 L1), seams as  */
+/* zero-rest stitches plus half-rigidity rails, and the suspension as       */
+/* nodal cables or, with one rigid pilot, a tree oriented from the canopy   */
+/* leaves to the harness roots.  Entities are taken in stable-ID order, so  */
+/* the input order does not matter.  Stable IDs are non-zero.               */
+/* ------------------------------------------------------------------------ */
+typedef struct swb_scene_vertex {        /* Vertex                        */
+    uint64_t id;
+    swb_vec3 position;                   /* m                             */
+} swb_scene_vertex;
+
+typedef struct swb_scene_fabric {        /* FabricMaterial                */
+    uint64_t id;
+    double warp_stiffness, weft_stiffness, shear_stiffness; /* N/m       */
+    double bending_stiffness;            /* N m (0: no hinge)             */
+    double areal_density;                /* kg/m^2                        */
+    double damping_seconds;
+    double porosity;                     /* fraction in [0, 1]            */
+    double permeability;                 /* m^2                           */
+} swb_scene_fabric;
+
+typedef struct swb_scene_triangle {      /* Triangle                      */
+    uint64_t id;
+    uint64_t vertex_ids[3];
+    double chart[3][2];                  /* material coordinates, m       */
+    uint64_t material_id;
+    uint64_t sheet_id;                   /* hinges only within one sheet   */
+} swb_scene_triangle;
+
+typedef struct swb_scene_seam_material { /* SeamMaterial                  */
+    uint64_t id;
+    double linear_density;               /* kg/m                          */
+    double axial_stiffness;              /* N                             */
+} swb_scene_seam_material;
+
+typedef struct swb_scene_seam {          /* Seam: two chains of `count`
+                                            vertex IDs in seam_vertex_ids */
+    uint64_t id;
+    uint64_t material_id;
+    uint64_t first_begin, second_begin, count;
+} swb_scene_seam;
+
+typedef struct swb_scene_line_material { /* LineMaterial                  */
+    uint64_t id;
+    double diameter, linear_density, axial_stiffness, drag_coefficient;
+} swb_scene_line_material;
+
+typedef struct swb_scene_pilot {         /* Pilot                         */
+    uint64_t id;
+    double mass;
+    swb_vec3 center_of_mass, linear_velocity;
+    swb_quat body_to_world;
+    swb_vec3 principal_inertia;
+} swb_scene_pilot;
+
+typedef struct swb_scene_junction {      /* SuspensionJunction            */
+    uint64_t id;
+    swb_vec3 position;
+    double mass;
+    uint32_t fixed;
+    uint32_t reserved;
+} swb_scene_junction;
+
+#define SWB_ATTACH_SURFACE_VERTEX 1u
+#define SWB_ATTACH_PILOT_HARNESS 2u
+#define SWB_ATTACH_JUNCTION 3u
+typedef struct swb_scene_attachment {    /* Attachment: one target by kind */
+    uint64_t id;
+    uint32_t kind;                       /* SWB_ATTACH_*                  */
+    uint32_t reserved;
+    uint64_t vertex_id, pilot_id, junction_id;
+    swb_vec3 pilot_local_position;
+} swb_scene_attachment;
+
+typedef struct swb_scene_line {          /* SuspensionLine                */
+    uint64_t id;
+    uint64_t start_attachment_id, end_attachment_id, material_id;
+    double rest_length;
+    uint32_t role;                       /* 1 suspension, 2 riser, 3 brake,
+                                            4 harness                     */
+    uint32_t reserved;
+} swb_scene_line;
+
+typedef struct swb_scene {
+    uint64_t vertex_count;          const swb_scene_vertex* vertices;
+    uint64_t fabric_count;          const swb_scene_fabric* fabrics;
+    uint64_t triangle_count;        const swb_scene_triangle* triangles;
+    uint64_t seam_material_count;   const swb_scene_seam_material* seam_materials;
+    uint64_t seam_count;            const swb_scene_seam* seams;
+    uint64_t seam_vertex_id_count;  const uint64_t* seam_vertex_ids;
+    uint64_t line_material_count;   const swb_scene_line_material* line_materials;
+    uint64_t pilot_count;           const swb_scene_pilot* pilots;
+    uint64_t junction_count;        const swb_scene_junction* junctions;
+    uint64_t attachment_count;      const swb_scene_attachment* attachments;
+    uint64_t line_count;            const swb_scene_line* lines;
+} swb_scene;
+
+typedef struct swb_scene_settings {      /* SceneStructureSettings        */
+    double seam_coincidence_tolerance;   /* 1e-9 m                        */
+    int32_t suspension_solver_iterations;/* 12                            */
+    uint32_t has_fabric_self_contact;
+    double suspension_attachment_tolerance;   /* 1e-10                    */
+    double suspension_minimum_line_length;    /* 1e-10 m                  */
+    double suspension_maximum_line_residual;  /* 2e-4 m                   */
+    double suspension_maximum_control_work;   /* 1e6 J                    */
+    swb_fabric_contact_def fabric_self_contact;
+} swb_scene_settings;
+
+/* The first diagnostic (in the reference's order: entity kind, stable ID,
+ * code, message) and the assembly totals. */
+typedef struct swb_scene_report {
+    uint32_t assembled;
+    uint32_t diagnostic_count;
+    uint32_t first_code;           /* SceneStructureDiagnosticCode: 1 invalid
+                                      scene, 2 mapping overflow, 3 material
+                                      incompatible, 4 degenerate material
+                                      coordinates, 5 zero-mass dynamic node,
+                                      6 unsupported pilot, 7 unsupported pilot
+                                      harness, 8 unsupported suspension
+                                      topology, 9 unsupported seam,
+                                      10 unsupported bending topology      */
+    uint32_t first_validation_code;/* scene ValidationCode for code 1, or 0 */
+    uint32_t first_entity_kind;    /* EntityKind (scene.h:239-253)         */
+    uint32_t reserved;
+    uint64_t first_entity_id;
+    double total_fabric_mass;      /* kg                                   */
+    double total_seam_mass;        /* kg                                   */
+    char first_message[160];
+} swb_scene_report;
+
+void swb_default_scene_settings(swb_scene_settings* out);
+/* Assembles `scene`; on success *out owns the definition (free with
+ * swb_definition_destroy).  A scene the reference refuses returns
+ * SWB_INVALID_ARGUMENT with *out NULL and the diagnostics in `report`
+ * (nullable). */
+swb_status swb_assemble_scene(const swb_scene* scene,
+                              const swb_scene_settings* settings,
+                              swb_definition** out,
+                              swb_scene_report* report);
+
 /* Copies an arbitrary definition into an owned one (for permutation). */
 swb_status swb_definition_copy(const swb_structure_definition* source,
                                swb_definition** out);

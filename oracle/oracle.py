@@ -49,6 +49,9 @@ _REF = {
     "swref_last_error": (C.c_char_p, []),
     "swref_physical_cores": (C.c_uint, []),
     "swref_last_error_detail": (C.c_int, [P(abi.ErrorDetail)]),
+    "swref_assemble_scene": (C.c_int, [P(abi.Scene), P(abi.SceneSettings), P(C.c_void_p), P(abi.SceneReport)]),
+    "swref_assembly_view": (P(abi.StructureDefinition), [C.c_void_p]),
+    "swref_assembly_destroy": (None, [C.c_void_p]),
     "swref_create": (C.c_int, [P(abi.StructureDefinition), P(C.c_void_p)]),
     "swref_destroy": (None, [C.c_void_p]),
     "swref_fingerprint": (C.c_uint64, [C.c_void_p]),
@@ -364,3 +367,25 @@ def ref_port_mass_flows(zones, ports, air=(287.05, 1.4)):
     status = ref_library().swref_port_mass_flows(C.byref(a), z.ctypes.data, len(z), p.ctypes.data, len(p),
                                                  out.ctypes.data, C.byref(failed))
     return status, out, failed.value
+
+
+class RefAssembly:
+    """The reference build's assembleSceneStructure of a scene: `report`, and
+    `pointer`/`view` of its definition (None when refused)."""
+
+    def __init__(self, scene, settings):
+        lib = ref_library()
+        self.report = abi.SceneReport()
+        self._h = C.c_void_p()
+        self.status = lib.swref_assemble_scene(C.byref(scene.view), C.byref(settings), C.byref(self._h),
+                                               C.byref(self.report))
+        self.view = lib.swref_assembly_view(self._h).contents if self._h.value else None
+
+    @property
+    def pointer(self):
+        return C.pointer(self.view)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            ref_library().swref_assembly_destroy(self._h)
+            self._h = C.c_void_p()

@@ -16,6 +16,8 @@
 #include "simwing_b200.h"
 
 #include "structure.h"
+#include "scene.h"
+#include "scene_structure.h"
 #include <softwing/parallel.h>
 #include <softwing/soft_body.h>
 #include <softwing/suspension.h>
@@ -267,9 +269,277 @@ StructureStepSettings convert(const swb_step_settings& s) {
 
 }  // namespace
 
+// A reference StructureDefinition held as the C-ABI's plain arrays.
+struct RefAssembly {
+    std::vector<swb_node_def> nodes;
+    std::vector<swb_triangle_def> triangles;
+    std::vector<swb_constraint_def> constraints;
+    std::vector<swb_membrane_def> membranes;
+    std::vector<swb_dihedral_def> dihedrals;
+    swb_fabric_contact_def contact{};
+    swb_suspension_def suspension{};
+    std::vector<swb_suspension_attachment> attachments;
+    std::vector<swb_suspension_junction> junctions;
+    std::vector<swb_pilot_harness> harness;
+    std::vector<swb_suspension_segment> segments;
+    swb_structure_definition view{};
+};
+
+void export_definition(const StructureDefinition& d, RefAssembly& a) {
+    for (const auto& n : d.nodes)
+        a.nodes.push_back({{n.positionMeters.x, n.positionMeters.y, n.positionMeters.z}, n.massKg,
+                           n.fixed ? 1u : 0u, 0u});
+    for (const auto& t : d.triangles) {
+        swb_triangle_def x{};
+        for (int k = 0; k < 3; ++k) x.nodes[k] = t.nodes[k];
+        a.triangles.push_back(x);
+    }
+    for (const auto& c : d.constraints)
+        a.constraints.push_back({static_cast<uint32_t>(c.kind), 0u, c.firstNode, c.secondNode, c.restLengthMeters,
+                                 c.complianceMetersPerNewton});
+    for (const auto& m : d.membranes) {
+        swb_membrane_def x{};
+        x.triangle = m.triangle;
+        for (int k = 0; k < 3; ++k) {
+            x.chart[k][0] = m.materialCoordinates[k].x;
+            x.chart[k][1] = m.materialCoordinates[k].y;
+        }
+        x.material.warp_stiffness = m.material.warpStiffnessNewtonsPerMeter;
+        x.material.weft_stiffness = m.material.weftStiffnessNewtonsPerMeter;
+        x.material.coupling_stiffness = m.material.couplingStiffnessNewtonsPerMeter;
+        x.material.shear_stiffness = m.material.shearStiffnessNewtonsPerMeter;
+        x.material.warp_pretension = m.material.warpPreTensionNewtonsPerMeter;
+        x.material.weft_pretension = m.material.weftPreTensionNewtonsPerMeter;
+        x.material.damping_seconds = m.material.dampingSeconds;
+        x.material.compression_stiffness_ratio = m.material.compressionStiffnessRatio;
+        x.role = static_cast<uint32_t>(m.role);
+        a.membranes.push_back(x);
+    }
+    for (const auto& h : d.dihedrals) {
+        swb_dihedral_def x{};
+        for (int k = 0; k < 4; ++k) x.nodes[k] = h.nodes[k];
+        x.rest_angle = h.restAngleRadians;
+        x.compliance = h.complianceRadiansPerNewtonMeter;
+        a.dihedrals.push_back(x);
+    }
+    a.view = swb_structure_definition{};
+    if (d.fabricSelfContact) {
+        const auto& c = *d.fabricSelfContact;
+        a.contact = {c.halfThicknessMeters, c.normalComplianceMetersPerNewton, c.staticFriction, c.dynamicFriction};
+        a.view.fabric_self_contact = &a.contact;
+    }
+    if (d.suspension) {
+        const auto& sd = *d.suspension;
+        swb_suspension_def& x = a.suspension;
+        x.pilot_stable_id = sd.pilotStableId;
+        x.pilot_mass = sd.pilotMassKg;
+        x.pilot_com_local = {sd.pilotCenterOfMassLocalMeters.x, sd.pilotCenterOfMassLocalMeters.y,
+                             sd.pilotCenterOfMassLocalMeters.z};
+        x.pilot_initial_com_world = {sd.pilotInitialCenterOfMassWorldMeters.x, sd.pilotInitialCenterOfMassWorldMeters.y,
+                                     sd.pilotInitialCenterOfMassWorldMeters.z};
+        x.pilot_initial_linear_velocity = {sd.pilotInitialLinearVelocityMetersPerSecond.x,
+                                           sd.pilotInitialLinearVelocityMetersPerSecond.y,
+                                           sd.pilotInitialLinearVelocityMetersPerSecond.z};
+        x.pilot_initial_angular_velocity = {sd.pilotInitialAngularVelocityRadiansPerSecond.x,
+                                            sd.pilotInitialAngularVelocityRadiansPerSecond.y,
+                                            sd.pilotInitialAngularVelocityRadiansPerSecond.z};
+        x.pilot_initial_body_to_world = {sd.pilotInitialBodyToWorld.w, sd.pilotInitialBodyToWorld.x,
+                                         sd.pilotInitialBodyToWorld.y, sd.pilotInitialBodyToWorld.z};
+        x.pilot_principal_inertia = {sd.pilotPrincipalInertiaKgSquareMeters.x, sd.pilotPrincipalInertiaKgSquareMeters.y,
+                                     sd.pilotPrincipalInertiaKgSquareMeters.z};
+        for (const auto& t : sd.attachments) a.attachments.push_back({t.stableId, t.node});
+        for (const auto& j : sd.junctions) a.junctions.push_back({j.stableId, j.node});
+        for (const auto& h : sd.harnessPoints)
+            a.harness.push_back({h.stableId, {h.localPositionMeters.x, h.localPositionMeters.y, h.localPositionMeters.z}});
+        for (const auto& g : sd.segments) {
+            swb_suspension_segment y{};
+            y.stable_id = g.stableId;
+            y.from = {static_cast<uint32_t>(g.from.kind), 0u, g.from.stableId};
+            y.to = {static_cast<uint32_t>(g.to.kind), 0u, g.to.stableId};
+            y.rest_length = g.restLengthMeters;
+            y.axial_stiffness = g.axialStiffnessNewtons;
+            y.axial_damping = g.axialDampingNewtonSecondsPerMeter;
+            y.role = g.role;
+            a.segments.push_back(y);
+        }
+        x.attachment_count = a.attachments.size();
+        x.attachments = a.attachments.data();
+        x.junction_count = a.junctions.size();
+        x.junctions = a.junctions.data();
+        x.harness_count = a.harness.size();
+        x.harness_points = a.harness.data();
+        x.segment_count = a.segments.size();
+        x.segments = a.segments.data();
+        x.solver_iterations = sd.solverIterations;
+        x.attachment_tolerance = sd.attachmentTolerance;
+        x.minimum_line_length = sd.minimumLineLengthMeters;
+        x.maximum_line_residual = sd.maximumLineResidualMeters;
+        x.maximum_control_work = sd.maximumControlWorkJoules;
+        a.view.suspension = &a.suspension;
+    }
+    a.view.node_count = a.nodes.size();
+    a.view.nodes = a.nodes.data();
+    a.view.triangle_count = a.triangles.size();
+    a.view.triangles = a.triangles.data();
+    a.view.constraint_count = a.constraints.size();
+    a.view.constraints = a.constraints.data();
+    a.view.membrane_count = a.membranes.size();
+    a.view.membranes = a.membranes.data();
+    a.view.dihedral_count = a.dihedrals.size();
+    a.view.dihedrals = a.dihedrals.data();
+}
+
+// The reference Scene of a swb_scene: the structural fields as given, plus
+// what validateScene wants that a swb_scene does not carry (metadata, one
+// outside and one cell region on the two sides of every triangle, names).
+Scene scene_of(const swb_scene& c) {
+    Scene s;
+    s.metadata.designChecksum = "synthetic";
+    s.metadata.exporterVersion = "synthetic";
+    s.regions.push_back({1, RegionKind::Outside, "outside"});
+    s.regions.push_back({2, RegionKind::Cell, "cell"});
+    for (uint64_t i = 0; i < c.vertex_count; ++i)
+        s.vertices.push_back({c.vertices[i].id, {c.vertices[i].position.x, c.vertices[i].position.y,
+                                                 c.vertices[i].position.z}});
+    for (uint64_t i = 0; i < c.fabric_count; ++i) {
+        const swb_scene_fabric& f = c.fabrics[i];
+        FabricMaterial m;
+        m.id = f.id;
+        m.name = "fabric";
+        m.warpStiffnessNewtonsPerMeter = f.warp_stiffness;
+        m.weftStiffnessNewtonsPerMeter = f.weft_stiffness;
+        m.shearStiffnessNewtonsPerMeter = f.shear_stiffness;
+        m.bendingStiffnessNewtonMeters = f.bending_stiffness;
+        m.arealDensityKgPerSquareMeter = f.areal_density;
+        m.dampingSeconds = f.damping_seconds;
+        m.porosityFraction = f.porosity;
+        m.permeabilitySquareMeters = f.permeability;
+        s.fabricMaterials.push_back(m);
+    }
+    for (uint64_t i = 0; i < c.triangle_count; ++i) {
+        const swb_scene_triangle& t = c.triangles[i];
+        Triangle x;
+        x.id = t.id;
+        for (int k = 0; k < 3; ++k) {
+            x.vertexIds[k] = t.vertex_ids[k];
+            x.materialCoordinates[k] = {t.chart[k][0], t.chart[k][1]};
+        }
+        x.negativeSideRegionId = 2;
+        x.positiveSideRegionId = 1;
+        x.materialId = t.material_id;
+        x.sheetId = t.sheet_id;
+        x.role = SurfaceRole::Skin;
+        s.triangles.push_back(x);
+    }
+    for (uint64_t i = 0; i < c.seam_material_count; ++i)
+        s.seamMaterials.push_back({c.seam_materials[i].id, "seam", c.seam_materials[i].linear_density,
+                                   c.seam_materials[i].axial_stiffness});
+    for (uint64_t i = 0; i < c.seam_count; ++i) {
+        const swb_scene_seam& m = c.seams[i];
+        Seam x;
+        x.id = m.id;
+        x.materialId = m.material_id;
+        x.firstOrderedVertexIds.assign(c.seam_vertex_ids + m.first_begin, c.seam_vertex_ids + m.first_begin + m.count);
+        x.secondOrderedVertexIds.assign(c.seam_vertex_ids + m.second_begin,
+                                        c.seam_vertex_ids + m.second_begin + m.count);
+        s.seams.push_back(x);
+    }
+    for (uint64_t i = 0; i < c.line_material_count; ++i) {
+        const swb_scene_line_material& m = c.line_materials[i];
+        s.lineMaterials.push_back({m.id, "line", m.diameter, m.linear_density, m.axial_stiffness, m.drag_coefficient});
+    }
+    for (uint64_t i = 0; i < c.pilot_count; ++i) {
+        const swb_scene_pilot& p = c.pilots[i];
+        Pilot x;
+        x.id = p.id;
+        x.name = "pilot";
+        x.massKg = p.mass;
+        x.centerOfMassPositionMeters = {p.center_of_mass.x, p.center_of_mass.y, p.center_of_mass.z};
+        x.linearVelocityMetersPerSecond = {p.linear_velocity.x, p.linear_velocity.y, p.linear_velocity.z};
+        x.bodyToWorld = {p.body_to_world.w, p.body_to_world.x, p.body_to_world.y, p.body_to_world.z};
+        x.principalInertiaKgSquareMeters = {p.principal_inertia.x, p.principal_inertia.y, p.principal_inertia.z};
+        s.pilots.push_back(x);
+    }
+    for (uint64_t i = 0; i < c.junction_count; ++i) {
+        const swb_scene_junction& j = c.junctions[i];
+        s.suspensionJunctions.push_back({j.id, {j.position.x, j.position.y, j.position.z}, j.mass, j.fixed != 0});
+    }
+    for (uint64_t i = 0; i < c.attachment_count; ++i) {
+        const swb_scene_attachment& a = c.attachments[i];
+        Attachment x;
+        x.id = a.id;
+        x.kind = static_cast<AttachmentKind>(a.kind);
+        x.vertexId = a.vertex_id;
+        x.pilotId = a.pilot_id;
+        x.pilotLocalPositionMeters = {a.pilot_local_position.x, a.pilot_local_position.y, a.pilot_local_position.z};
+        x.suspensionJunctionId = a.junction_id;
+        s.attachments.push_back(x);
+    }
+    for (uint64_t i = 0; i < c.line_count; ++i) {
+        const swb_scene_line& l = c.lines[i];
+        SuspensionLine x;
+        x.id = l.id;
+        x.startAttachmentId = l.start_attachment_id;
+        x.endAttachmentId = l.end_attachment_id;
+        x.materialId = l.material_id;
+        x.restLengthMeters = l.rest_length;
+        x.role = static_cast<SuspensionLineRole>(l.role);
+        s.suspensionLines.push_back(x);
+    }
+    return s;
+}
+
 extern "C" {
 
 const char* swref_last_error(void) { return g_error.c_str(); }
+
+// assembleSceneStructure on the reference build: the definition (valid
+// until swref_assembly_destroy) and the first diagnostic.
+int swref_assemble_scene(const swb_scene* scene, const swb_scene_settings* settings, void** out,
+                         swb_scene_report* report) {
+    try {
+        *out = nullptr;
+        SceneStructureSettings st;
+        st.seamCoincidenceToleranceMeters = settings->seam_coincidence_tolerance;
+        st.suspensionSolverIterations = settings->suspension_solver_iterations;
+        st.suspensionAttachmentTolerance = settings->suspension_attachment_tolerance;
+        st.suspensionMinimumLineLengthMeters = settings->suspension_minimum_line_length;
+        st.suspensionMaximumLineResidualMeters = settings->suspension_maximum_line_residual;
+        st.suspensionMaximumControlWorkJoules = settings->suspension_maximum_control_work;
+        if (settings->has_fabric_self_contact) {
+            const auto& c = settings->fabric_self_contact;
+            st.fabricSelfContact = StructureFabricContactDefinition{c.half_thickness, c.normal_compliance,
+                                                                    c.static_friction, c.dynamic_friction};
+        }
+        const SceneStructureAssembly a = assembleSceneStructure(scene_of(*scene), {}, st);
+        std::memset(report, 0, sizeof(*report));
+        report->diagnostic_count = static_cast<uint32_t>(a.diagnostics.size());
+        if (!a.diagnostics.empty()) {
+            const auto& d = a.diagnostics.front();
+            report->first_code = static_cast<uint32_t>(d.code);
+            report->first_validation_code = d.sceneValidationCode ? static_cast<uint32_t>(*d.sceneValidationCode) : 0u;
+            report->first_entity_kind = static_cast<uint32_t>(d.entityKind);
+            report->first_entity_id = d.entityId;
+            std::snprintf(report->first_message, sizeof report->first_message, "%s", d.message.c_str());
+        }
+        if (!a.ok()) return SWB_INVALID_ARGUMENT;
+        report->assembled = 1;
+        report->total_fabric_mass = a.totalFabricMassKg;
+        report->total_seam_mass = a.totalSeamMassKg;
+        auto* r = new RefAssembly;
+        export_definition(a.definition, *r);
+        *out = r;
+        return SWB_OK;
+    } catch (...) {
+        return translate();
+    }
+}
+
+const swb_structure_definition* swref_assembly_view(void* assembly) {
+    return &static_cast<RefAssembly*>(assembly)->view;
+}
+
+void swref_assembly_destroy(void* assembly) { delete static_cast<RefAssembly*>(assembly); }
 
 int swref_last_error_detail(swb_error_detail* out) {
     if (!out) return SWB_INVALID_ARGUMENT;

@@ -390,6 +390,43 @@ def generate_calibration_wing(**overrides) -> Definition:
     return generate_wing(**dict(CALIBRATION_WING, **overrides))
 
 
+class SceneArrays:
+    """A swb_scene over ctypes arrays (kept alive here): `items` maps each
+    array name of abi.SCENE_ARRAYS to a list of its ctypes records (or, for
+    seam_vertex_id, of IDs)."""
+
+    def __init__(self, **items):
+        self.view = abi.Scene()
+        self._keep = []
+        for name, ctype, field in abi.SCENE_ARRAYS:
+            values = items.get(name, [])
+            arr = (ctype * max(len(values), 1))(*values)
+            self._keep.append(arr)
+            setattr(self.view, name + "_count", len(values))
+            setattr(self.view, field, C.cast(arr, C.POINTER(ctype)))
+
+
+def SceneSettings(**overrides) -> abi.SceneSettings:
+    s = abi.SceneSettings()
+    abi.library().swb_default_scene_settings(C.byref(s))
+    for key, value in overrides.items():
+        setattr(s, key, value)
+    return s
+
+
+def assemble_scene(scene: SceneArrays, settings: abi.SceneSettings | None = None):
+    """simwing::fsi::assembleSceneStructure (scene_structure.cpp:894-1284):
+    returns (Definition or None when refused, the report)."""
+    report = abi.SceneReport()
+    out = C.c_void_p()
+    st = settings if settings is not None else SceneSettings()
+    status = abi.library().swb_assemble_scene(C.byref(scene.view), C.byref(st), C.byref(out), C.byref(report))
+    if status == abi.INVALID_ARGUMENT and not report.assembled and report.diagnostic_count:
+        return None, report
+    _check(status)
+    return Definition(out.value), report
+
+
 def wing_batch_parameters(count: int = 64, seed: int = 2024):
     """Seeded uneven wing sizes of the batched workload: cells ~ U{20..60},
     chordwise in {30, 45, 60}, aspect ratio ~ U(4.5, 7), per-wing compliance

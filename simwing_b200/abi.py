@@ -116,6 +116,85 @@ class ContactKey(C.Structure):
                 ("first", C.c_uint64 * 3), ("second", C.c_uint64 * 3)]
 
 
+# Scene assembly (swb_assemble_scene)
+class SceneVertex(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("position", Vec3)]
+
+
+class SceneFabric(C.Structure):
+    _fields_ = [("id", C.c_uint64)] + [(n, C.c_double) for n in (
+        "warp_stiffness", "weft_stiffness", "shear_stiffness", "bending_stiffness", "areal_density",
+        "damping_seconds", "porosity", "permeability")]
+
+
+class SceneTriangle(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("vertex_ids", C.c_uint64 * 3), ("chart", (C.c_double * 2) * 3),
+                ("material_id", C.c_uint64), ("sheet_id", C.c_uint64)]
+
+
+class SceneSeamMaterial(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("linear_density", C.c_double), ("axial_stiffness", C.c_double)]
+
+
+class SceneSeam(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("id", "material_id", "first_begin", "second_begin", "count")]
+
+
+class SceneLineMaterial(C.Structure):
+    _fields_ = [("id", C.c_uint64)] + [(n, C.c_double) for n in (
+        "diameter", "linear_density", "axial_stiffness", "drag_coefficient")]
+
+
+class ScenePilot(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("mass", C.c_double), ("center_of_mass", Vec3), ("linear_velocity", Vec3),
+                ("body_to_world", Quat), ("principal_inertia", Vec3)]
+
+
+class SceneJunction(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("position", Vec3), ("mass", C.c_double), ("fixed", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+ATTACH_SURFACE_VERTEX, ATTACH_PILOT_HARNESS, ATTACH_JUNCTION = 1, 2, 3
+
+
+class SceneAttachment(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("kind", C.c_uint32), ("reserved", C.c_uint32), ("vertex_id", C.c_uint64),
+                ("pilot_id", C.c_uint64), ("junction_id", C.c_uint64), ("pilot_local_position", Vec3)]
+
+
+class SceneLine(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("id", "start_attachment_id", "end_attachment_id", "material_id")] + \
+               [("rest_length", C.c_double), ("role", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+SCENE_ARRAYS = (("vertex", SceneVertex, "vertices"), ("fabric", SceneFabric, "fabrics"),
+                ("triangle", SceneTriangle, "triangles"), ("seam_material", SceneSeamMaterial, "seam_materials"),
+                ("seam", SceneSeam, "seams"), ("seam_vertex_id", C.c_uint64, "seam_vertex_ids"),
+                ("line_material", SceneLineMaterial, "line_materials"), ("pilot", ScenePilot, "pilots"),
+                ("junction", SceneJunction, "junctions"), ("attachment", SceneAttachment, "attachments"),
+                ("line", SceneLine, "lines"))
+
+
+class Scene(C.Structure):
+    _fields_ = [f for name, ctype, field in SCENE_ARRAYS for f in ((name + "_count", C.c_uint64),
+                                                                   (field, C.POINTER(ctype)))]
+
+
+class SceneSettings(C.Structure):
+    _fields_ = [("seam_coincidence_tolerance", C.c_double), ("suspension_solver_iterations", C.c_int32),
+                ("has_fabric_self_contact", C.c_uint32), ("suspension_attachment_tolerance", C.c_double),
+                ("suspension_minimum_line_length", C.c_double), ("suspension_maximum_line_residual", C.c_double),
+                ("suspension_maximum_control_work", C.c_double), ("fabric_self_contact", FabricContactDef)]
+
+
+class SceneReport(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("assembled", "diagnostic_count", "first_code", "first_validation_code",
+                                           "first_entity_kind", "reserved")] + \
+               [("first_entity_id", C.c_uint64), ("total_fabric_mass", C.c_double), ("total_seam_mass", C.c_double),
+                ("first_message", C.c_char * 160)]
+
+
 # softwing::SuspensionPhase in declaration order (suspension.h:27-38)
 SUSPENSION_PHASES = ("Parse", "Validation", "AttachmentResolution", "GraphConstruction", "Control", "Prediction",
                      "LineSolve", "GroundSolve", "Certification", "Diagnostics")
@@ -304,6 +383,8 @@ _PROTOTYPES = {
     "swb_plan_schedule": (C.c_int, [P(StructureDefinition), P(SolverOptions), P(ScheduleReport), C.c_void_p,
                                     C.c_void_p]),
     "swb_plan_membrane_order": (C.c_int, [P(StructureDefinition), P(SolverOptions), C.c_void_p]),
+    "swb_default_scene_settings": (None, [P(SceneSettings)]),
+    "swb_assemble_scene": (C.c_int, [P(Scene), P(SceneSettings), P(C.c_void_p), P(SceneReport)]),
     "swb_structure_autotune_report": (C.c_int, [C.c_void_p, P(AutotuneReport)]),
     "swb_default_batch_options": (None, [P(BatchOptions)]),
     "swb_batch_create": (C.c_int, [C.c_void_p, C.c_uint64, P(BatchOptions), P(C.c_void_p)]),
