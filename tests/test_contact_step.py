@@ -213,17 +213,21 @@ def test_candidate_inspection_needs_contact(cuda_device):
         s.contact_candidates()
 
 
-def test_contact_checkpoint_replay_is_bitwise(cuda_device):
+@pytest.mark.parametrize("name,warm", [("two_sheets", 0), ("stacked_hard", 2)])
+def test_contact_checkpoint_replay_is_bitwise(cuda_device, name, warm):
     """The checkpoint image carries the contact multiplier table (the warm
     starts and the record book that carry over between steps, as
     SoftBodyCheckpoint::State holds contactMultipliers and contactRecords)
     and the contact diagnostics: replay after a restore is bit for bit.  The
     reference's own contact checkpoint fixture (two sheets inside each
-    other's envelope, simwing_structure_test.cpp:297-329)."""
-    d = two_sheets()
-    st = step_settings(iterations=4)
+    other's envelope, simwing_structure_test.cpp:297-329), whose contact is
+    active in the first step, checkpointed before it; and the resting
+    stacked sheets, checkpointed after two steps, whose contacts stay active
+    (with warm-started multipliers) in the replayed steps."""
+    make, st, _, _, _ = CASES[name]
+    d = make()
     s = sw.Structure(d)
-    for _ in range(2):
+    for _ in range(warm):
         s.step(st)
     image = s.checkpoint()
     first = [s.step(st) for _ in range(3)]
@@ -235,7 +239,7 @@ def test_contact_checkpoint_replay_is_bitwise(cuda_device):
     for a, b in zip(first, again):
         assert a.active_contact_count == b.active_contact_count
         assert a.maximum_contact_penetration == b.maximum_contact_penetration
-    assert any(a.active_contact_count > 0 for a in first)
+    assert first[0].active_contact_count > 0 if warm == 0 else all(a.active_contact_count > 0 for a in first)
     # a tampered image is refused, the state untouched
     bad = bytearray(image)
     bad[-60] ^= 0x40
@@ -262,6 +266,9 @@ def test_failed_contact_step_restores_the_multiplier_table(cuda_device, failure)
     before = tried.checkpoint()
     # the compliant stacked sheets' fourth step fails in the swept query, as
     # the reference's does (see CASES)
-    with pytest.raises(sw.ContactStepError if failure == "contact" else sw.NonFiniteState):
+    # a non-finite prediction is refused by the contact broadphase (its
+    # inputs must be finite) or by the finite-state check, whichever reads it
+    # first; either way the step fails as a whole
+    with pytest.raises(sw.ContactStepError if failure == "contact" else (sw.NonFiniteState, sw.ContactStepError)):
         tried.step(SLIDE)
     assert tried.checkpoint() == before == twin.checkpoint()
