@@ -146,32 +146,55 @@ def membrane_wing_leg(sw, st, steps, device, flush):
 
 
 def contact_leg(sw, steps, device, reference_steps, with_reference):
-    """Fabric self-contact: two stacked 16 x 16 sheets (512 nodes, 900
-    triangles), the free one 1 mm inside the contact envelope of the pinned
-    one, compliant contact (1e-3 m/N) with friction, 8 iterations, tilted
-    gravity.  One step from the same initial state, repeated (the state is
-    restored between steps: the reference's swept query gives up on
-    persistent resting contact after a few steps).  Device time from CUDA
-    events; the reference build's Structure timed on the host beside it."""
-    d = sw.stacked_sheets(n=16, compliance=1e-3)
+    """Fabric self-contact: two stacked sheets, the free one 1 mm inside the
+    contact envelope of the pinned one, compliant contact (1e-3 m/N) with
+    friction, 8 iterations, tilted gravity.  16 x 16 (512 nodes, 900
+    triangles): one step from the same initial state, repeated (the state
+    is restored between steps), the reference build's Structure timed on
+    the host beside it.  80 x 80 (12,800 nodes, 24,964 triangles, the
+    contact configuration's size): the first step from rest (restored and
+    repeated) and the steps that follow it, consecutive, until the swept
+    query gives up on the persistent resting contact (as the reference's
+    does after a few steps) or four steps.  Device time from CUDA events."""
     st = sw.StepSettings(time_step=1.0 / 120.0, substeps=1, constraint_iterations=8, gravity=(2.0, 0.0, -9.81),
                          velocity_damping=0.25)
+
+    def first_step(s, repeats):
+        image = s.checkpoint()
+        for _ in range(2):
+            s.step(st, diagnostics=False)
+            s.restore(image)
+        times = []
+        for _ in range(repeats):
+            s.step(st, diagnostics=False)
+            times.append(s.last_step_ms())
+            s.restore(image)
+        return float(sum(times)) / len(times)
+
+    d = sw.stacked_sheets(n=16, compliance=1e-3)
     s = sw.Structure(d, sw.SolverOptions(device=device))
-    image = s.checkpoint()
-    for _ in range(3):
-        s.step(st, diagnostics=False)
-        s.restore(image)
-    times = []
-    for _ in range(steps):
-        s.step(st, diagnostics=False)
-        times.append(s.last_step_ms())
-        s.restore(image)
+    first = first_step(s, steps)
     diag = s.step(st)
     s.close()
     out = {"workload": "stacked 16x16 sheets, compliant fabric self-contact with friction, 8 iterations, "
                        "one step from rest", "nodes": d.counts()["nodes"], "triangles": d.counts()["triangles"],
-           "active_contacts": int(diag.active_contact_count), "steps": steps,
-           "device_ms_per_step": float(sum(times)) / steps}
+           "active_contacts": int(diag.active_contact_count), "steps": steps, "device_ms_per_step": first}
+    big = sw.stacked_sheets(n=80, compliance=1e-3)
+    s = sw.Structure(big, sw.SolverOptions(device=device))
+    first = first_step(s, 3)
+    consecutive = []
+    try:
+        s.step(st, diagnostics=False)
+        for _ in range(3):
+            s.step(st, diagnostics=False)
+            consecutive.append(s.last_step_ms())
+    except sw.ContactStepError:
+        pass
+    s.close()
+    out["sheets_80x80"] = {"triangles": big.counts()["triangles"], "nodes": big.counts()["nodes"],
+                           "first_step_ms": first, "consecutive_steps": len(consecutive),
+                           "consecutive_ms_per_step": float(sum(consecutive)) / len(consecutive) if consecutive
+                           else None}
     if with_reference:
         from oracle import oracle as O
 

@@ -322,11 +322,11 @@ enum {
     SWB_OPT_NO_GRAPH = 1u << 1,    /* batched: launch without CUDA graphs    */
     SWB_OPT_GRID = 1u << 2,        /* force the grid schedule                */
     SWB_OPT_SPLIT_STAGES = 1u << 3, /* cluster schedule with split stages:
-                                      interior constraints coloured per CTA
-                                      behind CTA barriers, cluster barriers
-                                      only where constraints span CTAs (fewer
-                                      cluster barriers, more stages)         */
-    SWB_OPT_AUTOTUNE = 1u << 4     /* swb_structure_create builds the cluster
+                                      stages of records that touch only the
+                                      executing CTA's patch behind CTA
+                                      barriers, cluster barriers after the
+                                      stages of records that span CTAs       */
+    SWB_OPT_AUTOTUNE = 1u << 4,    /* swb_structure_create builds the cluster
                                       schedule for several block sizes (the
                                       widest stage, 512, 768 threads), with
                                       and without split stages and on the
@@ -339,6 +339,14 @@ enum {
                                       and 768 threads) and with SWB_OPT_GRID.
                                       swb_structure_autotune_report lists
                                       the candidates.                         */
+    SWB_OPT_CONTACT_ONE_CLUSTER = 1u << 5 /* fabric self-contact: run the
+                                      detection phases (broadphase, swept
+                                      queries) on the structure's cluster
+                                      alone; by default, on surfaces of
+                                      16,384 vertices and edges or more,
+                                      clusters beside it join them (a
+                                      cooperative launch), with results bit
+                                      for bit the same                       */
 };
 
 void swb_default_solver_options(swb_solver_options* out);
@@ -438,6 +446,15 @@ swb_status swb_diagnostics_noalloc(int32_t device,
                                    const uint8_t* kinds,
                                    uint64_t constraint_count,
                                    swb_diagnostics* out);
+
+/* The device forms of the step's two short math functions on host arrays
+ * (no counterpart in the reference; for checking them on the GPU they run
+ * on): which = SWB_FAST_ATAN2 gives out[i] = atan2(a[i], b[i]) by the
+ * device's polynomial form, SWB_FAST_RCP gives out[i] = 1 / a[i] by the
+ * approximate reciprocal.  count may be 0. */
+#define SWB_FAST_ATAN2 0u
+#define SWB_FAST_RCP 1u
+swb_status swb_fast_math_eval(uint32_t which, const float* a, const float* b, float* out, uint64_t count);
 
 /* Structure::nodeStates (structure.h:288, structure.cpp:725-734). */
 swb_status swb_structure_read_nodes(const swb_structure* structure,

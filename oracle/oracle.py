@@ -213,6 +213,80 @@ class PortStructure(_Base):
         return out
 
 
+class RecentredF32:
+    """The FP32-rounded restatement (PortStructure(float_vectors=True)) in
+    the frame the device keeps: FP32 coordinates relative to an FP64 origin
+    on a 1/256 m grid, which starts at the pilot's centre of mass (the
+    centre of the nodes' bounding box without a pilot) and moves to the
+    pilot's grid point after every step in which the pilot has left the
+    origin by more than a quarter metre.  Its long runs show how far FP32
+    arithmetic of the reference algorithm itself drifts from the FP64
+    run.  positions() and the diagnostics' centre of mass are in world
+    coordinates."""
+
+    def __init__(self, definition):
+        self._s = PortStructure(definition, float_vectors=True)
+        v = definition.view
+        if v.suspension:
+            c = v.suspension.contents.pilot_initial_com_world
+            o = np.array([c.x, c.y, c.z])
+        else:
+            x = self._s.positions()
+            o = 0.5 * (x.min(axis=0) + x.max(axis=0))
+        self.origin = np.zeros(3)
+        self._has_pilot = bool(v.suspension)
+        self._shift(np.round(o * 256.0) / 256.0)
+
+    def _shift(self, d):
+        s = self._s.node_states()
+        s[:, 0:2, :] -= d
+        self._s.write_node_states(s)
+        if self._has_pilot:
+            p = self._s.payload()[0]
+            c = p.center_of_mass
+            self._s.write_payload(abi.PayloadState(abi.Vec3(c.x - d[0], c.y - d[1], c.z - d[2]), p.body_to_world,
+                                                   p.linear_velocity, p.angular_velocity))
+        self.origin = self.origin + d
+
+    def write_state(self, states, payload=None):
+        """Node states (and the pilot's state) in world coordinates; the
+        origin moves to the pilot's grid point (to the bounding-box centre
+        without a pilot)."""
+        s = np.array(states, dtype=np.float64)
+        if payload is not None:
+            c = payload.center_of_mass
+            o = np.array([c.x, c.y, c.z])
+        else:
+            o = 0.5 * (s[:, 0, :].min(axis=0) + s[:, 0, :].max(axis=0))
+        o = np.round(o * 256.0) / 256.0
+        # as the device stores them: FP32 offsets and velocities
+        s[:, 0:2, :] = (s[:, 0:2, :] - o).astype(np.float32)
+        s[:, 2, :] = s[:, 2, :].astype(np.float32)
+        self._s.write_node_states(s)
+        if payload is not None:
+            c = payload.center_of_mass
+            self._s.write_payload(abi.PayloadState(abi.Vec3(c.x - o[0], c.y - o[1], c.z - o[2]), payload.body_to_world,
+                                                   payload.linear_velocity, payload.angular_velocity))
+        self.origin = o
+
+    def step(self, settings):
+        g = self._s.step(settings)
+        c = g.center_of_mass
+        g.center_of_mass = abi.Vec3(c.x + self.origin[0], c.y + self.origin[1], c.z + self.origin[2])
+        if self._has_pilot:
+            pc = self._s.payload()[0].center_of_mass
+            pc = np.array([pc.x, pc.y, pc.z])
+            if np.abs(pc).max() > 0.25:
+                self._shift(np.round(pc * 256.0) / 256.0)
+        return g
+
+    def positions(self):
+        return self._s.positions() + self.origin
+
+    def close(self):
+        self._s.close()
+
+
 class RefStructure(_Base):
     """The reference's own Structure adapter (FP64, compiled from source)."""
     _prefix = "swref_"

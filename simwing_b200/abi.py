@@ -326,12 +326,14 @@ class WingParams(C.Structure):
                 ("attachments_per_cell", C.c_uint32)]
 
 
+FAST_ATAN2, FAST_RCP = 0, 1
+
 # status codes
 OK, INVALID_ARGUMENT, OUT_OF_RANGE, SUSPENSION_ERROR, CONTACT_ERROR, NON_FINITE, SYNC_TIMEOUT, \
     CUDA_ERROR, UNSUPPORTED, OUT_OF_MEMORY = range(10)
 
 DISTANCE, CABLE, SUSPENSION_TIE, SEAM_STITCH = 1, 2, 3, 4
-OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID, OPT_SPLIT_STAGES, OPT_AUTOTUNE = 1, 2, 4, 8, 16
+OPT_GLOBAL_ONLY, OPT_NO_GRAPH, OPT_GRID, OPT_SPLIT_STAGES, OPT_AUTOTUNE, OPT_CONTACT_ONE_CLUSTER = 1, 2, 4, 8, 16, 32
 
 
 class AutotuneCandidate(C.Structure):
@@ -368,6 +370,7 @@ _PROTOTYPES = {
     "swb_structure_diagnostics": (C.c_int, [C.c_void_p, P(Diagnostics)]),
     "swb_diagnostics_noalloc": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, P(Diagnostics)]),
+    "swb_fast_math_eval": (C.c_int, [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64]),
     "swb_structure_read_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swb_structure_read_positions_f32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swb_structure_write_nodes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),

@@ -295,6 +295,28 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     __shared__ double mom_pred[kMomentumFields], mom_cur[kMomentumFields];
     __shared__ double mom_ptot[kMomentumFields], mom_tot[kMomentumFields];
     cg::cluster_group cluster = cg::this_cluster();
+    if constexpr (kContact) {
+        // a helper cluster of a contact launch: only the detection phases
+        if (blockIdx.x >= static_cast<unsigned>(p.ctas)) {
+            const ClusterInstance& I0 = p.instances[0];
+            ContactCtx h{};
+            h.C = I0.contact;
+            h.me = cluster.block_rank();
+            h.ctas = p.ctas;
+            h.pos_in = I0.pos_in;
+            for (int k = 0; k < 3; ++k) h.o[k] = I0.origin_in[k];
+            h.dt = p.dt64;
+            h.status = I0.status;
+            h.grank = blockIdx.x;
+            h.gctas = gridDim.x;
+            h.helpers = p.helper_clusters;
+            h.grid = p.grid;
+            h.grid.status = I0.status;
+            h.grid.blocks = gridDim.x;
+            contact_helper(h, cluster, p.iterations);
+            return;
+        }
+    }
     ClusterSlot slot{};
     if constexpr (kPacked) {
         slot = p.slots[blockIdx.x];
@@ -357,8 +379,13 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         cctx.dt = p.dt64;
         cctx.status = I.status;
         cctx.x_base = smem_addr(x);
-        cctx.node_level = p.smem_levels ? reinterpret_cast<uint32_t*>(smem + p.smem_levels) : I.contact->node_level;
         cctx.v_delta = smem_addr(v) - smem_addr(x);
+        cctx.grank = me;
+        cctx.gctas = gridDim.x;
+        cctx.helpers = p.helper_clusters;
+        cctx.grid = p.grid;
+        cctx.grid.status = I.status;
+        cctx.grid.blocks = gridDim.x;
         // multipliers and records restart every substep (beginContactSubstep,
         // contact.cpp:1043-1055)
         if (me == 0 && tid == 0) {
@@ -470,7 +497,6 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     next.index = ~0u;
     if (p.iterations > 0 && S > 0) next = load_record(recs(kind_of(0)), stage_lo(0) + tid, stage_hi(0));
     const uint64_t sync0 = I.kind[0].sync_mask, sync1 = I.kind[1].sync_mask;
-    const int interior0 = I.kind[0].interior_stages, interior1 = I.kind[1].interior_stages;
     // line iteration beside the last two stages: neither touches a
     // suspension endpoint node, so running it there gives the same result as
     // running it after them.  The last warp of the suspension CTA (no record
@@ -525,19 +551,16 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             } else if constexpr (kPacked) {
                 cluster.sync();
             } else {
-                // split stages: a cluster barrier where the next stage may read
-                // what another CTA wrote, else a CTA barrier (after the
-                // single-CTA tail's writes to peer nodes are made visible);
+                // split stages: a CTA barrier between two stages of records
+                // that touch only the CTA's own patch, else a cluster barrier;
                 // membrane stages are classic
                 const int kind = kind_of(g);
                 const int gl = local_of(g);
                 const uint64_t mask = kind == 0 ? sync0 : sync1;
-                if (kind == 2 || gl >= 64 || ((mask >> gl) & 1ull)) {
+                if (kind == 2 || gl >= 64 || ((mask >> gl) & 1ull))
                     cluster.sync();
-                } else {
-                    if (gl >= (kind ? interior1 : interior0)) asm volatile("fence.acq_rel.cluster;" ::: "memory");
+                else
                     __syncthreads();
-                }
             }
         }
         if (susp_c && line_stage < 0) {

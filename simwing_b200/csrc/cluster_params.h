@@ -118,12 +118,6 @@ struct ContactDev {
     // level schedule of a key-ordered pass: an item's level is one more than
     // the last level among the earlier items sharing one of its nodes, so
     // the items of a level share no node and run together
-    uint32_t* node_level;              // [slots]
-    uint32_t* item_level;              // [cand_cap]
-    uint32_t* level_start;             // [cand_cap + 2]
-    uint32_t* level_fill;              // [cand_cap + 2]
-    uint32_t* level_items;             // [cand_cap]
-    uint32_t* level_meta;              // [0] levels
     uint32_t* hit;                     // [cand_cap] the candidates in contact, in key order
     // binned broadphase: the triangles (for vertex rows) and the edges (for
     // edge rows) bucketed by the low end of their boxes along `axis`
@@ -145,15 +139,17 @@ struct ContactDev {
     unsigned long long* reduce;        // [2] active records, largest penetration (bits)
     unsigned long long* fail;          // [1] the failing feature first in key order, packed with its
                                        // detail code (contact_fail_at); all ones when none failed
-    // cluster-wide levels of a key-ordered pass (cluster_levels): node
-    // buckets of the (node, item) pairs, each item's predecessors through
-    // its nodes, and the round flags of the longest-path relaxation
+    // order links of a key-ordered pass (cluster_order, run_order): node
+    // buckets of the (node, item) pairs, each item's followers through its
+    // nodes, the count of items each one still waits for, and the two
+    // rounds' item lists
     uint32_t* lv_node_start;           // [slots + 1] counts, then bucket starts
     uint32_t* lv_node_fill;            // [slots]
     uint32_t* lv_pairs;                // [6 * cand_cap]
-    uint32_t* lv_pred;                 // [6 * cand_cap]
+    uint32_t* lv_succ;                 // [6 * cand_cap]
+    uint32_t* lv_nsucc;                // [cand_cap]
     uint32_t* lv_npred;                // [cand_cap]
-    uint32_t* lv_flag;                 // [3]
+    uint32_t* lv_front;                // [2 * cand_cap]
 };
 
 // Per-instance tables and state (one cluster each).
@@ -271,8 +267,13 @@ struct ClusterParams {
     long long copy_budget;
     uint32_t smem_x, smem_v;       // byte offsets of node and force/velocity arrays
     uint32_t smem_offsets;         // byte offset of the CTA's stage offsets
-    uint32_t smem_levels;          // contact: byte offset of rank 0's node levels (slots x u32), 0 = global
     TapeStep tape;                 // taping launches: where this step's tape goes
+    // contact launches: clusters after the first that join only the contact
+    // detection phases (broadphase and swept queries), synchronised with the
+    // structure's cluster by the bounded grid barrier `grid` over all CTAs
+    // of the (cooperative) launch; 0 = the structure's cluster alone
+    int helper_clusters;
+    dev::GridBarrier grid;
 };
 
 // Parameters of the reverse step kernel (one structure, one cluster).

@@ -390,24 +390,16 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
             K.interior_stages = 0;
             K.boundary_stages = K.stages;
         } else {
-            // interior constraints: coloured per CTA
-            int I = 0;
-            for (int c = 0; c < ctas; ++c) {
-                std::vector<size_t> ids;
-                std::vector<std::array<uint32_t, 4>> sub;
-                std::vector<int> subc;
-                for (size_t i = 0; i < m; ++i)
-                    if (interior[i] && cta_of[i] == c) {
-                        ids.push_back(i);
-                        sub.push_back(nodes[i]);
-                        subc.push_back(counts[i]);
-                    }
-                std::vector<int> col;
-                I = std::max(I, dsatur_colour(sub, subc, col));
-                for (size_t j = 0; j < ids.size(); ++j) colour[ids[j]] = col[j];
-            }
-            // constraints spanning CTAs: one colouring; the suffix of small
-            // colours becomes the single-CTA tail
+            // Split stages.  A record whose nodes all lie in its CTA's patch
+            // is interior; the others (boundary records) are coloured first
+            // and alone, so they take only as many colours as the most
+            // boundary records at one node need.  Interior records then
+            // take the smallest colour free at all of their nodes,
+            // boundary colours included, and open a colour of their own
+            // only where none is.  The stages of interior-only colours run
+            // first, each closed by a CTA barrier (a CTA touches its own
+            // patch only), the last by a cluster barrier; every stage with
+            // boundary records is closed by a cluster barrier.
             std::vector<size_t> ids;
             std::vector<std::array<uint32_t, 4>> sub;
             std::vector<int> subc;
@@ -418,28 +410,58 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
                     subc.push_back(counts[i]);
                 }
             std::vector<int> col;
-            const int B = dsatur_colour(sub, subc, col);
-            std::vector<size_t> size(B, 0);
-            for (int c : col) ++size[c];
-            int tail = B;
-            while (tail > 0 && size[tail - 1] <= kClusterTailColourMax) --tail;
-            // the tail runs on the CTA owning most of its nodes
-            std::vector<size_t> owned(ctas, 0);
-            for (size_t j = 0; j < ids.size(); ++j)
-                if (col[j] >= tail)
-                    for (int q = 0; q < subc[j]; ++q) ++owned[part[sub[j][q]]];
-            K.tail_cta = tail < B ? static_cast<int>(std::max_element(owned.begin(), owned.end()) - owned.begin()) : -1;
+            int B = dsatur_colour(sub, subc, col);
+            if (B > 1) B = reduce_colours(sub, subc, N, B, col, kColourSearchMoves);
+            // colours in use at each node (bit c: colour c), boundary first
+            std::vector<std::vector<uint64_t>> used(N);
+            auto taken = [&](uint32_t n, int c) {
+                const auto& u = used[n];
+                return static_cast<size_t>(c >> 6) < u.size() && ((u[c >> 6] >> (c & 63)) & 1ull);
+            };
+            auto take = [&](uint32_t n, int c) {
+                auto& u = used[n];
+                if (u.size() <= static_cast<size_t>(c >> 6)) u.resize((c >> 6) + 1, 0ull);
+                u[c >> 6] |= 1ull << (c & 63);
+            };
             for (size_t j = 0; j < ids.size(); ++j) {
-                colour[ids[j]] = I + col[j];
-                if (col[j] >= tail) cta_of[ids[j]] = K.tail_cta;
+                colour[ids[j]] = col[j];
+                for (int q = 0; q < subc[j]; ++q) take(sub[j][q], col[j]);
             }
-            K.stages = I + B;
-            K.interior_stages = I;
-            K.boundary_stages = tail;
-            K.tail_stages = B - tail;
+            // interior records, most constrained first (largest node degree sum)
+            std::vector<uint32_t> degree(N, 0);
+            for (size_t i = 0; i < m; ++i)
+                for (int q = 0; q < counts[i]; ++q) ++degree[nodes[i][q]];
+            std::vector<size_t> inner;
+            for (size_t i = 0; i < m; ++i)
+                if (interior[i]) inner.push_back(i);
+            auto weight = [&](size_t i) {
+                uint32_t w = 0;
+                for (int q = 0; q < counts[i]; ++q) w += degree[nodes[i][q]];
+                return w;
+            };
+            std::stable_sort(inner.begin(), inner.end(), [&](size_t a, size_t b) { return weight(a) > weight(b); });
+            int total = B;
+            for (size_t i : inner) {
+                int c = 0;
+                for (;; ++c) {
+                    bool free = true;
+                    for (int q = 0; q < counts[i] && free; ++q) free = !taken(nodes[i][q], c);
+                    if (free) break;
+                }
+                colour[i] = c;
+                for (int q = 0; q < counts[i]; ++q) take(nodes[i][q], c);
+                total = std::max(total, c + 1);
+            }
+            // stage order: interior-only colours, then the boundary colours
+            std::vector<int> stage_of(total);
+            const int inner_only = total - B;
+            for (int c = 0; c < total; ++c) stage_of[c] = c >= B ? c - B : inner_only + c;
+            for (size_t i = 0; i < m; ++i) colour[i] = stage_of[colour[i]];
+            K.stages = total;
+            K.interior_stages = inner_only;
+            K.boundary_stages = B;
             K.cluster_sync.assign(K.stages, 1);
-            for (int g = 0; g + 1 < I; ++g) K.cluster_sync[g] = 0;
-            for (int g = I + tail; g + 1 < I + B; ++g) K.cluster_sync[g] = 0;
+            for (int g = 0; g + 1 < inner_only; ++g) K.cluster_sync[g] = 0;
         }
         const int stages = K.stages;
         // records CTA-major, stage within, definition order within

@@ -53,8 +53,9 @@ struct ClusterKind {
     std::vector<uint32_t> def_index;
     uint32_t max_cta_records = 0;  // multipliers held in shared memory per CTA
     std::vector<uint8_t> cluster_sync;  // [stages]: 1 = cluster barrier after the stage, 0 = CTA barrier
-    int interior_stages = 0, boundary_stages = 0, tail_stages = 0;
-    int tail_cta = -1;
+    // split stages: the first interior_stages stages hold only records whose
+    // nodes all lie in the executing CTA's patch; boundary_stages follow
+    int interior_stages = 0, boundary_stages = 0;
 };
 
 struct ClusterSchedule {
@@ -139,10 +140,6 @@ bool build_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t
 // Move budget of the search for a colouring with fewer colours (per colour
 // count tried).
 constexpr long kColourSearchMoves = 300000;
-
-// Boundary colours with at most this many records may form the single-CTA
-// tail of a kind's split stages.
-constexpr size_t kClusterTailColourMax = 256;
 
 // Checks the invariants the cluster kernel relies on; raises on failure.
 void verify_cluster_schedule(const OwnedDefinition& d, const std::vector<uint32_t>& suspension_nodes,

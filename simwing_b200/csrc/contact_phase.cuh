@@ -87,8 +87,21 @@ struct ContactCtx {
     int* status;
     uint32_t x_base;           // shared address of this CTA's node array
     uint32_t v_delta;          // offset from the node array to the velocity array
-    uint32_t* node_level;      // rank 0: node levels of the key-ordered passes (shared or global memory)
+    // the detection phases run over every CTA of the launch: the structure's
+    // cluster and `helpers` helper clusters (grank = this CTA's rank among
+    // gctas), with the grid barrier between phases when there are helpers
+    uint32_t grank, gctas;
+    int helpers;
+    GridBarrier grid;
 };
+
+// The barrier between two detection phases.
+__device__ __forceinline__ void detect_sync(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
+    if (c.helpers)
+        grid_sync(c.grid);
+    else
+        cluster.sync();
+}
 
 using contact::D3;
 
@@ -210,7 +223,7 @@ __device__ __forceinline__ Bins make_bins(const unsigned long long* range, uint3
 __device__ __forceinline__ void contact_snapshot(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     for (uint32_t i = threadIdx.x; i < c.n; i += blockDim.x) C.snapshot[c.base + i] = c.x[i];
-    const uint32_t gt = c.me * blockDim.x + threadIdx.x, stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
+    const uint32_t gt = c.grank * blockDim.x + threadIdx.x, stride = c.gctas * blockDim.x;
     for (uint32_t i = gt; i <= C.bins_cap; i += stride) {
         C.tbin[i] = 0u;
         C.tbin_fill[i] = 0u;
@@ -223,10 +236,10 @@ __device__ __forceinline__ void contact_snapshot(const ContactCtx& c) {
 static __device__ __noinline__ void contact_boxes(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     const uint32_t total = C.nv + C.ne + C.nt;
-    const uint32_t stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
+    const uint32_t stride = c.gctas * blockDim.x;
     const int a = C.axis, a2 = C.axis2;
     // warp-uniform trip count: every lane takes part in the warp reductions
-    for (uint32_t base = c.me * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+    for (uint32_t base = c.grank * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
         const uint32_t i = base + (threadIdx.x & 31);
         bool tri = false, edge = false;
         unsigned long long lo_key = 0, ext_key = 0, lo_key2 = 0, ext_key2 = 0;
@@ -281,7 +294,7 @@ static __device__ __noinline__ void contact_boxes(const ContactCtx& c) {
 // (every thread of the cluster).
 __device__ __noinline__ void contact_bin_counts(const ContactCtx& c) {
     const ContactDev& C = *c.C;
-    const uint32_t gt = c.me * blockDim.x + threadIdx.x, stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
+    const uint32_t gt = c.grank * blockDim.x + threadIdx.x, stride = c.gctas * blockDim.x;
     const int a = C.axis, a2 = C.axis2;
     const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 6, C.bins_cap);
     for (uint32_t t = gt; t < C.nt; t += stride) {
@@ -297,7 +310,7 @@ __device__ __noinline__ void contact_bin_counts(const ContactCtx& c) {
 // Columns into their buckets (every thread of the cluster).
 __device__ __noinline__ void contact_bin_scatter(const ContactCtx& c) {
     const ContactDev& C = *c.C;
-    const uint32_t gt = c.me * blockDim.x + threadIdx.x, stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
+    const uint32_t gt = c.grank * blockDim.x + threadIdx.x, stride = c.gctas * blockDim.x;
     const int a = C.axis, a2 = C.axis2;
     const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 6, C.bins_cap);
     for (uint32_t t = gt; t < C.nt; t += stride) {
@@ -321,7 +334,7 @@ __device__ __noinline__ void contact_bin_scatter(const ContactCtx& c) {
 __device__ __noinline__ void contact_rows(const ContactCtx& c, bool write) {
     const ContactDev& C = *c.C;
     const uint32_t rows = C.nv + C.ne;
-    const uint32_t warps = (static_cast<uint32_t>(c.ctas) * blockDim.x) >> 5;
+    const uint32_t warps = (c.gctas * blockDim.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
     const int a = C.axis;
     const contact::Box* vb = reinterpret_cast<const contact::Box*>(C.vbox);
@@ -329,7 +342,7 @@ __device__ __noinline__ void contact_rows(const ContactCtx& c, bool write) {
     const contact::Box* tb = reinterpret_cast<const contact::Box*>(C.tbox);
     const int a2 = C.axis2;
     const Bins bt = make_bins(C.range, C.bins_cap), be = make_bins(C.range + 6, C.bins_cap);
-    for (uint32_t row = (c.me * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
+    for (uint32_t row = (c.grank * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
         const bool vertex_row = row < C.nv;
         const contact::Box b = vertex_row ? vb[row] : eb[row - C.nv];
         const Bins& g = vertex_row ? bt : be;
@@ -435,13 +448,14 @@ __device__ __forceinline__ uint32_t slot_addr(const ContactCtx& c, uint32_t slot
 }
 
 // Per candidate: the swept query, the snapshot's closest features, and what
-// the serial pass needs of the feature's nodes (cluster addresses, inverse
-// masses, effective inverse mass).
+// the serial pass needs of the feature's nodes (slots, inverse masses,
+// effective inverse mass; the structure's cluster turns the slots of the
+// candidates in contact into cluster addresses).
 __device__ __noinline__ void contact_queries(const ContactCtx& c) {
     const ContactDev& C = *c.C;
     const unsigned long long count = C.offsets[C.nv + C.ne];
-    const uint32_t stride = static_cast<uint32_t>(c.ctas) * blockDim.x;
-    const uint32_t gt = c.me * blockDim.x + threadIdx.x;
+    const uint32_t stride = c.gctas * blockDim.x;
+    const uint32_t gt = c.grank * blockDim.x + threadIdx.x;
     contact::Interval* queue =
         reinterpret_cast<contact::Interval*>(C.queues) + static_cast<size_t>(gt) * C.queue_stride;
     for (unsigned long long i = gt; i < count; i += stride) {
@@ -464,14 +478,12 @@ __device__ __noinline__ void contact_queries(const ContactCtx& c) {
         }();
         for (int k = 0; k < q.fc; ++k) {
             const float w = C.snapshot[q.f[k]].w;
-            out.addr[k] = slot_addr(c, q.f[k]);
             out.slot[k] = q.f[k];
             out.inv[k] = w;
             eff += static_cast<double>(w) * g.fw[k] * g.fw[k];
         }
         for (int k = 0; k < q.sc; ++k) {
             const float w = C.snapshot[q.s[k]].w;
-            out.addr[q.fc + k] = slot_addr(c, q.s[k]);
             out.slot[q.fc + k] = q.s[k];
             out.inv[q.fc + k] = w;
             eff += static_cast<double>(w) * g.sw[k] * g.sw[k];
@@ -493,7 +505,7 @@ __device__ __noinline__ void contact_queries(const ContactCtx& c) {
     }
 }
 
-// ---- key-ordered passes, level by level ---------------------------------------
+// ---- key-ordered passes, in rounds of node-disjoint items ----------------------
 
 __device__ __forceinline__ uint32_t cluster_tid(const ContactCtx& c) { return c.me * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint32_t cluster_threads(const ContactCtx& c) {
@@ -559,106 +571,32 @@ __device__ __noinline__ void block_scan(const uint32_t* in, uint32_t n, uint32_t
     __syncthreads();
 }
 
-// Folds a batch of up to 32 items, one per lane of the calling warp, into
-// the node levels in lane order (lane 0 does the folding); returns the
-// largest level so far.
-static __device__ __noinline__ uint32_t fold_levels(uint32_t* level, uint32_t* item_level, uint32_t batch,
-                                                    uint32_t mine_n, const uint32_t* mine, uint32_t levels) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t m0 = mine[0], m1 = mine[1], m2 = mine[2], m3 = mine[3], m4 = mine[4], m5 = mine[5];
-    for (uint32_t k = 0; k < batch; ++k) {
-        const uint32_t n = __shfl_sync(0xffffffffu, mine_n, k);
-        const uint32_t s0 = __shfl_sync(0xffffffffu, m0, k), s1 = __shfl_sync(0xffffffffu, m1, k);
-        const uint32_t s2 = __shfl_sync(0xffffffffu, m2, k), s3 = __shfl_sync(0xffffffffu, m3, k);
-        const uint32_t s4 = __shfl_sync(0xffffffffu, m4, k), s5 = __shfl_sync(0xffffffffu, m5, k);
-        if (lane == 0) {
-            uint32_t l = 0;
-            if (n) {
-                l = level[s0];
-                if (n > 1) l = max(l, level[s1]);
-                if (n > 2) l = max(l, level[s2]);
-                if (n > 3) l = max(l, level[s3]);
-                if (n > 4) l = max(l, level[s4]);
-                if (n > 5) l = max(l, level[s5]);
-                ++l;
-                level[s0] = l;
-                if (n > 1) level[s1] = l;
-                if (n > 2) level[s2] = l;
-                if (n > 3) level[s3] = l;
-                if (n > 4) level[s4] = l;
-                if (n > 5) level[s5] = l;
-                levels = max(levels, l);
-            }
-            item_level[k] = l;
-        }
-    }
-    return levels;
-}
-
-// Levels of `items` in order (rank 0's block): get(i, slots) returns the
-// item's nodes (0: the item takes no level).  The lanes of warp 0 fetch the
-// nodes of 32 consecutive items at once and lane 0 folds them into the node
-// levels in order; the level sizes are then counted by the block and
-// scanned.  Leaves the levels' starts in level_start[1 .. levels + 1] and the
-// level count in level_meta[0].
+// The order links of `items` taken in order (every thread of every CTA
+// calls it): get(i, slots) returns item i's nodes (0: the item touches no
+// node).  Item j must follow item i when i < j and they share a node; it is
+// enough that each item follows the item just before it in each of its
+// nodes' lists.  The (node, item) pairs are bucketed by node with a counting
+// sort, each bucket is put in item order, and each item gets, per node, a
+// link to the next item of the bucket (lv_succ, lv_nsucc) and the count of
+// items it follows (lv_npred).  Items that follow none of the others can run
+// first, together: they share no node.
 template <class Get>
-__device__ __forceinline__ void assign_levels(const ContactCtx& c, uint32_t items, uint32_t slots, Get get) {
-    const ContactDev& C = *c.C;
-    uint32_t* level = c.node_level;
-    for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) level[i] = 0;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        const uint32_t lane = threadIdx.x;
-        uint32_t levels = 0;
-        for (uint32_t base = 0; base < items; base += 32) {
-            uint32_t mine[6] = {0, 0, 0, 0, 0, 0};
-            const uint32_t mine_n = base + lane < items ? get(base + lane, mine) : 0u;
-            const uint32_t batch = min(32u, items - base);
-            levels = fold_levels(level, C.item_level + base, batch, mine_n, mine, levels);
-        }
-        if (lane == 0) C.level_meta[0] = levels;
-    }
-    __syncthreads();
-    const uint32_t levels = C.level_meta[0];
-    for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) {
-        const uint32_t l = C.item_level[i];
-        if (l) atomicAdd(&C.level_start[l], 1u);
-    }
-    __syncthreads();
-    block_scan(C.level_start + 1, levels, C.level_start + 1);
-}
-
-// Levels of `items` in order, over the whole cluster (every thread of every
-// CTA calls it): get(i, slots) returns item i's nodes (0: the item takes no
-// level).  An item's level is one more than the largest level among the
-// earlier items sharing one of its nodes (1 without one), as a serial fold
-// in item order gives it.  The (node, item) pairs are bucketed by node with
-// a counting sort and each bucket is put in item order, so an item's
-// predecessors are the items just before it in its nodes' buckets; the
-// longest path over these links is then relaxed in rounds, each lifting
-// every item to one more than its predecessors' largest level, until a
-// round changes nothing (at most `items` rounds: a path has at most `items`
-// links).  Leaves item_level[], the level count in level_meta[0] and the
-// levels' starts in level_start[1 .. levels + 1], as the serial fold does.
-template <class Get>
-__device__ __noinline__ void cluster_levels(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
-                                            uint32_t items, uint32_t slots, Get get) {
+__device__ __noinline__ void cluster_order(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
+                                           uint32_t items, uint32_t slots, Get get) {
     const ContactDev& C = *c.C;
     const uint32_t gt = cluster_tid(c), stride = cluster_threads(c);
     uint32_t* count = C.lv_node_start;  // counts, then (scanned in place) bucket starts
     for (uint32_t i = gt; i <= slots; i += stride) count[i] = 0;
     for (uint32_t i = gt; i < slots; i += stride) C.lv_node_fill[i] = 0;
-    for (uint32_t i = gt; i < items; i += stride) C.lv_npred[i] = 0;
-    if (gt == 0) {
-        C.level_meta[0] = 0;
-        C.lv_flag[0] = C.lv_flag[1] = C.lv_flag[2] = 0;
+    for (uint32_t i = gt; i < items; i += stride) {
+        C.lv_npred[i] = 0;
+        C.lv_nsucc[i] = 0;
     }
     cluster.sync();
     uint32_t s6[6];
     for (uint32_t i = gt; i < items; i += stride) {
         const uint32_t n = get(i, s6);
         for (uint32_t q = 0; q < n; ++q) atomicAdd(&count[s6[q]], 1u);
-        C.item_level[i] = n ? 1u : 0u;
     }
     cluster.sync();
     if (c.me == 0) block_scan(count, slots, count);
@@ -668,8 +606,6 @@ __device__ __noinline__ void cluster_levels(const ContactCtx& c, cooperative_gro
         for (uint32_t q = 0; q < n; ++q) C.lv_pairs[count[s6[q]] + atomicAdd(&C.lv_node_fill[s6[q]], 1u)] = i;
     }
     cluster.sync();
-    // each node's bucket in item order; an item's predecessor through the
-    // node is the item before it there
     for (uint32_t v = gt; v < slots; v += stride) {
         const uint32_t lo = count[v], hi = count[v + 1];
         for (uint32_t a = lo + 1; a < hi; ++a) {
@@ -682,80 +618,51 @@ __device__ __noinline__ void cluster_levels(const ContactCtx& c, cooperative_gro
             C.lv_pairs[b] = x;
         }
         for (uint32_t a = lo + 1; a < hi; ++a) {
-            const uint32_t j = C.lv_pairs[a];
-            C.lv_pred[static_cast<size_t>(j) * 6 + atomicAdd(&C.lv_npred[j], 1u)] = C.lv_pairs[a - 1];
+            const uint32_t i = C.lv_pairs[a - 1], j = C.lv_pairs[a];
+            C.lv_succ[static_cast<size_t>(i) * 6 + atomicAdd(&C.lv_nsucc[i], 1u)] = j;
+            atomicAdd(&C.lv_npred[j], 1u);
         }
     }
     cluster.sync();
-    // longest path: rounds until one changes nothing; round r reports on
-    // flag r % 3 and clears the flag round r + 1 will use (last read two
-    // barriers ago)
-    for (uint32_t r = 0; r <= items; ++r) {
-        bool changed = false;
-        for (uint32_t i = gt; i < items; i += stride) {
-            const uint32_t np = C.lv_npred[i];
-            if (!np) continue;
-            uint32_t l = 0;
-            for (uint32_t k = 0; k < np; ++k) l = max(l, __ldcg(C.item_level + C.lv_pred[static_cast<size_t>(i) * 6 + k]));
-            ++l;
-            if (l > __ldcg(C.item_level + i)) {
-                __stcg(C.item_level + i, l);
-                changed = true;
+}
+
+// Runs work(id[item]) (work(item) without `id`) for `items` items in an
+// order that keeps, for every node, the items touching it in item order
+// (the calling block, after cluster_order): rounds, each running together
+// the items whose earlier neighbours have all run (they share no node), a
+// block barrier after each.  The nodes may live in any CTA of the cluster,
+// but only this block's threads touch them until the cluster barrier that
+// follows, so the block barrier orders one round's writes before the next
+// round's reads.  Every item ends a round with all its links released, so a
+// round runs at least one item and there are at most `items` rounds.
+template <class Work>
+__device__ __forceinline__ void run_order(const ContactDev& C, uint32_t items, const uint32_t* id, Work work) {
+    __shared__ uint32_t front_n[2];
+    uint32_t* front[2] = {C.lv_front, C.lv_front + C.cand_cap};
+    if (threadIdx.x < 2) front_n[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < items; i += blockDim.x)
+        if (__ldcg(C.lv_npred + i) == 0u) front[0][atomicAdd(&front_n[0], 1u)] = i;
+    __syncthreads();
+    uint32_t done = 0;
+    for (uint32_t r = 0; r < items && done < items; ++r) {
+        const uint32_t cur = r & 1u, n = front_n[cur];
+        for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+            const uint32_t i = front[cur][k];
+            work(id ? id[i] : i);
+            const uint32_t m = C.lv_nsucc[i];
+            for (uint32_t q = 0; q < m; ++q) {
+                const uint32_t j = C.lv_succ[static_cast<size_t>(i) * 6 + q];
+                if (atomicSub(&C.lv_npred[j], 1u) == 1u) front[cur ^ 1u][atomicAdd(&front_n[cur ^ 1u], 1u)] = j;
             }
         }
-        if (changed) C.lv_flag[r % 3] = 1u;
-        if (gt == 0) C.lv_flag[(r + 1) % 3] = 0u;
-        cluster.sync();
-        if (*reinterpret_cast<const volatile uint32_t*>(C.lv_flag + r % 3) == 0u) break;
-    }
-    // the levels' sizes and starts (rank 0's block)
-    if (c.me == 0) {
-        for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) atomicMax(C.level_meta, __ldcg(C.item_level + i));
+        done += n;
         __syncthreads();
-        const uint32_t levels = C.level_meta[0];
-        for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) {
-            const uint32_t l = __ldcg(C.item_level + i);
-            if (l) atomicAdd(&C.level_start[l], 1u);
-        }
-        __syncthreads();
-        block_scan(C.level_start + 1, levels, C.level_start + 1);
-    }
-}
-
-// Clears the level tables for `items` items (every thread of the cluster).
-__device__ __forceinline__ void reset_levels(const ContactCtx& c, uint32_t items, uint32_t slots) {
-    const ContactDev& C = *c.C;
-    const uint32_t gt = cluster_tid(c), stride = cluster_threads(c);
-    (void)slots;
-    for (uint32_t i = gt; i < items + 2; i += stride) {
-        C.level_start[i] = 0;
-        C.level_fill[i] = 0;
-    }
-}
-
-// Buckets the items by level (every thread of the calling block); a bucket
-// holds id[item], or the item itself without `id`.
-__device__ __forceinline__ void scatter_levels(const ContactDev& C, uint32_t items, const uint32_t* id = nullptr) {
-    for (uint32_t i = threadIdx.x; i < items; i += blockDim.x) {
-        const uint32_t l = __ldcg(C.item_level + i);  // written by every CTA of the cluster
-        if (l) C.level_items[C.level_start[l] + atomicAdd(&C.level_fill[l], 1u)] = id ? id[i] : i;
+        if (threadIdx.x == 0) front_n[cur] = 0;
+        // read by every thread before the reset above takes effect two
+        // rounds later: the next round's barrier separates them
     }
     __syncthreads();
-}
-
-// Runs work(item) level by level inside the calling block: the items of a
-// level touch disjoint nodes.  The nodes may live in any CTA of the
-// cluster, but only this block's threads touch them until the cluster
-// barrier that follows, so a block barrier orders one level's writes before
-// the next level's reads.
-template <class Work>
-__device__ __forceinline__ void run_levels(const ContactDev& C, Work work) {
-    const uint32_t levels = C.level_meta[0];
-    for (uint32_t l = 1; l <= levels; ++l) {
-        const uint32_t lo = C.level_start[l], hi = C.level_start[l + 1];
-        for (uint32_t k = lo + threadIdx.x; k < hi; k += blockDim.x) work(C.level_items[k]);
-        __syncthreads();
-    }
 }
 
 __device__ __forceinline__ bool impact_state(uint32_t s) {
@@ -855,8 +762,8 @@ static __device__ __noinline__ void project_one(const ContactCtx& c, uint32_t i)
     out = e;
 }
 
-// The contact iteration's projections in key order, level by level, and the
-// next multiplier table (the merge of this iteration's candidates in
+// The contact iteration's projections in key order (rounds of candidates
+// that share no node), and the next multiplier table (the merge of this iteration's candidates in
 // contact with the previous table's other entries).
 __device__ __noinline__ void contact_project(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
     const ContactDev& C = *c.C;
@@ -868,7 +775,6 @@ __device__ __noinline__ void contact_project(const ContactCtx& c, cooperative_gr
     const uint32_t gt = cluster_tid(c), stride = cluster_threads(c);
     const uint32_t slots = c.pbeg[c.ctas];
     // reset
-    reset_levels(c, count, slots);
     for (uint32_t k = gt; k < old_n; k += stride) C.mark_b[k] = 1u;
     cluster.sync();
     // in contact or not; warm-start entry; previous entries taken over
@@ -896,8 +802,8 @@ __device__ __noinline__ void contact_project(const ContactCtx& c, cooperative_gr
     }
     cluster.sync();
     // ranks of the two merged lists and the candidates in contact (rank 0's
-    // block); their levels (the cluster); their projections, level by level
-    // (rank 0's block)
+    // block); their order links (the cluster); their projections, round by
+    // round (rank 0's block)
     if (c.me == 0) {
         block_scan(C.mark_a, count, C.mark_a);
         block_scan(C.mark_b, old_n, C.mark_b);
@@ -908,17 +814,20 @@ __device__ __noinline__ void contact_project(const ContactCtx& c, cooperative_gr
     cluster.sync();
     if (!contact_failed(c.status)) {  // uniform: read after the barrier
         const uint32_t hits = C.mark_a[count];
-        cluster_levels(c, cluster, hits, slots, [&](uint32_t h, uint32_t* s) -> uint32_t {
+        // cluster addresses of the nodes of the candidates in contact (read
+        // by rank 0's rounds after cluster_order's barriers)
+        for (uint32_t h = gt; h < hits; h += stride) {
+            ContactQuery& Q = C.query[C.hit[h]];
+            for (uint32_t j = 0; j < Q.fc + Q.sc; ++j) Q.addr[j] = slot_addr(c, Q.slot[j]);
+        }
+        cluster_order(c, cluster, hits, slots, [&](uint32_t h, uint32_t* s) -> uint32_t {
             const ContactQuery& Q = C.query[C.hit[h]];
             const uint32_t n = Q.fc + Q.sc;
 #pragma unroll
             for (int j = 0; j < 6; ++j) s[j] = j < static_cast<int>(n) ? Q.slot[j] : 0u;
             return n;
         });
-        if (c.me == 0) {
-            scatter_levels(C, hits, C.hit);
-            run_levels(C, [&](uint32_t i) { project_one(c, i); });
-        }
+        if (c.me == 0) run_order(C, hits, C.hit, [&](uint32_t i) { project_one(c, i); });
     }
     cluster.sync();
     if (contact_failed(c.status)) return;  // uniform: read after the barrier
@@ -998,7 +907,7 @@ __device__ __noinline__ void contact_certify_all(const ContactCtx& c, cooperativ
             r.sw[j] = Q.sw[j];
         }
         for (int j = 0; j < 6; ++j) {
-            r.addr[j] = Q.addr[j];
+            r.addr[j] = j < static_cast<int>(fc + sc) ? slot_addr(c, Q.slot[j]) : 0u;
             r.slot[j] = Q.slot[j];
             r.inv[j] = Q.inv[j];
         }
@@ -1079,30 +988,40 @@ static __device__ __noinline__ void friction_one(const ContactCtx& c, const Cont
 __device__ __forceinline__ uint32_t* C_bins_t(const ContactCtx& c) { return c.C->tbin; }
 __device__ __forceinline__ uint32_t* C_bins_e(const ContactCtx& c) { return c.C->ebin; }
 
-// Broadphase and queries of the current state (phases snapshot .. queries).
+// Broadphase and queries of the current state (phases snapshot .. queries),
+// over every CTA of the launch (the structure's cluster and its helpers).
 __device__ __forceinline__ void contact_detect(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
     cluster.sync();  // every CTA's projections (local and remote) are done
     contact_snapshot(c);
-    cluster.sync();
+    detect_sync(c, cluster);
     contact_boxes(c);
-    cluster.sync();
+    detect_sync(c, cluster);
     if (!contact_failed(c.status)) contact_bin_counts(c);
-    cluster.sync();
-    if (c.me == 0 && !contact_failed(c.status)) {
+    detect_sync(c, cluster);
+    if (c.grank == 0 && !contact_failed(c.status)) {
         block_scan(C_bins_t(c), make_bins(c.C->range, c.C->bins_cap).count(), C_bins_t(c));
         block_scan(C_bins_e(c), make_bins(c.C->range + 6, c.C->bins_cap).count(), C_bins_e(c));
     }
-    cluster.sync();
+    detect_sync(c, cluster);
     if (!contact_failed(c.status)) contact_bin_scatter(c);
-    cluster.sync();
+    detect_sync(c, cluster);
     if (!contact_failed(c.status)) contact_rows(c, false);
-    cluster.sync();
-    if (c.me == 0 && !contact_failed(c.status)) contact_scan(c);
-    cluster.sync();
+    detect_sync(c, cluster);
+    if (c.grank == 0 && !contact_failed(c.status)) contact_scan(c);
+    detect_sync(c, cluster);
     if (!contact_failed(c.status)) contact_rows(c, true);
-    cluster.sync();
+    detect_sync(c, cluster);
     if (!contact_failed(c.status)) contact_queries(c);
-    cluster.sync();
+    detect_sync(c, cluster);
+}
+
+// A helper cluster's part of a launch: the detection phases of every
+// contact iteration and of the certification, in the order the structure's
+// cluster runs them.
+__device__ __forceinline__ void contact_helper(const ContactCtx& c, cooperative_groups::cluster_group& cluster,
+                                               int iterations) {
+    for (int it = 0; it < iterations; ++it) contact_detect(c, cluster);
+    contact_detect(c, cluster);
 }
 
 __device__ __forceinline__ void contact_iteration(const ContactCtx& c, cooperative_groups::cluster_group& cluster) {
@@ -1128,19 +1047,14 @@ __device__ __forceinline__ void contact_friction(const ContactCtx& c, cooperativ
     cluster.sync();  // every CTA has finalized its velocities
     const bool skip = contact_failed(c.status);
     const uint32_t records = skip ? 0u : static_cast<uint32_t>(diag->records);
-    reset_levels(c, records, c.pbeg[c.ctas]);
-    cluster.sync();
-    cluster_levels(c, cluster, records, c.pbeg[c.ctas], [&](uint32_t i, uint32_t* s) -> uint32_t {
+    cluster_order(c, cluster, records, c.pbeg[c.ctas], [&](uint32_t i, uint32_t* s) -> uint32_t {
         const ContactRecordDev& r = C.records[i];
         const uint32_t n = r.fc + r.sc;
 #pragma unroll
         for (int j = 0; j < 6; ++j) s[j] = j < static_cast<int>(n) ? r.slot[j] : 0u;
         return n;
     });
-    if (c.me == 0) {
-        scatter_levels(C, records);
-        run_levels(C, [&](uint32_t i) { friction_one(c, C.records[i]); });
-    }
+    if (c.me == 0) run_order(C, records, nullptr, [&](uint32_t i) { friction_one(c, C.records[i]); });
     cluster.sync();
 }
 

@@ -91,11 +91,19 @@ __device__ __forceinline__ bool grid_sync(const GridBarrier& g) {
                 atomicAdd(g.generation, 1u);
             } else {
                 const long long start = clock64();
+                unsigned int polls = 0, pause = 32;
                 while (ld_acquire(g.generation) == gen) {
                     if (clock64() - start > g.budget) {
                         atomicOr(g.status, kStatusSyncTimeout);
                         ok = 0;
                         break;
+                    }
+                    // a long wait (a contact helper cluster waiting for the
+                    // structure's sweep) backs off, so that the spinning
+                    // CTAs do not load the memory system the others use
+                    if (++polls > 64) {
+                        __nanosleep(pause);
+                        if (pause < 1024) pause *= 2;
                     }
                 }
             }

@@ -25,6 +25,29 @@ void cuda_check(cudaError_t e, const char* what) {
 
 namespace {
 
+// A point on the origin grid (1/256 m) nearest to x.
+double origin_grid(double x) { return std::nearbyint(x * 256.0) / 256.0; }
+
+void initial_origin(const OwnedDefinition& def, double o[3]) {
+    o[0] = o[1] = o[2] = 0.0;
+    if (def.has_suspension) {
+        const swb_vec3& c = def.suspension.pilot_initial_com_world;
+        o[0] = origin_grid(c.x);
+        o[1] = origin_grid(c.y);
+        o[2] = origin_grid(c.z);
+        return;
+    }
+    if (def.nodes.empty()) return;
+    double lo[3], hi[3];
+    for (int k = 0; k < 3; ++k) lo[k] = hi[k] = (&def.nodes[0].position.x)[k];
+    for (const auto& n : def.nodes)
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], (&n.position.x)[k]);
+            hi[k] = std::max(hi[k], (&n.position.x)[k]);
+        }
+    for (int k = 0; k < 3; ++k) o[k] = origin_grid(0.5 * (lo[k] + hi[k]));
+}
+
 template <class T>
 T* dalloc(std::vector<void*>& owned, size_t count) {
     void* p = nullptr;
@@ -289,13 +312,20 @@ void StructureImpl::build(const swb_structure_definition& definition, const swb_
     }
 
     // ---- device images -------------------------------------------------------
+    // The node states are FP32 offsets from an FP64 origin on a 1/256 m grid
+    // (a shift by a grid step is exact in both).  The origin starts at the
+    // pilot's centre of mass when there is one (the step recentres there
+    // whenever the pilot has moved a quarter metre), else at the centre of
+    // the nodes' bounding box, so that the offsets are as small as the
+    // structure allows from the first step on.
+    initial_origin(def, origin0);
     // nodes (slot order)
     std::vector<float4> pos(N), vel(N, make_float4(0, 0, 0, 0));
     for (uint64_t s = 0; s < N; ++s) {
         const swb_node_def& n = def.nodes[node_of_slot[s]];
         const float w = n.fixed ? 0.0f : static_cast<float>(1.0 / n.mass);
-        pos[s] = make_float4(static_cast<float>(n.position.x), static_cast<float>(n.position.y),
-                             static_cast<float>(n.position.z), w);
+        pos[s] = make_float4(static_cast<float>(n.position.x - origin0[0]), static_cast<float>(n.position.y - origin0[1]),
+                             static_cast<float>(n.position.z - origin0[2]), w);
     }
     inv_mass.resize(N);
     for (uint64_t s = 0; s < N; ++s) inv_mass[s] = pos[s].w;
@@ -359,7 +389,7 @@ void (*StructureImpl::step_kernel() const)(ClusterParams) {
 // Capacities: up to kContactCapacity candidates per phase (and as many
 // warm-started features and records); beyond that the step fails with
 // SWB_CONTACT_ERROR.
-void StructureImpl::setup_contact() {
+void StructureImpl::setup_contact(const swb_solver_options& opt) {
     constexpr uint64_t kContactCapacity = uint64_t(1) << 20;
     const ContactSurface& S = contact_surface;
     ContactDev c{};
@@ -394,20 +424,42 @@ void StructureImpl::setup_contact() {
     c.cand_cap = cap;
     c.cand = dalloc<unsigned long long>(owned, cap);
     c.query = dalloc<ContactQuery>(owned, cap);
+    // helper clusters of the detection phases: as many as can be resident
+    // beside the structure's cluster in one cooperative launch, at most
+    // kMaxContactHelpers, for surfaces of kContactHelperRows candidate rows
+    // or more (on smaller ones the grid barriers cost more than the spread
+    // work saves: 16 x 16 sheets, 2,000 rows, step in 18.0 ms with helpers
+    // against 14.1 ms without)
+    contact_helpers = 0;
+    if (!(opt.flags & SWB_OPT_CONTACT_ONE_CLUSTER) && c.nv + c.ne >= kContactHelperRows) {
+        const auto kernel = step_kernel();
+        cudaLaunchConfig_t cfg{};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = static_cast<unsigned>(G);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(G);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = cluster_smem;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem_cap)) == cudaSuccess &&
+            (G <= 8 || cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) &&
+            cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) == cudaSuccess)
+            contact_helpers = std::clamp(clusters - 1, 0, kMaxContactHelpers);
+        (void)cudaGetLastError();
+    }
     c.queue_stride = static_cast<uint32_t>(c.ccd.interval_subdivisions + 1);
-    c.queues = dalloc<double>(owned, static_cast<size_t>(G) * threads * c.queue_stride * 4);
+    c.queues = dalloc<double>(owned, static_cast<size_t>(G) * (1 + contact_helpers) * threads * c.queue_stride * 4);
     for (int b = 0; b < 2; ++b) c.table[b] = dalloc<ContactEntry>(owned, cap);
     c.table_meta = dalloc<uint32_t>(owned, 2);
     cuda_check(cudaMemsetAsync(c.table_meta, 0, 2 * sizeof(uint32_t), stream), "memset");
     c.table_cap = cap;
     c.records = dalloc<ContactRecordDev>(owned, cap);
     c.record_cap = cap;
-    c.node_level = dalloc<uint32_t>(owned, def.nodes.size());
-    c.item_level = dalloc<uint32_t>(owned, cap);
-    c.level_start = dalloc<uint32_t>(owned, cap + 2);
-    c.level_fill = dalloc<uint32_t>(owned, cap + 2);
-    c.level_items = dalloc<uint32_t>(owned, cap);
-    c.level_meta = dalloc<uint32_t>(owned, 2);
     c.hit = dalloc<uint32_t>(owned, cap);
     // binned broadphase along the longest extent of the initial geometry
     {
@@ -444,9 +496,10 @@ void StructureImpl::setup_contact() {
     c.lv_node_start = dalloc<uint32_t>(owned, def.nodes.size() + 1);
     c.lv_node_fill = dalloc<uint32_t>(owned, std::max<size_t>(def.nodes.size(), 1));
     c.lv_pairs = dalloc<uint32_t>(owned, 6 * cap);
-    c.lv_pred = dalloc<uint32_t>(owned, 6 * cap);
+    c.lv_succ = dalloc<uint32_t>(owned, 6 * cap);
+    c.lv_nsucc = dalloc<uint32_t>(owned, cap);
     c.lv_npred = dalloc<uint32_t>(owned, cap);
-    c.lv_flag = dalloc<uint32_t>(owned, 3);
+    c.lv_front = dalloc<uint32_t>(owned, 2 * cap);
     c.fail = dalloc<unsigned long long>(owned, 1);
     cuda_check(cudaMemsetAsync(c.fail, 0xff, sizeof(unsigned long long), stream), "memset");
     d_contact = dupload(owned, std::vector<ContactDev>{c}, stream);
@@ -499,13 +552,6 @@ void StructureImpl::upload_cluster_tables() {
     }
     cp.smem_offsets = off;
     off = align16(off + (total_stages(csched) + 3) * 4u);
-    // contact: rank 0 keeps the node levels of its key-ordered passes in
-    // shared memory when they fit (else in global memory)
-    const uint32_t levels_bytes = align16(static_cast<uint32_t>(def.nodes.size()) * 4u);
-    if (def.has_contact && off + levels_bytes <= smem_cap) {
-        cp.smem_levels = off;
-        off += levels_bytes;
-    }
     cluster_smem = off;
     base.seam_offsets = dupload(owned, csched.seam_offsets, stream);
     base.seam_ab = dupload(owned, csched.seam_ab, stream);
@@ -684,7 +730,8 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
         if (qw < 0 || (qw == 0 && (qx < 0 || (qx == 0 && (qy < 0 || (qy == 0 && qz < 0)))))) {
             qw = -qw; qx = -qx; qy = -qy; qz = -qz;
         }
-        pstate.com = make_float3(s.pilot_initial_com_world.x, s.pilot_initial_com_world.y, s.pilot_initial_com_world.z);
+        pstate.com = make_float3(s.pilot_initial_com_world.x - origin0[0], s.pilot_initial_com_world.y - origin0[1],
+                                 s.pilot_initial_com_world.z - origin0[2]);
         pstate.q = make_float4(qw, qx, qy, qz);
         pstate.v = make_float3(s.pilot_initial_linear_velocity.x, s.pilot_initial_linear_velocity.y,
                                s.pilot_initial_linear_velocity.z);
@@ -695,7 +742,7 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
     d_payload_def = dupload(owned, std::vector<DevPayloadDef>{pdef}, stream);
     for (int i = 0; i < 3; ++i) {
         d_payload[i] = dupload(owned, std::vector<DevPayloadState>{pstate}, stream);
-        d_origin[i] = dupload(owned, std::vector<double>{0.0, 0.0, 0.0}, stream);
+        d_origin[i] = dupload(owned, std::vector<double>{origin0[0], origin0[1], origin0[2]}, stream);
     }
     d_control = dalloc<Control>(owned, 1);
     cuda_check(cudaMemsetAsync(d_control, 0, sizeof(Control), stream), "memset");
@@ -714,7 +761,7 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
     p.copy_budget = 4000000000LL;
 
     if (cluster_mode) {
-        if (def.has_contact) setup_contact();
+        if (def.has_contact) setup_contact(opt);
         // One instance record per (input, output) buffer pair so a launch
         // only selects a pointer.
         std::vector<ClusterInstance> inst(9);
@@ -893,19 +940,37 @@ void StructureImpl::launch_substep(const swb_step_settings& st, int in, int out,
         cp.cable_pairs = st.cable_sweep_pairs;
         if (!cp.instances || in == out) raise(SWB_CUDA_ERROR, "internal error: cluster instance table");
         if (first) cuda_check(cudaMemsetAsync(d_control, 0, offsetof(Control, shift), stream), "control reset");
+        // contact: the helper clusters join the detection phases; the launch
+        // is cooperative so that every cluster is resident at once (a grid
+        // barrier spans them)
+        cp.helper_clusters = contact_helpers;
+        cp.grid = params.barrier;
         cudaLaunchConfig_t cfg{};
-        cudaLaunchAttribute attr[1];
+        cudaLaunchAttribute attr[2];
         attr[0].id = cudaLaunchAttributeClusterDimension;
         attr[0].val.clusterDim.x = static_cast<unsigned>(G);
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
-        cfg.gridDim = dim3(G);
+        attr[1].id = cudaLaunchAttributeCooperative;
+        attr[1].val.cooperative = 1;
+        cfg.gridDim = dim3(G * (1 + contact_helpers));
         cfg.blockDim = dim3(threads);
         cfg.dynamicSmemBytes = cluster_smem;
         cfg.stream = stream;
         cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        cuda_check(cudaLaunchKernelEx(&cfg, step_kernel(), cp), "cudaLaunchKernelEx (cluster)");
+        cfg.numAttrs = contact_helpers > 0 ? 2 : 1;
+        cudaError_t rc = cudaLaunchKernelEx(&cfg, step_kernel(), cp);
+        if (rc != cudaSuccess && contact_helpers > 0) {
+            // no cooperative launch of this many clusters: the structure's
+            // cluster alone from now on (the results are the same)
+            (void)cudaGetLastError();
+            contact_helpers = 0;
+            cp.helper_clusters = 0;
+            cfg.gridDim = dim3(G);
+            cfg.numAttrs = 1;
+            rc = cudaLaunchKernelEx(&cfg, step_kernel(), cp);
+        }
+        cuda_check(rc, "cudaLaunchKernelEx (cluster)");
         return;
     }
     StepParams p = params;
@@ -1551,6 +1616,23 @@ swb_status swb_structure_write_nodes(swb_structure* s, const swb_node_state* in,
                 !std::isfinite(st.previous_position.x) || !std::isfinite(st.previous_position.y) ||
                 !std::isfinite(st.previous_position.z))
                 raise(SWB_INVALID_ARGUMENT, "node state must be finite");
+        }
+        if (!m.def.has_suspension && count) {
+            // without a pilot to follow, the origin moves to the centre of
+            // the written positions' bounding box (a suspension structure's
+            // origin follows its pilot: swb_structure_write_payload)
+            double lo[3], hi[3];
+            for (int k = 0; k < 3; ++k) lo[k] = hi[k] = (&in[0].position.x)[k];
+            for (uint64_t n = 0; n < count; ++n)
+                for (int k = 0; k < 3; ++k) {
+                    lo[k] = std::min(lo[k], (&in[n].position.x)[k]);
+                    hi[k] = std::max(hi[k], (&in[n].position.x)[k]);
+                }
+            for (int k = 0; k < 3; ++k) o[k] = origin_grid(0.5 * (lo[k] + hi[k]));
+            cuda_check(cudaMemcpyAsync(m.d_origin[m.cur], o, sizeof(o), cudaMemcpyHostToDevice, m.stream), "write");
+        }
+        for (uint64_t n = 0; n < count; ++n) {
+            const auto& st = in[n];
             const uint32_t sl = m.slot_of_node[n];
             const float w = m.inv_mass[sl];
             pos[sl] = make_float4(st.position.x - o[0], st.position.y - o[1], st.position.z - o[2], w);
@@ -1632,7 +1714,30 @@ swb_status swb_structure_write_payload(swb_structure* s, const swb_payload_state
         DevPayloadState pay;
         double o[3];
         m.fetch(pos, prev, vel, pay, o);
-        pay.com = make_float3(in->center_of_mass.x - o[0], in->center_of_mass.y - o[1], in->center_of_mass.z - o[2]);
+        const double c[3] = {in->center_of_mass.x, in->center_of_mass.y, in->center_of_mass.z};
+        if (!std::isfinite(c[0]) || !std::isfinite(c[1]) || !std::isfinite(c[2]))
+            raise(SWB_INVALID_ARGUMENT, "payload state must be finite");
+        // the origin follows the pilot, as the step's recentring keeps it:
+        // the node offsets are re-expressed from the new origin, so the
+        // pilot's first step from an imported state is taken in small
+        // coordinates too
+        const double n[3] = {origin_grid(c[0]), origin_grid(c[1]), origin_grid(c[2])};
+        if (std::max({std::fabs(n[0] - o[0]), std::fabs(n[1] - o[1]), std::fabs(n[2] - o[2])}) > 0.25) {
+            for (auto* v : {&pos, &prev})
+                for (float4& x : *v) {
+                    x.x = static_cast<float>(static_cast<double>(x.x) + (o[0] - n[0]));
+                    x.y = static_cast<float>(static_cast<double>(x.y) + (o[1] - n[1]));
+                    x.z = static_cast<float>(static_cast<double>(x.z) + (o[2] - n[2]));
+                }
+            for (int k = 0; k < 3; ++k) o[k] = n[k];
+            const size_t N = pos.size();
+            cuda_check(cudaMemcpyAsync(m.d_pos[m.cur], pos.data(), N * sizeof(float4), cudaMemcpyHostToDevice, m.stream),
+                       "write");
+            cuda_check(cudaMemcpyAsync(m.d_prev[m.cur], prev.data(), N * sizeof(float4), cudaMemcpyHostToDevice,
+                                       m.stream), "write");
+            cuda_check(cudaMemcpyAsync(m.d_origin[m.cur], o, sizeof(o), cudaMemcpyHostToDevice, m.stream), "write");
+        }
+        pay.com = make_float3(c[0] - o[0], c[1] - o[1], c[2] - o[2]);
         pay.q = make_float4(in->body_to_world.w, in->body_to_world.x, in->body_to_world.y, in->body_to_world.z);
         pay.v = make_float3(in->linear_velocity.x, in->linear_velocity.y, in->linear_velocity.z);
         pay.w = make_float3(in->angular_velocity.x, in->angular_velocity.y, in->angular_velocity.z);

@@ -47,6 +47,12 @@ cudaError_t adjoint_kernel_launch(const cudaLaunchConfig_t& cfg, const AdjointPa
 // Status words written by the step kernels -> status and message.
 swb_status decode_status(const int status[2], std::string& message);
 
+// Helper clusters a contact launch may add beside the structure's cluster.
+constexpr int kMaxContactHelpers = 8;
+// Contact surfaces with fewer candidate rows (vertices plus edges) keep
+// their detection phases on the structure's cluster.
+constexpr uint32_t kContactHelperRows = 16384;
+
 struct StructureImpl {
     OwnedDefinition def;
     bool cluster_mode = false;
@@ -65,6 +71,7 @@ struct StructureImpl {
     int device = -1;
     int sm_count = 0;
     int G = 0;
+    int contact_helpers = 0;  // helper clusters of the contact detection phases
     int threads = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -75,6 +82,7 @@ struct StructureImpl {
     float4* d_prev[3] = {};
     DevPayloadState* d_payload[3] = {};
     double* d_origin[3] = {};
+    double origin0[3] = {0.0, 0.0, 0.0};  // the FP64 origin the initial FP32 offsets are taken from
     int cur = 0;
     std::vector<float> inv_mass;  // by slot
     float4* d_force = nullptr;
@@ -119,7 +127,7 @@ struct StructureImpl {
     ~StructureImpl();
     void build(const swb_structure_definition& definition, const swb_solver_options* options);
     void upload_cluster_tables();
-    void setup_contact();
+    void setup_contact(const swb_solver_options& opt);
     // The step with the force buffer already written on the device (the
     // coupling's impulse gather): skips the upload of the pending loads.
     bool device_forces = false;

@@ -16,11 +16,17 @@ is the mean squared distance of the fabric (triangle) nodes to it after a
     class (distance, cable, dihedral), the riser rest lengths and the pilot
     mass -- and the loss;
   * central finite differences (h = 1e-4, relative) of the FP64 loss for a
-    sample of those parameters;
+    sample of those parameters, and the same with h = 1e-6: where the two
+    differ, a line cable crosses its slack/taut switch within +-1e-4 along
+    the rollout, and the wide difference is no derivative;
+  * the loss of the same rollout with FP32 arithmetic (the restatement with
+    every vector result rounded to FP32, in the device's frame:
+    oracle.RecentredF32), which shows how far FP32 arithmetic of the
+    reference algorithm moves the loss over the rollout;
   * a hash of the device sweep order the FP64 runs used (the test checks
     that the device still sweeps in that order).
 
-    python tests/golden/make_calibration.py      (about 10 minutes, 8 cores)
+    python tests/golden/make_calibration.py      (about 15 minutes, 8 cores)
 """
 import hashlib
 import multiprocessing as mp
@@ -33,7 +39,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "calibration.npz")
-SETTLE, STEPS, H = 60, 240, 1e-4
+SETTLE, STEPS, H, H_FINE = 60, 240, 1e-4, 1e-6
 
 
 def settings():
@@ -92,6 +98,23 @@ def rollout_loss(args):
     orc = O.PortStructure(perturbed(d, kind, index, factor, sw.line_groups(d)).permuted(do, ho))
     orc.write_node_states(data["state"])
     orc.write_payload(payload_struct(data["payload"]))
+    for _ in range(STEPS):
+        orc.step(settings())
+    x = orc.positions()
+    w = weights_of(d)
+    return float(np.sum(w[:, None] * (x - data["target"]) ** 2) / np.sum(w))
+
+
+def f32_loss(_):
+    """The loss of the rollout with FP32 arithmetic (pool worker)."""
+    import simwing_b200 as sw
+    from oracle import oracle as O
+
+    d = sw.generate_calibration_wing()
+    _, do, ho = sw.plan_schedule(d)
+    data = np.load(OUT + ".partial.npz")
+    orc = O.RecentredF32(d.permuted(do, ho))
+    orc.write_state(data["state"], payload_struct(data["payload"]))
     for _ in range(STEPS):
         orc.step(settings())
     x = orc.positions()
@@ -159,28 +182,33 @@ def main():
     # central differences of the FP64 loss for a sample of the parameters
     sample = [("line", int(i)) for i in np.linspace(0, len(lines) - 1, 8).round().astype(int)]
     sample += [("class", 0), ("class", 1), ("class", 2), ("riser", 0), ("riser", 1), ("mass", 0)]
-    jobs = [(k, i, f) for k, i in sample for f in (1.0 + H, 1.0 - H)]
+    jobs = [(k, i, f) for k, i in sample for f in (1.0 + H, 1.0 - H, 1.0 + H_FINE, 1.0 - H_FINE)]
     with mp.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
+        f32 = pool.map_async(f32_loss, [0])
         losses = pool.map(rollout_loss, jobs)
-    fd = []
+        loss_f32 = f32.get()[0]
+    fd, fd_fine = [], []
     for n, (kind, index) in enumerate(sample):
-        dl = (losses[2 * n] - losses[2 * n + 1]) / (2.0 * H)
+        scale = 1.0
         if kind == "line":
-            dl /= float(np.sum(rest0[lines[index]]))       # per unit length of the line, as grad_lines
+            scale = float(np.sum(rest0[lines[index]]))       # per unit length of the line, as grad_lines
         elif kind == "riser":
-            dl /= seg_rest[index]
+            scale = seg_rest[index]
         elif kind == "mass":
-            dl /= segs.pilot_mass
-        fd.append(dl)
+            scale = segs.pilot_mass
+        fd.append((losses[4 * n] - losses[4 * n + 1]) / (2.0 * H) / scale)
+        fd_fine.append((losses[4 * n + 2] - losses[4 * n + 3]) / (2.0 * H_FINE) / scale)
     np.savez_compressed(OUT, state=state, payload=payload, target=target, loss=np.array(ref["loss"]),
                         grad_lines=grad_lines, grad_classes=grad_classes,
                         grad_riser_rest=ref["d_segment_rest"][: segs.segment_count],
                         grad_pilot_mass=np.array(ref["d_mass"]),
                         fd_kind=np.array([k for k, _ in sample]), fd_index=np.array([i for _, i in sample]),
-                        fd_value=np.array(fd), final=ref["final"].astype(np.float32),
+                        fd_value=np.array(fd), fd_fine_value=np.array(fd_fine), loss_f32=np.array(loss_f32),
+                        final=ref["final"].astype(np.float32),
                         order_hash=np.array(order_hash(do, ho)), settle=np.array(SETTLE), steps=np.array(STEPS))
     os.remove(OUT + ".partial.npz")
-    print("wrote", OUT, "loss", ref["loss"], "fd", dict(zip([f"{k}{i}" for k, i in sample], np.round(fd, 8))))
+    print("wrote", OUT, "loss", ref["loss"], "FP32 loss", loss_f32,
+          "fd", dict(zip([f"{k}{i}" for k, i in sample], np.round(fd, 8))))
 
 
 if __name__ == "__main__":

@@ -19,16 +19,17 @@ are stored in FP32 (the tests compare at 1e-3 m).  A hash of each case's
 sweep order is stored too: the tests check that the device still sweeps in
 that order.
 
-Each case also runs a second time in FP64 from the same state with every
-position moved by N(0, 1e-7 m) (about the rounding of an FP32 position of
-a metre): how far that run ends from the first measures how strongly the
-configuration itself amplifies a perturbation of the size FP32 rounding
-makes.  Stored per case: the largest deviation of the fabric (triangle)
-nodes and of the other (line) nodes from the first run's shape at the
-position steps (each relative to its centre of mass), and the largest
-differences of the two norms and of the centre of mass over all steps.
+Each case also runs a second time with FP32 arithmetic: the restatement
+with every vector result rounded to FP32 (oracle.RecentredF32), in the
+frame the device keeps (FP32 offsets from an FP64 origin that follows the
+pilot on a 1/256 m grid).  How far that run ends from the FP64 run measures
+how far FP32 arithmetic of the reference algorithm itself drifts over the
+free run.  Stored per case: the largest deviation of the fabric (triangle)
+nodes and of the other (line) nodes from the FP64 shape at the position
+steps (each relative to its centre of mass), and the largest differences
+of the two norms and of the centre of mass over all steps.
 
-    python tests/golden/make_free_run.py       (about 10 minutes, 6 cores)
+    python tests/golden/make_free_run.py       (about 15 minutes, 6 cores)
 """
 import hashlib
 import multiprocessing as mp
@@ -59,14 +60,11 @@ def order_hash(*orders):
     return h.hexdigest()
 
 
-PERTURBATION = 1e-7
-
-
 def run_case(job):
-    """One FP64 run of a case; `perturbed` moves every initial position by
-    N(0, PERTURBATION).  Returns the per-step diagnostics and the positions
-    (FP64) at the position steps."""
-    name, perturbed = job
+    """One run of a case, FP64 or FP32 (see above).  Returns the per-step
+    diagnostics (centre of mass in world coordinates) and the positions at
+    the position steps."""
+    name, kind = job
     import simwing_b200 as sw
     from oracle import oracle as O
 
@@ -79,12 +77,7 @@ def run_case(job):
     od = d.permuted(*orders)
     st = sw.StepSettings(time_step=1.0 / 120.0, substeps=1, constraint_iterations=48, gravity=(0.0, 0.0, -9.81),
                          velocity_damping=0.25)
-    orc = O.PortStructure(od)
-    if perturbed:
-        s0 = orc.node_states()
-        s0[:, 0, :] += np.random.default_rng(1).normal(0.0, PERTURBATION, s0[:, 0, :].shape)
-        s0[:, 1, :] = s0[:, 0, :]
-        orc.write_node_states(s0)
+    orc = O.PortStructure(od) if kind == "fp64" else O.RecentredF32(od)
     positions, diag = {}, []
     t0 = time.time()
     for k in range(1, steps + 1):
@@ -95,17 +88,17 @@ def run_case(job):
             positions[k] = orc.positions()
     fabric = np.zeros(d.node_count, dtype=bool)
     fabric[d.triangles()["nodes"].astype(np.int64).ravel()] = True
-    print(name, "perturbed" if perturbed else "", "%.0f s" % (time.time() - t0), diag[-1][:3], flush=True)
+    print(name, kind, "%.0f s" % (time.time() - t0), diag[-1][:3], flush=True)
     return {"diag": np.array(diag), "positions": positions, "order_hash": order_hash(*orders), "fabric": fabric}
 
 
 def main():
-    jobs = [(name, p) for name in CASES for p in (False, True)]
+    jobs = [(name, kind) for name in CASES for kind in ("fp64", "f32")]
     with mp.get_context("spawn").Pool(len(jobs)) as pool:
         runs = dict(zip(jobs, pool.map(run_case, jobs)))
     out = {}
     for name, (_, steps, keep) in CASES.items():
-        a, b = runs[(name, False)], runs[(name, True)]
+        a, b = runs[(name, "fp64")], runs[(name, "f32")]
         out[f"{name}_diag"] = a["diag"]
         out[f"{name}_order_hash"] = np.array(a["order_hash"])
         out[f"{name}_steps"] = np.array(steps)
@@ -117,12 +110,14 @@ def main():
                          (a["positions"][k] - a["diag"][k - 1, 3:6])).max(axis=1)
             shape_fabric.append(float(dev[a["fabric"]].max()))
             shape_lines.append(float(dev[~a["fabric"]].max()) if (~a["fabric"]).any() else 0.0)
-        out[f"{name}_sens_shape_fabric"] = np.array(shape_fabric)
-        out[f"{name}_sens_shape_lines"] = np.array(shape_lines)
-        out[f"{name}_sens_norms"] = np.array(float(np.abs(b["diag"][:, :2] - a["diag"][:, :2]).max()))
-        out[f"{name}_sens_com"] = np.array(float(np.abs(b["diag"][:, 3:6] - a["diag"][:, 3:6]).max()))
+        out[f"{name}_f32_shape_fabric"] = np.array(shape_fabric)
+        out[f"{name}_f32_shape_lines"] = np.array(shape_lines)
+        out[f"{name}_f32_norms"] = np.array(float(np.abs(b["diag"][:, :2] - a["diag"][:, :2]).max()))
+        out[f"{name}_f32_com"] = np.array(float(np.abs(b["diag"][:, 3:6] - a["diag"][:, 3:6]).max()))
+        out[f"{name}_f32_strain"] = np.array(float(np.max(np.abs(b["diag"][:, 2] - a["diag"][:, 2]) /
+                                                         np.maximum(a["diag"][:, 2], 1e-300))))
     np.savez_compressed(OUT, **out)
-    print("wrote", OUT, {k: out[k] for k in out if "sens" in k})
+    print("wrote", OUT, {k: out[k] for k in out if "_f32_" in k})
 
 
 if __name__ == "__main__":

@@ -213,8 +213,8 @@ def test_candidate_inspection_needs_contact(cuda_device):
         s.contact_candidates()
 
 
-@pytest.mark.parametrize("name,warm", [("two_sheets", 0), ("stacked_hard", 2)])
-def test_contact_checkpoint_replay_is_bitwise(cuda_device, name, warm):
+@pytest.mark.parametrize("name,warm,replay", [("two_sheets", 0, 3), ("stacked_hard", 2, 1)])
+def test_contact_checkpoint_replay_is_bitwise(cuda_device, name, warm, replay):
     """The checkpoint image carries the contact multiplier table (the warm
     starts and the record book that carry over between steps, as
     SoftBodyCheckpoint::State holds contactMultipliers and contactRecords)
@@ -222,19 +222,20 @@ def test_contact_checkpoint_replay_is_bitwise(cuda_device, name, warm):
     reference's own contact checkpoint fixture (two sheets inside each
     other's envelope, simwing_structure_test.cpp:297-329), whose contact is
     active in the first step, checkpointed before it; and the resting
-    stacked sheets, checkpointed after two steps, whose contacts stay active
-    (with warm-started multipliers) in the replayed steps."""
+    stacked sheets, checkpointed after two steps, whose third step (the last
+    of the steps the parity test above runs) has active contacts with
+    multipliers warm-started from the table the image carries."""
     make, st, _, _, _ = CASES[name]
     d = make()
     s = sw.Structure(d)
     for _ in range(warm):
         s.step(st)
     image = s.checkpoint()
-    first = [s.step(st) for _ in range(3)]
+    first = [s.step(st) for _ in range(replay)]
     states = s.node_states()
     s.restore(image)
     assert s.checkpoint() == image
-    again = [s.step(st) for _ in range(3)]
+    again = [s.step(st) for _ in range(replay)]
     np.testing.assert_array_equal(s.node_states(), states)
     for a, b in zip(first, again):
         assert a.active_contact_count == b.active_contact_count
@@ -272,3 +273,32 @@ def test_failed_contact_step_restores_the_multiplier_table(cuda_device, failure)
     with pytest.raises(sw.ContactStepError if failure == "contact" else (sw.NonFiniteState, sw.ContactStepError)):
         tried.step(SLIDE)
     assert tried.checkpoint() == before == twin.checkpoint()
+
+
+@pytest.mark.parametrize("name", ["two_sheets", "stacked_hard", "stacked_compliant"])
+def test_helper_clusters_change_nothing(cuda_device, name):
+    """The detection phases (broadphase, swept queries) run over helper
+    clusters beside the structure's cluster by default; the candidate lists
+    and queries, and so the steps, are bit for bit those of the structure's
+    cluster alone (SWB_OPT_CONTACT_ONE_CLUSTER)."""
+    make, st, steps, _, fails_at = CASES[name]
+    d = make()
+    a = sw.Structure(d)
+    b = sw.Structure(d, sw.SolverOptions(flags=sw.abi.OPT_CONTACT_ONE_CLUSTER))
+    for k in range(steps if fails_at is None else fails_at):
+        ga, gb = a.step(st), b.step(st)
+        assert ga.active_contact_count == gb.active_contact_count
+        assert ga.maximum_contact_penetration == gb.maximum_contact_penetration
+        np.testing.assert_array_equal(a.node_states(), b.node_states())
+
+
+def test_helper_clusters_on_a_large_scene(cuda_device):
+    """The same on 48 x 48 stacked sheets (a candidate list of about 100,000
+    features spread over every cluster), three consecutive steps."""
+    d = stacked_sheets(n=48, compliance=1e-3)
+    a = sw.Structure(d)
+    b = sw.Structure(d, sw.SolverOptions(flags=sw.abi.OPT_CONTACT_ONE_CLUSTER))
+    for _ in range(3):
+        ga, gb = a.step(SLIDE), b.step(SLIDE)
+        assert ga.active_contact_count == gb.active_contact_count
+    np.testing.assert_array_equal(a.node_states(), b.node_states())

@@ -169,10 +169,16 @@ def test_cluster_schedule_invariants(ctas, split):
 
 
 def test_split_stages_cut_cluster_barriers_on_the_full_wing():
+    """Split stages: the stages of records inside one CTA's patch end in CTA
+    barriers, so fewer cluster barriers than the classic schedule's one per
+    stage (the schedule verifier checks that no node is touched by two CTAs
+    between cluster barriers)."""
     d = sw.generate_wing()
     classic, _, _ = sw.plan_schedule(d)
     split, _, _ = sw.plan_schedule(d, sw.SolverOptions(flags=abi.OPT_SPLIT_STAGES))
-    assert split.cluster_barriers_per_iteration <= 16 < classic.cluster_barriers_per_iteration
+    assert classic.cluster_barriers_per_iteration == classic.local_stages_per_iteration
+    assert split.cluster_barriers_per_iteration < classic.cluster_barriers_per_iteration
+    assert split.local_stages_per_iteration > split.cluster_barriers_per_iteration
 
 
 def test_full_wing_fits_one_cluster():
