@@ -447,6 +447,25 @@ swb_status swb_diagnostics_noalloc(int32_t device,
                                    uint64_t constraint_count,
                                    swb_diagnostics* out);
 
+/* A ground plane under the structure (no counterpart in the reference's
+ * structural step, which has none: its only plane is the payload's support
+ * plane, which the adapter leaves free).  After every constraint iteration
+ * each free node is projected back onto the side normal . x >= offset
+ * (world coordinates, metres; `normal` of unit length), rigidly; with
+ * friction > 0 its motion over the substep along the plane is then
+ * resisted by Coulomb friction: stopped while it stays below friction x
+ * the depth of the normal correction, else shortened by that length.
+ * enabled = 0 (or a null pointer) removes the plane.  Differentiable
+ * rollouts take the frictionless plane. */
+typedef struct swb_ground {
+    swb_vec3 normal;
+    double offset;
+    double friction;
+    uint32_t enabled;
+    uint32_t reserved;
+} swb_ground;
+swb_status swb_structure_set_ground(swb_structure* structure, const swb_ground* ground);
+
 /* The device forms of the step's two short math functions on host arrays
  * (no counterpart in the reference; for checking them on the GPU they run
  * on): which = SWB_FAST_ATAN2 gives out[i] = atan2(a[i], b[i]) by the
@@ -624,6 +643,11 @@ swb_status swb_batch_step(swb_batch* batch,
                           const swb_step_settings* settings,
                           int32_t steps,
                           int32_t* statuses);
+
+/* The ground plane of swb_structure_set_ground for every structure of the
+ * batch (one plane for the whole launch); a null pointer or enabled = 0
+ * removes it. */
+swb_status swb_batch_set_ground(swb_batch* batch, const swb_ground* ground);
 
 typedef struct swb_batch_report {
     int32_t structures;

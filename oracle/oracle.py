@@ -44,6 +44,7 @@ _PORT = {
     "swo_write_payload": (C.c_int, [C.c_void_p, P(abi.PayloadState)]),
     "swo_read_segment_lambdas": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swo_evaluate_dihedral": (None, [C.c_void_p, C.c_void_p]),
+    "swo_set_ground": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 _REF = {
     "swref_last_error": (C.c_char_p, []),
@@ -80,7 +81,7 @@ _ADJ = {
     "swa_rollout_gradient": (C.c_int, [P(abi.StructureDefinition), P(abi.StepSettings), C.c_int, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        P(C.c_double), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                       P(C.c_double)]),
+                                       P(C.c_double), C.c_void_p]),
 }
 
 _libs = {}
@@ -206,6 +207,10 @@ class PortStructure(_Base):
 
     def write_payload(self, p):
         self._check(self._lib().swo_write_payload(self._h, C.byref(p)))
+
+    def set_ground(self, normal=(0.0, 0.0, 1.0), offset=0.0, friction=0.0, enabled=True):
+        g = abi.Ground(abi.Vec3(*normal), float(offset), float(friction), 1 if enabled else 0, 0)
+        self._check(self._lib().swo_set_ground(self._h, C.byref(g)))
 
     def segment_lambdas(self, n):
         out = np.zeros(n)
@@ -340,7 +345,7 @@ def adjoint_library() -> C.CDLL:
 
 
 def rollout_gradient(definition, settings, steps, target, weights, forces=None, state=None, payload=None,
-                     trajectory=None, trajectory_payloads=None):
+                     trajectory=None, trajectory_payloads=None, ground=None):
     """FP64 loss and gradient of sum_i w_i |x_i(T) - target_i|^2 / sum w over
     `steps` steps (the definition's insertion order is the sweep order) from
     `state` (N x 3 x 3 node states as read_nodes returns: position, previous,
@@ -349,6 +354,7 @@ def rollout_gradient(definition, settings, steps, target, weights, forces=None, 
     pilot).  `trajectory` (steps x N x 3 x 3) and `trajectory_payloads`
     (steps x 13), when given, restart every step s > 0 from that state, so
     the reverse sweep is evaluated along another solver's trajectory.
+    `ground` = (normal xyz, offset) adds the frictionless ground plane.
     Returns a dict: loss, final (N x 3), d_rest and d_comp
     (per constraint), d_dihedral_comp (per dihedral), d_segment_rest (per
     suspension segment, definition order), d_mass."""
@@ -373,6 +379,7 @@ def rollout_gradient(definition, settings, steps, target, weights, forces=None, 
     out = {"final": np.zeros((n, 3)), "d_rest": np.zeros(max(m, 1)), "d_comp": np.zeros(max(m, 1)),
            "d_dihedral_comp": np.zeros(max(h, 1)), "d_segment_rest": np.zeros(max(ns, 1))}
     loss, mass = C.c_double(), C.c_double()
+    g = None if ground is None else np.ascontiguousarray([*ground[0], ground[1]], dtype=np.float64)
     rc = lib.swa_rollout_gradient(definition.pointer, C.byref(settings), int(steps),
                                   None if x0 is None else x0.ctypes.data, None if p0 is None else p0.ctypes.data,
                                   None if traj is None else traj.ctypes.data,
@@ -380,7 +387,8 @@ def rollout_gradient(definition, settings, steps, target, weights, forces=None, 
                                   None if f is None else f.ctypes.data, target.ctypes.data, weights.ctypes.data,
                                   C.byref(loss), out["final"].ctypes.data, out["d_rest"].ctypes.data,
                                   out["d_comp"].ctypes.data, out["d_dihedral_comp"].ctypes.data,
-                                  out["d_segment_rest"].ctypes.data, C.byref(mass))
+                                  out["d_segment_rest"].ctypes.data, C.byref(mass),
+                                  None if g is None else g.ctypes.data)
     if rc != 0:
         raise OracleError(abi.INVALID_ARGUMENT, lib.swa_last_error().decode())
     out["d_rest"], out["d_comp"] = out["d_rest"][:m], out["d_comp"][:m]

@@ -679,6 +679,7 @@ struct StepTape {
     Payload<double> P_end;                            // after the iterations
     std::vector<V3<double>> fin_x, fin_v;             // attachment nodes at finish
     std::vector<double> fin_lambda;
+    std::vector<uint8_t> ground_moved;                // [it * n + i]: the ground plane moved the node
 };
 
 struct Rollout {
@@ -690,6 +691,11 @@ struct Rollout {
     Payload<double> P;
     std::vector<StepTape> tape;
     std::vector<uint64_t> seams;  // seam stitch indices in sweep order
+    // frictionless ground plane normal . x >= offset after each iteration
+    // (the device's swb_structure_set_ground; no reference counterpart)
+    bool ground = false;
+    V3<double> ground_normal{0, 0, 1};
+    double ground_offset = 0.0;
 };
 
 bool forward_step(Rollout& R, bool record) {
@@ -762,6 +768,16 @@ bool forward_step(Rollout& R, bool record) {
             for (const Seg& s : M.seg) rest.push_back(s.rest);
             if (!line_iteration(M, P, xs, seg_lambda, rest, M.mass, R.dt)) return false;
             for (size_t k = 0; k < M.att_nodes.size(); ++k) x[M.att_nodes[k]] = xs[k];
+        }
+        if (R.ground) {
+            if (record) T.ground_moved.resize(static_cast<size_t>(R.iterations) * M.n, 0);
+            for (uint64_t i = 0; i < M.n; ++i) {
+                if (M.w[i] == 0.0) continue;
+                const double c = dot(R.ground_normal, x[i]) - R.ground_offset;
+                if (!(c < 0.0)) continue;
+                x[i] = sub(x[i], mul(R.ground_normal, c));
+                if (record) T.ground_moved[static_cast<size_t>(it) * M.n + i] = 1;
+            }
         }
     }
     if (R.iterations > 0)
@@ -893,6 +909,12 @@ void reverse_step(const Rollout& R, const StepTape& T, std::vector<V3<double>>& 
     // ---- iterations -------------------------------------------------------------
     std::vector<double> lamb(M.m, 0.0), hlamb(M.h, 0.0), seglamb(ns, 0.0);
     for (int it = R.iterations - 1; it >= 0; --it) {
+        // the ground plane closed the iteration: a node it moved keeps only
+        // its position along the plane
+        if (R.ground)
+            for (uint64_t i = 0; i < M.n; ++i)
+                if (T.ground_moved[static_cast<size_t>(it) * M.n + i])
+                    xb[i] = sub(xb[i], mul(R.ground_normal, dot(R.ground_normal, xb[i])));
         if (M.susp) {
             // inputs: com 3, q 4, lambda ns, xs 3*na, rest ns, mass 1
             constexpr int N = 3 + 4 + 2 + 6 + 2 + 1;
@@ -1016,6 +1038,7 @@ const char* swa_last_error() { return g_err.c_str(); }
 // load.  `step_states` / `step_payloads` (nullable; steps x node_count x 6
 // and steps x 13 in the same layouts) restart every step s > 0 from a given
 // trajectory, so that the reverse sweep runs along another solver's states.
+// `ground` (nullable: none) is a frictionless ground plane (normal xyz, offset).
 // Then evaluates the loss against `target` (node_count xyz) with node weights `weights` and its gradient.  Outputs
 // (nullable): final positions (node_count xyz), d rest / d compliance per
 // constraint, d compliance per dihedral, d rest per suspension segment
@@ -1025,7 +1048,7 @@ int swa_rollout_gradient(const swb_structure_definition* def, const swb_step_set
                          const double* step_payloads, const double* forces, const double* target,
                          const double* weights, double* loss,
                          double* final_xyz, double* d_rest, double* d_comp, double* d_dihedral_comp,
-                         double* d_segment_rest, double* d_mass) {
+                         double* d_segment_rest, double* d_mass, const double* ground) {
     try {
         Rollout R;
         if (!build_model(*def, R.M, g_err)) return 1;
@@ -1040,6 +1063,11 @@ int swa_rollout_gradient(const swb_structure_definition* def, const swb_step_set
         R.g = fromabi(st->gravity);
         R.ref = fromabi(st->damping_reference_velocity);
         R.iterations = st->constraint_iterations;
+        if (ground) {
+            R.ground = true;
+            R.ground_normal = {ground[0], ground[1], ground[2]};
+            R.ground_offset = ground[3];
+        }
         if (forces)
             for (uint64_t i = 0; i < M.n; ++i) R.M.pending[i] = {forces[3 * i], forces[3 * i + 1], forces[3 * i + 2]};
         for (uint64_t i = 0; i < M.m; ++i)

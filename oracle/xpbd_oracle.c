@@ -308,6 +308,11 @@ typedef struct swo_structure {
     double minimum_line_length, maximum_line_residual;
     double max_residual;
     V3 line_force, line_moment;
+    /* ground plane (swb_structure_set_ground; no counterpart in the
+     * reference, so its parity is the device's against this restatement) */
+    int ground;
+    V3 ground_normal;
+    double ground_offset, ground_friction;
 } swo_structure;
 
 /* ---------------- membranes (soft_body.cpp, membrane.cpp) ---------------- */
@@ -1191,6 +1196,40 @@ typedef struct {
     Payload payload, previous_payload;
 } Saved;
 
+/* The ground plane after each iteration: a free node below it goes back
+ * onto it along the normal; with friction its motion along the plane since
+ * the substep's start is stopped while it is at most friction x the
+ * correction, else shortened by that length. */
+static void ground_pass(swo_structure* s) {
+    const V3 n = s->ground_normal;
+    for (uint64_t i = 0; i < s->n; ++i) {
+        Node* p = &s->nodes[i];
+        if (!(p->w > 0.0)) continue;
+        const double c = dot(n, p->x) - s->ground_offset;
+        if (!(c < 0.0)) continue;
+        p->x = sub(p->x, smul(c, n));
+        if (s->ground_friction > 0.0) {
+            V3 d = sub(p->x, p->prev);
+            d = sub(d, smul(dot(n, d), n));
+            const double length = sqrt(dot(d, d)), limit = -s->ground_friction * c;
+            const double k = length <= limit ? 1.0 : limit / length;
+            p->x = sub(p->x, smul(k, d));
+        }
+    }
+}
+
+swb_status swo_set_ground(swo_structure* s, const swb_ground* g) {
+    if (!g || !g->enabled) {
+        s->ground = 0;
+        return SWB_OK;
+    }
+    s->ground = 1;
+    s->ground_normal = fromabi(g->normal);
+    s->ground_offset = g->offset;
+    s->ground_friction = g->friction;
+    return SWB_OK;
+}
+
 static swb_status substep(swo_structure* s, double dt, const swb_step_settings* st) {
     const V3 g = fromabi(st->gravity);
     pressure_scatter(s);
@@ -1237,6 +1276,7 @@ static swb_status substep(swo_structure* s, double dt, const swb_step_settings* 
             swb_status r = line_iteration(s, dt);
             if (r != SWB_OK) return r;
         }
+        if (s->ground) ground_pass(s);
     }
     if (st->constraint_iterations > 0)
         for (int q = 0; q < closing; ++q) cable_pair(s, inv_dt2);

@@ -665,6 +665,13 @@ class Structure:
     def set_uniform_pressure(self, pressure: float) -> None:
         _check(self._lib.swb_structure_set_uniform_pressure(self._h, float(pressure)))
 
+    def set_ground(self, normal=(0.0, 0.0, 1.0), offset: float = 0.0, friction: float = 0.0,
+                   enabled: bool = True) -> None:
+        """A ground plane normal . x >= offset (swb_structure_set_ground);
+        enabled=False removes it."""
+        g = abi.Ground(Vec3(*normal), float(offset), float(friction), 1 if enabled else 0, 0)
+        _check(self._lib.swb_structure_set_ground(self._h, C.byref(g)))
+
     def step(self, settings: abi.StepSettings | None = None, diagnostics: bool = True):
         s = settings if settings is not None else StepSettings()
         d = abi.Diagnostics()
@@ -860,6 +867,13 @@ class Batch:
 
     def structure(self, index: int) -> Structure:
         return self._structures[index]
+
+    def set_ground(self, normal=(0.0, 0.0, 1.0), offset: float = 0.0, friction: float = 0.0,
+                   enabled: bool = True) -> None:
+        """The ground plane of Structure.set_ground for every structure of
+        the batch (swb_batch_set_ground)."""
+        g = abi.Ground(Vec3(*normal), float(offset), float(friction), 1 if enabled else 0, 0)
+        _check(self._lib.swb_batch_set_ground(self._h, C.byref(g)))
 
     def step(self, settings: abi.StepSettings, steps: int = 1) -> np.ndarray:
         """Steps every structure; returns the per-structure status codes.

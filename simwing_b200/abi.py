@@ -270,6 +270,11 @@ class SegmentState(C.Structure):
                 ("commanded_rest_length", C.c_double), ("tension", C.c_double)]
 
 
+class Ground(C.Structure):
+    _fields_ = [("normal", Vec3), ("offset", C.c_double), ("friction", C.c_double), ("enabled", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
 class Wrench(C.Structure):
     _fields_ = [("force", Vec3), ("moment", Vec3)]
 
@@ -365,6 +370,7 @@ _PROTOTYPES = {
     "swb_structure_set_external_forces": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swb_structure_set_face_pressure": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double]),
     "swb_structure_set_uniform_pressure": (C.c_int, [C.c_void_p, C.c_double]),
+    "swb_structure_set_ground": (C.c_int, [C.c_void_p, C.c_void_p]),
     "swb_structure_step": (C.c_int, [C.c_void_p, P(StepSettings), P(Diagnostics)]),
     "swb_structure_step_many": (C.c_int, [C.c_void_p, P(StepSettings), C.c_int32, P(Diagnostics)]),
     "swb_structure_diagnostics": (C.c_int, [C.c_void_p, P(Diagnostics)]),
@@ -395,6 +401,7 @@ _PROTOTYPES = {
     "swb_batch_size": (C.c_uint64, [C.c_void_p]),
     "swb_batch_structure": (C.c_void_p, [C.c_void_p, C.c_uint64]),
     "swb_batch_step": (C.c_int, [C.c_void_p, P(StepSettings), C.c_int32, C.c_void_p]),
+    "swb_batch_set_ground": (C.c_int, [C.c_void_p, C.c_void_p]),
     "swb_batch_get_report": (C.c_int, [C.c_void_p, P(BatchReport)]),
     "swb_batch_last_step_ms": (C.c_double, [C.c_void_p]),
     "swb_rollout_create": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, P(C.c_void_p)]),

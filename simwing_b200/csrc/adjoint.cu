@@ -225,7 +225,7 @@ struct RolloutImpl {
         if (!tape.empty() && tape_iterations == iterations) return;
         for (TapeStep& t : tape)
             for (void* q : {static_cast<void*>(t.dist), static_cast<void*>(t.dih), static_cast<void*>(t.seam),
-                            static_cast<void*>(t.line), static_cast<void*>(t.finish)}) {
+                            static_cast<void*>(t.line), static_cast<void*>(t.finish), static_cast<void*>(t.ground)}) {
                 cudaFree(q);
                 owned.erase(std::remove(owned.begin(), owned.end(), q), owned.end());
             }
@@ -238,6 +238,7 @@ struct RolloutImpl {
             t.seam = ralloc<float4>(owned, 2 * static_cast<size_t>(rs));
             t.line = ralloc<PilotTape>(owned, it);
             t.finish = ralloc<PilotTape>(owned, 1);
+            t.ground = ralloc<uint8_t>(owned, it * S->def.nodes.size());
             t.r0 = r0;
             t.r1 = r1;
             t.rs = rs;
@@ -313,6 +314,8 @@ struct RolloutImpl {
         if (st.cable_sweep_pairs != 0)
             raise(SWB_UNSUPPORTED, "differentiable rollouts with load-path cable sweep pairs are not available");
         if (st.substeps != 1) raise(SWB_UNSUPPORTED, "differentiable rollouts take one substep per step");
+        if (S->cparams.ground && S->cparams.ground_friction > 0.0f)
+            raise(SWB_UNSUPPORTED, "differentiable rollouts take a frictionless ground plane");
         const size_t N = S->def.nodes.size();
         double wsum = 0.0;
         for (size_t i = 0; i < N; ++i) {
@@ -400,6 +403,8 @@ struct RolloutImpl {
         ap.damping = static_cast<float>(std::exp(-settings.velocity_damping * dt));
         ap.gravity = make_float3(settings.gravity.x, settings.gravity.y, settings.gravity.z);
         ap.iterations = settings.constraint_iterations;
+        ap.ground = S->cparams.ground;
+        ap.ground_normal = S->cparams.ground_normal;
         cudaLaunchAttribute attr[1];
         const cudaLaunchConfig_t cfg = config(smem, attr);
         int cur = 0;

@@ -459,7 +459,25 @@ __global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(con
     // second one's barrier.
     const int line_stage = I.susp_cta >= 0 ? I.line_stage : -1;
     const bool line_warp = line_stage >= 0 && owner && (tid >> 5) == static_cast<int>(blockDim.x >> 5) - 1;
+    const uint32_t slots = __ldg(I.patch_begin + p.ctas);
     for (int it = p.iterations - 1; it >= 0; --it) {
+        // the ground plane closed the forward iteration: a node it moved
+        // kept only its position along the plane (x' = x - n (n.x - off)),
+        // so its adjoint loses the normal component
+        if (p.ground) {
+            const uint8_t* moved = p.tape.ground + static_cast<size_t>(it) * slots + base;
+            const float3 nrm = p.ground_normal;
+            for (uint32_t i = tid; i < n; i += blockDim.x) {
+                if (!moved[i]) continue;
+                float4 B = xb[i];
+                const float d = nrm.x * B.x + nrm.y * B.y + nrm.z * B.z;
+                B.x -= d * nrm.x;
+                B.y -= d * nrm.y;
+                B.z -= d * nrm.z;
+                xb[i] = B;
+            }
+            cluster.sync();
+        }
         if (I.susp_cta >= 0 && line_stage < 0) {
             if (pilot_warp) line_reverse(pa, *ap, p.line_jac + static_cast<size_t>(it) * line_block, xb);
             cluster.sync();

@@ -226,6 +226,7 @@ struct BatchImpl {
     size_t smem_limit = 0;
     cudaLaunchAttribute launch_attr[1] = {};
     double last_ms = 0.0;
+    swb_ground ground{};   // the launch's ground plane (enabled = 0: none)
     std::vector<int> candidates;
     std::vector<int> candidate_threads;
     std::vector<double> candidate_ms;
@@ -350,6 +351,13 @@ struct BatchImpl {
         cp.smem_x = 0;
         cp.smem_v = P.smem_v;
         cp.smem_offsets = P.smem_offsets;
+        if (ground.enabled) {
+            cp.ground = 1;
+            cp.ground_normal = make_float3(static_cast<float>(ground.normal.x), static_cast<float>(ground.normal.y),
+                                           static_cast<float>(ground.normal.z));
+            cp.ground_offset = ground.offset;
+            cp.ground_friction = static_cast<float>(ground.friction);
+        }
         return cp;
     }
 
@@ -607,6 +615,28 @@ swb_status swb_batch_step(swb_batch* batch, const swb_step_settings* settings, i
     if (call != SWB_OK) return call;
     if (result != SWB_OK) set_last_error(message);
     return result;
+}
+
+swb_status swb_batch_set_ground(swb_batch* batch, const swb_ground* g) {
+    return swb::guarded([&] {
+        if (!batch) swb::raise(SWB_INVALID_ARGUMENT, "null batch");
+        swb::BatchImpl& b = batch->b;
+        if (!g || !g->enabled) {
+            b.ground = swb_ground{};
+        } else {
+            const double nn = g->normal.x * g->normal.x + g->normal.y * g->normal.y + g->normal.z * g->normal.z;
+            if (!std::isfinite(nn) || std::fabs(nn - 1.0) > 1e-9)
+                swb::raise(SWB_INVALID_ARGUMENT, "ground normal must be a unit vector");
+            if (!std::isfinite(g->offset) || !std::isfinite(g->friction) || g->friction < 0.0)
+                swb::raise(SWB_INVALID_ARGUMENT, "ground offset and friction must be finite, friction >= 0");
+            b.ground = *g;
+        }
+        // the captured graph holds the old parameters
+        if (b.graph) {
+            cudaGraphExecDestroy(b.graph);
+            b.graph = nullptr;
+        }
+    });
 }
 
 swb_status swb_batch_get_report(const swb_batch* batch, swb_batch_report* out) {

@@ -252,6 +252,38 @@ __device__ __forceinline__ void tape_pilot(PilotTape& t, const DevPayloadState& 
     }
 }
 
+// The ground plane (swb_structure_set_ground) on this CTA's nodes: a free
+// node below the plane is moved back onto it along the normal; with
+// friction its motion along the plane since the step start (`start`) is
+// then stopped while it is at most friction x the correction, else
+// shortened by that length.  `tape` (taping launches) records which nodes
+// the plane moved.
+__device__ __forceinline__ void ground_pass(float4* x, uint32_t n, float3 nrm, float off, float mu,
+                                            const float4* start, uint8_t* tape) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        float4 X = x[i];
+        const float c = X.w != 0.0f ? dot(nrm, f3(X)) - off : 0.0f;
+        const bool active = c < 0.0f;
+        if (active) {
+            X.x -= c * nrm.x;
+            X.y -= c * nrm.y;
+            X.z -= c * nrm.z;
+            if (mu > 0.0f) {
+                const float4 P = __ldg(start + i);
+                float3 d = make_float3(X.x - P.x, X.y - P.y, X.z - P.z);
+                d = d - nrm * dot(nrm, d);
+                const float len = length(d), lim = -mu * c;
+                const float k = len <= lim ? 1.0f : lim / len;
+                X.x -= d.x * k;
+                X.y -= d.y * k;
+                X.z -= d.z * k;
+            }
+            x[i] = X;
+        }
+        if (tape) tape[i] = active ? 1u : 0u;
+    }
+}
+
 // kPacked = false: one structure per cluster (cluster index = structure).
 // One load-path cable pair (soft_body.cpp:1265-1286): the levels of the
 // reverse and the forward pass over this CTA's cable and tie records, a
@@ -322,8 +354,8 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         slot = p.slots[blockIdx.x];
         if (slot.instance < 0) {
             // idle rank: take every cluster barrier the busy ranks take
-            const int barriers = 3 + p.iterations * (slot.stages + slot.suspension) +
-                                 (p.iterations > 0 ? slot.seam_stages : 0) + (slot.guard ? 3 : 0);
+            const int barriers = 3 + p.iterations * (slot.stages + slot.suspension + (p.ground ? 1 : 0)) +
+                                 (p.iterations > 0 ? slot.seam_stages : 0) + (slot.guard && !p.ground ? 3 : 0);
             for (int b = 0; b < barriers; ++b) cluster.sync();
             return;
         }
@@ -346,8 +378,15 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     // momentum guard: `guard` = this structure runs it; `guard_c` = the
     // cluster takes its barriers (a packed cluster when any of its
     // structures runs it); `sctas` = the structure's ranks
-    const bool guard = I.momentum_guard != 0;
-    const bool guard_c = kPacked ? slot.guard != 0 : guard;
+    // a ground plane is an external load, as the pilot's lines and contact
+    // are: the momentum guard stands down while one is set
+    const bool guard = I.momentum_guard != 0 && !p.ground;
+    const bool guard_c = kPacked ? slot.guard != 0 && !p.ground : guard;
+    const float ground_off =
+        p.ground ? static_cast<float>(p.ground_offset - (p.ground_normal.x * I.origin_in[0] +
+                                                         p.ground_normal.y * I.origin_in[1] +
+                                                         p.ground_normal.z * I.origin_in[2]))
+                 : 0.0f;
     const int sctas = kPacked ? slot.ctas : p.ctas;
 
     if (tid < p.ctas) peers[tid] = cluster.map_shared_rank(x, tid);
@@ -571,6 +610,12 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             cluster.sync();
         }
         if constexpr (kContact) contact_iteration(cctx, cluster);
+        if (p.ground) {
+            uint8_t* gt = nullptr;
+            if constexpr (kTape) gt = p.tape.ground + static_cast<size_t>(it) * pbeg_s[sctas] + base;
+            ground_pass(x, n, p.ground_normal, ground_off, p.ground_friction, I.pos_in + base, gt);
+            cluster.sync();
+        }
     }
     // closing cable pairs
     for (int q = 0; q < (p.iterations > 0 ? closing_pairs : pairs); ++q)

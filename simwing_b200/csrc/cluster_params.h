@@ -234,6 +234,7 @@ struct TapeStep {
     float4* seam;
     PilotTape* line;       // [iterations]
     PilotTape* finish;     // [1]
+    uint8_t* ground;       // [iterations][slots]: 1 where the ground projection moved the node
     uint32_t r0, r1, rs;   // records per kind and seam records
     const AdjointPilot* pilot;
 };
@@ -274,6 +275,12 @@ struct ClusterParams {
     // of the (cooperative) launch; 0 = the structure's cluster alone
     int helper_clusters;
     dev::GridBarrier grid;
+    // ground plane (swb_structure_set_ground), the same for every structure
+    // of the launch: normal . x >= offset in world coordinates; 0 = none
+    int ground;
+    float ground_friction;
+    float3 ground_normal;
+    double ground_offset;
 };
 
 // Parameters of the reverse step kernel (one structure, one cluster).
@@ -301,6 +308,8 @@ struct AdjointParams {
     float3 gravity;
     int iterations;
     uint32_t smem_xb, smem_vb, smem_lam0, smem_lam1, smem_acc0r, smem_acc0c, smem_acc1c, smem_offsets;
+    int ground;                    // the frictionless ground plane of the forward step (ClusterParams)
+    float3 ground_normal;
 };
 
 }  // namespace swb

@@ -1535,6 +1535,28 @@ swb_status swb_structure_set_face_pressure(swb_structure* s, uint64_t triangle, 
     });
 }
 
+swb_status swb_structure_set_ground(swb_structure* s, const swb_ground* g) {
+    return guarded([&] {
+        if (!s) raise(SWB_INVALID_ARGUMENT, "null structure");
+        StructureImpl& m = s->s;
+        if (!g || !g->enabled) {
+            m.cparams.ground = 0;
+            return;
+        }
+        const double nn = g->normal.x * g->normal.x + g->normal.y * g->normal.y + g->normal.z * g->normal.z;
+        if (!std::isfinite(nn) || std::fabs(nn - 1.0) > 1e-9)
+            raise(SWB_INVALID_ARGUMENT, "ground normal must be a unit vector");
+        if (!std::isfinite(g->offset) || !std::isfinite(g->friction) || g->friction < 0.0)
+            raise(SWB_INVALID_ARGUMENT, "ground offset and friction must be finite, friction >= 0");
+        if (!m.cluster_mode) raise(SWB_UNSUPPORTED, "the ground plane needs the cluster schedule");
+        m.cparams.ground = 1;
+        m.cparams.ground_normal = make_float3(static_cast<float>(g->normal.x), static_cast<float>(g->normal.y),
+                                              static_cast<float>(g->normal.z));
+        m.cparams.ground_offset = g->offset;
+        m.cparams.ground_friction = static_cast<float>(g->friction);
+    });
+}
+
 swb_status swb_structure_set_uniform_pressure(swb_structure* s, double dp) {
     return guarded([&] {
         if (!s) raise(SWB_INVALID_ARGUMENT, "null structure");

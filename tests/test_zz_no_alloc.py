@@ -76,10 +76,15 @@ def assert_matches(got, ref):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["patch", "wing"])
 def test_noalloc_diagnostics_match_structure_diagnostics_twice(cuda_device, name):
-    # the wing has no pilot here, so the state carries no frame offset and
-    # the node arrays read back are the device's FP32 values exactly
+    # the wing has no pilot here, and both definitions are moved so that
+    # their bounding box is centred on the origin: the state's FP64 origin
+    # (the box's centre on a 1/256 m grid) is then zero, and the node arrays
+    # read back are the device's FP32 values exactly
     definition = sw.generate_patch() if name == "patch" else \
         sw.generate_wing(cells=8, chordwise=16, spanwise_per_cell=2, rib_layers=3, pilot=0)
+    pos = definition.nodes()["position"]
+    for axis in "xyz":
+        pos[axis] -= 0.5 * (pos[axis].min() + pos[axis].max())
     with sw.Structure(definition) as structure:
         settings = step_settings()
         for call in range(2):
