@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--batch-size", type=int, default=64)
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-batched-adjoint", action="store_true")
     p.add_argument("--no-membrane-wing", action="store_true")
     p.add_argument("--no-contact", action="store_true")
     p.add_argument("--no-coupling", action="store_true")
@@ -366,6 +367,68 @@ def adjoint_leg(sw, st, device, steps=240, interval=16):
     return out
 
 
+def batched_adjoint_leg(sw, st, device, wings=32, steps=240, interval=16, group=16):
+    """Batched adjoint with contact: `wings` (32) wings of cells ~ U{30..50}
+    x 45 chordwise (about 20-35k triangles), each with its line rest
+    lengths scaled by lognormal(0, 0.03) from its own seed, settled 20
+    steps, above a frictionless ground plane 0.3 m under its pilot (the
+    ground-plane contact of the configuration; its line-line contact is not
+    built); per wing a `steps`-step rollout with a checkpoint every
+    `interval` steps, forward plus backward, the loss the mean squared
+    distance of the fabric nodes to their settled positions.  The rollouts
+    run side by side, `group` at a time (swb_rollout_forward_many and
+    swb_rollout_backward_many); the time is the host's around those calls,
+    tape allocation of the first backward included."""
+    import time
+
+    import numpy as np
+
+    rng = np.random.default_rng(2025)
+    specs = [dict(cells=int(rng.integers(30, 51)), chordwise=45, seed=7000 + i) for i in range(wings)]
+    opts = sw.SolverOptions(device=device)
+    total_fwd = total_bwd = 0.0
+    tri, hits = [], 0
+    for start in range(0, wings, group):
+        structures, rollouts, targets, weights = [], [], [], []
+        for spec in specs[start:start + group]:
+            d = sw.generate_wing(**spec)
+            tri.append(int(d.counts()["triangles"]))
+            wrng = np.random.default_rng(spec["seed"])
+            rest = d.constraints()["rest_length"]
+            for g in sw.line_groups(d):
+                rest[g] *= float(np.exp(wrng.normal(0.0, 0.03)))
+            s = sw.Structure(d, opts)
+            for _ in range(20):
+                s.step(st, diagnostics=False)
+            pilot_z = s.suspension_state().center_of_mass[2]
+            s.set_ground((0.0, 0.0, 1.0), pilot_z - 0.3, 0.0)
+            w = np.zeros(s.node_count)
+            w[d.triangles()["nodes"].astype(np.int64).ravel()] = 1.0
+            structures.append(s)
+            targets.append(s.positions())
+            weights.append(w)
+            rollouts.append(sw.Rollout(s, steps, interval))
+        t0 = time.perf_counter()
+        sw.rollout_forward_many(rollouts, st, targets, weights)
+        t1 = time.perf_counter()
+        grads = sw.rollout_backward_many(rollouts)
+        t2 = time.perf_counter()
+        total_fwd += t1 - t0
+        total_bwd += t2 - t1
+        hits += sum(1 for g in grads if np.isfinite(g["d_rest"]).all())
+        for r in rollouts:
+            r.close()
+        for s in structures:
+            s.close()
+    return {"workload": f"{wings} wings, cells U{{30..50}} x 45 chordwise, line rest lengths x lognormal(0, 0.03), "
+                        f"frictionless ground plane 0.3 m under each pilot; {steps}-step rollout forward + backward "
+                        f"per wing, checkpoint every {interval} steps, {group} rollouts side by side",
+            "wings": wings, "triangles_min": min(tri), "triangles_max": max(tri), "steps": steps,
+            "forward_s": total_fwd, "backward_s": total_bwd,
+            "wing_gradients_per_s": wings / (total_fwd + total_bwd), "finite_gradients": hits,
+            "line_line_contact": "not built"}
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -602,6 +665,9 @@ def main():
     adjoint = None
     if not args.no_adjoint and rank == 0:
         adjoint = adjoint_leg(sw, st, local, args.adjoint_steps, args.adjoint_interval)
+    batched_adjoint = None
+    if not args.no_batched_adjoint and rank == 0:
+        batched_adjoint = batched_adjoint_leg(sw, st, local)
 
     membrane_wing = None
     if not args.no_membrane_wing and rank == 0:
@@ -640,6 +706,7 @@ def main():
             "final_diagnostics": {"finite": bool(diag.finite), "max_distance_error": diag.maximum_distance_error},
             "batched": batched,
             "adjoint": adjoint,
+            "batched_adjoint": batched_adjoint,
             "membrane_wing": membrane_wing,
             "contact": contact,
             "coupling": coupling,

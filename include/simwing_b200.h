@@ -715,6 +715,26 @@ swb_status swb_rollout_forward(swb_rollout* rollout,
                                double* loss);
 swb_status swb_rollout_backward(swb_rollout* rollout,
                                 const swb_rollout_gradient* gradient);
+/* The forward of `count` rollouts at once (targets_xyz[k], weights[k] and
+ * losses[k] as for swb_rollout_forward): every rollout's launches are
+ * enqueued first, each on its structure's own stream, so that the
+ * structures run side by side on the device, and then each is waited for.
+ * `statuses` (nullable, `count` entries) receives each rollout's status;
+ * the return value is SWB_OK or the first failure. */
+swb_status swb_rollout_forward_many(swb_rollout* const* rollouts,
+                                    uint64_t count,
+                                    const swb_step_settings* settings,
+                                    const double* const* targets_xyz,
+                                    const double* const* weights,
+                                    double* losses,
+                                    int32_t* statuses);
+/* The backward of `count` rollouts at once, as swb_rollout_forward_many
+ * runs their forwards; gradients[k] (or none with a null array) receives
+ * rollout k's gradient. */
+swb_status swb_rollout_backward_many(swb_rollout* const* rollouts,
+                                     uint64_t count,
+                                     const swb_rollout_gradient* gradients,
+                                     int32_t* statuses);
 /* World positions at the end of the last forward (node_count x 3). */
 swb_status swb_rollout_final_positions(const swb_rollout* rollout,
                                        double* xyz,

@@ -935,21 +935,29 @@ class Rollout:
                                              C.byref(loss)))
         return loss.value
 
-    def backward(self) -> dict:
+    def _gradient_buffers(self):
         v = self._structure._definition.view
         m, h = v.constraint_count, v.dihedral_count
         ns = v.suspension.contents.segment_count if v.suspension else 0
         out = {"d_rest": np.zeros(max(m, 1)), "d_comp": np.zeros(max(m, 1)),
-               "d_dihedral_comp": np.zeros(max(h, 1)), "d_segment_rest": np.zeros(max(ns, 1))}
-        mass = np.zeros(1)
+               "d_dihedral_comp": np.zeros(max(h, 1)), "d_segment_rest": np.zeros(max(ns, 1)), "mass": np.zeros(1)}
         g = abi.RolloutGradient(out["d_rest"].ctypes.data, out["d_comp"].ctypes.data,
                                 out["d_dihedral_comp"].ctypes.data, out["d_segment_rest"].ctypes.data,
-                                mass.ctypes.data)
-        _check(self._lib.swb_rollout_backward(self._h, C.byref(g)))
+                                out["mass"].ctypes.data)
+        return out, g, (m, h, ns)
+
+    @staticmethod
+    def _gradient_result(out, sizes) -> dict:
+        m, h, ns = sizes
         out["d_rest"], out["d_comp"] = out["d_rest"][:m], out["d_comp"][:m]
         out["d_dihedral_comp"], out["d_segment_rest"] = out["d_dihedral_comp"][:h], out["d_segment_rest"][:ns]
-        out["d_mass"] = float(mass[0])
+        out["d_mass"] = float(out.pop("mass")[0])
         return out
+
+    def backward(self) -> dict:
+        out, g, sizes = self._gradient_buffers()
+        _check(self._lib.swb_rollout_backward(self._h, C.byref(g)))
+        return self._gradient_result(out, sizes)
 
     def final_positions(self) -> np.ndarray:
         n = self._structure.node_count
@@ -962,3 +970,34 @@ class Rollout:
 
     def backward_ms(self) -> float:
         return float(self._lib.swb_rollout_backward_ms(self._h))
+
+
+def rollout_forward_many(rollouts, settings: abi.StepSettings, targets, weights) -> np.ndarray:
+    """The forwards of several rollouts at once (swb_rollout_forward_many):
+    their structures run side by side on the device.  Returns the losses."""
+    lib = abi.library()
+    k = len(rollouts)
+    ts = [np.ascontiguousarray(t, dtype=np.float64).reshape(r._structure.node_count, 3)
+          for r, t in zip(rollouts, targets)]
+    ws = [np.ascontiguousarray(w, dtype=np.float64).reshape(r._structure.node_count) for r, w in zip(rollouts, weights)]
+    handles = (C.c_void_p * k)(*[r._h for r in rollouts])
+    tp = (C.c_void_p * k)(*[t.ctypes.data for t in ts])
+    wp = (C.c_void_p * k)(*[w.ctypes.data for w in ws])
+    losses = np.zeros(k)
+    statuses = np.zeros(k, dtype=np.int32)
+    _check(lib.swb_rollout_forward_many(handles, k, C.byref(settings), tp, wp, losses.ctypes.data,
+                                        statuses.ctypes.data))
+    return losses
+
+
+def rollout_backward_many(rollouts) -> list:
+    """The backwards of several rollouts at once (swb_rollout_backward_many);
+    one gradient dict per rollout, as Rollout.backward returns it."""
+    lib = abi.library()
+    k = len(rollouts)
+    bufs = [r._gradient_buffers() for r in rollouts]
+    grads = (abi.RolloutGradient * k)(*[b[1] for b in bufs])
+    handles = (C.c_void_p * k)(*[r._h for r in rollouts])
+    statuses = np.zeros(k, dtype=np.int32)
+    _check(lib.swb_rollout_backward_many(handles, k, grads, statuses.ctypes.data))
+    return [Rollout._gradient_result(out, sizes) for out, _, sizes in bufs]

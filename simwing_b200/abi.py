@@ -408,6 +408,9 @@ _PROTOTYPES = {
     "swb_rollout_destroy": (None, [C.c_void_p]),
     "swb_rollout_forward": (C.c_int, [C.c_void_p, P(StepSettings), C.c_void_p, C.c_void_p, P(C.c_double)]),
     "swb_rollout_backward": (C.c_int, [C.c_void_p, P(RolloutGradient)]),
+    "swb_rollout_forward_many": (C.c_int, [C.c_void_p, C.c_uint64, P(StepSettings), C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]),
+    "swb_rollout_backward_many": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "swb_rollout_final_positions": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swb_rollout_forward_ms": (C.c_double, [C.c_void_p]),
     "swb_rollout_backward_ms": (C.c_double, [C.c_void_p]),

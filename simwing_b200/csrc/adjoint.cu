@@ -310,6 +310,12 @@ struct RolloutImpl {
     }
 
     void forward(const swb_step_settings& st, const double* target, const double* weights, double* out_loss) {
+        forward_launch(st, target, weights);
+        forward_collect(target, weights, out_loss);
+    }
+
+    // The forward's launches on the structure's stream (no wait for them).
+    void forward_launch(const swb_step_settings& st, const double* target, const double* weights) {
         S->validate_settings(st);
         if (st.cable_sweep_pairs != 0)
             raise(SWB_UNSUPPORTED, "differentiable rollouts with load-path cable sweep pairs are not available");
@@ -338,6 +344,13 @@ struct RolloutImpl {
         cuda_check(cudaEventRecord(ev0, S->stream), "event");
         for (int c = 0; c < segments; ++c) run_segment_forward(c, false);
         cuda_check(cudaEventRecord(ev1, S->stream), "event");
+    }
+
+    // Waits for the forward's launches; the loss and the final state.
+    void forward_collect(const double* target, const double* weights, double* out_loss) {
+        const size_t N = S->def.nodes.size();
+        double wsum = 0.0;
+        for (size_t i = 0; i < N; ++i) wsum += weights[i];
         check_status();
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ev0, ev1);
@@ -373,6 +386,12 @@ struct RolloutImpl {
     }
 
     void backward(const swb_rollout_gradient* out) {
+        backward_launch();
+        backward_collect(out);
+    }
+
+    // The backward's launches on the structure's stream (no wait for them).
+    void backward_launch() {
         if (!have_forward) raise(SWB_INVALID_ARGUMENT, "backward needs a forward first");
         cuda_check(cudaSetDevice(S->device), "cudaSetDevice");
         const size_t N = S->def.nodes.size();
@@ -422,6 +441,11 @@ struct RolloutImpl {
             }
         }
         cuda_check(cudaEventRecord(ev1, st), "event");
+    }
+
+    // Waits for the backward's launches; the gradients in definition order.
+    void backward_collect(const swb_rollout_gradient* out) {
+        cudaStream_t st = S->stream;
         check_status();
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, ev0, ev1);
@@ -493,6 +517,67 @@ swb_status swb_rollout_backward(swb_rollout* rollout, const swb_rollout_gradient
     return guarded([&] {
         if (!rollout) raise(SWB_INVALID_ARGUMENT, "null argument");
         rollout->r.backward(gradient);
+    });
+}
+
+swb_status swb_rollout_forward_many(swb_rollout* const* rollouts, uint64_t count, const swb_step_settings* settings,
+                                    const double* const* targets_xyz, const double* const* weights,
+                                    double* losses, int32_t* statuses) {
+    return guarded([&] {
+        if ((!rollouts || !targets_xyz || !weights) && count) raise(SWB_INVALID_ARGUMENT, "null argument");
+        if (!settings) raise(SWB_INVALID_ARGUMENT, "null argument");
+        for (uint64_t k = 0; k < count; ++k)
+            if (!rollouts[k] || !targets_xyz[k] || !weights[k]) raise(SWB_INVALID_ARGUMENT, "null argument");
+        // every rollout's launches first, each on its structure's stream, so
+        // that the structures run side by side; then each is waited for
+        std::vector<swb_status> st(count, SWB_OK);
+        std::vector<std::string> msg(count);
+        auto run = [&](uint64_t k, auto&& body) {
+            if (st[k] != SWB_OK) return;
+            try {
+                body();
+            } catch (const Error& e) {
+                st[k] = e.status;
+                msg[k] = e.what();
+            }
+        };
+        for (uint64_t k = 0; k < count; ++k)
+            run(k, [&] { rollouts[k]->r.forward_launch(*settings, targets_xyz[k], weights[k]); });
+        for (uint64_t k = 0; k < count; ++k)
+            run(k, [&] { rollouts[k]->r.forward_collect(targets_xyz[k], weights[k], losses ? losses + k : nullptr); });
+        for (uint64_t k = 0; k < count; ++k) {
+            if (statuses) statuses[k] = st[k];
+        }
+        for (uint64_t k = 0; k < count; ++k)
+            if (st[k] != SWB_OK) raise(st[k], "rollout " + std::to_string(k) + ": " + msg[k]);
+    });
+}
+
+swb_status swb_rollout_backward_many(swb_rollout* const* rollouts, uint64_t count,
+                                     const swb_rollout_gradient* gradients, int32_t* statuses) {
+    return guarded([&] {
+        if (!rollouts && count) raise(SWB_INVALID_ARGUMENT, "null argument");
+        for (uint64_t k = 0; k < count; ++k)
+            if (!rollouts[k]) raise(SWB_INVALID_ARGUMENT, "null argument");
+        std::vector<swb_status> st(count, SWB_OK);
+        std::vector<std::string> msg(count);
+        auto run = [&](uint64_t k, auto&& body) {
+            if (st[k] != SWB_OK) return;
+            try {
+                body();
+            } catch (const Error& e) {
+                st[k] = e.status;
+                msg[k] = e.what();
+            }
+        };
+        for (uint64_t k = 0; k < count; ++k) run(k, [&] { rollouts[k]->r.backward_launch(); });
+        for (uint64_t k = 0; k < count; ++k)
+            run(k, [&] { rollouts[k]->r.backward_collect(gradients ? gradients + k : nullptr); });
+        for (uint64_t k = 0; k < count; ++k) {
+            if (statuses) statuses[k] = st[k];
+        }
+        for (uint64_t k = 0; k < count; ++k)
+            if (st[k] != SWB_OK) raise(st[k], "rollout " + std::to_string(k) + ": " + msg[k]);
     });
 }
 

@@ -195,3 +195,48 @@ def test_rollout_rejects_what_it_cannot_differentiate(cuda_device):
         r.forward(step_settings(), np.zeros((s.node_count, 3)), np.zeros(s.node_count))
     with pytest.raises(sw.InvalidArgument):
         sw.Rollout(s, 0)
+
+
+def test_rollouts_side_by_side_equal_one_at_a_time(cuda_device):
+    """swb_rollout_forward_many / backward_many enqueue every rollout's
+    launches on its own structure's stream before waiting for any: three
+    wings of different sizes, one with a ground plane, give bit for bit the
+    losses and gradients they give one at a time."""
+    st = step_settings()
+    defs = [sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, seed=s) for s in (1, 2)]
+    defs.append(sw.generate_wing(cells=6, chordwise=12, spanwise_per_cell=2, rib_layers=2, seed=3))
+
+    def make():
+        out = []
+        for k, d in enumerate(defs):
+            s = sw.Structure(d)
+            for _ in range(20):
+                s.step(st, diagnostics=False)
+            if k == 2:
+                pilot_z = s.suspension_state().center_of_mass[2]
+                s.set_ground((0.0, 0.0, 1.0), pilot_z - 0.02, 0.0)
+            out.append(s)
+        return out
+
+    rng = np.random.default_rng(9)
+    structures = make()
+    targets = [s.node_states()[:, 0, :] + rng.normal(0.0, 0.02, (s.node_count, 3)) for s in structures]
+    weights = [np.ones(s.node_count) for s in structures]
+    one = []
+    for s, t, w in zip(structures, targets, weights):
+        r = sw.Rollout(s, 32, 16)
+        loss = r.forward(st, t, w)
+        one.append((loss, r.backward()))
+        r.close()
+    rollouts = [sw.Rollout(s, 32, 16) for s in structures]
+    losses = sw.rollout_forward_many(rollouts, st, targets, weights)
+    grads = sw.rollout_backward_many(rollouts)
+    for (loss, g), l2, g2 in zip(one, losses, grads):
+        assert loss == l2
+        for key in ("d_rest", "d_comp", "d_dihedral_comp", "d_segment_rest"):
+            np.testing.assert_array_equal(g[key], g2[key])
+        assert g["d_mass"] == g2["d_mass"]
+    for r in rollouts:
+        r.close()
+    for s in structures:
+        s.close()
