@@ -466,6 +466,24 @@ typedef struct swb_ground {
 } swb_ground;
 swb_status swb_structure_set_ground(swb_structure* structure, const swb_ground* ground);
 
+/* Line-line contact (no counterpart in the reference, which rejects segment
+ * contact: contact.cpp:2336-2339): the suspension lines' cable segments are
+ * kept 2 x radius apart.  Once per substep, at the predicted positions, the
+ * pairs of segments that share no node and come within 2 x radius + margin
+ * of each other (by their boxes) become candidates; after every constraint
+ * iteration the candidates are projected in key order (by segment, the
+ * segments ordered by their smaller, then larger definition node index):
+ * the closest points of the two segments pushed apart to 2 x radius,
+ * rigidly.  enabled = 0 (or a null pointer) removes it.  Single structures
+ * only (batches and differentiable rollouts refuse it). */
+typedef struct swb_line_contact {
+    double radius;
+    double margin;
+    uint32_t enabled;
+    uint32_t reserved;
+} swb_line_contact;
+swb_status swb_structure_set_line_contact(swb_structure* structure, const swb_line_contact* contact);
+
 /* The device forms of the step's two short math functions on host arrays
  * (no counterpart in the reference; for checking them on the GPU they run
  * on): which = SWB_FAST_ATAN2 gives out[i] = atan2(a[i], b[i]) by the

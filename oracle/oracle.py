@@ -45,6 +45,7 @@ _PORT = {
     "swo_read_segment_lambdas": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "swo_evaluate_dihedral": (None, [C.c_void_p, C.c_void_p]),
     "swo_set_ground": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "swo_set_line_contact": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 _REF = {
     "swref_last_error": (C.c_char_p, []),
@@ -211,6 +212,10 @@ class PortStructure(_Base):
     def set_ground(self, normal=(0.0, 0.0, 1.0), offset=0.0, friction=0.0, enabled=True):
         g = abi.Ground(abi.Vec3(*normal), float(offset), float(friction), 1 if enabled else 0, 0)
         self._check(self._lib().swo_set_ground(self._h, C.byref(g)))
+
+    def set_line_contact(self, radius, margin=0.0, enabled=True):
+        lc = abi.LineContact(float(radius), float(margin), 1 if enabled else 0, 0)
+        self._check(self._lib().swo_set_line_contact(self._h, C.byref(lc)))
 
     def segment_lambdas(self, n):
         out = np.zeros(n)

@@ -313,6 +313,15 @@ typedef struct swo_structure {
     int ground;
     V3 ground_normal;
     double ground_offset, ground_friction;
+    /* line-line contact (swb_structure_set_line_contact; the reference
+     * rejects segment contact, so its parity is the device's against this
+     * restatement): cable segments by (smaller, larger) node, the substep's
+     * candidate pairs in key order */
+    int lines;
+    double line_radius, line_reach;
+    uint64_t nseg_lines, npairs, pairs_cap;
+    uint64_t (*line_seg)[2];
+    uint64_t (*line_pair)[2];
 } swo_structure;
 
 /* ---------------- membranes (soft_body.cpp, membrane.cpp) ---------------- */
@@ -608,6 +617,7 @@ void swo_destroy(swo_structure* s) {
     if (!s) return;
     free(s->nodes); free(s->tri); free(s->pressure); free(s->dist);
     free(s->dih); free(s->pending); free(s->seg); free(s->hang_local); free(s->mem); free(s->load_path);
+    free(s->line_seg); free(s->line_pair);
     free(s);
 }
 
@@ -1218,6 +1228,122 @@ static void ground_pass(swo_structure* s) {
     }
 }
 
+static int cmp_seg(const void* a, const void* b) {
+    const uint64_t* x = (const uint64_t*)a;
+    const uint64_t* y = (const uint64_t*)b;
+    if (x[0] != y[0]) return x[0] < y[0] ? -1 : 1;
+    if (x[1] != y[1]) return x[1] < y[1] ? -1 : 1;
+    return 0;
+}
+
+swb_status swo_set_line_contact(swo_structure* s, const swb_line_contact* lc) {
+    if (!lc || !lc->enabled) {
+        s->lines = 0;
+        return SWB_OK;
+    }
+    if (!s->line_seg) {
+        uint64_t k = 0;
+        s->line_seg = malloc((s->m + 1) * sizeof *s->line_seg);
+        for (uint64_t i = 0; i < s->m; ++i)
+            if (s->dist[i].kind == SWB_CONSTRAINT_CABLE) {
+                const uint64_t a = s->dist[i].a, b = s->dist[i].b;
+                s->line_seg[k][0] = a < b ? a : b;
+                s->line_seg[k][1] = a < b ? b : a;
+                ++k;
+            }
+        qsort(s->line_seg, k, sizeof *s->line_seg, cmp_seg);
+        uint64_t u = 0;
+        for (uint64_t i = 0; i < k; ++i)
+            if (u == 0 || cmp_seg(s->line_seg[u - 1], s->line_seg[i]) != 0) {
+                s->line_seg[u][0] = s->line_seg[i][0];
+                s->line_seg[u][1] = s->line_seg[i][1];
+                ++u;
+            }
+        s->nseg_lines = u;
+    }
+    s->lines = 1;
+    s->line_radius = lc->radius;
+    s->line_reach = lc->radius + 0.5 * lc->margin;
+    return SWB_OK;
+}
+
+/* The substep's candidate pairs at the predicted positions: segments that
+ * share no node and whose boxes, widened by the reach, overlap, in key
+ * order. */
+static void line_broadphase(swo_structure* s) {
+    s->npairs = 0;
+    const double r = s->line_reach;
+    for (uint64_t i = 0; i < s->nseg_lines; ++i) {
+        const V3 a = s->nodes[s->line_seg[i][0]].x, b = s->nodes[s->line_seg[i][1]].x;
+        for (uint64_t j = i + 1; j < s->nseg_lines; ++j) {
+            const uint64_t* q = s->line_seg[j];
+            if (q[0] == s->line_seg[i][0] || q[0] == s->line_seg[i][1] || q[1] == s->line_seg[i][0] ||
+                q[1] == s->line_seg[i][1])
+                continue;
+            const V3 c = s->nodes[q[0]].x, d = s->nodes[q[1]].x;
+            if (fmin(a.x, b.x) - r > fmax(c.x, d.x) + r || fmin(c.x, d.x) - r > fmax(a.x, b.x) + r ||
+                fmin(a.y, b.y) - r > fmax(c.y, d.y) + r || fmin(c.y, d.y) - r > fmax(a.y, b.y) + r ||
+                fmin(a.z, b.z) - r > fmax(c.z, d.z) + r || fmin(c.z, d.z) - r > fmax(a.z, b.z) + r)
+                continue;
+            if (s->npairs == s->pairs_cap) {
+                s->pairs_cap = s->pairs_cap ? 2 * s->pairs_cap : 64;
+                s->line_pair = realloc(s->line_pair, s->pairs_cap * sizeof *s->line_pair);
+            }
+            s->line_pair[s->npairs][0] = i;
+            s->line_pair[s->npairs][1] = j;
+            ++s->npairs;
+        }
+    }
+}
+
+/* The candidates' projections in key order: the segments' closest points
+ * (Ericson's segment-segment method) pushed apart to 2 x radius. */
+static void line_project(swo_structure* s) {
+    const double gap = 2.0 * s->line_radius;
+    for (uint64_t k = 0; k < s->npairs; ++k) {
+        Node* A = &s->nodes[s->line_seg[s->line_pair[k][0]][0]];
+        Node* B = &s->nodes[s->line_seg[s->line_pair[k][0]][1]];
+        Node* C = &s->nodes[s->line_seg[s->line_pair[k][1]][0]];
+        Node* D = &s->nodes[s->line_seg[s->line_pair[k][1]][1]];
+        const V3 d1 = sub(B->x, A->x), d2 = sub(D->x, C->x), r = sub(A->x, C->x);
+        const double eps = 1.0e-12;
+        const double a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+        double ps = 0.0, pt = 0.0;
+        if (a <= eps && e <= eps) {
+        } else if (a <= eps) {
+            pt = fmin(fmax(f / e, 0.0), 1.0);
+        } else {
+            const double c = dot(d1, r);
+            if (e <= eps) {
+                ps = fmin(fmax(-c / a, 0.0), 1.0);
+            } else {
+                const double b = dot(d1, d2), denom = a * e - b * b;
+                ps = denom != 0.0 ? fmin(fmax((b * f - c * e) / denom, 0.0), 1.0) : 0.0;
+                pt = (b * ps + f) / e;
+                if (pt < 0.0) {
+                    pt = 0.0;
+                    ps = fmin(fmax(-c / a, 0.0), 1.0);
+                } else if (pt > 1.0) {
+                    pt = 1.0;
+                    ps = fmin(fmax((b - c) / a, 0.0), 1.0);
+                }
+            }
+        }
+        const V3 diff = sub(add(A->x, smul(ps, d1)), add(C->x, smul(pt, d2)));
+        const double dist = sqrt(dot(diff, diff));
+        if (!(dist < gap) || !(dist > 0.0)) continue;
+        const V3 n = smul(1.0 / dist, diff);
+        const double wa = A->w * (1.0 - ps), wb = B->w * ps, wc = C->w * (1.0 - pt), wd = D->w * pt;
+        const double W = wa * (1.0 - ps) + wb * ps + wc * (1.0 - pt) + wd * pt;
+        if (!(W > 0.0)) continue;
+        const double dl = (gap - dist) / W;
+        A->x = add(A->x, smul(wa * dl, n));
+        B->x = add(B->x, smul(wb * dl, n));
+        C->x = sub(C->x, smul(wc * dl, n));
+        D->x = sub(D->x, smul(wd * dl, n));
+    }
+}
+
 swb_status swo_set_ground(swo_structure* s, const swb_ground* g) {
     if (!g || !g->enabled) {
         s->ground = 0;
@@ -1246,6 +1372,7 @@ static swb_status substep(swo_structure* s, double dt, const swb_step_settings* 
     }
     const double damping = exp(-st->velocity_damping * dt);
     predict(s, dt, g, damping, fromabi(st->damping_reference_velocity));
+    if (s->lines) line_broadphase(s);
     int preserve = !s->has_suspension && (s->h > 0 || s->nm > 0);
     for (uint64_t i = 0; preserve && i < s->n; ++i)
         if (!(s->nodes[i].w > 0.0)) preserve = 0;
@@ -1276,6 +1403,7 @@ static swb_status substep(swo_structure* s, double dt, const swb_step_settings* 
             swb_status r = line_iteration(s, dt);
             if (r != SWB_OK) return r;
         }
+        if (s->lines) line_project(s);
         if (s->ground) ground_pass(s);
     }
     if (st->constraint_iterations > 0)

@@ -672,6 +672,12 @@ class Structure:
         g = abi.Ground(Vec3(*normal), float(offset), float(friction), 1 if enabled else 0, 0)
         _check(self._lib.swb_structure_set_ground(self._h, C.byref(g)))
 
+    def set_line_contact(self, radius: float, margin: float = 0.0, enabled: bool = True) -> None:
+        """Line-line contact of the cable segments, kept 2 x radius apart
+        (swb_structure_set_line_contact); enabled=False removes it."""
+        lc = abi.LineContact(float(radius), float(margin), 1 if enabled else 0, 0)
+        _check(self._lib.swb_structure_set_line_contact(self._h, C.byref(lc)))
+
     def step(self, settings: abi.StepSettings | None = None, diagnostics: bool = True):
         s = settings if settings is not None else StepSettings()
         d = abi.Diagnostics()

@@ -275,6 +275,10 @@ class Ground(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
+class LineContact(C.Structure):
+    _fields_ = [("radius", C.c_double), ("margin", C.c_double), ("enabled", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class Wrench(C.Structure):
     _fields_ = [("force", Vec3), ("moment", Vec3)]
 
@@ -371,6 +375,7 @@ _PROTOTYPES = {
     "swb_structure_set_face_pressure": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double]),
     "swb_structure_set_uniform_pressure": (C.c_int, [C.c_void_p, C.c_double]),
     "swb_structure_set_ground": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "swb_structure_set_line_contact": (C.c_int, [C.c_void_p, C.c_void_p]),
     "swb_structure_step": (C.c_int, [C.c_void_p, P(StepSettings), P(Diagnostics)]),
     "swb_structure_step_many": (C.c_int, [C.c_void_p, P(StepSettings), C.c_int32, P(Diagnostics)]),
     "swb_structure_diagnostics": (C.c_int, [C.c_void_p, P(Diagnostics)]),

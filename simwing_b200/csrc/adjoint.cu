@@ -322,6 +322,7 @@ struct RolloutImpl {
         if (st.substeps != 1) raise(SWB_UNSUPPORTED, "differentiable rollouts take one substep per step");
         if (S->cparams.ground && S->cparams.ground_friction > 0.0f)
             raise(SWB_UNSUPPORTED, "differentiable rollouts take a frictionless ground plane");
+        if (S->line_contact) raise(SWB_UNSUPPORTED, "differentiable rollouts do not take line-line contact");
         const size_t N = S->def.nodes.size();
         double wsum = 0.0;
         for (size_t i = 0; i < N; ++i) {

@@ -409,7 +409,11 @@ struct BatchImpl {
     swb_status step(const swb_step_settings& st, int steps, int32_t* statuses, std::string& first_message) {
         if (steps < 1) raise(SWB_INVALID_ARGUMENT, "steps must be positive");
         const size_t n = size();
-        for (size_t i = 0; i < n; ++i) P.members[i]->s.validate_settings(st);
+        for (size_t i = 0; i < n; ++i) {
+            P.members[i]->s.validate_settings(st);
+            if (P.members[i]->s.line_contact)
+                raise(SWB_UNSUPPORTED, "line-line contact is not available in batches (single structures only)");
+        }
         if (st.cable_sweep_pairs != 0) raise(SWB_UNSUPPORTED, "load-path cable sweep pairs are not available in batches");
         cuda_check(cudaSetDevice(device), "cudaSetDevice");
         std::vector<char> alive(n, 1);

@@ -16,6 +16,7 @@
 #include "cluster_params.h"
 #include "membrane.cuh"
 #include "contact_phase.cuh"
+#include "line_contact.cuh"
 #include "step_kernel.cuh"
 
 namespace swb {
@@ -382,6 +383,10 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
     // are: the momentum guard stands down while one is set
     const bool guard = I.momentum_guard != 0 && !p.ground;
     const bool guard_c = kPacked ? slot.guard != 0 && !p.ground : guard;
+    // line-line contact: the substep's candidate pairs are counted afresh
+    const LineContactDev* lines = kPacked ? nullptr : I.lines;
+    auto line_addr = [&](uint32_t ref) { return node_addr(ref, me, rank_base, x_base); };
+    if (lines && me == 0 && tid == 0) *lines->count = 0;
     const float ground_off =
         p.ground ? static_cast<float>(p.ground_offset - (p.ground_normal.x * I.origin_in[0] +
                                                          p.ground_normal.y * I.origin_in[1] +
@@ -485,6 +490,11 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         cta_momentum_sums(x, v, n, mom_pred, mom_scratch);
     }
     cluster.sync();
+    if (lines) {
+        line_broadphase(*lines, me, static_cast<uint32_t>(sctas), cluster, line_addr, I.status);
+        cluster.sync();
+        if (me == 0) line_sort(*lines, lines->sort);
+    }
 
     // ---- constraint iterations ------------------------------------------------
     // Stages of one iteration: distance colours, membrane colours, then
@@ -610,6 +620,10 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
             cluster.sync();
         }
         if constexpr (kContact) contact_iteration(cctx, cluster);
+        if (lines) {
+            if (me == 0 && tid == 0) line_project(*lines, line_addr);
+            cluster.sync();
+        }
         if (p.ground) {
             uint8_t* gt = nullptr;
             if constexpr (kTape) gt = p.tape.ground + static_cast<size_t>(it) * pbeg_s[sctas] + base;

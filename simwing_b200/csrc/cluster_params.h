@@ -152,6 +152,22 @@ struct ContactDev {
     uint32_t* lv_front;                // [2 * cand_cap]
 };
 
+// Line-line contact of one structure: the cable segments (node references
+// rank << 12 | index of both ends, in key order: by the smaller, then the
+// larger node index of the definition) and each step's candidate pairs.
+struct LineContactDev {
+    uint32_t segments;
+    uint32_t capacity;                 // candidate pairs a step may hold
+    const uint32_t* seg;               // [segments] ref(a) | ref(b) << 16
+    const uint2* seg_nodes;            // [segments] definition node indices (a, b), for the shared-node test
+    float radius;                      // line radius: segments are kept 2 radius apart
+    float reach;                       // box half-margin of the step's broadphase: radius + margin / 2
+    float4* box;                       // [segments][2] the step's predicted boxes (lo, hi)
+    uint32_t* pair;                    // [capacity] candidate pairs i << 16 | j, i < j, sorted after the broadphase
+    uint32_t* sort;                    // [capacity] scratch of the sort
+    uint32_t* count;                   // [1] candidate pairs of the step
+};
+
 // Per-instance tables and state (one cluster each).
 struct ClusterInstance {
     const float4* pos_in;
@@ -194,6 +210,9 @@ struct ClusterInstance {
     const uint32_t* pair_rec;
     // Fabric self-contact, or nullptr.  Single-structure launches only.
     const ContactDev* contact;
+    // Line-line contact (swb_structure_set_line_contact), or nullptr.
+    // Single-structure launches only.
+    const LineContactDev* lines;
     ContactDiagDev* contact_diag;  // the output state's contact diagnostics
 };
 

@@ -49,6 +49,7 @@ enum : int {
     kContactCandidates = 16,     // more candidates than the device list holds
     kContactTable = 17,          // more warm-started features than the device table holds
     kContactRecords = 18,        // more records than the device book holds
+    kContactLinePairs = 19,      // more line-line candidate pairs than the device list holds
 };
 
 __device__ __forceinline__ void contact_fail(int* status, int code) {

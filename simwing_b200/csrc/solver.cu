@@ -377,6 +377,72 @@ static void membrane_constants(const swb_membrane_def& m, float4 out[kMembraneAu
     out[4] = make_float4(f(kyy), f(kzz), f(kxy), 0.0f);
 }
 
+// One instance record per (input, output) buffer pair, so that a launch only
+// selects a pointer; uploaded again when a setting they carry changes.
+void StructureImpl::upload_instances() {
+    std::vector<ClusterInstance> inst(9);
+    for (int in = 0; in < 3; ++in)
+        for (int out = 0; out < 3; ++out) {
+            ClusterInstance c = cluster_base;
+            c.pos_in = d_pos[in]; c.vel_in = d_vel[in];
+            c.pos_out = d_pos[out]; c.vel_out = d_vel[out]; c.prev_out = d_prev[out];
+            c.force = d_force;
+            c.tri_offsets = d_tri_off; c.tri_list = d_tri_list; c.tri = d_tri;
+            c.susp_cta = def.has_suspension ? susp_owner : -1;
+            c.payload_def = d_payload_def;
+            c.payload_in = d_payload[in]; c.payload_out = d_payload[out];
+            c.origin_in = d_origin[in]; c.origin_out = d_origin[out];
+            c.membrane_residual = d_mres[out];
+            c.contact = d_contact;
+            c.contact_diag = d_cdiag[out];
+            c.lines = line_contact ? d_lines : nullptr;
+            c.status = d_control->status;
+            c.recentre = def.has_suspension ? 1 : 0;
+            inst[in * 3 + out] = c;
+        }
+    if (!d_instances) {
+        d_instances = dupload(owned, inst, stream);
+    } else {
+        cuda_check(cudaMemcpyAsync(d_instances, inst.data(), inst.size() * sizeof(ClusterInstance),
+                                   cudaMemcpyHostToDevice, stream), "instance upload");
+        cuda_check(cudaStreamSynchronize(stream), "instance upload");
+    }
+}
+
+// The cable segments of line-line contact and their step scratch (once).
+void StructureImpl::setup_line_contact() {
+    std::vector<std::pair<uint64_t, uint64_t>> segs;
+    for (const auto& c : def.constraints)
+        if (c.kind == SWB_CONSTRAINT_CABLE)
+            segs.push_back({std::min(c.first_node, c.second_node), std::max(c.first_node, c.second_node)});
+    std::sort(segs.begin(), segs.end());
+    segs.erase(std::unique(segs.begin(), segs.end()), segs.end());
+    if (segs.size() > 65535) raise(SWB_UNSUPPORTED, "line-line contact takes at most 65,535 cable segments");
+    auto ref = [&](uint64_t node) {
+        const uint32_t slot = slot_of_node[node];
+        uint32_t cta = 0;
+        while (cta + 1 < static_cast<uint32_t>(G) && csched.patch_begin[cta + 1] <= slot) ++cta;
+        return (cta << 12) | (slot - csched.patch_begin[cta]);
+    };
+    std::vector<uint32_t> seg(segs.size());
+    std::vector<uint2> nodes(segs.size());
+    for (size_t i = 0; i < segs.size(); ++i) {
+        seg[i] = ref(segs[i].first) | (ref(segs[i].second) << 16);
+        nodes[i] = make_uint2(static_cast<uint32_t>(segs[i].first), static_cast<uint32_t>(segs[i].second));
+    }
+    LineContactDev L{};
+    L.segments = static_cast<uint32_t>(segs.size());
+    L.capacity = 1u << 16;
+    L.seg = dupload(owned, seg, stream);
+    L.seg_nodes = dupload(owned, nodes, stream);
+    L.box = dalloc<float4>(owned, 2 * std::max<size_t>(segs.size(), 1));
+    L.pair = dalloc<uint32_t>(owned, L.capacity);
+    L.sort = dalloc<uint32_t>(owned, L.capacity);
+    L.count = dalloc<uint32_t>(owned, 1);
+    lines_host = L;
+    d_lines = dupload(owned, std::vector<LineContactDev>{L}, stream);
+}
+
 void (*StructureImpl::step_kernel() const)(ClusterParams) {
     if (def.has_contact)
         return def.membranes.empty() ? dev::xpbd_cluster_contact_kernel : dev::xpbd_cluster_contact_membrane_kernel;
@@ -762,28 +828,7 @@ void StructureImpl::finish_build(const swb_solver_options& opt, const cudaDevice
 
     if (cluster_mode) {
         if (def.has_contact) setup_contact(opt);
-        // One instance record per (input, output) buffer pair so a launch
-        // only selects a pointer.
-        std::vector<ClusterInstance> inst(9);
-        for (int in = 0; in < 3; ++in)
-            for (int out = 0; out < 3; ++out) {
-                ClusterInstance c = cluster_base;
-                c.pos_in = d_pos[in]; c.vel_in = d_vel[in];
-                c.pos_out = d_pos[out]; c.vel_out = d_vel[out]; c.prev_out = d_prev[out];
-                c.force = d_force;
-                c.tri_offsets = d_tri_off; c.tri_list = d_tri_list; c.tri = d_tri;
-                c.susp_cta = def.has_suspension ? susp_owner : -1;
-                c.payload_def = d_payload_def;
-                c.payload_in = d_payload[in]; c.payload_out = d_payload[out];
-                c.origin_in = d_origin[in]; c.origin_out = d_origin[out];
-                c.membrane_residual = d_mres[out];
-                c.contact = d_contact;
-                c.contact_diag = d_cdiag[out];
-                c.status = d_control->status;
-                c.recentre = def.has_suspension ? 1 : 0;
-                inst[in * 3 + out] = c;
-            }
-        d_instances = dupload(owned, inst, stream);
+        upload_instances();
         cparams.copy_budget = 4000000000LL;
         // The attribute is a per-kernel limit shared by every structure in
         // the process: it is raised to the device limit, never set to this
@@ -1100,8 +1145,9 @@ swb_status decode_status(const int status[2], std::string& message) {
             "Contact broadphase input failed: positions must be finite",
             "contact candidates exceed the device list (1,048,576 per phase)",
             "contact features exceed the device multiplier table",
-            "contact records exceed the device record book"};
-        message = std::string("ContactStepError: ") + what[std::clamp(status[1], 0, 18)];
+            "contact records exceed the device record book",
+            "line-line contact pairs exceed the device list"};
+        message = std::string("ContactStepError: ") + what[std::clamp(status[1], 0, 19)];
         return SWB_CONTACT_ERROR;
     }
     if (status[0] & dev::kStatusMembrane) {
@@ -1532,6 +1578,31 @@ swb_status swb_structure_set_face_pressure(swb_structure* s, uint64_t triangle, 
         if (!std::isfinite(dp)) raise(SWB_INVALID_ARGUMENT, "Pressure difference must be finite");
         s->s.pressure[triangle] = dp;
         s->s.pressure_dirty = true;
+    });
+}
+
+swb_status swb_structure_set_line_contact(swb_structure* s, const swb_line_contact* lc) {
+    return guarded([&] {
+        if (!s) raise(SWB_INVALID_ARGUMENT, "null structure");
+        StructureImpl& m = s->s;
+        if (!lc || !lc->enabled) {
+            if (m.line_contact) {
+                m.line_contact = false;
+                m.upload_instances();
+            }
+            return;
+        }
+        if (!std::isfinite(lc->radius) || !(lc->radius > 0.0) || !std::isfinite(lc->margin) || lc->margin < 0.0)
+            raise(SWB_INVALID_ARGUMENT, "line contact radius must be finite and positive, margin finite and >= 0");
+        if (!m.cluster_mode) raise(SWB_UNSUPPORTED, "line-line contact needs the cluster schedule");
+        if (!m.d_lines) m.setup_line_contact();
+        LineContactDev L = m.lines_host;
+        L.radius = static_cast<float>(lc->radius);
+        L.reach = static_cast<float>(lc->radius + 0.5 * lc->margin);
+        m.lines_host = L;
+        cuda_check(cudaMemcpyAsync(m.d_lines, &L, sizeof(L), cudaMemcpyHostToDevice, m.stream), "line contact");
+        m.line_contact = true;
+        m.upload_instances();
     });
 }
 

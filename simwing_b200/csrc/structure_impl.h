@@ -72,6 +72,10 @@ struct StructureImpl {
     int sm_count = 0;
     int G = 0;
     int contact_helpers = 0;  // helper clusters of the contact detection phases
+    // line-line contact (swb_structure_set_line_contact)
+    bool line_contact = false;
+    LineContactDev lines_host{};
+    LineContactDev* d_lines = nullptr;
     int threads = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -128,6 +132,8 @@ struct StructureImpl {
     void build(const swb_structure_definition& definition, const swb_solver_options* options);
     void upload_cluster_tables();
     void setup_contact(const swb_solver_options& opt);
+    void setup_line_contact();
+    void upload_instances();
     // The step with the force buffer already written on the device (the
     // coupling's impulse gather): skips the upload of the pending loads.
     bool device_forces = false;

@@ -200,8 +200,9 @@ def test_rollout_rejects_what_it_cannot_differentiate(cuda_device):
 def test_rollouts_side_by_side_equal_one_at_a_time(cuda_device):
     """swb_rollout_forward_many / backward_many enqueue every rollout's
     launches on its own structure's stream before waiting for any: three
-    wings of different sizes, one with a ground plane, give bit for bit the
-    losses and gradients they give one at a time."""
+    wings of different sizes, one against a wall (a plane 1 cm inside its
+    trailing edge), give bit for bit the losses and gradients they give one
+    at a time."""
     st = step_settings()
     defs = [sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, seed=s) for s in (1, 2)]
     defs.append(sw.generate_wing(cells=6, chordwise=12, spanwise_per_cell=2, rib_layers=2, seed=3))
@@ -213,8 +214,8 @@ def test_rollouts_side_by_side_equal_one_at_a_time(cuda_device):
             for _ in range(20):
                 s.step(st, diagnostics=False)
             if k == 2:
-                pilot_z = s.suspension_state().center_of_mass[2]
-                s.set_ground((0.0, 0.0, 1.0), pilot_z - 0.02, 0.0)
+                x_max = s.node_states()[:, 0, 0].max()
+                s.set_ground((-1.0, 0.0, 0.0), -(x_max - 0.01), 0.0)
             out.append(s)
         return out
 

@@ -1,0 +1,226 @@
+"""Line-line contact (swb_structure_set_line_contact).
+
+The reference rejects contact between two line colliders
+(src/softwing/contact.cpp:2336-2339), so this contact has no reference
+counterpart and its parity is pinned to this project's own FP64
+restatement in the oracle port (`swo_set_line_contact`,
+oracle/xpbd_oracle.c): the substep's candidates are the pairs of cable
+segments that share no node and whose boxes at the predicted positions,
+widened by radius + margin / 2, overlap; after every iteration they are
+projected in key order, the segments' closest points pushed apart to
+2 x radius.  Known answers pin the restatement (two crossing segments end
+exactly 2 x radius apart; segments that share a node or lie beyond reach
+are left alone); on the GPU the device matches the port per step on
+crossing ropes and on a wing whose lines are nodal cables, and the
+refusals (batches, rollouts, grid schedule, bad radius) hold."""
+import numpy as np
+import pytest
+
+import simwing_b200 as sw
+from simwing_b200 import abi
+from oracle import oracle as O
+from tests.conftest import step_settings
+from tests.test_gpu_parity import REL_TOL, rel_error, sync_oracle_to_device
+
+RADIUS = 0.004
+
+
+def two_segments(dz, angle=np.pi / 2, mass=0.01):
+    """Two free two-node cables of length 0.2 m crossing above the origin,
+    the first dz above the second."""
+    c, s = 0.1 * np.cos(angle), 0.1 * np.sin(angle)
+    nodes = [(-0.1, 0.0, 0.5 * dz, mass, False), (0.1, 0.0, 0.5 * dz, mass, False),
+             (-c, -s, -0.5 * dz, mass, False), (c, s, -0.5 * dz, mass, False)]
+    cons = [(abi.CABLE, 0, 1, 0.2, 1e-8), (abi.CABLE, 2, 3, 0.2, 1e-8)]
+    return sw.definition_from_arrays(nodes, constraints=cons)
+
+
+def segment_distance(p1, q1, p2, q2):
+    """Closest distance of two segments, by dense sampling of the first
+    and projection onto the second (test-side check, independent of the
+    port's closed form)."""
+    t = np.linspace(0.0, 1.0, 2001)[:, None]
+    a = p1 + t * (q1 - p1)
+    d = q2 - p2
+    u = np.clip(((a - p2) @ d) / (d @ d), 0.0, 1.0)[:, None]
+    return float(np.linalg.norm(a - (p2 + u * d), axis=1).min())
+
+
+def zero_gravity(iterations, cable_sweep_pairs=None):
+    st = step_settings(iterations=iterations, gravity=(0.0, 0.0, 0.0), damping=0.0)
+    if cable_sweep_pairs is not None:
+        st.cable_sweep_pairs = cable_sweep_pairs
+    return st
+
+
+def test_port_crossing_segments_end_two_radii_apart():
+    port = O.PortStructure(two_segments(0.001))
+    port.set_line_contact(RADIUS, 0.0)
+    port.step(zero_gravity(iterations=4))
+    x = port.node_states()[:, 0, :]
+    # equal masses, crossing at both midpoints: each segment moves half the
+    # overlap along z, rigidly
+    np.testing.assert_allclose(x[:2, 2], RADIUS, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(x[2:, 2], -RADIUS, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(x[:, :2], two_segments(0.001).positions()[:, :2], rtol=0, atol=1e-12)
+    assert segment_distance(x[0], x[1], x[2], x[3]) == pytest.approx(2 * RADIUS, abs=1e-9)
+
+
+def test_port_heavier_segment_moves_less():
+    d = two_segments(0.0, angle=np.pi / 3)
+    nodes = d.nodes()
+    nodes["mass"][:2] = 0.03  # three times the second segment's mass
+    port = O.PortStructure(d)
+    port.set_line_contact(RADIUS, 0.0)
+    z0 = d.positions()[:, 2].copy()
+    # no separation direction at zero distance: nothing moves
+    port.step(zero_gravity(iterations=2))
+    np.testing.assert_array_equal(port.node_states()[:, 0, 2], z0)
+    d2 = two_segments(0.002, angle=np.pi / 3)
+    d2.nodes()["mass"][:2] = 0.03
+    port = O.PortStructure(d2)
+    port.set_line_contact(RADIUS, 0.0)
+    port.step(zero_gravity(iterations=2))
+    x = port.node_states()[:, 0, :]
+    up, down = x[0, 2] - 0.001, -0.001 - x[2, 2]
+    assert up == pytest.approx((2 * RADIUS - 0.002) / 4, rel=1e-9)
+    assert down == pytest.approx(3 * (2 * RADIUS - 0.002) / 4, rel=1e-9)
+
+
+@pytest.mark.parametrize("case", ["shared node", "beyond reach", "disabled"])
+def test_port_leaves_pairs_alone(case):
+    if case == "shared node":
+        # a sharp V: two cables meeting at node 1, their far ends 1 mm apart
+        # (no candidate: the closest points of such a pair are the shared node)
+        nodes = [(-0.2, 0.0005, 0.0, 0.01, False), (0.0, 0.0, 0.0, 0.01, False), (-0.2, -0.0005, 0.0, 0.01, False)]
+        rest = float(np.hypot(0.2, 0.0005))
+        d = sw.definition_from_arrays(nodes, constraints=[(abi.CABLE, 0, 1, rest, 1e-8),
+                                                          (abi.CABLE, 1, 2, rest, 1e-8)])
+    else:
+        d = two_segments(3 * RADIUS)
+    port = O.PortStructure(d)
+    port.set_line_contact(RADIUS, 0.0)
+    if case == "disabled":
+        d = two_segments(0.001)
+        port = O.PortStructure(d)
+        port.set_line_contact(RADIUS, 0.0)
+        port.set_line_contact(RADIUS, 0.0, enabled=False)
+    x0 = port.node_states()[:, 0, :].copy()
+    port.step(zero_gravity(iterations=4, cable_sweep_pairs=0))
+    x = port.node_states()[:, 0, :]
+    assert np.abs(x - x0).max() <= 1e-9 * max(1.0, np.abs(x0).max()), np.abs(x - x0).max()
+
+
+def crossing_ropes(k=6, n=12, mass=0.02):
+    """k ropes of n nodes, each pinned at its top end, hanging slanted so
+    that all of them cross the vertical axis at mid height, 2 mm apart in
+    y: every rope overlaps every other at the start."""
+    nodes, cons = [], []
+    for i in range(k):
+        a = 0.1 * (i - 0.5 * (k - 1))
+        y = 0.002 * i
+        top = np.array([a, y, 1.0])
+        bottom = np.array([-a, y, 0.0])
+        base = len(nodes)
+        for j in range(n):
+            p = top + (bottom - top) * j / (n - 1)
+            nodes.append((p[0], p[1], p[2], mass, j == 0))
+        seg = float(np.linalg.norm(bottom - top)) / (n - 1)
+        cons += [(abi.CABLE, base + j, base + j + 1, seg, 1e-7) for j in range(n - 1)]
+    return sw.definition_from_arrays(nodes, constraints=cons)
+
+
+def cable_segments(d):
+    c = d.constraints()
+    keep = c["kind"] == abi.CABLE
+    return np.stack([c["first_node"][keep], c["second_node"][keep]], axis=1).astype(np.int64)
+
+
+def min_separation(x, segs):
+    """The smallest closest distance over pairs of segments that share no
+    node and whose midpoints lie within 0.15 m."""
+    best = np.inf
+    mids = 0.5 * (x[segs[:, 0]] + x[segs[:, 1]])
+    for i in range(len(segs)):
+        for j in range(i + 1, len(segs)):
+            if set(segs[i]) & set(segs[j]) or np.linalg.norm(mids[i] - mids[j]) > 0.15:
+                continue
+            best = min(best, segment_distance(x[segs[i, 0]], x[segs[i, 1]], x[segs[j, 0]], x[segs[j, 1]]))
+    return best
+
+
+def test_port_ropes_are_kept_apart():
+    d = crossing_ropes()
+    port = O.PortStructure(d)
+    port.set_line_contact(RADIUS, 0.002)
+    st = step_settings(gravity=(1.0, 2.0, -9.81))
+    for _ in range(10):
+        port.step(st)
+    x = port.node_states()[:, 0, :]
+    assert min_separation(x, cable_segments(d)) >= 2 * RADIUS * 0.9
+
+
+@pytest.mark.gpu
+def test_device_matches_the_port_on_crossing_ropes(cuda_device):
+    d = crossing_ropes()
+    dev = sw.Structure(d)
+    dev.set_line_contact(RADIUS, 0.002)
+    orc = O.PortStructure(dev.oracle_definition())
+    orc.set_line_contact(RADIUS, 0.002)
+    st = step_settings(gravity=(1.0, 2.0, -9.81))
+    errs = []
+    for _ in range(40):
+        sync_oracle_to_device(dev, orc)
+        dev.step(st, diagnostics=False)
+        orc.step(st)
+        errs.append(rel_error(dev.node_states(), orc.node_states()))
+    assert max(errs) <= REL_TOL, max(errs)
+    assert min_separation(dev.node_states()[:, 0, :], cable_segments(d)) >= 2 * RADIUS * 0.9
+
+
+@pytest.mark.gpu
+def test_device_matches_the_port_on_a_wing_with_cable_lines(cuda_device):
+    """The small wing without its pilot: the cascaded lines are nodal
+    cables, the segments near each junction come within reach of one
+    another."""
+    d = sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, pilot=0)
+    assert d.counts()["cable"] > 0
+    dev = sw.Structure(d)
+    dev.set_line_contact(0.002, 0.004)
+    orc = O.PortStructure(dev.oracle_definition())
+    orc.set_line_contact(0.002, 0.004)
+    st = step_settings()
+    errs = []
+    for _ in range(30):
+        sync_oracle_to_device(dev, orc)
+        dev.step(st, diagnostics=False)
+        orc.step(st)
+        errs.append(rel_error(dev.node_states(), orc.node_states()))
+    assert max(errs) <= REL_TOL, max(errs)
+
+
+@pytest.mark.gpu
+def test_line_contact_refusals(cuda_device):
+    d = crossing_ropes(k=3, n=6)
+    s = sw.Structure(d)
+    with pytest.raises(sw.InvalidArgument):
+        s.set_line_contact(0.0)
+    with pytest.raises(sw.InvalidArgument):
+        s.set_line_contact(RADIUS, -1.0)
+    s.set_line_contact(RADIUS)
+    st = step_settings()
+    s.step(st, diagnostics=False)
+    with pytest.raises(sw.Unsupported):
+        r = sw.Rollout(s, 4, 2)
+        r.forward(st, s.node_states()[:, 0, :], np.ones(s.node_count))
+    s.set_line_contact(RADIUS, enabled=False)
+    s.step(st, diagnostics=False)
+    s.close()
+    grid = sw.Structure(d, sw.SolverOptions(flags=abi.OPT_GRID))
+    with pytest.raises(sw.Unsupported):
+        grid.set_line_contact(RADIUS)
+    grid.close()
+    with sw.Batch([d, d]) as batch:
+        batch.structure(1).set_line_contact(RADIUS)
+        with pytest.raises(sw.Unsupported):
+            batch.step(st, 1)
