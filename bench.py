@@ -391,7 +391,7 @@ def batched_adjoint_leg(sw, st, device, wings=32, steps=240, interval=16, group=
     specs = [dict(cells=int(rng.integers(30, 51)), chordwise=45, seed=7000 + i) for i in range(wings)]
     opts = sw.SolverOptions(device=device)
     total_fwd = total_bwd = 0.0
-    tri, hits = [], 0
+    tri, hits, overflowed = [], 0, 0
     for start in range(0, wings, group):
         structures, rollouts, targets, weights = [], [], [], []
         for spec in specs[start:start + group]:
@@ -415,11 +415,13 @@ def batched_adjoint_leg(sw, st, device, wings=32, steps=240, interval=16, group=
         t0 = time.perf_counter()
         sw.rollout_forward_many(rollouts, st, targets, weights)
         t1 = time.perf_counter()
-        grads = sw.rollout_backward_many(rollouts)
+        statuses = np.zeros(len(rollouts), dtype=np.int32)
+        sw.rollout_backward_many(rollouts, statuses)
         t2 = time.perf_counter()
         total_fwd += t1 - t0
         total_bwd += t2 - t1
-        hits += sum(1 for g in grads if np.isfinite(g["d_rest"]).all())
+        hits += int((statuses == sw.abi.OK).sum())
+        overflowed += int((statuses == sw.abi.NON_FINITE).sum())
         for r in rollouts:
             r.close()
         for s in structures:
@@ -430,6 +432,10 @@ def batched_adjoint_leg(sw, st, device, wings=32, steps=240, interval=16, group=
             "wings": wings, "triangles_min": min(tri), "triangles_max": max(tri), "steps": steps,
             "forward_s": total_fwd, "backward_s": total_bwd,
             "wing_gradients_per_s": wings / (total_fwd + total_bwd), "finite_gradients": hits,
+            "overflowed_gradients": overflowed,
+            "overflow_note": "SWB_NON_FINITE: the free-falling wing's tip trailing edge flutters, and the rollout's "
+                             "sensitivity outgrows FP32 in the reverse sweep (the FP64 adjoint along the same device "
+                             "trajectory reaches 3.5e19 after 48 steps on such a wing)",
             "line_line_contact": "refused in rollouts"}
 
 

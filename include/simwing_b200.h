@@ -731,6 +731,12 @@ swb_status swb_rollout_forward(swb_rollout* rollout,
                                const double* target_xyz,
                                const double* weights,
                                double* loss);
+/* The gradient of the last forward's loss.  SWB_NON_FINITE when an entry
+ * is not finite (the arrays are written all the same): the reverse sweep
+ * runs in FP32, and a rollout whose sensitivity to its parameters grows
+ * past FP32's range over its length (an unstable flutter of the fabric
+ * amplifies the adjoint step by step) overflows; shorter rollouts stay
+ * finite. */
 swb_status swb_rollout_backward(swb_rollout* rollout,
                                 const swb_rollout_gradient* gradient);
 /* The forward of `count` rollouts at once (targets_xyz[k], weights[k] and

@@ -996,14 +996,21 @@ def rollout_forward_many(rollouts, settings: abi.StepSettings, targets, weights)
     return losses
 
 
-def rollout_backward_many(rollouts) -> list:
+def rollout_backward_many(rollouts, statuses: np.ndarray | None = None) -> list:
     """The backwards of several rollouts at once (swb_rollout_backward_many);
-    one gradient dict per rollout, as Rollout.backward returns it."""
+    one gradient dict per rollout, as Rollout.backward returns it.  With
+    `statuses` (an int32 array, one entry per rollout) the call fills it and
+    raises only when it fails as a whole (each rollout's own failure, as
+    SWB_NON_FINITE for an overflowed gradient, is left in its entry)."""
     lib = abi.library()
     k = len(rollouts)
     bufs = [r._gradient_buffers() for r in rollouts]
     grads = (abi.RolloutGradient * k)(*[b[1] for b in bufs])
     handles = (C.c_void_p * k)(*[r._h for r in rollouts])
-    statuses = np.zeros(k, dtype=np.int32)
-    _check(lib.swb_rollout_backward_many(handles, k, grads, statuses.ctypes.data))
+    own = statuses is None
+    st = np.zeros(k, dtype=np.int32) if own else statuses
+    assert st.dtype == np.int32 and st.shape == (k,)
+    status = lib.swb_rollout_backward_many(handles, k, grads, st.ctypes.data)
+    if own or not (st != abi.OK).any():
+        _check(status)
     return [Rollout._gradient_result(out, sizes) for out, _, sizes in bufs]

@@ -463,7 +463,20 @@ struct RolloutImpl {
         cuda_check(cudaMemcpyAsync(seg.data(), g_seg, 8 * sizeof(double), cudaMemcpyDeviceToHost, st), "read");
         cuda_check(cudaMemcpyAsync(&mass, g_mass, sizeof(double), cudaMemcpyDeviceToHost, st), "read");
         cuda_check(cudaStreamSynchronize(st), "read");
-        if (!out) return;
+        bool finite = std::isfinite(mass);
+        for (const std::vector<double>* v : {&rest0, &comp0, &comp1, &seg})
+            for (double x : *v) finite = finite && std::isfinite(x);
+        if (out) write_gradient(out, rest0, comp0, comp1, seg, mass);
+        if (!finite)
+            raise(SWB_NON_FINITE,
+                  "the gradient is not finite: the FP32 reverse sweep overflowed (the rollout's sensitivity to its "
+                  "parameters outgrew FP32's range over its length, as an unstable flutter makes it); the output "
+                  "arrays hold the values reached");
+    }
+
+    void write_gradient(const swb_rollout_gradient* out, const std::vector<double>& rest0,
+                        const std::vector<double>& comp0, const std::vector<double>& comp1,
+                        const std::vector<double>& seg, double mass) const {
         const ClusterSchedule& cs = S->csched;
         const size_t M = S->def.constraints.size(), H = S->def.dihedrals.size();
         if (out->d_rest || out->d_compliance)

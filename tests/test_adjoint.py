@@ -241,3 +241,38 @@ def test_rollouts_side_by_side_equal_one_at_a_time(cuda_device):
         r.close()
     for s in structures:
         s.close()
+
+
+def test_overflowed_gradient_is_reported(cuda_device):
+    """A gradient beyond FP32's range comes back as SWB_NON_FINITE, the
+    arrays written all the same: a target 1e42 m away makes the reverse
+    sweep's FP32 seed overflow (the loss itself, in FP64, stays finite).  Side by side, the other rollout's
+    status stays SWB_OK and its gradient equals the one it gives alone."""
+    st = step_settings()
+    d = sw.generate_patch(nx=12, ny=12, seed=4)
+    a, b = sw.Structure(d), sw.Structure(d)
+    n = a.node_count
+    target = a.positions().copy()
+    w = np.ones(n)
+    far = target.copy()
+    far[5] = 1e42
+    r = sw.Rollout(a, 4, 2)
+    r.forward(st, far, w)
+    with pytest.raises(sw.NonFiniteState):
+        r.backward()
+    good = sw.Rollout(b, 4, 2)
+    good.forward(st, target, w)
+    alone = good.backward()
+    r.forward(st, far, w)
+    good.forward(st, target, w)
+    statuses = np.zeros(2, dtype=np.int32)
+    grads = sw.rollout_backward_many([r, good], statuses)
+    assert list(statuses) == [abi.NON_FINITE, abi.OK]
+    assert not np.isfinite(grads[0]["d_rest"]).all()
+    np.testing.assert_array_equal(grads[1]["d_rest"], alone["d_rest"])
+    with pytest.raises(sw.NonFiniteState):
+        sw.rollout_backward_many([r, good])
+    r.close()
+    good.close()
+    a.close()
+    b.close()
