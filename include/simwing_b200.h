@@ -475,7 +475,9 @@ swb_status swb_structure_set_ground(swb_structure* structure, const swb_ground* 
  * segments ordered by their smaller, then larger definition node index):
  * the closest points of the two segments pushed apart to 2 x radius,
  * rigidly.  enabled = 0 (or a null pointer) removes it.  Single structures
- * only (batches and differentiable rollouts refuse it). */
+ * and their differentiable rollouts (which tape up to 4,096 candidates per
+ * step and fail the backward with SWB_CONTACT_ERROR beyond that); batches
+ * refuse it. */
 typedef struct swb_line_contact {
     double radius;
     double margin;

@@ -82,7 +82,7 @@ _ADJ = {
     "swa_rollout_gradient": (C.c_int, [P(abi.StructureDefinition), P(abi.StepSettings), C.c_int, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        P(C.c_double), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                       P(C.c_double), C.c_void_p]),
+                                       P(C.c_double), C.c_void_p, C.c_void_p]),
 }
 
 _libs = {}
@@ -350,7 +350,7 @@ def adjoint_library() -> C.CDLL:
 
 
 def rollout_gradient(definition, settings, steps, target, weights, forces=None, state=None, payload=None,
-                     trajectory=None, trajectory_payloads=None, ground=None):
+                     trajectory=None, trajectory_payloads=None, ground=None, lines=None):
     """FP64 loss and gradient of sum_i w_i |x_i(T) - target_i|^2 / sum w over
     `steps` steps (the definition's insertion order is the sweep order) from
     `state` (N x 3 x 3 node states as read_nodes returns: position, previous,
@@ -359,7 +359,8 @@ def rollout_gradient(definition, settings, steps, target, weights, forces=None, 
     pilot).  `trajectory` (steps x N x 3 x 3) and `trajectory_payloads`
     (steps x 13), when given, restart every step s > 0 from that state, so
     the reverse sweep is evaluated along another solver's trajectory.
-    `ground` = (normal xyz, offset) adds the frictionless ground plane.
+    `ground` = (normal xyz, offset) adds the frictionless ground plane;
+    `lines` = (radius, margin) adds line-line contact of the cable segments.
     Returns a dict: loss, final (N x 3), d_rest and d_comp
     (per constraint), d_dihedral_comp (per dihedral), d_segment_rest (per
     suspension segment, definition order), d_mass."""
@@ -385,6 +386,7 @@ def rollout_gradient(definition, settings, steps, target, weights, forces=None, 
            "d_dihedral_comp": np.zeros(max(h, 1)), "d_segment_rest": np.zeros(max(ns, 1))}
     loss, mass = C.c_double(), C.c_double()
     g = None if ground is None else np.ascontiguousarray([*ground[0], ground[1]], dtype=np.float64)
+    lc = None if lines is None else np.ascontiguousarray(lines, dtype=np.float64)
     rc = lib.swa_rollout_gradient(definition.pointer, C.byref(settings), int(steps),
                                   None if x0 is None else x0.ctypes.data, None if p0 is None else p0.ctypes.data,
                                   None if traj is None else traj.ctypes.data,
@@ -393,7 +395,8 @@ def rollout_gradient(definition, settings, steps, target, weights, forces=None, 
                                   C.byref(loss), out["final"].ctypes.data, out["d_rest"].ctypes.data,
                                   out["d_comp"].ctypes.data, out["d_dihedral_comp"].ctypes.data,
                                   out["d_segment_rest"].ctypes.data, C.byref(mass),
-                                  None if g is None else g.ctypes.data)
+                                  None if g is None else g.ctypes.data,
+                                  None if lc is None else lc.ctypes.data)
     if rc != 0:
         raise OracleError(abi.INVALID_ARGUMENT, lib.swa_last_error().decode())
     out["d_rest"], out["d_comp"] = out["d_rest"][:m], out["d_comp"][:m]

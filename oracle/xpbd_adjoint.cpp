@@ -680,6 +680,8 @@ struct StepTape {
     std::vector<V3<double>> fin_x, fin_v;             // attachment nodes at finish
     std::vector<double> fin_lambda;
     std::vector<uint8_t> ground_moved;                // [it * n + i]: the ground plane moved the node
+    std::vector<std::array<size_t, 2>> line_pairs;    // the step's line-line candidates (segment indices), key order
+    std::vector<std::array<V3<double>, 4>> line_in;   // [it * pairs + k]: the candidate's end nodes before it
 };
 
 struct Rollout {
@@ -696,7 +698,81 @@ struct Rollout {
     bool ground = false;
     V3<double> ground_normal{0, 0, 1};
     double ground_offset = 0.0;
+    // line-line contact of the cable segments (the device's
+    // swb_structure_set_line_contact; no reference counterpart): segments by
+    // (smaller, larger) node, the radius and the box reach
+    bool lines = false;
+    double line_radius = 0.0, line_reach = 0.0;
+    std::vector<std::array<uint64_t, 2>> line_seg;
 };
+
+// Closest points of two segments (Ericson, Real-Time Collision Detection
+// 5.1.9) as the device computes them, the clamps as constants.
+template <class T> T clamp01(const T& x) { return val(x) < 0.0 ? T(0.0) : (val(x) > 1.0 ? T(1.0) : x); }
+
+// One line-line projection: the segments' closest points pushed apart to
+// `gap`, rigidly, the correction shared by the end nodes by inverse mass and
+// barycentric weight.
+template <class T>
+void project_line_pair(V3<T>& A, V3<T>& B, V3<T>& C, V3<T>& D, const double w[4], double gap) {
+    const V3<T> d1 = sub(B, A), d2 = sub(D, C), r = sub(A, C);
+    constexpr double eps = 1.0e-12;
+    const T a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    T s(0.0), t(0.0);
+    if (val(a) <= eps && val(e) <= eps) {
+    } else if (val(a) <= eps) {
+        t = clamp01(f / e);
+    } else {
+        const T c = dot(d1, r);
+        if (val(e) <= eps) {
+            s = clamp01(-c / a);
+        } else {
+            const T b = dot(d1, d2), denom = a * e - b * b;
+            s = val(denom) != 0.0 ? clamp01((b * f - c * e) / denom) : T(0.0);
+            t = (b * s + f) / e;
+            if (val(t) < 0.0) {
+                t = T(0.0);
+                s = clamp01(-c / a);
+            } else if (val(t) > 1.0) {
+                t = T(1.0);
+                s = clamp01((b - c) / a);
+            }
+        }
+    }
+    const V3<T> diff = sub(add(A, mul(d1, s)), add(C, mul(d2, t)));
+    const T dist = sqrt(dot(diff, diff));
+    if (!(val(dist) < gap) || !(val(dist) > 0.0)) return;
+    const V3<T> n = mul(diff, T(1.0) / dist);
+    const T wa = w[0] * (1.0 - s), wb = w[1] * s, wc = w[2] * (1.0 - t), wd = w[3] * t;
+    const T W = wa * (1.0 - s) + wb * s + wc * (1.0 - t) + wd * t;
+    if (!(val(W) > 0.0)) return;
+    const T dl = (gap - dist) / W;
+    A = add(A, mul(n, wa * dl));
+    B = add(B, mul(n, wb * dl));
+    C = sub(C, mul(n, wc * dl));
+    D = sub(D, mul(n, wd * dl));
+}
+
+// The step's line-line candidates at the predicted positions: segments that
+// share no node and whose boxes, widened by the reach, overlap, in key order.
+std::vector<std::array<size_t, 2>> line_candidates(const Rollout& R, const std::vector<V3<double>>& x) {
+    std::vector<std::array<size_t, 2>> out;
+    const double r = R.line_reach;
+    const auto& S = R.line_seg;
+    for (size_t i = 0; i < S.size(); ++i) {
+        const V3<double> a = x[S[i][0]], b = x[S[i][1]];
+        for (size_t j = i + 1; j < S.size(); ++j) {
+            if (S[j][0] == S[i][0] || S[j][0] == S[i][1] || S[j][1] == S[i][0] || S[j][1] == S[i][1]) continue;
+            const V3<double> c = x[S[j][0]], d = x[S[j][1]];
+            if (std::fmin(a.x, b.x) - r > std::fmax(c.x, d.x) + r || std::fmin(c.x, d.x) - r > std::fmax(a.x, b.x) + r ||
+                std::fmin(a.y, b.y) - r > std::fmax(c.y, d.y) + r || std::fmin(c.y, d.y) - r > std::fmax(a.y, b.y) + r ||
+                std::fmin(a.z, b.z) - r > std::fmax(c.z, d.z) + r || std::fmin(c.z, d.z) - r > std::fmax(a.z, b.z) + r)
+                continue;
+            out.push_back({i, j});
+        }
+    }
+    return out;
+}
 
 bool forward_step(Rollout& R, bool record) {
     const Model& M = R.M;
@@ -729,6 +805,12 @@ bool forward_step(Rollout& R, bool record) {
         const V3<double> acc = add(R.g, mul(force[i], M.w[i]));
         v[i] = add(R.ref, mul(sub(add(v[i], mul(acc, R.dt)), R.ref), R.damping));
         x[i] = add(x[i], mul(v[i], R.dt));
+    }
+    std::vector<std::array<size_t, 2>> line_pairs;
+    if (R.lines) line_pairs = line_candidates(R, x);
+    if (record) {
+        T.line_pairs = line_pairs;
+        T.line_in.resize(static_cast<size_t>(R.iterations) * line_pairs.size());
     }
     std::vector<double> lam(M.m, 0.0), hlam(M.h, 0.0);
     if (record) {
@@ -768,6 +850,14 @@ bool forward_step(Rollout& R, bool record) {
             for (const Seg& s : M.seg) rest.push_back(s.rest);
             if (!line_iteration(M, P, xs, seg_lambda, rest, M.mass, R.dt)) return false;
             for (size_t k = 0; k < M.att_nodes.size(); ++k) x[M.att_nodes[k]] = xs[k];
+        }
+        for (size_t k = 0; k < line_pairs.size(); ++k) {
+            const auto& s1 = R.line_seg[line_pairs[k][0]];
+            const auto& s2 = R.line_seg[line_pairs[k][1]];
+            const uint64_t nd[4] = {s1[0], s1[1], s2[0], s2[1]};
+            if (record) T.line_in[it * line_pairs.size() + k] = {x[nd[0]], x[nd[1]], x[nd[2]], x[nd[3]]};
+            const double w[4] = {M.w[nd[0]], M.w[nd[1]], M.w[nd[2]], M.w[nd[3]]};
+            project_line_pair(x[nd[0]], x[nd[1]], x[nd[2]], x[nd[3]], w, 2.0 * R.line_radius);
         }
         if (R.ground) {
             if (record) T.ground_moved.resize(static_cast<size_t>(R.iterations) * M.n, 0);
@@ -915,6 +1005,31 @@ void reverse_step(const Rollout& R, const StepTape& T, std::vector<V3<double>>& 
             for (uint64_t i = 0; i < M.n; ++i)
                 if (T.ground_moved[static_cast<size_t>(it) * M.n + i])
                     xb[i] = sub(xb[i], mul(R.ground_normal, dot(R.ground_normal, xb[i])));
+        // the line-line projections, last candidate first: each one's
+        // Jacobian by forward mode at its taped inputs, its transpose applied
+        // to the adjoints of its four end nodes
+        for (size_t k = T.line_pairs.size(); k-- > 0;) {
+            const auto& s1 = R.line_seg[T.line_pairs[k][0]];
+            const auto& s2 = R.line_seg[T.line_pairs[k][1]];
+            const uint64_t nd[4] = {s1[0], s1[1], s2[0], s2[1]};
+            const auto& in = T.line_in[it * T.line_pairs.size() + k];
+            V3<Dual<12>> q[4];
+            for (int c = 0; c < 4; ++c) q[c] = seed3<12>(in[c], 3 * c);
+            const double w[4] = {M.w[nd[0]], M.w[nd[1]], M.w[nd[2]], M.w[nd[3]]};
+            project_line_pair(q[0], q[1], q[2], q[3], w, 2.0 * R.line_radius);
+            double ob[12], ib[12] = {};
+            for (int c = 0; c < 4; ++c) {
+                ob[3 * c] = xb[nd[c]].x;
+                ob[3 * c + 1] = xb[nd[c]].y;
+                ob[3 * c + 2] = xb[nd[c]].z;
+            }
+            for (int c = 0; c < 4; ++c) {
+                const Dual<12>* o[3] = {&q[c].x, &q[c].y, &q[c].z};
+                for (int k3 = 0; k3 < 3; ++k3)
+                    for (int j = 0; j < 12; ++j) ib[j] += ob[3 * c + k3] * o[k3]->d[j];
+            }
+            for (int c = 0; c < 4; ++c) xb[nd[c]] = {ib[3 * c], ib[3 * c + 1], ib[3 * c + 2]};
+        }
         if (M.susp) {
             // inputs: com 3, q 4, lambda ns, xs 3*na, rest ns, mass 1
             constexpr int N = 3 + 4 + 2 + 6 + 2 + 1;
@@ -1039,6 +1154,8 @@ const char* swa_last_error() { return g_err.c_str(); }
 // and steps x 13 in the same layouts) restart every step s > 0 from a given
 // trajectory, so that the reverse sweep runs along another solver's states.
 // `ground` (nullable: none) is a frictionless ground plane (normal xyz, offset).
+// `lines` (nullable: none) is line-line contact of the cable segments
+// (radius, margin).
 // Then evaluates the loss against `target` (node_count xyz) with node weights `weights` and its gradient.  Outputs
 // (nullable): final positions (node_count xyz), d rest / d compliance per
 // constraint, d compliance per dihedral, d rest per suspension segment
@@ -1048,7 +1165,7 @@ int swa_rollout_gradient(const swb_structure_definition* def, const swb_step_set
                          const double* step_payloads, const double* forces, const double* target,
                          const double* weights, double* loss,
                          double* final_xyz, double* d_rest, double* d_comp, double* d_dihedral_comp,
-                         double* d_segment_rest, double* d_mass, const double* ground) {
+                         double* d_segment_rest, double* d_mass, const double* ground, const double* lines) {
     try {
         Rollout R;
         if (!build_model(*def, R.M, g_err)) return 1;
@@ -1067,6 +1184,16 @@ int swa_rollout_gradient(const swb_structure_definition* def, const swb_step_set
             R.ground = true;
             R.ground_normal = {ground[0], ground[1], ground[2]};
             R.ground_offset = ground[3];
+        }
+        if (lines) {
+            R.lines = true;
+            R.line_radius = lines[0];
+            R.line_reach = lines[0] + 0.5 * lines[1];
+            for (uint64_t i = 0; i < M.m; ++i)
+                if (M.kind[i] == SWB_CONSTRAINT_CABLE)
+                    R.line_seg.push_back({std::min(M.ca[i], M.cb[i]), std::max(M.ca[i], M.cb[i])});
+            std::sort(R.line_seg.begin(), R.line_seg.end());
+            R.line_seg.erase(std::unique(R.line_seg.begin(), R.line_seg.end()), R.line_seg.end());
         }
         if (forces)
             for (uint64_t i = 0; i < M.n; ++i) R.M.pending[i] = {forces[3 * i], forces[3 * i + 1], forces[3 * i + 2]};

@@ -53,6 +53,11 @@ struct RolloutImpl {
     std::vector<StateBuf> ck, sg;      // checkpoints (segments + 1), segment states (interval + 1)
     std::vector<TapeStep> tape;        // per step of a segment
     int tape_iterations = -1;
+    bool tape_lines = false;           // the tapes hold line-line contact arrays
+    std::vector<ClusterInstance> rec_host;  // d_records' host copy
+    bool rec_lines = false;            // d_records carry the structure's line-line contact
+    bool fwd_lines = false;            // the last forward ran with line-line contact
+    static constexpr uint32_t kLineTapeCap = 4096;  // line-line candidates a tape step holds
     float* line_jac = nullptr;  // per-iteration line-iteration Jacobians of the reverse step
     ClusterInstance* d_records = nullptr;  // step k of a segment: sg[k] -> sg[k + 1]
     AdjointPilot* d_pilot = nullptr;
@@ -183,6 +188,7 @@ struct RolloutImpl {
             c.recentre = S->def.has_suspension ? 1 : 0;
             rec[k] = c;
         }
+        rec_host = rec;
         d_records = ralloc<ClusterInstance>(owned, rec.size());
         cuda_check(cudaMemcpyAsync(d_records, rec.data(), rec.size() * sizeof(ClusterInstance), cudaMemcpyHostToDevice,
                                    S->stream), "records upload");
@@ -221,11 +227,26 @@ struct RolloutImpl {
         cuda_check(cudaStreamSynchronize(S->stream), "rollout setup");
     }
 
+    // The step records carry the structure's line-line contact when it is
+    // set (its candidate lists are the structure's scratch).
+    void sync_records() {
+        const bool want = S->line_contact;
+        if (want == rec_lines) return;
+        for (ClusterInstance& c : rec_host) c.lines = want ? S->d_lines : nullptr;
+        cuda_check(cudaMemcpyAsync(d_records, rec_host.data(), rec_host.size() * sizeof(ClusterInstance),
+                                   cudaMemcpyHostToDevice, S->stream),
+                   "records upload");
+        rec_lines = want;
+    }
+
     void ensure_tapes(int iterations) {
-        if (!tape.empty() && tape_iterations == iterations) return;
+        if (!tape.empty() && tape_iterations == iterations && tape_lines == S->line_contact) return;
         for (TapeStep& t : tape)
             for (void* q : {static_cast<void*>(t.dist), static_cast<void*>(t.dih), static_cast<void*>(t.seam),
-                            static_cast<void*>(t.line), static_cast<void*>(t.finish), static_cast<void*>(t.ground)}) {
+                            static_cast<void*>(t.line), static_cast<void*>(t.finish), static_cast<void*>(t.ground),
+                            static_cast<void*>(t.line_pairs), static_cast<void*>(t.line_level_off),
+                            static_cast<void*>(t.line_count), static_cast<void*>(t.line_in)}) {
+                if (!q) continue;
                 cudaFree(q);
                 owned.erase(std::remove(owned.begin(), owned.end(), q), owned.end());
             }
@@ -239,6 +260,13 @@ struct RolloutImpl {
             t.line = ralloc<PilotTape>(owned, it);
             t.finish = ralloc<PilotTape>(owned, 1);
             t.ground = ralloc<uint8_t>(owned, it * S->def.nodes.size());
+            if (S->line_contact) {
+                t.line_cap = kLineTapeCap;
+                t.line_pairs = ralloc<uint32_t>(owned, kLineTapeCap);
+                t.line_level_off = ralloc<uint32_t>(owned, kLineTapeCap + 1);
+                t.line_count = ralloc<uint32_t>(owned, 2);
+                t.line_in = ralloc<float4>(owned, it * kLineTapeCap * 4);
+            }
             t.r0 = r0;
             t.r1 = r1;
             t.rs = rs;
@@ -256,6 +284,7 @@ struct RolloutImpl {
             line_jac = ralloc<float>(owned, it * nin * nout);
         }
         tape_iterations = iterations;
+        tape_lines = S->line_contact;
     }
 
     ClusterParams step_params(int k, const TapeStep* t) const {
@@ -322,7 +351,6 @@ struct RolloutImpl {
         if (st.substeps != 1) raise(SWB_UNSUPPORTED, "differentiable rollouts take one substep per step");
         if (S->cparams.ground && S->cparams.ground_friction > 0.0f)
             raise(SWB_UNSUPPORTED, "differentiable rollouts take a frictionless ground plane");
-        if (S->line_contact) raise(SWB_UNSUPPORTED, "differentiable rollouts do not take line-line contact");
         const size_t N = S->def.nodes.size();
         double wsum = 0.0;
         for (size_t i = 0; i < N; ++i) {
@@ -336,6 +364,8 @@ struct RolloutImpl {
         settings = st;
         have_forward = false;
         cuda_check(cudaSetDevice(S->device), "cudaSetDevice");
+        sync_records();
+        fwd_lines = S->line_contact;
         if (S->pressure_dirty) S->upload_pressure();
         if (S->forces_dirty) S->upload_forces();
         cuda_check(cudaMemsetAsync(S->d_control, 0, offsetof(Control, shift), S->stream), "control reset");
@@ -394,7 +424,10 @@ struct RolloutImpl {
     // The backward's launches on the structure's stream (no wait for them).
     void backward_launch() {
         if (!have_forward) raise(SWB_INVALID_ARGUMENT, "backward needs a forward first");
+        if (S->line_contact != fwd_lines)
+            raise(SWB_INVALID_ARGUMENT, "line-line contact was switched between the forward and the backward");
         cuda_check(cudaSetDevice(S->device), "cudaSetDevice");
+        sync_records();
         const size_t N = S->def.nodes.size();
         ensure_tapes(settings.constraint_iterations);
         cudaStream_t st = S->stream;

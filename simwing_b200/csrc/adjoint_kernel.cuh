@@ -478,6 +478,13 @@ __global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(con
             }
             cluster.sync();
         }
+        // the line-line projections followed the pilot's line iteration
+        if (I.lines) {
+            if (me == 0)
+                line_contact_reverse(*I.lines, p.tape, it,
+                                     [&](uint32_t ref) { return node_addr(ref, me, 0u, x_base); });
+            cluster.sync();
+        }
         if (I.susp_cta >= 0 && line_stage < 0) {
             if (pilot_warp) line_reverse(pa, *ap, p.line_jac + static_cast<size_t>(it) * line_block, xb);
             cluster.sync();

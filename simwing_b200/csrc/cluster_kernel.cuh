@@ -494,6 +494,9 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         line_broadphase(*lines, me, static_cast<uint32_t>(sctas), cluster, line_addr, I.status);
         cluster.sync();
         if (me == 0) line_sort(*lines, lines->sort);
+        if constexpr (kTape) {
+            if (me == 0 && !line_tape_step(*lines, p.tape) && tid == 0) contact_fail(I.status, kContactLineTape);
+        }
     }
 
     // ---- constraint iterations ------------------------------------------------
@@ -621,7 +624,12 @@ __global__ void __launch_bounds__(kClusterMaxThreads) xpbd_cluster_kernel_t(cons
         }
         if constexpr (kContact) contact_iteration(cctx, cluster);
         if (lines) {
-            if (me == 0 && tid == 0) line_project(*lines, line_addr);
+            float4* line_tape = nullptr;
+            if constexpr (kTape) {
+                if (lines->count[0] <= p.tape.line_cap)
+                    line_tape = p.tape.line_in + static_cast<size_t>(it) * p.tape.line_cap * 4;
+            }
+            if (me == 0) line_project(*lines, line_addr, line_tape);
             cluster.sync();
         }
         if (p.ground) {

@@ -164,8 +164,10 @@ struct LineContactDev {
     float reach;                       // box half-margin of the step's broadphase: radius + margin / 2
     float4* box;                       // [segments][2] the step's predicted boxes (lo, hi)
     uint32_t* pair;                    // [capacity] candidate pairs i << 16 | j, i < j, sorted after the broadphase
-    uint32_t* sort;                    // [capacity] scratch of the sort
-    uint32_t* count;                   // [1] candidate pairs of the step
+    uint32_t* sort;                    // [capacity] scratch of the sort, then each sorted pair's level
+    uint32_t* order;                   // [capacity] the pairs by level, key order within a level
+    uint32_t* level_off;               // [capacity + 1] each level's first place in `order`
+    uint32_t* count;                   // [2] candidate pairs of the step, their level count
 };
 
 // Per-instance tables and state (one cluster each).
@@ -254,6 +256,14 @@ struct TapeStep {
     PilotTape* line;       // [iterations]
     PilotTape* finish;     // [1]
     uint8_t* ground;       // [iterations][slots]: 1 where the ground projection moved the node
+    // line-line contact (null without it): the step's candidates in level
+    // order, the level offsets, [count, level count], and each candidate's
+    // four end nodes before its projection, [iterations][line_cap][4]
+    uint32_t* line_pairs;
+    uint32_t* line_level_off;
+    uint32_t* line_count;
+    float4* line_in;
+    uint32_t line_cap;
     uint32_t r0, r1, rs;   // records per kind and seam records
     const AdjointPilot* pilot;
 };

@@ -50,6 +50,7 @@ enum : int {
     kContactTable = 17,          // more warm-started features than the device table holds
     kContactRecords = 18,        // more records than the device book holds
     kContactLinePairs = 19,      // more line-line candidate pairs than the device list holds
+    kContactLineTape = 20,       // more line-line candidates than a rollout's tape holds
 };
 
 __device__ __forceinline__ void contact_fail(int* status, int code) {

@@ -438,7 +438,9 @@ void StructureImpl::setup_line_contact() {
     L.box = dalloc<float4>(owned, 2 * std::max<size_t>(segs.size(), 1));
     L.pair = dalloc<uint32_t>(owned, L.capacity);
     L.sort = dalloc<uint32_t>(owned, L.capacity);
-    L.count = dalloc<uint32_t>(owned, 1);
+    L.order = dalloc<uint32_t>(owned, L.capacity);
+    L.level_off = dalloc<uint32_t>(owned, L.capacity + 1);
+    L.count = dalloc<uint32_t>(owned, 2);
     lines_host = L;
     d_lines = dupload(owned, std::vector<LineContactDev>{L}, stream);
 }
@@ -1146,8 +1148,9 @@ swb_status decode_status(const int status[2], std::string& message) {
             "contact candidates exceed the device list (1,048,576 per phase)",
             "contact features exceed the device multiplier table",
             "contact records exceed the device record book",
-            "line-line contact pairs exceed the device list"};
-        message = std::string("ContactStepError: ") + what[std::clamp(status[1], 0, 19)];
+            "line-line contact pairs exceed the device list",
+            "line-line contact candidates exceed the rollout's tape"};
+        message = std::string("ContactStepError: ") + what[std::clamp(status[1], 0, 20)];
         return SWB_CONTACT_ERROR;
     }
     if (status[0] & dev::kStatusMembrane) {

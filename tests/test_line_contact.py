@@ -12,7 +12,12 @@ projected in key order, the segments' closest points pushed apart to
 exactly 2 x radius apart; segments that share a node or lie beyond reach
 are left alone); on the GPU the device matches the port per step on
 crossing ropes and on a wing whose lines are nodal cables, and the
-refusals (batches, rollouts, grid schedule, bad radius) hold."""
+refusals (batches, grid schedule, bad radius) hold.  Differentiable
+rollouts take it: the FP64 adjoint's reverse of a projection (its Jacobian
+by forward mode at the taped inputs) agrees with central differences of
+its own forward, and the device's rollout gradient, whose reverse of a
+projection is written out by hand, agrees with the FP64 adjoint along the
+device trajectory."""
 import numpy as np
 import pytest
 
@@ -210,10 +215,12 @@ def test_line_contact_refusals(cuda_device):
     s.set_line_contact(RADIUS)
     st = step_settings()
     s.step(st, diagnostics=False)
-    with pytest.raises(sw.Unsupported):
-        r = sw.Rollout(s, 4, 2)
-        r.forward(st, s.node_states()[:, 0, :], np.ones(s.node_count))
+    r = sw.Rollout(s, 4, 2)
+    r.forward(st, s.node_states()[:, 0, :], np.ones(s.node_count))
     s.set_line_contact(RADIUS, enabled=False)
+    with pytest.raises(sw.InvalidArgument):
+        r.backward()  # switched between the forward and the backward
+    r.close()
     s.step(st, diagnostics=False)
     s.close()
     grid = sw.Structure(d, sw.SolverOptions(flags=abi.OPT_GRID))
@@ -224,3 +231,78 @@ def test_line_contact_refusals(cuda_device):
         batch.structure(1).set_line_contact(RADIUS)
         with pytest.raises(sw.Unsupported):
             batch.step(st, 1)
+
+
+ROPES_STEPS = 8
+
+
+def ropes_rollout_case():
+    """Four crossing ropes from rest (every rope within reach of the others
+    at the crossing), a target near the start, tilted gravity."""
+    d = crossing_ropes(k=4, n=8)
+    st = step_settings(gravity=(1.0, 2.0, -9.81))
+    rng = np.random.default_rng(1)
+    x0 = d.positions()
+    return d, st, x0 + rng.normal(0.0, 0.01, x0.shape), np.ones(d.node_count)
+
+
+def test_fp64_adjoint_with_line_contact_against_finite_differences():
+    d, st, target, w = ropes_rollout_case()
+    lines = (RADIUS, 0.002)
+    g = O.rollout_gradient(d, st, ROPES_STEPS, target, w, lines=lines)
+    plain = O.rollout_gradient(d, st, ROPES_STEPS, target, w)
+    assert abs(g["loss"] - plain["loss"]) > 0.1 * plain["loss"]  # the contact acts
+    rng = np.random.default_rng(2)
+    u = rng.normal(size=d.view.constraint_count)
+    h = 1e-7
+    a, b = d.copy(), d.copy()
+    a.constraints()["rest_length"][:] += h * u
+    b.constraints()["rest_length"][:] -= h * u
+    fd = (O.rollout_gradient(a, st, ROPES_STEPS, target, w, lines=lines)["loss"] -
+          O.rollout_gradient(b, st, ROPES_STEPS, target, w, lines=lines)["loss"]) / (2 * h)
+    assert abs(g["d_rest"] @ u - fd) <= 1e-6 * abs(fd), (g["d_rest"] @ u, fd)
+    c0 = d.constraints()["compliance"].copy()
+    a, b = d.copy(), d.copy()
+    a.constraints()["compliance"][:] = c0 * (1 + 1e-5)
+    b.constraints()["compliance"][:] = c0 * (1 - 1e-5)
+    fd = (O.rollout_gradient(a, st, ROPES_STEPS, target, w, lines=lines)["loss"] -
+          O.rollout_gradient(b, st, ROPES_STEPS, target, w, lines=lines)["loss"]) / 2e-5
+    assert abs((g["d_comp"] * c0).sum() - fd) <= 1e-4 * abs(fd)
+    # the adjoint's forward is the port's
+    port = O.PortStructure(d)
+    port.set_line_contact(*lines)
+    for _ in range(ROPES_STEPS):
+        port.step(st)
+    np.testing.assert_array_equal(g["final"], port.node_states()[:, 0, :])
+
+
+@pytest.mark.gpu
+def test_rollout_gradient_with_line_contact(cuda_device):
+    """The device rollout with line contact: its final positions are those of
+    plain steps, and its gradient agrees with the FP64 adjoint along the
+    device trajectory within 1e-3 per parameter class."""
+    from tests.test_adjoint import relative, to_definition_order
+
+    d, st, target, w = ropes_rollout_case()
+    s = sw.Structure(d)
+    s.set_line_contact(RADIUS, 0.002)
+    state = s.node_states()
+    r = sw.Rollout(s, ROPES_STEPS, 4)
+    r.forward(st, target, w)
+    grad = r.backward()
+    final = r.final_positions()
+    r.close()
+    traj = [state]
+    for _ in range(ROPES_STEPS):
+        s.step(st, diagnostics=False)
+        traj.append(s.node_states())
+    np.testing.assert_allclose(final, traj[-1][:, 0, :], rtol=0, atol=1e-6)
+    ref = O.rollout_gradient(s.oracle_definition(), st, ROPES_STEPS, target, w, state=state,
+                             trajectory=np.array(traj[:-1]), lines=(RADIUS, 0.002))
+    order = s.sweep_order(abi.SWEEP_DISTANCE)
+    c0 = d.constraints()["compliance"]
+    mine = {"rest": grad["d_rest"], "comp": grad["d_comp"] * c0}
+    theirs = {"rest": to_definition_order(ref["d_rest"], order), "comp": to_definition_order(ref["d_comp"], order) * c0}
+    errors = {k: relative(mine[k], theirs[k]) for k in mine}
+    assert all(v <= 1e-3 for v in errors.values()), errors
+    s.close()
