@@ -166,6 +166,7 @@ struct LineContactDev {
     uint32_t* pair;                    // [capacity] candidate pairs i << 16 | j, i < j, sorted after the broadphase
     uint32_t* sort;                    // [capacity] scratch of the sort, then each sorted pair's level
     uint32_t* order;                   // [capacity] the pairs by level, key order within a level
+    uint32_t* pred;                    // [capacity][4] per node the latest earlier pair with it (~0u: none)
     uint32_t* level_off;               // [capacity + 1] each level's first place in `order`
     uint32_t* count;                   // [2] candidate pairs of the step, their level count
 };

@@ -62,7 +62,9 @@ __device__ __forceinline__ SegmentClosest segment_closest(float3 p1, float3 d1, 
 }
 
 // The substep's candidate pairs (every thread of every CTA; a cluster
-// barrier inside, and one must follow before rank 0 sorts them).
+// barrier inside, and one must follow before rank 0 sorts them).  The pair
+// tests are spread evenly: the triangle of pairs is cut into runs of equal
+// length, one per thread.
 template <class Addr>
 __device__ void line_broadphase(const LineContactDev& L, uint32_t me, uint32_t ctas,
                                 cooperative_groups::cluster_group& cluster, Addr addr, int* status) {
@@ -75,20 +77,38 @@ __device__ void line_broadphase(const LineContactDev& L, uint32_t me, uint32_t c
             make_float4(fmaxf(A.x, B.x) + L.reach, fmaxf(A.y, B.y) + L.reach, fmaxf(A.z, B.z) + L.reach, 0.0f);
     }
     cluster.sync();
-    for (uint32_t i = gt; i < L.segments; i += stride) {
+    // the triangle of pairs (i < j), row by row, cut into equal runs, one
+    // per thread of the cluster
+    const uint64_t S = L.segments, P = S * (S - 1) / 2;
+    const uint64_t chunk = (P + stride - 1) / stride;
+    const uint64_t p0 = static_cast<uint64_t>(gt) * chunk, p1 = min(P, p0 + chunk);
+    if (p0 >= p1) return;
+    auto row_start = [&](uint64_t i) { return i * (2 * S - i - 1) / 2; };
+    const double b = 2.0 * static_cast<double>(S) - 1.0;
+    uint64_t i = static_cast<uint64_t>(max(0.0, floor((b - sqrt(max(0.0, b * b - 8.0 * static_cast<double>(p0)))) * 0.5)));
+    i = min(i, S - 2);
+    while (i > 0 && row_start(i) > p0) --i;
+    while (i + 2 < S && row_start(i + 1) <= p0) ++i;
+    uint64_t j = i + 1 + (p0 - row_start(i)), left = p1 - p0;
+    while (left > 0) {
         const float4 lo = __ldcg(L.box + 2 * i), hi = __ldcg(L.box + 2 * i + 1);
         const uint2 ni = L.seg_nodes[i];
-        for (uint32_t j = i + 1; j < L.segments; ++j) {
+        const uint64_t jend = min(S, j + left);
+        left -= jend - j;
+#pragma unroll 4
+        for (; j < jend; ++j) {
             const float4 lo2 = __ldcg(L.box + 2 * j), hi2 = __ldcg(L.box + 2 * j + 1);
             if (lo.x > hi2.x || lo2.x > hi.x || lo.y > hi2.y || lo2.y > hi.y || lo.z > hi2.z || lo2.z > hi.z) continue;
             const uint2 nj = L.seg_nodes[j];
             if (ni.x == nj.x || ni.x == nj.y || ni.y == nj.x || ni.y == nj.y) continue;
             const uint32_t k = atomicAdd(L.count, 1u);
             if (k < L.capacity)
-                L.pair[k] = (i << 16) | j;
+                L.pair[k] = (static_cast<uint32_t>(i) << 16) | static_cast<uint32_t>(j);
             else
                 contact_fail(status, kContactLinePairs);
         }
+        ++i;
+        j = i + 1;
     }
 }
 
@@ -98,19 +118,16 @@ __device__ void line_broadphase(const LineContactDev& L, uint32_t me, uint32_t c
 // when none does.  Candidates of one level share no node, and every node
 // meets its candidates in key order level by level, so projecting the
 // levels in turn, each level's candidates side by side, gives the serial
-// key-order sweep's results exactly.  The levels are found by sweeps over
-// the earlier candidates until none changes (as many sweeps as the longest
-// chain, plus one); they go to `scratch`, their count to count[1].  Reads
+// key-order sweep's results exactly.  Each candidate's predecessors (per
+// node, the latest earlier candidate with that node) are found once; the
+// levels then follow by sweeps until none changes (as many sweeps as the
+// longest chain, plus one).  They go to `scratch`, their count to
+// count[1], and the candidates, ordered by level, to `order`.  Reads
 // the candidate count after the cluster barrier that followed the
 // broadphase.
 __device__ __forceinline__ uint4 line_pair_nodes(const LineContactDev& L, uint32_t pr) {
     const uint2 a = L.seg_nodes[pr >> 16], b = L.seg_nodes[pr & 0xffffu];
     return make_uint4(a.x, a.y, b.x, b.y);
-}
-__device__ __forceinline__ bool line_share(uint4 p, uint4 q) {
-    return p.x == q.x || p.x == q.y || p.x == q.z || p.x == q.w || p.y == q.x || p.y == q.y || p.y == q.z ||
-           p.y == q.w || p.z == q.x || p.z == q.y || p.z == q.z || p.z == q.w || p.w == q.x || p.w == q.y ||
-           p.w == q.z || p.w == q.w;
 }
 __device__ void line_sort(const LineContactDev& L, uint32_t* scratch) {
     const uint32_t n = min(L.count[0], L.capacity);
@@ -123,16 +140,36 @@ __device__ void line_sort(const LineContactDev& L, uint32_t* scratch) {
         L.pair[rank] = mine;
     }
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) scratch[k] = 0u;
+    // each candidate's predecessors: for each of its four nodes the latest
+    // earlier candidate (key order) that has the node, ~0u for none
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+        const uint4 mine = line_pair_nodes(L, L.pair[k]);
+        const uint32_t v[4] = {mine.x, mine.y, mine.z, mine.w};
+        uint32_t pred[4] = {~0u, ~0u, ~0u, ~0u};
+        uint32_t open = 4;
+        for (uint32_t q = k; q-- > 0 && open > 0;) {
+            const uint4 o = line_pair_nodes(L, L.pair[q]);
+            for (int c = 0; c < 4; ++c)
+                if (pred[c] == ~0u && (v[c] == o.x || v[c] == o.y || v[c] == o.z || v[c] == o.w)) {
+                    pred[c] = q;
+                    --open;
+                }
+        }
+        for (int c = 0; c < 4; ++c) __stcg(L.pred + 4 * k + c, pred[c]);
+        __stcg(scratch + k, 0u);
+    }
     __syncthreads();
+    // the levels: sweeps of level = 1 + the predecessors' highest level
+    // until none changes (as many as the longest chain, plus one)
     uint32_t top = 0;
     for (uint32_t sweep = 0; sweep <= n; ++sweep) {
         bool changed = false;
         for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
-            const uint4 mine = line_pair_nodes(L, L.pair[k]);
             uint32_t lv = 0;
-            for (uint32_t q = 0; q < k; ++q)
-                if (line_share(mine, line_pair_nodes(L, L.pair[q]))) lv = max(lv, __ldcg(scratch + q) + 1u);
+            for (int c = 0; c < 4; ++c) {
+                const uint32_t q = __ldcg(L.pred + 4 * k + c);
+                if (q != ~0u) lv = max(lv, __ldcg(scratch + q) + 1u);
+            }
             if (lv != __ldcg(scratch + k)) changed = true;
             top = max(top, lv);
             // the block barrier below orders this store before the next
@@ -179,7 +216,7 @@ __device__ void line_sort(const LineContactDev& L, uint32_t* scratch) {
 template <class Addr>
 __device__ __forceinline__ void line_project_one(const LineContactDev& L, uint32_t pr, Addr addr, float4* tape) {
     const float gap = 2.0f * L.radius;
-    const uint32_t s1 = L.seg[pr >> 16], s2 = L.seg[pr & 0xffffu];
+    const uint32_t s1 = __ldg(L.seg + (pr >> 16)), s2 = __ldg(L.seg + (pr & 0xffffu));
     const uint32_t aa = addr(s1 & 0xffffu), ab = addr(s1 >> 16), ac = addr(s2 & 0xffffu), ad = addr(s2 >> 16);
     float4 A = ld_node(aa), B = ld_node(ab), Cn = ld_node(ac), D = ld_node(ad);
     if (tape) {
@@ -216,9 +253,20 @@ __device__ __forceinline__ void line_project_one(const LineContactDev& L, uint32
 template <class Addr>
 __device__ void line_project(const LineContactDev& L, Addr addr, float4* tape = nullptr) {
     const uint32_t top = L.count[1];
+    // each thread's first candidate of the next level is looked up before
+    // the current level's projections (the lists stay fixed for the substep)
+    uint32_t next = ~0u;
+    if (top > 0 && L.level_off[0] + threadIdx.x < L.level_off[1]) next = L.order[L.level_off[0] + threadIdx.x];
     for (uint32_t lv = 0; lv < top; ++lv) {
         const uint32_t lo = L.level_off[lv], hi = L.level_off[lv + 1];
-        for (uint32_t k = lo + threadIdx.x; k < hi; k += blockDim.x)
+        const uint32_t cur = next;
+        next = ~0u;
+        if (lv + 1 < top) {
+            const uint32_t nlo = L.level_off[lv + 1], nhi = L.level_off[lv + 2];
+            if (nlo + threadIdx.x < nhi) next = L.order[nlo + threadIdx.x];
+        }
+        if (cur != ~0u) line_project_one(L, cur, addr, tape ? tape + 4 * (lo + threadIdx.x) : nullptr);
+        for (uint32_t k = lo + threadIdx.x + blockDim.x; k < hi; k += blockDim.x)
             line_project_one(L, L.order[k], addr, tape ? tape + 4 * k : nullptr);
         __syncthreads();
     }

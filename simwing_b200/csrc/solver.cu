@@ -439,6 +439,7 @@ void StructureImpl::setup_line_contact() {
     L.pair = dalloc<uint32_t>(owned, L.capacity);
     L.sort = dalloc<uint32_t>(owned, L.capacity);
     L.order = dalloc<uint32_t>(owned, L.capacity);
+    L.pred = dalloc<uint32_t>(owned, 4 * static_cast<size_t>(L.capacity));
     L.level_off = dalloc<uint32_t>(owned, L.capacity + 1);
     L.count = dalloc<uint32_t>(owned, 2);
     lines_host = L;
