@@ -434,7 +434,8 @@ def batched_adjoint_leg(sw, st, device, wings=32, steps=240, interval=16, group=
         for s in structures:
             s.close()
     return {"workload": f"{wings} wings, cells U{{30..50}} x 45 chordwise, line rest lengths x lognormal(0, 0.03), "
-                        f"frictionless contact plane 1 cm inside each trailing edge; {steps}-step rollout forward + backward "
+                        f"frictionless contact plane 1 cm inside each trailing edge, line-line contact "
+                        f"({LINE_RADIUS * 1000:g} mm radius, {LINE_MARGIN * 1000:g} mm margin); {steps}-step rollout forward + backward "
                         f"per wing, checkpoint every {interval} steps, {group} rollouts side by side",
             "wings": wings, "triangles_min": min(tri), "triangles_max": max(tri), "steps": steps,
             "forward_s": total_fwd, "backward_s": total_bwd,
