@@ -311,3 +311,43 @@ def test_rollout_gradient_with_line_contact(cuda_device):
     errors = {k: relative(mine[k], theirs[k]) for k in mine}
     assert all(v <= 1e-3 for v in errors.values()), errors
     s.close()
+
+
+@pytest.mark.gpu
+def test_wing_rollout_gradient_with_line_contact(cuda_device):
+    """The small wing with its pilot and line-line contact of its cascaded
+    lines (2 mm radius, 4 mm margin: candidates near every junction), a
+    16-step rollout: the calibration parameters' gradient (each line's rest
+    length, the compliance classes, the risers and the pilot mass) agrees
+    with the FP64 adjoint along the device trajectory within 1e-3."""
+    from tests.test_adjoint import calibration_parameters, payload_vector, relative, to_definition_order
+
+    d = sw.generate_wing(cells=4, chordwise=10, spanwise_per_cell=2, rib_layers=2, seed=3)
+    st = step_settings()
+    s = sw.Structure(d)
+    s.set_line_contact(0.002, 0.004)
+    for _ in range(20):
+        s.step(st, diagnostics=False)
+    state, pay = s.node_states(), payload_vector(s)
+    rng = np.random.default_rng(7)
+    target = state[:, 0, :] + rng.normal(0.0, 0.01, state[:, 0, :].shape)
+    w = np.ones(d.node_count)
+    steps = 16
+    r = sw.Rollout(s, steps, 8)
+    r.forward(st, target, w)
+    grad = r.backward()
+    r.close()
+    traj, tpay = [state], [pay]
+    for _ in range(steps - 1):
+        s.step(st, diagnostics=False)
+        traj.append(s.node_states())
+        tpay.append(payload_vector(s))
+    ref = O.rollout_gradient(s.oracle_definition(), st, steps, target, w, state=state, payload=pay,
+                             trajectory=np.array(traj), trajectory_payloads=np.array(tpay), lines=(0.002, 0.004))
+    ref["d_rest"] = to_definition_order(ref["d_rest"], s.sweep_order(abi.SWEEP_DISTANCE))
+    ref["d_comp"] = to_definition_order(ref["d_comp"], s.sweep_order(abi.SWEEP_DISTANCE))
+    ref["d_dihedral_comp"] = to_definition_order(ref["d_dihedral_comp"], s.sweep_order(abi.SWEEP_DIHEDRAL))
+    mine, theirs = calibration_parameters(d, grad), calibration_parameters(d, ref)
+    errors = {k: relative(mine[k], theirs[k]) for k in theirs}
+    assert all(v <= 1e-3 for v in errors.values()), errors
+    s.close()
