@@ -246,29 +246,33 @@ __device__ __forceinline__ void line_project_one(const LineContactDev& L, uint32
 }
 
 // Rank 0's block: the candidates' projections, level by level (line_sort
-// left them ordered by level, with the levels' offsets), each level's
-// candidates side by side.  Taping launches pass `tape` ([capacity][4] of
-// this iteration): each candidate's four end nodes before its projection,
-// at its place in that order.
+// left them ordered by level, with the levels' offsets), on the block's
+// first warp: most levels hold fewer candidates than a warp has lanes, and
+// a warp barrier between levels costs far less than a block barrier (the
+// widest levels take a few rounds of the warp instead).  Taping launches
+// pass `tape` ([capacity][4] of this iteration): each candidate's four end
+// nodes before its projection, at its place in that order.  The caller's
+// cluster barrier publishes the result.
 template <class Addr>
 __device__ void line_project(const LineContactDev& L, Addr addr, float4* tape = nullptr) {
-    const uint32_t top = L.count[1];
-    // each thread's first candidate of the next level is looked up before
-    // the current level's projections (the lists stay fixed for the substep)
+    if (threadIdx.x >= 32) return;
+    const uint32_t lane = threadIdx.x, top = L.count[1];
+    // each lane's first candidate of the next level is looked up before the
+    // current level's projections (the lists stay fixed for the substep)
     uint32_t next = ~0u;
-    if (top > 0 && L.level_off[0] + threadIdx.x < L.level_off[1]) next = L.order[L.level_off[0] + threadIdx.x];
+    if (top > 0 && L.level_off[0] + lane < L.level_off[1]) next = L.order[L.level_off[0] + lane];
     for (uint32_t lv = 0; lv < top; ++lv) {
         const uint32_t lo = L.level_off[lv], hi = L.level_off[lv + 1];
         const uint32_t cur = next;
         next = ~0u;
         if (lv + 1 < top) {
             const uint32_t nlo = L.level_off[lv + 1], nhi = L.level_off[lv + 2];
-            if (nlo + threadIdx.x < nhi) next = L.order[nlo + threadIdx.x];
+            if (nlo + lane < nhi) next = L.order[nlo + lane];
         }
-        if (cur != ~0u) line_project_one(L, cur, addr, tape ? tape + 4 * (lo + threadIdx.x) : nullptr);
-        for (uint32_t k = lo + threadIdx.x + blockDim.x; k < hi; k += blockDim.x)
+        if (cur != ~0u) line_project_one(L, cur, addr, tape ? tape + 4 * (lo + lane) : nullptr);
+        for (uint32_t k = lo + lane + 32; k < hi; k += 32)
             line_project_one(L, L.order[k], addr, tape ? tape + 4 * k : nullptr);
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -373,17 +377,19 @@ __device__ __forceinline__ void line_reverse_one(const float4 in[4], float gap_f
         g3[c] = make_float3(static_cast<float>(g[c].x), static_cast<float>(g[c].y), static_cast<float>(g[c].z));
 }
 
-// The reverse of an iteration's line-line projections, rank 0's block:
-// the taped levels from the last, each level's candidates side by side, on
-// the node adjoints (`addr` gives a node's adjoint in the cluster window).
+// The reverse of an iteration's line-line projections, on rank 0's first
+// warp: the taped levels from the last, each level's candidates side by
+// side, on the node adjoints (`addr` gives a node's adjoint in the cluster
+// window).  The caller's cluster barrier publishes the result.
 template <class Addr>
 __device__ void line_contact_reverse(const LineContactDev& L, const TapeStep& t, int it, Addr addr) {
     const uint32_t top = t.line_count[1];
     const float gap = 2.0f * L.radius;
     const float4* in_it = t.line_in + static_cast<size_t>(it) * t.line_cap * 4;
+    if (threadIdx.x >= 32) return;
     for (uint32_t lv = top; lv-- > 0;) {
         const uint32_t lo = t.line_level_off[lv], hi = t.line_level_off[lv + 1];
-        for (uint32_t k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+        for (uint32_t k = lo + threadIdx.x; k < hi; k += 32) {
             const uint32_t pr = t.line_pairs[k];
             const uint32_t s1 = L.seg[pr >> 16], s2 = L.seg[pr & 0xffffu];
             const uint32_t ad[4] = {addr(s1 & 0xffffu), addr(s1 >> 16), addr(s2 & 0xffffu), addr(s2 >> 16)};
@@ -397,7 +403,7 @@ __device__ void line_contact_reverse(const LineContactDev& L, const TapeStep& t,
             line_reverse_one(in, gap, g);
             for (int c = 0; c < 4; ++c) st_node(ad[c], make_float4(g[c].x, g[c].y, g[c].z, G[c].w));
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
