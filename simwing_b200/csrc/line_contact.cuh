@@ -380,9 +380,10 @@ __device__ __forceinline__ void line_reverse_one(const float4 in[4], float gap_f
 // The reverse of an iteration's line-line projections, on rank 0's first
 // warp: the taped levels from the last, each level's candidates side by
 // side, on the node adjoints (`addr` gives a node's adjoint in the cluster
-// window).  The caller's cluster barrier publishes the result.
+// window).  The caller's cluster barrier publishes the result.  Not
+// inlined: the reverse kernel's main loop keeps its registers.
 template <class Addr>
-__device__ void line_contact_reverse(const LineContactDev& L, const TapeStep& t, int it, Addr addr) {
+__device__ __noinline__ void line_contact_reverse(const LineContactDev& L, const TapeStep& t, int it, Addr addr) {
     const uint32_t top = t.line_count[1];
     const float gap = 2.0f * L.radius;
     const float4* in_it = t.line_in + static_cast<size_t>(it) * t.line_cap * 4;
