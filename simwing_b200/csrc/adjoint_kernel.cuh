@@ -327,7 +327,9 @@ __device__ __forceinline__ void reverse_record(const ClusterRecord& r, int kind,
 // kMaxThreads: the launch bound.  Up to 512 threads a thread has the
 // registers (128) to prefetch the next stage's record and tape entries; the
 // 768-thread instantiation (80 registers) loads them when it reaches them.
-template <int kMaxThreads>
+// kLines: the instantiation that reverses line-line contact (the others
+// carry none of its code, so their registers stay as they were).
+template <int kMaxThreads, bool kLines = false>
 __global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(const __grid_constant__ AdjointParams p) {
     constexpr bool kPrefetch = kMaxThreads <= 512;
     namespace cg = cooperative_groups;
@@ -479,7 +481,7 @@ __global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(con
             cluster.sync();
         }
         // the line-line projections followed the pilot's line iteration
-        if (I.lines) {
+        if constexpr (kLines) {
             if (me == 0)
                 line_contact_reverse(*I.lines, p.tape, it,
                                      [&](uint32_t ref) { return node_addr(ref, me, 0u, x_base); });
@@ -575,6 +577,8 @@ __global__ void __launch_bounds__(kMaxThreads) xpbd_cluster_adjoint_kernel_t(con
 
 inline constexpr auto xpbd_cluster_adjoint_kernel = &xpbd_cluster_adjoint_kernel_t<kClusterMaxThreads>;
 inline constexpr auto xpbd_cluster_adjoint_kernel_narrow = &xpbd_cluster_adjoint_kernel_t<512>;
+inline constexpr auto xpbd_cluster_adjoint_lines_kernel = &xpbd_cluster_adjoint_kernel_t<kClusterMaxThreads, true>;
+inline constexpr auto xpbd_cluster_adjoint_lines_kernel_narrow = &xpbd_cluster_adjoint_kernel_t<512, true>;
 
 }  // namespace dev
 }  // namespace swb

@@ -1055,6 +1055,8 @@ size_t dynamic_smem_limit(const cudaDeviceProp& prop) {
                           reinterpret_cast<const void*>(dev::xpbd_cluster_tape_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_kernel),
                           reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_kernel_narrow),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_lines_kernel),
+                          reinterpret_cast<const void*>(dev::xpbd_cluster_adjoint_lines_kernel_narrow),
                           reinterpret_cast<const void*>(dev::xpbd_step_kernel)}) {
         cudaFuncAttributes a{};
         if (cudaFuncGetAttributes(&a, k) == cudaSuccess) reserve = std::max(reserve, a.sharedSizeBytes + 256);
@@ -1101,7 +1103,8 @@ cudaError_t tape_kernel_launch(const cudaLaunchConfig_t& cfg, const ClusterParam
 
 cudaError_t adjoint_kernel_limits(int max_dynamic_smem, bool non_portable_cluster) {
     cudaError_t rc = cudaSuccess;
-    for (auto kernel : {dev::xpbd_cluster_adjoint_kernel, dev::xpbd_cluster_adjoint_kernel_narrow}) {
+    for (auto kernel : {dev::xpbd_cluster_adjoint_kernel, dev::xpbd_cluster_adjoint_kernel_narrow,
+                        dev::xpbd_cluster_adjoint_lines_kernel, dev::xpbd_cluster_adjoint_lines_kernel_narrow}) {
         if (rc == cudaSuccess)
             rc = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem);
         if (rc == cudaSuccess && non_portable_cluster)
@@ -1111,11 +1114,13 @@ cudaError_t adjoint_kernel_limits(int max_dynamic_smem, bool non_portable_cluste
 }
 
 // Blocks of up to 512 threads take the instantiation with that launch bound
-// (registers for the tape prefetch).
+// (registers for the tape prefetch); tapes with line-line contact (their
+// line arrays are allocated only then) the instantiation that reverses it.
 cudaError_t adjoint_kernel_launch(const cudaLaunchConfig_t& cfg, const AdjointParams& params) {
-    return cudaLaunchKernelEx(&cfg, cfg.blockDim.x <= 512 ? dev::xpbd_cluster_adjoint_kernel_narrow
-                                                          : dev::xpbd_cluster_adjoint_kernel,
-                              params);
+    const bool narrow = cfg.blockDim.x <= 512, lines = params.tape.line_count != nullptr;
+    auto kernel = lines ? (narrow ? dev::xpbd_cluster_adjoint_lines_kernel_narrow : dev::xpbd_cluster_adjoint_lines_kernel)
+                        : (narrow ? dev::xpbd_cluster_adjoint_kernel_narrow : dev::xpbd_cluster_adjoint_kernel);
+    return cudaLaunchKernelEx(&cfg, kernel, params);
 }
 
 swb_status decode_status(const int status[2], std::string& message) {
