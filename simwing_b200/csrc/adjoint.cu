@@ -265,6 +265,7 @@ struct RolloutImpl {
                 t.line_pairs = ralloc<uint32_t>(owned, kLineTapeCap);
                 t.line_level_off = ralloc<uint32_t>(owned, kLineTapeCap + 1);
                 t.line_count = ralloc<uint32_t>(owned, 2);
+                cuda_check(cudaMemsetAsync(t.line_count, 0, 2 * sizeof(uint32_t), S->stream), "memset");
                 t.line_in = ralloc<float4>(owned, it * kLineTapeCap * 4);
             }
             t.r0 = r0;

@@ -278,10 +278,17 @@ __device__ void line_project(const LineContactDev& L, Addr addr, float4* tape = 
 
 // Taping launches, rank 0's block after line_sort: the step's candidates
 // in level order, the level offsets and the counts into the tape; false
-// (and nothing taped) when they exceed its capacity.
+// when they exceed its capacity, and then the tape holds no candidate (its
+// reverse does nothing; the step's failure is reported).
 __device__ bool line_tape_step(const LineContactDev& L, const TapeStep& t) {
     const uint32_t n = min(L.count[0], L.capacity), top = L.count[1];
-    if (n > t.line_cap) return false;
+    if (n > t.line_cap) {
+        if (threadIdx.x == 0) {
+            t.line_count[0] = 0;
+            t.line_count[1] = 0;
+        }
+        return false;
+    }
     for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) t.line_pairs[k] = L.order[k];
     for (uint32_t l = threadIdx.x; l <= top; l += blockDim.x) t.line_level_off[l] = L.level_off[l];
     if (threadIdx.x == 0) {
@@ -387,7 +394,7 @@ __device__ __noinline__ void line_contact_reverse(const LineContactDev& L, const
     const uint32_t top = t.line_count[1];
     const float gap = 2.0f * L.radius;
     const float4* in_it = t.line_in + static_cast<size_t>(it) * t.line_cap * 4;
-    if (threadIdx.x >= 32) return;
+    if (threadIdx.x >= 32 || t.line_count[0] > t.line_cap || top > t.line_count[0]) return;
     for (uint32_t lv = top; lv-- > 0;) {
         const uint32_t lo = t.line_level_off[lv], hi = t.line_level_off[lv + 1];
         for (uint32_t k = lo + threadIdx.x; k < hi; k += 32) {

@@ -116,15 +116,15 @@ def test_port_leaves_pairs_alone(case):
     assert np.abs(x - x0).max() <= 1e-9 * max(1.0, np.abs(x0).max()), np.abs(x - x0).max()
 
 
-def crossing_ropes(k=6, n=12, mass=0.02, rest_scale=1.0):
+def crossing_ropes(k=6, n=12, mass=0.02, rest_scale=1.0, spacing=0.002):
     """k ropes of n nodes, each pinned at its top end, hanging slanted so
-    that all of them cross the vertical axis at mid height, 2 mm apart in
-    y: every rope overlaps every other at the start.  The cables' rest
+    that all of them cross the vertical axis at mid height, `spacing` apart
+    in y: every rope overlaps every other at the start.  The cables' rest
     lengths are rest_scale x their initial lengths."""
     nodes, cons = [], []
     for i in range(k):
         a = 0.1 * (i - 0.5 * (k - 1))
-        y = 0.002 * i
+        y = spacing * i
         top = np.array([a, y, 1.0])
         bottom = np.array([-a, y, 0.0])
         base = len(nodes)
@@ -350,4 +350,24 @@ def test_wing_rollout_gradient_with_line_contact(cuda_device):
     mine, theirs = calibration_parameters(d, grad), calibration_parameters(d, ref)
     errors = {k: relative(mine[k], theirs[k]) for k in theirs}
     assert all(v <= 1e-3 for v in errors.values()), errors
+    s.close()
+
+
+@pytest.mark.gpu
+def test_rollout_tape_capacity(cuda_device):
+    """A rollout tapes at most 4,096 line-line candidates per step: 100
+    ropes crossing within 5 mm of one another give about 18,000 in the first
+    step; the plain step and the rollout's forward take them, the backward
+    fails with SWB_CONTACT_ERROR and says why."""
+    d = crossing_ropes(k=100, n=4, spacing=0.00005)
+    st = step_settings(iterations=4)
+    s = sw.Structure(d)
+    s.set_line_contact(RADIUS, 0.002)
+    r = sw.Rollout(s, 2, 2)
+    r.forward(st, s.positions(), np.ones(s.node_count))
+    with pytest.raises(sw.ContactStepError, match="rollout's tape"):
+        r.backward()
+    r.close()
+    s.step(st, diagnostics=False)
+    assert np.isfinite(s.node_states()).all()
     s.close()
