@@ -4,17 +4,19 @@
 // Once per substep, after the prediction, every CTA of the cluster boxes
 // the segments at their predicted positions and tests the pairs of
 // segments that share no node; a pair whose boxes, widened by `reach`,
-// overlap becomes a candidate.  Rank 0's block sorts the candidates by
-// key (first segment, then second) and into levels of candidates that share
-// no node.  After every iteration rank 0's block projects the candidates
-// level by level, which gives the key-order sweep's results: the closest
-// points of the
-// two segments (the segment-segment closest-point method of Ericson, Real-
-// Time Collision Detection, 5.1.9) pushed apart along their separation to
-// 2 x radius, rigidly, the correction shared by the four end nodes in
-// proportion to their inverse masses and barycentric weights.  Parity is
-// pinned to the FP64 port's restatement (the reference's structural step
-// has no line-line contact: it rejects segment contact).
+// overlap becomes a candidate.  Rank 0's block sorts the candidates by key
+// (first segment, then second) and into levels of candidates that share
+// no node.  After every iteration rank 0's first warp projects the
+// candidates level by level, which gives the key-order sweep's results:
+// the closest points of the two segments (the segment-segment
+// closest-point method of Ericson, Real-Time Collision Detection, 5.1.9)
+// pushed apart along their separation to 2 x radius, rigidly, the
+// correction shared by the four end nodes in proportion to their inverse
+// masses and barycentric weights.  Rollouts tape each step's candidates
+// and the projections' inputs, and the reverse kernel runs each
+// projection's vector-Jacobian product.  Parity is pinned to the FP64
+// port's restatement (the reference's structural step has no line-line
+// contact: it rejects segment contact).
 #pragma once
 
 #include <cooperative_groups.h>
