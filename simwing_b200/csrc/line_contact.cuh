@@ -66,7 +66,7 @@ __device__ __forceinline__ SegmentClosest segment_closest(float3 p1, float3 d1, 
 // The substep's candidate pairs (every thread of every CTA; a cluster
 // barrier inside, and one must follow before rank 0 sorts them).  The pair
 // tests are spread evenly: the triangle of pairs is cut into runs of equal
-// length, one per thread.
+// length, one per warp, whose lanes take the run's pairs in turn.
 template <class Addr>
 __device__ void line_broadphase(const LineContactDev& L, uint32_t me, uint32_t ctas,
                                 cooperative_groups::cluster_group& cluster, Addr addr, int* status) {
@@ -80,37 +80,49 @@ __device__ void line_broadphase(const LineContactDev& L, uint32_t me, uint32_t c
     }
     cluster.sync();
     // the triangle of pairs (i < j), row by row, cut into equal runs, one
-    // per thread of the cluster
+    // per warp of the cluster; a warp's lanes take its pairs in turn, so
+    // that they read neighbouring boxes together
     const uint64_t S = L.segments, P = S * (S - 1) / 2;
-    const uint64_t chunk = (P + stride - 1) / stride;
-    const uint64_t p0 = static_cast<uint64_t>(gt) * chunk, p1 = min(P, p0 + chunk);
-    if (p0 >= p1) return;
+    const uint64_t warps = stride / 32, chunk = (P + warps - 1) / warps;
+    const uint64_t run = gt / 32, lane = gt % 32;
+    const uint64_t p0 = run * chunk + lane, end = min(P, run * chunk + chunk);
+    if (p0 >= end) return;
     auto row_start = [&](uint64_t i) { return i * (2 * S - i - 1) / 2; };
     const double b = 2.0 * static_cast<double>(S) - 1.0;
     uint64_t i = static_cast<uint64_t>(max(0.0, floor((b - sqrt(max(0.0, b * b - 8.0 * static_cast<double>(p0)))) * 0.5)));
     i = min(i, S - 2);
     while (i > 0 && row_start(i) > p0) --i;
     while (i + 2 < S && row_start(i + 1) <= p0) ++i;
-    uint64_t j = i + 1 + (p0 - row_start(i)), left = p1 - p0;
-    while (left > 0) {
-        const float4 lo = __ldcg(L.box + 2 * i), hi = __ldcg(L.box + 2 * i + 1);
-        const uint2 ni = L.seg_nodes[i];
-        const uint64_t jend = min(S, j + left);
-        left -= jend - j;
-#pragma unroll 4
-        for (; j < jend; ++j) {
-            const float4 lo2 = __ldcg(L.box + 2 * j), hi2 = __ldcg(L.box + 2 * j + 1);
-            if (lo.x > hi2.x || lo2.x > hi.x || lo.y > hi2.y || lo2.y > hi.y || lo.z > hi2.z || lo2.z > hi.z) continue;
+    uint64_t j = i + 1 + (p0 - row_start(i));
+    float4 lo = __ldcg(L.box + 2 * i), hi = __ldcg(L.box + 2 * i + 1);
+    uint2 ni = L.seg_nodes[i];
+    for (uint64_t p = p0; p < end; p += 32) {
+        const float4 lo2 = __ldcg(L.box + 2 * j), hi2 = __ldcg(L.box + 2 * j + 1);
+        if (!(lo.x > hi2.x || lo2.x > hi.x || lo.y > hi2.y || lo2.y > hi.y || lo.z > hi2.z || lo2.z > hi.z)) {
             const uint2 nj = L.seg_nodes[j];
-            if (ni.x == nj.x || ni.x == nj.y || ni.y == nj.x || ni.y == nj.y) continue;
-            const uint32_t k = atomicAdd(L.count, 1u);
-            if (k < L.capacity)
-                L.pair[k] = (static_cast<uint32_t>(i) << 16) | static_cast<uint32_t>(j);
-            else
-                contact_fail(status, kContactLinePairs);
+            if (!(ni.x == nj.x || ni.x == nj.y || ni.y == nj.x || ni.y == nj.y)) {
+                const uint32_t k = atomicAdd(L.count, 1u);
+                if (k < L.capacity)
+                    L.pair[k] = (static_cast<uint32_t>(i) << 16) | static_cast<uint32_t>(j);
+                else
+                    contact_fail(status, kContactLinePairs);
+            }
         }
-        ++i;
-        j = i + 1;
+        // the pair 32 places on, across row ends
+        j += 32;
+        bool moved = false;
+        while (j >= S && i + 2 < S) {
+            const uint64_t over = j - S;
+            ++i;
+            j = i + 1 + over;
+            moved = true;
+        }
+        if (j >= S) break;  // past the last pair
+        if (moved) {
+            lo = __ldcg(L.box + 2 * i);
+            hi = __ldcg(L.box + 2 * i + 1);
+            ni = L.seg_nodes[i];
+        }
     }
 }
 
